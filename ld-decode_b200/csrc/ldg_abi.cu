@@ -1,0 +1,497 @@
+// C ABI of the ldgpu demodulator / TBC (declared in include/ldgpu.h).
+//
+// A context owns the device copies of one RFDecode configuration: filter
+// half spectra (float32), twiddle tables, the sinc table, the demodulator's
+// parked-spectrum scratch and a staging arena for callers that pass host
+// buffers.  Device buffers passed in are used in place and the call only
+// enqueues work; host buffers make the call copy in, run and copy out
+// synchronously (the plain, one-block-at-a-time form the reference's
+// DemodCache workers use).
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ldg_demod.cuh"
+#include "ldg_fft.cuh"
+#include "ldg_tbc.cuh"
+#include "ldgpu.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define LDG_CK(call)                                                                          \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(LDG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+struct ldg_ctx {
+    int device = 0;
+    int system = LDG_NTSC;
+    int blocklen = ldg::kN;
+    double fs_hz = 40e6;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    float2* d_filter[LDG_NFILTERS] = {};
+    float2* d_audio[2] = {};
+    int a_lowbin[2] = {0, 0};
+    double a_rate[2] = {0, 0};
+    double a_low[2] = {0, 0};
+    float2* d_tw = nullptr;  // 256 hi + 128 lo
+    float* d_lut = nullptr;
+    float2* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    char* d_stage = nullptr;
+    size_t stage_bytes = 0;
+    ldg::TbcField* d_fields = nullptr;
+    int fields_cap = 0;
+    double* d_seg = nullptr;
+    size_t seg_cap = 0;
+    double* d_ll = nullptr;
+    size_t ll_cap = 0;
+    int* d_status = nullptr;
+    std::mutex mu;
+};
+
+namespace {
+
+int grow(void** p, size_t* cap, size_t need) {
+    if (need <= *cap) return LDG_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    size_t sz = need + need / 4;
+    LDG_CK(cudaMalloc(p, sz));
+    *cap = sz;
+    return LDG_OK;
+}
+
+bool slice_ok(const ldg_slice& s, int n) {
+    return s.len >= 0 && s.start >= 0 && (s.len == 0 || (long long)s.start + s.len <= n) &&
+           s.roll >= 0 && s.roll < n;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ldg_abi_version(void) { return LDG_ABI_VERSION; }
+
+const char* ldg_last_error(void) { return g_err.c_str(); }
+
+int ldg_device_count(int32_t* count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    if (count) *count = n;
+    return LDG_OK;
+}
+
+int ldg_ctx_create(ldg_ctx** out, int32_t device, int32_t system, int32_t blocklen, double fs_hz) {
+    if (!out) return fail(LDG_ERR_ARG, "ldg_ctx_create: out is NULL");
+    *out = nullptr;
+    if (system != LDG_NTSC && system != LDG_PAL) return fail(LDG_ERR_ARG, "ldg_ctx_create: system must be NTSC or PAL");
+    if (blocklen != ldg::kN)
+        return fail(LDG_ERR_UNSUPPORTED, "ldg_ctx_create: only blocklen 32768 (the reference BLOCKSIZE) is supported");
+    if (!(fs_hz > 0)) return fail(LDG_ERR_ARG, "ldg_ctx_create: fs_hz must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(LDG_ERR_CUDA, "ldg_ctx_create: no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return fail(LDG_ERR_ARG, "ldg_ctx_create: bad device index");
+    DeviceGuard g(device);
+    ldg_ctx* c = new ldg_ctx();
+    c->device = device;
+    c->system = system;
+    c->blocklen = blocklen;
+    c->fs_hz = fs_hz;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(LDG_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    // twiddles W_N^k = exp(-2 pi i k/N) in FP64, stored FP32
+    std::vector<float2> tw(ldg::kTwHi + ldg::kTwLo);
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int a = 0; a < ldg::kTwHi; ++a) {
+        const double ang = -two_pi * (double)(128 * a) / ldg::kN;
+        tw[a] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+    for (int b = 0; b < ldg::kTwLo; ++b) {
+        const double ang = -two_pi * (double)b / ldg::kN;
+        tw[ldg::kTwHi + b] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+    if (cudaMalloc(&c->d_tw, tw.size() * sizeof(float2)) != cudaSuccess ||
+        cudaMemcpy(c->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess || cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
+        const std::string msg = cudaGetErrorString(cudaGetLastError());
+        ldg_ctx_destroy(c);
+        return fail(LDG_ERR_CUDA, "ldg_ctx_create: " + msg);
+    }
+    *out = c;
+    return LDG_OK;
+}
+
+void ldg_ctx_destroy(ldg_ctx* c) {
+    if (!c) return;
+    DeviceGuard g(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& f : c->d_filter) cudaFree(f);
+    for (auto& a : c->d_audio) cudaFree(a);
+    cudaFree(c->d_tw);
+    cudaFree(c->d_lut);
+    cudaFree(c->d_scratch);
+    cudaFree(c->d_stage);
+    cudaFree(c->d_fields);
+    cudaFree(c->d_seg);
+    cudaFree(c->d_ll);
+    cudaFree(c->d_status);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int ldg_set_filter(ldg_ctx* c, int32_t which, const double* reim, int64_t nbins) {
+    if (!c || !reim) return fail(LDG_ERR_ARG, "ldg_set_filter: NULL argument");
+    if (which < 0 || which >= LDG_NFILTERS) return fail(LDG_ERR_ARG, "ldg_set_filter: bad filter slot");
+    if (nbins != ldg::kM + 1) return fail(LDG_ERR_ARG, "ldg_set_filter: nbins must be blocklen/2+1");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    std::vector<float2> h(nbins);
+    for (int64_t k = 0; k < nbins; ++k) h[k] = make_float2((float)reim[2 * k], (float)reim[2 * k + 1]);
+    if (!c->d_filter[which]) LDG_CK(cudaMalloc(&c->d_filter[which], nbins * sizeof(float2)));
+    LDG_CK(cudaStreamSynchronize(c->stream));
+    LDG_CK(cudaMemcpy(c->d_filter[which], h.data(), nbins * sizeof(float2), cudaMemcpyHostToDevice));
+    return LDG_OK;
+}
+
+int ldg_set_audio(ldg_ctx* c, int32_t ch, int32_t lowbin, int32_t nbins, const double* filt1, double a1_freq,
+                  double low_freq) {
+    if (!c || !filt1) return fail(LDG_ERR_ARG, "ldg_set_audio: NULL argument");
+    if (ch < 0 || ch > 1) return fail(LDG_ERR_ARG, "ldg_set_audio: channel must be 0 or 1");
+    if (nbins != 1024) return fail(LDG_ERR_UNSUPPORTED, "ldg_set_audio: only 1024-bin audio bands are supported");
+    if (lowbin < 1 || lowbin + nbins / 2 >= ldg::kM) return fail(LDG_ERR_ARG, "ldg_set_audio: band outside the spectrum");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    std::vector<float2> h(nbins / 2 + 1);
+    for (int k = 0; k <= nbins / 2; ++k) h[k] = make_float2((float)filt1[2 * k], (float)filt1[2 * k + 1]);
+    if (!c->d_audio[ch]) LDG_CK(cudaMalloc(&c->d_audio[ch], h.size() * sizeof(float2)));
+    LDG_CK(cudaStreamSynchronize(c->stream));
+    LDG_CK(cudaMemcpy(c->d_audio[ch], h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    c->a_lowbin[ch] = lowbin;
+    c->a_rate[ch] = a1_freq;
+    c->a_low[ch] = low_freq;
+    return LDG_OK;
+}
+
+int ldg_set_sinc_lut(ldg_ctx* c, const float* lut, int32_t rows, int32_t taps) {
+    if (!c || !lut) return fail(LDG_ERR_ARG, "ldg_set_sinc_lut: NULL argument");
+    if (rows != 65537 || taps != 16) return fail(LDG_ERR_UNSUPPORTED, "ldg_set_sinc_lut: table must be 65537 x 16");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    const size_t bytes = (size_t)rows * taps * sizeof(float);
+    if (!c->d_lut) LDG_CK(cudaMalloc(&c->d_lut, bytes));
+    LDG_CK(cudaStreamSynchronize(c->stream));
+    LDG_CK(cudaMemcpy(c->d_lut, lut, bytes, cudaMemcpyHostToDevice));
+    return LDG_OK;
+}
+
+int ldg_demod_scratch_bytes(ldg_ctx* c, int64_t nblocks, int64_t* bytes) {
+    if (!c || !bytes) return fail(LDG_ERR_ARG, "ldg_demod_scratch_bytes: NULL argument");
+    const long long grid = nblocks < c->sms ? nblocks : c->sms;
+    *bytes = (int64_t)(grid * ldg::kScratchPerCta);
+    return LDG_OK;
+}
+
+int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
+    if (!c || !a) return fail(LDG_ERR_ARG, "ldg_demod_blocks: NULL argument");
+    if (!a->in) return fail(LDG_ERR_ARG, "demodblock called without raw or FFT data");
+    if (a->in_kind != LDG_IN_INT16 && a->in_kind != LDG_IN_FLOAT32)
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks: in_kind must be LDG_IN_INT16 or LDG_IN_FLOAT32");
+    if (a->nblocks < 0 || a->in_stride < 0) return fail(LDG_ERR_ARG, "ldg_demod_blocks: negative size");
+    if (a->nblocks > (1LL << 30)) return fail(LDG_ERR_ARG, "ldg_demod_blocks: too many blocks");
+    const int N = ldg::kN;
+    if (!slice_ok(a->video, N) || !slice_ok(a->rfhpf, N) || !slice_ok(a->efm, N) || !slice_ok(a->audio, 1024))
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks: output slice outside the block");
+    if (a->roll_05 < 0 || a->roll_05 >= N || a->roll_burst < 0 || a->roll_burst >= N)
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks: roll outside the block");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->d_filter[LDG_F_VIDEO_G]) return fail(LDG_ERR_STATE, "ldg_demod_blocks: RFVideo filter not set");
+    const bool want_video[4] = {a->out_demod != nullptr, a->out_05 != nullptr, a->out_burst != nullptr,
+                                a->out_pilot != nullptr};
+    const int fslot[4] = {LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT};
+    for (int o = 0; o < 4; ++o)
+        if (want_video[o] && !c->d_filter[fslot[o]]) return fail(LDG_ERR_STATE, "ldg_demod_blocks: video filter not set");
+    if (a->out_rfhpf && !c->d_filter[LDG_F_RFHPF]) return fail(LDG_ERR_STATE, "ldg_demod_blocks: rfhpf filter not set");
+    if (a->out_efm && !c->d_filter[LDG_F_EFM]) return fail(LDG_ERR_STATE, "ldg_demod_blocks: EFM filter not set");
+    const bool audio = a->out_audio_left || a->out_audio_right;
+    if (audio && (!c->d_audio[0] || !c->d_audio[1])) return fail(LDG_ERR_STATE, "ldg_demod_blocks: audio bands not set");
+    if (a->nblocks == 0) return LDG_OK;
+
+    DeviceGuard g(c->device);
+    cudaStream_t st = a->stream ? (cudaStream_t)a->stream : c->stream;
+    const long long nb = a->nblocks;
+    const int grid = (int)(nb < c->sms ? nb : c->sms);
+    int rc = grow((void**)&c->d_scratch, &c->scratch_bytes, (size_t)grid * ldg::kScratchPerCta);
+    if (rc) return rc;
+
+    // host/device placement of every buffer; host ones go through the arena
+    const size_t esz = a->in_kind == LDG_IN_INT16 ? 2 : 4;
+    const size_t in_elems = (size_t)((nb - 1) * a->in_stride + N);
+    struct Buf { void* user; size_t bytes; size_t off; bool host; };
+    Buf bufs[10];
+    int nbuf = 0;
+    auto add = [&](void* p, size_t bytes) -> int {
+        const int i = nbuf++;
+        bufs[i].user = p;
+        bufs[i].bytes = bytes;
+        bufs[i].host = p && !is_device_ptr(p);
+        bufs[i].off = 0;
+        return i;
+    };
+    const int i_in = add(const_cast<void*>(a->in), in_elems * esz);
+    float* vids[4] = {a->out_demod, a->out_05, a->out_burst, a->out_pilot};
+    int i_vid[4];
+    for (int o = 0; o < 4; ++o) i_vid[o] = add(vids[o], (size_t)nb * a->video.len * 4);
+    const int i_raw = add(a->out_raw, (size_t)nb * a->video.len * 4);
+    const int i_hp = add(a->out_rfhpf, (size_t)nb * a->rfhpf.len * 4);
+    const int i_efm = add(a->out_efm, (size_t)nb * a->efm.len * 2);
+    const int i_al = add(a->out_audio_left, (size_t)nb * a->audio.len * 4);
+    const int i_ar = add(a->out_audio_right, (size_t)nb * a->audio.len * 4);
+    size_t stage = 0;
+    bool any_host = false;
+    for (int i = 0; i < nbuf; ++i) {
+        if (bufs[i].host && bufs[i].bytes) {
+            bufs[i].off = stage;
+            stage += (bufs[i].bytes + 255) & ~size_t(255);
+            any_host = true;
+        }
+    }
+    if (stage) {
+        rc = grow((void**)&c->d_stage, &c->stage_bytes, stage);
+        if (rc) return rc;
+    }
+    auto dev = [&](int i) -> void* {
+        if (!bufs[i].user) return nullptr;
+        return bufs[i].host ? (void*)(c->d_stage + bufs[i].off) : bufs[i].user;
+    };
+    if (bufs[i_in].host) LDG_CK(cudaMemcpyAsync(dev(i_in), a->in, bufs[i_in].bytes, cudaMemcpyHostToDevice, st));
+
+    ldg::DemodParams p;
+    memset(&p, 0, sizeof(p));
+    p.in = dev(i_in);
+    p.in_kind = a->in_kind;
+    p.in_stride = a->in_stride;
+    p.nblocks = (int)nb;
+    p.fs_hz = (float)c->fs_hz;
+    p.f_rfhpf = c->d_filter[LDG_F_RFHPF];
+    p.f_g = c->d_filter[LDG_F_VIDEO_G];
+    for (int o = 0; o < 4; ++o) {
+        p.f_video[o] = c->d_filter[fslot[o]];
+        p.o_video[o] = (float*)dev(i_vid[o]);
+    }
+    p.f_efm = c->d_filter[LDG_F_EFM];
+    p.o_raw = (float*)dev(i_raw);
+    p.o_rfhpf = a->rfhpf.len ? (float*)dev(i_hp) : nullptr;
+    p.o_efm = a->efm.len ? (int16_t*)dev(i_efm) : nullptr;
+    p.s_video = {a->video.start, a->video.len, 0};
+    if (a->video.len == 0)
+        for (int o = 0; o < 4; ++o) p.o_video[o] = nullptr;
+    if (a->video.len == 0) p.o_raw = nullptr;
+    p.roll[ldg::OUT_DEMOD] = 0;
+    p.roll[ldg::OUT_05] = a->roll_05;
+    p.roll[ldg::OUT_BURST] = a->roll_burst;
+    p.roll[ldg::OUT_PILOT] = 0;
+    p.s_rfhpf = {a->rfhpf.start, a->rfhpf.len, 0};
+    p.s_efm = {a->efm.start, a->efm.len, 0};
+    p.audio = audio && a->audio.len > 0;
+    for (int ch = 0; ch < 2; ++ch) {
+        p.a_lowbin[ch] = c->a_lowbin[ch];
+        p.a_filt1[ch] = c->d_audio[ch];
+        p.a_low[ch] = (float)c->a_low[ch];
+    }
+    p.a_rate = (float)c->a_rate[0];
+    p.o_audio[0] = (float*)dev(i_al);
+    p.o_audio[1] = (float*)dev(i_ar);
+    p.s_audio = {a->audio.start, a->audio.len, 0};
+    p.scratch = c->d_scratch;
+    p.tw_hi = c->d_tw;
+    p.tw_lo = c->d_tw + ldg::kTwHi;
+
+    cudaError_t e = ldg::launch_demod(p, grid, st);
+    if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("demod launch: ") + cudaGetErrorString(e));
+    if (any_host) {
+        for (int i = 1; i < nbuf; ++i)
+            if (bufs[i].host && bufs[i].bytes)
+                LDG_CK(cudaMemcpyAsync(bufs[i].user, dev(i), bufs[i].bytes, cudaMemcpyDeviceToHost, st));
+        LDG_CK(cudaStreamSynchronize(st));
+    }
+    return LDG_OK;
+}
+
+int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, void* stream) {
+    if (!c || (!fields && nfields)) return fail(LDG_ERR_ARG, "ldg_tbc_fields: NULL argument");
+    if (nfields < 0) return fail(LDG_ERR_ARG, "ldg_tbc_fields: negative field count");
+    if (nfields == 0) return LDG_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->d_lut) return fail(LDG_ERR_STATE, "ldg_tbc_fields: sinc table not set");
+    size_t ll_total = 0, seg_total = 0;
+    long long max_nout = 0;
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_tbc_field& f = fields[i];
+        if (!f.buf || !f.linelocs) return fail(LDG_ERR_ARG, "ldg_tbc_fields: NULL buffer");
+        if (f.nlines < 2 || f.nlines > 513) return fail(LDG_ERR_ARG, "ldg_tbc_fields: nlines must be in [2, 513]");
+        if (f.outwidth <= 0 || f.linesout <= 0 || f.outlinecount <= 0 || f.lineoffset < 0 || f.buf_len <= 0)
+            return fail(LDG_ERR_ARG, "ldg_tbc_fields: bad field geometry");
+        if (!(f.inlinelen > 0) || !(f.outlinelen > 0) || !(f.hz_ire != 0))
+            return fail(LDG_ERR_ARG, "ldg_tbc_fields: bad line length or level");
+        ll_total += f.nlines;
+        seg_total += f.nlines - 1;
+        const long long n = (long long)f.linesout * f.outwidth;
+        if (n > max_nout) max_nout = n;
+    }
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    int rc = grow((void**)&c->d_ll, &c->ll_cap, ll_total * sizeof(double));
+    if (rc) return rc;
+    rc = grow((void**)&c->d_seg, &c->seg_cap, seg_total * sizeof(double));
+    if (rc) return rc;
+    if (nfields > c->fields_cap) {
+        cudaFree(c->d_fields);
+        c->d_fields = nullptr;
+        c->fields_cap = 0;
+        LDG_CK(cudaMalloc(&c->d_fields, nfields * sizeof(ldg::TbcField)));
+        c->fields_cap = nfields;
+    }
+    // staging for host buffers / outputs
+    std::vector<ldg::TbcField> h(nfields);
+    std::vector<double> lls(ll_total);
+    size_t stage = 0;
+    struct Host { size_t buf_off, f32_off, u16_off; bool buf, f32, u16; };
+    std::vector<Host> hs(nfields);
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_tbc_field& f = fields[i];
+        const size_t nout = (size_t)f.linesout * f.outwidth;
+        Host& x = hs[i];
+        x.buf = !is_device_ptr(f.buf);
+        x.f32 = f.out_f32 && !is_device_ptr(f.out_f32);
+        x.u16 = f.out_u16 && !is_device_ptr(f.out_u16);
+        auto take = [&](size_t bytes) { size_t o = stage; stage += (bytes + 255) & ~size_t(255); return o; };
+        x.buf_off = x.buf ? take((size_t)f.buf_len * 4) : 0;
+        x.f32_off = x.f32 ? take(nout * 4) : 0;
+        x.u16_off = x.u16 ? take(nout * 2) : 0;
+    }
+    bool any_host = stage > 0;
+    if (stage) {
+        rc = grow((void**)&c->d_stage, &c->stage_bytes, stage);
+        if (rc) return rc;
+    }
+    size_t llo = 0, sego = 0;
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_tbc_field& f = fields[i];
+        ldg::TbcField& d = h[i];
+        const Host& x = hs[i];
+        if (is_device_ptr(f.linelocs)) {
+            LDG_CK(cudaMemcpyAsync(c->d_ll + llo, f.linelocs, f.nlines * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        } else {
+            memcpy(lls.data() + llo, f.linelocs, f.nlines * sizeof(double));
+        }
+        d.buf = x.buf ? (const float*)(c->d_stage + x.buf_off) : f.buf;
+        if (x.buf) LDG_CK(cudaMemcpyAsync((void*)d.buf, f.buf, (size_t)f.buf_len * 4, cudaMemcpyHostToDevice, st));
+        d.buf_len = f.buf_len;
+        d.linelocs = c->d_ll + llo;
+        d.nlines = f.nlines;
+        d.lineoffset = f.lineoffset;
+        d.outwidth = f.outwidth;
+        d.linesout = f.linesout;
+        d.nwow = (long long)(f.outlinecount + f.lineoffset + 1) * (long long)f.outlinelen;
+        d.coord_f32 = f.coord_f32;
+        d.inlinelen = f.inlinelen;
+        d.outscale = f.inlinelen / f.outlinelen;
+        d.u16_scale = f.out_scale / f.hz_ire;
+        d.u16_offset = f.output_zero - f.vsync_ire * f.out_scale - f.ire0 * d.u16_scale;
+        d.seg_level = c->d_seg + sego;
+        d.status = c->d_status;
+        d.out_f32 = x.f32 ? (float*)(c->d_stage + x.f32_off) : f.out_f32;
+        d.out_u16 = x.u16 ? (uint16_t*)(c->d_stage + x.u16_off) : f.out_u16;
+        llo += f.nlines;
+        sego += f.nlines - 1;
+    }
+    // linelocs given in host memory: one copy for all of them (device ones were copied above)
+    {
+        size_t o = 0;
+        for (int i = 0; i < nfields; ++i) {
+            if (!is_device_ptr(fields[i].linelocs))
+                LDG_CK(cudaMemcpyAsync(c->d_ll + o, lls.data() + o, fields[i].nlines * sizeof(double),
+                                       cudaMemcpyHostToDevice, st));
+            o += fields[i].nlines;
+        }
+    }
+    LDG_CK(cudaMemcpyAsync(c->d_fields, h.data(), nfields * sizeof(ldg::TbcField), cudaMemcpyHostToDevice, st));
+    cudaError_t e = ldg::launch_tbc(c->d_fields, nfields, max_nout, c->d_lut, 15.0, st);
+    if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
+    if (any_host) {
+        for (int i = 0; i < nfields; ++i) {
+            const size_t nout = (size_t)fields[i].linesout * fields[i].outwidth;
+            if (hs[i].f32) LDG_CK(cudaMemcpyAsync(fields[i].out_f32, h[i].out_f32, nout * 4, cudaMemcpyDeviceToHost, st));
+            if (hs[i].u16) LDG_CK(cudaMemcpyAsync(fields[i].out_u16, h[i].out_u16, nout * 2, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    // the host copies of h/lls must stay alive until the async copies are done
+    LDG_CK(cudaStreamSynchronize(st));
+    int status = 0;
+    LDG_CK(cudaMemcpy(&status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) {
+        LDG_CK(cudaMemset(c->d_status, 0, sizeof(int)));
+        if (status & ldg::LDG_TBC_BAD_LINES) return fail(LDG_ERR_ARG, "ldg_tbc_fields: too many lines for the wow statistics");
+        return fail(LDG_ERR_RANGE, "ldg_tbc_fields: a resampling tap fell outside the field buffer (those pixels are 0)");
+    }
+    (void)any_host;
+    return LDG_OK;
+}
+
+int ldg_synchronize(ldg_ctx* c) {
+    if (!c) return fail(LDG_ERR_ARG, "ldg_synchronize: NULL context");
+    DeviceGuard g(c->device);
+    LDG_CK(cudaStreamSynchronize(c->stream));
+    return LDG_OK;
+}
+
+}  // extern "C"

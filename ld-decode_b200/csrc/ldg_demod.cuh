@@ -1,0 +1,63 @@
+// Parameters of the fused per-block RF demodulator kernel.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ldg {
+
+// Real-output spectra applied to the demodulated block (order fixed).
+enum VideoOut { OUT_DEMOD = 0, OUT_05, OUT_BURST, OUT_PILOT, OUT_NVIDEO };
+
+struct OutSlice {
+    int start;  // first sample of the N-point block that is stored
+    int len;    // samples stored per block (0: output not requested)
+    int roll;   // value at n is taken from sample (n + roll) mod N
+};
+
+struct DemodParams {
+    // input: block b's first sample is in + b * in_stride (elements)
+    const void* in;
+    int in_kind;          // 0 int16, 1 float32
+    long long in_stride;
+    int nblocks;
+
+    float fs_hz;          // input sample rate
+    // half spectra, bins 0..N/2 (float2[N/2+1]); G = RFVideo * MTF^m
+    const float2* f_rfhpf;
+    const float2* f_g;
+    const float2* f_video[OUT_NVIDEO];
+    const float2* f_efm;
+
+    // outputs (nullptr: not requested); block b writes at ptr + b * len
+    float* o_raw;         // demod_raw
+    float* o_video[OUT_NVIDEO];
+    float* o_rfhpf;
+    int16_t* o_efm;
+    OutSlice s_video;     // raw/demod/05/burst/pilot share start/len
+    int roll[OUT_NVIDEO];
+    OutSlice s_rfhpf;
+    OutSlice s_efm;
+
+    // analog audio (two channels)
+    int audio;            // 0/1
+    int a_lowbin[2];
+    const float2* a_filt1[2];  // 513 weights per channel (bins 0..512)
+    float a_rate;         // sample rate of the decimated band (a1_freq)
+    float a_low[2];       // low_freq added back per channel
+    float* o_audio[2];
+    OutSlice s_audio;     // over the 1024-sample band output
+
+    // per-CTA global scratch (2 * N/2 float2 per CTA), L2 resident
+    float2* scratch;
+    const float2* tw_hi;
+    const float2* tw_lo;
+};
+
+// Dynamic shared memory the kernel needs.
+constexpr int kSmemFloat2 = (16384 + 1024) + 2 * (1024 + 64) + 256 + 128;
+constexpr size_t kSmemBytes = size_t(kSmemFloat2) * 8;
+constexpr size_t kScratchPerCta = size_t(2) * 16384 * 8;
+
+cudaError_t launch_demod(const DemodParams& p, int grid, cudaStream_t stream);
+
+}  // namespace ldg

@@ -1,0 +1,33 @@
+// Device-side descriptor of one field for the TBC kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ldg {
+
+enum { LDG_TBC_BAD_LINES = 1, LDG_TBC_OUT_OF_RANGE = 2 };
+
+struct TbcField {
+    const float* buf;
+    long long buf_len;
+    const double* linelocs;
+    int nlines;
+    int lineoffset;
+    int outwidth;
+    int linesout;
+    long long nwow;      // pixels in the wow statistics: (outlinecount+lineoffset+1)*outlinelen
+    int coord_f32;
+    double inlinelen;
+    double outscale;     // inlinelen / outlinelen
+    double u16_scale;    // out_scale / hz_ire
+    double u16_offset;   // output_zero - vsync_ire*out_scale - ire0*u16_scale
+    double* seg_level;   // nlines-1 level-adjust factors (device scratch)
+    int* status;         // LDG_TBC_* bits
+    float* out_f32;
+    uint16_t* out_u16;
+};
+
+cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout, const float* lut,
+                       double threshold_mult, cudaStream_t stream);
+
+}  // namespace ldg

@@ -1,0 +1,156 @@
+"""Field: per-field line locations and time-base correction.
+
+Mirrors lddecode.core.Field / FieldNTSC / FieldPAL (lddecode/core.py:
+1587-3495).  `downscale()` keeps the reference signature
+(core.py:2626-2722) and returns (dsout, dsaudio, efmout); the resampling
+(computewow_scaled + scale_field + hz_to_output_array) runs on the GPU
+through ldg_tbc_fields.  The sync / line-location logic (process()) is the
+host restatement in ldgpu.linelocs.
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import lib as L
+from .linelocs import FieldLogic, FieldLogicNTSC, FieldLogicPAL
+
+
+def tbc_descriptor(rf, buf, linelocs, lineoffset, outwidth, linesout, outlinecount, levels,
+                   out_u16=None, out_f32=None, coord_f32=False, buf_len=None):
+    """Fill an ldg_tbc_field from numpy arrays or raw device pointers.
+
+    `levels` = (ire0, hz_ire, vsync_ire, out_scale, output_zero)."""
+    d = L.TbcField()
+    d.buf = buf if isinstance(buf, int) else buf.ctypes.data
+    d.buf_len = int(buf_len if buf_len is not None else len(buf))
+    d.linelocs = linelocs if isinstance(linelocs, int) else linelocs.ctypes.data
+    d.nlines = int(len(linelocs)) if not isinstance(linelocs, int) else 0
+    d.lineoffset = int(lineoffset)
+    d.outwidth = int(outwidth)
+    d.linesout = int(linesout)
+    d.outlinecount = int(outlinecount)
+    d.coord_f32 = 1 if coord_f32 else 0
+    d.inlinelen = float(rf.linelen)
+    d.outlinelen = float(rf.SysParams["outlinelen"])
+    d.ire0, d.hz_ire, d.vsync_ire, d.out_scale, d.output_zero = [float(v) for v in levels]
+    d.out_f32 = None if out_f32 is None else (out_f32 if isinstance(out_f32, int) else out_f32.ctypes.data)
+    d.out_u16 = None if out_u16 is None else (out_u16 if isinstance(out_u16, int) else out_u16.ctypes.data)
+    return d
+
+
+def tbc_fields(rf, descs, stream=None):
+    """Run ldg_tbc_fields on a list of descriptors."""
+    rf._load_lut()
+    arr = (L.TbcField * len(descs))(*descs)
+    L.check(rf._ctx._lib.ldg_tbc_fields(rf._ctx.handle, arr, len(descs), stream))
+
+
+class Field(FieldLogic):
+    """A decoded field (core.py:1587-1635 constructor arguments)."""
+
+    # coordinates rounded to float32 as the reference does (utils.py:160);
+    # False keeps them in FP64 (the accuracy target)
+    coord_f32 = False
+
+    def levels(self):
+        return (self.rf.DecoderParams["ire0"], self.rf.DecoderParams["hz_ire"],
+                self.rf.DecoderParams["vsync_ire"], self.out_scale, self.rf.SysParams["outputZero"])
+
+    def hz_to_output(self, input):
+        """core.py:1714-1734 (array path: same arithmetic as the GPU)."""
+        ire0, hz_ire, vsync_ire, out_scale, ozero = self.levels()
+        if isinstance(input, np.ndarray):
+            scale = out_scale / hz_ire
+            offset = ozero - vsync_ire * out_scale - ire0 * scale
+            v = input.astype(np.float64) * scale + offset + 0.5
+            return np.clip(v, 0, 65535).astype(np.uint16)
+        reduced = (input - ire0) / hz_ire
+        reduced -= vsync_ire
+        return np.uint16(np.clip((reduced * out_scale) + ozero, 0, 65535) + 0.5)
+
+    def computewow_scaled(self):
+        """Host FP64 restatement of core.py:2591-2623 (the GPU recomputes the
+        same values internally; this is for callers that want the arrays)."""
+        act = np.asarray(self.linelocs, dtype=np.float64)
+        n = len(act)
+        exp = np.array([i * self.inlinelen for i in range(n)], dtype=np.float64)
+        nout = self.outlinecount * self.outlinelen + (self.lineoffset + 1) * self.outlinelen
+        x = np.arange(nout) * (self.inlinelen / self.outlinelen)
+        seg = np.clip(np.searchsorted(exp, x, side="right") - 1, 0, n - 2)
+        x0, x1 = exp[seg], exp[seg + 1]
+        y0, y1 = act[seg], act[seg + 1]
+        w = 1.0 / (x1 - x0)
+        self.interpolated_pixel_locs = y0 * (w * (x1 - x)) + y1 * (w * (x - x0))
+        self.wowfactors = y0 * (-w) + y1 * w
+        return self.interpolated_pixel_locs, self.wowfactors
+
+    def downscale(self, lineinfo=None, linesout=None, outwidth=None, channel="demod", audio=0,
+                  final=False, lastfieldwritten=None):
+        """core.py:2626-2722: resample to outwidth x linesout (float32, or
+        uint16 levels if final) on the GPU; EFM slice; analog audio."""
+        if lineinfo is None:
+            lineinfo = self.linelocs
+        if outwidth is None:
+            outwidth = self.outlinelen
+        if linesout is None:
+            linesout = self.outlinecount
+        if self.wow_level_adjust_smoothing:
+            raise NotImplementedError("wow_level_adjust_smoothing is not available on the GPU path")
+        if self.wow_interpolation_method != "linear":
+            raise NotImplementedError("only linear wow interpolation is available on the GPU path")
+        buf = np.ascontiguousarray(self.data["video"][channel], dtype=np.float32)
+        ll = np.ascontiguousarray(lineinfo, dtype=np.float64)
+        nout = linesout * outwidth
+        dsout = np.empty(nout, dtype=np.float32)
+        pic = np.empty(nout, dtype=np.uint16) if final else None
+        desc = tbc_descriptor(self.rf, buf, ll, self.lineoffset, outwidth, linesout, self.outlinecount,
+                              self.levels(), out_u16=pic, out_f32=dsout, coord_f32=self.coord_f32)
+        tbc_fields(self.rf, [desc])
+
+        dsaudio = None
+        if audio != 0 and self.rf.decode_analog_audio:
+            from .audio import downscale_audio
+            dsaudio, self.audio_next_offset = downscale_audio(
+                self.data["audio"], lineinfo, self.rf, self.linecount, self.audio_offset(audio, lastfieldwritten),
+                audio)
+        self.dsaudio = dsaudio
+
+        if self.rf.decode_digital_audio:
+            self.efmout = self.data["efm"][int(self.linelocs[1]):int(self.linelocs[self.linecount + 1])]
+        else:
+            self.efmout = None
+        if final:
+            self.dspicture = pic
+            return pic, self.dsaudio, self.efmout
+        return dsout, self.dsaudio, self.efmout
+
+    def audio_offset(self, audio, lastfieldwritten):
+        """A/V alignment offset of the first audio sample (core.py:2644-2670)."""
+        if lastfieldwritten and audio >= 16000:
+            sp = self.rf.SysParams
+            rf_samples_per_field = self.rf.freq_hz / sp["FPS"] / 2
+            read_gap = (self.readloc - lastfieldwritten[1]) / rf_samples_per_field
+            field_number = int(np.round(lastfieldwritten[0] + read_gap))
+            linecount = sum(sp["field_lines"]) * (field_number // 2)
+            if not self.isFirstField:
+                linecount += sp["field_lines"][0]
+            samples_per_line = (sp["line_period"] / 1000000) / (1 / audio)
+            cnt = linecount * samples_per_line
+            frac = cnt - np.floor(cnt)
+            return (1 - frac) * (1 / audio) if frac > .5 else -frac * (1 / audio)
+        return 0
+
+
+class FieldNTSC(FieldLogicNTSC, Field):
+    def downscale(self, lineoffset=0, final=False, *args, **kwargs):
+        """core.py:3442-3451: audio only on the final pass."""
+        if final is False and "audio" in kwargs:
+            kwargs["audio"] = 0
+        return Field.downscale(self, final=final, *args, **kwargs)
+
+
+class FieldPAL(FieldLogicPAL, Field):
+    def downscale(self, final=False, *args, **kwargs):
+        """core.py:3205-3207."""
+        return Field.downscale(self, final=final, *args, **kwargs)

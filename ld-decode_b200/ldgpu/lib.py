@@ -1,0 +1,138 @@
+"""ctypes binding of the ldgpu C ABI (include/ldgpu.h).
+
+The shared library is built in-tree (ld-decode_b200/build.py) next to this
+file.  There is no CPU fallback: if the library is missing or cannot be
+loaded, `load()` raises, and so does every GPU entry point of the package.
+"""
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libldgpu.so")
+
+LDG_OK = 0
+LDG_NTSC, LDG_PAL = 0, 1
+LDG_IN_INT16, LDG_IN_FLOAT32 = 0, 1
+(LDG_F_RFHPF, LDG_F_VIDEO_G, LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT,
+ LDG_F_EFM) = range(7)
+LDG_NFILTERS = 7
+
+ERRORS = {-1: "argument", -2: "cuda", -3: "state", -4: "unsupported", -5: "range"}
+
+# Every exported symbol with its (restype, argtypes); checked by the tests.
+c_p = ctypes.c_void_p
+
+
+class Slice(ctypes.Structure):
+    _fields_ = [("start", ctypes.c_int32), ("len", ctypes.c_int32), ("roll", ctypes.c_int32)]
+
+
+class DemodArgs(ctypes.Structure):
+    _fields_ = [
+        ("in_", c_p), ("in_kind", ctypes.c_int32), ("in_stride", ctypes.c_int64),
+        ("nblocks", ctypes.c_int64),
+        ("out_demod", c_p), ("out_raw", c_p), ("out_05", c_p), ("out_burst", c_p),
+        ("out_pilot", c_p), ("out_rfhpf", c_p), ("out_efm", c_p),
+        ("out_audio_left", c_p), ("out_audio_right", c_p),
+        ("video", Slice), ("roll_05", ctypes.c_int32), ("roll_burst", ctypes.c_int32),
+        ("rfhpf", Slice), ("efm", Slice), ("audio", Slice), ("stream", c_p),
+    ]
+
+
+class TbcField(ctypes.Structure):
+    _fields_ = [
+        ("buf", c_p), ("buf_len", ctypes.c_int64), ("linelocs", c_p), ("nlines", ctypes.c_int32),
+        ("lineoffset", ctypes.c_int32), ("outwidth", ctypes.c_int32), ("linesout", ctypes.c_int32),
+        ("outlinecount", ctypes.c_int32), ("coord_f32", ctypes.c_int32),
+        ("inlinelen", ctypes.c_double), ("outlinelen", ctypes.c_double),
+        ("ire0", ctypes.c_double), ("hz_ire", ctypes.c_double), ("vsync_ire", ctypes.c_double),
+        ("out_scale", ctypes.c_double), ("output_zero", ctypes.c_double),
+        ("out_f32", c_p), ("out_u16", c_p),
+    ]
+
+
+SIGNATURES = {
+    "ldg_abi_version": (ctypes.c_int, []),
+    "ldg_last_error": (ctypes.c_char_p, []),
+    "ldg_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
+    "ldg_ctx_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.c_int32, ctypes.c_double]),
+    "ldg_ctx_destroy": (None, [c_p]),
+    "ldg_set_filter": (ctypes.c_int, [c_p, ctypes.c_int32, c_p, ctypes.c_int64]),
+    "ldg_set_audio": (ctypes.c_int, [c_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_p,
+                                     ctypes.c_double, ctypes.c_double]),
+    "ldg_set_sinc_lut": (ctypes.c_int, [c_p, c_p, ctypes.c_int32, ctypes.c_int32]),
+    "ldg_demod_blocks": (ctypes.c_int, [c_p, ctypes.POINTER(DemodArgs)]),
+    "ldg_tbc_fields": (ctypes.c_int, [c_p, ctypes.POINTER(TbcField), ctypes.c_int32, c_p]),
+    "ldg_synchronize": (ctypes.c_int, [c_p]),
+    "ldg_demod_scratch_bytes": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class LdgError(RuntimeError):
+    """A failed ldgpu C-ABI call (code and message from ldg_last_error)."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"ldgpu error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def load(path=None):
+    """Load (once) and return the ctypes handle of libldgpu.so."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = path or LIBPATH
+        if not os.path.exists(p):
+            raise ImportError(f"ldgpu CUDA library not built: {p} is missing "
+                              "(run python ld-decode_b200/build.py)")
+        lib = ctypes.CDLL(p)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(rc):
+    if rc != LDG_OK:
+        msg = load().ldg_last_error()
+        raise LdgError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def device_count():
+    n = ctypes.c_int32(0)
+    check(load().ldg_device_count(ctypes.byref(n)))
+    return n.value
+
+
+class Context:
+    """Owns one ldg_ctx (device filters, twiddles, scratch, staging)."""
+
+    def __init__(self, system, blocklen, fs_hz, device=0):
+        lib = load()
+        self._lib = lib
+        h = c_p()
+        check(lib.ldg_ctx_create(ctypes.byref(h), int(device), LDG_PAL if system == "PAL" else LDG_NTSC,
+                                 int(blocklen), float(fs_hz)))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.ldg_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

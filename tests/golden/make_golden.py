@@ -1,0 +1,236 @@
+#!/usr/bin/env python3
+"""Regenerate the golden fixtures in this folder from the unmodified reference.
+
+Runs happycube/ld-decode's own Python code (imported from /root/reference,
+read-only, in the development container only) on seeded synthetic inputs made
+by ldgpu.synth, and saves small .npz fixtures:
+
+  filters_<cfg>.npz  -- RFDecode filter bank summaries (sampled bins, sums),
+                        audio slice geometry, computedelays results;
+  demod_<cfg>.npz    -- one input block and the reference demodblock outputs
+                        (subsampled video/rfhpf/efm, full audio) at two MTF levels;
+  field_<sys>.npz    -- a capture, and for two consecutive fields the
+                        reference's sync pulses, line locations, field flags,
+                        TBC coordinates summary and the final uint16 picture;
+  sinc_lut_rows.npz  -- sampled rows of the reference's shipped sinc table.
+
+Nothing at test time reads /root/reference; only this script does.
+Usage: python tests/golden/make_golden.py
+"""
+
+import hashlib
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = "/root/reference"
+
+os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
+sys.dont_write_bytecode = True
+sys.path.insert(0, os.path.join(REPO, "ld-decode_b200"))
+sys.path.insert(0, REF)
+
+import numpy as np  # noqa: E402
+
+from lddecode import core as refcore  # noqa: E402
+from ldgpu.synth import synth_capture  # noqa: E402
+
+STRIDE = 9
+COORD_STRIDE = 101
+CAPTURE_START = 123457
+FILTER_STEP = 61
+
+CONFIGS = {
+    "ntsc": dict(system="NTSC", decode_analog_audio=44100, decode_digital_audio=True),
+    "pal": dict(system="PAL", decode_analog_audio=44100, decode_digital_audio=True),
+    "ntsc_lowband": dict(system="NTSC", decode_analog_audio=44100, decode_digital_audio=True,
+                         extra_options={"lowband": True, "deemp_str": 1.5,
+                                        "NTSC_ColorNotchFilter": True, "MTF_level": 0.7,
+                                        "MTF_offset": 0.1}),
+    "pal_lowband": dict(system="PAL", decode_analog_audio=44100, decode_digital_audio=True,
+                        extra_options={"lowband": True, "deemp_coeff": (2.0, 7.0)}),
+}
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def filters_fixture(name, kw):
+    rf = refcore.RFDecode(**kw)
+    out = {}
+    idx = np.arange(0, rf.blocklen, FILTER_STEP)
+    for k, v in rf.Filters.items():
+        if isinstance(v, np.ndarray):
+            out["F_" + k] = v[idx]
+            out["Fsum_" + k] = np.array([np.sum(v), np.sum(np.abs(v) ** 2)])
+        else:
+            out["S_" + k] = np.array(v)
+    for ch in ("left", "right"):
+        a = rf.audio[ch]
+        out[f"A_{ch}_geom"] = np.array([a.lowbin, a.nbins, a.a1_freq, a.low_freq], dtype=np.float64)
+        out[f"A_{ch}_filt1"] = a.filt1
+        out[f"A_{ch}_audio2"] = a.audio2_filter[idx]
+    out["delays"] = np.array([rf.delays["video_sync"], rf.delays["video_white"],
+                              rf.delays["video_rot"]], dtype=np.float64)
+    out["limits"] = np.array([*rf.limits["sync"], *rf.limits["viewable"]], dtype=np.float64)
+    out["blockcut_end"] = np.array(rf.blockcut_end)
+    out["bin_idx"] = idx
+    np.savez_compressed(os.path.join(HERE, f"filters_{name}.npz"), **out)
+    return rf
+
+
+def demod_fixture(name, rf, kw, seed):
+    cap = synth_capture(kw["system"], rf.blocklen + 4096, seed=seed).numpy()
+    block = cap[1000:1000 + rf.blocklen].copy()
+    out = {"block": block}
+    for tag, mtf in (("m0", 0), ("m1", 1)):
+        rv = rf.demodblock(data=block, mtf_level=mtf, cut=True)
+        for k in rv["video"].dtype.names:
+            v = np.asarray(rv["video"][k])
+            out[f"{tag}_{k}"] = v[::STRIDE]
+            out[f"{tag}_{k}_sum"] = np.array([np.sum(v.astype(np.float64)),
+                                              np.sum(v.astype(np.float64) ** 2)])
+        out[f"{tag}_rfhpf"] = rv["rfhpf"][::STRIDE]
+        out[f"{tag}_efm"] = rv["efm"][::STRIDE]
+        out[f"{tag}_efm_sum"] = np.array([np.sum(rv["efm"].astype(np.int64))])
+        out[f"{tag}_audio_left"] = np.asarray(rv["audio"]["audio_left"])
+        out[f"{tag}_audio_right"] = np.asarray(rv["audio"]["audio_right"])
+    # uncut form, video only
+    rv = rf.demodblock(data=block, mtf_level=1, cut=False)
+    for k in rv["video"].dtype.names:
+        out[f"full_{k}"] = np.asarray(rv["video"][k])[::STRIDE]
+    out["full_audio_left"] = np.asarray(rv["audio"]["audio_left"])
+    out["full_efm"] = rv["efm"][::STRIDE]
+    out["mtf_scaled"] = np.array([((1 * rf.mtf_mult) + rf.mtf_offset) * rf.DecoderParams["MTF_basemult"]])
+    np.savez_compressed(os.path.join(HERE, f"demod_{name}.npz"), **out)
+
+
+class BlockSource:
+    """Per-block demod outputs over a capture, assembled into field reads the
+    way DemodCache.read + LDdecode.decodefield do (core.py:1343-1413,
+    4030-4042)."""
+
+    def __init__(self, rf, cap, mtf):
+        self.rf, self.cap, self.mtf = rf, cap, mtf
+        self.U = rf.blocklen - rf.blockcut - rf.blockcut_end
+        self.cache = {}
+
+    def block(self, b):
+        if b not in self.cache:
+            raw = self.cap[b * self.U:b * self.U + self.rf.blocklen]
+            if len(raw) < self.rf.blocklen:
+                return None
+            rv = self.rf.demodblock(data=raw, mtf_level=self.mtf, cut=True)
+            rv["input"] = raw[self.rf.blockcut:-self.rf.blockcut_end]
+            self.cache[b] = rv
+        return self.cache[b]
+
+    def read_field(self, start):
+        readloc = max(int(start - self.rf.blockcut), 0)
+        bs = self.rf.blocklen
+        begin = (readloc // bs) * bs
+        length = ((self.readlen // bs) + 2) * bs
+        end = begin + length
+        blocks = range(begin // self.U, end // self.U + 1)
+        parts = [self.block(b) for b in blocks]
+        if any(p is None for p in parts):
+            return None
+        rv = {
+            "input": np.concatenate([p["input"] for p in parts]),
+            "video": np.concatenate([p["video"] for p in parts]).view(np.recarray),
+            "rfhpf": np.concatenate([p["rfhpf"] for p in parts]),
+            "startloc": (begin // self.U) * self.U,
+        }
+        return rv, readloc
+
+
+def field_fixture(system, seed, nfields=2):
+    kw = dict(system=system, decode_analog_audio=0, decode_digital_audio=False)
+    rf = refcore.RFDecode(**kw)
+    src = BlockSource(rf, None, 1)
+    fieldcls = refcore.FieldPAL if system == "PAL" else refcore.FieldNTSC
+    if system == "PAL":
+        src.readlen = rf.linelen * 400
+    else:
+        src.readlen = ((rf.linelen * 350) // 16384) * 16384
+    fieldlen = int(rf.freq_hz / (rf.SysParams["FPS"] * 2))
+    ncap = nfields * fieldlen + src.readlen + 8 * rf.blocklen
+    cap = synth_capture(system, ncap, seed=seed, start=CAPTURE_START).numpy()
+    src.cap = cap
+    out = {"capture_sha256": np.array(sha(cap)), "capture_len": np.array(ncap),
+           "capture_seed": np.array(seed), "capture_start": np.array(CAPTURE_START),
+           "mtf_level": np.array(1.0)}
+    prev = None
+    start = 0
+    i = 0
+    skipped = []
+    while i < nfields:
+        rd = src.read_field(start)
+        assert rd is not None
+        decode, readloc = rd
+        f = fieldcls(rf, decode, prevfield=prev, initphase=(i == 0), fields_written=i,
+                     readloc=decode["startloc"])
+        f.process()
+        if not f.valid:
+            # readfield moves on by nextfieldoffset after an invalid field
+            skipped.append(start)
+            start = start + f.nextfieldoffset
+            prev = None
+            assert len(skipped) < 4
+            continue
+        dsout, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+        p = f"f{i}_"
+        out[p + "start"] = np.array(start)
+        out[p + "readloc"] = np.array(readloc)
+        out[p + "startloc"] = np.array(decode["startloc"])
+        out[p + "pulse_start"] = np.array([q.start for q in f.rawpulses], dtype=np.int64)
+        out[p + "pulse_len"] = np.array([q.len for q in f.rawpulses], dtype=np.int64)
+        out[p + "valid_type"] = np.array([v[0] for v in f.validpulses], dtype=np.int64)
+        out[p + "valid_start"] = np.array([v[1].start for v in f.validpulses], dtype=np.int64)
+        out[p + "valid_good"] = np.array([bool(v[2]) for v in f.validpulses])
+        out[p + "linelocs1"] = np.array(f.linelocs1, dtype=np.float64)
+        out[p + "linelocs2"] = np.array(f.linelocs2, dtype=np.float64)
+        out[p + "linelocs"] = np.array(f.linelocs, dtype=np.float64)
+        out[p + "linebad"] = np.array(f.linebad, dtype=bool)
+        out[p + "flags"] = np.array([int(f.isFirstField), f.linecount, f.lineoffset,
+                                     f.fieldPhaseID, f.sync_confidence], dtype=np.int64)
+        out[p + "nextfieldoffset"] = np.array(f.nextfieldoffset, dtype=np.float64)
+        out[p + "burstmedian"] = np.array(f.burstmedian, dtype=np.float64)
+        out[p + "coords"] = f.interpolated_pixel_locs[::COORD_STRIDE]
+        out[p + "wow"] = f.wowfactors[::COORD_STRIDE]
+        out[p + "wow_stats"] = np.array([len(f.wowfactors), np.median(f.wowfactors)])
+        out[p + "dspicture"] = np.asarray(f.dspicture)
+        out[p + "levels"] = np.array([rf.DecoderParams["ire0"], rf.DecoderParams["hz_ire"],
+                                      rf.DecoderParams["vsync_ire"], f.out_scale,
+                                      rf.SysParams["outputZero"]], dtype=np.float64)
+        # where the next field read starts (decodefield/readfield offset logic)
+        offset = f.nextfieldoffset - (readloc - decode["startloc"])
+        start = start + offset
+        prev = f
+        i += 1
+    out["skipped_starts"] = np.array(skipped, dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, f"field_{system.lower()}.npz"), **out)
+
+
+def lut_fixture():
+    lut = np.load(os.path.join(REF, "lddecode", "sinc_lut.npz"))["downscale_sinc_lut"]
+    rows = np.concatenate([np.arange(0, 65537, 997), [32767, 32768, 65535, 65536]])
+    np.savez_compressed(os.path.join(HERE, "sinc_lut_rows.npz"), rows=rows, values=lut[rows],
+                        sha256=np.array(sha(lut)))
+
+
+def main():
+    lut_fixture()
+    for i, (name, kw) in enumerate(CONFIGS.items()):
+        rf = filters_fixture(name, kw)
+        if name in ("ntsc", "pal"):
+            demod_fixture(name, rf, kw, seed=11 + i)
+    field_fixture("NTSC", seed=21)
+    field_fixture("PAL", seed=22)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

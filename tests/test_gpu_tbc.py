@@ -1,0 +1,124 @@
+"""GPU parity of the time-base corrector (Field.downscale on the B200).
+
+Line locations come from the reference's golden fields; the demodulated
+field buffer is the oracle's (FP64) or the GPU's own.  Bars:
+  * compat mode (float32 coordinates, as the reference) vs the reference's
+    picture: within 1 LSB, >= 99 % exact;
+  * FP64 mode vs the FP64 oracle on the same buffer: within 1 LSB on
+    >= 99.99 % of samples;
+  * GPU demod + GPU TBC vs the FP64 oracle end to end: within 1 LSB on
+    >= 99.99 % of samples.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from helpers import oracle_capture
+from oracle import tbc as otbc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", params=["NTSC", "PAL"])
+def case(request, cuda_ok):
+    from ldgpu import RFDecode
+    from ldgpu.fieldread import field_window
+    from ldgpu.synth import synth_capture
+    system = request.param
+    g = golden("field_" + system.lower())
+    rf = RFDecode(system=system)
+    cap = synth_capture(system, int(g["capture_len"]), seed=int(g["capture_seed"]),
+                        start=int(g["capture_start"])).numpy()
+    w = field_window(rf, float(g["f0_start"]))
+    mtf = rf.scaled_mtf(float(g["mtf_level"]))
+    buf = oracle_capture(rf, cap, w.first_block, w.nblocks, mtf)["demod"]
+    yield rf, g, cap, w, buf
+    rf.close()
+
+
+def _field(rf, g, buf, coord_f32):
+    from ldgpu.field import FieldNTSC, FieldPAL
+    cls = FieldPAL if rf.system == "PAL" else FieldNTSC
+    isfirst, linecount, lineoffset = (int(v) for v in g["f0_flags"][:3])
+    f = cls(rf, {"video": {"demod": buf}, "startloc": int(g["f0_startloc"])})
+    f.linelocs = g["f0_linelocs"]
+    f.lineoffset = lineoffset
+    f.linecount = linecount
+    f.isFirstField = bool(isfirst)
+    f.coord_f32 = coord_f32
+    ire0, hz_ire, vsync_ire, out_scale, ozero = g["f0_levels"]
+    f.out_scale = out_scale
+    return f
+
+
+def _oracle_picture(rf, g, buf, coord_f32):
+    outw = rf.SysParams["outlinelen"]
+    outlines = rf.SysParams["frame_lines"] // 2 + 1
+    lineoffset = int(g["f0_flags"][2])
+    coords, wow = otbc.pixel_coords(g["f0_linelocs"], rf.linelen, outw, outlines, lineoffset)
+    ds = otbc.scale_field(buf, coords, wow, rf.downscale_sinc_lut, lineoffset, outw, outlines * outw,
+                          coord_f32=coord_f32)
+    ire0, hz_ire, vsync_ire, out_scale, ozero = g["f0_levels"]
+    return ds, otbc.hz_to_output(ds, ire0, hz_ire, ozero, vsync_ire, out_scale)
+
+
+def test_tbc_compat_matches_reference_picture(case):
+    rf, g, cap, w, buf = case
+    f = _field(rf, g, buf, coord_f32=True)
+    pic, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+    d = np.abs(pic.astype(int) - g["f0_dspicture"].astype(int))
+    print(rf.system, "compat vs reference: max", d.max(), "exact", np.mean(d == 0))
+    assert d.max() <= 1 and np.mean(d == 0) >= 0.99
+
+
+def test_tbc_fp64_matches_oracle(case):
+    rf, g, cap, w, buf = case
+    f = _field(rf, g, buf, coord_f32=False)
+    ds, _, _ = f.downscale(linesout=f.outlinecount, final=False)
+    pic, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+    ods, opic = _oracle_picture(rf, g, buf, coord_f32=False)
+    assert np.abs(ds.astype(np.float64) - ods).max() < 2.0  # Hz
+    d = np.abs(pic.astype(int) - opic.astype(int))
+    print(rf.system, "fp64 vs oracle: max", d.max(), "within1", np.mean(d <= 1))
+    assert d.max() <= 1 and np.mean(d <= 1) >= 0.9999
+
+
+def test_demod_plus_tbc_end_to_end(case):
+    """GPU demod of the field's blocks, then GPU TBC, vs the FP64 oracle."""
+    import torch
+    rf, g, cap, w, buf = case
+    U = rf.blocklen - rf.blockcut - rf.blockcut_end
+    dcap = torch.from_numpy(cap).cuda()
+    dem = torch.empty(w.nblocks * U, dtype=torch.float32, device="cuda")
+    rf.demod_blocks_device(dcap.data_ptr() + 2 * w.first_block * U, w.nblocks, U,
+                           {"demod": dem.data_ptr()}, mtf_level=float(g["mtf_level"]))
+    gbuf = dem.cpu().numpy()
+    rms = float(np.sqrt(np.mean((gbuf.astype(np.float64) - buf) ** 2)))
+    print(rf.system, "field demod rms Hz", rms)
+    assert rms < 1000.0
+    f = _field(rf, g, gbuf, coord_f32=False)
+    pic, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+    _, opic = _oracle_picture(rf, g, buf, coord_f32=False)
+    d = np.abs(pic.astype(int) - opic.astype(int))
+    print(rf.system, "e2e vs oracle: max", d.max(), "within1", np.mean(d <= 1), "exact", np.mean(d == 0))
+    assert np.mean(d <= 1) >= 0.9999
+
+
+def test_tbc_batched_fields(case):
+    """Several fields in one launch give the same pictures as one by one."""
+    from ldgpu.field import tbc_descriptor, tbc_fields
+    rf, g, cap, w, buf = case
+    f = _field(rf, g, buf, coord_f32=False)
+    single, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+    outs = []
+    descs = []
+    for shift in (0.0, 0.25, -0.5):
+        ll = np.ascontiguousarray(g["f0_linelocs"] + shift)
+        o = np.empty(f.outlinecount * f.outlinelen, dtype=np.uint16)
+        outs.append((ll, o))
+        descs.append(tbc_descriptor(rf, buf, ll, f.lineoffset, f.outlinelen, f.outlinecount,
+                                    f.outlinecount, f.levels(), out_u16=o))
+    tbc_fields(rf, descs)
+    np.testing.assert_array_equal(outs[0][1], single)
+    assert not np.array_equal(outs[1][1], single)

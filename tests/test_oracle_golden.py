@@ -1,0 +1,103 @@
+"""Pin the CPU oracle (oracle/) against the reference's own outputs.
+
+The golden fixtures were produced by running the unmodified reference on
+the same inputs (tests/golden/make_golden.py).  The oracle uses the
+product's host filter design, which test_host.py pins separately.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from ldgpu.fieldread import field_window
+from ldgpu.rfdecode import RFParams
+from ldgpu.synth import synth_capture
+from oracle import demod as odemod
+from oracle import tbc as otbc
+
+STRIDE = 9
+
+
+def _rf(system, **kw):
+    rf = RFParams(system=system, decode_analog_audio=44100, decode_digital_audio=True, **kw)
+    rf.delays = {"video_rot": 3}
+    return rf
+
+
+def oracle_block(rf, block, mtf_scaled, cut=True):
+    return odemod.demodblock(block, rf.Filters, system=rf.system, freq_hz=rf.freq_hz,
+                             blocklen=rf.blocklen, blockcut=rf.blockcut, blockcut_end=rf.blockcut_end,
+                             video_rot=rf.delays["video_rot"], mtf_level=mtf_scaled, cut=cut,
+                             efm=True, audio=rf.audio)
+
+
+@pytest.mark.parametrize("system", ["NTSC", "PAL"])
+def test_oracle_demod_matches_reference(system):
+    g = golden("demod_" + system.lower())
+    rf = _rf(system)
+    for tag, mtf in (("m0", 0.0), ("m1", rf.scaled_mtf(1))):
+        rv = oracle_block(rf, g["block"], mtf)
+        names = ["demod", "demod_raw", "demod_05", "demod_burst"] + (["demod_pilot"] if system == "PAL" else [])
+        for k in names:
+            mine = rv["video"][k][::STRIDE]
+            ref = g[f"{tag}_{k}"]
+            # both are float32 casts of FP64 results; allow one float32 ulp (~1 Hz)
+            assert np.abs(mine.astype(np.float64) - ref).max() <= 2.0, (tag, k)
+            assert np.mean(mine == ref) > 0.99, (tag, k)
+        np.testing.assert_allclose(rv["rfhpf"][::STRIDE], g[f"{tag}_rfhpf"], rtol=0, atol=1e-3)
+        assert np.abs(rv["efm"][::STRIDE].astype(int) - g[f"{tag}_efm"]).max() <= 1
+        for ch in ("audio_left", "audio_right"):
+            assert np.abs(rv["audio"][ch].astype(np.float64) - g[f"{tag}_{ch}"]).max() <= 1.0
+    rv = oracle_block(rf, g["block"], rf.scaled_mtf(1), cut=False)
+    for k in ("demod", "demod_05", "demod_burst"):
+        assert np.abs(rv["video"][k][::STRIDE].astype(np.float64) - g[f"full_{k}"]).max() <= 2.0
+    assert np.abs(rv["efm"][::STRIDE].astype(int) - g["full_efm"]).max() <= 1
+    assert len(rv["audio"]["audio_left"]) == 1024
+
+
+def field_demod_oracle(rf, cap, window, mtf_scaled, keys=("demod",)):
+    """Capture-wide concatenated oracle outputs for one field window."""
+    U = rf.blocklen - rf.blockcut - rf.blockcut_end
+    outs = {k: [] for k in keys}
+    for b in range(window.first_block, window.first_block + window.nblocks):
+        raw = cap[b * U:b * U + rf.blocklen]
+        rv = odemod.demodblock(raw, rf.Filters, system=rf.system, freq_hz=rf.freq_hz,
+                               blocklen=rf.blocklen, blockcut=rf.blockcut,
+                               blockcut_end=rf.blockcut_end, video_rot=3,
+                               mtf_level=mtf_scaled, cut=True)
+        for k in keys:
+            outs[k].append(rv["video"][k])
+    return {k: np.concatenate(v) for k, v in outs.items()}
+
+
+@pytest.mark.parametrize("system", ["NTSC", "PAL"])
+def test_oracle_tbc_matches_reference(system):
+    """Oracle coordinates, wow and the uint16 picture (compat mode: the
+    reference's float32 coordinate cast) against the reference's fields."""
+    g = golden("field_" + system.lower())
+    rf = RFParams(system=system)
+    cap = synth_capture(system, int(g["capture_len"]), seed=int(g["capture_seed"]),
+                        start=int(g["capture_start"])).numpy()
+    lut = rf.downscale_sinc_lut
+    outw = rf.SysParams["outlinelen"]
+    outlines = rf.SysParams["frame_lines"] // 2 + 1
+    for i in range(2):
+        p = f"f{i}_"
+        w = field_window(rf, float(g[p + "start"]))
+        assert w.startloc == int(g[p + "startloc"])
+        buf = field_demod_oracle(rf, cap, w, rf.scaled_mtf(float(g["mtf_level"])))["demod"]
+        ll = g[p + "linelocs"]
+        isfirst, linecount, lineoffset = g[p + "flags"][:3]
+        coords, wow = otbc.pixel_coords(ll, rf.linelen, outw, outlines, int(lineoffset))
+        np.testing.assert_allclose(coords[::101], g[p + "coords"], rtol=0, atol=1e-8)
+        np.testing.assert_allclose(wow[::101], g[p + "wow"], rtol=1e-12)
+        assert len(wow) == int(g[p + "wow_stats"][0])
+        assert np.median(wow) == g[p + "wow_stats"][1]
+        ds = otbc.scale_field(buf, coords, wow, lut, int(lineoffset), outw, outlines * outw,
+                              coord_f32=True)
+        ire0, hz_ire, vsync_ire, out_scale, ozero = g[p + "levels"]
+        pic = otbc.hz_to_output(ds, ire0, hz_ire, ozero, vsync_ire, out_scale)
+        ref = g[p + "dspicture"]
+        d = np.abs(pic.astype(int) - ref.astype(int))
+        assert d.max() <= 1, (i, d.max())
+        assert np.mean(d == 0) > 0.99, (i, np.mean(d == 0))
