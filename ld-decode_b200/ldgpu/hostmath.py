@@ -26,13 +26,15 @@ def calczc(data, start_offset, target, edge=0, count=16, reverse=False):
     s = int(start_offset)
     icount = int(count + 1)
     if edge == 0:
-        edge = 1 if data[s] < target else -1
-    loc = _first_cross(np.asarray(data[s:s + icount]), target, edge == 1)
+        edge = 1 if float(data[s]) < target else -1
+    # comparisons and interpolation in float64, as the reference's numba code
+    # promotes float32 samples against a float64 target
+    loc = _first_cross(np.asarray(data[s:s + icount], dtype=np.float64), target, edge == 1)
     if loc is None:
         return None
     x = s + loc
-    a = data[x - 1] - target
-    b = data[x] - target
+    a = float(data[x - 1]) - target
+    b = float(data[x]) - target
     y = -a / (-a + b) if b - a != 0 else 0
     return x - 1 + y
 

@@ -399,6 +399,10 @@ class RFDecode(RFParams):
         }
         return dec, emp
 
+    def synchronize(self):
+        """Wait for the work queued on the context's own stream."""
+        L.check(self._ctx._lib.ldg_synchronize(self._ctx.handle))
+
     def close(self):
         self._ctx.close()
 

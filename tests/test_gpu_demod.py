@@ -109,8 +109,7 @@ def test_batched_equals_plain(rf):
     torch.cuda.synchronize()
     rf.demod_blocks_device(dcap.data_ptr(), nb, U, {k: v.data_ptr() for k, v in outs.items()},
                            mtf_level=1, cut=True)
-    L = __import__("ldgpu.lib", fromlist=["check"])
-    L.check(rf._ctx._lib.ldg_synchronize(rf._ctx.handle))
+    rf.synchronize()
     for b in range(nb):
         plain = rf.demodblock(data=cap[b * U:b * U + rf.blocklen], mtf_level=1, cut=True)
         for k in keys:

@@ -93,6 +93,7 @@ def test_demod_plus_tbc_end_to_end(case):
     dem = torch.empty(w.nblocks * U, dtype=torch.float32, device="cuda")
     rf.demod_blocks_device(dcap.data_ptr() + 2 * w.first_block * U, w.nblocks, U,
                            {"demod": dem.data_ptr()}, mtf_level=float(g["mtf_level"]))
+    rf.synchronize()
     gbuf = dem.cpu().numpy()
     rms = float(np.sqrt(np.mean((gbuf.astype(np.float64) - buf) ** 2)))
     print(rf.system, "field demod rms Hz", rms)
