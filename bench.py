@@ -1,0 +1,496 @@
+#!/usr/bin/env python3
+"""Throughput benchmark: RF demodulation + time-base correction on B200.
+
+Workload (default): an NTSC 10 s capture -- 400 M int16 samples at 40 MSPS
+from the seeded synthetic generator (ldgpu.synth), about 12.6 k overlap-save
+blocks and 600 fields.  One step = every block of the capture through the
+fused demodulator in one launch (all outputs: demod, demod_raw, demod_05,
+demod_burst, rfhpf, EFM, analog audio stage 1) + every field through the
+TBC in one batched launch (uint16 4fsc fields).  Field line locations are
+found before timing by the host Field.process() logic over the GPU outputs.
+
+Prints one JSON line (rank 0).  `--impl reference` times the CPU oracle (a
+numpy restatement of the reference's demodblock + scale_field) on the host
+cores instead, on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): each rank decodes its own capture (different seed);
+no data-path collective; timing is the max over ranks.
+"""
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "ld-decode_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "RF MSPS demod+TBC on 1 B200 (batched FP32 vs plain) + HBM roofline %"
+BYTES_PER_SAMPLE_DEMOD = 2 + 4 * 4 + 4 + 2  # input + 4 video f32 + rfhpf f32 + efm i16 (per output sample)
+AUDIO_BYTES_PER_BLOCK = 2 * 991 * 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ldgpu", choices=["ldgpu", "reference"])
+    ap.add_argument("--system", default="NTSC", choices=["NTSC", "PAL"])
+    ap.add_argument("--seconds", type=float, default=10.0)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if not self.proc:
+            return out
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if sm:
+            out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                   "samples": len(sm)}
+        return out
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def field_chain(rf, host, nblocks):
+    """Line locations of every field, following decodefield's read chain
+    (core.py:4030-4097, 4165-4186): host Field.process() over the GPU-demodulated
+    capture-wide arrays (no AGC / MTF redo)."""
+    from ldgpu.field import FieldNTSC, FieldPAL
+    from ldgpu.fieldread import field_window
+    cls = FieldPAL if rf.system == "PAL" else FieldNTSC
+    fields = []
+    start = 0.0
+    prev = None
+    while True:
+        w = field_window(rf, start)
+        if w.first_block + w.nblocks > nblocks:
+            break
+        sl = slice(w.startloc, w.startloc + w.length)
+        dec = {"video": {k: v[sl] for k, v in host.items()}, "startloc": w.startloc}
+        f = cls(rf, dec, prevfield=prev, fields_written=len(fields), readloc=w.startloc)
+        f.process()
+        if not f.valid:
+            start += f.nextfieldoffset
+            prev = None
+            continue
+        fields.append((w, np.ascontiguousarray(f.linelocs, dtype=np.float64), f.lineoffset, f.levels()))
+        start += f.nextfieldoffset - (w.readloc - w.startloc)
+        prev = f
+        if prev is not None:
+            prev.prevfield = None  # keep one field of history, as readfield does
+    return fields
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from ldgpu import RFDecode
+    from ldgpu import lib as L
+    from ldgpu.field import tbc_descriptor, tbc_fields
+    from ldgpu.fieldread import blocks_in_capture
+    from ldgpu.synth import synth_capture
+
+    system = args.system
+    rf = RFDecode(system=system, decode_analog_audio=44100, decode_digital_audio=True, device=local)
+    N = rf.blocklen
+    U = N - rf.blockcut - rf.blockcut_end
+    nsamples = int(args.seconds * rf.freq_hz)
+    nblocks = blocks_in_capture(rf, nsamples)
+    nout = nblocks * U
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
+
+    cap = synth_capture(system, nsamples, seed=args.seed + rank, device="cuda")
+    keys = ["demod", "demod_raw", "demod_05", "demod_burst"] + (["demod_pilot"] if system == "PAL" else [])
+    outs = {k: torch.empty(nout, dtype=torch.float32, device="cuda") for k in keys}
+    outs["rfhpf"] = torch.empty(nout, dtype=torch.float32, device="cuda")
+    outs["efm"] = torch.empty(nout, dtype=torch.int16, device="cuda")
+    outs["audio_left"] = torch.empty(nblocks * 991, dtype=torch.float32, device="cuda")
+    outs["audio_right"] = torch.empty(nblocks * 991, dtype=torch.float32, device="cuda")
+    ptrs = {k: v.data_ptr() for k, v in outs.items()}
+
+    def demod():
+        rf.demod_blocks_device(cap.data_ptr(), nblocks, U, ptrs, mtf_level=1, stream=sh)
+
+    demod()
+    torch.cuda.synchronize()
+    # ---- line locations (host, before timing)
+    t0 = time.time()
+    fkeys = ["demod", "demod_05", "demod_burst"] + (["demod_pilot"] if system == "PAL" else [])
+    host = {k: outs[k].cpu().numpy() for k in fkeys}
+    fields = field_chain(rf, host, nblocks)
+    t_linelocs = time.time() - t0
+    del host
+    nf = len(fields)
+    outlinelen = rf.SysParams["outlinelen"]
+    outlines = rf.SysParams["frame_lines"] // 2 + 1
+    fsz = outlinelen * outlines
+    pics = torch.empty(nf * fsz, dtype=torch.uint16, device="cuda")
+    ll_dev = [torch.from_numpy(ll).cuda() for (_, ll, _, _) in fields]
+    descs = (L.TbcField * nf)()
+    for i, (w, ll, lineoffset, levels) in enumerate(fields):
+        descs[i] = tbc_descriptor(rf, outs["demod"].data_ptr() + 4 * w.startloc, ll_dev[i].data_ptr(),
+                                  lineoffset, outlinelen, outlines, outlines, levels,
+                                  out_u16=pics.data_ptr() + 2 * i * fsz, buf_len=w.length,
+                                  nlines=len(ll))
+
+    def tbc():
+        tbc_fields(rf, descs, stream=sh)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        demod()
+        tbc()
+    torch.cuda.synchronize()
+
+    # ---- timed device-resident steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clk = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    for e0, e1, e2 in ev:
+        e0.record(stream)
+        demod()
+        e1.record(stream)
+        tbc()
+        e2.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    step_ms = [e0.elapsed_time(e2) for e0, _, e2 in ev]
+    demod_ms = [e0.elapsed_time(e1) for e0, e1, _ in ev]
+    tbc_ms = [e1.elapsed_time(e2) for _, e1, e2 in ev]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+
+    # ---- end to end: pinned host capture in, fields/efm/audio out
+    e2e = None
+    if not args.no_e2e:
+        hcap = cap.cpu().pin_memory()
+        hpics = torch.empty(nf * fsz, dtype=torch.uint16).pin_memory()
+        hefm = torch.empty(nout, dtype=torch.int16).pin_memory()
+        hal = torch.empty(nblocks * 991, dtype=torch.float32).pin_memory()
+        har = torch.empty(nblocks * 991, dtype=torch.float32).pin_memory()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            cap.copy_(hcap, non_blocking=True)
+            demod()
+            tbc()
+            hpics.copy_(pics, non_blocking=True)
+            hefm.copy_(outs["efm"], non_blocking=True)
+            hal.copy_(outs["audio_left"], non_blocking=True)
+            har.copy_(outs["audio_right"], non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        h2d = nsamples * 2
+        d2h = nf * fsz * 2 + nout * 2 + 2 * nblocks * 991 * 4
+        e2e = {"value": world * nout / (e2e_ms * 1e-3) / 1e6, "unit": "MSPS", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+               "path": "pinned host capture -> ldg_demod_blocks + ldg_tbc_fields -> host fields, EFM, audio"}
+
+    # ---- plain form: one demodblock() call per block through the Python API
+    plain = None
+    if rank == 0:
+        hc = cap[: 64 * U + N].cpu().numpy()
+        for b in range(3):
+            rf.demodblock(data=hc[b * U:b * U + N], mtf_level=1, cut=True)
+        t0 = time.perf_counter()
+        nplain = 64
+        for b in range(nplain):
+            rf.demodblock(data=hc[b * U:b * U + N], mtf_level=1, cut=True)
+        dt = time.perf_counter() - t0
+        plain = {"value": nplain * U / dt / 1e6, "unit": "MSPS",
+                 "form": "RFDecode.demodblock per block, host numpy in/out (DemodCache worker style)"}
+
+    # ---- roofline of the dominant kernel (demod)
+    peak, peak_kind = peaks()
+    dmed = statistics.median(demod_ms)
+    demod_bytes = nout * BYTES_PER_SAMPLE_DEMOD + nblocks * AUDIO_BYTES_PER_BLOCK
+    achieved = demod_bytes / (dmed * 1e-3) / 1e9
+    # TBC: uint16 field written + the demod span of the field read once
+    tbc_bytes = nf * fsz * 2 + sum(int(ll[-1] - ll[0]) * 4 for (_, ll, _, _) in fields)
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "demod_kernel_traffic.json")
+    if os.path.exists(prof):
+        try:
+            with open(prof) as f:
+                tj = json.load(f)
+            traffic = tj["dram_bytes_per_block"] * nblocks
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(rf, cap, fields, U, nblocks, max_blocks=256)
+
+    res = {
+        "metric": METRIC,
+        "value": world * nout / (ms_per_step * 1e-3) / 1e6,
+        "unit": "MSPS",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generator, ldgpu.synth)",
+        "config": {
+            "workload": f"{system} {args.seconds:g} s capture, {nsamples} int16 samples at 40 MSPS, "
+                        f"{nblocks} blocks x 32768 (stride {U}), {nf} fields per GPU",
+            "outputs": "demod, demod_raw, demod_05, demod_burst" + (", demod_pilot" if system == "PAL" else "")
+                       + ", rfhpf, efm, audio L/R stage 1, uint16 TBC fields",
+            "linelocs": f"host Field.process over GPU demod outputs before timing ({t_linelocs:.1f} s; not in the step)",
+            "l2": "inputs (800 MB) and outputs (> 8 GB) exceed L2 each step; no flush",
+            "parallelism": f"replicas x{world} (one capture per GPU)",
+            "mtf_level": 1,
+        },
+        "fields_per_s": world * nf / (ms_per_step * 1e-3),
+        "kernel_ms": {"demod_median": dmed, "tbc_median": statistics.median(tbc_ms)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "ldg::demod_kernel",
+                     "algorithmic_bytes_per_launch": demod_bytes},
+        "tbc_roofline": {"achieved": tbc_bytes / (statistics.median(tbc_ms) * 1e-3) / 1e9, "unit": "GB/s"},
+        "e2e": e2e,
+        "plain": plain,
+        "cpu_baseline": cpu,
+        "gpu_launches": 3 * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    rf.close()
+
+
+def cpu_demod_sample(rfp, cap, blocks, U, threads):
+    """Oracle demod of `blocks` (list of block indices) with a thread pool."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import demod as odemod
+    N = rfp.blocklen
+
+    def one(b):
+        return odemod.demodblock(cap[b * U:b * U + N], rfp.Filters, system=rfp.system, freq_hz=rfp.freq_hz,
+                                 blockcut_end=rfp.blockcut_end, video_rot=rfp.delays["video_rot"],
+                                 mtf_level=rfp.scaled_mtf(1), cut=True, efm=True, audio=rfp.audio)
+    with ThreadPoolExecutor(threads) as ex:
+        return list(ex.map(one, blocks))
+
+
+def cpu_tbc_sample(rfp, outs_by_block, fields, U, first_block):
+    from oracle import tbc as otbc
+    outw = rfp.SysParams["outlinelen"]
+    outlines = rfp.SysParams["frame_lines"] // 2 + 1
+    demod = np.concatenate([o["video"]["demod"] for o in outs_by_block])
+    n = 0
+    for (w, ll, lineoffset, levels) in fields:
+        lo = w.startloc - first_block * U
+        if lo < 0 or lo + w.length > len(demod):
+            continue
+        buf = demod[lo:lo + w.length]
+        coords, wow = otbc.pixel_coords(ll, rfp.linelen, outw, outlines, lineoffset)
+        ds = otbc.scale_field(buf, coords, wow, rfp.downscale_sinc_lut, lineoffset, outw, outlines * outw)
+        otbc.hz_to_output(ds, levels[0], levels[1], levels[4], levels[2], levels[3])
+        n += 1
+    return n
+
+
+def cpu_baseline(rf, cap, fields, U, nblocks, max_blocks):
+    """The CPU oracle on a bounded sample of the workload, all host threads."""
+    threads = os.cpu_count() or 1
+    hc = cap[: (max_blocks + 1) * U + rf.blocklen].cpu().numpy()
+    nb = min(max_blocks, nblocks)
+    t0 = time.perf_counter()
+    outs = cpu_demod_sample(rf, hc, list(range(nb)), U, threads)
+    t1 = time.perf_counter()
+    nft = cpu_tbc_sample(rf, outs, fields, U, 0)
+    t2 = time.perf_counter()
+    return {"value": nb * U / (t2 - t0) / 1e6, "unit": "MSPS", "cores": threads, "kind": "port",
+            "sample": f"first {nb} blocks ({nb * U} samples) demod + TBC of the {nft} fields inside them; "
+                      f"demod {t1 - t0:.1f} s, TBC {t2 - t1:.1f} s",
+            "impl": "oracle/ numpy FP64 restatement of demodblock + scale_field"}
+
+
+def run_reference(args):
+    """CPU reference arm: the oracle on the host cores, rank 0 only."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    import torch
+    from ldgpu.fieldread import blocks_in_capture
+    from ldgpu.rfdecode import RFParams
+    from ldgpu.synth import synth_capture
+
+    rf = RFParams(system=args.system, decode_analog_audio=44100, decode_digital_audio=True)
+    rf.delays = {"video_rot": 3}
+    N = rf.blocklen
+    U = N - rf.blockcut - rf.blockcut_end
+    nblk = 80  # blocks per step (~2.5 M samples, ~3 fields)
+    nsamples = (nblk - 1) * U + N
+    cap = synth_capture(args.system, nsamples, seed=args.seed).numpy()
+    threads = os.cpu_count() or 1
+    # line locations of the fields in the sample: host Field logic over the oracle outputs
+    outs = cpu_demod_sample(rf, cap, list(range(nblk)), U, threads)
+    from ldgpu.linelocs import FieldLogicNTSC, FieldLogicPAL
+    host = {k: np.concatenate([o["video"][k] for o in outs]) for k in
+            ["demod", "demod_05", "demod_burst"] + (["demod_pilot"] if args.system == "PAL" else [])}
+    fields = _fields_cpu(rf, host, nblk, FieldLogicPAL if args.system == "PAL" else FieldLogicNTSC)
+    for _ in range(args.warmup):
+        o = cpu_demod_sample(rf, cap, list(range(nblk)), U, threads)
+        cpu_tbc_sample(rf, o, fields, U, 0)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o = cpu_demod_sample(rf, cap, list(range(nblk)), U, threads)
+        nft = cpu_tbc_sample(rf, o, fields, U, 0)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = nblk * U / dt / 1e6
+    res = {"metric": METRIC, "value": v, "unit": "MSPS", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, ldgpu.synth)",
+           "impl": "reference",
+           "config": {"workload": f"{args.system} capture sample: {nblk} blocks x 32768 (stride {U}), "
+                                  f"{nft} fields per step (bounded sample of the {args.seconds:g} s workload)",
+                      "parallelism": f"{threads} host threads"},
+           "cpu_baseline": {"value": v, "unit": "MSPS", "cores": threads, "kind": "port",
+                            "sample": f"{nblk} blocks demod + TBC of {nft} fields per step"},
+           "e2e": {"value": v, "unit": "MSPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(res), flush=True)
+
+
+def _fields_cpu(rf, host, nblocks, cls):
+    from ldgpu.fieldread import field_window
+    fields = []
+    start = 0.0
+    prev = None
+    while True:
+        w = field_window(rf, start)
+        if w.first_block + w.nblocks > nblocks:
+            break
+        sl = slice(w.startloc, w.startloc + w.length)
+        f = cls(rf, {"video": {k: v[sl] for k, v in host.items()}, "startloc": w.startloc},
+                prevfield=prev, fields_written=len(fields), readloc=w.startloc)
+        f.process()
+        if not f.valid:
+            start += f.nextfieldoffset
+            prev = None
+            continue
+        lv = (rf.DecoderParams["ire0"], rf.DecoderParams["hz_ire"], rf.DecoderParams["vsync_ire"],
+              f.out_scale, rf.SysParams["outputZero"])
+        fields.append((w, np.asarray(f.linelocs, dtype=np.float64), f.lineoffset, lv))
+        start += f.nextfieldoffset - (w.readloc - w.startloc)
+        prev = f
+    return fields
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

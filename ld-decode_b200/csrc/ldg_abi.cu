@@ -428,15 +428,12 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         const ldg_tbc_field& f = fields[i];
         ldg::TbcField& d = h[i];
         const Host& x = hs[i];
-        if (is_device_ptr(f.linelocs)) {
-            LDG_CK(cudaMemcpyAsync(c->d_ll + llo, f.linelocs, f.nlines * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        } else {
-            memcpy(lls.data() + llo, f.linelocs, f.nlines * sizeof(double));
-        }
+        const bool ll_dev = is_device_ptr(f.linelocs);
+        if (!ll_dev) memcpy(lls.data() + llo, f.linelocs, f.nlines * sizeof(double));
         d.buf = x.buf ? (const float*)(c->d_stage + x.buf_off) : f.buf;
         if (x.buf) LDG_CK(cudaMemcpyAsync((void*)d.buf, f.buf, (size_t)f.buf_len * 4, cudaMemcpyHostToDevice, st));
         d.buf_len = f.buf_len;
-        d.linelocs = c->d_ll + llo;
+        d.linelocs = ll_dev ? f.linelocs : c->d_ll + llo;
         d.nlines = f.nlines;
         d.lineoffset = f.lineoffset;
         d.outwidth = f.outwidth;

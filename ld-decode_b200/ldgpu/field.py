@@ -17,15 +17,16 @@ from .linelocs import FieldLogic, FieldLogicNTSC, FieldLogicPAL
 
 
 def tbc_descriptor(rf, buf, linelocs, lineoffset, outwidth, linesout, outlinecount, levels,
-                   out_u16=None, out_f32=None, coord_f32=False, buf_len=None):
-    """Fill an ldg_tbc_field from numpy arrays or raw device pointers.
+                   out_u16=None, out_f32=None, coord_f32=False, buf_len=None, nlines=None):
+    """Fill an ldg_tbc_field from numpy arrays or raw device pointers (ints;
+    then buf_len / nlines must be given).
 
     `levels` = (ire0, hz_ire, vsync_ire, out_scale, output_zero)."""
     d = L.TbcField()
     d.buf = buf if isinstance(buf, int) else buf.ctypes.data
     d.buf_len = int(buf_len if buf_len is not None else len(buf))
     d.linelocs = linelocs if isinstance(linelocs, int) else linelocs.ctypes.data
-    d.nlines = int(len(linelocs)) if not isinstance(linelocs, int) else 0
+    d.nlines = int(nlines if nlines is not None else len(linelocs))
     d.lineoffset = int(lineoffset)
     d.outwidth = int(outwidth)
     d.linesout = int(linesout)
@@ -40,10 +41,10 @@ def tbc_descriptor(rf, buf, linelocs, lineoffset, outwidth, linesout, outlinecou
 
 
 def tbc_fields(rf, descs, stream=None):
-    """Run ldg_tbc_fields on a list of descriptors."""
+    """Run ldg_tbc_fields on a list (or prebuilt ctypes array) of descriptors."""
     rf._load_lut()
-    arr = (L.TbcField * len(descs))(*descs)
-    L.check(rf._ctx._lib.ldg_tbc_fields(rf._ctx.handle, arr, len(descs), stream))
+    arr = descs if isinstance(descs, ctypes.Array) else (L.TbcField * len(descs))(*descs)
+    L.check(rf._ctx._lib.ldg_tbc_fields(rf._ctx.handle, arr, len(arr), stream))
 
 
 class Field(FieldLogic):
