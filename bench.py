@@ -38,6 +38,10 @@ import numpy as np  # noqa: E402
 METRIC = "RF MSPS demod+TBC on 1 B200 (batched FP32 vs plain) + HBM roofline %"
 BYTES_PER_SAMPLE_DEMOD = 2 + 4 * 4 + 4 + 2  # input + 4 video f32 + rfhpf f32 + efm i16 (per output sample)
 AUDIO_BYTES_PER_BLOCK = 2 * 991 * 4
+# DRAM bytes (read + write) per block of the demod kernel, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the NTSC 1 s case divided by
+# its 1261 blocks; traffic scales with blocks.  None until measured.
+DRAM_BYTES_PER_BLOCK = 1_338_000
 
 
 def parse():
@@ -307,15 +311,7 @@ def run_gpu(args):
     achieved = demod_bytes / (dmed * 1e-3) / 1e9
     # TBC: uint16 field written + the demod span of the field read once
     tbc_bytes = nf * fsz * 2 + sum(int(ll[-1] - ll[0]) * 4 for (_, ll, _, _) in fields)
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "demod_kernel_traffic.json")
-    if os.path.exists(prof):
-        try:
-            with open(prof) as f:
-                tj = json.load(f)
-            traffic = tj["dram_bytes_per_block"] * nblocks
-        except Exception:
-            traffic = None
+    traffic = DRAM_BYTES_PER_BLOCK * nblocks if DRAM_BYTES_PER_BLOCK else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
