@@ -53,7 +53,9 @@ enum {
     LDG_F_BURST = 4,   /* FVideoBurst               (core.py:664-668, 816) */
     LDG_F_PILOT = 5,   /* FVideoPilot, PAL          (core.py:670-679, 820) */
     LDG_F_EFM = 6,     /* Fefm                      (core.py:422-465, 848) */
-    LDG_NFILTERS = 7
+    LDG_F_VIDEO_G_ODD = 7, /* RFVideo * MTF^mtf * exp(+2 pi i k/N): the
+                              odd-sample half of the analytic inverse FFT */
+    LDG_NFILTERS = 8
 };
 
 /* input sample type of ldg_demod_args.in */

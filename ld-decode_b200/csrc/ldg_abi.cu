@@ -70,7 +70,8 @@ struct ldg_ctx {
     int a_lowbin[2] = {0, 0};
     double a_rate[2] = {0, 0};
     double a_low[2] = {0, 0};
-    float2* d_tw = nullptr;  // 256 hi + 128 lo
+    float2* d_tw16 = nullptr;  // W_16384^i
+    float2* d_tw32 = nullptr;  // W_32768^k, k <= 8192
     float* d_lut = nullptr;
     float2* d_scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -148,19 +149,21 @@ int ldg_ctx_create(ldg_ctx** out, int32_t device, int32_t system, int32_t blockl
         delete c;
         return fail(LDG_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
     }
-    // twiddles W_N^k = exp(-2 pi i k/N) in FP64, stored FP32
-    std::vector<float2> tw(ldg::kTwHi + ldg::kTwLo);
+    // twiddle tables in FP64, stored FP32
     const double two_pi = 6.283185307179586476925286766559;
-    for (int a = 0; a < ldg::kTwHi; ++a) {
-        const double ang = -two_pi * (double)(128 * a) / ldg::kN;
-        tw[a] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    std::vector<float2> t16(ldg::kT16), t32(ldg::kT32);
+    for (int i = 0; i < ldg::kT16; ++i) {
+        const double ang = -two_pi * (double)i / ldg::kT16;
+        t16[i] = make_float2((float)std::cos(ang), (float)std::sin(ang));
     }
-    for (int b = 0; b < ldg::kTwLo; ++b) {
-        const double ang = -two_pi * (double)b / ldg::kN;
-        tw[ldg::kTwHi + b] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    for (int k = 0; k < ldg::kT32; ++k) {
+        const double ang = -two_pi * (double)k / ldg::kN;
+        t32[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
     }
-    if (cudaMalloc(&c->d_tw, tw.size() * sizeof(float2)) != cudaSuccess ||
-        cudaMemcpy(c->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+    if (cudaMalloc(&c->d_tw16, t16.size() * sizeof(float2)) != cudaSuccess ||
+        cudaMemcpy(c->d_tw16, t16.data(), t16.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc(&c->d_tw32, t32.size() * sizeof(float2)) != cudaSuccess ||
+        cudaMemcpy(c->d_tw32, t32.data(), t32.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess || cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
         const std::string msg = cudaGetErrorString(cudaGetLastError());
         ldg_ctx_destroy(c);
@@ -176,7 +179,8 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& f : c->d_filter) cudaFree(f);
     for (auto& a : c->d_audio) cudaFree(a);
-    cudaFree(c->d_tw);
+    cudaFree(c->d_tw16);
+    cudaFree(c->d_tw32);
     cudaFree(c->d_lut);
     cudaFree(c->d_scratch);
     cudaFree(c->d_stage);
@@ -207,7 +211,8 @@ int ldg_set_audio(ldg_ctx* c, int32_t ch, int32_t lowbin, int32_t nbins, const d
     if (!c || !filt1) return fail(LDG_ERR_ARG, "ldg_set_audio: NULL argument");
     if (ch < 0 || ch > 1) return fail(LDG_ERR_ARG, "ldg_set_audio: channel must be 0 or 1");
     if (nbins != 1024) return fail(LDG_ERR_UNSUPPORTED, "ldg_set_audio: only 1024-bin audio bands are supported");
-    if (lowbin < 1 || lowbin + nbins / 2 >= ldg::kM) return fail(LDG_ERR_ARG, "ldg_set_audio: band outside the spectrum");
+    if (lowbin < 1 || lowbin + nbins / 2 > ldg::kM / 2)
+        return fail(LDG_ERR_ARG, "ldg_set_audio: band outside the spectrum");
     std::lock_guard<std::mutex> lk(c->mu);
     DeviceGuard g(c->device);
     std::vector<float2> h(nbins / 2 + 1);
@@ -253,7 +258,8 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     if (a->roll_05 < 0 || a->roll_05 >= N || a->roll_burst < 0 || a->roll_burst >= N)
         return fail(LDG_ERR_ARG, "ldg_demod_blocks: roll outside the block");
     std::lock_guard<std::mutex> lk(c->mu);
-    if (!c->d_filter[LDG_F_VIDEO_G]) return fail(LDG_ERR_STATE, "ldg_demod_blocks: RFVideo filter not set");
+    if (!c->d_filter[LDG_F_VIDEO_G] || !c->d_filter[LDG_F_VIDEO_G_ODD])
+        return fail(LDG_ERR_STATE, "ldg_demod_blocks: RFVideo filter not set");
     const bool want_video[4] = {a->out_demod != nullptr, a->out_05 != nullptr, a->out_burst != nullptr,
                                 a->out_pilot != nullptr};
     const int fslot[4] = {LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT};
@@ -323,6 +329,7 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     p.fs_hz = (float)c->fs_hz;
     p.f_rfhpf = c->d_filter[LDG_F_RFHPF];
     p.f_g = c->d_filter[LDG_F_VIDEO_G];
+    p.f_godd = c->d_filter[LDG_F_VIDEO_G_ODD];
     for (int o = 0; o < 4; ++o) {
         p.f_video[o] = c->d_filter[fslot[o]];
         p.o_video[o] = (float*)dev(i_vid[o]);
@@ -352,8 +359,8 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     p.o_audio[1] = (float*)dev(i_ar);
     p.s_audio = {a->audio.start, a->audio.len, 0};
     p.scratch = c->d_scratch;
-    p.tw_hi = c->d_tw;
-    p.tw_lo = c->d_tw + ldg::kTwHi;
+    p.tw16 = c->d_tw16;
+    p.tw32 = c->d_tw32;
 
     cudaError_t e = ldg::launch_demod(p, grid, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("demod launch: ") + cudaGetErrorString(e));
@@ -373,7 +380,7 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
     std::lock_guard<std::mutex> lk(c->mu);
     if (!c->d_lut) return fail(LDG_ERR_STATE, "ldg_tbc_fields: sinc table not set");
     size_t ll_total = 0, seg_total = 0;
-    long long max_nout = 0;
+    int max_lines = 0;
     for (int i = 0; i < nfields; ++i) {
         const ldg_tbc_field& f = fields[i];
         if (!f.buf || !f.linelocs) return fail(LDG_ERR_ARG, "ldg_tbc_fields: NULL buffer");
@@ -382,10 +389,11 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
             return fail(LDG_ERR_ARG, "ldg_tbc_fields: bad field geometry");
         if (!(f.inlinelen > 0) || !(f.outlinelen > 0) || !(f.hz_ire != 0))
             return fail(LDG_ERR_ARG, "ldg_tbc_fields: bad line length or level");
+        if (f.outlinelen != (double)(int)f.outlinelen)
+            return fail(LDG_ERR_ARG, "ldg_tbc_fields: outlinelen must be an integer");
         ll_total += f.nlines;
         seg_total += f.nlines - 1;
-        const long long n = (long long)f.linesout * f.outwidth;
-        if (n > max_nout) max_nout = n;
+        if (f.linesout > max_lines) max_lines = f.linesout;
     }
     DeviceGuard g(c->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
@@ -442,6 +450,7 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         d.coord_f32 = f.coord_f32;
         d.inlinelen = f.inlinelen;
         d.outscale = f.inlinelen / f.outlinelen;
+        d.outlinelen_i = (int)f.outlinelen;
         d.u16_scale = f.out_scale / f.hz_ire;
         d.u16_offset = f.output_zero - f.vsync_ire * f.out_scale - f.ire0 * d.u16_scale;
         d.seg_level = c->d_seg + sego;
@@ -462,7 +471,7 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         }
     }
     LDG_CK(cudaMemcpyAsync(c->d_fields, h.data(), nfields * sizeof(ldg::TbcField), cudaMemcpyHostToDevice, st));
-    cudaError_t e = ldg::launch_tbc(c->d_fields, nfields, max_nout, c->d_lut, 15.0, st);
+    cudaError_t e = ldg::launch_tbc(c->d_fields, nfields, max_lines, c->d_lut, 15.0, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
     if (any_host) {
         for (int i = 0; i < nfields; ++i) {

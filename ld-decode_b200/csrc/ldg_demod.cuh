@@ -24,7 +24,8 @@ struct DemodParams {
     float fs_hz;          // input sample rate
     // half spectra, bins 0..N/2 (float2[N/2+1]); G = RFVideo * MTF^m
     const float2* f_rfhpf;
-    const float2* f_g;
+    const float2* f_g;      // RFVideo * MTF^m
+    const float2* f_godd;   // G * W_N^-k (odd-sample spectrum of the analytic signal)
     const float2* f_video[OUT_NVIDEO];
     const float2* f_efm;
 
@@ -49,12 +50,12 @@ struct DemodParams {
 
     // per-CTA global scratch (2 * N/2 float2 per CTA), L2 resident
     float2* scratch;
-    const float2* tw_hi;
-    const float2* tw_lo;
+    const float2* tw16;     // W_16384^i, i < 16384
+    const float2* tw32;     // W_32768^k, k <= 8192
 };
 
 // Dynamic shared memory the kernel needs.
-constexpr int kSmemFloat2 = (16384 + 1024) + 2 * (1024 + 64) + 256 + 128;
+constexpr int kSmemFloat2 = (16384 + 1024) + 2 * (1024 + 64);
 constexpr size_t kSmemBytes = size_t(kSmemFloat2) * 8;
 constexpr size_t kScratchPerCta = size_t(2) * 16384 * 8;
 

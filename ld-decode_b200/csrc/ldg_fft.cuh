@@ -11,20 +11,28 @@
 // padded by one float2 per 16 (pad(i) = i + i/16), which makes the
 // stride-16 stores of the first pass bank-conflict free.
 //
-// Twiddles W_N^k = exp(-2 pi i k / N), N = 32768, come from two small
-// tables built on the host in FP64 and stored as FP32:
-// W_N^k = hi[k >> 7] * lo[k & 127].
+// The first pass can take its inputs from a loader functor (global memory,
+// with a filter product fused in) and the last pass can hand its outputs to
+// a storer functor (straight to global memory), which saves a shared-memory
+// round trip at each end.
+//
+// Twiddles come from tables built on the host in FP64 and stored as FP32:
+// T16[i] = exp(-2 pi i i/16384) (the pass twiddles W_{Ns R}^{k r} are
+// T16[k r 16384/(Ns R)]); a radix-16 butterfly reads W^k, W^2k, W^4k, W^8k
+// and forms the other eleven by at most three complex products.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 namespace ldg {
 
 constexpr int kN = 32768;          // real block length
 constexpr int kM = kN / 2;         // complex FFT length
 constexpr int kThreads = 1024;     // threads per demod CTA
-constexpr int kTwHi = kN / 128;    // 256 coarse twiddles
-constexpr int kTwLo = 128;         // 128 fine twiddles
+constexpr int kT16 = 16384;        // entries of the pass twiddle table
+constexpr int kT32 = kM / 2 + 1;   // entries of the real-FFT twiddle table W_N^k, k <= M/2
 
 __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int padded(int n) { return n + (n >> 4); }
@@ -37,17 +45,16 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 
-// Twiddle tables in shared memory.
-struct Twiddles {
-    const float2* hi;  // hi[a] = W_N^(128 a), a < 256
-    const float2* lo;  // lo[b] = W_N^b, b < 128
-    // W_N^k for 0 <= k < N; conj() of it for the inverse direction.
-    template <bool INV>
-    __device__ __forceinline__ float2 w(int k) const {
-        float2 t = cmul(hi[(k >> 7) & (kTwHi - 1)], lo[k & (kTwLo - 1)]);
-        return INV ? cconj(t) : t;
-    }
+struct Tables {
+    const float2* t16;  // W_16384^i, i < 16384
+    const float2* t32;  // W_32768^k, k <= 8192
 };
+
+template <bool INV>
+__device__ __forceinline__ float2 tw16(const Tables& t, int i) {
+    const float2 w = __ldg(t.t16 + (i & (kT16 - 1)));
+    return INV ? cconj(w) : w;
+}
 
 // cos/sin(2 pi m / 32) for m = 0..15
 __device__ __forceinline__ float c32(int m) {
@@ -86,7 +93,7 @@ __host__ __device__ constexpr int bitrev(int i, int bits) {
 }
 
 // R-point DFT in registers, decimation in frequency; on return v[i] holds
-// output bin bitrev(i).  R is 4, 16 or 32.
+// output bin bitrev(i).  R is 4 or 16.
 template <int R, bool INV>
 __device__ __forceinline__ void dft_dif(float2 (&v)[R]) {
 #pragma unroll
@@ -104,22 +111,59 @@ __device__ __forceinline__ void dft_dif(float2 (&v)[R]) {
     }
 }
 
+// Multiply v[r] by W^(e r) for r = 1..R-1, W^e = T16[e] (e in table units).
+template <int R, bool INV>
+__device__ __forceinline__ void apply_twiddles(float2 (&v)[R], const Tables& t, int e) {
+    if constexpr (R == 4) {
+        const float2 w1 = tw16<INV>(t, e), w2 = tw16<INV>(t, 2 * e), w3 = tw16<INV>(t, 3 * e);
+        v[1] = cmul(v[1], w1);
+        v[2] = cmul(v[2], w2);
+        v[3] = cmul(v[3], w3);
+    } else {
+        const float2 w1 = tw16<INV>(t, e), w2 = tw16<INV>(t, 2 * e);
+        const float2 w4 = tw16<INV>(t, 4 * e), w8 = tw16<INV>(t, 8 * e);
+        const float2 w3 = cmul(w2, w1), w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
+        v[1] = cmul(v[1], w1);
+        v[2] = cmul(v[2], w2);
+        v[3] = cmul(v[3], w3);
+        v[4] = cmul(v[4], w4);
+        v[5] = cmul(v[5], w5);
+        v[6] = cmul(v[6], w6);
+        v[7] = cmul(v[7], w7);
+        v[8] = cmul(v[8], w8);
+        v[9] = cmul(v[9], cmul(w8, w1));
+        v[10] = cmul(v[10], cmul(w8, w2));
+        v[11] = cmul(v[11], cmul(w8, w3));
+        v[12] = cmul(v[12], cmul(w8, w4));
+        v[13] = cmul(v[13], cmul(w8, w5));
+        v[14] = cmul(v[14], cmul(w8, w6));
+        v[15] = cmul(v[15], cmul(w8, w7));
+    }
+}
+
+// Loader / storer placeholder: read / write the shared working set.
+struct SmemIO {};
+
 // One Stockham pass of radix R over NB independent padded M-point working
-// sets laid out back to back (set b starts at S + b * padded(M)) in shared
-// memory.  Ns = product of the radices of the earlier passes.  The pass
-// twiddle W_{Ns R}^{k r} is read as W_N^{k r N/(Ns R)}.  All threads of the
-// CTA must call it; it starts with the loads (callers sync before) and ends
-// with a barrier.
-template <int R, int M, int NB, bool INV>
-__device__ __forceinline__ void stockham_pass(float2* S, int Ns, const Twiddles& tw) {
+// sets laid out back to back (set b starts at S + b * padded(M)).
+// Ns = product of the radices of the earlier passes.  `ld(b, idx)` supplies
+// the inputs when LD is not SmemIO; `st(b, idx, value)` consumes the outputs
+// when ST is not SmemIO.  All threads of the CTA must call it; it starts
+// with the loads (callers sync before) and ends with a barrier.  Kept out
+// of line so each pass gets the whole 64-register budget (inlined into the
+// demod kernel, live state around the passes made the allocator spill).
+template <int R, int M, int NB, bool INV, class LD, class ST>
+__device__ __noinline__ void stockham_pass(float2* S, int Ns, const Tables& t, const LD& ld, const ST& st) {
     constexpr int B = M / R;                       // butterflies per set
     constexpr int BT = B * NB;                     // butterflies per pass
     constexpr int PER = (BT + kThreads - 1) / kThreads;
     static_assert(BT % kThreads == 0 || BT < kThreads, "butterfly count");
     constexpr int bits = ilog2(R);
     constexpr int stride = padded(M);
+    constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
+    constexpr bool to_smem = std::is_same<ST, SmemIO>::value;
     float2 v[PER][R];
-    const int scale = kN / (Ns * R);
+    const int scale = kT16 / (Ns * R);
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
         const int jt = threadIdx.x + q * kThreads;
@@ -127,16 +171,19 @@ __device__ __forceinline__ void stockham_pass(float2* S, int Ns, const Twiddles&
             const int b = jt / B, j = jt - b * B;
             const float2* Sb = S + b * stride;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[q][r] = Sb[pad(j + r * B)];
-            const int k = j % Ns;
-            if (Ns > 1) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], tw.w<INV>((k * r * scale) & (kN - 1)));
+            for (int r = 0; r < R; ++r) {
+                if constexpr (from_smem) {
+                    v[q][r] = Sb[pad(j + r * B)];
+                } else {
+                    v[q][r] = ld(b, j + r * B);
+                }
             }
+            if (Ns > 1) apply_twiddles<R, INV>(v[q], t, (j % Ns) * scale);
             dft_dif<R, INV>(v[q]);
         }
     }
-    __syncthreads();
+    // loads from shared memory must all complete before any thread stores
+    if constexpr (from_smem && to_smem) __syncthreads();
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
         const int jt = threadIdx.x + q * kThreads;
@@ -146,30 +193,39 @@ __device__ __forceinline__ void stockham_pass(float2* S, int Ns, const Twiddles&
             const int k = j % Ns;
             const int d = (j / Ns) * Ns * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) Sb[pad(d + r * Ns)] = v[q][bitrev(r, bits)];
+            for (int r = 0; r < R; ++r) {
+                if constexpr (to_smem) {
+                    Sb[pad(d + r * Ns)] = v[q][bitrev(r, bits)];
+                } else {
+                    st(b, d + r * Ns, v[q][bitrev(r, bits)]);
+                }
+            }
         }
     }
     __syncthreads();
 }
 
 // Unnormalised 16384-point complex FFT of the padded working set S.
-// The radix-4 pass runs 4 butterflies per thread (16 values, as the others).
-// Forward uses exp(-2 pi i nk/M); inverse exp(+2 pi i nk/M).
-template <bool INV>
-__device__ __noinline__ void fft16k(float2* S, const Twiddles& tw) {
-    stockham_pass<16, kM, 1, INV>(S, 1, tw);
-    stockham_pass<16, kM, 1, INV>(S, 16, tw);
-    stockham_pass<16, kM, 1, INV>(S, 256, tw);
-    stockham_pass<4, kM, 1, INV>(S, 4096, tw);
+// Forward uses exp(-2 pi i nk/M); inverse exp(+2 pi i nk/M).  The first
+// pass reads through `ld` and the last pass writes through `st` unless they
+// are SmemIO.  Callers must __syncthreads() before when S was just written.
+template <bool INV, class LD = SmemIO, class ST = SmemIO>
+__device__ __forceinline__ void fft16k(float2* S, const Tables& t, const LD& ld = LD(), const ST& st = ST()) {
+    const SmemIO s;
+    stockham_pass<16, kM, 1, INV>(S, 1, t, ld, s);
+    stockham_pass<16, kM, 1, INV>(S, 16, t, s, s);
+    stockham_pass<16, kM, 1, INV>(S, 256, t, s, s);
+    stockham_pass<4, kM, 1, INV>(S, 4096, t, s, st);
 }
 
 // Two independent unnormalised 1024-point complex FFTs (the analog-audio
 // sub-bands), sets at S and S + padded(1024).
 template <bool INV>
-__device__ __forceinline__ void fft1k_x2(float2* S, const Twiddles& tw) {
-    stockham_pass<16, 1024, 2, INV>(S, 1, tw);
-    stockham_pass<16, 1024, 2, INV>(S, 16, tw);
-    stockham_pass<4, 1024, 2, INV>(S, 256, tw);
+__device__ __forceinline__ void fft1k_x2(float2* S, const Tables& t) {
+    const SmemIO s;
+    stockham_pass<16, 1024, 2, INV>(S, 1, t, s, s);
+    stockham_pass<16, 1024, 2, INV>(S, 16, t, s, s);
+    stockham_pass<4, 1024, 2, INV>(S, 256, t, s, s);
 }
 
 }  // namespace ldg

@@ -21,15 +21,6 @@ namespace {
 constexpr int kWowThreads = 512;
 constexpr int kMaxSeg = kWowThreads;  // segments (lines - 1) per field handled
 
-// The spline segment of output pixel i: j with j*inl <= x < (j+1)*inl,
-// x = i * outscale, clamped to [0, nseg-1] (a degree-1 B-spline's interval).
-__device__ __forceinline__ int segment_of(double x, double inl, int nseg) {
-    int j = (int)floor(x / inl);
-    if ((double)j * inl > x) --j;
-    if ((double)(j + 1) * inl <= x) ++j;
-    return min(max(j, 0), nseg - 1);
-}
-
 __device__ __forceinline__ long long first_pixel_at(double xk, double outscale) {
     // smallest i >= 0 with i * outscale >= xk (same FP product as the gather)
     long long i = (long long)ceil(xk / outscale);
@@ -142,59 +133,107 @@ __global__ void __launch_bounds__(kWowThreads) wow_levels_kernel(const TbcField*
     }
 }
 
-__global__ void __launch_bounds__(256) tbc_gather_kernel(const TbcField* fields, const float* lut,
-                                                         int nfields) {
-    const int fi = blockIdx.y;
-    if (fi >= nfields) return;
-    const TbcField& f = fields[fi];
-    const long long nout = (long long)f.linesout * f.outwidth;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nout) return;
-    const long long ig = i + (long long)f.outwidth * (f.lineoffset + 1);
+constexpr int kGatherThreads = 256;
+constexpr int kSpanMax = 6144;  // staged input samples per output line (24 KB)
+
+// Input coordinate (FP64) of output pixel ig, optionally rounded to float32
+// as the reference does; the spline segment j is also returned.
+__device__ __forceinline__ double pixel_coord(const TbcField& f, long long ig, int nseg, int& j) {
     const double inl = f.inlinelen;
-    const int nseg = f.nlines - 1;
     const double x = __dmul_rn((double)ig, f.outscale);
-    const int j = segment_of(x, inl, nseg);
+    // nominal segment from the integer pixel index, then exact comparisons
+    j = (int)(ig / (long long)f.outlinelen_i);
+    j = min(max(j, 0), nseg - 1);
+    while (j > 0 && (double)j * inl > x) --j;
+    while (j < nseg - 1 && (double)(j + 1) * inl <= x) ++j;
     const double x0 = (double)j * inl, x1 = (double)(j + 1) * inl;
     const double y0 = f.linelocs[j], y1 = f.linelocs[j + 1];
     const double w = 1.0 / (x1 - x0);
     double c = __dadd_rn(__dmul_rn(y0, __dmul_rn(w, x1 - x)), __dmul_rn(y1, __dmul_rn(w, x - x0)));
     if (f.coord_f32) c = (double)__double2float_rn(c);
-    const long long ci = (long long)c;
-    const double ph = __dmul_rn(c - (double)ci, 65536.0);
-    const int ps = (int)ph;
-    const float alpha = __double2float_rn(ph - (double)ps);
-    const float* w0 = lut + (size_t)ps * 16;
-    const float* w1 = w0 + 16;
-    const long long start = ci - 7;
-    double acc = 0.0;
-    if (start >= 0 && start + 16 <= f.buf_len && ps >= 0 && ps < 65536) {
-#pragma unroll
-        for (int t = 0; t < 16; ++t) {
-            const float ws = __ldg(w0 + t);
-            const float wt = fmaf(alpha, __ldg(w1 + t) - ws, ws);
-            acc += (double)(__ldg(f.buf + start + t) * wt);
-        }
-    } else if (f.status) {
-        atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
+    return c;
+}
+
+// One CTA per (output line, field): stage the line's input span in shared
+// memory, then one thread per output pixel.
+__global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcField* fields, const float* lut,
+                                                                    int nfields) {
+    __shared__ float span[kSpanMax];
+    __shared__ long long span_base;
+    __shared__ int span_len;
+    const int fi = blockIdx.y;
+    if (fi >= nfields) return;
+    const TbcField& f = fields[fi];
+    const int line = blockIdx.x;
+    if (line >= f.linesout) return;
+    const int nseg = f.nlines - 1;
+    const long long i0 = (long long)line * f.outwidth;
+    const long long ig0 = i0 + (long long)f.outwidth * (f.lineoffset + 1);
+    if (threadIdx.x == 0) {
+        int j;
+        const double c0 = pixel_coord(f, ig0, nseg, j);
+        const double c1 = pixel_coord(f, ig0 + f.outwidth - 1, nseg, j);
+        long long lo = (long long)fmin(c0, c1) - 8;
+        long long hi = (long long)fmax(c0, c1) + 10;
+        lo = max(lo, 0LL);
+        hi = min(hi, f.buf_len);
+        span_base = lo;
+        span_len = (hi > lo && hi - lo <= kSpanMax) ? (int)(hi - lo) : 0;
     }
-    const float out = (float)(f.seg_level[j] * acc);
-    if (f.out_f32) f.out_f32[i] = out;
-    if (f.out_u16) {
-        double v = (double)out * f.u16_scale + f.u16_offset + 0.5;
-        v = fmin(fmax(v, 0.0), 65535.0);
-        f.out_u16[i] = (uint16_t)(unsigned)v;
+    __syncthreads();
+    const long long base = span_base;
+    const int slen = span_len;
+    for (int k = threadIdx.x; k < slen; k += kGatherThreads) span[k] = __ldg(f.buf + base + k);
+    __syncthreads();
+
+    for (int c = threadIdx.x; c < f.outwidth; c += kGatherThreads) {
+        int j;
+        const double cc = pixel_coord(f, ig0 + c, nseg, j);
+        const long long ci = (long long)cc;
+        const double ph = __dmul_rn(cc - (double)ci, 65536.0);
+        const int ps = (int)ph;
+        const float alpha = __double2float_rn(ph - (double)ps);
+        const long long start = ci - 7;
+        double acc = 0.0;
+        if (start >= 0 && start + 16 <= f.buf_len && ps >= 0 && ps < 65536) {
+            const float4* w0 = reinterpret_cast<const float4*>(lut + (size_t)ps * 16);
+            const float4* w1 = w0 + 4;
+            const long long rel = start - base;
+            const bool staged = slen > 0 && rel >= 0 && rel + 16 <= slen;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 a = __ldg(w0 + q);
+                const float4 b = __ldg(w1 + q);
+                const float wa[4] = {fmaf(alpha, b.x - a.x, a.x), fmaf(alpha, b.y - a.y, a.y),
+                                     fmaf(alpha, b.z - a.z, a.z), fmaf(alpha, b.w - a.w, a.w)};
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const float v = staged ? span[rel + 4 * q + t] : __ldg(f.buf + start + 4 * q + t);
+                    acc += (double)(v * wa[t]);
+                }
+            }
+        } else if (f.status) {
+            atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
+        }
+        const float out = (float)(f.seg_level[j] * acc);
+        const long long i = i0 + c;
+        if (f.out_f32) f.out_f32[i] = out;
+        if (f.out_u16) {
+            double v = (double)out * f.u16_scale + f.u16_offset + 0.5;
+            v = fmin(fmax(v, 0.0), 65535.0);
+            f.out_u16[i] = (uint16_t)(unsigned)v;
+        }
     }
 }
 
-cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout, const float* lut,
+cudaError_t launch_tbc(const TbcField* dfields, int nfields, int max_lines, const float* lut,
                        double threshold_mult, cudaStream_t stream) {
     if (nfields <= 0) return cudaSuccess;
     wow_levels_kernel<<<nfields, kWowThreads, 0, stream>>>(dfields, threshold_mult);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    dim3 grid((unsigned)((max_nout + 255) / 256), (unsigned)nfields);
-    tbc_gather_kernel<<<grid, 256, 0, stream>>>(dfields, lut, nfields);
+    dim3 grid((unsigned)max_lines, (unsigned)nfields);
+    tbc_gather_kernel<<<grid, kGatherThreads, 0, stream>>>(dfields, lut, nfields);
     return cudaGetLastError();
 }
 

@@ -19,6 +19,7 @@ struct TbcField {
     int coord_f32;
     double inlinelen;
     double outscale;     // inlinelen / outlinelen
+    int outlinelen_i;    // outlinelen (integer) for the nominal segment of a pixel
     double u16_scale;    // out_scale / hz_ire
     double u16_offset;   // output_zero - vsync_ire*out_scale - ire0*u16_scale
     double* seg_level;   // nlines-1 level-adjust factors (device scratch)
@@ -27,7 +28,7 @@ struct TbcField {
     uint16_t* out_u16;
 };
 
-cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout, const float* lut,
+cudaError_t launch_tbc(const TbcField* dfields, int nfields, int max_lines, const float* lut,
                        double threshold_mult, cudaStream_t stream);
 
 }  // namespace ldg

@@ -16,8 +16,8 @@ LDG_OK = 0
 LDG_NTSC, LDG_PAL = 0, 1
 LDG_IN_INT16, LDG_IN_FLOAT32 = 0, 1
 (LDG_F_RFHPF, LDG_F_VIDEO_G, LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT,
- LDG_F_EFM) = range(7)
-LDG_NFILTERS = 7
+ LDG_F_EFM, LDG_F_VIDEO_G_ODD) = range(8)
+LDG_NFILTERS = 8
 
 ERRORS = {-1: "argument", -2: "cuda", -3: "state", -4: "unsupported", -5: "range"}
 

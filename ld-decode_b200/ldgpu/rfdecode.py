@@ -195,7 +195,11 @@ class RFDecode(RFParams):
         if mtf_level != 0:
             g = g * (self.Filters["MTF"] ** mtf_level)
         m = self.blocklen // 2
-        self._set_filter(L.LDG_F_VIDEO_G, np.ascontiguousarray(g[:m + 1]))
+        gh = np.ascontiguousarray(g[:m + 1])
+        self._set_filter(L.LDG_F_VIDEO_G, gh)
+        # odd output samples of the one-sided inverse: G[k] * exp(+2 pi i k / N)
+        k = np.arange(m + 1)
+        self._set_filter(L.LDG_F_VIDEO_G_ODD, gh * np.exp(2j * np.pi * k / self.blocklen))
         self._mtf_loaded = mtf_level
 
     def _load_lut(self):
