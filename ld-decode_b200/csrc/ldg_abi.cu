@@ -318,6 +318,9 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
         if (!bufs[i].user) return nullptr;
         return bufs[i].host ? (void*)(c->d_stage + bufs[i].off) : bufs[i].user;
     };
+    // the kernel reads samples in pairs: 4-byte (int16) / 8-byte (float32) aligned block starts
+    if ((a->in_stride & 1) != 0 || (reinterpret_cast<uintptr_t>(dev(i_in)) & (esz == 2 ? 3 : 7)) != 0)
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks: input blocks must start on an even sample of an aligned buffer");
     if (bufs[i_in].host) LDG_CK(cudaMemcpyAsync(dev(i_in), a->in, bufs[i_in].bytes, cudaMemcpyHostToDevice, st));
 
     ldg::DemodParams p;

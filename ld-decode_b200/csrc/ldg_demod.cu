@@ -84,7 +84,7 @@ struct RealStorer {
     __device__ void operator()(int, int m, float2 v) const {
         const int i0 = (2 * m - roll - start) & (kN - 1);
         const int i1 = (i0 + 1) & (kN - 1);
-        if (((i0 & 1) == 0) && i0 + 1 < len) {
+        if (((i0 & 1) == 0) && i0 + 1 < len && ((reinterpret_cast<uintptr_t>(out + i0) & 7) == 0)) {
             *reinterpret_cast<float2*>(out + i0) = make_float2(v.x * kInvM, v.y * kInvM);
         } else {
             if (i0 < len) out[i0] = v.x * kInvM;
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
                 const float dodd = fm_disc(zo, ze, kfs);
                 if (oraw) {
                     const int i0 = 2 * m - vs;
-                    if (((i0 & 1) == 0) && i0 >= 0 && i0 + 1 < vl) {
+                    if (i0 >= 0 && i0 + 1 < vl && ((reinterpret_cast<uintptr_t>(oraw + i0) & 7) == 0)) {
                         *reinterpret_cast<float2*>(oraw + i0) = make_float2(de, dodd);
                     } else {
                         if (i0 >= 0 && i0 < vl) oraw[i0] = de;
