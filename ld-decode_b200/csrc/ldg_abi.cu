@@ -453,7 +453,7 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         d.coord_f32 = f.coord_f32;
         d.inlinelen = f.inlinelen;
         d.outscale = f.inlinelen / f.outlinelen;
-        d.outlinelen_i = (int)f.outlinelen;
+        d.inv_inl = 1.0 / f.inlinelen;
         d.u16_scale = f.out_scale / f.hz_ire;
         d.u16_offset = f.output_zero - f.vsync_ire * f.out_scale - f.ire0 * d.u16_scale;
         d.seg_level = c->d_seg + sego;

@@ -206,9 +206,17 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
     extern __shared__ float2 smem[];
     float2* S = smem;
     float2* A = smem + padded(kM);
+    float2* s2 = A + 2 * padded(1024);
+    float2* s3 = s2 + kS2;
+    float2* s4 = s3 + kS3;
+    load_pass_tables(s2, s3, s4, p.tw16);
     Tables t;
     t.t16 = p.tw16;
     t.t32 = p.tw32;
+    t.s2 = s2;
+    t.s3 = s3;
+    t.s4 = s4;
+    __syncthreads();
 
     for (int blk = blockIdx.x; blk < p.nblocks; blk += gridDim.x) {
         float2* parkX = p.scratch + (size_t)blockIdx.x * 2 * kM;

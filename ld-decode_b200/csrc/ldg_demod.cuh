@@ -55,7 +55,7 @@ struct DemodParams {
 };
 
 // Dynamic shared memory the kernel needs.
-constexpr int kSmemFloat2 = (16384 + 1024) + 2 * (1024 + 64);
+constexpr int kSmemFloat2 = (16384 + 1024) + 2 * (1024 + 64) + 4 * 16 + 4 * 256 + 4096;
 constexpr size_t kSmemBytes = size_t(kSmemFloat2) * 8;
 constexpr size_t kScratchPerCta = size_t(2) * 16384 * 8;
 

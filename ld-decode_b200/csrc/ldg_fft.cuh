@@ -16,10 +16,10 @@
 // a storer functor (straight to global memory), which saves a shared-memory
 // round trip at each end.
 //
-// Twiddles come from tables built on the host in FP64 and stored as FP32:
-// T16[i] = exp(-2 pi i i/16384) (the pass twiddles W_{Ns R}^{k r} are
-// T16[k r 16384/(Ns R)]); a radix-16 butterfly reads W^k, W^2k, W^4k, W^8k
-// and forms the other eleven by at most three complex products.
+// Twiddles come from a table built on the host in FP64 and stored as FP32,
+// T16[i] = exp(-2 pi i i/16384), copied into small per-pass shared tables
+// at kernel start; a radix-16 butterfly reads W^k, W^2k, W^4k, W^8k and
+// forms the other eleven by at most three complex products.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -46,14 +46,27 @@ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 
 struct Tables {
-    const float2* t16;  // W_16384^i, i < 16384
-    const float2* t32;  // W_32768^k, k <= 8192
+    const float2* t16;  // global: W_16384^i, i < 16384
+    const float2* t32;  // global: W_32768^k, k <= 8192 (real-FFT pre/post-processing)
+    // shared-memory pass tables, laid out so a warp reads consecutive entries
+    const float2* s2;   // [4][16]:   W_256^(k 2^r)  (pass Ns = 16, radix 16)
+    const float2* s3;   // [4][256]:  W_4096^(k 2^r) (pass Ns = 256, radix 16)
+    const float2* s4;   // [4096]:    W_16384^k      (pass Ns = 4096, radix 4)
 };
 
-template <bool INV>
-__device__ __forceinline__ float2 tw16(const Tables& t, int i) {
-    const float2 w = __ldg(t.t16 + (i & (kT16 - 1)));
-    return INV ? cconj(w) : w;
+constexpr int kS2 = 4 * 16, kS3 = 4 * 256, kS4 = 4096;  // float2 entries of the shared tables
+
+// Fill the shared pass tables from the global W_16384 table (all threads).
+__device__ __forceinline__ void load_pass_tables(float2* s2, float2* s3, float2* s4, const float2* t16) {
+    for (int i = threadIdx.x; i < kS4; i += blockDim.x) s4[i] = __ldg(t16 + i);
+    for (int i = threadIdx.x; i < kS3; i += blockDim.x) {
+        const int r = i >> 8, k = i & 255;
+        s3[i] = __ldg(t16 + ((k << r) * 4 & 16383));
+    }
+    for (int i = threadIdx.x; i < kS2; i += blockDim.x) {
+        const int r = i >> 4, k = i & 15;
+        s2[i] = __ldg(t16 + ((k << r) * 64 & 16383));
+    }
 }
 
 // cos/sin(2 pi m / 32) for m = 0..15
@@ -111,17 +124,30 @@ __device__ __forceinline__ void dft_dif(float2 (&v)[R]) {
     }
 }
 
-// Multiply v[r] by W^(e r) for r = 1..R-1, W^e = T16[e] (e in table units).
-template <int R, bool INV>
-__device__ __forceinline__ void apply_twiddles(float2 (&v)[R], const Tables& t, int e) {
+template <bool INV>
+__device__ __forceinline__ float2 sw(const float2* tab, int i) {
+    const float2 w = tab[i];
+    return INV ? cconj(w) : w;
+}
+
+// Multiply v[r] by the pass twiddle W_{Ns R}^(k r), r = 1..R-1, from the
+// shared tables (radix 16: W^k, W^2k, W^4k, W^8k read, the rest formed by at
+// most three complex products; radix 4: W^k read, W^2k, W^3k formed).
+template <int R, int M, int Ns, bool INV>
+__device__ __forceinline__ void apply_twiddles(float2 (&v)[R], const Tables& t, int k) {
     if constexpr (R == 4) {
-        const float2 w1 = tw16<INV>(t, e), w2 = tw16<INV>(t, 2 * e), w3 = tw16<INV>(t, 3 * e);
+        static_assert((M == 16384 && Ns == 4096) || (M == 1024 && Ns == 256), "radix-4 pass");
+        const float2 w1 = sw<INV>(t.s4, M == 16384 ? k : 16 * k);
+        const float2 w2 = cmul(w1, w1);
+        const float2 w3 = cmul(w2, w1);
         v[1] = cmul(v[1], w1);
         v[2] = cmul(v[2], w2);
         v[3] = cmul(v[3], w3);
     } else {
-        const float2 w1 = tw16<INV>(t, e), w2 = tw16<INV>(t, 2 * e);
-        const float2 w4 = tw16<INV>(t, 4 * e), w8 = tw16<INV>(t, 8 * e);
+        static_assert(Ns == 16 || (Ns == 256 && M == 16384), "radix-16 pass");
+        const float2* tab = Ns == 16 ? t.s2 : t.s3;
+        const float2 w1 = sw<INV>(tab, k), w2 = sw<INV>(tab, Ns + k);
+        const float2 w4 = sw<INV>(tab, 2 * Ns + k), w8 = sw<INV>(tab, 3 * Ns + k);
         const float2 w3 = cmul(w2, w1), w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
         v[1] = cmul(v[1], w1);
         v[2] = cmul(v[2], w2);
@@ -146,14 +172,15 @@ struct SmemIO {};
 
 // One Stockham pass of radix R over NB independent padded M-point working
 // sets laid out back to back (set b starts at S + b * padded(M)).
-// Ns = product of the radices of the earlier passes.  `ld(b, idx)` supplies
+// Ns = product of the radices of the earlier passes (a template constant,
+// so the index arithmetic reduces to shifts and masks).  `ld(b, idx)` supplies
 // the inputs when LD is not SmemIO; `st(b, idx, value)` consumes the outputs
 // when ST is not SmemIO.  All threads of the CTA must call it; it starts
 // with the loads (callers sync before) and ends with a barrier.  Kept out
 // of line so each pass gets the whole 64-register budget (inlined into the
 // demod kernel, live state around the passes made the allocator spill).
-template <int R, int M, int NB, bool INV, class LD, class ST>
-__device__ __noinline__ void stockham_pass(float2* S, int Ns, const Tables& t, const LD& ld, const ST& st) {
+template <int R, int M, int NB, int Ns, bool INV, class LD, class ST>
+__device__ __noinline__ void stockham_pass(float2* S, const Tables& t, const LD& ld, const ST& st) {
     constexpr int B = M / R;                       // butterflies per set
     constexpr int BT = B * NB;                     // butterflies per pass
     constexpr int PER = (BT + kThreads - 1) / kThreads;
@@ -163,7 +190,6 @@ __device__ __noinline__ void stockham_pass(float2* S, int Ns, const Tables& t, c
     constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
     constexpr bool to_smem = std::is_same<ST, SmemIO>::value;
     float2 v[PER][R];
-    const int scale = kT16 / (Ns * R);
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
         const int jt = threadIdx.x + q * kThreads;
@@ -178,7 +204,7 @@ __device__ __noinline__ void stockham_pass(float2* S, int Ns, const Tables& t, c
                     v[q][r] = ld(b, j + r * B);
                 }
             }
-            if (Ns > 1) apply_twiddles<R, INV>(v[q], t, (j % Ns) * scale);
+            if constexpr (Ns > 1) apply_twiddles<R, M, Ns, INV>(v[q], t, j % Ns);
             dft_dif<R, INV>(v[q]);
         }
     }
@@ -212,10 +238,10 @@ __device__ __noinline__ void stockham_pass(float2* S, int Ns, const Tables& t, c
 template <bool INV, class LD = SmemIO, class ST = SmemIO>
 __device__ __forceinline__ void fft16k(float2* S, const Tables& t, const LD& ld = LD(), const ST& st = ST()) {
     const SmemIO s;
-    stockham_pass<16, kM, 1, INV>(S, 1, t, ld, s);
-    stockham_pass<16, kM, 1, INV>(S, 16, t, s, s);
-    stockham_pass<16, kM, 1, INV>(S, 256, t, s, s);
-    stockham_pass<4, kM, 1, INV>(S, 4096, t, s, st);
+    stockham_pass<16, kM, 1, 1, INV>(S, t, ld, s);
+    stockham_pass<16, kM, 1, 16, INV>(S, t, s, s);
+    stockham_pass<16, kM, 1, 256, INV>(S, t, s, s);
+    stockham_pass<4, kM, 1, 4096, INV>(S, t, s, st);
 }
 
 // Two independent unnormalised 1024-point complex FFTs (the analog-audio
@@ -223,9 +249,9 @@ __device__ __forceinline__ void fft16k(float2* S, const Tables& t, const LD& ld 
 template <bool INV>
 __device__ __forceinline__ void fft1k_x2(float2* S, const Tables& t) {
     const SmemIO s;
-    stockham_pass<16, 1024, 2, INV>(S, 1, t, s, s);
-    stockham_pass<16, 1024, 2, INV>(S, 16, t, s, s);
-    stockham_pass<4, 1024, 2, INV>(S, 256, t, s, s);
+    stockham_pass<16, 1024, 2, 1, INV>(S, t, s, s);
+    stockham_pass<16, 1024, 2, 16, INV>(S, t, s, s);
+    stockham_pass<4, 1024, 2, 256, INV>(S, t, s, s);
 }
 
 }  // namespace ldg

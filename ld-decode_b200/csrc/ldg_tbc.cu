@@ -25,7 +25,7 @@ __device__ __forceinline__ long long first_pixel_at(double xk, double outscale) 
     // smallest i >= 0 with i * outscale >= xk (same FP product as the gather)
     long long i = (long long)ceil(xk / outscale);
     if (i < 0) i = 0;
-    while (i > 0 && __dmul_rn((double)(i - 1), outscale) >= xk) --i;
+    while (i > 0 && __dmul_rn((double)(i - 1), outscale) >= xk) --i;  // one or two steps
     while (__dmul_rn((double)i, outscale) < xk) ++i;
     return i;
 }
@@ -53,30 +53,42 @@ __device__ void bitonic_sort(double* key, long long* wt) {
 }
 
 // Weighted median (numpy convention: mean of the two middle elements for an
-// even count) of the sorted (key, wt) list, total count n.
+// even count) of the sorted (key, wt) list, total count n.  Block-wide
+// inclusive scan of the weights (warp shuffles + one shared pass).
 __device__ double weighted_median(const double* key, const long long* wt, long long* csum,
                                   long long n) {
+    __shared__ long long warp_tot[kWowThreads / 32];
     __shared__ double res[2];
-    // inclusive prefix sum (serial over <= 512 entries by one thread: cheap)
-    if (threadIdx.x == 0) {
-        long long acc = 0;
-        for (int i = 0; i < kWowThreads; ++i) {
-            acc += wt[i];
-            csum[i] = acc;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    long long x = wt[t];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        long long y = lane < kWowThreads / 32 ? warp_tot[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long z = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += z;
         }
-        const long long r1 = (n & 1) ? n / 2 : n / 2 - 1;
-        const long long r2 = n / 2;
-        double v1 = 0, v2 = 0;
-        for (int i = 0; i < kWowThreads; ++i) {
-            if (wt[i] == 0) continue;
-            const long long lo = csum[i] - wt[i];
-            if (r1 >= lo && r1 < csum[i]) v1 = key[i];
-            if (r2 >= lo && r2 < csum[i]) v2 = key[i];
-        }
-        res[0] = (n & 1) ? v2 : (v1 + v2) / 2;
+        if (lane < kWowThreads / 32) warp_tot[lane] = y;
     }
     __syncthreads();
-    const double r = res[0];
+    const long long incl = x + (w ? warp_tot[w - 1] : 0);
+    csum[t] = incl;
+    const long long r1 = (n & 1) ? n / 2 : n / 2 - 1;
+    const long long r2 = n / 2;
+    const long long lo = incl - wt[t];
+    if (wt[t] > 0) {
+        if (r1 >= lo && r1 < incl) res[0] = key[t];
+        if (r2 >= lo && r2 < incl) res[1] = key[t];
+    }
+    __syncthreads();
+    const double r = (n & 1) ? res[1] : (res[0] + res[1]) / 2;
     __syncthreads();
     return r;
 }
@@ -137,18 +149,20 @@ constexpr int kGatherThreads = 256;
 constexpr int kSpanMax = 6144;  // staged input samples per output line (24 KB)
 
 // Input coordinate (FP64) of output pixel ig, optionally rounded to float32
-// as the reference does; the spline segment j is also returned.
+// as the reference does; the spline segment j is also returned.  The
+// segment is found from x * (1/inlinelen) and then fixed by exact
+// comparisons with the integer knots; w = 1/(x1 - x0) = 1/inlinelen is
+// precomputed with the same rounding.
 __device__ __forceinline__ double pixel_coord(const TbcField& f, long long ig, int nseg, int& j) {
     const double inl = f.inlinelen;
     const double x = __dmul_rn((double)ig, f.outscale);
-    // nominal segment from the integer pixel index, then exact comparisons
-    j = (int)(ig / (long long)f.outlinelen_i);
+    j = (int)(x * f.inv_inl);
     j = min(max(j, 0), nseg - 1);
-    while (j > 0 && (double)j * inl > x) --j;
-    while (j < nseg - 1 && (double)(j + 1) * inl <= x) ++j;
+    if (j > 0 && (double)j * inl > x) --j;
+    if (j < nseg - 1 && (double)(j + 1) * inl <= x) ++j;
     const double x0 = (double)j * inl, x1 = (double)(j + 1) * inl;
-    const double y0 = f.linelocs[j], y1 = f.linelocs[j + 1];
-    const double w = 1.0 / (x1 - x0);
+    const double y0 = __ldg(f.linelocs + j), y1 = __ldg(f.linelocs + j + 1);
+    const double w = f.inv_inl;
     double c = __dadd_rn(__dmul_rn(y0, __dmul_rn(w, x1 - x)), __dmul_rn(y1, __dmul_rn(w, x - x0)));
     if (f.coord_f32) c = (double)__double2float_rn(c);
     return c;
@@ -186,42 +200,65 @@ __global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcFie
     for (int k = threadIdx.x; k < slen; k += kGatherThreads) span[k] = __ldg(f.buf + base + k);
     __syncthreads();
 
-    for (int c = threadIdx.x; c < f.outwidth; c += kGatherThreads) {
-        int j;
-        const double cc = pixel_coord(f, ig0 + c, nseg, j);
-        const long long ci = (long long)cc;
-        const double ph = __dmul_rn(cc - (double)ci, 65536.0);
-        const int ps = (int)ph;
-        const float alpha = __double2float_rn(ph - (double)ps);
-        const long long start = ci - 7;
-        double acc = 0.0;
-        if (start >= 0 && start + 16 <= f.buf_len && ps >= 0 && ps < 65536) {
-            const float4* w0 = reinterpret_cast<const float4*>(lut + (size_t)ps * 16);
-            const float4* w1 = w0 + 4;
-            const long long rel = start - base;
-            const bool staged = slen > 0 && rel >= 0 && rel + 16 <= slen;
+    constexpr int P = 4;  // pixels per thread per round (independent loads in flight)
+    for (int c0 = threadIdx.x; c0 < f.outwidth; c0 += P * kGatherThreads) {
+        int jj[P], ps[P];
+        long long ci[P];
+        float alpha[P];
+        bool ok[P];
+#pragma unroll
+        for (int u = 0; u < P; ++u) {
+            const int c = c0 + u * kGatherThreads;
+            ok[u] = c < f.outwidth;
+            const double cc = pixel_coord(f, ig0 + (ok[u] ? c : 0), nseg, jj[u]);
+            ci[u] = (long long)cc;
+            const double ph = __dmul_rn(cc - (double)ci[u], 65536.0);
+            ps[u] = (int)ph;
+            alpha[u] = __double2float_rn(ph - (double)ps[u]);
+            ok[u] = ok[u] && ci[u] - 7 >= 0 && ci[u] + 9 <= f.buf_len && ps[u] >= 0 && ps[u] < 65536;
+        }
+        float4 wa[P][4], wb[P][4];
+#pragma unroll
+        for (int u = 0; u < P; ++u) {
+            const float4* w0 = reinterpret_cast<const float4*>(lut + (size_t)(ok[u] ? ps[u] : 0) * 16);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const float4 a = __ldg(w0 + q);
-                const float4 b = __ldg(w1 + q);
-                const float wa[4] = {fmaf(alpha, b.x - a.x, a.x), fmaf(alpha, b.y - a.y, a.y),
-                                     fmaf(alpha, b.z - a.z, a.z), fmaf(alpha, b.w - a.w, a.w)};
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    const float v = staged ? span[rel + 4 * q + t] : __ldg(f.buf + start + 4 * q + t);
-                    acc += (double)(v * wa[t]);
-                }
+                wa[u][q] = __ldg(w0 + q);
+                wb[u][q] = __ldg(w0 + 4 + q);
             }
-        } else if (f.status) {
-            atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
         }
-        const float out = (float)(f.seg_level[j] * acc);
-        const long long i = i0 + c;
-        if (f.out_f32) f.out_f32[i] = out;
-        if (f.out_u16) {
-            double v = (double)out * f.u16_scale + f.u16_offset + 0.5;
-            v = fmin(fmax(v, 0.0), 65535.0);
-            f.out_u16[i] = (uint16_t)(unsigned)v;
+#pragma unroll
+        for (int u = 0; u < P; ++u) {
+            const int c = c0 + u * kGatherThreads;
+            if (c >= f.outwidth) continue;
+            double acc = 0.0;
+            if (ok[u]) {
+                const long long start = ci[u] - 7;
+                const long long rel = start - base;
+                const bool staged = slen > 0 && rel >= 0 && rel + 16 <= slen;
+                const float al = alpha[u];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 a = wa[u][q], b = wb[u][q];
+                    const float wq[4] = {fmaf(al, b.x - a.x, a.x), fmaf(al, b.y - a.y, a.y),
+                                         fmaf(al, b.z - a.z, a.z), fmaf(al, b.w - a.w, a.w)};
+#pragma unroll
+                    for (int tt = 0; tt < 4; ++tt) {
+                        const float v = staged ? span[rel + 4 * q + tt] : __ldg(f.buf + start + 4 * q + tt);
+                        acc += (double)(v * wq[tt]);
+                    }
+                }
+            } else if (f.status) {
+                atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
+            }
+            const float out = (float)(f.seg_level[jj[u]] * acc);
+            const long long i = i0 + c;
+            if (f.out_f32) f.out_f32[i] = out;
+            if (f.out_u16) {
+                double v = (double)out * f.u16_scale + f.u16_offset + 0.5;
+                v = fmin(fmax(v, 0.0), 65535.0);
+                f.out_u16[i] = (uint16_t)(unsigned)v;
+            }
         }
     }
 }

@@ -19,7 +19,7 @@ struct TbcField {
     int coord_f32;
     double inlinelen;
     double outscale;     // inlinelen / outlinelen
-    int outlinelen_i;    // outlinelen (integer) for the nominal segment of a pixel
+    double inv_inl;      // 1.0 / inlinelen (the degree-1 spline basis weight)
     double u16_scale;    // out_scale / hz_ire
     double u16_offset;   // output_zero - vsync_ire*out_scale - ire0*u16_scale
     double* seg_level;   // nlines-1 level-adjust factors (device scratch)
