@@ -383,7 +383,7 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
     std::lock_guard<std::mutex> lk(c->mu);
     if (!c->d_lut) return fail(LDG_ERR_STATE, "ldg_tbc_fields: sinc table not set");
     size_t ll_total = 0, seg_total = 0;
-    int max_lines = 0;
+    long long max_nout = 0;
     for (int i = 0; i < nfields; ++i) {
         const ldg_tbc_field& f = fields[i];
         if (!f.buf || !f.linelocs) return fail(LDG_ERR_ARG, "ldg_tbc_fields: NULL buffer");
@@ -396,7 +396,7 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
             return fail(LDG_ERR_ARG, "ldg_tbc_fields: outlinelen must be an integer");
         ll_total += f.nlines;
         seg_total += f.nlines - 1;
-        if (f.linesout > max_lines) max_lines = f.linesout;
+        if ((long long)f.linesout * f.outwidth > max_nout) max_nout = (long long)f.linesout * f.outwidth;
     }
     DeviceGuard g(c->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
@@ -474,7 +474,7 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         }
     }
     LDG_CK(cudaMemcpyAsync(c->d_fields, h.data(), nfields * sizeof(ldg::TbcField), cudaMemcpyHostToDevice, st));
-    cudaError_t e = ldg::launch_tbc(c->d_fields, nfields, max_lines, c->d_lut, 15.0, st);
+    cudaError_t e = ldg::launch_tbc(c->d_fields, nfields, max_nout, c->d_lut, 15.0, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
     if (any_host) {
         for (int i = 0; i < nfields; ++i) {

@@ -185,6 +185,7 @@ __device__ __noinline__ void stockham_pass(float2* S, const Tables& t, const LD&
     constexpr int BT = B * NB;                     // butterflies per pass
     constexpr int PER = (BT + kThreads - 1) / kThreads;
     static_assert(BT % kThreads == 0 || BT < kThreads, "butterfly count");
+    static_assert(B % 16 == 0 && (Ns == 1 || Ns % 16 == 0) && (Ns > 1 || R == 16), "padding offsets");
     constexpr int bits = ilog2(R);
     constexpr int stride = padded(M);
     constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
@@ -195,11 +196,13 @@ __device__ __noinline__ void stockham_pass(float2* S, const Tables& t, const LD&
         const int jt = threadIdx.x + q * kThreads;
         if (jt < BT) {
             const int b = jt / B, j = jt - b * B;
-            const float2* Sb = S + b * stride;
+            // pad(j + r B) = pad(j) + r padded(B) because B is a multiple of 16:
+            // one base register, compile-time offsets
+            const float2* Sb = S + b * stride + pad(j);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if constexpr (from_smem) {
-                    v[q][r] = Sb[pad(j + r * B)];
+                    v[q][r] = Sb[r * padded(B)];
                 } else {
                     v[q][r] = ld(b, j + r * B);
                 }
@@ -215,13 +218,16 @@ __device__ __noinline__ void stockham_pass(float2* S, const Tables& t, const LD&
         const int jt = threadIdx.x + q * kThreads;
         if (jt < BT) {
             const int b = jt / B, j = jt - b * B;
-            float2* Sb = S + b * stride;
             const int k = j % Ns;
             const int d = (j / Ns) * Ns * R + k;
+            // pad(d + r Ns) = pad(d) + r padded(Ns) for Ns a multiple of 16; for
+            // Ns = 1, d = 16 j and pad(d + r) = pad(d) + r
+            float2* Sb = S + b * stride + pad(d);
+            constexpr int step = Ns >= 16 ? padded(Ns) : Ns;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if constexpr (to_smem) {
-                    Sb[pad(d + r * Ns)] = v[q][bitrev(r, bits)];
+                    Sb[r * step] = v[q][bitrev(r, bits)];
                 } else {
                     st(b, d + r * Ns, v[q][bitrev(r, bits)]);
                 }

@@ -8,7 +8,7 @@
 //                      (slopes of the expected->actual line-location spline),
 //                      their pixel-weighted median and 15*MAD outlier rule ->
 //                      one level-adjust factor per segment.
-//   tbc_gather_kernel  one thread per output pixel: FP64 spline coordinate,
+//   tbc_gather_kernel  one thread per output pixels: FP64 spline coordinate,
 //                      optional float32 rounding (the reference's own cast),
 //                      16-tap windowed-sinc gather with linear interpolation
 //                      between LUT phases, level adjust, uint16 conversion.
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kWowThreads) wow_levels_kernel(const TbcField*
 }
 
 constexpr int kGatherThreads = 256;
-constexpr int kSpanMax = 6144;  // staged input samples per output line (24 KB)
+constexpr int kGatherPix = 2;  // output pixels per thread (independent loads in flight)
 
 // Input coordinate (FP64) of output pixel ig, optionally rounded to float32
 // as the reference does; the spline segment j is also returned.  The
@@ -168,110 +168,79 @@ __device__ __forceinline__ double pixel_coord(const TbcField& f, long long ig, i
     return c;
 }
 
-// One CTA per (output line, field): stage the line's input span in shared
-// memory, then one thread per output pixel.
+// One thread per kGatherPix output pixels of one field; blockIdx.y is the
+// field.  No shared staging: the 16 taps of neighbouring pixels overlap and
+// are served from L1, the two LUT rows of a pixel are 128 contiguous bytes.
 __global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcField* fields, const float* lut,
                                                                     int nfields) {
-    __shared__ float span[kSpanMax];
-    __shared__ long long span_base;
-    __shared__ int span_len;
     const int fi = blockIdx.y;
     if (fi >= nfields) return;
     const TbcField& f = fields[fi];
-    const int line = blockIdx.x;
-    if (line >= f.linesout) return;
+    const long long nout = (long long)f.linesout * f.outwidth;
+    const long long i0 = ((long long)blockIdx.x * kGatherThreads) * kGatherPix + threadIdx.x;
+    if (i0 >= nout) return;
     const int nseg = f.nlines - 1;
-    const long long i0 = (long long)line * f.outwidth;
-    const long long ig0 = i0 + (long long)f.outwidth * (f.lineoffset + 1);
-    if (threadIdx.x == 0) {
-        int j;
-        const double c0 = pixel_coord(f, ig0, nseg, j);
-        const double c1 = pixel_coord(f, ig0 + f.outwidth - 1, nseg, j);
-        long long lo = (long long)fmin(c0, c1) - 8;
-        long long hi = (long long)fmax(c0, c1) + 10;
-        lo = max(lo, 0LL);
-        hi = min(hi, f.buf_len);
-        span_base = lo;
-        span_len = (hi > lo && hi - lo <= kSpanMax) ? (int)(hi - lo) : 0;
+    const long long igbase = (long long)f.outwidth * (f.lineoffset + 1);
+    int jj[kGatherPix], ps[kGatherPix];
+    long long st[kGatherPix];
+    float alpha[kGatherPix];
+    bool ok[kGatherPix];
+#pragma unroll
+    for (int u = 0; u < kGatherPix; ++u) {
+        const long long i = i0 + (long long)u * kGatherThreads;
+        const double cc = pixel_coord(f, igbase + (i < nout ? i : 0), nseg, jj[u]);
+        const long long ci = (long long)cc;
+        const double ph = __dmul_rn(cc - (double)ci, 65536.0);
+        ps[u] = (int)ph;
+        alpha[u] = __double2float_rn(ph - (double)ps[u]);
+        st[u] = ci - 7;
+        ok[u] = i < nout && st[u] >= 0 && st[u] + 16 <= f.buf_len && ps[u] >= 0 && ps[u] < 65536;
     }
-    __syncthreads();
-    const long long base = span_base;
-    const int slen = span_len;
-    for (int k = threadIdx.x; k < slen; k += kGatherThreads) span[k] = __ldg(f.buf + base + k);
-    __syncthreads();
-
-    constexpr int P = 4;  // pixels per thread per round (independent loads in flight)
-    for (int c0 = threadIdx.x; c0 < f.outwidth; c0 += P * kGatherThreads) {
-        int jj[P], ps[P];
-        long long ci[P];
-        float alpha[P];
-        bool ok[P];
 #pragma unroll
-        for (int u = 0; u < P; ++u) {
-            const int c = c0 + u * kGatherThreads;
-            ok[u] = c < f.outwidth;
-            const double cc = pixel_coord(f, ig0 + (ok[u] ? c : 0), nseg, jj[u]);
-            ci[u] = (long long)cc;
-            const double ph = __dmul_rn(cc - (double)ci[u], 65536.0);
-            ps[u] = (int)ph;
-            alpha[u] = __double2float_rn(ph - (double)ps[u]);
-            ok[u] = ok[u] && ci[u] - 7 >= 0 && ci[u] + 9 <= f.buf_len && ps[u] >= 0 && ps[u] < 65536;
-        }
-        float4 wa[P][4], wb[P][4];
-#pragma unroll
-        for (int u = 0; u < P; ++u) {
-            const float4* w0 = reinterpret_cast<const float4*>(lut + (size_t)(ok[u] ? ps[u] : 0) * 16);
+    for (int u = 0; u < kGatherPix; ++u) {
+        const long long i = i0 + (long long)u * kGatherThreads;
+        if (i >= nout) continue;
+        double acc = 0.0;
+        if (ok[u]) {
+            const float4* w0 = reinterpret_cast<const float4*>(lut + (size_t)ps[u] * 16);
+            const float* src = f.buf + st[u];
+            const float al = alpha[u];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                wa[u][q] = __ldg(w0 + q);
-                wb[u][q] = __ldg(w0 + 4 + q);
+                const float4 a = __ldg(w0 + q), b = __ldg(w0 + 4 + q);
+                const float wq[4] = {fmaf(al, b.x - a.x, a.x), fmaf(al, b.y - a.y, a.y),
+                                     fmaf(al, b.z - a.z, a.z), fmaf(al, b.w - a.w, a.w)};
+#pragma unroll
+                for (int tt = 0; tt < 4; ++tt) acc += (double)(__ldg(src + 4 * q + tt) * wq[tt]);
             }
+        } else if (f.status) {
+            atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
         }
-#pragma unroll
-        for (int u = 0; u < P; ++u) {
-            const int c = c0 + u * kGatherThreads;
-            if (c >= f.outwidth) continue;
-            double acc = 0.0;
-            if (ok[u]) {
-                const long long start = ci[u] - 7;
-                const long long rel = start - base;
-                const bool staged = slen > 0 && rel >= 0 && rel + 16 <= slen;
-                const float al = alpha[u];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float4 a = wa[u][q], b = wb[u][q];
-                    const float wq[4] = {fmaf(al, b.x - a.x, a.x), fmaf(al, b.y - a.y, a.y),
-                                         fmaf(al, b.z - a.z, a.z), fmaf(al, b.w - a.w, a.w)};
-#pragma unroll
-                    for (int tt = 0; tt < 4; ++tt) {
-                        const float v = staged ? span[rel + 4 * q + tt] : __ldg(f.buf + start + 4 * q + tt);
-                        acc += (double)(v * wq[tt]);
-                    }
-                }
-            } else if (f.status) {
-                atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
-            }
-            const float out = (float)(f.seg_level[jj[u]] * acc);
-            const long long i = i0 + c;
-            if (f.out_f32) f.out_f32[i] = out;
-            if (f.out_u16) {
-                double v = (double)out * f.u16_scale + f.u16_offset + 0.5;
-                v = fmin(fmax(v, 0.0), 65535.0);
-                f.out_u16[i] = (uint16_t)(unsigned)v;
-            }
+        const float out = (float)(f.seg_level[jj[u]] * acc);
+        if (f.out_f32) f.out_f32[i] = out;
+        if (f.out_u16) {
+            double v = (double)out * f.u16_scale + f.u16_offset + 0.5;
+            v = fmin(fmax(v, 0.0), 65535.0);
+            f.out_u16[i] = (uint16_t)(unsigned)v;
         }
     }
 }
 
-cudaError_t launch_tbc(const TbcField* dfields, int nfields, int max_lines, const float* lut,
+cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout, const float* lut,
                        double threshold_mult, cudaStream_t stream) {
     if (nfields <= 0) return cudaSuccess;
     wow_levels_kernel<<<nfields, kWowThreads, 0, stream>>>(dfields, threshold_mult);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    dim3 grid((unsigned)max_lines, (unsigned)nfields);
-    tbc_gather_kernel<<<grid, kGatherThreads, 0, stream>>>(dfields, lut, nfields);
-    return cudaGetLastError();
+    const long long per_cta = (long long)kGatherThreads * kGatherPix;
+    const unsigned gx = (unsigned)((max_nout + per_cta - 1) / per_cta);
+    for (int off = 0; off < nfields; off += 65535) {  // grid.y limit
+        const int n = nfields - off < 65535 ? nfields - off : 65535;
+        tbc_gather_kernel<<<dim3(gx, (unsigned)n), kGatherThreads, 0, stream>>>(dfields + off, lut, n);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace ldg

@@ -28,7 +28,7 @@ struct TbcField {
     uint16_t* out_u16;
 };
 
-cudaError_t launch_tbc(const TbcField* dfields, int nfields, int max_lines, const float* lut,
+cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout, const float* lut,
                        double threshold_mult, cudaStream_t stream);
 
 }  // namespace ldg
