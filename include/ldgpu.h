@@ -158,6 +158,24 @@ int ldg_synchronize(ldg_ctx* ctx);
  * (bytes; parked spectra, one slot per resident CTA). */
 int ldg_demod_scratch_bytes(ldg_ctx* ctx, int64_t nblocks, int64_t* bytes);
 
+/* Allocation-free form of ldg_demod_blocks -- no counterpart in the
+ * reference.  For callers that cannot call cudaMalloc while decoding (a
+ * process whose device memory belongs to another allocator's pool, or a
+ * capture loop that cannot afford cudaMalloc's device-wide synchronisation):
+ * it calls no cudaMalloc/cudaFree and no allocating library routine.  All
+ * buffers must be device memory (host buffers are rejected: staging them
+ * would allocate).  The demodulator's scratch is a static device array of
+ * 32 CTA slots x 256 KB (8 MB) that every GPU loading the library keeps
+ * until exit; `ctas` is the number of CTA slots to use (0: min(nblocks,
+ * 32)), and ctas > 32 is rejected with LDG_ERR_ARG.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller;
+ * nothing in it needs clearing between calls.  The filters and tables still
+ * come from `ctx`, which is created (and allocates) beforehand.  Enqueues
+ * on args->stream (or the context's stream) and returns without waiting. */
+int ldg_demod_blocks_noalloc(ldg_ctx* ctx, const ldg_demod_args* args, int32_t ctas);
+
 #ifdef __cplusplus
 }
 #endif

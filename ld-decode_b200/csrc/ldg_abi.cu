@@ -15,6 +15,7 @@
 
 #include "ldg_demod.cuh"
 #include "ldg_fft.cuh"
+#include "ldg_noalloc.h"
 #include "ldg_tbc.cuh"
 #include "ldgpu.h"
 
@@ -504,3 +505,94 @@ int ldg_synchronize(ldg_ctx* c) {
 }
 
 }  // extern "C"
+
+namespace ldg {
+
+int noalloc_fail(int code, const std::string& msg) { return fail(code, msg); }
+
+void* noalloc_stream(ldg_ctx* c, const ldg_demod_args* a) { return a->stream ? a->stream : (void*)c->stream; }
+
+int noalloc_prepare(ldg_ctx* c, const ldg_demod_args* a, int ctas, int max_slots, DemodParams* p, int* grid,
+                    int* device) {
+    *grid = 0;
+    if (!c || !a) return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: NULL argument");
+    if (!a->in) return fail(LDG_ERR_ARG, "demodblock called without raw or FFT data");
+    if (a->in_kind != LDG_IN_INT16 && a->in_kind != LDG_IN_FLOAT32)
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: in_kind must be LDG_IN_INT16 or LDG_IN_FLOAT32");
+    if (a->nblocks < 0 || a->in_stride < 0 || a->nblocks > (1LL << 30))
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: bad block count or stride");
+    if (ctas < 0 || ctas > max_slots)
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: ctas = " + std::to_string(ctas) +
+                                     " exceeds the static scratch (" + std::to_string(max_slots) +
+                                     " CTA slots of 256 KB); use 0 < ctas <= " + std::to_string(max_slots));
+    const int N = kN;
+    if (!slice_ok(a->video, N) || !slice_ok(a->rfhpf, N) || !slice_ok(a->efm, N) || !slice_ok(a->audio, 1024))
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: output slice outside the block");
+    if (a->roll_05 < 0 || a->roll_05 >= N || a->roll_burst < 0 || a->roll_burst >= N)
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: roll outside the block");
+    const void* ptrs[10] = {a->in, a->out_demod, a->out_raw, a->out_05, a->out_burst, a->out_pilot,
+                            a->out_rfhpf, a->out_efm, a->out_audio_left, a->out_audio_right};
+    for (const void* q : ptrs)
+        if (q && !is_device_ptr(q))
+            return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: all buffers must be device memory (no host staging)");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->d_filter[LDG_F_VIDEO_G] || !c->d_filter[LDG_F_VIDEO_G_ODD])
+        return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: RFVideo filter not set");
+    const int fslot[4] = {LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT};
+    float* vids[4] = {a->out_demod, a->out_05, a->out_burst, a->out_pilot};
+    for (int o = 0; o < 4; ++o)
+        if (vids[o] && !c->d_filter[fslot[o]]) return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: video filter not set");
+    if (a->out_rfhpf && !c->d_filter[LDG_F_RFHPF]) return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: rfhpf filter not set");
+    if (a->out_efm && !c->d_filter[LDG_F_EFM]) return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: EFM filter not set");
+    const bool audio = a->out_audio_left || a->out_audio_right;
+    if (audio && (!c->d_audio[0] || !c->d_audio[1]))
+        return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: audio bands not set");
+    const size_t esz = a->in_kind == LDG_IN_INT16 ? 2 : 4;
+    if ((a->in_stride & 1) != 0 || (reinterpret_cast<uintptr_t>(a->in) & (esz == 2 ? 3 : 7)) != 0)
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: input blocks must start on an even sample of an aligned buffer");
+    *device = c->device;
+    if (a->nblocks == 0) return LDG_OK;
+    const long long nb = a->nblocks;
+    const int cap = ctas ? ctas : max_slots;
+    *grid = (int)(nb < cap ? nb : cap);
+
+    memset(p, 0, sizeof(*p));
+    p->in = a->in;
+    p->in_kind = a->in_kind;
+    p->in_stride = a->in_stride;
+    p->nblocks = (int)nb;
+    p->fs_hz = (float)c->fs_hz;
+    p->f_rfhpf = c->d_filter[LDG_F_RFHPF];
+    p->f_g = c->d_filter[LDG_F_VIDEO_G];
+    p->f_godd = c->d_filter[LDG_F_VIDEO_G_ODD];
+    for (int o = 0; o < 4; ++o) {
+        p->f_video[o] = c->d_filter[fslot[o]];
+        p->o_video[o] = a->video.len ? vids[o] : nullptr;
+    }
+    p->f_efm = c->d_filter[LDG_F_EFM];
+    p->o_raw = a->video.len ? a->out_raw : nullptr;
+    p->o_rfhpf = a->rfhpf.len ? a->out_rfhpf : nullptr;
+    p->o_efm = a->efm.len ? a->out_efm : nullptr;
+    p->s_video = {a->video.start, a->video.len, 0};
+    p->roll[OUT_DEMOD] = 0;
+    p->roll[OUT_05] = a->roll_05;
+    p->roll[OUT_BURST] = a->roll_burst;
+    p->roll[OUT_PILOT] = 0;
+    p->s_rfhpf = {a->rfhpf.start, a->rfhpf.len, 0};
+    p->s_efm = {a->efm.start, a->efm.len, 0};
+    p->audio = audio && a->audio.len > 0;
+    for (int ch = 0; ch < 2; ++ch) {
+        p->a_lowbin[ch] = c->a_lowbin[ch];
+        p->a_filt1[ch] = c->d_audio[ch];
+        p->a_low[ch] = (float)c->a_low[ch];
+    }
+    p->a_rate = (float)c->a_rate[0];
+    p->o_audio[0] = a->out_audio_left;
+    p->o_audio[1] = a->out_audio_right;
+    p->s_audio = {a->audio.start, a->audio.len, 0};
+    p->tw16 = c->d_tw16;
+    p->tw32 = c->d_tw32;
+    return LDG_OK;
+}
+
+}  // namespace ldg

@@ -1,0 +1,19 @@
+// Internal helpers shared by the allocation-free demod entry point
+// (ldg_noalloc.cu) and the context implementation (ldg_abi.cu).
+#pragma once
+#include <string>
+
+#include "ldg_demod.cuh"
+#include "ldgpu.h"
+
+namespace ldg {
+
+// Validate `a` for the allocation-free path (device buffers only) and fill
+// `p` (all but p->scratch).  grid = ctas, or min(nblocks, max_slots) when
+// ctas == 0; ctas > max_slots is rejected.  Allocates nothing.
+int noalloc_prepare(ldg_ctx* ctx, const ldg_demod_args* a, int ctas, int max_slots, DemodParams* p, int* grid,
+                    int* device);
+int noalloc_fail(int code, const std::string& msg);
+void* noalloc_stream(ldg_ctx* ctx, const ldg_demod_args* a);
+
+}  // namespace ldg

@@ -68,6 +68,7 @@ SIGNATURES = {
     "ldg_tbc_fields": (ctypes.c_int, [c_p, ctypes.POINTER(TbcField), ctypes.c_int32, c_p]),
     "ldg_synchronize": (ctypes.c_int, [c_p]),
     "ldg_demod_scratch_bytes": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
+    "ldg_demod_blocks_noalloc": (ctypes.c_int, [c_p, ctypes.POINTER(DemodArgs), ctypes.c_int32]),
 }
 
 _lib = None
