@@ -176,6 +176,43 @@ int ldg_demod_scratch_bytes(ldg_ctx* ctx, int64_t nblocks, int64_t* bytes);
  * on args->stream (or the context's stream) and returns without waiting. */
 int ldg_demod_blocks_noalloc(ldg_ctx* ctx, const ldg_demod_args* args, int32_t ctas);
 
+/* ---- AC3-RF (2.88 MHz QPSK) demodulation, lddecode/ac3rf.py ---- */
+
+typedef struct ldg_ac3 ldg_ac3;
+typedef struct ldg_ac3_dpll ldg_ac3_dpll;
+
+/* Text of the last failing ldg_ac3_* call on this thread. */
+const char* ldg_ac3_last_error(void);
+
+/* Front-end filters of Ac3RfDemodulator (ac3rf.py:315-357): the half-band
+ * taps (19 before and between the mixer, 23 for the last /2), the RRC
+ * matched filter, and the NCO cos/sin tables of 2^lut_bits entries with the
+ * accumulator step per 10 MHz sample.  float32 taps as the reference's
+ * _FirDecimStage uses them; zero taps are skipped as it does. */
+int ldg_ac3_create(ldg_ac3** out, int32_t device, const float* hb19, int32_t n19, const float* hb23, int32_t n23,
+                   const float* rrc, int32_t nrrc, int32_t lut_bits, const float* cos_lut, const float* sin_lut,
+                   int32_t phase_step);
+void ldg_ac3_destroy(ldg_ac3* ac3);
+
+/* Baseband I/Q at fs/16 (2.5 MHz for 40 MSPS) of a raw RF stream that
+ * starts at absolute sample 0 (filter history zero before it); `in` holds
+ * the absolute samples [in_first, in_first + nsamples) and must reach back
+ * over the filters' history of the requested outputs (1134 samples before
+ * 16 * out_first, unless in_first == 0).  Final outputs
+ * [out_first, out_first+out_count), with out_first+out_count <=
+ * ceil((in_first+nsamples)/16).  Equal to feeding the same samples, in any
+ * chunking, through the reference's pre-mix stages, mixer and post-mix
+ * stages (ac3rf.py:372-392). */
+int ldg_ac3_frontend(ldg_ac3* ac3, const void* in, int32_t in_kind, int64_t in_first, int64_t nsamples,
+                     int64_t out_first, int64_t out_count, float* out_i, float* out_q, void* stream);
+
+/* Symbol-timing DPLL of AC3_DPLL (ac3rf.py:200-299), host code, streaming:
+ * state carries across calls.  Writes at most n symbols (values 0..3). */
+int ldg_ac3_dpll_create(ldg_ac3_dpll** out, double final_fs);
+void ldg_ac3_dpll_destroy(ldg_ac3_dpll* dpll);
+int ldg_ac3_dpll_reclock(ldg_ac3_dpll* dpll, const float* in_i, const float* in_q, int64_t n, uint8_t* out,
+                         int64_t* nout);
+
 #ifdef __cplusplus
 }
 #endif

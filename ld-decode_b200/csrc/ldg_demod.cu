@@ -42,7 +42,7 @@ __device__ __forceinline__ float fm_disc(float2 a, float2 b, float k) {
 struct InLoader16 {  // x[2m], x[2m+1] from int16 samples
     const int16_t* x;
     __device__ float2 operator()(int, int m) const {
-        const int w = __ldg(reinterpret_cast<const int*>(x) + m);
+        const int w = __ldcs(reinterpret_cast<const int*>(x) + m);  // read once: streaming
         return make_float2((float)(int16_t)(w & 0xffff), (float)(int16_t)(((unsigned)w) >> 16));
     }
 };
@@ -84,11 +84,12 @@ struct RealStorer {
     __device__ void operator()(int, int m, float2 v) const {
         const int i0 = (2 * m - roll - start) & (kN - 1);
         const int i1 = (i0 + 1) & (kN - 1);
+        // streaming stores: outputs are not re-read here, keep L2 for the parked spectra
         if (((i0 & 1) == 0) && i0 + 1 < len && ((reinterpret_cast<uintptr_t>(out + i0) & 7) == 0)) {
-            *reinterpret_cast<float2*>(out + i0) = make_float2(v.x * kInvM, v.y * kInvM);
+            __stcs(reinterpret_cast<float2*>(out + i0), make_float2(v.x * kInvM, v.y * kInvM));
         } else {
-            if (i0 < len) out[i0] = v.x * kInvM;
-            if (i1 < len) out[i1] = v.y * kInvM;
+            if (i0 < len) __stcs(out + i0, v.x * kInvM);
+            if (i1 < len) __stcs(out + i1, v.y * kInvM);
         }
     }
 };
@@ -104,8 +105,8 @@ struct EfmStorer {
     __device__ void operator()(int, int m, float2 v) const {
         const int i0 = (2 * m - start) & (kN - 1);
         const int i1 = (i0 + 1) & (kN - 1);
-        if (i0 < len) out[i0] = to_efm(v.x);
-        if (i1 < len) out[i1] = to_efm(v.y);
+        if (i0 < len) __stcs(reinterpret_cast<short*>(out) + i0, (short)to_efm(v.x));
+        if (i1 < len) __stcs(reinterpret_cast<short*>(out) + i1, (short)to_efm(v.y));
     }
 };
 
@@ -196,7 +197,7 @@ __device__ void audio_stage(const DemodParams& p, float2* A, const Tables& t, in
         if (i < 0 || i >= p.s_audio.len || oa == nullptr) continue;
         const float2* Ab = A + ch * stride;
         const float d = (n == 0) ? 0.0f : fm_disc(Ab[pad(n)], Ab[pad(n - 1)], kk);
-        oa[(long long)blk * p.s_audio.len + i] = d + (ch ? p.a_low[1] : p.a_low[0]);
+        __stcs(oa + (long long)blk * p.s_audio.len + i, d + (ch ? p.a_low[1] : p.a_low[0]));
     }
 }
 
@@ -273,10 +274,10 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
                 if (oraw) {
                     const int i0 = 2 * m - vs;
                     if (i0 >= 0 && i0 + 1 < vl && ((reinterpret_cast<uintptr_t>(oraw + i0) & 7) == 0)) {
-                        *reinterpret_cast<float2*>(oraw + i0) = make_float2(de, dodd);
+                        __stcs(reinterpret_cast<float2*>(oraw + i0), make_float2(de, dodd));
                     } else {
-                        if (i0 >= 0 && i0 < vl) oraw[i0] = de;
-                        if (i0 + 1 >= 0 && i0 + 1 < vl) oraw[i0 + 1] = dodd;
+                        if (i0 >= 0 && i0 < vl) __stcs(oraw + i0, de);
+                        if (i0 + 1 >= 0 && i0 + 1 < vl) __stcs(oraw + i0 + 1, dodd);
                     }
                 }
                 parkX[m] = make_float2(fminf(fmaxf(de, 1500000.0f), clip_hi), fminf(fmaxf(dodd, 1500000.0f), clip_hi));

@@ -69,6 +69,16 @@ SIGNATURES = {
     "ldg_synchronize": (ctypes.c_int, [c_p]),
     "ldg_demod_scratch_bytes": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "ldg_demod_blocks_noalloc": (ctypes.c_int, [c_p, ctypes.POINTER(DemodArgs), ctypes.c_int32]),
+    "ldg_ac3_last_error": (ctypes.c_char_p, []),
+    "ldg_ac3_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int32, c_p, ctypes.c_int32, c_p,
+                                      ctypes.c_int32, c_p, ctypes.c_int32, ctypes.c_int32, c_p, c_p,
+                                      ctypes.c_int32]),
+    "ldg_ac3_destroy": (None, [c_p]),
+    "ldg_ac3_frontend": (ctypes.c_int, [c_p, c_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
+                                        ctypes.c_int64, ctypes.c_int64, c_p, c_p, c_p]),
+    "ldg_ac3_dpll_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_double]),
+    "ldg_ac3_dpll_destroy": (None, [c_p]),
+    "ldg_ac3_dpll_reclock": (ctypes.c_int, [c_p, c_p, c_p, ctypes.c_int64, c_p, ctypes.POINTER(ctypes.c_int64)]),
 }
 
 _lib = None

@@ -172,11 +172,13 @@ def _rrc(beta, sps_, span):
 
 
 def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
-                  efm=True, qpsk=False, device="cpu", start=0, scale=2000.0):
+                  efm=True, qpsk=False, device="cpu", start=0, scale=2000.0, return_symbols=False):
     """int16 torch tensor of `nsamples` RF samples at 40 MSPS.
 
     `start` offsets the absolute sample index (so different seeds/offsets give
-    different field phases).  The same (system, nsamples, seed, start, device
+    different field phases).  With qpsk=True the 2.88 MHz carrier is
+    differential QPSK at 288 kbaud (RRC, alpha 0.5); return_symbols=True also
+    returns the transmitted symbols (per chunk, concatenated).  The same (system, nsamples, seed, start, device
     type) always gives the same capture.
     """
     dev = torch.device(device)
@@ -190,6 +192,8 @@ def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
     sigma = math.sqrt(0.5 / (10 ** (snr_db / 10)))
     out = torch.empty(nsamples, dtype=torch.int16, device=dev)
     phase = 0
+    qpsk_phase = 0.0
+    qpsk_syms = []
     for c0 in range(0, nsamples, CHUNK):
         clen = min(CHUNK, nsamples - c0)
         gen = torch.Generator(device=dev)
@@ -216,8 +220,14 @@ def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
             sig = sig + 0.12 * _fftconv(e, efm_taps)[128:128 + clen]
         if qpsk:
             nsym = int(clen * sym_rate / FS_HZ) + 16
+            # differential QPSK: symbol s advances the transmitted carrier phase by
+            # 0, -90, +90 or 180 degrees; a receiver mixing with exp(+j w t) sees
+            # the negated step, which its differential detector reports as s
             syms = torch.randint(0, 4, (nsym,), generator=gen, device=dev)
-            iq = torch.exp(1j * (math.pi / 4 + math.pi / 2 * syms.to(torch.float64)))
+            step = torch.tensor([0.0, -0.5, 0.5, 1.0], dtype=torch.float64, device=dev)[syms]
+            iq = torch.exp(1j * (math.pi / 4 + math.pi * (qpsk_phase + torch.cumsum(step, 0))))
+            qpsk_phase = float(torch.remainder(qpsk_phase + step.sum(), 2.0).item())
+            qpsk_syms.append(syms.to(torch.uint8).cpu())
             up = torch.zeros(nsym * sps_, dtype=torch.complex128, device=dev)
             up[::sps_] = iq
             bb = torch.complex(_fftconv(up.real, rrc), _fftconv(up.imag, rrc))
@@ -229,4 +239,6 @@ def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
             sig = sig + 0.15 * (bbi * car).real
         sig = sig + sigma * torch.randn(clen, generator=gen, device=dev, dtype=torch.float64)
         out[c0:c0 + clen] = torch.clamp(torch.round(sig * scale), -32768, 32767).to(torch.int16)
+    if return_symbols:
+        return out, (torch.cat(qpsk_syms).numpy() if qpsk_syms else None)
     return out

@@ -12,7 +12,10 @@ by ldgpu.synth, and saves small .npz fixtures:
   field_<sys>.npz    -- a capture, and for two consecutive fields the
                         reference's sync pulses, line locations, field flags,
                         TBC coordinates summary and the final uint16 picture;
-  sinc_lut_rows.npz  -- sampled rows of the reference's shipped sinc table.
+  sinc_lut_rows.npz  -- sampled rows of the reference's shipped sinc table;
+  ac3_loopback.npz   -- AC3-RF demodulator (lddecode/ac3rf.py) on a seeded
+                        DQPSK signal: baseband I/Q windows and the symbols of
+                        a clean (streamed in uneven blocks) and a noisy run.
 
 Nothing at test time reads /root/reference; only this script does.
 Usage: python tests/golden/make_golden.py
@@ -221,7 +224,50 @@ def lut_fixture():
                         sha256=np.array(sha(lut)))
 
 
+def ac3_fixture():
+    from lddecode import ac3rf
+    sys.path.insert(0, REPO)
+    from oracle.ac3 import dqpsk_signal
+
+    tx = np.random.default_rng(4242).integers(0, 4, 6000).astype(np.uint8)
+    table = np.cos(2 * np.pi * np.arange(1000) / 1000).astype(np.float32)
+    clean = dqpsk_signal(tx, cos_table=table)
+    noisy = dqpsk_signal(tx, noise_int=64, noise_scale=0.25 / 74.5, seed=99, cos_table=table)
+
+    # baseband I/Q through the reference's own stages (demodulate_to_symbols
+    # without its DPLL, ac3rf.py:372-394)
+    d = ac3rf.Ac3RfDemodulator(40e6)
+    data = clean
+    for st in d.pre_mix_filters:
+        data = st.process(data)
+    ph = (d._phase_step * np.arange(len(data))) & ((1 << d._PHASE_ACCUM_BITS) - 1)
+    re, im = data * d._cos_lut[ph], data * d._sin_lut[ph]
+    for st in d.post_mix_filters:
+        re, im = st.process(re, im)
+    windows = np.array([[0, 3000], [20000, 23000], [len(re) - 3000, len(re)]])
+    iq_i = np.concatenate([re[a:b] for a, b in windows])
+    iq_q = np.concatenate([im[a:b] for a, b in windows])
+
+    d = ac3rf.Ac3RfDemodulator(40e6)
+    blocks = [100001, 65536, 999999]
+    rx, pos, k = b"", 0, 0
+    while pos < len(clean):
+        n = blocks[k % 3]
+        rx += d.demodulate_to_symbols(clean[pos:pos + n])
+        pos += n
+        k += 1
+    rx_noisy = ac3rf.Ac3RfDemodulator(40e6).demodulate_to_symbols(noisy)
+    np.savez_compressed(os.path.join(HERE, "ac3_loopback.npz"), tx=tx, cos_table=table,
+                        n_iq=np.array(len(re)), windows=windows, iq_i=iq_i, iq_q=iq_q,
+                        rx_clean=np.frombuffer(rx, np.uint8), rx_noisy=np.frombuffer(rx_noisy, np.uint8),
+                        blocks=np.array(blocks), clean_sha256=np.array(sha(clean)),
+                        hb19=ac3rf.halfband_kaiser(19), hb23=ac3rf.halfband_kaiser(23),
+                        rrc=ac3rf.rrc_filter(55, 2.5e6 / ac3rf.SYMBOL_RATE, 0.7),
+                        noisy_sha256=np.array(sha(noisy)))
+
+
 def main():
+    ac3_fixture()
     lut_fixture()
     for i, (name, kw) in enumerate(CONFIGS.items()):
         rf = filters_fixture(name, kw)
