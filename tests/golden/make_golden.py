@@ -13,6 +13,9 @@ by ldgpu.synth, and saves small .npz fixtures:
                         reference's sync pulses, line locations, field flags,
                         TBC coordinates summary and the final uint16 picture;
   sinc_lut_rows.npz  -- sampled rows of the reference's shipped sinc table;
+  audio_downscale.npz -- analog audio downscale (core.py:1423-1580) for a set of
+                        seeded line-location / audio cases: locs, wow factors,
+                        int16 output, next-field offset, mute flag;
   ac3_loopback.npz   -- AC3-RF demodulator (lddecode/ac3rf.py) on a seeded
                         DQPSK signal: baseband I/Q windows and the symbols of
                         a clean (streamed in uneven blocks) and a noisy run.
@@ -224,6 +227,50 @@ def lut_fixture():
                         sha256=np.array(sha(lut)))
 
 
+AUDIO_CASES = [
+    # name, system, linecount, freq, timeoffset, audio dtype, audio length, glitch line
+    ("ntsc_44100", "NTSC", 263, 44100, 1.2e-5, "float64", 28800, 120),
+    ("ntsc_locked", "NTSC", 262, -2.8, 0.0, "float64", 28800, None),
+    ("pal_44100", "PAL", 312, 44100, -5e-6, "float32", 32600, 200),
+    ("ntsc_short", "NTSC", 263, 44100, 0.0, "float64", 20000, None),
+]
+
+
+def audio_case_inputs(system, linecount, dtype, alen, glitch, seed, line_period, audio_freqs):
+    """Seeded line locations (linear wow plus a glitch line) and integer-valued
+    FM-audio samples around the two carriers; shared with the tests."""
+    rng = np.random.default_rng(seed)
+    linelen = int(np.round(40e6 / (1e6 / line_period)))
+    n = linecount + 12
+    wow = 1 + 0.002 * np.sin(np.arange(n) / 37.0)
+    lineinfo = 1000.5 + np.concatenate([[0], np.cumsum(wow[:-1] * linelen)])
+    if glitch is not None:
+        lineinfo[glitch:] += 60.0
+    lf, rf_ = audio_freqs
+    left = lf + rng.integers(-150000, 150000, alen).astype(np.float64)
+    right = rf_ + rng.integers(-150000, 150000, alen).astype(np.float64)
+    return lineinfo, left.astype(dtype), right.astype(dtype), linelen
+
+
+def audio_fixture():
+    out = {}
+    for k, (name, system, linecount, freq, toff, dtype, alen, glitch) in enumerate(AUDIO_CASES):
+        sp = refcore.SysParams_NTSC if system == "NTSC" else refcore.SysParams_PAL
+        lineinfo, left, right, linelen = audio_case_inputs(
+            system, linecount, dtype, alen, glitch, 500 + k, sp["line_period"],
+            (sp["audio_lfreq"], sp["audio_rfreq"]))
+        locs, swow, arange, frametime = refcore._downscale_audio_compute_locs_and_swow(
+            lineinfo, sp["line_period"], linelen, linecount, toff, freq, 32)
+        o16, failed = refcore._downscale_audio_to_output(arange, locs, swow, left, right,
+                                                         sp["audio_lfreq"], sp["audio_rfreq"])
+        out[name + "_locs"] = locs
+        out[name + "_swow"] = swow
+        out[name + "_out"] = o16
+        out[name + "_next"] = np.array(arange[-1] - frametime)
+        out[name + "_failed"] = np.array(failed)
+    np.savez_compressed(os.path.join(HERE, "audio_downscale.npz"), **out)
+
+
 def ac3_fixture():
     from lddecode import ac3rf
     sys.path.insert(0, REPO)
@@ -267,6 +314,7 @@ def ac3_fixture():
 
 
 def main():
+    audio_fixture()
     ac3_fixture()
     lut_fixture()
     for i, (name, kw) in enumerate(CONFIGS.items()):

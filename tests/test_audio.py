@@ -1,0 +1,72 @@
+"""Analog audio downscale (ldgpu.audio) against the reference's outputs on
+seeded cases (tests/golden/audio_downscale.npz), and the sample-count pins of
+the reference's own tests/test_audio_rate.py."""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+
+sys.path.insert(0, GOLDEN)
+from make_golden import AUDIO_CASES, audio_case_inputs  # noqa: E402
+
+from ldgpu import audio as A  # noqa: E402
+from ldgpu.params import sysparams  # noqa: E402
+
+
+@pytest.mark.parametrize("case", AUDIO_CASES, ids=[c[0] for c in AUDIO_CASES])
+def test_downscale_audio_matches_reference(case):
+    g = golden("audio_downscale")
+    name, system, linecount, freq, toff, dtype, alen, glitch = case
+    k = AUDIO_CASES.index(case)
+    sp = sysparams(system)
+    lineinfo, left, right, linelen = audio_case_inputs(
+        system, linecount, dtype, alen, glitch, 500 + k, sp["line_period"], (sp["audio_lfreq"], sp["audio_rfreq"]))
+    locs, swow, arange, frametime = A.compute_locs_and_swow(lineinfo, sp["line_period"], linelen, linecount,
+                                                            toff, freq, 32)
+    np.testing.assert_array_equal(locs, g[name + "_locs"])
+    np.testing.assert_array_equal(swow, g[name + "_swow"])
+    assert arange[-1] - frametime == float(g[name + "_next"])
+    out, failed = A.to_output(arange, locs, swow, left, right, sp["audio_lfreq"], sp["audio_rfreq"])
+    np.testing.assert_array_equal(out, g[name + "_out"])
+    assert failed == bool(g[name + "_failed"])
+
+
+def test_downscale_audio_entry_point_and_warning(caplog):
+    """downscale_audio(audio, lineinfo, rf, ...) with an RFDecode-like object,
+    the rv dict, and the mute warning of a capture too short for the field."""
+    from ldgpu.rfdecode import RFParams
+    rf = RFParams(system="NTSC", decode_analog_audio=44100)
+    g = golden("audio_downscale")
+    name, system, linecount, freq, toff, dtype, alen, glitch = AUDIO_CASES[3]
+    sp = rf.SysParams
+    lineinfo, left, right, linelen = audio_case_inputs(
+        system, linecount, dtype, alen, glitch, 503, sp["line_period"], (sp["audio_lfreq"], sp["audio_rfreq"]))
+    assert linelen == rf.linelen and rf.Filters["audio_fdiv"] == 32
+    audio = np.rec.array([left, right], names=["audio_left", "audio_right"])
+    rv = {}
+    with caplog.at_level("WARNING"):
+        out, nxt = A.downscale_audio(audio, lineinfo, rf, linecount, toff, freq, rv)
+    assert "muting samples" in caplog.text
+    np.testing.assert_array_equal(out, g[name + "_out"])
+    assert rv["audio_next_offset"] == nxt == float(g[name + "_next"])
+
+
+def _count(freq, linecount=525, linelen=910):
+    lineinfo = np.arange(0, (linecount + 4) * linelen, linelen, dtype=np.double)
+    _, swow, arange, _ = A.compute_locs_and_swow(lineinfo, sysparams("NTSC")["line_period"], linelen,
+                                                 linecount, 0.0, freq, 32)
+    return len(arange) - 1, swow
+
+
+def test_ntsc_locked_rate_sample_counts():
+    """Pins of the reference's tests/test_audio_rate.py: -2.8 gives exactly
+    1470 samples per 525-line frame with unity wow; 44100 gives 1471."""
+    n, swow = _count(-2.8)
+    assert n == 1470
+    np.testing.assert_allclose(swow, 1.0, atol=1e-9)
+    assert 1_000_000 / sysparams("NTSC")["line_period"] * 2.8 == 44055.944055944055
+    assert _count(44100)[0] == 1471
