@@ -213,6 +213,136 @@ void ldg_ac3_dpll_destroy(ldg_ac3_dpll* dpll);
 int ldg_ac3_dpll_reclock(ldg_ac3_dpll* dpll, const float* in_i, const float* in_q, int64_t n, uint8_t* out,
                          int64_t* nout);
 
+/* ---- Line locations of every field of a capture (batched) ------------------
+ *
+ * The reference finds a field's line locations in Field.process()
+ * (core.py:1636-1653, FieldNTSC.process 3477-3495, FieldPAL.process
+ * 3209-3239) one field at a time, each from the previous one.  Batched here
+ * in three steps: ldg_sync_runs (GPU) finds the sync-level runs of demod_05
+ * over the whole capture; ldg_field_chain (host) walks the fields and
+ * computes the pulse-level line locations; ldg_lines_refine (GPU) does the
+ * per-line H-sync, colour-burst (NTSC) and pilot (PAL) refinement of all
+ * fields and writes their final FP64 line locations, ready for
+ * ldg_tbc_fields.  No counterpart in the reference as one call; the
+ * per-field results equal Field.process()'s. */
+
+#define LDG_CHAIN_MAX_LINES 336
+
+enum {
+    LDG_CHAIN_STOP_END = 0,     /* the next field's read runs past the capture */
+    LDG_CHAIN_STOP_FULL = 1,    /* max_plans fields planned */
+    LDG_CHAIN_STOP_PREV = 2,    /* the next field's result depends on the previous field's refined lines */
+    LDG_CHAIN_STOP_LEVELS = 3,  /* the next field needs the reference's level re-calibration */
+    LDG_CHAIN_STOP_ERROR = 4    /* the next field has no line to fill gaps from (the reference raises) */
+};
+
+typedef struct ldg_chain_params {
+    int32_t system;             /* 0 NTSC, 1 PAL */
+    int32_t num_pulses;         /* SysParams numPulses */
+    int32_t field_lines[2];
+    int32_t outlinecount;       /* frame_lines // 2 + 1 */
+    int32_t proclines;          /* outlinecount + 10 (+3 PAL) */
+    double freq;                /* MHz */
+    double freq_hz;
+    double linelen;             /* rf.linelen */
+    double inlinelen;
+    double linefreq0;           /* rf.samplesperline * rf.linelen (usectoinpx factor) */
+    double hsync_pulse_us, eq_pulse_us, vsync_pulse_us;
+    double first_field_h[2];
+    double hsync_tolerance;
+    double ire0, hz_ire, vsync_ire;
+    int64_t max_pulse_len;      /* findpulses max_len (5000) */
+    int64_t blocklen, blockcut, blockcut_end, readlen;
+    int64_t nblocks;            /* demodulated blocks of the capture */
+} ldg_chain_params;
+
+typedef struct ldg_chain_state {
+    double start;               /* LDdecode's read position of the next field */
+    int32_t prev_valid;         /* the previous field was valid (Field.prevfield set) */
+    int32_t prev_isfirst;
+    int64_t prev_startloc;
+    int32_t fields_written;
+    int32_t pad;
+} ldg_chain_state;
+
+typedef struct ldg_field_plan {
+    double start;
+    int64_t readloc, first_block, nblocks, startloc, length;  /* the field's read window (fieldread) */
+    int32_t valid, isfirst, linecount, proclines, has_prev, sync_confidence;
+    double nextfieldoffset;
+    double linelocs1[LDG_CHAIN_MAX_LINES];   /* pulse-level line locations (field-local samples) */
+    uint8_t linebad[LDG_CHAIN_MAX_LINES];
+} ldg_field_plan;
+
+/* Runs of demod_05 <= threshold over a capture-wide output array `d05`
+ * (device, n samples), sorted: run_start/run_len (host arrays of capacity
+ * `cap`) and, for runs longer than min_long samples, the FP64 mean of
+ * d05[start + trim_lo, start + len - trim_hi) (NaN otherwise).  A run still
+ * open at the end of the array is not reported.  LDG_ERR_RANGE if more
+ * than `cap` runs (*nruns then holds the count needed).  Synchronises
+ * `stream`. */
+int ldg_sync_runs(ldg_ctx* ctx, const float* d05, int64_t n, double threshold, int64_t min_long, int64_t trim_lo,
+                  int64_t trim_hi, int64_t* run_start, int64_t* run_len, double* run_mean, int64_t cap,
+                  int64_t* nruns, void* stream);
+
+/* Host: walk fields from state_in through the runs, writing one plan per
+ * field read (valid or not) until a stop condition (*stop, LDG_CHAIN_STOP_*);
+ * state_out continues the walk.  Pure host code (no GPU). */
+int ldg_field_chain(const ldg_chain_params* params, const int64_t* run_start, const int64_t* run_len,
+                    const double* run_mean, int64_t nruns, const ldg_chain_state* state_in,
+                    ldg_chain_state* state_out, ldg_field_plan* plans, int32_t max_plans, int32_t* nplans,
+                    int32_t* stop);
+const char* ldg_chain_last_error(void);
+
+typedef struct ldg_lines_consts {
+    int32_t system;             /* 0 NTSC, 1 PAL */
+    int32_t pad;
+    double freq;                /* MHz */
+    double linelen;             /* rf.linelen */
+    double linefreq0;           /* rf.samplesperline * rf.linelen */
+    double samplesperline;      /* rf.samplesperline */
+    double half_sync;           /* iretohz(vsync_ire / 2) */
+    double lo_ok, hi_ok;        /* iretohz(-55), iretohz(30) */
+    double hz_ire;
+    double fsc_mhz, pilot_mhz;
+} ldg_lines_consts;
+
+typedef struct ldg_lines_args {
+    ldg_lines_consts k;
+    const float* d05;           /* capture-wide outputs (device) */
+    const float* demod;
+    const float* burst;         /* demod_burst (NTSC) */
+    const float* pilot;         /* demod_pilot (PAL) */
+    int64_t capture_len;        /* samples in each capture-wide array */
+    int32_t nfields;            /* valid fields, in chain order */
+    int32_t proclines;
+    const int64_t* startloc;    /* per field (device) */
+    const int64_t* wlen;
+    const int32_t* isfirst;
+    const int32_t* linecount;   /* 262/263 as compute_linelocs sets it */
+    const int32_t* has_prev;    /* the previous field in the chain is this list's previous entry */
+    const double* linelocs1;    /* nfields x LDG_CHAIN_MAX_LINES */
+    const uint8_t* linebad1;
+    double prev_phase_adjust;   /* NTSC: phase_adjust_median of the field before the first one */
+    double* linelocs;           /* out: final line locations, nfields x LDG_CHAIN_MAX_LINES */
+    uint8_t* linebad;           /* out */
+    double* phase_adjust;       /* out, NTSC: per-field phase_adjust_median */
+    int32_t* field_phase;       /* out, NTSC: fieldPhaseID */
+    void* scratch;              /* ldg_lines_scratch_bytes(nfields) bytes of device memory */
+    void* stream;
+} ldg_lines_args;
+
+int64_t ldg_lines_scratch_bytes(int32_t nfields);
+
+/* sizeof of an ABI struct by its type name (binding checks), -1 if unknown. */
+int64_t ldg_abi_sizeof(const char* name);
+
+/* GPU refinement of all fields' line locations: refine_linelocs_hsync,
+ * compute_deriv_error, NTSC refine_linelocs_burst + fix_badlines + the
+ * 117.25-degree subcarrier shift, PAL refine_linelocs_pilot x2 +
+ * fix_badlines.  All pointers device memory; asynchronous on `stream`. */
+int ldg_lines_refine(ldg_ctx* ctx, const ldg_lines_args* args);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,7 +23,7 @@ LIB = os.path.join(HERE, "ldgpu", "libldgpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
 
-SOURCES = ["ldg_demod.cu", "ldg_tbc.cu", "ldg_abi.cu", "ldg_noalloc.cu", "ldg_ac3.cu"]
+SOURCES = ["ldg_demod.cu", "ldg_tbc.cu", "ldg_abi.cu", "ldg_noalloc.cu", "ldg_ac3.cu", "ldg_chain.cpp", "ldg_lines.cu"]
 
 
 def nvcc():
@@ -34,7 +34,7 @@ def nvcc():
 
 
 def _inputs():
-    files = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))]
+    files = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h", ".cpp"))]
     files.append(os.path.join(INCLUDE, "ldgpu.h"))
     files.append(os.path.abspath(__file__))
     return files
@@ -55,7 +55,7 @@ def build(force=False, verbose=False):
     cc = nvcc()
     objs = []
     for src in SOURCES:
-        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         cmd = [cc, *ARCH, *FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if verbose or r.returncode:

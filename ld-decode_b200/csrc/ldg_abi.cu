@@ -85,6 +85,8 @@ struct ldg_ctx {
     double* d_ll = nullptr;
     size_t ll_cap = 0;
     int* d_status = nullptr;
+    void* d_lines = nullptr;  // sync-run scan scratch (ldg_sync_runs)
+    size_t lines_cap = 0;
     std::mutex mu;
 };
 
@@ -189,6 +191,7 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     cudaFree(c->d_seg);
     cudaFree(c->d_ll);
     cudaFree(c->d_status);
+    cudaFree(c->d_lines);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -509,6 +512,20 @@ int ldg_synchronize(ldg_ctx* c) {
 namespace ldg {
 
 int noalloc_fail(int code, const std::string& msg) { return fail(code, msg); }
+
+int lines_fail(int code, const std::string& msg) { return fail(code, msg); }
+
+int ctx_device(const ldg_ctx* c) { return c->device; }
+
+std::mutex& ctx_mutex(ldg_ctx* c) { return c->mu; }
+
+cudaStream_t ctx_stream(const ldg_ctx* c) { return c->stream; }
+
+int ctx_lines_scratch(ldg_ctx* c, size_t need, void** out) {
+    int rc = grow(&c->d_lines, &c->lines_cap, need);
+    *out = c->d_lines;
+    return rc;
+}
 
 void* noalloc_stream(ldg_ctx* c, const ldg_demod_args* a) { return a->stream ? a->stream : (void*)c->stream; }
 

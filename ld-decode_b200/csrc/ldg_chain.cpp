@@ -1,0 +1,727 @@
+// Field read chain and pulse-level line locations, on the host in FP64.
+//
+// Restates the part of Field.process() that works on sync pulses
+// (lddecode/core.py:1760-2481): pulse timing classes (get_timings), the
+// vertical-blanking state machine (run_vblank_state_machine, refinepulses),
+// line 0 and field parity (getBlankRange, processVBlank, getLine0), mean
+// line length (computeLineLen) and the integer-rounded line slots with gap
+// filling (compute_linelocs), plus LDdecode.readfield's next-field offset
+// (core.py:4090-4097) that walks field after field through a capture.
+//
+// The pulses themselves come from the GPU: runs of demod_05 at or below the
+// sync threshold over the whole capture-wide output array, and the mean
+// level inside every long run (ldg_sync_runs).  A field read window
+// [startloc, startloc + length) sees the runs that start after its first
+// sample and end before its last one, exactly the pulses findpulses
+// (utils.py:1101-1157) finds in the window.
+//
+// Decisions that depend on the previous field's GPU-refined line locations
+// (the line-0 vote of getLine0 when it can change the result, the
+// skip_check limit of processVBlank) are detected and reported instead of
+// guessed: the chain stops before such a field (LDG_CHAIN_STOP_PREV) and
+// the caller decodes it with full information.  The same holds for the
+// reference's level-recalibration branches of getpulses
+// (LDG_CHAIN_STOP_LEVELS).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "ldg_chain.h"
+
+namespace {
+
+enum { HSYNC = 0, EQPL1 = 1, VSYNC = 2, EQPL2 = 3 };
+
+struct Pulse {
+    long long start;
+    long long len;
+};
+
+struct VPulse {
+    int type;
+    Pulse p;
+    bool good;
+};
+
+inline bool inrange(double a, double lo, double hi) { return a >= lo && a <= hi; }
+
+// numpy round-half-to-even of a double, as int
+inline long long nround(double x) { return (long long)std::nearbyint(x); }
+
+double median_of(std::vector<double> v) {
+    const size_t n = v.size();
+    std::sort(v.begin(), v.end());
+    if (n % 2) return v[n / 2];
+    return (v[n / 2 - 1] + v[n / 2]) / 2.0;
+}
+
+struct Timings {
+    double hsync_lo, hsync_hi, eq_lo, eq_hi, vsync_lo, vsync_hi;
+};
+
+struct VBlank {
+    bool ok = false;       // line0 found
+    long long line0 = 0;
+    bool isfirst = false;
+    int firstblank = 0;
+    int conf = 0;
+    bool zeroed_conf = false;  // the branch that sets sync_confidence = 0
+    bool operator==(const VBlank& o) const {
+        return ok == o.ok && line0 == o.line0 && isfirst == o.isfirst && firstblank == o.firstblank &&
+               conf == o.conf && zeroed_conf == o.zeroed_conf;
+    }
+};
+
+class FieldPulses {
+public:
+    FieldPulses(const LdgChainParams& P, std::vector<Pulse> raw) : P(P), raw(std::move(raw)) {}
+
+    double usectoinpx(double x) const { return x * P.linefreq0; }
+
+    Timings get_timings() const {
+        const double lo = usectoinpx(P.hsync_pulse_us - 1.75), hi = usectoinpx(P.hsync_pulse_us + 2);
+        std::vector<double> hl;
+        for (const Pulse& p : raw)
+            if (inrange((double)p.len, lo, hi)) hl.push_back((double)p.len);
+        const double med = hl.empty() ? P.hsync_pulse_us : median_of(hl);
+        const double off = med - usectoinpx(P.hsync_pulse_us);
+        Timings t;
+        t.hsync_lo = med + usectoinpx(-0.5);
+        t.hsync_hi = med + usectoinpx(0.5);
+        t.eq_lo = usectoinpx(P.eq_pulse_us - 0.5) + off;
+        t.eq_hi = usectoinpx(P.eq_pulse_us + 0.5) + off;
+        t.vsync_lo = usectoinpx(P.vsync_pulse_us * 0.5) + off;
+        t.vsync_hi = usectoinpx(P.vsync_pulse_us + 1) + off;
+        return t;
+    }
+
+    bool qualitycheck(const VPulse& prev, int type, const Pulse& p) const {
+        double lo, hi;
+        if (prev.type > 0 && type > 0) {
+            lo = 0.4;
+            hi = 0.6;
+        } else if (prev.type == 0 && type == 0) {
+            lo = 0.9;
+            hi = 1.1;
+        } else {
+            lo = 0.4;
+            hi = 1.1;
+        }
+        const double linelen = (double)(p.start - prev.p.start) / P.inlinelen;
+        return inrange(linelen, lo, hi);
+    }
+
+    // core.py:1825-1911
+    bool vblank_state_machine(size_t from, size_t to, const Timings& LT, std::vector<VPulse>& valid) const {
+        bool done = false;
+        double state_end = 0;
+        double state_length = 0;  // 0: None
+        const double half = P.num_pulses / 2.0;
+        for (size_t k = from; k < to; ++k) {
+            const Pulse& p = raw[k];
+            int stype = -1;
+            const int state = valid.empty() ? -1 : valid.back().type;
+            const bool is_h = inrange((double)p.len, LT.hsync_lo, LT.hsync_hi);
+            const bool is_eq = inrange((double)p.len, LT.eq_lo, LT.eq_hi);
+            const bool is_v = inrange((double)p.len, LT.vsync_lo, LT.vsync_hi);
+            if (state == -1) {
+                if (is_h) stype = HSYNC;
+            } else if (state == HSYNC) {
+                if (is_h) stype = HSYNC;
+                else if (is_eq) {
+                    stype = EQPL1;
+                    state_length = half;
+                } else if (is_v) stype = VSYNC;
+            } else if (state == EQPL1) {
+                if (is_eq) stype = EQPL1;
+                else if (is_v) {
+                    stype = VSYNC;
+                    state_length = half;
+                } else if (is_h) stype = HSYNC;
+            } else if (state == VSYNC) {
+                if (is_eq) {
+                    stype = EQPL2;
+                    state_length = half;
+                } else if (is_v) stype = VSYNC;
+                else if ((double)p.start > state_end && is_h) stype = HSYNC;
+            } else if (state == EQPL2) {
+                if (is_eq) stype = EQPL2;
+                else if (is_h) {
+                    stype = HSYNC;
+                    done = true;
+                }
+            }
+            if (stype >= 0 && stype != state) {
+                if ((double)p.start < state_end) stype = -1;
+                else if (state_length != 0) {
+                    state_end = (double)p.start + (state_length - 0.1) * P.inlinelen;
+                    state_length = 0;
+                }
+            }
+            if (stype >= 0) {
+                const bool good = valid.empty() ? false : qualitycheck(valid.back(), stype, p);
+                valid.push_back({stype, p, good});
+            }
+            if (done) return true;
+        }
+        return done;
+    }
+
+    // core.py:1913-1949
+    std::vector<VPulse> refinepulses(const Timings& LT) const {
+        std::vector<VPulse> valid;
+        size_t i = 0;
+        while (i < raw.size()) {
+            const Pulse& cur = raw[i];
+            if (inrange((double)cur.len, LT.hsync_lo, LT.hsync_hi)) {
+                const bool good = valid.empty() ? false : qualitycheck(valid.back(), HSYNC, cur);
+                valid.push_back({HSYNC, cur, good});
+                i += 1;
+            } else if (i > 2 && inrange((double)cur.len, LT.eq_lo, LT.eq_hi) && !valid.empty() &&
+                       valid.back().type == HSYNC) {
+                std::vector<VPulse> vb;
+                const bool done = vblank_state_machine(i - 2, std::min(raw.size(), i + 24), LT, vb);
+                if (done) {
+                    for (size_t k = 2; k < vb.size(); ++k) valid.push_back(vb[k]);
+                    i += vb.size() - 2;
+                } else {
+                    i += 1;
+                }
+            } else {
+                i += 1;
+            }
+        }
+        return valid;
+    }
+
+    // core.py:1951-1978; returns false when no blanking range is found
+    static bool blank_range(const std::vector<VPulse>& vp, int start, int& firstblank, int& lastblank) {
+        const int n = (int)vp.size();
+        int firstvsync = -1;
+        for (int k = std::max(start, 0); k < n; ++k)
+            if (vp[k].type == VSYNC) {
+                firstvsync = k;
+                break;
+            }
+        if (firstvsync < 0 || firstvsync < 10) return false;
+        for (int newstart = firstvsync - 10; newstart < firstvsync - 4; ++newstart) {
+            int fb = -1;
+            for (int k = newstart; k < n; ++k)
+                if (vp[k].type > 0) {
+                    fb = k;
+                    break;
+                }
+            if (fb < 0) continue;
+            int hs = -1;
+            for (int k = fb; k < n; ++k)
+                if (vp[k].type == 0) {
+                    hs = k;
+                    break;
+                }
+            if (hs < 0) continue;
+            const int lb = hs - 1;
+            if (lb - fb > 12) {
+                firstblank = fb;
+                lastblank = lb;
+                return true;
+            }
+        }
+        return false;
+    }
+
+    // Python's negative-index wrap for validpulses[idx]
+    static const VPulse& at(const std::vector<VPulse>& vp, int idx) {
+        return vp[idx < 0 ? idx + (int)vp.size() : idx];
+    }
+
+    // core.py:1988-2088; limit < 0 means None
+    VBlank process_vblank(const std::vector<VPulse>& vp, int start, int limit) const {
+        VBlank r;
+        int firstblank, lastblank;
+        if (!blank_range(vp, start, firstblank, lastblank)) return r;
+        const int lastvalid = limit < 0 ? (int)vp.size() : start + limit;
+        if (firstblank > lastvalid) return r;
+        const long long loc_presync = at(vp, firstblank - 1).p.start;
+        const int n = (int)vp.size() - firstblank;
+        const int np_ = P.num_pulses;
+        const int order[3] = {VSYNC, EQPL1, EQPL2};
+        for (int oi = 0; oi < 3; ++oi) {
+            const int ty = order[oi];
+            int grouploc = -1;
+            for (int j = 0; j < lastblank - firstblank; ++j) {
+                // ptmatch[j:j+numPulses].all(), slices truncated at the end
+                bool all = true;
+                for (int k = j; k < std::min(j + np_, n); ++k)
+                    if (vp[firstblank + k].type != ty) {
+                        all = false;
+                        break;
+                    }
+                if (!all) continue;
+                int cnt = 0;
+                for (int k = j; k < std::min(j + np_ + 4, n); ++k) cnt += vp[firstblank + k].type == ty;
+                if (cnt != np_) break;
+                // gaps = diff(diff(starts)), lengths = diff(lens) over the group
+                double gmax = -1e300, lmax = -1e300;
+                for (int k = j; k + 2 < j + np_; ++k) {
+                    const long long a = vp[firstblank + k].p.start, b = vp[firstblank + k + 1].p.start,
+                                    c = vp[firstblank + k + 2].p.start;
+                    gmax = std::max(gmax, (double)((c - b) - (b - a)));
+                }
+                for (int k = j; k + 1 < j + np_; ++k)
+                    lmax = std::max(lmax, (double)(vp[firstblank + k + 1].p.len - vp[firstblank + k].p.len));
+                if (gmax < P.freq * 0.2 && lmax < P.freq * 0.2) {
+                    grouploc = j;
+                    break;
+                }
+            }
+            if (grouploc < 0) continue;
+            const long long firstloc = vp[firstblank + grouploc].p.start;
+            const double distfroml1 = ((ty - 1) * np_) * 0.5;
+            const double dist = (double)(firstloc - loc_presync) / P.inlinelen;
+            const long long hdist = nround(dist * 2);
+            const long long hmod = ((hdist % 2) + 2) % 2;
+            bool isfirst = hmod == (long long)(P.first_field_h[1] != 1.0);
+            if (std::fmod(distfroml1 * 2, 2.0) != 0.0) isfirst = !isfirst;
+            const double eqgap = P.first_field_h[isfirst ? 1 : 0];
+            const double line0 = (double)firstloc - ((eqgap + distfroml1) * P.inlinelen);
+            r.ok = true;
+            r.line0 = (long long)line0;  // int() truncates toward zero
+            r.isfirst = isfirst;
+            r.firstblank = firstblank;
+            r.conf = 100;
+            return r;
+        }
+        if (at(vp, firstblank - 1).good && vp[firstblank].good && vp[lastblank].good && vp[lastblank + 1].good) {
+            const double gap1 = (double)(vp[firstblank].p.start - at(vp, firstblank - 1).p.start);
+            const double gap2 = (double)(vp[lastblank + 1].p.start - vp[lastblank].p.start);
+            bool isfirst;
+            if (P.system == 1 && inrange(std::fabs(gap2 - gap1), 0, P.freq * 1)) {
+                isfirst = inrange(gap1 / P.inlinelen, 0.45, 0.55);
+            } else if (P.system == 0 && inrange(std::fabs(gap2 + gap1), P.inlinelen * 1.4, P.inlinelen * 1.6)) {
+                isfirst = inrange(gap1 / P.inlinelen, 0.95, 1.05);
+            } else {
+                r.zeroed_conf = true;
+                return r;
+            }
+            r.ok = true;
+            r.line0 = at(vp, firstblank - 1).p.start;
+            r.isfirst = isfirst;
+            r.firstblank = firstblank;
+            r.conf = 50;
+            return r;
+        }
+        return r;
+    }
+
+    // core.py:2090-2119
+    double compute_line_len(const std::vector<VPulse>& vp) const {
+        int lr0 = -1, lr1 = -1;
+        int c0 = -1, c1 = 0;
+        bool have = false;
+        for (int i = 0; i < (int)vp.size(); ++i) {
+            if (vp[i].type != 0) {
+                if (have && c1 > lr1) {
+                    lr0 = c0;
+                    lr1 = c1;
+                }
+                have = false;
+            } else if (!have) {
+                have = true;
+                c0 = i;
+                c1 = 0;
+            } else {
+                c1 += 1;
+            }
+        }
+        if (have && c1 > lr1) {
+            lr0 = c0;
+            lr1 = c1;
+        }
+        double sum = 0;
+        long long cnt = 0;
+        for (int i = lr0 + 1; i < lr0 + lr1; ++i) {
+            const long long ll = vp[i].p.start - vp[i - 1].p.start;
+            if (inrange((double)ll / P.inlinelen, 0.95, 1.05)) {
+                sum += (double)ll;
+                cnt += 1;
+            }
+        }
+        return cnt ? sum / (double)cnt : P.inlinelen;
+    }
+
+    const LdgChainParams& P;
+    std::vector<Pulse> raw;
+};
+
+// Line slots from pulses for a given line 0 (core.py:2394-2481).
+struct Slots {
+    bool ok = false;
+    bool error = false;     // no valid line anywhere to fill from (the reference raises)
+    bool skipdetected = false;
+    double nextfield = 0;
+    std::vector<double> filled;
+    std::vector<unsigned char> err;
+};
+
+Slots line_slots(const LdgChainParams& P, const std::vector<VPulse>& vp, const std::vector<Pulse>& raw,
+                 double line0loc, double meanlinelen, double lastlineloc, bool have_lastline, int linecount,
+                 bool have_vblank_next, double vblank_next, int proclines) {
+    Slots s;
+    bool skipdetected = false;
+    if (have_lastline) skipdetected = (lastlineloc - line0loc) / P.inlinelen < (double)(linecount - 5);
+    s.skipdetected = skipdetected;
+    const double lastline = ((double)raw.back().start - line0loc) / meanlinelen;
+    if (lastline < proclines) {
+        s.nextfield = line0loc - (meanlinelen * 20);
+        return s;
+    }
+    std::map<long long, long long> ll_dict;
+    std::map<long long, double> ll_dist;
+    for (const VPulse& p : vp) {
+        double lineloc = ((double)p.p.start - line0loc) / meanlinelen;
+        long long rlineloc = nround(lineloc);
+        double dist = std::fabs(lineloc - (double)rlineloc);
+        if (skipdetected) {
+            const double lineloc_end = linecount - ((lastlineloc - (double)p.p.start) / meanlinelen);
+            const long long rend = nround(lineloc_end);
+            const double dist_end = std::fabs(lineloc_end - (double)rend);
+            if (p.type == 0 && rlineloc > 23 && dist_end < dist) {
+                lineloc = lineloc_end;
+                rlineloc = rend;
+                dist = dist_end;
+            }
+        }
+        auto it = ll_dist.find(rlineloc);
+        if (dist > P.hsync_tolerance || (it != ll_dist.end() && dist > it->second)) continue;
+        if (rlineloc > 0 && !p.good) {
+            if (p.type > 0 || (p.type == 0 && rlineloc < 10)) continue;
+        }
+        ll_dict[rlineloc] = p.p.start;
+        ll_dist[rlineloc] = dist;
+    }
+    std::vector<double> linelocs(proclines);
+    for (int l = 0; l < proclines; ++l) {
+        auto it = ll_dict.find(l);
+        linelocs[l] = it != ll_dict.end() ? (double)it->second : -1.0;
+    }
+    std::vector<double> filled = linelocs;
+    std::vector<unsigned char> err(proclines, 0);
+    const int olc = P.outlinecount;
+    if (filled[0] < 0) {
+        int next_valid = -1;
+        for (int i = 0; i < std::min(olc + 1, proclines); ++i)
+            if (linelocs[i] > 0) {
+                next_valid = i;
+                break;
+            }
+        if (next_valid < 0) {
+            s.nextfield = line0loc + (P.inlinelen * olc - 7);
+            return s;
+        }
+        filled[0] = filled[next_valid] - (next_valid * meanlinelen);
+        if (filled[0] < P.inlinelen) {
+            s.nextfield = line0loc + (P.inlinelen * olc - 7);
+            return s;
+        }
+    }
+    for (int l = 1; l < proclines; ++l) {
+        if (filled[l] < 0) {
+            err[l] = 1;
+            int pv = -1, nv = -1;
+            for (int i = l; i >= 0; --i)
+                if (linelocs[i] > 0) {
+                    pv = i;
+                    break;
+                }
+            for (int i = l; i < std::min(olc + 1, proclines); ++i)
+                if (linelocs[i] > 0) {
+                    nv = i;
+                    break;
+                }
+            if (pv < 0) {
+                if (nv < 0) {
+                    s.error = true;  // the reference raises here
+                    return s;
+                }
+                filled[l] = linelocs[nv] - (P.inlinelen * (nv - l));
+            } else if (nv >= 0) {
+                const double avglen = (linelocs[nv] - linelocs[pv]) / (double)(nv - pv);
+                filled[l] = linelocs[pv] + (avglen * (l - pv));
+            } else {
+                filled[l] = linelocs[pv] + (P.inlinelen * (l - pv));
+            }
+        }
+    }
+    s.ok = true;
+    s.filled = filled;
+    s.err = err;
+    s.nextfield = have_vblank_next ? vblank_next - (P.inlinelen * 8) : filled[olc - 7];
+    return s;
+}
+
+bool same_slots(const Slots& a, const Slots& b) {
+    return a.ok == b.ok && a.nextfield == b.nextfield && a.filled == b.filled && a.err == b.err;
+}
+
+// compute_deriv_error (core.py:2553-2564): second differences above 4 samples
+void deriv_error(const std::vector<double>& ll, std::vector<unsigned char>& bad) {
+    const int n = (int)ll.size();
+    for (int j = 0; j + 2 < n; ++j) {
+        const double d2 = std::fabs((ll[j + 2] - ll[j + 1]) - (ll[j + 1] - ll[j]));
+        if (d2 > 4) {
+            bad[j + 1] = 1;
+            bad[j + 2] = 1;
+        }
+    }
+}
+
+struct Window {
+    long long readloc, first_block, nblocks, startloc, length;
+};
+
+// LDdecode.decodefield's read of blocks (core.py:4030-4042, 1358-1409)
+Window field_window(const LdgChainParams& P, double start) {
+    Window w;
+    w.readloc = std::max((long long)(start - P.blockcut), 0LL);
+    const long long bs = P.blocklen;
+    const long long U = P.blocklen - P.blockcut - P.blockcut_end;
+    const long long begin = (w.readloc / bs) * bs;
+    const long long length = ((P.readlen / bs) + 2) * bs;
+    const long long end = begin + length;
+    w.first_block = begin / U;
+    const long long last = end / U;
+    w.nblocks = last - w.first_block + 1;
+    w.startloc = w.first_block * U;
+    w.length = w.nblocks * U;
+    return w;
+}
+
+thread_local std::string g_chain_err;
+
+}  // namespace
+
+extern "C" {
+
+const char* ldg_chain_last_error(void) { return g_chain_err.c_str(); }
+
+int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int64_t* run_len, const double* run_mean,
+                    int64_t nruns, const LdgChainState* state_in, LdgChainState* state_out, LdgFieldPlan* plans,
+                    int32_t max_plans, int32_t* nplans, int32_t* stop) {
+    if (!P || (!run_start && nruns) || (!run_len && nruns) || (!run_mean && nruns) || !state_in || !state_out ||
+        !plans || !nplans || !stop) {
+        g_chain_err = "ldg_field_chain: NULL argument";
+        return -1;
+    }
+    if (P->proclines > LDG_CHAIN_MAX_LINES || P->proclines < P->outlinecount + 1) {
+        g_chain_err = "ldg_field_chain: proclines out of range";
+        return -1;
+    }
+    LdgChainState st = *state_in;
+    int np_out = 0;
+    *stop = LDG_CHAIN_STOP_END;
+    const double minlength = 10.0 * P->linefreq0;  // usectoinpx(10)
+    while (np_out < max_plans) {
+        const Window w = field_window(*P, st.start);
+        if (w.first_block + w.nblocks > P->nblocks) {
+            *stop = LDG_CHAIN_STOP_END;
+            break;
+        }
+        // window pulses: runs starting after the first sample and ending before the last
+        const long long lo = w.startloc, hi = w.startloc + w.length;
+        const int64_t* b = std::upper_bound(run_start, run_start + nruns, (int64_t)lo);
+        std::vector<Pulse> raw;
+        std::vector<double> vmeans;
+        bool any_long = false;
+        for (const int64_t* q = b; q < run_start + nruns && *q < hi; ++q) {
+            const size_t k = q - run_start;
+            if (*q + run_len[k] > hi - 1) break;  // runs are sorted; an unterminated one ends the window
+            if (run_len[k] > P->max_pulse_len) continue;
+            raw.push_back({*q - lo, run_len[k]});
+            if ((double)run_len[k] > minlength) {
+                vmeans.push_back(run_mean[k]);
+                any_long = true;
+            }
+        }
+        LdgFieldPlan& pl = plans[np_out];
+        std::memset(&pl, 0, sizeof(pl));
+        pl.start = st.start;
+        pl.readloc = w.readloc;
+        pl.first_block = w.first_block;
+        pl.nblocks = w.nblocks;
+        pl.startloc = w.startloc;
+        pl.length = w.length;
+        pl.has_prev = st.prev_valid;
+        pl.proclines = P->proclines;
+
+        // getpulses (core.py:2242-2322)
+        if (raw.empty() && st.fields_written == 0) {
+            *stop = LDG_CHAIN_STOP_LEVELS;  // the reference re-levels ire0 from this field's data
+            break;
+        }
+        bool invalid = false;
+        double nextfieldoffset = 0;
+        bool have_next = false;
+        if (raw.empty()) {
+            invalid = true;  // compute_linelocs returns (None, None, None)
+        } else if (!any_long) {
+            invalid = true;  // getpulses returns None: no VSYNC-length pulse
+            if (st.fields_written == 0) {
+                nextfieldoffset = P->freq_hz;
+                have_next = true;
+            }
+        } else {
+            const double synclevel = median_of(vmeans);
+            const double sync_ire = (synclevel - P->ire0) / P->hz_ire;
+            if (!(std::fabs(sync_ire - P->vsync_ire) < 5)) {
+                *stop = LDG_CHAIN_STOP_LEVELS;  // black-level re-threshold of the pulses
+                break;
+            }
+        }
+        FieldPulses fp(*P, raw);
+        Slots slots;
+        bool isfirst = false;
+        int dep = 0;
+        if (!invalid) {
+            const Timings LT = fp.get_timings();
+            const std::vector<VPulse> vp = fp.refinepulses(LT);
+            const double meanlinelen = fp.compute_line_len(vp);
+            // getLine0 (core.py:2156-2239)
+            const VBlank loc_none = fp.process_vblank(vp, 0, -1);
+            VBlank loc = loc_none;
+            if (st.prev_valid) {
+                const VBlank loc_100 = fp.process_vblank(vp, 0, 100);
+                if (!(loc_100 == loc_none)) dep |= 1;  // needs the previous field's skip_check
+            }
+            int sync_conf = 100;
+            if (loc.zeroed_conf) sync_conf = 0;
+            bool have_l0next = false, first_next = false, have_vbn = false;
+            long long l0_next = 0;
+            double vbn = 0;
+            int conf_next = 0;
+            if (loc.ok) {
+                const VBlank nx = fp.process_vblank(vp, loc.firstblank + 40, -1);
+                if (nx.zeroed_conf) sync_conf = 0;
+                if (nx.ok) {
+                    have_vbn = true;
+                    vbn = (double)nx.line0;
+                    first_next = !nx.isfirst;
+                    conf_next = nx.conf;
+                    const double fieldlen = meanlinelen * P->field_lines[first_next ? 0 : 1];
+                    l0_next = nround(vbn - fieldlen);
+                    have_l0next = true;
+                    if (l0_next < 0) sync_conf = 10;
+                }
+            }
+            const bool have_prev_l0 = st.prev_valid != 0;
+            double l0 = 0;
+            bool have_l0 = false;
+            bool range = false;
+            double l0_lo = 0, l0_hi = 0;
+            if (loc.ok && have_l0next && have_prev_l0) {
+                // median of (l0_local, l0_next, l0_prev): somewhere between the first two
+                const int votes = (int)loc.isfirst + (int)(!st.prev_isfirst) + (int)first_next;
+                isfirst = votes >= 2;
+                l0_lo = (double)std::min(loc.line0, l0_next);
+                l0_hi = (double)std::max(loc.line0, l0_next);
+                range = true;
+                have_l0 = true;
+                l0 = l0_lo;
+            } else if (loc.ok && loc.conf > 50) {
+                sync_conf = std::min(sync_conf, 90);
+                l0 = (double)loc.line0;
+                isfirst = loc.isfirst;
+                have_l0 = true;
+            } else if (have_prev_l0) {
+                dep |= 2;  // line 0 is the previous field's refined line location
+            } else if (have_l0next) {
+                sync_conf = conf_next;
+                l0 = (double)l0_next;
+                isfirst = first_next;
+                have_l0 = true;
+            }
+            pl.sync_confidence = sync_conf;
+            if (dep) {
+                *stop = LDG_CHAIN_STOP_PREV;
+                break;
+            }
+            const int linecount = isfirst ? 263 : 262;
+            if (!have_l0) {
+                invalid = true;
+                nextfieldoffset = P->inlinelen * 200;
+                have_next = true;
+            } else {
+                slots = line_slots(*P, vp, raw, l0, meanlinelen, vbn, have_vbn, linecount, have_vbn, vbn,
+                                   P->proclines);
+                if (range && l0_hi != l0_lo) {
+                    const Slots s2 = line_slots(*P, vp, raw, l0_hi, meanlinelen, vbn, have_vbn, linecount,
+                                                have_vbn, vbn, P->proclines);
+                    // the slot assignment is piecewise constant in line 0; equal results at
+                    // both ends of the vote's range hold inside it unless the skip rule,
+                    // which compares against a line-0-independent estimate, is active
+                    if (!same_slots(slots, s2) || slots.skipdetected || s2.skipdetected) {
+                        *stop = LDG_CHAIN_STOP_PREV;
+                        break;
+                    }
+                }
+                if (slots.error) {
+                    *stop = LDG_CHAIN_STOP_ERROR;
+                    break;
+                }
+                if (!slots.ok) {
+                    invalid = true;
+                    nextfieldoffset = slots.nextfield;
+                    have_next = true;
+                }
+            }
+            pl.linecount = linecount;
+        }
+        if (invalid) {
+            if (!have_next) nextfieldoffset = P->linelen * 200;
+            pl.valid = 0;
+            pl.nextfieldoffset = nextfieldoffset;
+            st.start += nextfieldoffset;
+            st.prev_valid = 0;
+            np_out += 1;
+            continue;
+        }
+        // process(): compute_deriv_error on the pulse-level line locations
+        std::vector<unsigned char> bad = slots.err;
+        deriv_error(slots.filled, bad);
+        pl.valid = 1;
+        pl.isfirst = isfirst;
+        pl.nextfieldoffset = slots.nextfield;
+        for (int l = 0; l < P->proclines; ++l) {
+            pl.linelocs1[l] = slots.filled[l];
+            pl.linebad[l] = bad[l];
+        }
+        st.start += slots.nextfield - (double)(w.readloc - w.startloc);
+        st.prev_valid = 1;
+        st.prev_isfirst = isfirst;
+        st.prev_startloc = w.startloc;
+        st.fields_written += 1;
+        np_out += 1;
+    }
+    if (np_out >= max_plans && *stop == LDG_CHAIN_STOP_END) *stop = LDG_CHAIN_STOP_FULL;
+    *nplans = np_out;
+    *state_out = st;
+    return 0;
+}
+
+}  // extern "C"
+
+extern "C" int64_t ldg_abi_sizeof(const char* name) {
+    if (!name) return -1;
+    const std::string n(name);
+    if (n == "ldg_chain_params") return sizeof(ldg_chain_params);
+    if (n == "ldg_chain_state") return sizeof(ldg_chain_state);
+    if (n == "ldg_field_plan") return sizeof(ldg_field_plan);
+    if (n == "ldg_lines_consts") return sizeof(ldg_lines_consts);
+    if (n == "ldg_lines_args") return sizeof(ldg_lines_args);
+    if (n == "ldg_tbc_field") return sizeof(ldg_tbc_field);
+    if (n == "ldg_demod_args") return sizeof(ldg_demod_args);
+    if (n == "ldg_slice") return sizeof(ldg_slice);
+    return -1;
+}

@@ -1,0 +1,780 @@
+// Sync-pulse runs and per-line refinement of line locations on the GPU.
+//
+// ldg_sync_runs: runs of demod_05 at or below the sync threshold over a
+// whole capture-wide output array -- the pulses findpulses
+// (lddecode/utils.py:1101-1157) finds, for every field read window at once --
+// and the mean level inside the long ones (getpulses' VSYNC level check,
+// core.py:2242-2322).  Three passes over the array: edges counted per tile,
+// an exclusive scan of the tile counts, edges written in order; then one
+// warp per run pairs its edges and averages its interior.
+//
+// ldg_lines_refine: the per-line refinement of Field.process() for all
+// fields of a capture (pulse-level line locations from the host chain):
+//   lines_hsync_kernel   one CTA per field: refine_linelocs_hsync
+//                        (core.py:2483-2551), compute_deriv_error
+//                        (2553-2564); NTSC: the colour-burst zero crossings
+//                        of compute_line_bursts (2998-3047, clb_findbursts
+//                        utils.py:1339-1368) per line; PAL:
+//                        refine_linelocs_pilot twice (3054-3093) and
+//                        fix_badlines (2566-2589) -> final line locations.
+//   burst_chain_kernel   NTSC, one CTA walking the fields in order: the
+//                        burst phase of every line starts from the previous
+//                        field's phase_adjust_median (compute_burst_offsets,
+//                        core.py:3360-3388), two passes of the phase
+//                        update, the field's median and its field-1/4 flag.
+//   burst_apply_kernel   NTSC, one CTA per field: refine_linelocs_burst
+//                        (3390-3440), fix_badlines with linelocs2 as backup,
+//                        the 117.25-degree subcarrier shift (3493-3495).
+// Positions, fits and phases are FP64; samples are the float32 outputs.
+#include <cmath>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "ldgpu.h"
+
+struct ldg_ctx;
+
+namespace ldg {
+int lines_fail(int code, const std::string& msg);
+int ctx_device(const ldg_ctx* c);
+std::mutex& ctx_mutex(ldg_ctx* c);
+int ctx_lines_scratch(ldg_ctx* c, size_t need, void** out);
+}  // namespace ldg
+
+namespace {
+
+constexpr int kMaxL = LDG_CHAIN_MAX_LINES;
+constexpr int kEdgeTile = 8192;
+constexpr int kEdgeThreads = 256;
+constexpr int kLineThreads = 352;   // >= proclines (326 PAL)
+constexpr int kBurstLines = 266;    // compute_burst_offsets covers lines 0..265
+constexpr int kPilotLines = 323;    // refine_linelocs_pilot covers lines 0..322
+constexpr int kZc = 16;             // clb_findbursts' fixed zero-crossing slots
+
+// ---------------------------------------------------------------- sync runs
+
+__device__ __forceinline__ bool below(const float* x, long long i, double thr) { return (double)x[i] <= thr; }
+
+__global__ void __launch_bounds__(kEdgeThreads) edge_count_kernel(const float* __restrict__ x, long long n,
+                                                                   double thr, int* __restrict__ counts) {
+    const long long t0 = (long long)blockIdx.x * kEdgeTile;
+    int c = 0;
+    for (int j = 0; j < kEdgeTile / kEdgeThreads; ++j) {
+        const long long i = t0 + j * kEdgeThreads + threadIdx.x;
+        if (i < n) {
+            const bool b = below(x, i, thr);
+            const bool bp = i > 0 ? below(x, i - 1, thr) : false;
+            c += b != bp;
+        }
+    }
+    __shared__ int warp_sum[kEdgeThreads / 32];
+    int v = c;
+    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int w = 0; w < kEdgeThreads / 32; ++w) s += warp_sum[w];
+        counts[blockIdx.x] = s;
+    }
+}
+
+// exclusive scan of the tile counts (one CTA; ntiles is ~n / 8192)
+__global__ void __launch_bounds__(1024) edge_scan_kernel(const int* __restrict__ counts, long long ntiles,
+                                                         long long* __restrict__ offsets,
+                                                         long long* __restrict__ total) {
+    __shared__ long long part[1024];
+    __shared__ long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (long long base = 0; base < ntiles; base += 1024) {
+        const long long i = base + threadIdx.x;
+        const long long v = i < ntiles ? counts[i] : 0;
+        part[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            const long long add = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+            __syncthreads();
+            part[threadIdx.x] += add;
+            __syncthreads();
+        }
+        if (i < ntiles) offsets[i] = carry + part[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += part[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// edges as 2*i + (run start ? 1 : 0), in increasing i
+__global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const float* __restrict__ x, long long n,
+                                                                   double thr, const long long* __restrict__ offsets,
+                                                                   long long* __restrict__ edges, long long cap) {
+    __shared__ int warp_cnt[kEdgeThreads / 32];
+    const long long t0 = (long long)blockIdx.x * kEdgeTile;
+    long long out = offsets[blockIdx.x];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = 0; j < kEdgeTile / kEdgeThreads; ++j) {
+        const long long i = t0 + j * kEdgeThreads + threadIdx.x;
+        bool flag = false, b = false;
+        if (i < n) {
+            b = below(x, i, thr);
+            const bool bp = i > 0 ? below(x, i - 1, thr) : false;
+            flag = b != bp;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, flag);
+        if (lane == 0) warp_cnt[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, chunk = 0;
+        for (int w = 0; w < kEdgeThreads / 32; ++w) {
+            before += w < warp ? warp_cnt[w] : 0;
+            chunk += warp_cnt[w];
+        }
+        if (flag) {
+            const long long k = out + before + __popc(m & ((1u << lane) - 1u));
+            if (k < cap) edges[k] = 2 * i + (b ? 1 : 0);
+        }
+        out += chunk;
+        __syncthreads();
+    }
+}
+
+// one warp per run: pair edges 2r (start) and 2r+1 (end), interior mean of long runs
+__global__ void run_pair_kernel(const long long* __restrict__ edges, long long nruns, const float* __restrict__ x,
+                                long long min_long, long long trim_lo, long long trim_hi,
+                                long long* __restrict__ rs, long long* __restrict__ rl, double* __restrict__ rm) {
+    const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= nruns) return;
+    const long long s = edges[2 * r] >> 1, e = edges[2 * r + 1] >> 1;
+    const long long len = e - s;
+    double mean = nan("");
+    if (len > min_long) {
+        const long long lo = s + trim_lo, hi = s + len - trim_hi;
+        double acc = 0;
+        for (long long i = lo + lane; i < hi; i += 32) acc += (double)x[i];
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (hi > lo) mean = acc / (double)(hi - lo);
+    }
+    if (lane == 0) {
+        rs[r] = s;
+        rl[r] = len;
+        rm[r] = mean;
+    }
+}
+
+// --------------------------------------------------------- per-line helpers
+
+// calczc (utils.py:812-841) over x[0, n): first crossing of `target` within
+// count+1 samples from int(start); edge 0 decides rising/falling from
+// x[int(start)].  Comparisons and the interpolation in FP64.
+__device__ bool calczc(const float* x, long long n, double start_offset, double target, int edge, double count,
+                       double& out) {
+    const long long s = (long long)start_offset;
+    if (s < 0 || s >= n) return false;
+    const long long icount = (long long)(count + 1);
+    if (edge == 0) edge = (double)x[s] < target ? 1 : -1;
+    const long long end = min(s + icount, n);
+    long long loc = -1;
+    if (edge == 1) {
+        for (long long i = s + 1; i < end; ++i)
+            if ((double)x[i - 1] < target && (double)x[i] >= target) {
+                loc = i;
+                break;
+            }
+    } else {
+        for (long long i = s + 1; i < end; ++i)
+            if ((double)x[i - 1] > target && (double)x[i] <= target) {
+                loc = i;
+                break;
+            }
+    }
+    if (loc < 0) return false;
+    const double a = (double)x[loc - 1] - target, b = (double)x[loc] - target;
+    const double y = (b - a != 0) ? -a / (-a + b) : 0.0;
+    out = (double)(loc - 1) + y;
+    return true;
+}
+
+// np.median of a float32 slice (even length: float32 mean of the middle two)
+__device__ double median_f32(const float* x, long long lo, long long hi, long long n) {
+    lo = max(lo, 0LL);
+    hi = min(hi, n);
+    float v[128];
+    int m = 0;
+    for (long long i = lo; i < hi && m < 128; ++i) {
+        const float t = x[i];
+        int k = m++;
+        while (k > 0 && v[k - 1] > t) {
+            v[k] = v[k - 1];
+            --k;
+        }
+        v[k] = t;
+    }
+    if (m == 0) return nan("");
+    if (m & 1) return (double)v[m / 2];
+    return (double)((v[m / 2 - 1] + v[m / 2]) * 0.5f);
+}
+
+// get_linelen (core.py:1655-1672) with linecount + lineoffset = lc
+__device__ double line_len(const double* ll, int line, int lc, double linelen) {
+    double length;
+    if (line >= lc) length = ll[line] - ll[line - 1];
+    else if (line > 0) length = (ll[line + 1] - ll[line - 1]) / 2;
+    else length = ll[line + 1] - ll[line];
+    return length <= 0 ? linelen : length;
+}
+
+// second differences above 4 samples mark both later lines bad
+__device__ void deriv_error_block(const double* ll, unsigned char* bad, int nl) {
+    const int j = threadIdx.x;
+    bool b1 = false;
+    if (j + 2 < nl) b1 = fabs((ll[j + 2] - ll[j + 1]) - (ll[j + 1] - ll[j])) > 4;
+    __syncthreads();
+    if (b1) {
+        bad[j + 1] = 1;
+        bad[j + 2] = 1;
+    }
+    __syncthreads();
+}
+
+// fix_badlines' interpolation over good neighbours; reads ll, writes out
+__device__ void fix_badlines_block(const double* ll, const unsigned char* bad, double* out, int nl, int firstcheck) {
+    const int l = threadIdx.x;
+    if (l < nl) {
+        double v = ll[l];
+        if (bad[l]) {
+            int pg = l - 1;
+            while (pg >= 0 && bad[pg]) --pg;
+            int ng = l + 1;
+            while (ng < nl && bad[ng]) ++ng;
+            if (pg >= firstcheck && ng < nl) {
+                const double gap = (ll[ng] - ll[pg]) / (double)(ng - pg);
+                v = (gap * (double)(l - pg)) + ll[pg];
+            }
+        }
+        out[l] = v;
+    }
+    __syncthreads();
+}
+
+// block-wide sort of up to 512 doubles in shared memory (NaN-free keys)
+__device__ void bitonic512(double* k) {
+    for (int size = 2; size <= 512; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < 256; t += blockDim.x) {
+                const int i = 2 * t - (t & (stride - 1));
+                const int jx = i + stride;
+                const bool up = (i & size) == 0;
+                const double a = k[i], b = k[jx];
+                if ((a > b) == up) {
+                    k[i] = b;
+                    k[jx] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// median of the first `cnt` entries of a sorted array (np.median)
+__device__ __forceinline__ double sorted_median(const double* k, int cnt) {
+    if (cnt & 1) return k[cnt / 2];
+    return (k[cnt / 2 - 1] + k[cnt / 2]) / 2.0;
+}
+
+struct LineParams {
+    ldg_lines_args a;
+    int system;
+    double freq, linelen, linefreq0, samplesperline;
+    double half_sync, lo_ok, hi_ok, hz_ire, fsc_mhz, pilot_mhz;
+    struct BurstRec* rec;  // nfields x kBurstLines
+    double* ll2;           // nfields x kMaxL (NTSC linelocs2)
+    double* adjs;          // nfields x kBurstLines (NaN: none)
+    int* field14;          // per field
+};
+
+struct BurstRec {
+    float zcs[kZc];
+    double bstart, s_rem, zcburstdiv;
+    int count, rising, valid, pad;
+};
+
+// compute_line_bursts up to the phase update: the zero crossings of the
+// line's colour burst (they do not depend on the phase seed)
+__device__ void burst_record(const LineParams& P, const double* ll, int line, int lc, const float* burst,
+                             const float* demod, long long n, BurstRec& r) {
+    r.valid = 0;
+    r.count = 0;
+    r.rising = 0;
+    const long long s = (long long)ll[line];
+    const double s_rem = ll[line] - (double)s;
+    const double lfreq = P.samplesperline * line_len(ll, line, lc, P.linelen);
+    const double fsc_inv = 1 / P.fsc_mhz;
+    const long long bstart = (long long)(21 * fsc_inv * lfreq);
+    const long long bend = (long long)(28 * fsc_inv * lfreq);
+    long long lo = s + bstart, hi = min(s + bend, n);
+    if (lo < 0 || hi <= lo) return;
+    const int m = (int)min(hi - lo, 128LL);
+    float ba[128];
+    double acc = 0;
+    for (int k = 0; k < m; ++k) acc += (double)burst[lo + k];
+    const float mean_f = (float)(acc / m);
+    for (int k = 0; k < m; ++k) ba[k] = burst[lo + k] - mean_f;
+    double m2 = 0;
+    for (int k = 0; k < m; ++k) m2 += (double)ba[k];
+    m2 /= m;
+    double ss = 0;
+    for (int k = 0; k < m; ++k) {
+        const double d = (double)ba[k] - m2;
+        ss += d * d;
+    }
+    const double threshold = sqrt(ss / m);
+    double accd = 0;
+    for (int k = 0; k < m; ++k) accd += (double)demod[lo + k];
+    const float mean_d = (float)(accd / m);
+    float mx = 0;
+    for (int k = 0; k < m; ++k) mx = fmaxf(mx, fabsf(demod[lo + k] - mean_d));
+    if ((double)mx > 30 * P.hz_ire) return;
+    r.valid = 1;
+    r.bstart = (double)bstart;
+    r.s_rem = s_rem;
+    r.zcburstdiv = (lfreq * fsc_inv) / 2;
+    for (int k = 0; k < kZc; ++k) r.zcs[k] = 0.0f;
+    int c = 0;
+    long long j = 0;
+    const long long end = m - 1;
+    while (j < end && c < kZc) {
+        if ((double)fabsf(ba[j]) > threshold) {
+            double zc;
+            if (!calczc(ba, m, (double)j, 0.0, 0, 16, zc)) break;
+            if (ba[j] < 0) r.rising |= 1 << c;
+            r.zcs[c] = (float)zc;
+            ++c;
+            j = (long long)zc + 1;
+        } else {
+            ++j;
+        }
+    }
+    r.count = c;
+}
+
+// _angle_mean_phase / phase_distance helpers (core.py:3085-3093)
+__device__ __forceinline__ double phase_distance(double x, double c) {
+    double d = (x - floor(x)) - c;
+    if (d < -0.5) d += 1;
+    else if (d > 0.5) d -= 1;
+    return d;
+}
+
+// one refine_linelocs_pilot pass over ll (shared), in place
+__device__ void pilot_pass(const LineParams& P, double* ll, const float* pilot, long long n, double* zcs,
+                           double* plen, unsigned char* ok, double* red) {
+    const int l = threadIdx.x;
+    double zc = 0;
+    bool good = false;
+    if (l < kPilotLines) {
+        double adjfreq = P.freq;
+        if (l > 1) adjfreq /= (ll[l] - ll[l - 1]) / P.linelen;
+        plen[l] = (adjfreq / P.pilot_mhz) / 2;
+        const double b0 = ll[l];
+        const long long st = (long long)(b0 + 0.0);
+        long long sp = (long long)(b0 + 6 * P.linefreq0 + 0.0 + 1);
+        sp = min(sp, n);
+        const double lsoffset = ll[l] - (double)st;
+        if (st >= 0 && sp > st) {
+            const float* seg = pilot + st;
+            const long long m = sp - st;
+            long long peak = 0;
+            float best = -1.0f;
+            for (long long k = 0; k < m; ++k) {
+                const float v = fabsf(seg[k]);
+                if (v > best) {
+                    best = v;
+                    peak = k;
+                }
+            }
+            double zb;
+            if (calczc(seg, m, (double)peak, 0.0, 0, 16, zb)) {
+                zc = (zb - lsoffset) / plen[l];
+                good = true;
+            }
+        }
+        zcs[l] = zc;
+        ok[l] = good;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // a line without a crossing repeats the previous line's value
+        double last = 0;
+        for (int k = 0; k < kPilotLines; ++k) {
+            if (!ok[k]) zcs[k] = last;
+            last = zcs[k];
+        }
+    }
+    __syncthreads();
+    // mean phase of the fractional parts
+    double cs = 0, sn = 0;
+    if (l < kPilotLines) {
+        const double x = zcs[l];
+        const double x2 = x - (double)(int)x;
+        const double th = x2 * 3.14159265358979323846 * 2;
+        cs = cos(th);
+        sn = sin(th);
+    }
+    red[2 * l] = cs;
+    red[2 * l + 1] = sn;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0;
+        for (int k = 0; k < kPilotLines; ++k) {
+            a += red[2 * k];
+            b += red[2 * k + 1];
+        }
+        double am = atan2(b / kPilotLines, a / kPilotLines) / (3.14159265358979323846 * 2);
+        if (am < 0) am = 1 + am;
+        red[0] = am;
+    }
+    __syncthreads();
+    const double am = red[0];
+    if (l < kPilotLines) ll[l] += phase_distance(zcs[l], am) * plen[l];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P) {
+    const int f = blockIdx.x;
+    const ldg_lines_args& a = P.a;
+    const long long base = a.startloc[f];
+    const long long n = min((long long)a.wlen[f], (long long)(a.capture_len - base));
+    const float* d05 = a.d05 + base;
+    const int nl = a.proclines;
+    __shared__ double ll1[kMaxL], ll[kMaxL], tmp[kMaxL];
+    __shared__ unsigned char bad[kMaxL], okf[kMaxL];
+    __shared__ double red[2 * kLineThreads];
+    const int i = threadIdx.x;
+    if (i < nl) {
+        ll1[i] = a.linelocs1[(long long)f * kMaxL + i];
+        bad[i] = a.linebad1[(long long)f * kMaxL + i];
+    }
+    __syncthreads();
+    // refine_linelocs_hsync
+    if (i < nl) {
+        bool b = bad[i];
+        double v2 = ll1[i];
+        if ((i >= 3 && i <= 6) || (P.system == 1 && i >= 1 && i <= 2)) {
+            b = true;
+        } else {
+            const double l1 = ll1[i] - P.freq;
+            double zc;
+            if (calczc(d05, n, l1, P.half_sync, 0, P.freq * 2, zc) && !b) {
+                v2 = zc;
+                const long long lo = (long long)(zc - (P.freq * 0.75)), hi = min((long long)(zc + (P.freq * 8)), n);
+                float mn = INFINITY, mx = -INFINITY;
+                for (long long k = max(lo, 0LL); k < hi; ++k) {
+                    mn = fminf(mn, d05[k]);
+                    mx = fmaxf(mx, d05[k]);
+                }
+                if ((double)mn < P.lo_ok || (double)mx > P.hi_ok) {
+                    b = true;
+                } else {
+                    const double porch = median_f32(d05, (long long)(zc + (P.freq * 8)), (long long)(zc + (P.freq * 9)), n);
+                    const double sync = median_f32(d05, (long long)(zc + (P.freq * 1)), (long long)(zc + (P.freq * 2.5)), n);
+                    double zc2;
+                    if (calczc(d05, n, l1, (porch + sync) / 2, 0, 400, zc2) && fabs(zc2 - zc) < (P.freq / 2))
+                        v2 = zc2;
+                    else
+                        b = true;
+                }
+            } else {
+                b = true;
+            }
+        }
+        if (b) v2 = ll1[i];
+        ll[i] = v2;
+        bad[i] = b;
+    }
+    __syncthreads();
+    deriv_error_block(ll, bad, nl);
+    if (P.system == 0) {
+        // NTSC: linelocs2 out, burst zero crossings per line
+        if (i < nl) P.ll2[(long long)f * kMaxL + i] = ll[i];
+        if (i < nl) a.linebad[(long long)f * kMaxL + i] = bad[i];
+        if (i < kBurstLines && i < nl)
+            burst_record(P, ll, i, a.linecount[f], a.burst + base, a.demod + base, n,
+                         P.rec[(long long)f * kBurstLines + i]);
+        return;
+    }
+    // PAL: two pilot passes, then fix_badlines (no backup, lines from 0)
+    pilot_pass(P, ll, a.pilot + base, n, tmp, ll1, okf, red);
+    pilot_pass(P, ll, a.pilot + base, n, tmp, ll1, okf, red);
+    deriv_error_block(ll, bad, nl);
+    fix_badlines_block(ll, bad, tmp, nl, 0);
+    if (i < nl) {
+        a.linelocs[(long long)f * kMaxL + i] = tmp[i];
+        a.linebad[(long long)f * kMaxL + i] = bad[i];
+    }
+}
+
+// NTSC burst phase chain: fields in order, lines in parallel
+__global__ void __launch_bounds__(512) burst_chain_kernel(LineParams P) {
+    const ldg_lines_args& a = P.a;
+    __shared__ double keys[512];
+    __shared__ int rsum;
+    __shared__ int nadj;
+    double prev_pam = a.prev_phase_adjust;
+    const int l = threadIdx.x;
+    for (int f = 0; f < a.nfields; ++f) {
+        const double prev = a.has_prev[f] ? prev_pam : 0.0;
+        if (l == 0) {
+            rsum = 0;
+            nadj = 0;
+        }
+        __syncthreads();
+        double adj = nan("");
+        if (l < kBurstLines) {
+            const BurstRec& r = P.rec[(long long)f * kBurstLines + l];
+            if (r.valid) {
+                double pa = -prev;
+                int rising_count = 0;
+                for (int pass = 0; pass < 2; ++pass) {
+                    rising_count = 0;
+                    if (r.count) {
+                        double dev[kZc];
+                        int odd = 0;
+                        for (int k = 0; k < kZc; ++k) {
+                            const double cyc = ((r.bstart + (double)r.zcs[k] - r.s_rem) / r.zcburstdiv) + pa;
+                            const int rnd = (int)(cyc + .5);
+                            if (rnd % 2 != 0) odd |= 1 << k;
+                            dev[k] = (double)rnd - cyc;
+                        }
+                        // median of the 16 slots (sorting network by insertion)
+                        for (int x = 1; x < kZc; ++x) {
+                            const double t = dev[x];
+                            int y = x;
+                            while (y > 0 && dev[y - 1] > t) {
+                                dev[y] = dev[y - 1];
+                                --y;
+                            }
+                            dev[y] = t;
+                        }
+                        pa += (dev[kZc / 2 - 1] + dev[kZc / 2]) / 2.0;
+                        rising_count = __popc((unsigned)(r.rising ^ odd) & 0xffffu);
+                    }
+                }
+                const bool rising = (double)rising_count > ((double)r.count / 2);
+                adj = (-pa) / 2;
+                if (!(l % 2) && rising) atomicAdd(&rsum, 1);
+                atomicAdd(&nadj, 1);
+            }
+            P.adjs[(long long)f * kBurstLines + l] = adj;
+        }
+        keys[l] = (l < kBurstLines && !isnan(adj)) ? adj : INFINITY;
+        __syncthreads();
+        bitonic512(keys);
+        if (l == 0) {
+            const int cnt = nadj;
+            P.field14[f] = rsum > (cnt / 4);
+            // np.median of an empty list is NaN; the reference then carries NaN forward
+            const double med = cnt ? sorted_median(keys, cnt) : nan("");
+            a.phase_adjust[f] = med * 2;
+            keys[0] = med * 2;
+        }
+        __syncthreads();
+        prev_pam = keys[0];
+        __syncthreads();
+    }
+}
+
+// NTSC: refine_linelocs_burst's application, fix_badlines, subcarrier shift
+__global__ void __launch_bounds__(512) burst_apply_kernel(LineParams P, double shift) {
+    const int f = blockIdx.x;
+    const ldg_lines_args& a = P.a;
+    const int nl = a.proclines;
+    const int lc = a.linecount[f];
+    __shared__ double ll2[kMaxL], adj_ll[kMaxL], out[kMaxL], adjs[kBurstLines];
+    __shared__ unsigned char bad[kMaxL], has[kBurstLines];
+    __shared__ double keys[512];
+    __shared__ int nadj;
+    const int l = threadIdx.x;
+    if (l == 0) nadj = 0;
+    if (l < nl) {
+        ll2[l] = P.ll2[(long long)f * kMaxL + l];
+        bad[l] = a.linebad[(long long)f * kMaxL + l];
+    }
+    double an = nan("");
+    if (l < kBurstLines) an = P.adjs[(long long)f * kBurstLines + l];
+    __syncthreads();
+    if (l >= 1 && l < kBurstLines && l < nl && isnan(an)) bad[l] = 1;
+    __syncthreads();
+    double adj = nan("");
+    if (l < kBurstLines && l < nl) {
+        has[l] = 0;
+        if (!(isnan(ll2[l]) || bad[l]) && !isnan(an)) {
+            const double lfreq = P.samplesperline * line_len(ll2, l, lc, P.linelen);
+            adj = an * lfreq * (1 / P.fsc_mhz);
+            has[l] = 1;
+            atomicAdd(&nadj, 1);
+        }
+        adjs[l] = adj;
+    }
+    keys[l] = isnan(adj) ? INFINITY : adj;
+    if (l < nl) adj_ll[l] = ll2[l];
+    __syncthreads();
+    bitonic512(keys);
+    if (l == 0) {
+        const int cnt = nadj;
+        if (cnt) {
+            const double med = sorted_median(keys, cnt);
+            double lastvalid = med;
+            for (int k = 0; k < kBurstLines && k < nl; ++k) {
+                if (has[k] && adjs[k] - med >= -2 && adjs[k] - med <= 2) {
+                    adj_ll[k] += adjs[k];
+                    lastvalid = adjs[k];
+                } else {
+                    adj_ll[k] += lastvalid;
+                }
+            }
+            const bool first = a.isfirst[f] != 0, f14 = P.field14[f] != 0;
+            a.field_phase[f] = first ? (f14 ? 1 : 3) : (f14 ? 4 : 2);
+        } else {
+            a.field_phase[f] = 1;
+        }
+    }
+    __syncthreads();
+    // fix_badlines(linelocs3, linelocs2): deriv error, NaN from backup, interpolate (from line 1)
+    deriv_error_block(adj_ll, bad, nl);
+    if (l < nl && isnan(adj_ll[l])) adj_ll[l] = ll2[l];
+    __syncthreads();
+    fix_badlines_block(adj_ll, bad, out, nl, 1);
+    if (l < nl) {
+        a.linelocs[(long long)f * kMaxL + l] = out[l] - shift;
+        a.linebad[(long long)f * kMaxL + l] = bad[l];
+    }
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" {
+
+int ldg_sync_runs(ldg_ctx* c, const float* d05, int64_t n, double threshold, int64_t min_long, int64_t trim_lo,
+                  int64_t trim_hi, int64_t* run_start, int64_t* run_len, double* run_mean, int64_t cap,
+                  int64_t* nruns, void* stream) {
+    if (!c || !d05 || !run_start || !run_len || !run_mean || !nruns)
+        return ldg::lines_fail(LDG_ERR_ARG, "ldg_sync_runs: NULL argument");
+    if (n < 2 || cap < 1 || trim_lo < 0 || trim_hi < 0) return ldg::lines_fail(LDG_ERR_ARG, "ldg_sync_runs: bad size");
+    std::lock_guard<std::mutex> lk(ldg::ctx_mutex(c));
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(ldg::ctx_device(c));
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long ntiles = (n + kEdgeTile - 1) / kEdgeTile;
+    const long long ecap = 2 * cap + 2;
+    const size_t b_counts = align256(ntiles * sizeof(int)), b_off = align256(ntiles * sizeof(long long));
+    const size_t b_tot = 256, b_edges = align256(ecap * sizeof(long long));
+    const size_t b_runs = align256(cap * sizeof(long long));
+    const size_t need = b_counts + b_off + b_tot + b_edges + 2 * b_runs + align256(cap * sizeof(double));
+    void* scratch = nullptr;
+    auto done = [&](int rc) {
+        if (prev >= 0) cudaSetDevice(prev);
+        return rc;
+    };
+    if (ldg::ctx_lines_scratch(c, need, &scratch) != LDG_OK) return done(LDG_ERR_CUDA);
+    char* p = static_cast<char*>(scratch);
+    int* counts = reinterpret_cast<int*>(p);
+    long long* offsets = reinterpret_cast<long long*>(p + b_counts);
+    long long* total = reinterpret_cast<long long*>(p + b_counts + b_off);
+    long long* edges = reinterpret_cast<long long*>(p + b_counts + b_off + b_tot);
+    long long* rs = reinterpret_cast<long long*>(p + b_counts + b_off + b_tot + b_edges);
+    long long* rl = rs + b_runs / sizeof(long long);
+    double* rm = reinterpret_cast<double*>(rl + b_runs / sizeof(long long));
+    auto cuda_fail = [&](const char* what) {
+        return done(ldg::lines_fail(LDG_ERR_CUDA, std::string("ldg_sync_runs: ") + what + ": " +
+                                                      cudaGetErrorString(cudaGetLastError())));
+    };
+    edge_count_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, counts);
+    edge_scan_kernel<<<1, 1024, 0, st>>>(counts, ntiles, offsets, total);
+    long long nedges = 0;
+    if (cudaMemcpyAsync(&nedges, total, sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return cuda_fail("edge count");
+    const long long nr = nedges / 2;  // an odd count leaves a run open at the end
+    *nruns = nr;
+    if (nr > cap || nedges > ecap) return done(ldg::lines_fail(LDG_ERR_RANGE, "ldg_sync_runs: more runs than cap"));
+    edge_write_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, offsets, edges, ecap);
+    if (nr > 0) {
+        const long long threads = nr * 32;
+        run_pair_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(edges, nr, d05, min_long, trim_lo,
+                                                                           trim_hi, rs, rl, rm);
+        if (cudaMemcpyAsync(run_start, rs, nr * sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(run_len, rl, nr * sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(run_mean, rm, nr * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return cuda_fail("D2H");
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_fail("run pairing");
+    return done(LDG_OK);
+}
+
+int64_t ldg_lines_scratch_bytes(int32_t nfields) {
+    if (nfields < 0) return -1;
+    return (int64_t)(align256((size_t)nfields * kBurstLines * sizeof(BurstRec)) +
+                     align256((size_t)nfields * kMaxL * sizeof(double)) +
+                     align256((size_t)nfields * kBurstLines * sizeof(double)) +
+                     align256((size_t)nfields * sizeof(int)));
+}
+
+}  // extern "C"
+
+extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
+    if (!c || !a) return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: NULL argument");
+    if (a->nfields < 0 || a->proclines < 8 || a->proclines > kMaxL || (a->k.system != 0 && a->k.system != 1))
+        return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: bad size or system");
+    if (a->nfields == 0) return LDG_OK;
+    if (!a->d05 || !a->startloc || !a->wlen || !a->isfirst || !a->linecount || !a->has_prev || !a->linelocs1 ||
+        !a->linebad1 || !a->linelocs || !a->linebad || !a->scratch ||
+        (a->k.system == 0 && (!a->demod || !a->burst || !a->phase_adjust || !a->field_phase)) ||
+        (a->k.system == 1 && !a->pilot))
+        return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: NULL buffer");
+    if (a->k.system == 0 && a->proclines < kBurstLines)
+        return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: NTSC needs proclines >= 266");
+    if (a->k.system == 1 && a->proclines < kPilotLines)
+        return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: PAL needs proclines >= 323");
+    LineParams P;
+    P.a = *a;
+    P.system = a->k.system;
+    P.freq = a->k.freq;
+    P.linelen = a->k.linelen;
+    P.linefreq0 = a->k.linefreq0;
+    P.samplesperline = a->k.samplesperline;
+    P.half_sync = a->k.half_sync;
+    P.lo_ok = a->k.lo_ok;
+    P.hi_ok = a->k.hi_ok;
+    P.hz_ire = a->k.hz_ire;
+    P.fsc_mhz = a->k.fsc_mhz;
+    P.pilot_mhz = a->k.pilot_mhz;
+    char* s = static_cast<char*>(a->scratch);
+    const size_t nf = (size_t)a->nfields;
+    P.rec = reinterpret_cast<BurstRec*>(s);
+    s += align256(nf * kBurstLines * sizeof(BurstRec));
+    P.ll2 = reinterpret_cast<double*>(s);
+    s += align256(nf * kMaxL * sizeof(double));
+    P.adjs = reinterpret_cast<double*>(s);
+    s += align256(nf * kBurstLines * sizeof(double));
+    P.field14 = reinterpret_cast<int*>(s);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(ldg::ctx_device(c));
+    cudaStream_t st = (cudaStream_t)a->stream;
+    lines_hsync_kernel<<<a->nfields, kLineThreads, 0, st>>>(P);
+    if (P.system == 0) {
+        burst_chain_kernel<<<1, 512, 0, st>>>(P);
+        const double shift = (117.25 / 360) / P.fsc_mhz * P.freq;
+        burst_apply_kernel<<<a->nfields, 512, 0, st>>>(P, shift);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (prev >= 0) cudaSetDevice(prev);
+    if (e != cudaSuccess) return ldg::lines_fail(LDG_ERR_CUDA, std::string("ldg_lines_refine: ") + cudaGetErrorString(e));
+    return LDG_OK;
+}

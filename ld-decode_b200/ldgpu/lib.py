@@ -53,6 +53,53 @@ class TbcField(ctypes.Structure):
     ]
 
 
+LDG_CHAIN_MAX_LINES = 336
+(LDG_CHAIN_STOP_END, LDG_CHAIN_STOP_FULL, LDG_CHAIN_STOP_PREV, LDG_CHAIN_STOP_LEVELS,
+ LDG_CHAIN_STOP_ERROR) = range(5)
+c_i32, c_i64, c_f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+
+
+class ChainParams(ctypes.Structure):
+    _fields_ = [
+        ("system", c_i32), ("num_pulses", c_i32), ("field_lines", c_i32 * 2), ("outlinecount", c_i32),
+        ("proclines", c_i32), ("freq", c_f64), ("freq_hz", c_f64), ("linelen", c_f64), ("inlinelen", c_f64),
+        ("linefreq0", c_f64), ("hsync_pulse_us", c_f64), ("eq_pulse_us", c_f64), ("vsync_pulse_us", c_f64),
+        ("first_field_h", c_f64 * 2), ("hsync_tolerance", c_f64), ("ire0", c_f64), ("hz_ire", c_f64),
+        ("vsync_ire", c_f64), ("max_pulse_len", c_i64), ("blocklen", c_i64), ("blockcut", c_i64),
+        ("blockcut_end", c_i64), ("readlen", c_i64), ("nblocks", c_i64),
+    ]
+
+
+class ChainState(ctypes.Structure):
+    _fields_ = [("start", c_f64), ("prev_valid", c_i32), ("prev_isfirst", c_i32), ("prev_startloc", c_i64),
+                ("fields_written", c_i32), ("pad", c_i32)]
+
+
+class FieldPlan(ctypes.Structure):
+    _fields_ = [
+        ("start", c_f64), ("readloc", c_i64), ("first_block", c_i64), ("nblocks", c_i64), ("startloc", c_i64),
+        ("length", c_i64), ("valid", c_i32), ("isfirst", c_i32), ("linecount", c_i32), ("proclines", c_i32),
+        ("has_prev", c_i32), ("sync_confidence", c_i32), ("nextfieldoffset", c_f64),
+        ("linelocs1", c_f64 * LDG_CHAIN_MAX_LINES), ("linebad", ctypes.c_uint8 * LDG_CHAIN_MAX_LINES),
+    ]
+
+
+class LinesConsts(ctypes.Structure):
+    _fields_ = [("system", c_i32), ("pad", c_i32), ("freq", c_f64), ("linelen", c_f64), ("linefreq0", c_f64),
+                ("samplesperline", c_f64), ("half_sync", c_f64), ("lo_ok", c_f64), ("hi_ok", c_f64),
+                ("hz_ire", c_f64), ("fsc_mhz", c_f64), ("pilot_mhz", c_f64)]
+
+
+class LinesArgs(ctypes.Structure):
+    _fields_ = [
+        ("k", LinesConsts), ("d05", c_p), ("demod", c_p), ("burst", c_p), ("pilot", c_p), ("capture_len", c_i64),
+        ("nfields", c_i32), ("proclines", c_i32), ("startloc", c_p), ("wlen", c_p), ("isfirst", c_p),
+        ("linecount", c_p), ("has_prev", c_p), ("linelocs1", c_p), ("linebad1", c_p),
+        ("prev_phase_adjust", c_f64), ("linelocs", c_p), ("linebad", c_p), ("phase_adjust", c_p),
+        ("field_phase", c_p), ("scratch", c_p), ("stream", c_p),
+    ]
+
+
 SIGNATURES = {
     "ldg_abi_version": (ctypes.c_int, []),
     "ldg_last_error": (ctypes.c_char_p, []),
@@ -69,6 +116,15 @@ SIGNATURES = {
     "ldg_synchronize": (ctypes.c_int, [c_p]),
     "ldg_demod_scratch_bytes": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "ldg_demod_blocks_noalloc": (ctypes.c_int, [c_p, ctypes.POINTER(DemodArgs), ctypes.c_int32]),
+    "ldg_sync_runs": (ctypes.c_int, [c_p, c_p, c_i64, c_f64, c_i64, c_i64, c_i64, c_p, c_p, c_p, c_i64,
+                                     ctypes.POINTER(c_i64), c_p]),
+    "ldg_field_chain": (ctypes.c_int, [ctypes.POINTER(ChainParams), c_p, c_p, c_p, c_i64,
+                                       ctypes.POINTER(ChainState), ctypes.POINTER(ChainState), c_p, c_i32,
+                                       ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)]),
+    "ldg_chain_last_error": (ctypes.c_char_p, []),
+    "ldg_lines_scratch_bytes": (c_i64, [c_i32]),
+    "ldg_abi_sizeof": (c_i64, [ctypes.c_char_p]),
+    "ldg_lines_refine": (ctypes.c_int, [c_p, ctypes.POINTER(LinesArgs)]),
     "ldg_ac3_last_error": (ctypes.c_char_p, []),
     "ldg_ac3_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int32, c_p, ctypes.c_int32, c_p,
                                       ctypes.c_int32, c_p, ctypes.c_int32, ctypes.c_int32, c_p, c_p,

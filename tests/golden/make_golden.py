@@ -42,6 +42,9 @@ import numpy as np  # noqa: E402
 from lddecode import core as refcore  # noqa: E402
 from ldgpu.synth import synth_capture  # noqa: E402
 
+sys.path.insert(0, HERE)
+from audio_cases import AUDIO_CASES, audio_case_inputs  # noqa: E402
+
 STRIDE = 9
 COORD_STRIDE = 101
 CAPTURE_START = 123457
@@ -225,31 +228,6 @@ def lut_fixture():
     rows = np.concatenate([np.arange(0, 65537, 997), [32767, 32768, 65535, 65536]])
     np.savez_compressed(os.path.join(HERE, "sinc_lut_rows.npz"), rows=rows, values=lut[rows],
                         sha256=np.array(sha(lut)))
-
-
-AUDIO_CASES = [
-    # name, system, linecount, freq, timeoffset, audio dtype, audio length, glitch line
-    ("ntsc_44100", "NTSC", 263, 44100, 1.2e-5, "float64", 28800, 120),
-    ("ntsc_locked", "NTSC", 262, -2.8, 0.0, "float64", 28800, None),
-    ("pal_44100", "PAL", 312, 44100, -5e-6, "float32", 32600, 200),
-    ("ntsc_short", "NTSC", 263, 44100, 0.0, "float64", 20000, None),
-]
-
-
-def audio_case_inputs(system, linecount, dtype, alen, glitch, seed, line_period, audio_freqs):
-    """Seeded line locations (linear wow plus a glitch line) and integer-valued
-    FM-audio samples around the two carriers; shared with the tests."""
-    rng = np.random.default_rng(seed)
-    linelen = int(np.round(40e6 / (1e6 / line_period)))
-    n = linecount + 12
-    wow = 1 + 0.002 * np.sin(np.arange(n) / 37.0)
-    lineinfo = 1000.5 + np.concatenate([[0], np.cumsum(wow[:-1] * linelen)])
-    if glitch is not None:
-        lineinfo[glitch:] += 60.0
-    lf, rf_ = audio_freqs
-    left = lf + rng.integers(-150000, 150000, alen).astype(np.float64)
-    right = rf_ + rng.integers(-150000, 150000, alen).astype(np.float64)
-    return lineinfo, left.astype(dtype), right.astype(dtype), linelen
 
 
 def audio_fixture():

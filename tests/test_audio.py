@@ -11,7 +11,7 @@ import pytest
 from conftest import GOLDEN, golden
 
 sys.path.insert(0, GOLDEN)
-from make_golden import AUDIO_CASES, audio_case_inputs  # noqa: E402
+from audio_cases import AUDIO_CASES, audio_case_inputs  # noqa: E402
 
 from ldgpu import audio as A  # noqa: E402
 from ldgpu.params import sysparams  # noqa: E402

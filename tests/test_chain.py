@@ -1,0 +1,106 @@
+"""The native field chain (ldg_field_chain) against the host restatement of
+Field.process(): same reads, same validity, same windows, identical
+pulse-level line locations and bad-line flags, field parity and next-field
+offsets, on oracle-demodulated multi-field NTSC and PAL captures read from
+sample 0 (the first reads land mid-field and are invalid, as in the
+reference).  Host code only: runs without a GPU."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from helpers import oracle_capture
+from ldgpu import lib as L
+from ldgpu.fieldread import blocks_in_capture
+from ldgpu.lines import host_field_chain, host_sync_runs, run_chain
+from ldgpu.rfdecode import RFParams
+from ldgpu.synth import synth_capture
+
+NSAMPLES = {"NTSC": 5_200_000, "PAL": 6_000_000}
+
+
+@pytest.fixture(scope="module", params=["NTSC", "PAL"])
+def capture(request):
+    system = request.param
+    rf = RFParams(system=system)
+    rf.delays = {"video_rot": 3}
+    cap = synth_capture(system, NSAMPLES[system], seed=31, start=7777).numpy()
+    nb = blocks_in_capture(rf, len(cap))
+    keys = ("demod", "demod_05", "demod_burst") + (("demod_pilot",) if system == "PAL" else ())
+    arrays = oracle_capture(rf, cap, 0, nb, rf.scaled_mtf(1.0), keys=keys)
+    return rf, arrays, nb
+
+
+def test_chain_matches_host_process(capture, monkeypatch):
+    from ldgpu.linelocs import FieldLogic
+    rf, arrays, nb = capture
+    orig = FieldLogic.compute_linelocs
+
+    def recording(self):
+        rv = orig(self)
+        ll1, err, nxt = rv
+        self._pulse_level = (None if ll1 is None else np.array(ll1, np.float64),
+                             None if err is None else np.array(err), nxt)
+        return rv
+
+    monkeypatch.setattr(FieldLogic, "compute_linelocs", recording)
+    reads, _ = host_field_chain(rf, arrays, nb)
+    runs = host_sync_runs(rf, arrays["demod_05"])
+    plans, stop, st = run_chain(rf, runs, nb)
+    assert stop == L.LDG_CHAIN_STOP_END
+    assert len(plans) == len(reads)
+    nvalid = 0
+    for p, (w, f) in zip(plans, reads):
+        assert (p.startloc, p.length, p.readloc) == (w.startloc, w.length, w.readloc)
+        assert bool(p.valid) == bool(f.valid)
+        if not f.valid:
+            assert p.nextfieldoffset == pytest.approx(f.nextfieldoffset, abs=0)
+            continue
+        nvalid += 1
+        ll1, err, nxt = f._pulse_level
+        bad = f.compute_deriv_error(ll1, err)
+        n = p.proclines
+        np.testing.assert_array_equal(np.frombuffer(p.linelocs1, np.float64)[:n], np.asarray(ll1, np.float64))
+        np.testing.assert_array_equal(np.frombuffer(p.linebad, np.uint8)[:n].astype(bool), bad)
+        assert bool(p.isfirst) == bool(f.isFirstField)
+        assert p.linecount == (263 if f.isFirstField else 262)
+        assert p.nextfieldoffset == nxt
+        assert p.sync_confidence == f.sync_confidence
+    assert nvalid >= 5
+    print(rf.system, "reads", len(plans), "valid", nvalid)
+
+
+def test_chain_resumes_from_state(capture):
+    """Walking in pieces (max_plans) gives the same plans as one walk."""
+    rf, arrays, nb = capture
+    runs = host_sync_runs(rf, arrays["demod_05"])
+    whole, _, _ = run_chain(rf, runs, nb)
+    st = None
+    parts = []
+    while True:
+        plans, stop, st = run_chain(rf, runs, nb, st, max_plans=2)
+        parts.extend(plans)
+        if stop != L.LDG_CHAIN_STOP_FULL:
+            break
+    assert len(parts) == len(whole)
+    for a, b in zip(parts, whole):
+        assert bytes(a) == bytes(b)
+
+
+def test_chain_stops_on_level_recalibration():
+    """No pulses in the very first read: the reference re-levels ire0 from
+    the field's data, so the chain stops there (LDG_CHAIN_STOP_LEVELS)."""
+    rf = RFParams(system="NTSC")
+    z = np.zeros(0, np.int64)
+    plans, stop, _ = run_chain(rf, (z, z, np.zeros(0)), 200)
+    assert stop == L.LDG_CHAIN_STOP_LEVELS and plans == []
+
+
+def test_abi_struct_sizes():
+    h = L.load()
+    for name, t in [("ldg_chain_params", L.ChainParams), ("ldg_chain_state", L.ChainState),
+                    ("ldg_field_plan", L.FieldPlan), ("ldg_lines_consts", L.LinesConsts),
+                    ("ldg_lines_args", L.LinesArgs), ("ldg_tbc_field", L.TbcField),
+                    ("ldg_demod_args", L.DemodArgs), ("ldg_slice", L.Slice)]:
+        assert h.ldg_abi_sizeof(name.encode()) == ctypes.sizeof(t), name

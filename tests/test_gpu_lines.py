@@ -1,0 +1,125 @@
+"""Batched line locations on the B200 (ldgpu.lines.LineLocator) against the
+host restatement of Field.process() run field by field over the same GPU
+demodulator outputs: sync runs identical, the same valid fields and read
+windows, identical field parity / line counts / NTSC field phase IDs, FP64
+line locations equal to within 1e-6 samples, and TBC pictures from either
+set of line locations within 1 LSB.  The resume path (a field decoded on
+the host in the middle of a batch) gives the same results."""
+
+import numpy as np
+import pytest
+
+from ldgpu.fieldread import blocks_in_capture
+from ldgpu.lines import LineLocator, host_field_chain, host_sync_runs
+
+pytestmark = pytest.mark.gpu
+
+NSAMPLES = {"NTSC": 5_200_000, "PAL": 6_000_000}
+
+
+@pytest.fixture(scope="module", params=["NTSC", "PAL"])
+def capture(request, cuda_ok):
+    import torch
+    from ldgpu import RFDecode
+    from ldgpu.synth import synth_capture
+    system = request.param
+    rf = RFDecode(system=system)
+    cap = synth_capture(system, NSAMPLES[system], seed=31, start=7777).numpy()
+    nb = blocks_in_capture(rf, len(cap))
+    U = rf.blocklen - rf.blockcut - rf.blockcut_end
+    keys = ("demod", "demod_05", "demod_burst") + (("demod_pilot",) if system == "PAL" else ())
+    dcap = torch.from_numpy(cap).cuda()
+    arrays = {k: torch.empty(nb * U, dtype=torch.float32, device="cuda") for k in keys}
+    torch.cuda.synchronize()
+    rf.demod_blocks_device(dcap.data_ptr(), nb, U, {k: v.data_ptr() for k, v in arrays.items()}, mtf_level=1)
+    rf.synchronize()
+    host = {k: v.cpu().numpy() for k, v in arrays.items()}
+    reads, _ = host_field_chain(rf, host, nb)
+    yield rf, arrays, host, nb, [(w, f) for w, f in reads if f.valid]
+    rf.close()
+
+
+def _compare(rf, fields, ref):
+    assert len(fields) == len(ref)
+    worst = 0.0
+    for fl, (w, f) in zip(fields, ref):
+        assert (fl.window.startloc, fl.window.length) == (w.startloc, w.length)
+        assert fl.isFirstField == bool(f.isFirstField)
+        assert (fl.linecount, fl.lineoffset) == (f.linecount, f.lineoffset)
+        got = fl.linelocs if fl.linelocs is not None else fl._tensor.cpu().numpy()[:fl.nlines]
+        want = np.asarray(f.linelocs, np.float64)
+        assert got.shape == want.shape
+        d = float(np.abs(got - want).max())
+        worst = max(worst, d)
+        assert d < 1e-6, d
+        if rf.system == "NTSC":
+            assert fl.fieldPhaseID == f.fieldPhaseID
+            assert fl.phase_adjust_median == pytest.approx(float(f.phase_adjust_median), abs=1e-9)
+    return worst
+
+
+def test_sync_runs_match_host(capture):
+    rf, arrays, host, nb, ref = capture
+    loc = LineLocator(rf)
+    s, ln, m = loc.sync_runs(arrays["demod_05"].data_ptr(), arrays["demod_05"].numel())
+    hs, hl, hm = host_sync_runs(rf, host["demod_05"])
+    np.testing.assert_array_equal(s, hs)
+    np.testing.assert_array_equal(ln, hl)
+    np.testing.assert_array_equal(np.isnan(m), np.isnan(hm))
+    ok = ~np.isnan(m)
+    np.testing.assert_allclose(m[ok], hm[ok], rtol=1e-12)
+
+
+def test_batched_linelocs_match_host(capture):
+    rf, arrays, host, nb, ref = capture
+    loc = LineLocator(rf)
+    fields = loc.locate(arrays, nb)
+    assert loc.stats["host"] == 0 and loc.stats["batched"] == len(ref)
+    worst = _compare(rf, fields, ref)
+    print(rf.system, "fields", len(fields), "max |linelocs - host| samples", worst)
+
+
+def test_resume_after_host_field(capture):
+    """Decoding the third read on the host and resuming the batch after it
+    gives the same fields."""
+    rf, arrays, host, nb, ref = capture
+    loc = LineLocator(rf)
+    fields = loc.locate(arrays, nb, force_host={2, 4})
+    assert loc.stats["host"] == 2
+    _compare(rf, fields, ref)
+
+
+def test_tbc_from_batched_linelocs(capture):
+    import torch
+    from ldgpu.field import tbc_descriptor, tbc_fields
+    from ldgpu.linelocs import FieldLogicNTSC
+    rf, arrays, host, nb, ref = capture
+    fields = LineLocator(rf).locate(arrays, nb)
+    outw = rf.SysParams["outlinelen"]
+    outl = rf.SysParams["frame_lines"] // 2 + 1
+    dp = rf.DecoderParams
+    if rf.system == "PAL":
+        out_scale = np.double(0xD300 - 0x0100) / (100 - dp["vsync_ire"])
+    else:
+        out_scale = np.double(0xC800 - 0x0400) / (100 - dp["vsync_ire"])
+    levels = (dp["ire0"], dp["hz_ire"], dp["vsync_ire"], out_scale, rf.SysParams["outputZero"])
+    n = len(fields)
+    a = torch.empty((n, outl * outw), dtype=torch.int16, device="cuda")
+    b = torch.empty((n, outl * outw), dtype=torch.int16, device="cuda")
+    hl = [torch.from_numpy(np.ascontiguousarray(f.linelocs, np.float64)).cuda() for _, f in ref]
+    da, db = [], []
+    for i, (fl, (w, f)) in enumerate(zip(fields, ref)):
+        buf = arrays["demod"].data_ptr() + 4 * w.startloc
+        da.append(tbc_descriptor(rf, buf, fl.linelocs_ptr, fl.lineoffset, outw, outl, outl, levels,
+                                 out_u16=a[i].data_ptr(), buf_len=w.length, nlines=fl.nlines))
+        db.append(tbc_descriptor(rf, buf, hl[i].data_ptr(), f.lineoffset, outw, outl, outl, levels,
+                                 out_u16=b[i].data_ptr(), buf_len=w.length, nlines=len(hl[i])))
+    torch.cuda.synchronize()
+    tbc_fields(rf, da)
+    tbc_fields(rf, db)
+    rf.synchronize()
+    pa = a.cpu().numpy().view(np.uint16).astype(int)
+    pb = b.cpu().numpy().view(np.uint16).astype(int)
+    d = np.abs(pa - pb)
+    print(rf.system, "TBC batched vs host linelocs: max", d.max(), "exact", np.mean(d == 0))
+    assert d.max() <= 1 and np.mean(d == 0) > 0.9999
