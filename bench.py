@@ -5,13 +5,15 @@ Workload (default): an NTSC 10 s capture -- 400 M int16 samples at 40 MSPS
 from the seeded synthetic generator (ldgpu.synth), about 12.6 k overlap-save
 blocks and 600 fields.  One step = every block of the capture through the
 fused demodulator in one launch (all outputs: demod, demod_raw, demod_05,
-demod_burst, rfhpf, EFM, analog audio stage 1) + every field through the
-TBC in one batched launch (uint16 4fsc fields).  Field line locations are
-found before timing by the host Field.process() logic over the GPU outputs.
+demod_burst, rfhpf, EFM, analog audio stage 1), the line locations of every
+field (GPU sync-run scan, native field chain, GPU H-sync / burst / pilot
+refinement) and every field through the TBC in one batched launch (uint16
+4fsc fields).
 
 Prints one JSON line (rank 0).  `--impl reference` times the CPU oracle (a
 numpy restatement of the reference's demodblock + scale_field) on the host
-cores instead, on a bounded sample of the same workload.
+cores instead, on a bounded sample of the same workload; its line locations
+are computed outside its timed steps.
 
 Multi-GPU (torchrun): each rank decodes its own capture (different seed);
 no data-path collective; timing is the max over ranks.
@@ -128,36 +130,6 @@ def dist_env():
     return rank, world, local
 
 
-def field_chain(rf, host, nblocks):
-    """Line locations of every field, following decodefield's read chain
-    (core.py:4030-4097, 4165-4186): host Field.process() over the GPU-demodulated
-    capture-wide arrays (no AGC / MTF redo)."""
-    from ldgpu.field import FieldNTSC, FieldPAL
-    from ldgpu.fieldread import field_window
-    cls = FieldPAL if rf.system == "PAL" else FieldNTSC
-    fields = []
-    start = 0.0
-    prev = None
-    while True:
-        w = field_window(rf, start)
-        if w.first_block + w.nblocks > nblocks:
-            break
-        sl = slice(w.startloc, w.startloc + w.length)
-        dec = {"video": {k: v[sl] for k, v in host.items()}, "startloc": w.startloc}
-        f = cls(rf, dec, prevfield=prev, fields_written=len(fields), readloc=w.startloc)
-        f.process()
-        if not f.valid:
-            start += f.nextfieldoffset
-            prev = None
-            continue
-        fields.append((w, np.ascontiguousarray(f.linelocs, dtype=np.float64), f.lineoffset, f.levels()))
-        start += f.nextfieldoffset - (w.readloc - w.startloc)
-        prev = f
-        if prev is not None:
-            prev.prevfield = None  # keep one field of history, as readfield does
-    return fields
-
-
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -168,9 +140,9 @@ def run_gpu(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     from ldgpu import RFDecode
-    from ldgpu import lib as L
-    from ldgpu.field import tbc_descriptor, tbc_fields
+    from ldgpu.field import tbc_fields
     from ldgpu.fieldread import blocks_in_capture
+    from ldgpu.lines import LineLocator, field_levels, tbc_batch
     from ldgpu.synth import synth_capture
 
     system = args.system
@@ -196,65 +168,76 @@ def run_gpu(args):
     def demod():
         rf.demod_blocks_device(cap.data_ptr(), nblocks, U, ptrs, mtf_level=1, stream=sh)
 
-    demod()
-    torch.cuda.synchronize()
-    # ---- line locations (host, before timing)
-    t0 = time.time()
+    # ---- line locations of every field: GPU sync runs + native field chain + GPU refinement
     fkeys = ["demod", "demod_05", "demod_burst"] + (["demod_pilot"] if system == "PAL" else [])
-    host = {k: outs[k].cpu().numpy() for k in fkeys}
-    fields = field_chain(rf, host, nblocks)
-    t_linelocs = time.time() - t0
-    del host
-    nf = len(fields)
+    farr = {k: outs[k] for k in fkeys}
+    loc = LineLocator(rf)
+    levels = field_levels(rf)
+    host_ms = []
+
+    def linelocs():
+        t = time.perf_counter()
+        fl = loc.locate(farr, nblocks, stream=sh)
+        host_ms.append((time.perf_counter() - t) * 1e3)
+        return fl
+
+    demod()
+    flist = linelocs()
+    torch.cuda.synchronize()
+    nf = len(flist)
     outlinelen = rf.SysParams["outlinelen"]
     outlines = rf.SysParams["frame_lines"] // 2 + 1
     fsz = outlinelen * outlines
     pics = torch.empty(nf * fsz, dtype=torch.uint16, device="cuda")
-    ll_dev = [torch.from_numpy(ll).cuda() for (_, ll, _, _) in fields]
-    descs = (L.TbcField * nf)()
-    for i, (w, ll, lineoffset, levels) in enumerate(fields):
-        descs[i] = tbc_descriptor(rf, outs["demod"].data_ptr() + 4 * w.startloc, ll_dev[i].data_ptr(),
-                                  lineoffset, outlinelen, outlines, outlines, levels,
-                                  out_u16=pics.data_ptr() + 2 * i * fsz, buf_len=w.length,
-                                  nlines=len(ll))
 
-    def tbc():
-        tbc_fields(rf, descs, stream=sh)
+    def tbc(fl):
+        assert len(fl) == nf
+        tbc_fields(rf, tbc_batch(rf, fl, outs["demod"].data_ptr(), pics.data_ptr(), levels), stream=sh)
+
+    def step():
+        demod()
+        tbc(linelocs())
 
     def barrier():
         if world > 1:
             dist.barrier()
 
     for _ in range(args.warmup):
-        demod()
-        tbc()
+        step()
     torch.cuda.synchronize()
+    loc.stats = {k: 0 for k in loc.stats}
+    loc.timing = {}
+    host_ms.clear()
 
-    # ---- timed device-resident steps
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # ---- timed device-resident steps (line locations inside the step)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     clk = Clocks(local)
     barrier()
     torch.cuda.synchronize()
     clk.start()
-    for e0, e1, e2 in ev:
-        e0.record(stream)
+    for e in ev:
+        e[0].record(stream)
         demod()
-        e1.record(stream)
-        tbc()
-        e2.record(stream)
+        e[1].record(stream)
+        fl = linelocs()
+        e[2].record(stream)
+        tbc(fl)
+        e[3].record(stream)
     torch.cuda.synchronize()
     barrier()
     clocks = clk.stop()
-    step_ms = [e0.elapsed_time(e2) for e0, _, e2 in ev]
-    demod_ms = [e0.elapsed_time(e1) for e0, e1, _ in ev]
-    tbc_ms = [e1.elapsed_time(e2) for _, e1, e2 in ev]
+    step_ms = [e[0].elapsed_time(e[3]) for e in ev]
+    demod_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    ll_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    tbc_ms = [e[2].elapsed_time(e[3]) for e in ev]
+    segs = loc.stats["segments"] / args.steps
     total_ms = float(sum(step_ms))
     if world > 1:
         t = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
+    fields = [(f.window, f.host_linelocs(), f.lineoffset, levels) for f in flist]
 
     # ---- end to end: pinned host capture in, fields/efm/audio out
     e2e = None
@@ -270,8 +253,7 @@ def run_gpu(args):
         e0.record(stream)
         for _ in range(args.steps):
             cap.copy_(hcap, non_blocking=True)
-            demod()
-            tbc()
+            step()
             hpics.copy_(pics, non_blocking=True)
             hefm.copy_(outs["efm"], non_blocking=True)
             hal.copy_(outs["audio_left"], non_blocking=True)
@@ -288,7 +270,8 @@ def run_gpu(args):
         d2h = nf * fsz * 2 + nout * 2 + 2 * nblocks * 991 * 4
         e2e = {"value": world * nout / (e2e_ms * 1e-3) / 1e6, "unit": "MSPS", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-               "path": "pinned host capture -> ldg_demod_blocks + ldg_tbc_fields -> host fields, EFM, audio"}
+               "path": "pinned host capture -> ldg_demod_blocks -> ldg_sync_runs + ldg_field_chain + "
+                       "ldg_lines_refine -> ldg_tbc_fields -> host fields, EFM, audio"}
 
     # ---- plain form: one demodblock() call per block through the Python API
     plain = None
@@ -335,13 +318,16 @@ def run_gpu(args):
                         f"{nblocks} blocks x 32768 (stride {U}), {nf} fields per GPU",
             "outputs": "demod, demod_raw, demod_05, demod_burst" + (", demod_pilot" if system == "PAL" else "")
                        + ", rfhpf, efm, audio L/R stage 1, uint16 TBC fields",
-            "linelocs": f"host Field.process over GPU demod outputs before timing ({t_linelocs:.1f} s; not in the step)",
+            "linelocs": "in the step: GPU sync-run scan, native field chain, GPU H-sync/burst/pilot refinement "
+                        f"(FP64); {statistics.median(host_ms):.1f} ms host time per step inside it",
             "l2": "inputs (800 MB) and outputs (> 8 GB) exceed L2 each step; no flush",
             "parallelism": f"replicas x{world} (one capture per GPU)",
             "mtf_level": 1,
         },
         "fields_per_s": world * nf / (ms_per_step * 1e-3),
-        "kernel_ms": {"demod_median": dmed, "tbc_median": statistics.median(tbc_ms)},
+        "kernel_ms": {"demod_median": dmed, "linelocs_median": statistics.median(ll_ms),
+                      "tbc_median": statistics.median(tbc_ms)},
+        "linelocs_host_ms": {k: v / args.steps for k, v in loc.timing.items()},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "ldg::demod_kernel",
@@ -350,7 +336,8 @@ def run_gpu(args):
         "e2e": e2e,
         "plain": plain,
         "cpu_baseline": cpu,
-        "gpu_launches": 3 * args.steps,
+        # per step: demod 1, sync runs 4, refine 3 (NTSC) / 1 (PAL) per segment, TBC 2
+        "gpu_launches": int(args.steps * (1 + 4 + segs * (3 if system == "NTSC" else 1) + 2)),
         "clocks": clocks,
     }
     if rank == 0:
@@ -450,7 +437,8 @@ def run_reference(args):
                                   f"{nft} fields per step (bounded sample of the {args.seconds:g} s workload)",
                       "parallelism": f"{threads} host threads"},
            "cpu_baseline": {"value": v, "unit": "MSPS", "cores": threads, "kind": "port",
-                            "sample": f"{nblk} blocks demod + TBC of {nft} fields per step"},
+                            "sample": f"{nblk} blocks demod + TBC of {nft} fields per step (their line "
+                                      "locations computed once, outside the timed steps)"},
            "e2e": {"value": v, "unit": "MSPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(res), flush=True)
 

@@ -25,7 +25,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <map>
 #include <string>
 #include <vector>
 
@@ -51,11 +50,14 @@ inline bool inrange(double a, double lo, double hi) { return a >= lo && a <= hi;
 // numpy round-half-to-even of a double, as int
 inline long long nround(double x) { return (long long)std::nearbyint(x); }
 
+// np.median: the middle value, or the mean of the two middle values
 double median_of(std::vector<double> v) {
     const size_t n = v.size();
-    std::sort(v.begin(), v.end());
-    if (n % 2) return v[n / 2];
-    return (v[n / 2 - 1] + v[n / 2]) / 2.0;
+    std::nth_element(v.begin(), v.begin() + n / 2, v.end());
+    const double hi = v[n / 2];
+    if (n % 2) return hi;
+    const double lo = *std::max_element(v.begin(), v.begin() + n / 2);
+    return (lo + hi) / 2.0;
 }
 
 struct Timings {
@@ -84,6 +86,7 @@ public:
     Timings get_timings() const {
         const double lo = usectoinpx(P.hsync_pulse_us - 1.75), hi = usectoinpx(P.hsync_pulse_us + 2);
         std::vector<double> hl;
+        hl.reserve(raw.size());
         for (const Pulse& p : raw)
             if (inrange((double)p.len, lo, hi)) hl.push_back((double)p.len);
         const double med = hl.empty() ? P.hsync_pulse_us : median_of(hl);
@@ -173,6 +176,7 @@ public:
     // core.py:1913-1949
     std::vector<VPulse> refinepulses(const Timings& LT) const {
         std::vector<VPulse> valid;
+        valid.reserve(raw.size());
         size_t i = 0;
         while (i < raw.size()) {
             const Pulse& cur = raw[i];
@@ -378,8 +382,11 @@ Slots line_slots(const LdgChainParams& P, const std::vector<VPulse>& vp, const s
         s.nextfield = line0loc - (meanlinelen * 20);
         return s;
     }
-    std::map<long long, long long> ll_dict;
-    std::map<long long, double> ll_dist;
+    // ll_dict / ll_dist over the line slots that reach the output; slots
+    // outside [0, proclines) never influence it and are not kept
+    std::vector<double> linelocs(proclines, -1.0);
+    std::vector<double> ll_dist(proclines, 0.0);
+    std::vector<unsigned char> have(proclines, 0);
     for (const VPulse& p : vp) {
         double lineloc = ((double)p.p.start - line0loc) / meanlinelen;
         long long rlineloc = nround(lineloc);
@@ -394,18 +401,14 @@ Slots line_slots(const LdgChainParams& P, const std::vector<VPulse>& vp, const s
                 dist = dist_end;
             }
         }
-        auto it = ll_dist.find(rlineloc);
-        if (dist > P.hsync_tolerance || (it != ll_dist.end() && dist > it->second)) continue;
+        if (rlineloc < 0 || rlineloc >= proclines) continue;
+        if (dist > P.hsync_tolerance || (have[rlineloc] && dist > ll_dist[rlineloc])) continue;
         if (rlineloc > 0 && !p.good) {
             if (p.type > 0 || (p.type == 0 && rlineloc < 10)) continue;
         }
-        ll_dict[rlineloc] = p.p.start;
+        linelocs[rlineloc] = (double)p.p.start;
         ll_dist[rlineloc] = dist;
-    }
-    std::vector<double> linelocs(proclines);
-    for (int l = 0; l < proclines; ++l) {
-        auto it = ll_dict.find(l);
-        linelocs[l] = it != ll_dict.end() ? (double)it->second : -1.0;
+        have[rlineloc] = 1;
     }
     std::vector<double> filled = linelocs;
     std::vector<unsigned char> err(proclines, 0);
@@ -533,6 +536,7 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
         const long long lo = w.startloc, hi = w.startloc + w.length;
         const int64_t* b = std::upper_bound(run_start, run_start + nruns, (int64_t)lo);
         std::vector<Pulse> raw;
+        raw.reserve(1024);
         std::vector<double> vmeans;
         bool any_long = false;
         for (const int64_t* q = b; q < run_start + nruns && *q < hi; ++q) {

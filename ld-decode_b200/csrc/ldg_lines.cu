@@ -51,6 +51,7 @@ constexpr int kLineThreads = 352;   // >= proclines (326 PAL)
 constexpr int kBurstLines = 266;    // compute_burst_offsets covers lines 0..265
 constexpr int kPilotLines = 323;    // refine_linelocs_pilot covers lines 0..322
 constexpr int kZc = 16;             // clb_findbursts' fixed zero-crossing slots
+constexpr int kBurstThreads = 288;  // >= kBurstLines, whole warps
 
 // ---------------------------------------------------------------- sync runs
 
@@ -295,9 +296,11 @@ struct LineParams {
     int* field14;          // per field
 };
 
+// One line's colour-burst zero crossings as clb_findbursts uses them: the
+// seed-independent part of zc_cycles, (bstart + zcs - s_rem) / zcburstdiv,
+// for all 16 slots (unused slots hold zcs = 0), and the rising flags.
 struct BurstRec {
-    float zcs[kZc];
-    double bstart, s_rem, zcburstdiv;
+    double cyc[kZc];
     int count, rising, valid, pad;
 };
 
@@ -338,10 +341,9 @@ __device__ void burst_record(const LineParams& P, const double* ll, int line, in
     for (int k = 0; k < m; ++k) mx = fmaxf(mx, fabsf(demod[lo + k] - mean_d));
     if ((double)mx > 30 * P.hz_ire) return;
     r.valid = 1;
-    r.bstart = (double)bstart;
-    r.s_rem = s_rem;
-    r.zcburstdiv = (lfreq * fsc_inv) / 2;
-    for (int k = 0; k < kZc; ++k) r.zcs[k] = 0.0f;
+    const double zcburstdiv = (lfreq * fsc_inv) / 2;
+    float zcs[kZc];
+    for (int k = 0; k < kZc; ++k) zcs[k] = 0.0f;
     int c = 0;
     long long j = 0;
     const long long end = m - 1;
@@ -350,7 +352,7 @@ __device__ void burst_record(const LineParams& P, const double* ll, int line, in
             double zc;
             if (!calczc(ba, m, (double)j, 0.0, 0, 16, zc)) break;
             if (ba[j] < 0) r.rising |= 1 << c;
-            r.zcs[c] = (float)zc;
+            zcs[c] = (float)zc;
             ++c;
             j = (long long)zc + 1;
         } else {
@@ -358,6 +360,7 @@ __device__ void burst_record(const LineParams& P, const double* ll, int line, in
         }
     }
     r.count = c;
+    for (int k = 0; k < kZc; ++k) r.cyc[k] = ((double)bstart + (double)zcs[k] - s_rem) / zcburstdiv;
 }
 
 // _angle_mean_phase / phase_distance helpers (core.py:3085-3093)
@@ -516,73 +519,95 @@ __global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P)
     }
 }
 
-// NTSC burst phase chain: fields in order, lines in parallel
-__global__ void __launch_bounds__(512) burst_chain_kernel(LineParams P) {
+// np.median of 16 doubles (mean of the two middle ones), by rank
+__device__ __forceinline__ double median16(const double* v) {
+    double lo = 0, hi = 0;
+#pragma unroll
+    for (int i = 0; i < kZc; ++i) {
+        int r = 0;
+#pragma unroll
+        for (int j = 0; j < kZc; ++j) r += (v[j] < v[i]) || (v[j] == v[i] && j < i);
+        if (r == kZc / 2 - 1) lo = v[i];
+        if (r == kZc / 2) hi = v[i];
+    }
+    return (lo + hi) / 2.0;
+}
+
+// NTSC burst phase chain: fields in order (each seeds its lines' phase from
+// the previous field's median), lines in parallel.  Per field: two passes of
+// clb_findbursts' phase update per line, the field's median by rank and its
+// rising count; two barriers.  The next field's records are loaded while the
+// current one is worked on.
+__global__ void __launch_bounds__(kBurstThreads) burst_chain_kernel(LineParams P) {
     const ldg_lines_args& a = P.a;
-    __shared__ double keys[512];
-    __shared__ int rsum;
-    __shared__ int nadj;
+    __shared__ double keys[kBurstLines];
+    __shared__ double med2[2];
     double prev_pam = a.prev_phase_adjust;
     const int l = threadIdx.x;
+    const bool line = l < kBurstLines;
+    BurstRec cur;
+    cur.valid = 0;
+    if (line && a.nfields > 0) cur = P.rec[l];
     for (int f = 0; f < a.nfields; ++f) {
+        BurstRec nxt;
+        nxt.valid = 0;
+        if (line && f + 1 < a.nfields) nxt = P.rec[(long long)(f + 1) * kBurstLines + l];
         const double prev = a.has_prev[f] ? prev_pam : 0.0;
-        if (l == 0) {
-            rsum = 0;
-            nadj = 0;
-        }
-        __syncthreads();
-        double adj = nan("");
-        if (l < kBurstLines) {
-            const BurstRec& r = P.rec[(long long)f * kBurstLines + l];
-            if (r.valid) {
-                double pa = -prev;
-                int rising_count = 0;
-                for (int pass = 0; pass < 2; ++pass) {
-                    rising_count = 0;
-                    if (r.count) {
-                        double dev[kZc];
-                        int odd = 0;
-                        for (int k = 0; k < kZc; ++k) {
-                            const double cyc = ((r.bstart + (double)r.zcs[k] - r.s_rem) / r.zcburstdiv) + pa;
-                            const int rnd = (int)(cyc + .5);
-                            if (rnd % 2 != 0) odd |= 1 << k;
-                            dev[k] = (double)rnd - cyc;
-                        }
-                        // median of the 16 slots (sorting network by insertion)
-                        for (int x = 1; x < kZc; ++x) {
-                            const double t = dev[x];
-                            int y = x;
-                            while (y > 0 && dev[y - 1] > t) {
-                                dev[y] = dev[y - 1];
-                                --y;
-                            }
-                            dev[y] = t;
-                        }
-                        pa += (dev[kZc / 2 - 1] + dev[kZc / 2]) / 2.0;
-                        rising_count = __popc((unsigned)(r.rising ^ odd) & 0xffffu);
+        double adj = INFINITY;
+        bool ok = false, rising = false;
+        if (line && cur.valid) {
+            double pa = -prev;
+            int rising_count = 0;
+            for (int pass = 0; pass < 2; ++pass) {
+                rising_count = 0;
+                if (cur.count) {
+                    double dev[kZc];
+                    int odd = 0;
+#pragma unroll
+                    for (int k = 0; k < kZc; ++k) {
+                        const double cyc = cur.cyc[k] + pa;
+                        const int rnd = (int)(cyc + .5);
+                        if (rnd % 2 != 0) odd |= 1 << k;
+                        dev[k] = (double)rnd - cyc;
                     }
+                    pa += median16(dev);
+                    rising_count = __popc((unsigned)(cur.rising ^ odd) & 0xffffu);
                 }
-                const bool rising = (double)rising_count > ((double)r.count / 2);
-                adj = (-pa) / 2;
-                if (!(l % 2) && rising) atomicAdd(&rsum, 1);
-                atomicAdd(&nadj, 1);
             }
-            P.adjs[(long long)f * kBurstLines + l] = adj;
+            rising = (double)rising_count > ((double)cur.count / 2);
+            adj = (-pa) / 2;
+            ok = true;
         }
-        keys[l] = (l < kBurstLines && !isnan(adj)) ? adj : INFINITY;
+        if (line) {
+            keys[l] = adj;
+            P.adjs[(long long)f * kBurstLines + l] = ok ? adj : nan("");
+        }
+        const int cnt = __syncthreads_count(ok);
+        const int rsum = __syncthreads_count(ok && !(l % 2) && rising);
+        // rank among the valid values (ties by line): the middle one(s) give the median
+        if (ok) {
+            int r = 0;
+            for (int j = 0; j < kBurstLines; ++j) {
+                const double v = keys[j];
+                r += (v < adj) || (v == adj && j < l);
+            }
+            if (cnt & 1) {
+                if (r == cnt / 2) med2[0] = med2[1] = adj;
+            } else {
+                if (r == cnt / 2 - 1) med2[0] = adj;
+                if (r == cnt / 2) med2[1] = adj;
+            }
+        }
         __syncthreads();
-        bitonic512(keys);
+        // np.median of an empty list is NaN, which the reference then carries forward
+        const double med = cnt ? (med2[0] + med2[1]) / 2.0 : nan("");
+        prev_pam = med * 2;
         if (l == 0) {
-            const int cnt = nadj;
             P.field14[f] = rsum > (cnt / 4);
-            // np.median of an empty list is NaN; the reference then carries NaN forward
-            const double med = cnt ? sorted_median(keys, cnt) : nan("");
-            a.phase_adjust[f] = med * 2;
-            keys[0] = med * 2;
+            a.phase_adjust[f] = prev_pam;
         }
         __syncthreads();
-        prev_pam = keys[0];
-        __syncthreads();
+        cur = nxt;
     }
 }
 
@@ -769,7 +794,7 @@ extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
     cudaStream_t st = (cudaStream_t)a->stream;
     lines_hsync_kernel<<<a->nfields, kLineThreads, 0, st>>>(P);
     if (P.system == 0) {
-        burst_chain_kernel<<<1, 512, 0, st>>>(P);
+        burst_chain_kernel<<<1, kBurstThreads, 0, st>>>(P);
         const double shift = (117.25 / 360) / P.fsc_mhz * P.freq;
         burst_apply_kernel<<<a->nfields, 512, 0, st>>>(P, shift);
     }

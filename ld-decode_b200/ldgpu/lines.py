@@ -26,6 +26,7 @@ arrays (the reference's own order of work).
 
 import ctypes
 import math
+import time
 
 import numpy as np
 
@@ -33,6 +34,25 @@ from . import lib as L
 from .fieldread import field_window, readlen_for
 
 LDG_ERR_RANGE = -5
+
+
+def _dtype_of(struct, formats):
+    """numpy dtype with the exact layout of a ctypes structure."""
+    names = [n for n, _ in struct._fields_]
+    return np.dtype({"names": names, "formats": [formats[n] for n in names],
+                     "offsets": [getattr(struct, n).offset for n in names], "itemsize": ctypes.sizeof(struct)})
+
+
+_ML = L.LDG_CHAIN_MAX_LINES
+PLAN_DTYPE = _dtype_of(L.FieldPlan, {
+    "start": "f8", "readloc": "i8", "first_block": "i8", "nblocks": "i8", "startloc": "i8", "length": "i8",
+    "valid": "i4", "isfirst": "i4", "linecount": "i4", "proclines": "i4", "has_prev": "i4",
+    "sync_confidence": "i4", "nextfieldoffset": "f8", "linelocs1": ("f8", (_ML,)), "linebad": ("u1", (_ML,))})
+TBC_DTYPE = _dtype_of(L.TbcField, {
+    "buf": "u8", "buf_len": "i8", "linelocs": "u8", "nlines": "i4", "lineoffset": "i4", "outwidth": "i4",
+    "linesout": "i4", "outlinecount": "i4", "coord_f32": "i4", "inlinelen": "f8", "outlinelen": "f8",
+    "ire0": "f8", "hz_ire": "f8", "vsync_ire": "f8", "out_scale": "f8", "output_zero": "f8",
+    "out_f32": "u8", "out_u16": "u8"})
 
 
 def proclines_for(rf):
@@ -91,8 +111,10 @@ def sync_threshold(rf):
     return float(rf.iretohz(-20))
 
 
-def run_chain(rf, runs, nblocks, state=None, max_plans=4096):
-    """ldg_field_chain over host run arrays; returns (plans, stop, state)."""
+def run_chain(rf, runs, nblocks, state=None, max_plans=4096, out=None):
+    """ldg_field_chain over host run arrays; returns (plans, stop, state)
+    with plans a numpy record array (PLAN_DTYPE, the ldg_field_plan layout).
+    `out` is an optional reusable PLAN_DTYPE buffer."""
     lib = L.load()
     starts, lens, means = runs
     starts = np.ascontiguousarray(starts, dtype=np.int64)
@@ -101,15 +123,26 @@ def run_chain(rf, runs, nblocks, state=None, max_plans=4096):
     params = chain_params(rf, nblocks)
     st_in = state if state is not None else L.ChainState()
     st_out = L.ChainState()
-    plans = (L.FieldPlan * max_plans)()
+    plans = out if out is not None and len(out) >= max_plans else np.empty(max_plans, PLAN_DTYPE)
     n = ctypes.c_int32(0)
     stop = ctypes.c_int32(0)
     rc = lib.ldg_field_chain(ctypes.byref(params), starts.ctypes.data, lens.ctypes.data, means.ctypes.data,
-                             len(starts), ctypes.byref(st_in), ctypes.byref(st_out), plans, max_plans,
+                             len(starts), ctypes.byref(st_in), ctypes.byref(st_out), plans.ctypes.data, max_plans,
                              ctypes.byref(n), ctypes.byref(stop))
     if rc != 0:
         raise L.LdgError(rc, lib.ldg_chain_last_error().decode())
-    return [plans[i] for i in range(n.value)], stop.value, st_out
+    return plans[:n.value].view(np.recarray), stop.value, st_out
+
+
+def field_levels(rf):
+    """(ire0, hz_ire, vsync_ire, out_scale, outputZero) of Field.hz_to_output
+    (FieldNTSC / FieldPAL out_scale, core.py:3355, 3058)."""
+    dp = rf.DecoderParams
+    if rf.system == "PAL":
+        out_scale = np.double(0xD300 - 0x0100) / (100 - dp["vsync_ire"])
+    else:
+        out_scale = np.double(0xC800 - 0x0400) / (100 - dp["vsync_ire"])
+    return (dp["ire0"], dp["hz_ire"], dp["vsync_ire"], out_scale, rf.SysParams["outputZero"])
 
 
 def host_sync_runs(rf, d05):
@@ -166,17 +199,158 @@ class FieldLines:
     """Line locations of one field of a capture (device or host)."""
 
     def __init__(self, window, isfirst, linecount, lineoffset, linelocs_ptr=None, linelocs=None, nlines=0,
-                 field_phase=None, phase_adjust=None, sync_confidence=100):
+                 field_phase=None, phase_adjust=None, sync_confidence=100, rows=None):
         self.window = window
         self.sync_confidence = int(sync_confidence)
         self.isFirstField = bool(isfirst)
         self.linecount = int(linecount)
         self.lineoffset = int(lineoffset)
-        self.linelocs_ptr = linelocs_ptr   # device pointer (GPU batch) or None
+        self.linelocs_ptr = linelocs_ptr   # device pointer of the FP64 line locations
         self.linelocs = linelocs           # host array (host-decoded fields) or None
         self.nlines = int(nlines)
-        self.fieldPhaseID = field_phase
-        self.phase_adjust_median = phase_adjust
+        self._phase = field_phase          # int, or (device tensor, row)
+        self._pam = phase_adjust           # float, or (device tensor, row)
+        self._rows = rows                  # (device tensor, row) of a batched field
+
+    @staticmethod
+    def _value(v, cast):
+        if isinstance(v, tuple):
+            t, i = v
+            return cast(t[i].item())
+        return None if v is None else cast(v)
+
+    @property
+    def fieldPhaseID(self):
+        return self._value(self._phase, int)
+
+    @property
+    def phase_adjust_median(self):
+        return self._value(self._pam, float)
+
+    def host_linelocs(self):
+        """The line locations as a host float64 array."""
+        if self.linelocs is not None:
+            return self.linelocs
+        t, i = self._rows
+        return t[i].cpu().numpy()[:self.nlines].copy()
+
+
+class LocatedFields:
+    """The valid fields of a capture in read order: as arrays (read window,
+    parity, line counts, device pointers of the line locations) for the
+    batched TBC, and as FieldLines objects by index."""
+
+    def __init__(self, rf):
+        self.rf = rf
+        self._parts = []   # ("batch", plans, ll, pam, fph) | ("host", FieldLines, device tensor)
+        self._cache = None
+
+    def __len__(self):
+        return sum(len(p[1]) if p[0] == "batch" else 1 for p in self._parts)
+
+    def arrays(self):
+        """dict of per-field numpy arrays: startloc, length, readloc, isfirst,
+        linecount, lineoffset, nlines, linelocs_ptr."""
+        if self._cache is not None:
+            return self._cache
+        pal = self.rf.system == "PAL"
+        keys = ("startloc", "length", "readloc", "isfirst", "linecount", "lineoffset", "nlines", "linelocs_ptr")
+        cols = {k: [] for k in keys}
+        for part in self._parts:
+            if part[0] == "batch":
+                _, pl, ll, _, _ = part
+                n = len(pl)
+                isf = pl.isfirst.astype(bool)
+                cols["startloc"].append(pl.startloc)
+                cols["length"].append(pl.length)
+                cols["readloc"].append(pl.readloc)
+                cols["isfirst"].append(isf)
+                if pal:
+                    cols["linecount"].append(np.where(isf, 312, 313))
+                    cols["lineoffset"].append(np.where(isf, 2, 3))
+                else:
+                    cols["linecount"].append(pl.linecount.astype(np.int64))
+                    cols["lineoffset"].append(np.zeros(n, np.int64))
+                cols["nlines"].append(np.full(n, proclines_for(self.rf)))
+                rowb = ll.stride(0) * ll.element_size()
+                cols["linelocs_ptr"].append(np.uint64(ll.data_ptr()) + np.uint64(rowb) * np.arange(n, dtype=np.uint64))
+            else:
+                _, fl, dev = part
+                w = fl.window
+                cols["startloc"].append([w.startloc])
+                cols["length"].append([w.length])
+                cols["readloc"].append([w.readloc])
+                cols["isfirst"].append([fl.isFirstField])
+                cols["linecount"].append([fl.linecount])
+                cols["lineoffset"].append([fl.lineoffset])
+                cols["nlines"].append([fl.nlines])
+                cols["linelocs_ptr"].append(np.array([dev.data_ptr()], np.uint64))
+        self._cache = {k: (np.concatenate([np.asarray(x) for x in v]) if v else np.zeros(0, np.int64))
+                       for k, v in cols.items()}
+        return self._cache
+
+    def __getitem__(self, k):
+        if k < 0:
+            k += len(self)
+        for part in self._parts:
+            if part[0] == "host":
+                if k == 0:
+                    return part[1]
+                k -= 1
+                continue
+            _, pl, ll, pam, fph = part
+            if k < len(pl):
+                from .fieldread import FieldWindow
+                p = pl[k]
+                w = FieldWindow(int(p.readloc), int(p.first_block), int(p.nblocks), int(p.startloc), int(p.length))
+                pal = self.rf.system == "PAL"
+                rowb = ll.stride(0) * ll.element_size()
+                return FieldLines(w, p.isfirst, (312 if p.isfirst else 313) if pal else p.linecount,
+                                  (2 if p.isfirst else 3) if pal else 0, linelocs_ptr=ll.data_ptr() + k * rowb,
+                                  nlines=proclines_for(self.rf), field_phase=None if pal else (fph, k),
+                                  phase_adjust=None if pal else (pam, k), sync_confidence=p.sync_confidence,
+                                  rows=(ll, k))
+            k -= len(pl)
+        raise IndexError("field index out of range")
+
+    def __iter__(self):
+        for k in range(len(self)):
+            yield self[k]
+
+
+def tbc_batch(rf, fields, demod_ptr, out_u16_ptr, levels, coord_f32=False):
+    """ldg_tbc_field descriptors for LocatedFields (or a list of FieldLines):
+    uint16 fields of outlinelen x outlinecount written back to back at
+    out_u16_ptr, built as one numpy record array."""
+    outw = rf.SysParams["outlinelen"]
+    outl = rf.SysParams["frame_lines"] // 2 + 1
+    if isinstance(fields, LocatedFields):
+        a = fields.arrays()
+        startloc, length, ptr, nlines, lineoffset = (a["startloc"], a["length"], a["linelocs_ptr"], a["nlines"],
+                                                     a["lineoffset"])
+    else:
+        startloc = np.array([f.window.startloc for f in fields], np.int64)
+        length = np.array([f.window.length for f in fields], np.int64)
+        ptr = np.array([f.linelocs_ptr if f.linelocs_ptr is not None else f.linelocs.ctypes.data for f in fields],
+                       np.uint64)
+        nlines = np.array([f.nlines for f in fields])
+        lineoffset = np.array([f.lineoffset for f in fields])
+    n = len(startloc)
+    d = np.zeros(n, TBC_DTYPE)
+    d["buf"] = np.uint64(demod_ptr) + np.uint64(4) * startloc.astype(np.uint64)
+    d["buf_len"] = length
+    d["linelocs"] = ptr
+    d["nlines"] = nlines
+    d["lineoffset"] = lineoffset
+    d["outwidth"] = outw
+    d["linesout"] = outl
+    d["outlinecount"] = outl
+    d["coord_f32"] = 1 if coord_f32 else 0
+    d["inlinelen"] = float(rf.linelen)
+    d["outlinelen"] = float(outw)
+    d["ire0"], d["hz_ire"], d["vsync_ire"], d["out_scale"], d["output_zero"] = [float(v) for v in levels]
+    d["out_u16"] = np.uint64(out_u16_ptr) + np.uint64(2 * outw * outl) * np.arange(n, dtype=np.uint64)
+    return (L.TbcField * n).from_buffer_copy(d.tobytes()) if n else (L.TbcField * 0)()
 
 
 class LineLocator:
@@ -188,17 +362,29 @@ class LineLocator:
         self.torch = torch
         self.proclines = proclines_for(rf)
         self.pal = rf.system == "PAL"
-        self._bufs = []
         self.stats = {"batched": 0, "host": 0, "invalid": 0, "segments": 0}
+        self.timing = {}
+        self._plans = np.empty(4096, PLAN_DTYPE)
+        self._runbufs = None
+        self._keep = None
+
+    def _tick(self, key, t0):
+        t = time.perf_counter()
+        self.timing[key] = self.timing.get(key, 0.0) + (t - t0) * 1e3
+        return t
 
     def sync_runs(self, d05_ptr, n, stream=None, cap=None):
         """ldg_sync_runs over a device array; host (starts, lens, means)."""
         lib = L.load()
         rf = self.rf
         cap = int(cap or max(1024, n // 256))
-        starts = np.empty(cap, np.int64)
-        lens = np.empty(cap, np.int64)
-        means = np.empty(cap, np.float64)
+        if self._runbufs is None or len(self._runbufs[0]) < cap:
+            torch = self.torch
+            # pinned host buffers: the copies back run at full PCIe speed
+            self._runbufs = [torch.empty(cap, dtype=torch.int64).pin_memory(),
+                             torch.empty(cap, dtype=torch.int64).pin_memory(),
+                             torch.empty(cap, dtype=torch.float64).pin_memory()]
+        starts, lens, means = (t.numpy() for t in self._runbufs)
         nr = ctypes.c_int64(0)
         minlen = math.floor(10 * rf.samplesperline * rf.linelen)
         rc = lib.ldg_sync_runs(rf._ctx.handle, ctypes.c_void_p(d05_ptr), int(n), sync_threshold(rf), minlen,
@@ -211,26 +397,31 @@ class LineLocator:
         return starts[:k], lens[:k], means[:k]
 
     def _refine(self, arrays, capture_len, plans, prev_pam, stream):
-        """ldg_lines_refine over valid plans; returns device tensors."""
+        """ldg_lines_refine over valid plans (record array); device tensors."""
         torch = self.torch
         lib = L.load()
         nf = len(plans)
         dev = torch.device("cuda", torch.cuda.current_device())
-        maxl = L.LDG_CHAIN_MAX_LINES
-        startloc = torch.tensor([p.startloc for p in plans], dtype=torch.int64)
-        wlen = torch.tensor([p.length for p in plans], dtype=torch.int64)
-        isfirst = torch.tensor([p.isfirst for p in plans], dtype=torch.int32)
-        linecount = torch.tensor([p.linecount for p in plans], dtype=torch.int32)
-        has_prev = torch.tensor([p.has_prev for p in plans], dtype=torch.int32)
-        ll1 = np.empty((nf, maxl), np.float64)
-        bad1 = np.empty((nf, maxl), np.uint8)
-        for i, p in enumerate(plans):
-            ll1[i] = np.frombuffer(p.linelocs1, dtype=np.float64)
-            bad1[i] = np.frombuffer(p.linebad, dtype=np.uint8)
-        host = [startloc, wlen, isfirst, linecount, has_prev, torch.from_numpy(ll1), torch.from_numpy(bad1)]
-        d = [t.to(dev) for t in host]
-        out_ll = torch.empty((nf, maxl), dtype=torch.float64, device=dev)
-        out_bad = torch.empty((nf, maxl), dtype=torch.uint8, device=dev)
+        ml = L.LDG_CHAIN_MAX_LINES
+        # every per-field input in one pinned host block, one copy to the device
+        nb_i = 2 * nf * 8 + 3 * nf * 4
+        nb_i = (nb_i + 7) // 8 * 8
+        total = nb_i + nf * ml * 8 + nf * ml
+        hbuf = torch.empty(total, dtype=torch.uint8).pin_memory()
+        hb = hbuf.numpy()
+        i64 = hb[:2 * nf * 8].view(np.int64).reshape(2, nf)
+        i64[0] = plans.startloc
+        i64[1] = plans.length
+        i32 = hb[2 * nf * 8:2 * nf * 8 + 3 * nf * 4].view(np.int32).reshape(3, nf)
+        i32[0] = plans.isfirst
+        i32[1] = plans.linecount
+        i32[2] = plans.has_prev
+        hb[nb_i:nb_i + nf * ml * 8].view(np.float64).reshape(nf, ml)[:] = plans.linelocs1
+        hb[nb_i + nf * ml * 8:].reshape(nf, ml)[:] = plans.linebad
+        dbuf = hbuf.to(dev, non_blocking=True)
+        base = dbuf.data_ptr()
+        out_ll = torch.empty((nf, ml), dtype=torch.float64, device=dev)
+        out_bad = torch.empty((nf, ml), dtype=torch.uint8, device=dev)
         pam = torch.zeros(nf, dtype=torch.float64, device=dev)
         fph = torch.zeros(nf, dtype=torch.int32, device=dev)
         scratch = torch.empty(max(int(lib.ldg_lines_scratch_bytes(nf)), 256), dtype=torch.uint8, device=dev)
@@ -243,9 +434,13 @@ class LineLocator:
         a.capture_len = int(capture_len)
         a.nfields = nf
         a.proclines = self.proclines
-        a.startloc, a.wlen, a.isfirst, a.linecount, a.has_prev = [t.data_ptr() for t in d[:5]]
-        a.linelocs1 = d[5].data_ptr()
-        a.linebad1 = d[6].data_ptr()
+        a.startloc = base
+        a.wlen = base + nf * 8
+        a.isfirst = base + 2 * nf * 8
+        a.linecount = base + 2 * nf * 8 + nf * 4
+        a.has_prev = base + 2 * nf * 8 + 2 * nf * 4
+        a.linelocs1 = base + nb_i
+        a.linebad1 = base + nb_i + nf * ml * 8
         a.prev_phase_adjust = float(prev_pam)
         a.linelocs = out_ll.data_ptr()
         a.linebad = out_bad.data_ptr()
@@ -254,42 +449,36 @@ class LineLocator:
         a.scratch = scratch.data_ptr()
         a.stream = stream
         L.check(lib.ldg_lines_refine(self.rf._ctx.handle, ctypes.byref(a)))
-        self._bufs.append((d, scratch))
+        # device inputs and scratch return to the caching allocator on the
+        # stream the kernels run on, so any reuse is ordered after them
+        self._keep = (hbuf, dbuf, scratch)
         return out_ll, out_bad, pam, fph
-
-    def _field_lines(self, plan, ptr, fph=None, pam=None):
-        rf = self.rf
-        w = field_window(rf, plan.start)
-        if self.pal:
-            linecount = 312 if plan.isfirst else 313
-            lineoffset = 2 if plan.isfirst else 3
-        else:
-            linecount = plan.linecount
-            lineoffset = 0
-        return FieldLines(w, plan.isfirst, linecount, lineoffset, linelocs_ptr=ptr, nlines=self.proclines,
-                          field_phase=fph, phase_adjust=pam, sync_confidence=plan.sync_confidence)
 
     def locate(self, arrays, nblocks, stream=None, force_host=()):
         """Line locations of every field.  `arrays` maps output names
-        (demod, demod_05, demod_burst[, demod_pilot]) to capture-wide
-        float32 device tensors (one per output, equal lengths).  Returns the
-        FieldLines of the valid fields in read order; `self.stats` counts
-        batched, host-decoded and invalid reads.  `force_host` lists read
-        indices to decode with the host restatement (checks of the resume
-        path)."""
+        (demod, demod_05, demod_burst[, demod_pilot]) to capture-wide float32
+        device tensors of equal length.  Returns a LocatedFields of the
+        valid fields in read order; `self.stats` counts batched,
+        host-decoded and invalid reads and `self.timing` the host time of
+        each phase (ms).  `force_host` lists read indices to decode with the
+        host restatement (checks of the resume path)."""
         rf = self.rf
+        torch = self.torch
         capture_len = int(arrays["demod_05"].numel())
         ptrs = {k: v.data_ptr() for k, v in arrays.items()}
+        t = time.perf_counter()
         runs = self.sync_runs(ptrs["demod_05"], capture_len, stream)
+        t = self._tick("sync_runs", t)
         state = L.ChainState()
         prev_pam = 0.0
         prev_host = None     # host-decoded previous field (FieldLogic) if the last one was
-        last_dev = None      # FieldLines of the last batched field
+        last_dev = None      # index of the last batched field in `out`
         ire0 = float(rf.DecoderParams["ire0"])
-        fields = []
+        out = LocatedFields(rf)
         reads = 0
         while True:
-            plans, stop, st_out = run_chain(rf, runs, nblocks, state)
+            plans, stop, st_out = run_chain(rf, runs, nblocks, state, out=self._plans)
+            t = self._tick("chain", t)
             # a forced host decode cuts the segment at that read index
             cut = None
             for i in range(len(plans)):
@@ -300,28 +489,23 @@ class LineLocator:
                 plans = plans[:cut]
                 stop = L.LDG_CHAIN_STOP_PREV
                 st_out = self._state_after(plans, state)
-            valid = [p for p in plans if p.valid]
+            valid = plans[plans.valid != 0].copy().view(np.recarray)
             self.stats["invalid"] += len(plans) - len(valid)
             reads += len(plans)
-            if valid:
+            if len(valid):
                 self.stats["segments"] += 1
                 self.stats["batched"] += len(valid)
-                if prev_host is not None and valid[0].has_prev and not self.pal:
-                    prev_pam = float(prev_host.phase_adjust_median)
+                if not self.pal and valid.has_prev[0]:
+                    if prev_host is not None:
+                        prev_pam = float(prev_host.phase_adjust_median)
+                    elif last_dev is not None:
+                        prev_pam = float(out[last_dev].phase_adjust_median)
                 ll, bad, pam, fph = self._refine(ptrs, capture_len, valid, prev_pam, stream)
-                pam_h = pam.cpu().numpy() if not self.pal else None
-                fph_h = fph.cpu().numpy() if not self.pal else None
-                for i, p in enumerate(valid):
-                    fl = self._field_lines(p, ll[i].data_ptr(),
-                                           None if self.pal else int(fph_h[i]),
-                                           None if self.pal else float(pam_h[i]))
-                    fl._tensor = ll[i]
-                    fields.append(fl)
-                if not self.pal:
-                    prev_pam = float(pam_h[-1])
-                last_dev = fields[-1]
+                out._parts.append(("batch", valid, ll, pam, fph))
+                last_dev = len(out) - 1
                 prev_host = None
-            if stop in (L.LDG_CHAIN_STOP_END,):
+                t = self._tick("refine", t)
+            if stop == L.LDG_CHAIN_STOP_END:
                 break
             if stop == L.LDG_CHAIN_STOP_FULL:
                 state = st_out
@@ -333,7 +517,11 @@ class LineLocator:
                 break
             prevfield = None
             if state.prev_valid:
-                prevfield = prev_host if prev_host is not None else self._proxy(arrays, last_dev, prev_pam)
+                if prev_host is not None:
+                    prevfield = prev_host
+                else:
+                    fl = out[last_dev]
+                    prevfield = self._proxy(arrays, fl, fl.phase_adjust_median if not self.pal else 0.0)
             f = self._host_field(arrays, w, prevfield, state.fields_written)
             reads += 1
             self.stats["host"] += 1
@@ -342,13 +530,16 @@ class LineLocator:
                 state.start += f.nextfieldoffset
                 state.prev_valid = 0
                 prev_host = None
+                t = self._tick("host_fields", t)
                 continue
             ll_host = np.ascontiguousarray(f.linelocs, dtype=np.float64)
             fl = FieldLines(w, f.isFirstField, f.linecount, f.lineoffset, linelocs=ll_host, nlines=len(ll_host),
                             field_phase=getattr(f, "fieldPhaseID", None),
                             phase_adjust=getattr(f, "phase_adjust_median", None),
                             sync_confidence=f.sync_confidence)
-            fields.append(fl)
+            dev_ll = torch.from_numpy(ll_host).to(torch.device("cuda", torch.cuda.current_device()))
+            fl.linelocs_ptr = dev_ll.data_ptr()
+            out._parts.append(("host", fl, dev_ll))
             state.start += f.nextfieldoffset - (w.readloc - w.startloc)
             state.prev_valid = 1
             state.prev_isfirst = int(bool(f.isFirstField))
@@ -360,7 +551,8 @@ class LineLocator:
             if float(rf.DecoderParams["ire0"]) != ire0:
                 ire0 = float(rf.DecoderParams["ire0"])
                 runs = self.sync_runs(ptrs["demod_05"], capture_len, stream)
-        return fields
+            t = self._tick("host_fields", t)
+        return out
 
     def _state_after(self, plans, state):
         """Chain state after the given plans (for a forced cut)."""
@@ -401,7 +593,7 @@ class LineLocator:
         dec = {"video": self._window_host(arrays, fl.window, ("demod",)), "startloc": fl.window.startloc}
         p = cls(self.rf, dec)
         p.valid = True
-        p.linelocs = fl._tensor.cpu().numpy()[:fl.nlines].copy()
+        p.linelocs = fl.host_linelocs()
         p.linecount = fl.linecount
         p.lineoffset = fl.lineoffset
         p.isFirstField = fl.isFirstField
@@ -412,4 +604,3 @@ class LineLocator:
         # determine_field_number seeds from (field phase ID metadata only)
         p.phase_adjust = {l: None for l in range(7, 22, 4)}
         return p
-

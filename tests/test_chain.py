@@ -85,7 +85,7 @@ def test_chain_resumes_from_state(capture):
             break
     assert len(parts) == len(whole)
     for a, b in zip(parts, whole):
-        assert bytes(a) == bytes(b)
+        assert a.tobytes() == b.tobytes()
 
 
 def test_chain_stops_on_level_recalibration():
@@ -94,7 +94,7 @@ def test_chain_stops_on_level_recalibration():
     rf = RFParams(system="NTSC")
     z = np.zeros(0, np.int64)
     plans, stop, _ = run_chain(rf, (z, z, np.zeros(0)), 200)
-    assert stop == L.LDG_CHAIN_STOP_LEVELS and plans == []
+    assert stop == L.LDG_CHAIN_STOP_LEVELS and len(plans) == 0
 
 
 def test_abi_struct_sizes():

@@ -46,7 +46,7 @@ def _compare(rf, fields, ref):
         assert (fl.window.startloc, fl.window.length) == (w.startloc, w.length)
         assert fl.isFirstField == bool(f.isFirstField)
         assert (fl.linecount, fl.lineoffset) == (f.linecount, f.lineoffset)
-        got = fl.linelocs if fl.linelocs is not None else fl._tensor.cpu().numpy()[:fl.nlines]
+        got = fl.host_linelocs()
         want = np.asarray(f.linelocs, np.float64)
         assert got.shape == want.shape
         d = float(np.abs(got - want).max())
@@ -90,32 +90,27 @@ def test_resume_after_host_field(capture):
 
 
 def test_tbc_from_batched_linelocs(capture):
+    """TBC through tbc_batch over the batched line locations equals TBC with
+    the host line locations."""
     import torch
     from ldgpu.field import tbc_descriptor, tbc_fields
-    from ldgpu.linelocs import FieldLogicNTSC
+    from ldgpu.lines import field_levels, tbc_batch
     rf, arrays, host, nb, ref = capture
     fields = LineLocator(rf).locate(arrays, nb)
     outw = rf.SysParams["outlinelen"]
     outl = rf.SysParams["frame_lines"] // 2 + 1
-    dp = rf.DecoderParams
-    if rf.system == "PAL":
-        out_scale = np.double(0xD300 - 0x0100) / (100 - dp["vsync_ire"])
-    else:
-        out_scale = np.double(0xC800 - 0x0400) / (100 - dp["vsync_ire"])
-    levels = (dp["ire0"], dp["hz_ire"], dp["vsync_ire"], out_scale, rf.SysParams["outputZero"])
+    levels = field_levels(rf)
     n = len(fields)
     a = torch.empty((n, outl * outw), dtype=torch.int16, device="cuda")
     b = torch.empty((n, outl * outw), dtype=torch.int16, device="cuda")
     hl = [torch.from_numpy(np.ascontiguousarray(f.linelocs, np.float64)).cuda() for _, f in ref]
-    da, db = [], []
-    for i, (fl, (w, f)) in enumerate(zip(fields, ref)):
+    db = []
+    for i, (w, f) in enumerate(ref):
         buf = arrays["demod"].data_ptr() + 4 * w.startloc
-        da.append(tbc_descriptor(rf, buf, fl.linelocs_ptr, fl.lineoffset, outw, outl, outl, levels,
-                                 out_u16=a[i].data_ptr(), buf_len=w.length, nlines=fl.nlines))
         db.append(tbc_descriptor(rf, buf, hl[i].data_ptr(), f.lineoffset, outw, outl, outl, levels,
                                  out_u16=b[i].data_ptr(), buf_len=w.length, nlines=len(hl[i])))
     torch.cuda.synchronize()
-    tbc_fields(rf, da)
+    tbc_fields(rf, tbc_batch(rf, fields, arrays["demod"].data_ptr(), a.data_ptr(), levels))
     tbc_fields(rf, db)
     rf.synchronize()
     pa = a.cpu().numpy().view(np.uint16).astype(int)
