@@ -238,6 +238,12 @@ def run_gpu(args):
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
     fields = [(f.window, f.host_linelocs(), f.lineoffset, levels) for f in flist]
+    # the threaded field chain against one sequential walk over the same runs (untimed)
+    from ldgpu.lines import parallel_chain, run_chain
+    runs = [a.copy() for a in loc.sync_runs(farr["demod_05"].data_ptr(), nout, sh)]
+    p_plans, _, _ = parallel_chain(rf, runs, nblocks, None, loc.threads, loc._pool)
+    s_plans, _, _ = run_chain(rf, runs, nblocks, None, max_plans=8192)
+    chain_check = bool(p_plans.tobytes() == s_plans.tobytes())
 
     # ---- end to end: pinned host capture in, fields/efm/audio out
     e2e = None
@@ -328,6 +334,8 @@ def run_gpu(args):
         "kernel_ms": {"demod_median": dmed, "linelocs_median": statistics.median(ll_ms),
                       "tbc_median": statistics.median(tbc_ms)},
         "linelocs_host_ms": {k: v / args.steps for k, v in loc.timing.items()},
+        "linelocs_chain": {"threads": loc.threads, "equals_sequential_walk": chain_check,
+                           "segments": segs, "host_decoded": loc.stats["host"] / args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "ldg::demod_kernel",

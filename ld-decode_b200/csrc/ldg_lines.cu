@@ -519,31 +519,89 @@ __global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P)
     }
 }
 
-// np.median of 16 doubles (mean of the two middle ones), by rank
-__device__ __forceinline__ double median16(const double* v) {
-    double lo = 0, hi = 0;
-#pragma unroll
-    for (int i = 0; i < kZc; ++i) {
-        int r = 0;
-#pragma unroll
-        for (int j = 0; j < kZc; ++j) r += (v[j] < v[i]) || (v[j] == v[i] && j < i);
-        if (r == kZc / 2 - 1) lo = v[i];
-        if (r == kZc / 2) hi = v[i];
+// np.median of 16 doubles (mean of the two middle ones): Batcher's
+// odd-even merge sort network (63 compare-exchanges, the values stay in
+// registers)
+#define LDG_CS(a, b)                 \
+    {                                \
+        const double x_ = v[a];      \
+        const double y_ = v[b];      \
+        if (x_ > y_) {               \
+            v[a] = y_;               \
+            v[b] = x_;               \
+        }                            \
     }
-    return (lo + hi) / 2.0;
+__device__ __forceinline__ double median16(double* v) {
+    LDG_CS(0, 1) LDG_CS(2, 3) LDG_CS(4, 5) LDG_CS(6, 7)
+    LDG_CS(8, 9) LDG_CS(10, 11) LDG_CS(12, 13) LDG_CS(14, 15)
+    LDG_CS(0, 2) LDG_CS(1, 3) LDG_CS(4, 6) LDG_CS(5, 7)
+    LDG_CS(8, 10) LDG_CS(9, 11) LDG_CS(12, 14) LDG_CS(13, 15)
+    LDG_CS(1, 2) LDG_CS(5, 6) LDG_CS(9, 10) LDG_CS(13, 14)
+    LDG_CS(0, 4) LDG_CS(1, 5) LDG_CS(2, 6) LDG_CS(3, 7)
+    LDG_CS(8, 12) LDG_CS(9, 13) LDG_CS(10, 14) LDG_CS(11, 15)
+    LDG_CS(2, 4) LDG_CS(3, 5) LDG_CS(10, 12) LDG_CS(11, 13)
+    LDG_CS(1, 2) LDG_CS(3, 4) LDG_CS(5, 6) LDG_CS(9, 10)
+    LDG_CS(11, 12) LDG_CS(13, 14) LDG_CS(0, 8) LDG_CS(1, 9)
+    LDG_CS(2, 10) LDG_CS(3, 11) LDG_CS(4, 12) LDG_CS(5, 13)
+    LDG_CS(6, 14) LDG_CS(7, 15) LDG_CS(4, 8) LDG_CS(5, 9)
+    LDG_CS(6, 10) LDG_CS(7, 11) LDG_CS(2, 4) LDG_CS(3, 5)
+    LDG_CS(6, 8) LDG_CS(7, 9) LDG_CS(10, 12) LDG_CS(11, 13)
+    LDG_CS(1, 2) LDG_CS(3, 4) LDG_CS(5, 6) LDG_CS(7, 8)
+    LDG_CS(9, 10) LDG_CS(11, 12) LDG_CS(13, 14)
+    return (v[kZc / 2 - 1] + v[kZc / 2]) / 2.0;
+}
+#undef LDG_CS
+
+// (key, index) pairs in a strict total order
+__device__ __forceinline__ bool pair_less(double ka, int ia, double kb, int ib) {
+    return ka < kb || (ka == kb && ia < ib);
+}
+
+// ascending bitonic sort of one (key, index) pair per lane across a warp
+__device__ __forceinline__ void warp_sort_pairs(double& key, int& idx) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const double ok = __shfl_xor_sync(0xffffffffu, key, j);
+            const int oi = __shfl_xor_sync(0xffffffffu, idx, j);
+            const bool up = (lane & k) == 0;
+            const bool lower = (lane & j) == 0;
+            const bool partner_less = pair_less(ok, oi, key, idx);
+            // ascending block: the lower lane keeps the smaller pair
+            const bool take = lower == up ? partner_less : !partner_less;
+            if (take) {
+                key = ok;
+                idx = oi;
+            }
+        }
+    }
+}
+
+// number of pairs in a sorted run of 32 that order before (key, idx)
+__device__ __forceinline__ int run_rank(const double* rk, const int* ri, double key, int idx) {
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1)
+        if (pair_less(rk[lo + step - 1], ri[lo + step - 1], key, idx)) lo += step;
+    return lo + (pair_less(rk[lo], ri[lo], key, idx) ? 1 : 0);
 }
 
 // NTSC burst phase chain: fields in order (each seeds its lines' phase from
 // the previous field's median), lines in parallel.  Per field: two passes of
-// clb_findbursts' phase update per line, the field's median by rank and its
-// rising count; two barriers.  The next field's records are loaded while the
-// current one is worked on.
+// clb_findbursts' phase update per line; the field's median from per-warp
+// sorted runs (a value's rank is the sum of its positions in the runs); its
+// rising count.  The next field's records load while the current one is
+// worked on.
 __global__ void __launch_bounds__(kBurstThreads) burst_chain_kernel(LineParams P) {
+    constexpr int kWarps = kBurstThreads / 32;
     const ldg_lines_args& a = P.a;
-    __shared__ double keys[kBurstLines];
+    __shared__ double rkey[kWarps][32];
+    __shared__ int ridx[kWarps][32];
     __shared__ double med2[2];
     double prev_pam = a.prev_phase_adjust;
-    const int l = threadIdx.x;
+    const int l = threadIdx.x, lane = l & 31, warp = l >> 5;
     const bool line = l < kBurstLines;
     BurstRec cur;
     cur.valid = 0;
@@ -578,19 +636,18 @@ __global__ void __launch_bounds__(kBurstThreads) burst_chain_kernel(LineParams P
             adj = (-pa) / 2;
             ok = true;
         }
-        if (line) {
-            keys[l] = adj;
-            P.adjs[(long long)f * kBurstLines + l] = ok ? adj : nan("");
-        }
+        if (line) P.adjs[(long long)f * kBurstLines + l] = ok ? adj : nan("");
+        double sk = adj;
+        int si = l;
+        warp_sort_pairs(sk, si);
+        rkey[warp][lane] = sk;
+        ridx[warp][lane] = si;
         const int cnt = __syncthreads_count(ok);
         const int rsum = __syncthreads_count(ok && !(l % 2) && rising);
-        // rank among the valid values (ties by line): the middle one(s) give the median
         if (ok) {
             int r = 0;
-            for (int j = 0; j < kBurstLines; ++j) {
-                const double v = keys[j];
-                r += (v < adj) || (v == adj && j < l);
-            }
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) r += run_rank(rkey[w], ridx[w], adj, l);
             if (cnt & 1) {
                 if (r == cnt / 2) med2[0] = med2[1] = adj;
             } else {

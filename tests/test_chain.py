@@ -104,3 +104,16 @@ def test_abi_struct_sizes():
                     ("ldg_lines_args", L.LinesArgs), ("ldg_tbc_field", L.TbcField),
                     ("ldg_demod_args", L.DemodArgs), ("ldg_slice", L.Slice)]:
         assert h.ldg_abi_sizeof(name.encode()) == ctypes.sizeof(t), name
+
+
+def test_parallel_chain_equals_serial(capture):
+    """The chain walked in pieces joined at common states equals one walk."""
+    from ldgpu.lines import parallel_chain
+    rf, arrays, nb = capture
+    runs = host_sync_runs(rf, arrays["demod_05"])
+    whole, stop, st = run_chain(rf, runs, nb)
+    for nthreads in (2, 3):
+        got, stop2, st2 = parallel_chain(rf, runs, nb, None, nthreads, margin_blocks=100, min_seg_blocks=30)
+        assert stop2 == stop and st2.start == st.start
+        assert len(got) == len(whole)
+        assert got.tobytes() == whole.tobytes()
