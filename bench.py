@@ -241,7 +241,7 @@ def run_gpu(args):
     # the threaded field chain against one sequential walk over the same runs (untimed)
     from ldgpu.lines import parallel_chain, run_chain
     runs = [a.copy() for a in loc.sync_runs(farr["demod_05"].data_ptr(), nout, sh)]
-    p_plans, _, _ = parallel_chain(rf, runs, nblocks, None, loc.threads, loc._pool)
+    p_plans, _, _ = parallel_chain(rf, runs, nblocks, None, loc.threads, max_plans=8192)
     s_plans, _, _ = run_chain(rf, runs, nblocks, None, max_plans=8192)
     chain_check = bool(p_plans.tobytes() == s_plans.tobytes())
 

@@ -294,6 +294,20 @@ int ldg_field_chain(const ldg_chain_params* params, const int64_t* run_start, co
                     int32_t* stop);
 const char* ldg_chain_last_error(void);
 
+/* ldg_field_chain in `nthreads` pieces on host threads.  The read chain
+ * locks onto the signal (a field read is placed from the next vertical
+ * blanking interval on, whatever came before), so piece t > 0 starts from
+ * a guessed position at its first block and the previous piece, which runs
+ * margin_blocks past its end, is joined to it at the first chain state both
+ * reached (same read position and previous-field flags); the joined plans
+ * are re-walked from the true state.  The result equals ldg_field_chain's;
+ * where no common state is found the rest is walked sequentially.  Pieces
+ * shorter than min_seg_blocks: sequential. */
+int ldg_field_chain_mt(const ldg_chain_params* params, const int64_t* run_start, const int64_t* run_len,
+                       const double* run_mean, int64_t nruns, const ldg_chain_state* state_in,
+                       ldg_chain_state* state_out, ldg_field_plan* plans, int32_t max_plans, int32_t* nplans,
+                       int32_t* stop, int32_t nthreads, int64_t margin_blocks, int64_t min_seg_blocks);
+
 typedef struct ldg_lines_consts {
     int32_t system;             /* 0 NTSC, 1 PAL */
     int32_t pad;

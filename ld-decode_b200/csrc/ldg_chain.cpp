@@ -729,3 +729,195 @@ extern "C" int64_t ldg_abi_sizeof(const char* name) {
     if (n == "ldg_slice") return sizeof(ldg_slice);
     return -1;
 }
+
+// ---- the chain in pieces on host threads
+
+#include <thread>
+
+namespace {
+
+struct Key {
+    long long readloc;
+    int prev_valid, prev_isfirst;
+    bool written;
+    bool operator==(const Key& o) const {
+        return readloc == o.readloc && prev_valid == o.prev_valid && prev_isfirst == o.prev_isfirst &&
+               written == o.written;
+    }
+};
+
+long long readloc_of(const LdgChainParams& P, double start) { return std::max((long long)(start - P.blockcut), 0LL); }
+
+Key key_of(const LdgChainParams& P, const LdgChainState& s) {
+    return {readloc_of(P, s.start), s.prev_valid, s.prev_valid ? s.prev_isfirst : 0, s.fields_written > 0};
+}
+
+// the chain state after a plan, as ldg_field_chain advances it
+LdgChainState advance(const LdgChainState& s, const LdgFieldPlan& p) {
+    LdgChainState n = s;
+    if (p.valid) {
+        n.start += p.nextfieldoffset - (double)(p.readloc - p.startloc);
+        n.prev_valid = 1;
+        n.prev_isfirst = p.isfirst;
+        n.prev_startloc = p.startloc;
+        n.fields_written += 1;
+    } else {
+        n.start += p.nextfieldoffset;
+        n.prev_valid = 0;
+    }
+    return n;
+}
+
+struct Piece {
+    std::vector<LdgFieldPlan> plans;
+    LdgChainState in{}, out{};
+    int32_t stop = 0;
+    int rc = 0;
+};
+
+void run_piece(const LdgChainParams& P, int64_t limit, const int64_t* rs, const int64_t* rl, const double* rm,
+               int64_t nruns, int32_t cap, Piece& pc) {
+    LdgChainParams q = P;
+    q.nblocks = limit;
+    pc.plans.resize(cap);
+    int32_t n = 0;
+    pc.rc = ldg_field_chain(&q, rs, rl, rm, nruns, &pc.in, &pc.out, pc.plans.data(), cap, &n, &pc.stop);
+    pc.plans.resize(pc.rc == 0 ? n : 0);
+}
+
+}  // namespace
+
+extern "C" int ldg_field_chain_mt(const LdgChainParams* P, const int64_t* run_start, const int64_t* run_len,
+                                  const double* run_mean, int64_t nruns, const LdgChainState* state_in,
+                                  LdgChainState* state_out, LdgFieldPlan* plans, int32_t max_plans,
+                                  int32_t* nplans, int32_t* stop, int32_t nthreads, int64_t margin_blocks,
+                                  int64_t min_seg_blocks) {
+    if (!P || !state_in || !state_out || !plans || !nplans || !stop) {
+        g_chain_err = "ldg_field_chain_mt: NULL argument";
+        return -1;
+    }
+    const long long U = P->blocklen - P->blockcut - P->blockcut_end;
+    const long long b0 = std::max((long long)state_in->start / U, 0LL);
+    const long long seg = nthreads > 0 ? (P->nblocks - b0) / nthreads : 0;
+    if (nthreads <= 1 || seg < min_seg_blocks || U <= 0)
+        return ldg_field_chain(P, run_start, run_len, run_mean, nruns, state_in, state_out, plans, max_plans, nplans,
+                               stop);
+    std::vector<Piece> pcs(nthreads);
+    std::vector<int64_t> limit(nthreads);
+    for (int t = 0; t < nthreads; ++t) {
+        if (t == 0) {
+            pcs[t].in = *state_in;
+        } else {
+            pcs[t].in.start = (double)((b0 + t * seg) * U);
+            pcs[t].in.fields_written = state_in->fields_written + 1;
+        }
+        limit[t] = t == nthreads - 1 ? P->nblocks : std::min<long long>(P->nblocks, b0 + (t + 1) * seg + margin_blocks);
+    }
+    {
+        std::vector<std::thread> th;
+        // a field read advances at least ~10 blocks; a piece that fills its
+        // buffer stops (LDG_CHAIN_STOP_FULL) and the caller resumes
+        auto cap = [&](int t) {
+            const long long first = t == 0 ? b0 : b0 + t * seg;
+            return (int32_t)std::min<long long>(max_plans, (limit[t] - first) / 8 + 16);
+        };
+        for (int t = 1; t < nthreads; ++t)
+            th.emplace_back(run_piece, std::cref(*P), limit[t], run_start, run_len, run_mean, nruns, cap(t),
+                            std::ref(pcs[t]));
+        run_piece(*P, limit[0], run_start, run_len, run_mean, nruns, cap(0), pcs[0]);
+        for (auto& x : th) x.join();
+    }
+    for (const Piece& pc : pcs)
+        if (pc.rc != 0) return pc.rc;
+    // join the pieces: merged plans with the state before each of them
+    std::vector<LdgFieldPlan> merged = std::move(pcs[0].plans);
+    std::vector<LdgChainState> before;
+    {
+        LdgChainState s = pcs[0].in;
+        for (const LdgFieldPlan& p : merged) {
+            before.push_back(s);
+            s = advance(s, p);
+        }
+    }
+    int32_t stp = pcs[0].stop;
+    LdgChainState st_end = pcs[0].out;
+    bool serial_rest = false;
+    for (int t = 1; t < nthreads && stp == LDG_CHAIN_STOP_END; ++t) {
+        Piece& pc = pcs[t];
+        if (pc.plans.empty()) {
+            serial_rest = true;
+            break;
+        }
+        std::vector<Key> tk;
+        {
+            LdgChainState s = pc.in;
+            for (const LdgFieldPlan& p : pc.plans) {
+                tk.push_back(key_of(*P, s));
+                s = advance(s, p);
+            }
+        }
+        const long long lo = pc.plans[0].readloc;
+        int ji = -1, jj = -1;
+        for (size_t i = 0; i < before.size() && ji < 0; ++i) {
+            const Key k = key_of(*P, before[i]);
+            if (k.readloc < lo) continue;
+            for (size_t j = 0; j < tk.size(); ++j)
+                if (tk[j] == k) {
+                    ji = (int)i;
+                    jj = (int)j;
+                    break;
+                }
+        }
+        if (ji < 0) {
+            serial_rest = true;
+            break;
+        }
+        // re-walk the piece's plans from the true state; the fraction of a
+        // sample in `start` differs, the read windows must not
+        merged.resize(ji);
+        before.resize(ji);
+        LdgChainState s = ji ? advance(before.back(), merged.back()) : pcs[0].in;
+        bool moved = false;
+        for (size_t j = jj; j < pc.plans.size(); ++j) {
+            LdgFieldPlan p = pc.plans[j];
+            if (readloc_of(*P, s.start) != p.readloc) {
+                moved = true;
+                break;
+            }
+            p.start = s.start;
+            merged.push_back(p);
+            before.push_back(s);
+            s = advance(s, p);
+        }
+        st_end = s;
+        stp = pc.stop;
+        if (moved) {
+            serial_rest = true;
+            break;
+        }
+    }
+    if (serial_rest) {
+        std::vector<LdgFieldPlan> rest(std::max<int64_t>(max_plans - (int64_t)merged.size(), 1));
+        int32_t n = 0, sp = 0;
+        LdgChainState so{};
+        const int rc = ldg_field_chain(P, run_start, run_len, run_mean, nruns, &st_end, &so, rest.data(),
+                                       (int32_t)rest.size(), &n, &sp);
+        if (rc != 0) return rc;
+        merged.insert(merged.end(), rest.begin(), rest.begin() + n);
+        st_end = so;
+        stp = sp;
+    }
+    if ((int64_t)merged.size() > max_plans) {
+        // the caller's buffer is full: stop where it ends
+        LdgChainState s = pcs[0].in;
+        for (int32_t k = 0; k < max_plans; ++k) s = advance(s, merged[k]);
+        merged.resize(max_plans);
+        st_end = s;
+        stp = LDG_CHAIN_STOP_FULL;
+    }
+    std::copy(merged.begin(), merged.end(), plans);
+    *nplans = (int32_t)merged.size();
+    *state_out = st_end;
+    *stop = stp;
+    return 0;
+}

@@ -122,6 +122,9 @@ SIGNATURES = {
                                        ctypes.POINTER(ChainState), ctypes.POINTER(ChainState), c_p, c_i32,
                                        ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)]),
     "ldg_chain_last_error": (ctypes.c_char_p, []),
+    "ldg_field_chain_mt": (ctypes.c_int, [ctypes.POINTER(ChainParams), c_p, c_p, c_p, c_i64,
+                                          ctypes.POINTER(ChainState), ctypes.POINTER(ChainState), c_p, c_i32,
+                                          ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_i32, c_i64, c_i64]),
     "ldg_lines_scratch_bytes": (c_i64, [c_i32]),
     "ldg_abi_sizeof": (c_i64, [ctypes.c_char_p]),
     "ldg_lines_refine": (ctypes.c_int, [c_p, ctypes.POINTER(LinesArgs)]),

@@ -134,129 +134,30 @@ def run_chain(rf, runs, nblocks, state=None, max_plans=4096, out=None):
     return plans[:n.value].view(np.recarray), stop.value, st_out
 
 
-def _readloc(rf, start):
-    return max(int(start - rf.blockcut), 0)
-
-
-def _entry_keys(rf, plans, state):
-    """Key of the chain state before each plan: (read position, previous
-    field valid, its parity if valid, any field written).  Two states with
-    the same key read the same window and give the same plan apart from its
-    `start` value, whose fraction below one sample only rides along."""
-    out = []
-    start, pv, pf, fw = state.start, state.prev_valid, state.prev_isfirst, state.fields_written
-    for p in plans:
-        out.append((_readloc(rf, start), int(pv), int(pf) if pv else 0, fw > 0))
-        if p.valid:
-            start = start + p.nextfieldoffset - (p.readloc - p.startloc)
-            pv, pf, fw = 1, int(p.isfirst), fw + 1
-        else:
-            start = start + p.nextfieldoffset
-            pv = 0
-    return out
-
-
-def _retime(rf, plans, state):
-    """Walk `plans` from `state` as the chain does, rewriting each plan's
-    start; returns how many plans keep their read window and the state after
-    them."""
-    st = L.ChainState()
-    ctypes.memmove(ctypes.byref(st), ctypes.byref(state), ctypes.sizeof(st))
-    for k in range(len(plans)):
-        p = plans[k]
-        if _readloc(rf, st.start) != p.readloc:
-            return k, st
-        p.start = st.start
-        if p.valid:
-            st.start += p.nextfieldoffset - (p.readloc - p.startloc)
-            st.prev_valid = 1
-            st.prev_isfirst = p.isfirst
-            st.prev_startloc = p.startloc
-            st.fields_written += 1
-        else:
-            st.start += p.nextfieldoffset
-            st.prev_valid = 0
-    return len(plans), st
-
-
-def parallel_chain(rf, runs, nblocks, state=None, nthreads=8, pool=None, margin_blocks=None,
+def parallel_chain(rf, runs, nblocks, state=None, nthreads=8, max_plans=4096, out=None, margin_blocks=None,
                    min_seg_blocks=None):
-    """ldg_field_chain over a capture in `nthreads` pieces at once.
-
-    The read chain is sequential (each field's read position comes from the
-    previous field), but it locks onto the signal: from any start, the
-    following field is read from the next vertical blanking interval on,
-    whatever came before.  So piece t > 0 starts from a guessed position at
-    its first block; the previous piece runs on past its end until it
-    reaches a chain state that piece t also reached (same read position and
-    previous-field flags), and the two are joined there.  The joined plans
-    are re-walked from the true state, so they equal a single walk; where
-    no common state is found, or a re-walked read position moves, the walk
-    goes on sequentially from there.  Returns (plans, stop, state) like
-    run_chain."""
-    import concurrent.futures as cf
+    """ldg_field_chain_mt: the chain in `nthreads` pieces on host threads,
+    joined at common chain states (equal to one walk).  Margin and minimum
+    piece default to 5 fields + one read window and 6 fields of blocks."""
+    lib = L.load()
     U = rf.blocklen - rf.blockcut - rf.blockcut_end
-    state = state if state is not None else L.ChainState()
     field_blocks = int(rf.freq_hz / rf.SysParams["FPS"] / 2 / U) + 1
-    window_blocks = field_window(rf, 0.0).nblocks
-    margin = margin_blocks if margin_blocks is not None else 5 * field_blocks + window_blocks
+    margin = margin_blocks if margin_blocks is not None else 5 * field_blocks + field_window(rf, 0.0).nblocks
     min_seg = min_seg_blocks if min_seg_blocks is not None else 6 * field_blocks
-    b0 = max(int(state.start) // U, 0)
-    seg = (nblocks - b0) // max(nthreads, 1)
-    if nthreads <= 1 or seg < min_seg:
-        return run_chain(rf, runs, nblocks, state)
-    jobs = []
-    for t in range(nthreads):
-        if t == 0:
-            st = state
-        else:
-            st = L.ChainState()
-            st.start = float((b0 + t * seg) * U)
-            st.fields_written = state.fields_written + 1
-        limit = nblocks if t == nthreads - 1 else min(nblocks, b0 + (t + 1) * seg + margin)
-        jobs.append((st, limit))
-
-    def work(job):
-        st, limit = job
-        plans, stop, so = run_chain(rf, runs, limit, st, max_plans=8192)
-        return plans.copy().view(np.recarray), stop, so, st
-
-    if pool is not None:
-        results = list(pool.map(work, jobs))
-    else:
-        with cf.ThreadPoolExecutor(nthreads) as ex:
-            results = list(ex.map(work, jobs))
-    merged, stop, st_out, st0 = results[0]
-    keys = _entry_keys(rf, merged, st0)
-
-    def serial_rest(merged, st):
-        rest, stop, st_out = run_chain(rf, runs, nblocks, st, max_plans=8192)
-        return np.concatenate([merged, rest]).view(np.recarray), stop, st_out
-
-    for t in range(1, nthreads):
-        if stop != L.LDG_CHAIN_STOP_END:
-            break  # a real stop (or a full buffer) before the join: the caller resumes from st_out
-        plans_t, stop_t, so_t, st_t = results[t]
-        if not len(plans_t):
-            return serial_rest(merged, st_out)
-        index = {}
-        for jj, e in enumerate(_entry_keys(rf, plans_t, st_t)):
-            index.setdefault(e, jj)
-        lo = plans_t[0].readloc
-        join = next(((i, index[e]) for i, e in enumerate(keys) if e[0] >= lo and e in index), None)
-        if join is None:
-            return serial_rest(merged, st_out)
-        i, j = join
-        head = merged[:i]
-        _, st_join = _retime(rf, head.copy().view(np.recarray), st0)
-        tail = plans_t[j:].copy().view(np.recarray)
-        kept, st_tail = _retime(rf, tail, st_join)
-        merged = np.concatenate([head, tail[:kept]]).view(np.recarray)
-        if kept < len(tail):
-            return serial_rest(merged, st_tail)
-        keys = _entry_keys(rf, merged, st0)
-        stop, st_out = stop_t, st_tail
-    return merged, stop, st_out
+    starts, lens, means = (np.ascontiguousarray(a, dtype=d) for a, d in zip(runs, (np.int64, np.int64, np.float64)))
+    params = chain_params(rf, nblocks)
+    st_in = state if state is not None else L.ChainState()
+    st_out = L.ChainState()
+    plans = out if out is not None and len(out) >= max_plans else np.empty(max_plans, PLAN_DTYPE)
+    n = ctypes.c_int32(0)
+    stop = ctypes.c_int32(0)
+    rc = lib.ldg_field_chain_mt(ctypes.byref(params), starts.ctypes.data, lens.ctypes.data, means.ctypes.data,
+                                len(starts), ctypes.byref(st_in), ctypes.byref(st_out), plans.ctypes.data,
+                                max_plans, ctypes.byref(n), ctypes.byref(stop), int(nthreads), int(margin),
+                                int(min_seg))
+    if rc != 0:
+        raise L.LdgError(rc, lib.ldg_chain_last_error().decode())
+    return plans[:n.value].view(np.recarray), stop.value, st_out
 
 
 def field_levels(rf):
@@ -492,10 +393,8 @@ class LineLocator:
         self._plans = np.empty(4096, PLAN_DTYPE)
         self._runbufs = None
         self._keep = None
-        import concurrent.futures as cf
         import os
         self.threads = max(1, min(8, os.cpu_count() or 1))
-        self._pool = cf.ThreadPoolExecutor(self.threads) if self.threads > 1 else None
 
     def _tick(self, key, t0):
         t = time.perf_counter()
@@ -606,7 +505,7 @@ class LineLocator:
         out = LocatedFields(rf)
         reads = 0
         while True:
-            plans, stop, st_out = parallel_chain(rf, runs, nblocks, state, self.threads, self._pool)
+            plans, stop, st_out = parallel_chain(rf, runs, nblocks, state, self.threads, out=self._plans)
             t = self._tick("chain", t)
             # a forced host decode cuts the segment at that read index
             cut = None

@@ -114,6 +114,9 @@ def test_parallel_chain_equals_serial(capture):
     whole, stop, st = run_chain(rf, runs, nb)
     for nthreads in (2, 3):
         got, stop2, st2 = parallel_chain(rf, runs, nb, None, nthreads, margin_blocks=100, min_seg_blocks=30)
+        assert got.tobytes() == whole.tobytes()
+        # a margin too short to reach a common state falls back to walking on
+        got, stop2, st2 = parallel_chain(rf, runs, nb, None, nthreads, margin_blocks=0, min_seg_blocks=30)
         assert stop2 == stop and st2.start == st.start
         assert len(got) == len(whole)
         assert got.tobytes() == whole.tobytes()
