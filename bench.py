@@ -36,6 +36,8 @@ for p in (ROOT, os.path.join(ROOT, "ld-decode_b200")):
         sys.path.insert(0, p)
 
 import numpy as np  # noqa: E402
+from ldgpu.replicas import barrier as replica_barrier  # noqa: E402
+from ldgpu.replicas import capture_seed, dist_env, max_over_ranks  # noqa: E402
 
 METRIC = "RF MSPS demod+TBC on 1 B200 (batched FP32 vs plain) + HBM roofline %"
 BYTES_PER_SAMPLE_DEMOD = 2 + 4 * 4 + 4 + 2  # input + 4 video f32 + rfhpf f32 + efm i16 (per output sample)
@@ -123,13 +125,6 @@ class Clocks:
         return out
 
 
-def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
-
-
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -156,7 +151,7 @@ def run_gpu(args):
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
 
-    cap = synth_capture(system, nsamples, seed=args.seed + rank, device="cuda")
+    cap = synth_capture(system, nsamples, seed=capture_seed(args.seed, rank), device="cuda")
     keys = ["demod", "demod_raw", "demod_05", "demod_burst"] + (["demod_pilot"] if system == "PAL" else [])
     outs = {k: torch.empty(nout, dtype=torch.float32, device="cuda") for k in keys}
     outs["rfhpf"] = torch.empty(nout, dtype=torch.float32, device="cuda")
@@ -199,8 +194,7 @@ def run_gpu(args):
         tbc(linelocs())
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        replica_barrier(world)
 
     for _ in range(args.warmup):
         step()
@@ -231,11 +225,7 @@ def run_gpu(args):
     ll_ms = [e[1].elapsed_time(e[2]) for e in ev]
     tbc_ms = [e[2].elapsed_time(e[3]) for e in ev]
     segs = loc.stats["segments"] / args.steps
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(sum(step_ms)), world, "cuda")
     ms_per_step = total_ms / args.steps
     fields = [(f.window, f.host_linelocs(), f.lineoffset, levels) for f in flist]
     # the threaded field chain against one sequential walk over the same runs (untimed)
@@ -267,11 +257,7 @@ def run_gpu(args):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        e2e_ms = e0.elapsed_time(e1) / args.steps
-        if world > 1:
-            t = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, "cuda")
         h2d = nsamples * 2
         d2h = nf * fsz * 2 + nout * 2 + 2 * nblocks * 991 * 4
         e2e = {"value": world * nout / (e2e_ms * 1e-3) / 1e6, "unit": "MSPS", "h2d_bytes_per_step": h2d,
