@@ -344,6 +344,7 @@ typedef struct ldg_lines_args {
     int32_t* field_phase;       /* out, NTSC: fieldPhaseID */
     void* scratch;              /* ldg_lines_scratch_bytes(nfields) bytes of device memory */
     void* stream;
+    const double* prev_phase_adjust_dev;  /* if set: device copy of prev_phase_adjust (read in stream order) */
 } ldg_lines_args;
 
 int64_t ldg_lines_scratch_bytes(int32_t nfields);

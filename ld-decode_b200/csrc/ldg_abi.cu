@@ -86,6 +86,7 @@ struct ldg_ctx {
     size_t ll_cap = 0;
     int* d_status = nullptr;
     void* d_lines = nullptr;  // sync-run scan scratch (ldg_sync_runs)
+    int* d_counter = nullptr; // demod block counter (dynamic block hand-out)
     size_t lines_cap = 0;
     std::mutex mu;
 };
@@ -192,6 +193,7 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     cudaFree(c->d_ll);
     cudaFree(c->d_status);
     cudaFree(c->d_lines);
+    cudaFree(c->d_counter);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -368,6 +370,9 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     p.scratch = c->d_scratch;
     p.tw16 = c->d_tw16;
     p.tw32 = c->d_tw32;
+    if (!c->d_counter) LDG_CK(cudaMalloc(&c->d_counter, sizeof(int)));
+    LDG_CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), st));
+    p.work_counter = c->d_counter;
 
     cudaError_t e = ldg::launch_demod(p, grid, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("demod launch: ") + cudaGetErrorString(e));

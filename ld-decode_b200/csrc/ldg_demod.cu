@@ -219,7 +219,14 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
     t.s4 = s4;
     __syncthreads();
 
-    for (int blk = blockIdx.x; blk < p.nblocks; blk += gridDim.x) {
+    __shared__ int s_next;
+    int blk = blockIdx.x;
+    if (p.work_counter) {
+        if (threadIdx.x == 0) s_next = atomicAdd(p.work_counter, 1);
+        __syncthreads();
+        blk = s_next;
+    }
+    while (blk < p.nblocks) {
         float2* parkX = p.scratch + (size_t)blockIdx.x * 2 * kM;
         float2* parkZ = parkX + kM;
 
@@ -303,6 +310,14 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
             fft16k<true>(S, t, SmemIO(),
                          RealStorer{p.o_video[o] + (long long)blk * p.s_video.len, p.s_video.start, p.s_video.len,
                                     p.roll[o]});
+        }
+        if (p.work_counter) {
+            __syncthreads();
+            if (threadIdx.x == 0) s_next = atomicAdd(p.work_counter, 1);
+            __syncthreads();
+            blk = s_next;
+        } else {
+            blk += gridDim.x;
         }
     }
 }

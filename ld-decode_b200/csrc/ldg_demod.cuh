@@ -52,6 +52,11 @@ struct DemodParams {
     float2* scratch;
     const float2* tw16;     // W_16384^i, i < 16384
     const float2* tw32;     // W_32768^k, k <= 8192
+
+    // blocks handed out one at a time from this counter (zero at launch), so
+    // CTAs that start late -- SMs busy with another stream's kernels -- take
+    // fewer blocks; nullptr: CTA i takes blocks i, i + grid, ...
+    int* work_counter;
 };
 
 // Dynamic shared memory the kernel needs.

@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(kBurstThreads) burst_chain_kernel(LineParams P
     __shared__ double rkey[kWarps][32];
     __shared__ int ridx[kWarps][32];
     __shared__ double med2[2];
-    double prev_pam = a.prev_phase_adjust;
+    double prev_pam = a.prev_phase_adjust_dev ? *a.prev_phase_adjust_dev : a.prev_phase_adjust;
     const int l = threadIdx.x, lane = l & 31, warp = l >> 5;
     const bool line = l < kBurstLines;
     BurstRec cur;

@@ -96,7 +96,7 @@ class LinesArgs(ctypes.Structure):
         ("nfields", c_i32), ("proclines", c_i32), ("startloc", c_p), ("wlen", c_p), ("isfirst", c_p),
         ("linecount", c_p), ("has_prev", c_p), ("linelocs1", c_p), ("linebad1", c_p),
         ("prev_phase_adjust", c_f64), ("linelocs", c_p), ("linebad", c_p), ("phase_adjust", c_p),
-        ("field_phase", c_p), ("scratch", c_p), ("stream", c_p),
+        ("field_phase", c_p), ("scratch", c_p), ("stream", c_p), ("prev_phase_adjust_dev", c_p),
     ]
 
 

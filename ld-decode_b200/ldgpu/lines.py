@@ -344,10 +344,11 @@ class LocatedFields:
             yield self[k]
 
 
-def tbc_batch(rf, fields, demod_ptr, out_u16_ptr, levels, coord_f32=False):
-    """ldg_tbc_field descriptors for LocatedFields (or a list of FieldLines):
-    uint16 fields of outlinelen x outlinecount written back to back at
-    out_u16_ptr, built as one numpy record array."""
+def tbc_batch(rf, fields, demod_ptr, out_u16_ptr, levels, coord_f32=False, first=0, count=None):
+    """ldg_tbc_field descriptors for LocatedFields (or a list of FieldLines),
+    fields [first, first + count): field i is written as uint16
+    outlinelen x outlinecount at out_u16_ptr + i * field bytes; built as one
+    numpy record array."""
     outw = rf.SysParams["outlinelen"]
     outl = rf.SysParams["frame_lines"] // 2 + 1
     if isinstance(fields, LocatedFields):
@@ -361,6 +362,10 @@ def tbc_batch(rf, fields, demod_ptr, out_u16_ptr, levels, coord_f32=False):
                        np.uint64)
         nlines = np.array([f.nlines for f in fields])
         lineoffset = np.array([f.lineoffset for f in fields])
+    count = len(startloc) - first if count is None else count
+    sel = slice(first, first + count)
+    startloc, length, ptr, nlines, lineoffset = (np.asarray(x)[sel] for x in (startloc, length, ptr, nlines,
+                                                                              lineoffset))
     n = len(startloc)
     d = np.zeros(n, TBC_DTYPE)
     d["buf"] = np.uint64(demod_ptr) + np.uint64(4) * startloc.astype(np.uint64)
@@ -375,7 +380,8 @@ def tbc_batch(rf, fields, demod_ptr, out_u16_ptr, levels, coord_f32=False):
     d["inlinelen"] = float(rf.linelen)
     d["outlinelen"] = float(outw)
     d["ire0"], d["hz_ire"], d["vsync_ire"], d["out_scale"], d["output_zero"] = [float(v) for v in levels]
-    d["out_u16"] = np.uint64(out_u16_ptr) + np.uint64(2 * outw * outl) * np.arange(n, dtype=np.uint64)
+    d["out_u16"] = np.uint64(out_u16_ptr) + np.uint64(2 * outw * outl) * np.arange(first, first + n,
+                                                                                   dtype=np.uint64)
     return (L.TbcField * n).from_buffer_copy(d.tobytes()) if n else (L.TbcField * 0)()
 
 
@@ -392,7 +398,7 @@ class LineLocator:
         self.timing = {}
         self._plans = np.empty(4096, PLAN_DTYPE)
         self._runbufs = None
-        self._keep = None
+        self._keep = []
         import os
         self.threads = max(1, min(8, os.cpu_count() or 1))
 
@@ -424,8 +430,10 @@ class LineLocator:
         k = nr.value
         return starts[:k], lens[:k], means[:k]
 
-    def _refine(self, arrays, capture_len, plans, prev_pam, stream):
-        """ldg_lines_refine over valid plans (record array); device tensors."""
+    def _refine(self, arrays, capture_len, plans, prev_pam, stream, prev_pam_dev=None):
+        """ldg_lines_refine over valid plans (record array); device tensors.
+        The NTSC burst seed of the first field is `prev_pam`, or the device
+        double at `prev_pam_dev` when given (read in stream order)."""
         torch = self.torch
         lib = L.load()
         nf = len(plans)
@@ -470,6 +478,7 @@ class LineLocator:
         a.linelocs1 = base + nb_i
         a.linebad1 = base + nb_i + nf * ml * 8
         a.prev_phase_adjust = float(prev_pam)
+        a.prev_phase_adjust_dev = prev_pam_dev
         a.linelocs = out_ll.data_ptr()
         a.linebad = out_bad.data_ptr()
         a.phase_adjust = pam.data_ptr()
@@ -479,38 +488,82 @@ class LineLocator:
         L.check(lib.ldg_lines_refine(self.rf._ctx.handle, ctypes.byref(a)))
         # device inputs and scratch return to the caching allocator on the
         # stream the kernels run on, so any reuse is ordered after them
-        self._keep = (hbuf, dbuf, scratch)
+        self._keep.append((hbuf, dbuf, scratch))
         return out_ll, out_bad, pam, fph
 
     def locate(self, arrays, nblocks, stream=None, force_host=()):
         """Line locations of every field.  `arrays` maps output names
         (demod, demod_05, demod_burst[, demod_pilot]) to capture-wide float32
-        device tensors of equal length.  Returns a LocatedFields of the
+        device tensors of equal length; `stream` as for `advance`.  Returns a LocatedFields of the
         valid fields in read order; `self.stats` counts batched,
         host-decoded and invalid reads and `self.timing` the host time of
         each phase (ms).  `force_host` lists read indices to decode with the
         host restatement (checks of the resume path)."""
+        self.begin(arrays)
+        self.advance(nblocks, stream, force_host)
+        return self.fields
+
+    def begin(self, arrays):
+        """Start a capture whose outputs are (or will be) in `arrays`; the
+        fields come out as `advance` is told how many blocks are done."""
+        self._arrays = arrays
+        self._ptrs = {k: v.data_ptr() for k, v in arrays.items()}
+        self._cap_len = int(arrays["demod_05"].numel())
+        self._runs = (np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0, np.float64))
+        self._scan_lo = 0
+        self._state = L.ChainState()
+        self._pam = ("host", 0.0)       # NTSC burst seed for the next batched field
+        self._prev_host = None          # the previous field, if it was host-decoded
+        self._last_dev = None           # index of the last batched field
+        self._ire0 = float(self.rf.DecoderParams["ire0"])
+        self._reads = 0
+        self._keep = []
+        self.fields = LocatedFields(self.rf)
+
+    def _scan(self, hi, stream):
+        """Sync runs of demod_05 over [scan position, hi), appended."""
+        lo = self._scan_lo
+        if hi - lo < 2:
+            return
+        st, ln, mn = self.sync_runs(self._ptrs["demod_05"] + 4 * lo, hi - lo, stream)
+        if len(st):
+            st = st + lo
+            # the next scan restarts after the last complete run: what follows
+            # is above the threshold or the start of a run still open at hi
+            self._scan_lo = int(st[-1] + ln[-1])
+            self._runs = tuple(np.concatenate([a, b]) for a, b in zip(self._runs, (st, ln.copy(), mn.copy())))
+
+    def advance(self, nblocks, stream=None, force_host=()):
+        """Fields whose read windows lie within the first `nblocks` blocks
+        (demodulated and complete in stream order on `stream`): scans the
+        new samples, walks the chain, refines on the GPU.  `stream` is a
+        torch.cuda.Stream (device work and allocations are ordered on it) or
+        None.  Returns the range of new indices into `self.fields`."""
+        import contextlib
+        if isinstance(stream, self.torch.cuda.Stream):
+            with self.torch.cuda.stream(stream):
+                return self._advance(nblocks, stream.cuda_stream, force_host)
+        with contextlib.nullcontext():
+            return self._advance(nblocks, stream, force_host)
+
+    def _advance(self, nblocks, stream, force_host):
         rf = self.rf
         torch = self.torch
-        capture_len = int(arrays["demod_05"].numel())
-        ptrs = {k: v.data_ptr() for k, v in arrays.items()}
+        U = rf.blocklen - rf.blockcut - rf.blockcut_end
+        first_new = len(self.fields)
         t = time.perf_counter()
-        runs = self.sync_runs(ptrs["demod_05"], capture_len, stream)
+        self._scan(min(nblocks * U, self._cap_len), stream)
         t = self._tick("sync_runs", t)
-        state = L.ChainState()
-        prev_pam = 0.0
-        prev_host = None     # host-decoded previous field (FieldLogic) if the last one was
-        last_dev = None      # index of the last batched field in `out`
-        ire0 = float(rf.DecoderParams["ire0"])
-        out = LocatedFields(rf)
-        reads = 0
+        out = self.fields
+        arrays, ptrs = self._arrays, self._ptrs
+        state = self._state
         while True:
-            plans, stop, st_out = parallel_chain(rf, runs, nblocks, state, self.threads, out=self._plans)
+            plans, stop, st_out = parallel_chain(rf, self._runs, nblocks, state, self.threads, out=self._plans)
             t = self._tick("chain", t)
             # a forced host decode cuts the segment at that read index
             cut = None
             for i in range(len(plans)):
-                if reads + i in force_host:
+                if self._reads + i in force_host:
                     cut = i
                     break
             if cut is not None:
@@ -519,45 +572,50 @@ class LineLocator:
                 st_out = self._state_after(plans, state)
             valid = plans[plans.valid != 0].copy().view(np.recarray)
             self.stats["invalid"] += len(plans) - len(valid)
-            reads += len(plans)
+            self._reads += len(plans)
             if len(valid):
                 self.stats["segments"] += 1
                 self.stats["batched"] += len(valid)
+                pam_host, pam_dev = 0.0, None
                 if not self.pal and valid.has_prev[0]:
-                    if prev_host is not None:
-                        prev_pam = float(prev_host.phase_adjust_median)
-                    elif last_dev is not None:
-                        prev_pam = float(out[last_dev].phase_adjust_median)
-                ll, bad, pam, fph = self._refine(ptrs, capture_len, valid, prev_pam, stream)
+                    if self._pam[0] == "host":
+                        pam_host = self._pam[1]
+                    else:
+                        pam_dev = self._pam[1]
+                ll, bad, pam, fph = self._refine(ptrs, self._cap_len, valid, pam_host, stream, pam_dev)
                 out._parts.append(("batch", valid, ll, pam, fph))
-                last_dev = len(out) - 1
-                prev_host = None
+                out._cache = None
+                self._last_dev = len(out) - 1
+                self._prev_host = None
+                if not self.pal:
+                    self._pam = ("dev", pam.data_ptr() + 8 * (len(valid) - 1))
+                    self._keep.append(pam)
                 t = self._tick("refine", t)
-            if stop == L.LDG_CHAIN_STOP_END:
-                break
-            if stop == L.LDG_CHAIN_STOP_FULL:
-                state = st_out
-                continue
-            # decode the next field on the host, with the previous field's results
             state = st_out
+            if stop in (L.LDG_CHAIN_STOP_END, L.LDG_CHAIN_STOP_FULL):
+                if stop == L.LDG_CHAIN_STOP_FULL:
+                    continue
+                break
+            # decode the next field on the host, with the previous field's results
             w = field_window(rf, state.start)
             if w.first_block + w.nblocks > nblocks:
                 break
             prevfield = None
             if state.prev_valid:
-                if prev_host is not None:
-                    prevfield = prev_host
+                if self._prev_host is not None:
+                    prevfield = self._prev_host
                 else:
-                    fl = out[last_dev]
+                    fl = out[self._last_dev]
                     prevfield = self._proxy(arrays, fl, fl.phase_adjust_median if not self.pal else 0.0)
             f = self._host_field(arrays, w, prevfield, state.fields_written)
-            reads += 1
+            self._reads += 1
             self.stats["host"] += 1
             if not f.valid:
                 self.stats["invalid"] += 1
                 state.start += f.nextfieldoffset
                 state.prev_valid = 0
-                prev_host = None
+                self._prev_host = None
+                self._pam = ("host", 0.0)
                 t = self._tick("host_fields", t)
                 continue
             ll_host = np.ascontiguousarray(f.linelocs, dtype=np.float64)
@@ -568,19 +626,23 @@ class LineLocator:
             dev_ll = torch.from_numpy(ll_host).to(torch.device("cuda", torch.cuda.current_device()))
             fl.linelocs_ptr = dev_ll.data_ptr()
             out._parts.append(("host", fl, dev_ll))
+            out._cache = None
             state.start += f.nextfieldoffset - (w.readloc - w.startloc)
             state.prev_valid = 1
             state.prev_isfirst = int(bool(f.isFirstField))
             state.prev_startloc = w.startloc
             state.fields_written += 1
-            prev_host = f
-            if not self.pal:
-                prev_pam = float(f.phase_adjust_median)
-            if float(rf.DecoderParams["ire0"]) != ire0:
-                ire0 = float(rf.DecoderParams["ire0"])
-                runs = self.sync_runs(ptrs["demod_05"], capture_len, stream)
+            self._prev_host = f
+            self._pam = ("host", float(f.phase_adjust_median) if not self.pal else 0.0)
+            if float(rf.DecoderParams["ire0"]) != self._ire0:
+                # the level re-calibration changed the sync threshold: rescan
+                self._ire0 = float(rf.DecoderParams["ire0"])
+                self._scan_lo = 0
+                self._runs = (np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0, np.float64))
+                self._scan(min(nblocks * U, self._cap_len), stream)
             t = self._tick("host_fields", t)
-        return out
+        self._state = state
+        return first_new, len(out)
 
     def _state_after(self, plans, state):
         """Chain state after the given plans (for a forced cut)."""
