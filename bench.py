@@ -7,9 +7,11 @@ blocks and 600 fields.  One step = every block of the capture through the
 fused demodulator (all outputs: demod, demod_raw, demod_05, demod_burst,
 rfhpf, EFM, analog audio stage 1), the line locations of every field (GPU
 sync-run scan, native field chain, GPU H-sync / burst / pilot refinement)
-and every field through the TBC (uint16 4fsc fields).  The step runs in
-chunks of blocks: while the GPU demodulates chunk c+1, the host walks chunk
-c's fields and a higher-priority stream scans, refines and resamples them.
+and every field through the TBC (uint16 4fsc fields).  With --chunks > 1
+the step runs in chunks of blocks: while the GPU demodulates chunk c+1, the
+host walks chunk c's fields and a higher-priority stream scans, refines and
+resamples them (the persistent demod kernel holds every SM, so the overlap
+is limited to the gaps between chunks).
 
 Prints one JSON line (rank 0).  `--impl reference` times the CPU oracle (a
 numpy restatement of the reference's demodblock + scale_field) on the host
@@ -60,7 +62,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--chunks", type=int, default=4, help="pipeline chunks of blocks per step")
+    ap.add_argument("--chunks", type=int, default=1,
+                    help="pipeline chunks of blocks per step (1: demod, then line locations, then TBC)")
     return ap.parse_args()
 
 
