@@ -201,14 +201,18 @@ def run_gpu(args):
             evs.append(ev)
         for c in range(nchunks):
             streamB.wait_event(evs[c])
-            lo, hi = loc.advance(bounds[c + 1], stream=streamB)
-            if hi > lo and pics is not None:
+            loc.advance(bounds[c + 1], stream=streamB)
+            # TBC of each range of fields as its line locations become final
+            # (on stream A, so it overlaps the NTSC burst chain's next range)
+            while loc.ready and pics is not None:
+                lo, hi, ev = loc.ready.pop(0)
+                stream.wait_event(ev)
                 tbc_fields(rf, tbc_batch(rf, loc.fields, outs["demod"].data_ptr(), pics.data_ptr(), levels,
-                                         first=lo, count=hi - lo), stream=streamB.cuda_stream)
+                                         first=lo, count=hi - lo), stream=sh)
         marks["demod_end"] = evs[-1]
-        end = torch.cuda.Event(enable_timing=True)
-        end.record(streamB)
         stream.wait_stream(streamB)
+        end = torch.cuda.Event(enable_timing=True)
+        end.record(stream)
         marks["end"] = end
         return loc.fields
 

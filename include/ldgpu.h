@@ -345,6 +345,10 @@ typedef struct ldg_lines_args {
     void* scratch;              /* ldg_lines_scratch_bytes(nfields) bytes of device memory */
     void* stream;
     const double* prev_phase_adjust_dev;  /* if set: device copy of prev_phase_adjust (read in stream order) */
+    int32_t first_field;        /* work on fields [first_field, first_field + count) of the nfields */
+    int32_t count;              /* 0: to the end */
+    int32_t stages;             /* bits: 1 H-sync (PAL: all of PAL), 2 NTSC burst chain, 4 NTSC apply; 0: all */
+    int32_t pad2;
 } ldg_lines_args;
 
 int64_t ldg_lines_scratch_bytes(int32_t nfields);
@@ -355,7 +359,13 @@ int64_t ldg_abi_sizeof(const char* name);
 /* GPU refinement of all fields' line locations: refine_linelocs_hsync,
  * compute_deriv_error, NTSC refine_linelocs_burst + fix_badlines + the
  * 117.25-degree subcarrier shift, PAL refine_linelocs_pilot x2 +
- * fix_badlines.  All pointers device memory; asynchronous on `stream`. */
+ * fix_badlines.  All pointers device memory; asynchronous on `stream`.
+ * A call may do some stages for a range of the fields (the scratch layout is
+ * that of all nfields): stage 1 for all fields, then stages 2 and 4 range by
+ * range in order lets the fields of a finished range go on (e.g. to the TBC
+ * on another stream) while the NTSC burst chain, which walks the fields one
+ * after another, continues.  A range's burst chain starts from the previous
+ * field's phase_adjust output when first_field > 0. */
 int ldg_lines_refine(ldg_ctx* ctx, const ldg_lines_args* args);
 
 #ifdef __cplusplus

@@ -446,7 +446,7 @@ __device__ void pilot_pass(const LineParams& P, double* ll, const float* pilot, 
 }
 
 __global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P) {
-    const int f = blockIdx.x;
+    const int f = P.a.first_field + blockIdx.x;
     const ldg_lines_args& a = P.a;
     const long long base = a.startloc[f];
     const long long n = min((long long)a.wlen[f], (long long)(a.capture_len - base));
@@ -600,16 +600,19 @@ __global__ void __launch_bounds__(kBurstThreads) burst_chain_kernel(LineParams P
     __shared__ double rkey[kWarps][32];
     __shared__ int ridx[kWarps][32];
     __shared__ double med2[2];
-    double prev_pam = a.prev_phase_adjust_dev ? *a.prev_phase_adjust_dev : a.prev_phase_adjust;
+    const int f0 = a.first_field, f1 = a.first_field + a.count;
+    // a later range continues from the previous field's output
+    double prev_pam = f0 > 0 ? a.phase_adjust[f0 - 1]
+                             : (a.prev_phase_adjust_dev ? *a.prev_phase_adjust_dev : a.prev_phase_adjust);
     const int l = threadIdx.x, lane = l & 31, warp = l >> 5;
     const bool line = l < kBurstLines;
     BurstRec cur;
     cur.valid = 0;
-    if (line && a.nfields > 0) cur = P.rec[l];
-    for (int f = 0; f < a.nfields; ++f) {
+    if (line && f1 > f0) cur = P.rec[(long long)f0 * kBurstLines + l];
+    for (int f = f0; f < f1; ++f) {
         BurstRec nxt;
         nxt.valid = 0;
-        if (line && f + 1 < a.nfields) nxt = P.rec[(long long)(f + 1) * kBurstLines + l];
+        if (line && f + 1 < f1) nxt = P.rec[(long long)(f + 1) * kBurstLines + l];
         const double prev = a.has_prev[f] ? prev_pam : 0.0;
         double adj = INFINITY;
         bool ok = false, rising = false;
@@ -670,7 +673,7 @@ __global__ void __launch_bounds__(kBurstThreads) burst_chain_kernel(LineParams P
 
 // NTSC: refine_linelocs_burst's application, fix_badlines, subcarrier shift
 __global__ void __launch_bounds__(512) burst_apply_kernel(LineParams P, double shift) {
-    const int f = blockIdx.x;
+    const int f = P.a.first_field + blockIdx.x;
     const ldg_lines_args& a = P.a;
     const int nl = a.proclines;
     const int lc = a.linecount[f];
@@ -823,8 +826,12 @@ extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
         return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: NTSC needs proclines >= 266");
     if (a->k.system == 1 && a->proclines < kPilotLines)
         return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: PAL needs proclines >= 323");
+    if (a->first_field < 0 || a->first_field >= a->nfields || a->count < 0 ||
+        a->first_field + a->count > a->nfields || a->stages < 0 || a->stages > 7)
+        return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: bad field range or stages");
     LineParams P;
     P.a = *a;
+    if (P.a.count == 0) P.a.count = a->nfields - a->first_field;
     P.system = a->k.system;
     P.freq = a->k.freq;
     P.linelen = a->k.linelen;
@@ -849,11 +856,12 @@ extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
     cudaGetDevice(&prev);
     cudaSetDevice(ldg::ctx_device(c));
     cudaStream_t st = (cudaStream_t)a->stream;
-    lines_hsync_kernel<<<a->nfields, kLineThreads, 0, st>>>(P);
+    const int stages = a->stages ? a->stages : 7;
+    if (stages & 1) lines_hsync_kernel<<<P.a.count, kLineThreads, 0, st>>>(P);
     if (P.system == 0) {
-        burst_chain_kernel<<<1, kBurstThreads, 0, st>>>(P);
+        if (stages & 2) burst_chain_kernel<<<1, kBurstThreads, 0, st>>>(P);
         const double shift = (117.25 / 360) / P.fsc_mhz * P.freq;
-        burst_apply_kernel<<<a->nfields, 512, 0, st>>>(P, shift);
+        if (stages & 4) burst_apply_kernel<<<P.a.count, 512, 0, st>>>(P, shift);
     }
     cudaError_t e = cudaGetLastError();
     if (prev >= 0) cudaSetDevice(prev);

@@ -97,6 +97,7 @@ class LinesArgs(ctypes.Structure):
         ("linecount", c_p), ("has_prev", c_p), ("linelocs1", c_p), ("linebad1", c_p),
         ("prev_phase_adjust", c_f64), ("linelocs", c_p), ("linebad", c_p), ("phase_adjust", c_p),
         ("field_phase", c_p), ("scratch", c_p), ("stream", c_p), ("prev_phase_adjust_dev", c_p),
+        ("first_field", c_i32), ("count", c_i32), ("stages", c_i32), ("pad2", c_i32),
     ]
 
 

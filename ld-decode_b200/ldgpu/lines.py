@@ -399,8 +399,10 @@ class LineLocator:
         self._plans = np.empty(4096, PLAN_DTYPE)
         self._runbufs = None
         self._keep = []
+        self.ready = []
+        self.chain_range = 128   # NTSC fields per burst-chain launch
         import os
-        self.threads = max(1, min(8, os.cpu_count() or 1))
+        self.threads = max(1, min(16, os.cpu_count() or 1))
 
     def _tick(self, key, t0):
         t = time.perf_counter()
@@ -485,11 +487,30 @@ class LineLocator:
         a.field_phase = fph.data_ptr()
         a.scratch = scratch.data_ptr()
         a.stream = stream
-        L.check(lib.ldg_lines_refine(self.rf._ctx.handle, ctypes.byref(a)))
+        ts = torch.cuda.ExternalStream(stream) if stream else torch.cuda.current_stream()
+        ready = []
+        if self.pal:
+            L.check(lib.ldg_lines_refine(self.rf._ctx.handle, ctypes.byref(a)))
+            ev = torch.cuda.Event()
+            ev.record(ts)
+            ready.append((0, nf, ev))
+        else:
+            # H-sync of every field, then the burst chain range by range: each
+            # finished range can go on (TBC) while the chain walks the next
+            a.stages = 1
+            L.check(lib.ldg_lines_refine(self.rf._ctx.handle, ctypes.byref(a)))
+            for lo in range(0, nf, self.chain_range):
+                a.first_field = lo
+                a.count = min(self.chain_range, nf - lo)
+                a.stages = 6
+                L.check(lib.ldg_lines_refine(self.rf._ctx.handle, ctypes.byref(a)))
+                ev = torch.cuda.Event()
+                ev.record(ts)
+                ready.append((lo, lo + a.count, ev))
         # device inputs and scratch return to the caching allocator on the
         # stream the kernels run on, so any reuse is ordered after them
         self._keep.append((hbuf, dbuf, scratch))
-        return out_ll, out_bad, pam, fph
+        return out_ll, out_bad, pam, fph, ready
 
     def locate(self, arrays, nblocks, stream=None, force_host=()):
         """Line locations of every field.  `arrays` maps output names
@@ -519,6 +540,9 @@ class LineLocator:
         self._reads = 0
         self._keep = []
         self.fields = LocatedFields(self.rf)
+        # (first, end, event): fields whose line locations are final once the
+        # event has completed, in order
+        self.ready = []
 
     def _scan(self, hi, stream):
         """Sync runs of demod_05 over [scan position, hi), appended."""
@@ -582,7 +606,9 @@ class LineLocator:
                         pam_host = self._pam[1]
                     else:
                         pam_dev = self._pam[1]
-                ll, bad, pam, fph = self._refine(ptrs, self._cap_len, valid, pam_host, stream, pam_dev)
+                base = len(out)
+                ll, bad, pam, fph, ready = self._refine(ptrs, self._cap_len, valid, pam_host, stream, pam_dev)
+                self.ready.extend((base + lo, base + hi, ev) for lo, hi, ev in ready)
                 out._parts.append(("batch", valid, ll, pam, fph))
                 out._cache = None
                 self._last_dev = len(out) - 1
@@ -627,6 +653,9 @@ class LineLocator:
             fl.linelocs_ptr = dev_ll.data_ptr()
             out._parts.append(("host", fl, dev_ll))
             out._cache = None
+            ev = torch.cuda.Event()
+            ev.record()
+            self.ready.append((len(out) - 1, len(out), ev))
             state.start += f.nextfieldoffset - (w.readloc - w.startloc)
             state.prev_valid = 1
             state.prev_isfirst = int(bool(f.isFirstField))
