@@ -57,17 +57,49 @@ constexpr int kBurstThreads = 288;  // >= kBurstLines, whole warps
 
 __device__ __forceinline__ bool below(const float* x, long long i, double thr) { return (double)x[i] <= thr; }
 
+// the below-threshold flags of samples base-1 .. base+3 (4 per thread per
+// step; a float4 load when the array is 16-byte aligned)
+__device__ __forceinline__ unsigned four_flags(const float* __restrict__ x, long long n, long long base, double thr,
+                                               bool aligned) {
+    float v[4];
+    if (aligned && base + 3 < n) {
+        const float4 q = __ldcs(reinterpret_cast<const float4*>(x + base));
+        v[0] = q.x;
+        v[1] = q.y;
+        v[2] = q.z;
+        v[3] = q.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = base + k < n ? x[base + k] : 0.0f;
+    }
+    const bool prev = base > 0 && base - 1 < n ? below(x, base - 1, thr) : false;
+    unsigned b = prev ? 1u : 0u;  // bit 0: sample base-1; bit k+1: sample base+k
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (base + k < n && (double)v[k] <= thr) b |= 2u << k;
+    return b;
+}
+
+// edge bits of a thread's 4 samples (bit k: sample base+k starts or ends a run)
+__device__ __forceinline__ unsigned edge_bits(unsigned b, long long base, long long n) {
+    unsigned e = (b ^ (b >> 1)) & 0xfu;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (base + k >= n) e &= ~(1u << k);
+    return e;
+}
+
+constexpr int kEdgeSteps = kEdgeTile / (4 * kEdgeThreads);
+
 __global__ void __launch_bounds__(kEdgeThreads) edge_count_kernel(const float* __restrict__ x, long long n,
                                                                    double thr, int* __restrict__ counts) {
     const long long t0 = (long long)blockIdx.x * kEdgeTile;
+    const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
     int c = 0;
-    for (int j = 0; j < kEdgeTile / kEdgeThreads; ++j) {
-        const long long i = t0 + j * kEdgeThreads + threadIdx.x;
-        if (i < n) {
-            const bool b = below(x, i, thr);
-            const bool bp = i > 0 ? below(x, i - 1, thr) : false;
-            c += b != bp;
-        }
+#pragma unroll 2
+    for (int j = 0; j < kEdgeSteps; ++j) {
+        const long long base = t0 + (long long)j * 4 * kEdgeThreads + 4 * threadIdx.x;
+        if (base < n) c += __popc(edge_bits(four_flags(x, n, base, thr, aligned), base, n));
     }
     __shared__ int warp_sum[kEdgeThreads / 32];
     int v = c;
@@ -75,9 +107,9 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_count_kernel(const float* _
     if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = v;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int s = 0;
-        for (int w = 0; w < kEdgeThreads / 32; ++w) s += warp_sum[w];
-        counts[blockIdx.x] = s;
+        int sum = 0;
+        for (int w = 0; w < kEdgeThreads / 32; ++w) sum += warp_sum[w];
+        counts[blockIdx.x] = sum;
     }
 }
 
@@ -114,28 +146,39 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const float* _
                                                                    long long* __restrict__ edges, long long cap) {
     __shared__ int warp_cnt[kEdgeThreads / 32];
     const long long t0 = (long long)blockIdx.x * kEdgeTile;
+    const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
     long long out = offsets[blockIdx.x];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int j = 0; j < kEdgeTile / kEdgeThreads; ++j) {
-        const long long i = t0 + j * kEdgeThreads + threadIdx.x;
-        bool flag = false, b = false;
-        if (i < n) {
-            b = below(x, i, thr);
-            const bool bp = i > 0 ? below(x, i - 1, thr) : false;
-            flag = b != bp;
+    for (int j = 0; j < kEdgeSteps; ++j) {
+        const long long base = t0 + (long long)j * 4 * kEdgeThreads + 4 * threadIdx.x;
+        unsigned b = 0, e = 0;
+        if (base < n) {
+            b = four_flags(x, n, base, thr, aligned);
+            e = edge_bits(b, base, n);
         }
-        const unsigned m = __ballot_sync(0xffffffffu, flag);
-        if (lane == 0) warp_cnt[warp] = __popc(m);
+        const int cnt = __popc(e);
+        // inclusive warp scan of the per-thread counts
+        int inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) warp_cnt[warp] = inc;
         __syncthreads();
         int before = 0, chunk = 0;
+#pragma unroll
         for (int w = 0; w < kEdgeThreads / 32; ++w) {
             before += w < warp ? warp_cnt[w] : 0;
             chunk += warp_cnt[w];
         }
-        if (flag) {
-            const long long k = out + before + __popc(m & ((1u << lane) - 1u));
-            if (k < cap) edges[k] = 2 * i + (b ? 1 : 0);
-        }
+        long long k = out + before + inc - cnt;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (e & (1u << q)) {
+                if (k < cap) edges[k] = 2 * (base + q) + ((b >> (q + 1)) & 1u);
+                ++k;
+            }
         out += chunk;
         __syncthreads();
     }
@@ -216,6 +259,86 @@ __device__ double median_f32(const float* x, long long lo, long long hi, long lo
     if (m == 0) return nan("");
     if (m & 1) return (double)v[m / 2];
     return (double)((v[m / 2 - 1] + v[m / 2]) * 0.5f);
+}
+
+// Warp-cooperative forms (every lane returns the same result).
+
+// calczc with 32 samples tested per step and the first crossing by ballot
+__device__ bool warp_calczc(const float* x, long long n, double start_offset, double target, int edge, double count,
+                            double& out) {
+    const int lane = threadIdx.x & 31;
+    const long long s = (long long)start_offset;
+    if (s < 0 || s >= n) return false;
+    const long long icount = (long long)(count + 1);
+    if (edge == 0) edge = (double)x[s] < target ? 1 : -1;
+    const long long end = min(s + icount, n);
+    for (long long c0 = s + 1; c0 < end; c0 += 32) {
+        const long long i = c0 + lane;
+        bool hit = false;
+        if (i < end) {
+            const double a = (double)x[i - 1], b = (double)x[i];
+            hit = edge == 1 ? (a < target && b >= target) : (a > target && b <= target);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (m) {
+            const long long loc = c0 + __ffs(m) - 1;
+            const double a = (double)x[loc - 1] - target, b = (double)x[loc] - target;
+            out = (double)(loc - 1) + ((b - a != 0) ? -a / (-a + b) : 0.0);
+            return true;
+        }
+    }
+    return false;
+}
+
+__device__ void warp_minmax(const float* x, long long lo, long long hi, long long n, float& mn, float& mx) {
+    const int lane = threadIdx.x & 31;
+    lo = max(lo, 0LL);
+    hi = min(hi, n);
+    mn = INFINITY;
+    mx = -INFINITY;
+    for (long long i = lo + lane; i < hi; i += 32) {
+        const float v = x[i];
+        mn = fminf(mn, v);
+        mx = fmaxf(mx, v);
+    }
+    for (int o = 16; o; o >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+}
+
+// np.median of a float32 slice of up to 64 samples by rank (ties by
+// position); longer slices fall back to one lane
+__device__ double warp_median_f32(const float* x, long long lo, long long hi, long long n) {
+    const int lane = threadIdx.x & 31;
+    lo = max(lo, 0LL);
+    hi = min(hi, n);
+    const int m = (int)max(hi - lo, 0LL);
+    if (m == 0) return nan("");
+    if (m > 64) {
+        double r = 0;
+        if (lane == 0) r = median_f32(x, lo, hi, n);
+        return __shfl_sync(0xffffffffu, r, 0);
+    }
+    const float v0 = lane < m ? x[lo + lane] : 0.0f;
+    const float v1 = lane + 32 < m ? x[lo + 32 + lane] : 0.0f;
+    int r0 = 0, r1 = 0;
+    for (int j = 0; j < m; ++j) {
+        const float vj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
+        r0 += (vj < v0) || (vj == v0 && j < lane);
+        r1 += (vj < v1) || (vj == v1 && j < lane + 32);
+    }
+    const int ka = (m - 1) / 2, kb = m / 2;
+    auto pick = [&](int k) {
+        const unsigned m0 = __ballot_sync(0xffffffffu, lane < m && r0 == k);
+        const unsigned m1 = __ballot_sync(0xffffffffu, lane + 32 < m && r1 == k);
+        const float a = __shfl_sync(0xffffffffu, v0, m0 ? __ffs(m0) - 1 : 0);
+        const float b = __shfl_sync(0xffffffffu, v1, m1 ? __ffs(m1) - 1 : 0);
+        return m0 ? a : b;
+    };
+    const float va = pick(ka), vb = pick(kb);
+    if (m & 1) return (double)va;
+    return (double)((va + vb) * 0.5f);
 }
 
 // get_linelen (core.py:1655-1672) with linecount + lineoffset = lc
@@ -461,41 +584,44 @@ __global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P)
         bad[i] = a.linebad1[(long long)f * kMaxL + i];
     }
     __syncthreads();
-    // refine_linelocs_hsync
-    if (i < nl) {
-        bool b = bad[i];
-        double v2 = ll1[i];
-        if ((i >= 3 && i <= 6) || (P.system == 1 && i >= 1 && i <= 2)) {
-            b = true;
-        } else {
-            const double l1 = ll1[i] - P.freq;
-            double zc;
-            if (calczc(d05, n, l1, P.half_sync, 0, P.freq * 2, zc) && !b) {
-                v2 = zc;
-                const long long lo = (long long)(zc - (P.freq * 0.75)), hi = min((long long)(zc + (P.freq * 8)), n);
-                float mn = INFINITY, mx = -INFINITY;
-                for (long long k = max(lo, 0LL); k < hi; ++k) {
-                    mn = fminf(mn, d05[k]);
-                    mx = fmaxf(mx, d05[k]);
-                }
-                if ((double)mn < P.lo_ok || (double)mx > P.hi_ok) {
-                    b = true;
-                } else {
-                    const double porch = median_f32(d05, (long long)(zc + (P.freq * 8)), (long long)(zc + (P.freq * 9)), n);
-                    const double sync = median_f32(d05, (long long)(zc + (P.freq * 1)), (long long)(zc + (P.freq * 2.5)), n);
-                    double zc2;
-                    if (calczc(d05, n, l1, (porch + sync) / 2, 0, 400, zc2) && fabs(zc2 - zc) < (P.freq / 2))
-                        v2 = zc2;
-                    else
-                        b = true;
-                }
-            } else {
+    // refine_linelocs_hsync: one warp per line
+    {
+        const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+        for (int li = threadIdx.x >> 5; li < nl; li += nwarps) {
+            bool b = bad[li];
+            double v2 = ll1[li];
+            if ((li >= 3 && li <= 6) || (P.system == 1 && li >= 1 && li <= 2)) {
                 b = true;
+            } else {
+                const double l1 = ll1[li] - P.freq;
+                double zc;
+                if (warp_calczc(d05, n, l1, P.half_sync, 0, P.freq * 2, zc) && !b) {
+                    v2 = zc;
+                    float mn, mx;
+                    warp_minmax(d05, (long long)(zc - (P.freq * 0.75)), (long long)(zc + (P.freq * 8)), n, mn, mx);
+                    if ((double)mn < P.lo_ok || (double)mx > P.hi_ok) {
+                        b = true;
+                    } else {
+                        const double porch =
+                            warp_median_f32(d05, (long long)(zc + (P.freq * 8)), (long long)(zc + (P.freq * 9)), n);
+                        const double sync =
+                            warp_median_f32(d05, (long long)(zc + (P.freq * 1)), (long long)(zc + (P.freq * 2.5)), n);
+                        double zc2;
+                        if (warp_calczc(d05, n, l1, (porch + sync) / 2, 0, 400, zc2) && fabs(zc2 - zc) < (P.freq / 2))
+                            v2 = zc2;
+                        else
+                            b = true;
+                    }
+                } else {
+                    b = true;
+                }
+            }
+            if (b) v2 = ll1[li];
+            if (lane == 0) {
+                ll[li] = v2;
+                bad[li] = b;
             }
         }
-        if (b) v2 = ll1[i];
-        ll[i] = v2;
-        bad[i] = b;
     }
     __syncthreads();
     deriv_error_block(ll, bad, nl);
