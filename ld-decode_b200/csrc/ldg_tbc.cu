@@ -146,7 +146,6 @@ __global__ void __launch_bounds__(kWowThreads) wow_levels_kernel(const TbcField*
 }
 
 constexpr int kGatherThreads = 256;
-constexpr int kGatherPix = 2;  // output pixels per thread (independent loads in flight)
 
 // Input coordinate (FP64) of output pixel ig, optionally rounded to float32
 // as the reference does; the spline segment j is also returned.  The
@@ -168,61 +167,62 @@ __device__ __forceinline__ double pixel_coord(const TbcField& f, long long ig, i
     return c;
 }
 
-// One thread per kGatherPix output pixels of one field; blockIdx.y is the
-// field.  No shared staging: the 16 taps of neighbouring pixels overlap and
-// are served from L1, the two LUT rows of a pixel are 128 contiguous bytes.
+// One warp per 32 consecutive output pixels of one field; blockIdx.y is the
+// field.  Each lane computes its own pixel's FP64 coordinate; then groups of
+// 8 lanes gather one pixel at a time: lane k of a group reads taps 2k, 2k+1
+// of the input and of the two LUT rows, so a pixel's 64-byte input span and
+// its two 64-byte LUT rows are each one contiguous access (instead of 16
+// scattered ones per lane); the 8 partial sums meet by shuffles.
 __global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcField* fields, const float* lut,
                                                                     int nfields) {
     const int fi = blockIdx.y;
     if (fi >= nfields) return;
     const TbcField& f = fields[fi];
     const long long nout = (long long)f.linesout * f.outwidth;
-    const long long i0 = ((long long)blockIdx.x * kGatherThreads) * kGatherPix + threadIdx.x;
-    if (i0 >= nout) return;
+    const long long wbase = (long long)blockIdx.x * kGatherThreads + (threadIdx.x & ~31);
+    if (wbase >= nout) return;  // whole warps leave together
+    const int lane = threadIdx.x & 31, grp = lane >> 3, k = lane & 7;
+    const long long i = wbase + lane;
     const int nseg = f.nlines - 1;
     const long long igbase = (long long)f.outwidth * (f.lineoffset + 1);
-    int jj[kGatherPix], ps[kGatherPix];
-    long long st[kGatherPix];
-    float alpha[kGatherPix];
-    bool ok[kGatherPix];
-#pragma unroll
-    for (int u = 0; u < kGatherPix; ++u) {
-        const long long i = i0 + (long long)u * kGatherThreads;
-        const double cc = pixel_coord(f, igbase + (i < nout ? i : 0), nseg, jj[u]);
-        const long long ci = (long long)cc;
-        const double ph = __dmul_rn(cc - (double)ci, 65536.0);
-        ps[u] = (int)ph;
-        alpha[u] = __double2float_rn(ph - (double)ps[u]);
-        st[u] = ci - 7;
-        ok[u] = i < nout && st[u] >= 0 && st[u] + 16 <= f.buf_len && ps[u] >= 0 && ps[u] < 65536;
+    int jj;
+    const double cc = pixel_coord(f, igbase + (i < nout ? i : 0), nseg, jj);
+    const long long ci = (long long)cc;
+    const double ph = __dmul_rn(cc - (double)ci, 65536.0);
+    const int ps = (int)ph;
+    const float alpha = __double2float_rn(ph - (double)ps);
+    const long long st = ci - 7;
+    const bool ok = i < nout && st >= 0 && st + 16 <= f.buf_len && ps >= 0 && ps < 65536;
+    if (i < nout && !ok && f.status) atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
+    double mine = 0.0;
+#pragma unroll 2
+    for (int p = 0; p < 8; ++p) {
+        const int src = grp * 8 + p;  // the group's p-th pixel
+        const long long pst = __shfl_sync(0xffffffffu, st, src);
+        const int pps = __shfl_sync(0xffffffffu, ps, src);
+        const float pal = __shfl_sync(0xffffffffu, alpha, src);
+        const bool pok = __shfl_sync(0xffffffffu, ok, src);
+        double part = 0.0;
+        if (pok) {
+            const float2 a = __ldg(reinterpret_cast<const float2*>(lut + (size_t)pps * 16) + k);
+            const float2 b = __ldg(reinterpret_cast<const float2*>(lut + (size_t)(pps + 1) * 16) + k);
+            const float* in = f.buf + pst + 2 * k;
+            const float x0 = __ldg(in), x1 = __ldg(in + 1);
+            const float w0 = fmaf(pal, b.x - a.x, a.x), w1 = fmaf(pal, b.y - a.y, a.y);
+            part = (double)(x0 * w0) + (double)(x1 * w1);
+        }
+        part += __shfl_xor_sync(0xffffffffu, part, 1);
+        part += __shfl_xor_sync(0xffffffffu, part, 2);
+        part += __shfl_xor_sync(0xffffffffu, part, 4);
+        if (k == p) mine = part;
     }
-#pragma unroll
-    for (int u = 0; u < kGatherPix; ++u) {
-        const long long i = i0 + (long long)u * kGatherThreads;
-        if (i >= nout) continue;
-        double acc = 0.0;
-        if (ok[u]) {
-            const float4* w0 = reinterpret_cast<const float4*>(lut + (size_t)ps[u] * 16);
-            const float* src = f.buf + st[u];
-            const float al = alpha[u];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float4 a = __ldg(w0 + q), b = __ldg(w0 + 4 + q);
-                const float wq[4] = {fmaf(al, b.x - a.x, a.x), fmaf(al, b.y - a.y, a.y),
-                                     fmaf(al, b.z - a.z, a.z), fmaf(al, b.w - a.w, a.w)};
-#pragma unroll
-                for (int tt = 0; tt < 4; ++tt) acc += (double)(__ldg(src + 4 * q + tt) * wq[tt]);
-            }
-        } else if (f.status) {
-            atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
-        }
-        const float out = (float)(f.seg_level[jj[u]] * acc);
-        if (f.out_f32) f.out_f32[i] = out;
-        if (f.out_u16) {
-            double v = (double)out * f.u16_scale + f.u16_offset + 0.5;
-            v = fmin(fmax(v, 0.0), 65535.0);
-            f.out_u16[i] = (uint16_t)(unsigned)v;
-        }
+    if (i >= nout) return;
+    const float out = (float)(f.seg_level[jj] * mine);
+    if (f.out_f32) f.out_f32[i] = out;
+    if (f.out_u16) {
+        double v = (double)out * f.u16_scale + f.u16_offset + 0.5;
+        v = fmin(fmax(v, 0.0), 65535.0);
+        f.out_u16[i] = (uint16_t)(unsigned)v;
     }
 }
 
@@ -232,7 +232,7 @@ cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout,
     wow_levels_kernel<<<nfields, kWowThreads, 0, stream>>>(dfields, threshold_mult);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const long long per_cta = (long long)kGatherThreads * kGatherPix;
+    const long long per_cta = kGatherThreads;
     const unsigned gx = (unsigned)((max_nout + per_cta - 1) / per_cta);
     for (int off = 0; off < nfields; off += 65535) {  // grid.y limit
         const int n = nfields - off < 65535 ? nfields - off : 65535;
