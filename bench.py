@@ -7,11 +7,10 @@ blocks and 600 fields.  One step = every block of the capture through the
 fused demodulator (all outputs: demod, demod_raw, demod_05, demod_burst,
 rfhpf, EFM, analog audio stage 1), the line locations of every field (GPU
 sync-run scan, native field chain, GPU H-sync / burst / pilot refinement)
-and every field through the TBC (uint16 4fsc fields).  With --chunks > 1
-the step runs in chunks of blocks: while the GPU demodulates chunk c+1, the
-host walks chunk c's fields and a higher-priority stream scans, refines and
-resamples them (the persistent demod kernel holds every SM, so the overlap
-is limited to the gaps between chunks).
+and every field through the TBC (uint16 4fsc fields).  The step runs in
+chunks of blocks (--chunks): while the GPU demodulates chunk c+1 (one CTA
+per block, so other streams' kernels get SMs between blocks), the host walks
+chunk c's fields and higher-priority streams scan, refine and resample them.
 
 Prints one JSON line (rank 0).  `--impl reference` times the CPU oracle (a
 numpy restatement of the reference's demodblock + scale_field) on the host
@@ -62,7 +61,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--chunks", type=int, default=1,
+    ap.add_argument("--chunks", type=int, default=4,
                     help="pipeline chunks of blocks per step (1: demod, then line locations, then TBC)")
     return ap.parse_args()
 
@@ -177,7 +176,8 @@ def run_gpu(args):
     levels = field_levels(rf)
     nchunks = max(1, min(args.chunks, nblocks // 64))
     bounds = [round(c * nblocks / nchunks) for c in range(nchunks + 1)]
-    streamB = torch.cuda.Stream(priority=-1)
+    streamB = torch.cuda.Stream(priority=-1)   # line locations
+    streamC = torch.cuda.Stream(priority=-1)   # TBC of ranges whose line locations are final
     elem = {k: v.element_size() for k, v in outs.items()}
     per_block = {k: (991 if k.startswith("audio") else U) for k in outs}
 
@@ -203,14 +203,15 @@ def run_gpu(args):
             streamB.wait_event(evs[c])
             loc.advance(bounds[c + 1], stream=streamB)
             # TBC of each range of fields as its line locations become final
-            # (on stream A, so it overlaps the NTSC burst chain's next range)
+            # (stream C: overlaps the NTSC burst chain's next range and the demod)
             while loc.ready and pics is not None:
                 lo, hi, ev = loc.ready.pop(0)
-                stream.wait_event(ev)
+                streamC.wait_event(ev)
                 tbc_fields(rf, tbc_batch(rf, loc.fields, outs["demod"].data_ptr(), pics.data_ptr(), levels,
-                                         first=lo, count=hi - lo), stream=sh)
+                                         first=lo, count=hi - lo), stream=streamC.cuda_stream)
         marks["demod_end"] = evs[-1]
         stream.wait_stream(streamB)
+        stream.wait_stream(streamC)
         end = torch.cuda.Event(enable_timing=True)
         end.record(stream)
         marks["end"] = end
@@ -248,6 +249,7 @@ def run_gpu(args):
     torch.cuda.synchronize()
     barrier()
     clocks = clk.stop()
+    rf.demod_status()  # raises if any block was skipped
     step_ms = [t_start[k].elapsed_time(t_end[k]) for k in range(args.steps)]
     demod_ms = [t_start[k].elapsed_time(t_demod[k]) for k in range(args.steps)]
     tail_ms = [t_demod[k].elapsed_time(t_end[k]) for k in range(args.steps)]

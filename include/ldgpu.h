@@ -154,6 +154,12 @@ int ldg_tbc_fields(ldg_ctx* ctx, const ldg_tbc_field* fields, int32_t nfields, v
 /* Wait for all work queued on the context's stream. */
 int ldg_synchronize(ldg_ctx* ctx);
 
+/* Sticky error bits of the context's demodulator launches since the last
+ * call (cleared by reading): LDG_ERR_CUDA with flags = 1 when a block gave up
+ * waiting for its scratch slot and was skipped.  Synchronous.  No
+ * counterpart in the reference. */
+int ldg_demod_status(ldg_ctx* ctx, int32_t* flags);
+
 /* Device scratch the demodulator uses for a batch of `nblocks` blocks
  * (bytes; parked spectra, one slot per resident CTA). */
 int ldg_demod_scratch_bytes(ldg_ctx* ctx, int64_t nblocks, int64_t* bytes);

@@ -86,7 +86,8 @@ struct ldg_ctx {
     size_t ll_cap = 0;
     int* d_status = nullptr;
     void* d_lines = nullptr;  // sync-run scan scratch (ldg_sync_runs)
-    int* d_counter = nullptr; // demod block counter (dynamic block hand-out)
+    int* d_slots = nullptr;   // demod scratch-slot locks (nslots) and the error word after them
+    int nslots = 0;
     size_t lines_cap = 0;
     std::mutex mu;
 };
@@ -193,7 +194,7 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     cudaFree(c->d_ll);
     cudaFree(c->d_status);
     cudaFree(c->d_lines);
-    cudaFree(c->d_counter);
+    cudaFree(c->d_slots);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -280,9 +281,16 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     DeviceGuard g(c->device);
     cudaStream_t st = a->stream ? (cudaStream_t)a->stream : c->stream;
     const long long nb = a->nblocks;
-    const int grid = (int)(nb < c->sms ? nb : c->sms);
-    int rc = grow((void**)&c->d_scratch, &c->scratch_bytes, (size_t)grid * ldg::kScratchPerCta);
+    // one CTA per block; scratch slots for twice the SMs' worth of resident CTAs
+    const int nslots = 2 * c->sms;
+    const int grid = (int)nb;
+    int rc = grow((void**)&c->d_scratch, &c->scratch_bytes, (size_t)nslots * ldg::kScratchPerCta);
     if (rc) return rc;
+    if (!c->d_slots) {
+        LDG_CK(cudaMalloc(&c->d_slots, (nslots + 1) * sizeof(int)));
+        LDG_CK(cudaMemset(c->d_slots, 0, (nslots + 1) * sizeof(int)));
+        c->nslots = nslots;
+    }
 
     // host/device placement of every buffer; host ones go through the arena
     const size_t esz = a->in_kind == LDG_IN_INT16 ? 2 : 4;
@@ -370,9 +378,10 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     p.scratch = c->d_scratch;
     p.tw16 = c->d_tw16;
     p.tw32 = c->d_tw32;
-    if (!c->d_counter) LDG_CK(cudaMalloc(&c->d_counter, sizeof(int)));
-    LDG_CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), st));
-    p.work_counter = c->d_counter;
+    LDG_CK(cudaMemsetAsync(c->d_slots, 0, c->nslots * sizeof(int), st));
+    p.slot_lock = c->d_slots;
+    p.nslots = c->nslots;
+    p.error = c->d_slots + c->nslots;
 
     cudaError_t e = ldg::launch_demod(p, grid, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("demod launch: ") + cudaGetErrorString(e));
@@ -509,6 +518,19 @@ int ldg_synchronize(ldg_ctx* c) {
     if (!c) return fail(LDG_ERR_ARG, "ldg_synchronize: NULL context");
     DeviceGuard g(c->device);
     LDG_CK(cudaStreamSynchronize(c->stream));
+    return LDG_OK;
+}
+
+int ldg_demod_status(ldg_ctx* c, int32_t* flags) {
+    if (!c || !flags) return fail(LDG_ERR_ARG, "ldg_demod_status: NULL argument");
+    *flags = 0;
+    if (!c->d_slots) return LDG_OK;
+    DeviceGuard g(c->device);
+    int v = 0;
+    LDG_CK(cudaMemcpy(&v, c->d_slots + c->nslots, sizeof(int), cudaMemcpyDeviceToHost));
+    if (v) LDG_CK(cudaMemset(c->d_slots + c->nslots, 0, sizeof(int)));
+    *flags = v;
+    if (v) return fail(LDG_ERR_CUDA, "demod: a block gave up waiting for a scratch slot and was skipped");
     return LDG_OK;
 }
 

@@ -219,15 +219,29 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
     t.s4 = s4;
     __syncthreads();
 
-    __shared__ int s_next;
-    int blk = blockIdx.x;
-    if (p.work_counter) {
-        if (threadIdx.x == 0) s_next = atomicAdd(p.work_counter, 1);
+    __shared__ int s_got;
+    const bool per_block = p.slot_lock != nullptr;
+    const int slot = per_block ? (int)(blockIdx.x % (unsigned)p.nslots) : (int)blockIdx.x;
+    if (per_block) {
+        if (threadIdx.x == 0) {
+            int got = 0;
+            for (int tries = 0; tries < (1 << 22); ++tries) {
+                if (atomicCAS(p.slot_lock + slot, 0, 1) == 0) {
+                    got = 1;
+                    break;
+                }
+                __nanosleep(256);
+            }
+            if (!got) atomicOr(p.error, kDemodErrSlotWait);
+            __threadfence();
+            s_got = got;
+        }
         __syncthreads();
-        blk = s_next;
+        if (!s_got) return;
     }
+    int blk = blockIdx.x;
     while (blk < p.nblocks) {
-        float2* parkX = p.scratch + (size_t)blockIdx.x * 2 * kM;
+        float2* parkX = p.scratch + (size_t)slot * 2 * kM;
         float2* parkZ = parkX + kM;
 
         // ---- input spectrum X (first pass reads the block), parked; audio taps; rfhpf input
@@ -311,13 +325,15 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
                          RealStorer{p.o_video[o] + (long long)blk * p.s_video.len, p.s_video.start, p.s_video.len,
                                     p.roll[o]});
         }
-        if (p.work_counter) {
-            __syncthreads();
-            if (threadIdx.x == 0) s_next = atomicAdd(p.work_counter, 1);
-            __syncthreads();
-            blk = s_next;
-        } else {
-            blk += gridDim.x;
+        if (per_block) break;
+        blk += gridDim.x;
+    }
+    if (per_block) {
+        // every thread is done with the slot's scratch before it is handed on
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicExch(p.slot_lock + slot, 0);
         }
     }
 }

@@ -53,11 +53,19 @@ struct DemodParams {
     const float2* tw16;     // W_16384^i, i < 16384
     const float2* tw32;     // W_32768^k, k <= 8192
 
-    // blocks handed out one at a time from this counter (zero at launch), so
-    // CTAs that start late -- SMs busy with another stream's kernels -- take
-    // fewer blocks; nullptr: CTA i takes blocks i, i + grid, ...
-    int* work_counter;
+    // Scheduling.  slot_lock == nullptr: persistent CTAs, CTA i takes blocks
+    // i, i + grid, ... with scratch slot i.  Otherwise one CTA per block
+    // (grid = nblocks), so kernels of other streams get SMs between blocks;
+    // CTA b works in scratch slot b % nslots, which it holds under
+    // slot_lock[slot] (0 free, 1 held) for the block's duration.  A wait for
+    // a slot gives up after a bounded number of tries, sets *error and skips
+    // the block (never seen in practice: nslots exceeds the resident CTAs).
+    int* slot_lock;
+    int nslots;
+    int* error;
 };
+
+constexpr int kDemodErrSlotWait = 1;
 
 // Dynamic shared memory the kernel needs.
 constexpr int kSmemFloat2 = (16384 + 1024) + 2 * (1024 + 64) + 4 * 16 + 4 * 256 + 4096;

@@ -128,6 +128,7 @@ SIGNATURES = {
                                           ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_i32, c_i64, c_i64]),
     "ldg_lines_scratch_bytes": (c_i64, [c_i32]),
     "ldg_abi_sizeof": (c_i64, [ctypes.c_char_p]),
+    "ldg_demod_status": (ctypes.c_int, [c_p, ctypes.POINTER(c_i32)]),
     "ldg_lines_refine": (ctypes.c_int, [c_p, ctypes.POINTER(LinesArgs)]),
     "ldg_ac3_last_error": (ctypes.c_char_p, []),
     "ldg_ac3_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int32, c_p, ctypes.c_int32, c_p,

@@ -403,6 +403,12 @@ class RFDecode(RFParams):
         }
         return dec, emp
 
+    def demod_status(self):
+        """Raise if a demodulator block was skipped since the last check
+        (a wait for its scratch slot gave up); synchronous."""
+        flags = ctypes.c_int32(0)
+        L.check(self._ctx._lib.ldg_demod_status(self._ctx.handle, ctypes.byref(flags)))
+
     def synchronize(self):
         """Wait for the work queued on the context's own stream."""
         L.check(self._ctx._lib.ldg_synchronize(self._ctx.handle))

@@ -110,6 +110,7 @@ def test_batched_equals_plain(rf):
     rf.demod_blocks_device(dcap.data_ptr(), nb, U, {k: v.data_ptr() for k, v in outs.items()},
                            mtf_level=1, cut=True)
     rf.synchronize()
+    rf.demod_status()  # no block skipped
     for b in range(nb):
         plain = rf.demodblock(data=cap[b * U:b * U + rf.blocklen], mtf_level=1, cut=True)
         for k in keys:
