@@ -239,8 +239,10 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
         __syncthreads();
         if (!s_got) return;
     }
-    int blk = blockIdx.x;
-    while (blk < p.nblocks) {
+    int blk = per_block ? (int)blockIdx.x * p.blocks_per_cta : (int)blockIdx.x;
+    const int blk_end = per_block ? min(blk + p.blocks_per_cta, p.nblocks) : p.nblocks;
+    const int blk_step = per_block ? 1 : (int)gridDim.x;
+    while (blk < blk_end) {
         float2* parkX = p.scratch + (size_t)slot * 2 * kM;
         float2* parkZ = parkX + kM;
 
@@ -325,8 +327,7 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
                          RealStorer{p.o_video[o] + (long long)blk * p.s_video.len, p.s_video.start, p.s_video.len,
                                     p.roll[o]});
         }
-        if (per_block) break;
-        blk += gridDim.x;
+        blk += blk_step;
     }
     if (per_block) {
         // every thread is done with the slot's scratch before it is handed on

@@ -54,15 +54,16 @@ struct DemodParams {
     const float2* tw32;     // W_32768^k, k <= 8192
 
     // Scheduling.  slot_lock == nullptr: persistent CTAs, CTA i takes blocks
-    // i, i + grid, ... with scratch slot i.  Otherwise one CTA per block
-    // (grid = nblocks), so kernels of other streams get SMs between blocks;
-    // CTA b works in scratch slot b % nslots, which it holds under
-    // slot_lock[slot] (0 free, 1 held) for the block's duration.  A wait for
+    // i, i + grid, ... with scratch slot i.  Otherwise CTA i works through
+    // blocks [i * blocks_per_cta, (i + 1) * blocks_per_cta), so kernels of
+    // other streams get SMs between CTAs; it works in scratch slot
+    // i % nslots, which it holds under slot_lock[slot] (0 free, 1 held).  A wait for
     // a slot gives up after a bounded number of tries, sets *error and skips
     // the block (never seen in practice: nslots exceeds the resident CTAs).
     int* slot_lock;
     int nslots;
     int* error;
+    int blocks_per_cta;   // per-slot mode: consecutive blocks a CTA works through
 };
 
 constexpr int kDemodErrSlotWait = 1;
