@@ -62,6 +62,19 @@ double median_of(std::vector<double> v) {
 
 struct Timings {
     double hsync_lo, hsync_hi, eq_lo, eq_hi, vsync_lo, vsync_hi;
+    // the same ranges for integer pulse lengths: len >= lo <=> len >= ceil(lo)
+    long long ih_lo, ih_hi, ieq_lo, ieq_hi, iv_lo, iv_hi;
+    void integerise() {
+        ih_lo = (long long)std::ceil(hsync_lo);
+        ih_hi = (long long)std::floor(hsync_hi);
+        ieq_lo = (long long)std::ceil(eq_lo);
+        ieq_hi = (long long)std::floor(eq_hi);
+        iv_lo = (long long)std::ceil(vsync_lo);
+        iv_hi = (long long)std::floor(vsync_hi);
+    }
+    bool is_h(long long len) const { return len >= ih_lo && len <= ih_hi; }
+    bool is_eq(long long len) const { return len >= ieq_lo && len <= ieq_hi; }
+    bool is_v(long long len) const { return len >= iv_lo && len <= iv_hi; }
 };
 
 struct VBlank {
@@ -77,19 +90,48 @@ struct VBlank {
     }
 };
 
+// Integer spacing bounds equivalent to inrange(d / inlinelen, lo, hi) for
+// integer d: d / L is monotonic in d, so the smallest d whose quotient
+// reaches lo and the largest whose quotient stays <= hi decide it exactly.
+struct SpacingBounds {
+    long long lo, hi;
+};
+
+SpacingBounds spacing_bounds(double L, double lo, double hi) {
+    long long a = (long long)std::floor(lo * L) - 2;
+    while ((double)a / L < lo) ++a;
+    while ((double)(a - 1) / L >= lo) --a;
+    long long b = (long long)std::ceil(hi * L) + 2;
+    while ((double)b / L > hi) --b;
+    while ((double)(b + 1) / L <= hi) ++b;
+    return {a, b};
+}
+
 class FieldPulses {
 public:
-    FieldPulses(const LdgChainParams& P, std::vector<Pulse> raw) : P(P), raw(std::move(raw)) {}
+    FieldPulses(const LdgChainParams& P, std::vector<Pulse> raw) : P(P), raw(std::move(raw)) {
+        q_eq = spacing_bounds(P.inlinelen, 0.4, 0.6);
+        q_h = spacing_bounds(P.inlinelen, 0.9, 1.1);
+        q_mix = spacing_bounds(P.inlinelen, 0.4, 1.1);
+    }
 
     double usectoinpx(double x) const { return x * P.linefreq0; }
 
     Timings get_timings() const {
         const double lo = usectoinpx(P.hsync_pulse_us - 1.75), hi = usectoinpx(P.hsync_pulse_us + 2);
-        std::vector<double> hl;
+        // integer lengths within [lo, hi]: len >= ceil(lo), len <= floor(hi)
+        const long long ilo = (long long)std::ceil(lo), ihi = (long long)std::floor(hi);
+        std::vector<long long> hl;
         hl.reserve(raw.size());
         for (const Pulse& p : raw)
-            if (inrange((double)p.len, lo, hi)) hl.push_back((double)p.len);
-        const double med = hl.empty() ? P.hsync_pulse_us : median_of(hl);
+            if (p.len >= ilo && p.len <= ihi) hl.push_back(p.len);
+        double med = P.hsync_pulse_us;
+        if (!hl.empty()) {
+            const size_t n = hl.size();
+            std::nth_element(hl.begin(), hl.begin() + n / 2, hl.end());
+            const double h = (double)hl[n / 2];
+            med = (n % 2) ? h : ((double)*std::max_element(hl.begin(), hl.begin() + n / 2) + h) / 2.0;
+        }
         const double off = med - usectoinpx(P.hsync_pulse_us);
         Timings t;
         t.hsync_lo = med + usectoinpx(-0.5);
@@ -98,24 +140,20 @@ public:
         t.eq_hi = usectoinpx(P.eq_pulse_us + 0.5) + off;
         t.vsync_lo = usectoinpx(P.vsync_pulse_us * 0.5) + off;
         t.vsync_hi = usectoinpx(P.vsync_pulse_us + 1) + off;
+        t.integerise();
         return t;
     }
 
+    // pulse_qualitycheck (core.py:1803-1823): the spacing to the previous
+    // valid pulse, in lines, within 0.4-0.6 (both blanking pulses), 0.9-1.1
+    // (both H-sync) or 0.4-1.1
     bool qualitycheck(const VPulse& prev, int type, const Pulse& p) const {
-        double lo, hi;
-        if (prev.type > 0 && type > 0) {
-            lo = 0.4;
-            hi = 0.6;
-        } else if (prev.type == 0 && type == 0) {
-            lo = 0.9;
-            hi = 1.1;
-        } else {
-            lo = 0.4;
-            hi = 1.1;
-        }
-        const double linelen = (double)(p.start - prev.p.start) / P.inlinelen;
-        return inrange(linelen, lo, hi);
+        const SpacingBounds& q = (prev.type > 0 && type > 0) ? q_eq : (prev.type == 0 && type == 0) ? q_h : q_mix;
+        const long long d = p.start - prev.p.start;
+        return d >= q.lo && d <= q.hi;
     }
+
+    SpacingBounds q_eq, q_h, q_mix;
 
     // core.py:1825-1911
     bool vblank_state_machine(size_t from, size_t to, const Timings& LT, std::vector<VPulse>& valid) const {
@@ -127,9 +165,9 @@ public:
             const Pulse& p = raw[k];
             int stype = -1;
             const int state = valid.empty() ? -1 : valid.back().type;
-            const bool is_h = inrange((double)p.len, LT.hsync_lo, LT.hsync_hi);
-            const bool is_eq = inrange((double)p.len, LT.eq_lo, LT.eq_hi);
-            const bool is_v = inrange((double)p.len, LT.vsync_lo, LT.vsync_hi);
+            const bool is_h = LT.is_h(p.len);
+            const bool is_eq = LT.is_eq(p.len);
+            const bool is_v = LT.is_v(p.len);
             if (state == -1) {
                 if (is_h) stype = HSYNC;
             } else if (state == HSYNC) {
@@ -180,13 +218,14 @@ public:
         size_t i = 0;
         while (i < raw.size()) {
             const Pulse& cur = raw[i];
-            if (inrange((double)cur.len, LT.hsync_lo, LT.hsync_hi)) {
+            if (LT.is_h(cur.len)) {
                 const bool good = valid.empty() ? false : qualitycheck(valid.back(), HSYNC, cur);
                 valid.push_back({HSYNC, cur, good});
                 i += 1;
-            } else if (i > 2 && inrange((double)cur.len, LT.eq_lo, LT.eq_hi) && !valid.empty() &&
+            } else if (i > 2 && LT.is_eq(cur.len) && !valid.empty() &&
                        valid.back().type == HSYNC) {
                 std::vector<VPulse> vb;
+                vb.reserve(32);
                 const bool done = vblank_state_machine(i - 2, std::min(raw.size(), i + 24), LT, vb);
                 if (done) {
                     for (size_t k = 2; k < vb.size(); ++k) valid.push_back(vb[k]);
@@ -344,16 +383,16 @@ public:
             lr0 = c0;
             lr1 = c1;
         }
-        double sum = 0;
-        long long cnt = 0;
+        const SpacingBounds q = spacing_bounds(P.inlinelen, 0.95, 1.05);
+        long long sum = 0, cnt = 0;
         for (int i = lr0 + 1; i < lr0 + lr1; ++i) {
             const long long ll = vp[i].p.start - vp[i - 1].p.start;
-            if (inrange((double)ll / P.inlinelen, 0.95, 1.05)) {
-                sum += (double)ll;
+            if (ll >= q.lo && ll <= q.hi) {
+                sum += ll;
                 cnt += 1;
             }
         }
-        return cnt ? sum / (double)cnt : P.inlinelen;
+        return cnt ? (double)sum / (double)cnt : P.inlinelen;
     }
 
     const LdgChainParams& P;
@@ -387,7 +426,13 @@ Slots line_slots(const LdgChainParams& P, const std::vector<VPulse>& vp, const s
     std::vector<double> linelocs(proclines, -1.0);
     std::vector<double> ll_dist(proclines, 0.0);
     std::vector<unsigned char> have(proclines, 0);
-    for (const VPulse& p : vp) {
+    // only pulses within two lines of the slots can land in one (the skip rule
+    // only moves a pulse to a later slot); the valid pulses are in time order
+    const double s_lo = line0loc - 2.0 * meanlinelen, s_hi = line0loc + (proclines + 2.0) * meanlinelen;
+    const auto first = std::lower_bound(vp.begin(), vp.end(), s_lo,
+                                        [](const VPulse& a, double v) { return (double)a.p.start < v; });
+    for (auto it = first; it != vp.end() && (double)it->p.start <= s_hi; ++it) {
+        const VPulse& p = *it;
         double lineloc = ((double)p.p.start - line0loc) / meanlinelen;
         long long rlineloc = nround(lineloc);
         double dist = std::fabs(lineloc - (double)rlineloc);

@@ -404,6 +404,22 @@ class LineLocator:
         import os
         self.threads = max(1, min(16, os.cpu_count() or 1))
 
+    def _pinned(self, nbytes):
+        """A pinned host block from a ring of four; a block is reused once
+        the copy that last read it has completed."""
+        torch = self.torch
+        if not hasattr(self, "_pin_ring"):
+            self._pin_ring = [[None, None] for _ in range(4)]
+            self._pin_next = 0
+        slot = self._pin_ring[self._pin_next % 4]
+        self._pin_next = self._pin_next % 4 + 1
+        if slot[1] is not None:
+            slot[1].synchronize()
+        if slot[0] is None or slot[0].numel() < nbytes:
+            slot[0] = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8).pin_memory()
+        slot[1] = torch.cuda.Event()
+        return slot[0][:nbytes]
+
     def _tick(self, key, t0):
         t = time.perf_counter()
         self.timing[key] = self.timing.get(key, 0.0) + (t - t0) * 1e3
@@ -445,7 +461,7 @@ class LineLocator:
         nb_i = 2 * nf * 8 + 3 * nf * 4
         nb_i = (nb_i + 7) // 8 * 8
         total = nb_i + nf * ml * 8 + nf * ml
-        hbuf = torch.empty(total, dtype=torch.uint8).pin_memory()
+        hbuf = self._pinned(total)
         hb = hbuf.numpy()
         i64 = hb[:2 * nf * 8].view(np.int64).reshape(2, nf)
         i64[0] = plans.startloc
@@ -456,7 +472,9 @@ class LineLocator:
         i32[2] = plans.has_prev
         hb[nb_i:nb_i + nf * ml * 8].view(np.float64).reshape(nf, ml)[:] = plans.linelocs1
         hb[nb_i + nf * ml * 8:].reshape(nf, ml)[:] = plans.linebad
-        dbuf = hbuf.to(dev, non_blocking=True)
+        dbuf = torch.empty(total, dtype=torch.uint8, device=dev)
+        dbuf.copy_(hbuf, non_blocking=True)
+        self._pin_ring[self._pin_next - 1][1].record()
         base = dbuf.data_ptr()
         out_ll = torch.empty((nf, ml), dtype=torch.float64, device=dev)
         out_bad = torch.empty((nf, ml), dtype=torch.uint8, device=dev)
