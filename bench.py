@@ -139,7 +139,7 @@ def run_gpu(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     from ldgpu import RFDecode
-    from ldgpu.field import tbc_fields
+    from ldgpu.field import tbc_fields, tbc_status
     from ldgpu.fieldread import blocks_in_capture
     from ldgpu.lines import LineLocator, field_levels, tbc_batch
     from ldgpu.synth import synth_capture
@@ -208,7 +208,7 @@ def run_gpu(args):
                 lo, hi, ev = loc.ready.pop(0)
                 streamC.wait_event(ev)
                 tbc_fields(rf, tbc_batch(rf, loc.fields, outs["demod"].data_ptr(), pics.data_ptr(), levels,
-                                         first=lo, count=hi - lo), stream=streamC.cuda_stream)
+                                         first=lo, count=hi - lo), stream=streamC.cuda_stream, asynchronous=True)
         marks["demod_end"] = evs[-1]
         stream.wait_stream(streamB)
         stream.wait_stream(streamC)
@@ -250,6 +250,7 @@ def run_gpu(args):
     barrier()
     clocks = clk.stop()
     rf.demod_status()  # raises if any block was skipped
+    tbc_status(rf)     # raises if a TBC tap fell outside its field buffer
     step_ms = [t_start[k].elapsed_time(t_end[k]) for k in range(args.steps)]
     demod_ms = [t_start[k].elapsed_time(t_demod[k]) for k in range(args.steps)]
     tail_ms = [t_demod[k].elapsed_time(t_end[k]) for k in range(args.steps)]

@@ -151,6 +151,18 @@ int ldg_demod_blocks(ldg_ctx* ctx, const ldg_demod_args* args);
  * core.py:2691-2713). */
 int ldg_tbc_fields(ldg_ctx* ctx, const ldg_tbc_field* fields, int32_t nfields, void* stream);
 
+/* ldg_tbc_fields for device-resident buffers without waiting: enqueues on
+ * `stream` and returns (the descriptors go through one of four pinned
+ * workspaces, reused once their launch has completed).  Taps outside a
+ * field buffer are reported later by ldg_tbc_status.  Calls on one context
+ * must use one stream.  No counterpart in the reference. */
+int ldg_tbc_fields_async(ldg_ctx* ctx, const ldg_tbc_field* fields, int32_t nfields, void* stream);
+
+/* Sticky TBC error bits since the last call (cleared by reading);
+ * LDG_ERR_RANGE / LDG_ERR_ARG as ldg_tbc_fields would have returned.
+ * Synchronous.  No counterpart in the reference. */
+int ldg_tbc_status(ldg_ctx* ctx, int32_t* flags);
+
 /* Wait for all work queued on the context's stream. */
 int ldg_synchronize(ldg_ctx* ctx);
 

@@ -88,6 +88,18 @@ struct ldg_ctx {
     void* d_lines = nullptr;  // sync-run scan scratch (ldg_sync_runs)
     int* d_slots = nullptr;   // demod scratch-slot locks (nslots) and the error word after them
     int nslots = 0;
+    // ldg_tbc_fields_async workspaces, used in turn; a workspace is reused once
+    // the launch that last used it has completed
+    struct TbcWs {
+        ldg::TbcField* d_fields = nullptr;
+        ldg::TbcField* h_fields = nullptr;  // pinned
+        int cap = 0;
+        double* d_seg = nullptr;
+        size_t seg_cap = 0;
+        cudaEvent_t done = nullptr;
+        bool used = false;
+    } tws[4];
+    int tws_next = 0;
     size_t lines_cap = 0;
     std::mutex mu;
 };
@@ -195,6 +207,13 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     cudaFree(c->d_status);
     cudaFree(c->d_lines);
     cudaFree(c->d_slots);
+    for (auto& w : c->tws) {
+        if (w.used) cudaEventSynchronize(w.done);
+        cudaFree(w.d_fields);
+        cudaFreeHost(w.h_fields);
+        cudaFree(w.d_seg);
+        if (w.done) cudaEventDestroy(w.done);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -513,6 +532,96 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         return fail(LDG_ERR_RANGE, "ldg_tbc_fields: a resampling tap fell outside the field buffer (those pixels are 0)");
     }
     (void)any_host;
+    return LDG_OK;
+}
+
+int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, void* stream) {
+    if (!c || (!fields && nfields)) return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: NULL argument");
+    if (nfields < 0) return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: negative field count");
+    if (nfields == 0) return LDG_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->d_lut) return fail(LDG_ERR_STATE, "ldg_tbc_fields_async: sinc table not set");
+    size_t seg_total = 0;
+    long long max_nout = 0;
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_tbc_field& f = fields[i];
+        if (!f.buf || !f.linelocs) return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: NULL buffer");
+        if (f.nlines < 2 || f.nlines > 513) return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: nlines must be in [2, 513]");
+        if (f.outwidth <= 0 || f.linesout <= 0 || f.outlinecount <= 0 || f.lineoffset < 0 || f.buf_len <= 0)
+            return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: bad field geometry");
+        if (!(f.inlinelen > 0) || !(f.outlinelen > 0) || !(f.hz_ire != 0))
+            return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: bad line length or level");
+        if (f.outlinelen != (double)(int)f.outlinelen)
+            return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: outlinelen must be an integer");
+        if (!f.out_f32 && !f.out_u16) return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: no output");
+        seg_total += f.nlines - 1;
+        if ((long long)f.linesout * f.outwidth > max_nout) max_nout = (long long)f.linesout * f.outwidth;
+    }
+    DeviceGuard g(c->device);
+    // every buffer must already be device memory (checked on the first field's
+    // pointers; the batched callers allocate all fields alike)
+    const ldg_tbc_field& f0 = fields[0];
+    if (!is_device_ptr(f0.buf) || !is_device_ptr(f0.linelocs) || (f0.out_f32 && !is_device_ptr(f0.out_f32)) ||
+        (f0.out_u16 && !is_device_ptr(f0.out_u16)))
+        return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: buffers must be device memory");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    auto& w = c->tws[c->tws_next];
+    c->tws_next = (c->tws_next + 1) % 4;
+    if (w.used) LDG_CK(cudaEventSynchronize(w.done));
+    if (!w.done) LDG_CK(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming));
+    if (nfields > w.cap) {
+        cudaFree(w.d_fields);
+        cudaFreeHost(w.h_fields);
+        w.d_fields = nullptr;
+        w.h_fields = nullptr;
+        w.cap = 0;
+        LDG_CK(cudaMalloc(&w.d_fields, nfields * sizeof(ldg::TbcField)));
+        LDG_CK(cudaMallocHost(&w.h_fields, nfields * sizeof(ldg::TbcField)));
+        w.cap = nfields;
+    }
+    int rc = grow((void**)&w.d_seg, &w.seg_cap, seg_total * sizeof(double));
+    if (rc) return rc;
+    size_t sego = 0;
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_tbc_field& f = fields[i];
+        ldg::TbcField& d = w.h_fields[i];
+        d.buf = f.buf;
+        d.buf_len = f.buf_len;
+        d.linelocs = f.linelocs;
+        d.nlines = f.nlines;
+        d.lineoffset = f.lineoffset;
+        d.outwidth = f.outwidth;
+        d.linesout = f.linesout;
+        d.nwow = (long long)(f.outlinecount + f.lineoffset + 1) * (long long)f.outlinelen;
+        d.coord_f32 = f.coord_f32;
+        d.inlinelen = f.inlinelen;
+        d.outscale = f.inlinelen / f.outlinelen;
+        d.inv_inl = 1.0 / f.inlinelen;
+        d.u16_scale = f.out_scale / f.hz_ire;
+        d.u16_offset = f.output_zero - f.vsync_ire * f.out_scale - f.ire0 * d.u16_scale;
+        d.seg_level = w.d_seg + sego;
+        d.status = c->d_status;
+        d.out_f32 = f.out_f32;
+        d.out_u16 = f.out_u16;
+        sego += f.nlines - 1;
+    }
+    LDG_CK(cudaMemcpyAsync(w.d_fields, w.h_fields, nfields * sizeof(ldg::TbcField), cudaMemcpyHostToDevice, st));
+    cudaError_t e = ldg::launch_tbc(w.d_fields, nfields, max_nout, c->d_lut, 15.0, st);
+    if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
+    LDG_CK(cudaEventRecord(w.done, st));
+    w.used = true;
+    return LDG_OK;
+}
+
+int ldg_tbc_status(ldg_ctx* c, int32_t* flags) {
+    if (!c || !flags) return fail(LDG_ERR_ARG, "ldg_tbc_status: NULL argument");
+    DeviceGuard g(c->device);
+    int status = 0;
+    LDG_CK(cudaMemcpy(&status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) LDG_CK(cudaMemset(c->d_status, 0, sizeof(int)));
+    *flags = status;
+    if (status & ldg::LDG_TBC_BAD_LINES) return fail(LDG_ERR_ARG, "TBC: too many lines for the wow statistics");
+    if (status) return fail(LDG_ERR_RANGE, "TBC: a resampling tap fell outside the field buffer (those pixels are 0)");
     return LDG_OK;
 }
 

@@ -40,11 +40,21 @@ def tbc_descriptor(rf, buf, linelocs, lineoffset, outwidth, linesout, outlinecou
     return d
 
 
-def tbc_fields(rf, descs, stream=None):
-    """Run ldg_tbc_fields on a list (or prebuilt ctypes array) of descriptors."""
+def tbc_fields(rf, descs, stream=None, asynchronous=False):
+    """Run ldg_tbc_fields on a list (or prebuilt ctypes array) of descriptors;
+    asynchronous=True: ldg_tbc_fields_async (device buffers only; errors come
+    from tbc_status)."""
     rf._load_lut()
     arr = descs if isinstance(descs, ctypes.Array) else (L.TbcField * len(descs))(*descs)
-    L.check(rf._ctx._lib.ldg_tbc_fields(rf._ctx.handle, arr, len(arr), stream))
+    fn = rf._ctx._lib.ldg_tbc_fields_async if asynchronous else rf._ctx._lib.ldg_tbc_fields
+    L.check(fn(rf._ctx.handle, arr, len(arr), stream))
+
+
+def tbc_status(rf):
+    """Raise if an asynchronous TBC batch hit a tap outside its field buffer
+    (or had too many lines) since the last check; synchronous."""
+    flags = ctypes.c_int32(0)
+    L.check(rf._ctx._lib.ldg_tbc_status(rf._ctx.handle, ctypes.byref(flags)))
 
 
 class Field(FieldLogic):

@@ -129,6 +129,8 @@ SIGNATURES = {
     "ldg_lines_scratch_bytes": (c_i64, [c_i32]),
     "ldg_abi_sizeof": (c_i64, [ctypes.c_char_p]),
     "ldg_demod_status": (ctypes.c_int, [c_p, ctypes.POINTER(c_i32)]),
+    "ldg_tbc_fields_async": (ctypes.c_int, [c_p, c_p, c_i32, c_p]),
+    "ldg_tbc_status": (ctypes.c_int, [c_p, ctypes.POINTER(c_i32)]),
     "ldg_lines_refine": (ctypes.c_int, [c_p, ctypes.POINTER(LinesArgs)]),
     "ldg_ac3_last_error": (ctypes.c_char_p, []),
     "ldg_ac3_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int32, c_p, ctypes.c_int32, c_p,

@@ -93,7 +93,7 @@ def test_tbc_from_batched_linelocs(capture):
     """TBC through tbc_batch over the batched line locations equals TBC with
     the host line locations."""
     import torch
-    from ldgpu.field import tbc_descriptor, tbc_fields
+    from ldgpu.field import tbc_descriptor, tbc_fields, tbc_status
     from ldgpu.lines import field_levels, tbc_batch
     rf, arrays, host, nb, ref = capture
     fields = LineLocator(rf).locate(arrays, nb)
@@ -110,7 +110,10 @@ def test_tbc_from_batched_linelocs(capture):
         db.append(tbc_descriptor(rf, buf, hl[i].data_ptr(), f.lineoffset, outw, outl, outl, levels,
                                  out_u16=b[i].data_ptr(), buf_len=w.length, nlines=len(hl[i])))
     torch.cuda.synchronize()
-    tbc_fields(rf, tbc_batch(rf, fields, arrays["demod"].data_ptr(), a.data_ptr(), levels))
+    # the batched, non-waiting entry point for one; the per-field one for the other
+    tbc_fields(rf, tbc_batch(rf, fields, arrays["demod"].data_ptr(), a.data_ptr(), levels), asynchronous=True)
+    rf.synchronize()
+    tbc_status(rf)
     tbc_fields(rf, db)
     rf.synchronize()
     pa = a.cpu().numpy().view(np.uint16).astype(int)
