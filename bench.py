@@ -178,6 +178,7 @@ def run_gpu(args):
     bounds = [round(c * nblocks / nchunks) for c in range(nchunks + 1)]
     streamB = torch.cuda.Stream(priority=-1)   # line locations
     streamC = torch.cuda.Stream(priority=-1)   # TBC of ranges whose line locations are final
+    streamS = torch.cuda.Stream(priority=-1)   # sync-run scans
     elem = {k: v.element_size() for k, v in outs.items()}
     per_block = {k: (991 if k.startswith("audio") else U) for k in outs}
 
@@ -201,7 +202,8 @@ def run_gpu(args):
             evs.append(ev)
         for c in range(nchunks):
             streamB.wait_event(evs[c])
-            loc.advance(bounds[c + 1], stream=streamB)
+            streamS.wait_event(evs[c])
+            loc.advance(bounds[c + 1], stream=streamB, scan_stream=streamS)
             # TBC of each range of fields as its line locations become final
             # (stream C: overlaps the NTSC burst chain's next range and the demod)
             while loc.ready and pics is not None:
@@ -212,6 +214,7 @@ def run_gpu(args):
         marks["demod_end"] = evs[-1]
         stream.wait_stream(streamB)
         stream.wait_stream(streamC)
+        stream.wait_stream(streamS)
         end = torch.cuda.Event(enable_timing=True)
         end.record(stream)
         marks["end"] = end

@@ -302,7 +302,7 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     const long long nb = a->nblocks;
     // one CTA per block; scratch slots for twice the SMs' worth of resident CTAs
     const int nslots = 2 * c->sms;
-    const int per_cta = nb >= 16 * c->sms ? 4 : 1;  // a few blocks per CTA amortise its set-up
+    const int per_cta = nb >= 16 * c->sms ? 2 : 1;  // two blocks per CTA amortise its set-up
     const int grid = (int)((nb + per_cta - 1) / per_cta);
     int rc = grow((void**)&c->d_scratch, &c->scratch_bytes, (size_t)nslots * ldg::kScratchPerCta);
     if (rc) return rc;

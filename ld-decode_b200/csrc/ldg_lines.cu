@@ -184,27 +184,32 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const float* _
     }
 }
 
-// one warp per run: pair edges 2r (start) and 2r+1 (end), interior mean of long runs
-__global__ void run_pair_kernel(const long long* __restrict__ edges, long long nruns, const float* __restrict__ x,
-                                long long min_long, long long trim_lo, long long trim_hi,
-                                long long* __restrict__ rs, long long* __restrict__ rl, double* __restrict__ rm) {
-    const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// one warp per run: pair edges 2r (start) and 2r+1 (end), interior mean of long
+// runs; the run count is total / 2 (an odd total leaves a run open at the
+// end), read on the device, runs beyond `cap` are not written
+__global__ void run_pair_kernel(const long long* __restrict__ edges, const long long* __restrict__ total,
+                                long long cap, const float* __restrict__ x, long long min_long, long long trim_lo,
+                                long long trim_hi, long long* __restrict__ rs, long long* __restrict__ rl,
+                                double* __restrict__ rm) {
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (r >= nruns) return;
-    const long long s = edges[2 * r] >> 1, e = edges[2 * r + 1] >> 1;
-    const long long len = e - s;
-    double mean = nan("");
-    if (len > min_long) {
-        const long long lo = s + trim_lo, hi = s + len - trim_hi;
-        double acc = 0;
-        for (long long i = lo + lane; i < hi; i += 32) acc += (double)x[i];
-        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (hi > lo) mean = acc / (double)(hi - lo);
-    }
-    if (lane == 0) {
-        rs[r] = s;
-        rl[r] = len;
-        rm[r] = mean;
+    const long long nruns = min(*total / 2, cap);
+    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nruns; r += nwarps) {
+        const long long s = edges[2 * r] >> 1, e = edges[2 * r + 1] >> 1;
+        const long long len = e - s;
+        double mean = nan("");
+        if (len > min_long) {
+            const long long lo = s + trim_lo, hi = s + len - trim_hi;
+            double acc = 0;
+            for (long long i = lo + lane; i < hi; i += 32) acc += (double)x[i];
+            for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (hi > lo) mean = acc / (double)(hi - lo);
+        }
+        if (lane == 0) {
+            rs[r] = s;
+            rl[r] = len;
+            rm[r] = mean;
+        }
     }
 }
 
@@ -905,26 +910,25 @@ int ldg_sync_runs(ldg_ctx* c, const float* d05, int64_t n, double threshold, int
         return done(ldg::lines_fail(LDG_ERR_CUDA, std::string("ldg_sync_runs: ") + what + ": " +
                                                       cudaGetErrorString(cudaGetLastError())));
     };
+    // count, scan, write and pair back to back; the host learns the count once
     edge_count_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, counts);
     edge_scan_kernel<<<1, 1024, 0, st>>>(counts, ntiles, offsets, total);
+    edge_write_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, offsets, edges, ecap);
+    run_pair_kernel<<<4 * 148, 256, 0, st>>>(edges, total, cap, d05, min_long, trim_lo, trim_hi, rs, rl, rm);
     long long nedges = 0;
     if (cudaMemcpyAsync(&nedges, total, sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
-        return cuda_fail("edge count");
-    const long long nr = nedges / 2;  // an odd count leaves a run open at the end
+        return cuda_fail("run count");
+    const long long nr = nedges / 2;
     *nruns = nr;
     if (nr > cap || nedges > ecap) return done(ldg::lines_fail(LDG_ERR_RANGE, "ldg_sync_runs: more runs than cap"));
-    edge_write_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, offsets, edges, ecap);
     if (nr > 0) {
-        const long long threads = nr * 32;
-        run_pair_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(edges, nr, d05, min_long, trim_lo,
-                                                                           trim_hi, rs, rl, rm);
         if (cudaMemcpyAsync(run_start, rs, nr * sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaMemcpyAsync(run_len, rl, nr * sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaMemcpyAsync(run_mean, rm, nr * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
             return cuda_fail("D2H");
+        if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_fail("run copy");
     }
-    if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_fail("run pairing");
     return done(LDG_OK);
 }
 

@@ -575,26 +575,28 @@ class LineLocator:
             self._scan_lo = int(st[-1] + ln[-1])
             self._runs = tuple(np.concatenate([a, b]) for a, b in zip(self._runs, (st, ln.copy(), mn.copy())))
 
-    def advance(self, nblocks, stream=None, force_host=()):
+    def advance(self, nblocks, stream=None, force_host=(), scan_stream=None):
         """Fields whose read windows lie within the first `nblocks` blocks
         (demodulated and complete in stream order on `stream`): scans the
         new samples, walks the chain, refines on the GPU.  `stream` is a
         torch.cuda.Stream (device work and allocations are ordered on it) or
-        None.  Returns the range of new indices into `self.fields`."""
-        import contextlib
+        None.  The sync-run scan runs on `scan_stream` when given (so it need
+        not queue behind earlier refinement work on `stream`).  Returns the
+        range of new indices into `self.fields`."""
+        raw_scan = scan_stream.cuda_stream if isinstance(scan_stream, self.torch.cuda.Stream) else scan_stream
         if isinstance(stream, self.torch.cuda.Stream):
             with self.torch.cuda.stream(stream):
-                return self._advance(nblocks, stream.cuda_stream, force_host)
-        with contextlib.nullcontext():
-            return self._advance(nblocks, stream, force_host)
+                return self._advance(nblocks, stream.cuda_stream, force_host,
+                                     raw_scan if scan_stream is not None else stream.cuda_stream)
+        return self._advance(nblocks, stream, force_host, raw_scan if scan_stream is not None else stream)
 
-    def _advance(self, nblocks, stream, force_host):
+    def _advance(self, nblocks, stream, force_host, scan_stream):
         rf = self.rf
         torch = self.torch
         U = rf.blocklen - rf.blockcut - rf.blockcut_end
         first_new = len(self.fields)
         t = time.perf_counter()
-        self._scan(min(nblocks * U, self._cap_len), stream)
+        self._scan(min(nblocks * U, self._cap_len), scan_stream)
         t = self._tick("sync_runs", t)
         out = self.fields
         arrays, ptrs = self._arrays, self._ptrs
@@ -686,7 +688,7 @@ class LineLocator:
                 self._ire0 = float(rf.DecoderParams["ire0"])
                 self._scan_lo = 0
                 self._runs = (np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0, np.float64))
-                self._scan(min(nblocks * U, self._cap_len), stream)
+                self._scan(min(nblocks * U, self._cap_len), scan_stream)
             t = self._tick("host_fields", t)
         self._state = state
         return first_new, len(out)
