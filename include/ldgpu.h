@@ -194,6 +194,48 @@ int ldg_demod_scratch_bytes(ldg_ctx* ctx, int64_t nblocks, int64_t* bytes);
  * on args->stream (or the context's stream) and returns without waiting. */
 int ldg_demod_blocks_noalloc(ldg_ctx* ctx, const ldg_demod_args* args, int32_t ctas);
 
+/* ---- Mixed batches: many captures in one launch (no reference counterpart;
+ * the reference demodulates one capture's blocks at a time in
+ * DemodCache.worker, core.py:1165-1200) ---- */
+
+typedef struct ldg_queue ldg_queue;
+
+/* One capture of a mixed batch: the context of its configuration (system,
+ * filters, MTF, audio bands) and its blocks and outputs as for
+ * ldg_demod_blocks, all buffers device memory (args.stream is ignored). */
+typedef struct {
+    ldg_ctx* ctx;
+    ldg_demod_args args;
+} ldg_work_item;
+
+/* A device work queue on `device`: a persistent demodulator launch whose
+ * CTAs pop blocks of all submitted captures (NTSC and PAL mixed) until the
+ * queue is empty.  Every block's outputs are bit-identical to those of
+ * ldg_demod_blocks on its capture. */
+int ldg_queue_create(ldg_queue** out, int32_t device);
+void ldg_queue_destroy(ldg_queue* q);
+
+/* Replace the queue's captures (validated as ldg_demod_blocks validates a
+ * device batch).  Waits for the queue's previous run.  A run reads each
+ * item's context filters as they are then, so contexts must outlive the
+ * runs that use them. */
+int ldg_queue_submit(ldg_queue* q, const ldg_work_item* items, int32_t n);
+
+/* Scheduling: `grab` consecutive blocks per pop (1..64), `ctas` persistent
+ * CTAs (0: one per SM; at most 4 x SMs).  Default 1, 0. */
+int ldg_queue_set_schedule(ldg_queue* q, int32_t grab, int32_t ctas);
+
+/* Blocks submitted and the CTAs a run launches. */
+int ldg_queue_info(ldg_queue* q, int64_t* total_blocks, int32_t* grid);
+
+/* Demodulate every submitted block: reset of the queue head plus one
+ * persistent launch, enqueued on `stream` (NULL: the queue's own stream)
+ * without waiting.  use_graph != 0: the two are captured once into a CUDA
+ * graph (re-captured after a submit or schedule change) and the graph is
+ * launched.  Runs of one queue must not overlap on the GPU (they share its
+ * head and scratch): order them on one stream. */
+int ldg_queue_run(ldg_queue* q, void* stream, int32_t use_graph);
+
 /* ---- AC3-RF (2.88 MHz QPSK) demodulation, lddecode/ac3rf.py ---- */
 
 typedef struct ldg_ac3 ldg_ac3;

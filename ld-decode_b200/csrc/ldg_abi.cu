@@ -667,55 +667,45 @@ int ctx_lines_scratch(ldg_ctx* c, size_t need, void** out) {
 
 void* noalloc_stream(ldg_ctx* c, const ldg_demod_args* a) { return a->stream ? a->stream : (void*)c->stream; }
 
-int noalloc_prepare(ldg_ctx* c, const ldg_demod_args* a, int ctas, int max_slots, DemodParams* p, int* grid,
-                    int* device) {
-    *grid = 0;
-    if (!c || !a) return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: NULL argument");
+// Validates a batch whose buffers are all device memory and fills the
+// kernel parameters from it and the context's filters (scheduling fields
+// left zero).  `who` names the entry point in error messages.
+int device_params(ldg_ctx* c, const ldg_demod_args* a, const std::string& who, DemodParams* p) {
+    if (!c || !a) return fail(LDG_ERR_ARG, who + ": NULL argument");
     if (!a->in) return fail(LDG_ERR_ARG, "demodblock called without raw or FFT data");
     if (a->in_kind != LDG_IN_INT16 && a->in_kind != LDG_IN_FLOAT32)
-        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: in_kind must be LDG_IN_INT16 or LDG_IN_FLOAT32");
+        return fail(LDG_ERR_ARG, who + ": in_kind must be LDG_IN_INT16 or LDG_IN_FLOAT32");
     if (a->nblocks < 0 || a->in_stride < 0 || a->nblocks > (1LL << 30))
-        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: bad block count or stride");
-    if (ctas < 0 || ctas > max_slots)
-        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: ctas = " + std::to_string(ctas) +
-                                     " exceeds the static scratch (" + std::to_string(max_slots) +
-                                     " CTA slots of 256 KB); use 0 < ctas <= " + std::to_string(max_slots));
+        return fail(LDG_ERR_ARG, who + ": bad block count or stride");
     const int N = kN;
     if (!slice_ok(a->video, N) || !slice_ok(a->rfhpf, N) || !slice_ok(a->efm, N) || !slice_ok(a->audio, 1024))
-        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: output slice outside the block");
+        return fail(LDG_ERR_ARG, who + ": output slice outside the block");
     if (a->roll_05 < 0 || a->roll_05 >= N || a->roll_burst < 0 || a->roll_burst >= N)
-        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: roll outside the block");
+        return fail(LDG_ERR_ARG, who + ": roll outside the block");
     const void* ptrs[10] = {a->in, a->out_demod, a->out_raw, a->out_05, a->out_burst, a->out_pilot,
                             a->out_rfhpf, a->out_efm, a->out_audio_left, a->out_audio_right};
     for (const void* q : ptrs)
-        if (q && !is_device_ptr(q))
-            return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: all buffers must be device memory (no host staging)");
+        if (q && !is_device_ptr(q)) return fail(LDG_ERR_ARG, who + ": all buffers must be device memory (no host staging)");
     std::lock_guard<std::mutex> lk(c->mu);
     if (!c->d_filter[LDG_F_VIDEO_G] || !c->d_filter[LDG_F_VIDEO_G_ODD])
-        return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: RFVideo filter not set");
+        return fail(LDG_ERR_STATE, who + ": RFVideo filter not set");
     const int fslot[4] = {LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT};
     float* vids[4] = {a->out_demod, a->out_05, a->out_burst, a->out_pilot};
     for (int o = 0; o < 4; ++o)
-        if (vids[o] && !c->d_filter[fslot[o]]) return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: video filter not set");
-    if (a->out_rfhpf && !c->d_filter[LDG_F_RFHPF]) return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: rfhpf filter not set");
-    if (a->out_efm && !c->d_filter[LDG_F_EFM]) return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: EFM filter not set");
+        if (vids[o] && !c->d_filter[fslot[o]]) return fail(LDG_ERR_STATE, who + ": video filter not set");
+    if (a->out_rfhpf && !c->d_filter[LDG_F_RFHPF]) return fail(LDG_ERR_STATE, who + ": rfhpf filter not set");
+    if (a->out_efm && !c->d_filter[LDG_F_EFM]) return fail(LDG_ERR_STATE, who + ": EFM filter not set");
     const bool audio = a->out_audio_left || a->out_audio_right;
-    if (audio && (!c->d_audio[0] || !c->d_audio[1]))
-        return fail(LDG_ERR_STATE, "ldg_demod_blocks_noalloc: audio bands not set");
+    if (audio && (!c->d_audio[0] || !c->d_audio[1])) return fail(LDG_ERR_STATE, who + ": audio bands not set");
     const size_t esz = a->in_kind == LDG_IN_INT16 ? 2 : 4;
     if ((a->in_stride & 1) != 0 || (reinterpret_cast<uintptr_t>(a->in) & (esz == 2 ? 3 : 7)) != 0)
-        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: input blocks must start on an even sample of an aligned buffer");
-    *device = c->device;
-    if (a->nblocks == 0) return LDG_OK;
-    const long long nb = a->nblocks;
-    const int cap = ctas ? ctas : max_slots;
-    *grid = (int)(nb < cap ? nb : cap);
+        return fail(LDG_ERR_ARG, who + ": input blocks must start on an even sample of an aligned buffer");
 
     memset(p, 0, sizeof(*p));
     p->in = a->in;
     p->in_kind = a->in_kind;
     p->in_stride = a->in_stride;
-    p->nblocks = (int)nb;
+    p->nblocks = (int)a->nblocks;
     p->fs_hz = (float)c->fs_hz;
     p->f_rfhpf = c->d_filter[LDG_F_RFHPF];
     p->f_g = c->d_filter[LDG_F_VIDEO_G];
@@ -747,6 +737,23 @@ int noalloc_prepare(ldg_ctx* c, const ldg_demod_args* a, int ctas, int max_slots
     p->s_audio = {a->audio.start, a->audio.len, 0};
     p->tw16 = c->d_tw16;
     p->tw32 = c->d_tw32;
+    return LDG_OK;
+}
+
+int noalloc_prepare(ldg_ctx* c, const ldg_demod_args* a, int ctas, int max_slots, DemodParams* p, int* grid,
+                    int* device) {
+    *grid = 0;
+    if (ctas < 0 || ctas > max_slots)
+        return fail(LDG_ERR_ARG, "ldg_demod_blocks_noalloc: ctas = " + std::to_string(ctas) +
+                                     " exceeds the static scratch (" + std::to_string(max_slots) +
+                                     " CTA slots of 256 KB); use 0 < ctas <= " + std::to_string(max_slots));
+    const int rc = device_params(c, a, "ldg_demod_blocks_noalloc", p);
+    if (rc) return rc;
+    *device = c->device;
+    if (a->nblocks == 0) return LDG_OK;
+    const long long nb = a->nblocks;
+    const int cap = ctas ? ctas : max_slots;
+    *grid = (int)(nb < cap ? nb : cap);
     return LDG_OK;
 }
 

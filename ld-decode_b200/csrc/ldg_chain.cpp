@@ -772,6 +772,7 @@ extern "C" int64_t ldg_abi_sizeof(const char* name) {
     if (n == "ldg_tbc_field") return sizeof(ldg_tbc_field);
     if (n == "ldg_demod_args") return sizeof(ldg_demod_args);
     if (n == "ldg_slice") return sizeof(ldg_slice);
+    if (n == "ldg_work_item") return sizeof(ldg_work_item);
     return -1;
 }
 

@@ -201,23 +201,123 @@ __device__ void audio_stage(const DemodParams& p, float2* A, const Tables& t, in
     }
 }
 
-}  // namespace
+// One block: every requested output of block `blk` of p.  parkX/parkZ: this
+// CTA's scratch (kScratchPerCta).  Ends with the CTA's threads in step.
+__device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float2* S, float2* A, const Tables& t,
+                                            float2* parkX, float2* parkZ) {
+    // ---- input spectrum X (first pass reads the block), parked; audio taps; rfhpf input
+    if (p.in_kind == 0) {
+        fft16k<false>(S, t, InLoader16{static_cast<const int16_t*>(p.in) + (long long)blk * p.in_stride});
+    } else {
+        fft16k<false>(S, t, InLoader32{static_cast<const float*>(p.in) + (long long)blk * p.in_stride});
+    }
+    if (p.audio) {
+        for (int idx = threadIdx.x; idx < 2 * 511; idx += kThreads) {
+            const int ch = idx / 511, k = 513 + idx % 511;
+            A[ch * padded(1024) + pad(k)] = make_float2(0.f, 0.f);
+        }
+    }
+    {
+        AudioTaps au{A, {p.a_lowbin[0], p.a_lowbin[1]}, {p.a_filt1[0], p.a_filt1[1]}};
+        post_r2c(S, t, parkX, p.o_rfhpf ? p.f_rfhpf : nullptr, p.audio ? &au : nullptr);
+    }
+    __syncthreads();
+    if (p.audio) audio_stage(p, A, t, blk);
 
-__global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p) {
-    extern __shared__ float2 smem[];
-    float2* S = smem;
-    float2* A = smem + padded(kM);
-    float2* s2 = A + 2 * padded(1024);
+    // ---- rfhpf
+    if (p.o_rfhpf) {
+        fft16k<true>(S, t, SmemIO(),
+                     RealStorer{p.o_rfhpf + (long long)blk * p.s_rfhpf.len, p.s_rfhpf.start, p.s_rfhpf.len, 0});
+    }
+
+    // ---- EFM
+    if (p.o_efm) {
+        pre_c2r(S, t, parkX, p.f_efm);
+        __syncthreads();
+        fft16k<true>(S, t, SmemIO(), EfmStorer{p.o_efm + (long long)blk * p.s_efm.len, p.s_efm.start, p.s_efm.len});
+    }
+
+    // ---- analytic signal: even samples (parked), then odd samples (in S)
+    fft16k<true>(S, t, AnalyticLoader{parkX, p.f_g, p.f_godd, false}, ParkStorer{parkZ});
+    fft16k<true>(S, t, AnalyticLoader{parkX, p.f_g, p.f_godd, true});
+
+    // ---- FM discriminator: demod[2m] from (z_e[m], z_o[m-1]), demod[2m+1]
+    // from (z_o[m], z_e[m]); the clipped pairs replace X in the parking slot
+    {
+        const float kfs = p.fs_hz / kTwoPi;
+        const float clip_hi = p.fs_hz * 0.75f;
+        float* oraw = p.o_raw ? p.o_raw + (long long)blk * p.s_video.len : nullptr;
+        const int vs = p.s_video.start, vl = p.s_video.len;
+        for (int m = threadIdx.x; m < kM; m += kThreads) {
+            const float2 ze = parkZ[m];
+            const float2 zo = S[pad(m)];
+            const float de = (m == 0) ? 0.0f : fm_disc(ze, S[pad(m - 1)], kfs);
+            const float dodd = fm_disc(zo, ze, kfs);
+            if (oraw) {
+                const int i0 = 2 * m - vs;
+                if (i0 >= 0 && i0 + 1 < vl && ((reinterpret_cast<uintptr_t>(oraw + i0) & 7) == 0)) {
+                    __stcs(reinterpret_cast<float2*>(oraw + i0), make_float2(de, dodd));
+                } else {
+                    if (i0 >= 0 && i0 < vl) __stcs(oraw + i0, de);
+                    if (i0 + 1 >= 0 && i0 + 1 < vl) __stcs(oraw + i0 + 1, dodd);
+                }
+            }
+            parkX[m] = make_float2(fminf(fmaxf(de, 1500000.0f), clip_hi), fminf(fmaxf(dodd, 1500000.0f), clip_hi));
+        }
+    }
+    __syncthreads();
+
+    // ---- spectrum D of the clipped demod, then the video outputs
+    fft16k<false>(S, t, ParkLoader{parkX});
+    int first = -1;
+#pragma unroll
+    for (int o = 0; o < OUT_NVIDEO; ++o)
+        if (first < 0 && p.o_video[o]) first = o;
+    post_r2c(S, t, parkX, first >= 0 ? p.f_video[first] : nullptr, nullptr);
+    __syncthreads();
+#pragma unroll
+    for (int o = 0; o < OUT_NVIDEO; ++o) {
+        if (p.o_video[o] == nullptr) continue;
+        if (o != first) {
+            pre_c2r(S, t, parkX, p.f_video[o]);
+            __syncthreads();
+        }
+        fft16k<true>(S, t, SmemIO(),
+                     RealStorer{p.o_video[o] + (long long)blk * p.s_video.len, p.s_video.start, p.s_video.len,
+                                p.roll[o]});
+    }
+    __syncthreads();
+}
+
+struct CtaSmem {
+    float2* S;
+    float2* A;
+    Tables t;
+};
+
+// Carves the dynamic shared memory and loads the pass twiddle tables.
+__device__ __forceinline__ CtaSmem cta_setup(float2* smem, const float2* tw16, const float2* tw32) {
+    CtaSmem c;
+    c.S = smem;
+    c.A = smem + padded(kM);
+    float2* s2 = c.A + 2 * padded(1024);
     float2* s3 = s2 + kS2;
     float2* s4 = s3 + kS3;
-    load_pass_tables(s2, s3, s4, p.tw16);
-    Tables t;
-    t.t16 = p.tw16;
-    t.t32 = p.tw32;
-    t.s2 = s2;
-    t.s3 = s3;
-    t.s4 = s4;
+    load_pass_tables(s2, s3, s4, tw16);
+    c.t.t16 = tw16;
+    c.t.t32 = tw32;
+    c.t.s2 = s2;
+    c.t.s3 = s3;
+    c.t.s4 = s4;
     __syncthreads();
+    return c;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads, 1) demod_kernel(const __grid_constant__ DemodParams p) {
+    extern __shared__ float2 smem[];
+    const CtaSmem c = cta_setup(smem, p.tw16, p.tw32);
 
     __shared__ int s_got;
     const bool per_block = p.slot_lock != nullptr;
@@ -242,93 +342,9 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
     int blk = per_block ? (int)blockIdx.x * p.blocks_per_cta : (int)blockIdx.x;
     const int blk_end = per_block ? min(blk + p.blocks_per_cta, p.nblocks) : p.nblocks;
     const int blk_step = per_block ? 1 : (int)gridDim.x;
-    while (blk < blk_end) {
-        float2* parkX = p.scratch + (size_t)slot * 2 * kM;
-        float2* parkZ = parkX + kM;
-
-        // ---- input spectrum X (first pass reads the block), parked; audio taps; rfhpf input
-        if (p.in_kind == 0) {
-            fft16k<false>(S, t, InLoader16{static_cast<const int16_t*>(p.in) + (long long)blk * p.in_stride});
-        } else {
-            fft16k<false>(S, t, InLoader32{static_cast<const float*>(p.in) + (long long)blk * p.in_stride});
-        }
-        if (p.audio) {
-            for (int idx = threadIdx.x; idx < 2 * 511; idx += kThreads) {
-                const int ch = idx / 511, k = 513 + idx % 511;
-                A[ch * padded(1024) + pad(k)] = make_float2(0.f, 0.f);
-            }
-        }
-        {
-            AudioTaps au{A, {p.a_lowbin[0], p.a_lowbin[1]}, {p.a_filt1[0], p.a_filt1[1]}};
-            post_r2c(S, t, parkX, p.o_rfhpf ? p.f_rfhpf : nullptr, p.audio ? &au : nullptr);
-        }
-        __syncthreads();
-        if (p.audio) audio_stage(p, A, t, blk);
-
-        // ---- rfhpf
-        if (p.o_rfhpf) {
-            fft16k<true>(S, t, SmemIO(),
-                         RealStorer{p.o_rfhpf + (long long)blk * p.s_rfhpf.len, p.s_rfhpf.start, p.s_rfhpf.len, 0});
-        }
-
-        // ---- EFM
-        if (p.o_efm) {
-            pre_c2r(S, t, parkX, p.f_efm);
-            __syncthreads();
-            fft16k<true>(S, t, SmemIO(), EfmStorer{p.o_efm + (long long)blk * p.s_efm.len, p.s_efm.start, p.s_efm.len});
-        }
-
-        // ---- analytic signal: even samples (parked), then odd samples (in S)
-        fft16k<true>(S, t, AnalyticLoader{parkX, p.f_g, p.f_godd, false}, ParkStorer{parkZ});
-        fft16k<true>(S, t, AnalyticLoader{parkX, p.f_g, p.f_godd, true});
-
-        // ---- FM discriminator: demod[2m] from (z_e[m], z_o[m-1]), demod[2m+1]
-        // from (z_o[m], z_e[m]); the clipped pairs replace X in the parking slot
-        {
-            const float kfs = p.fs_hz / kTwoPi;
-            const float clip_hi = p.fs_hz * 0.75f;
-            float* oraw = p.o_raw ? p.o_raw + (long long)blk * p.s_video.len : nullptr;
-            const int vs = p.s_video.start, vl = p.s_video.len;
-            for (int m = threadIdx.x; m < kM; m += kThreads) {
-                const float2 ze = parkZ[m];
-                const float2 zo = S[pad(m)];
-                const float de = (m == 0) ? 0.0f : fm_disc(ze, S[pad(m - 1)], kfs);
-                const float dodd = fm_disc(zo, ze, kfs);
-                if (oraw) {
-                    const int i0 = 2 * m - vs;
-                    if (i0 >= 0 && i0 + 1 < vl && ((reinterpret_cast<uintptr_t>(oraw + i0) & 7) == 0)) {
-                        __stcs(reinterpret_cast<float2*>(oraw + i0), make_float2(de, dodd));
-                    } else {
-                        if (i0 >= 0 && i0 < vl) __stcs(oraw + i0, de);
-                        if (i0 + 1 >= 0 && i0 + 1 < vl) __stcs(oraw + i0 + 1, dodd);
-                    }
-                }
-                parkX[m] = make_float2(fminf(fmaxf(de, 1500000.0f), clip_hi), fminf(fmaxf(dodd, 1500000.0f), clip_hi));
-            }
-        }
-        __syncthreads();
-
-        // ---- spectrum D of the clipped demod, then the video outputs
-        fft16k<false>(S, t, ParkLoader{parkX});
-        int first = -1;
-#pragma unroll
-        for (int o = 0; o < OUT_NVIDEO; ++o)
-            if (first < 0 && p.o_video[o]) first = o;
-        post_r2c(S, t, parkX, first >= 0 ? p.f_video[first] : nullptr, nullptr);
-        __syncthreads();
-#pragma unroll
-        for (int o = 0; o < OUT_NVIDEO; ++o) {
-            if (p.o_video[o] == nullptr) continue;
-            if (o != first) {
-                pre_c2r(S, t, parkX, p.f_video[o]);
-                __syncthreads();
-            }
-            fft16k<true>(S, t, SmemIO(),
-                         RealStorer{p.o_video[o] + (long long)blk * p.s_video.len, p.s_video.start, p.s_video.len,
-                                    p.roll[o]});
-        }
-        blk += blk_step;
-    }
+    float2* parkX = p.scratch + (size_t)slot * 2 * kM;
+    float2* parkZ = parkX + kM;
+    for (; blk < blk_end; blk += blk_step) demod_block(p, blk, c.S, c.A, c.t, parkX, parkZ);
     if (per_block) {
         // every thread is done with the slot's scratch before it is handed on
         __syncthreads();
@@ -337,6 +353,67 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const DemodParams p)
             atomicExch(p.slot_lock + slot, 0);
         }
     }
+}
+
+// Persistent CTAs over a device work queue of blocks of many captures: each
+// CTA pops `grab` consecutive global block indices at a time from *head,
+// finds the capture that holds each (binary search over first_block), keeps
+// that capture's parameters in shared memory, and demodulates the block.
+__global__ void __launch_bounds__(kThreads, 1) demod_queue_kernel(const __grid_constant__ QueueParams q) {
+    extern __shared__ float2 smem[];
+    const CtaSmem c = cta_setup(smem, q.tw16, q.tw32);
+    __shared__ DemodParams sp;
+    __shared__ long long s_pop;
+    __shared__ int s_item;
+    float2* parkX = q.scratch + (size_t)blockIdx.x * 2 * kM;
+    float2* parkZ = parkX + kM;
+    int cur = -1;
+    for (;;) {
+        if (threadIdx.x == 0) s_pop = (long long)atomicAdd(q.head, (unsigned long long)q.grab);
+        __syncthreads();
+        const long long g0 = s_pop;
+        if (g0 >= q.total) break;
+        const long long g1 = min(g0 + (long long)q.grab, q.total);
+        for (long long g = g0; g < g1; ++g) {
+            if (threadIdx.x == 0) {
+                int lo = 0, hi = q.nitems - 1;  // last item whose first block is <= g
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (q.first_block[mid] <= g) lo = mid; else hi = mid - 1;
+                }
+                s_item = lo;
+            }
+            __syncthreads();
+            const int it = s_item;
+            if (it != cur) {
+                const int* src = reinterpret_cast<const int*>(q.items + it);
+                int* dst = reinterpret_cast<int*>(&sp);
+                for (int w = threadIdx.x; w < (int)(sizeof(DemodParams) / sizeof(int)); w += kThreads) dst[w] = src[w];
+                cur = it;
+                __syncthreads();
+            }
+            demod_block(sp, (int)(g - q.first_block[it]), c.S, c.A, c.t, parkX, parkZ);
+        }
+    }
+}
+
+cudaError_t prepare_demod_queue() {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(demod_queue_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kSmemBytes);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_demod_queue(const QueueParams& q, int grid, cudaStream_t stream) {
+    cudaError_t e = prepare_demod_queue();
+    if (e != cudaSuccess) return e;
+    if (q.total <= 0 || grid <= 0) return cudaSuccess;
+    demod_queue_kernel<<<grid, kThreads, kSmemBytes, stream>>>(q);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_demod(const DemodParams& p, int grid, cudaStream_t stream) {

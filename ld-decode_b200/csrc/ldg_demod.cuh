@@ -68,11 +68,29 @@ struct DemodParams {
 
 constexpr int kDemodErrSlotWait = 1;
 
+// A device work queue over the blocks of many captures (each with its own
+// parameters: system, filters, outputs).  Block g of the queue is block
+// g - first_block[i] of item i, first_block[i] <= g < first_block[i + 1].
+struct QueueParams {
+    const DemodParams* items;      // device array, nitems (scratch/slot fields unused)
+    const long long* first_block;  // device array, nitems + 1 (prefix sums)
+    int nitems;
+    int grab;                      // consecutive blocks taken per pop
+    long long total;               // first_block[nitems]
+    unsigned long long* head;      // next unclaimed block; 0 at launch
+    float2* scratch;               // kScratchPerCta per CTA of the launch
+    const float2* tw16;
+    const float2* tw32;
+};
+
 // Dynamic shared memory the kernel needs.
 constexpr int kSmemFloat2 = (16384 + 1024) + 2 * (1024 + 64) + 4 * 16 + 4 * 256 + 4096;
 constexpr size_t kSmemBytes = size_t(kSmemFloat2) * 8;
 constexpr size_t kScratchPerCta = size_t(2) * 16384 * 8;
 
 cudaError_t launch_demod(const DemodParams& p, int grid, cudaStream_t stream);
+// Sets the queue kernel's shared-memory size (call before a stream capture).
+cudaError_t prepare_demod_queue();
+cudaError_t launch_demod_queue(const QueueParams& q, int grid, cudaStream_t stream);
 
 }  // namespace ldg

@@ -14,6 +14,12 @@ namespace ldg {
 int noalloc_prepare(ldg_ctx* ctx, const ldg_demod_args* a, int ctas, int max_slots, DemodParams* p, int* grid,
                     int* device);
 int noalloc_fail(int code, const std::string& msg);
+
+// Validate a batch whose buffers are all device memory and fill `p` from it
+// and ctx's filters (scheduling fields zero); `who` names the caller in
+// error messages.
+int device_params(ldg_ctx* ctx, const ldg_demod_args* a, const std::string& who, DemodParams* p);
+int ctx_device(const ldg_ctx* ctx);
 void* noalloc_stream(ldg_ctx* ctx, const ldg_demod_args* a);
 
 }  // namespace ldg

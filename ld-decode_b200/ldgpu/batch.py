@@ -1,0 +1,280 @@
+"""Mixed batches: many captures of uneven length, NTSC and PAL together.
+
+The reference decodes one capture at a time, its blocks demodulated by
+DemodCache worker threads (lddecode/core.py:1165-1200) and its fields read
+one after another (LDdecode.readfield, core.py:4060-4200).  Here:
+
+* `DemodQueue` (ldg_queue_*): every block of every capture in one
+  persistent demodulator launch whose CTAs pop blocks from a device work
+  queue, replayed from a CUDA graph.  Each block's outputs are bit-identical
+  to demodulating its capture alone.
+* `autotune` times the queue's schedules (blocks per pop, persistent CTAs)
+  on the submitted batch and keeps the fastest.
+* `MixedBatch` runs the whole path for a list of device-resident captures:
+  the queue demodulation, line locations per capture (`LineLocator`), and
+  one TBC launch over the fields of all captures.
+* `waves` splits a list of captures into groups whose outputs fit a device
+  memory budget.
+"""
+
+import ctypes
+
+from . import lib as L
+
+U_KEYS = ("demod", "demod_raw", "demod_05", "demod_burst", "demod_pilot", "rfhpf", "efm")
+FIELD_KEYS = ("demod", "demod_05", "demod_burst", "demod_pilot")
+
+
+def _raw_stream(stream):
+    """Raw cudaStream_t of a torch.cuda.Stream or handle; None: torch's
+    current stream.  Torch's default stream (handle 0) is passed as
+    cudaStreamLegacy (1) so that work stays ordered with it (a NULL handle
+    would select the queue's own stream)."""
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    h = getattr(stream, "cuda_stream", stream)
+    return 1 if not h else h
+
+
+class DemodQueue:
+    """One ldg_queue: captures submitted together, demodulated in one launch."""
+
+    def __init__(self, device=0):
+        self._lib = L.load()
+        h = L.c_p()
+        L.check(self._lib.ldg_queue_create(ctypes.byref(h), int(device)))
+        self.handle = h
+        self.device = device
+        self.schedule = (1, 0)
+
+    def submit(self, items):
+        """items: (rf, in_ptr, nblocks, in_stride, outs, mtf_level) per
+        capture, as for RFDecode.demod_blocks_device (device pointers).  The
+        queue reads each capture's filters from its RFDecode's context when
+        it runs, so captures sharing an RFDecode must share mtf_level."""
+        mtf = {}
+        arr = (L.WorkItem * len(items))()
+        for i, (rf, in_ptr, nblocks, stride, outs, level) in enumerate(items):
+            if mtf.setdefault(id(rf), level) != level:
+                raise ValueError("captures sharing an RFDecode must use one mtf_level per queue")
+            a, _ = rf.demod_args(in_ptr, nblocks, stride, outs, level)
+            arr[i].ctx = rf._ctx.handle
+            arr[i].args = a
+        self._items = list(items)  # keep the RFDecodes alive while the queue may run
+        L.check(self._lib.ldg_queue_submit(self.handle, arr, len(arr)))
+
+    def set_schedule(self, grab=1, ctas=0):
+        L.check(self._lib.ldg_queue_set_schedule(self.handle, int(grab), int(ctas)))
+        self.schedule = (int(grab), int(ctas))
+
+    def info(self):
+        """(blocks submitted, CTAs a run launches)."""
+        total = ctypes.c_int64(0)
+        grid = ctypes.c_int32(0)
+        L.check(self._lib.ldg_queue_info(self.handle, ctypes.byref(total), ctypes.byref(grid)))
+        return total.value, grid.value
+
+    def run(self, stream=None, graph=True):
+        """Enqueue one pass over every submitted block on `stream` (a
+        torch.cuda.Stream or raw handle; None: torch's current stream)."""
+        L.check(self._lib.ldg_queue_run(self.handle, _raw_stream(stream), 1 if graph else 0))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.ldg_queue_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(queue, stream=None, grabs=(1, 2, 4, 8), ctas=(0,), reps=3, graph=True):
+    """Time every (grab, ctas) schedule on the queue's submitted batch with
+    CUDA events on `stream` (one untimed run each, then the best of `reps`)
+    and keep the fastest.  Returns {"best": (grab, ctas), "ms": {...}}."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    times = {}
+    for g in grabs:
+        for c in ctas:
+            queue.set_schedule(g, c)
+            queue.run(st, graph)
+            best = None
+            for _ in range(reps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                queue.run(st, graph)
+                e1.record(st)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+            times[(g, c)] = best
+    choice = min(times, key=times.get)
+    queue.set_schedule(*choice)
+    return {"best": choice, "ms": times}
+
+
+def output_bytes_per_sample(system, audio=True, efm=True):
+    """Device bytes the demodulator's outputs take per input sample."""
+    n = 4 * (5 if system == "PAL" else 4) + 4 + (2 if efm else 0) + (8 * 991 / 31712 if audio else 0)
+    return n
+
+
+def waves(lengths, systems, budget_bytes, in_bytes=2):
+    """Group capture indices (in order) so that each group's inputs and
+    demodulator outputs stay within `budget_bytes`."""
+    groups, cur, used = [], [], 0
+    for i, (n, s) in enumerate(zip(lengths, systems)):
+        need = n * (in_bytes + output_bytes_per_sample(s))
+        if cur and used + need > budget_bytes:
+            groups.append(cur)
+            cur, used = [], 0
+        cur.append(i)
+        used += need
+    if cur:
+        groups.append(cur)
+    return groups
+
+
+class MixedBatch:
+    """The demod + TBC path over many device-resident captures at once.
+
+    captures: list of (system, int16 device tensor).  One RFDecode per
+    system (analog audio and EFM outputs on), one DemodQueue over all
+    captures' blocks, one LineLocator per capture, one TBC launch.  Work is
+    enqueued on `self.stream` (a torch.cuda.Stream of its own) unless a
+    stream is given; wait for it (or torch.cuda.synchronize()) before
+    reading the outputs."""
+
+    def __init__(self, captures, device=0, mtf_level=1, rfs=None, queue=None):
+        import torch
+        from .fieldread import blocks_in_capture
+        from .rfdecode import RFDecode
+        self.torch = torch
+        self.device = device
+        self.stream = torch.cuda.Stream(device=device)
+        # the captures may still be being written on the caller's stream
+        self.stream.wait_stream(torch.cuda.current_stream(device))
+        self.captures = captures
+        self.mtf_level = mtf_level
+        self.rfs = dict(rfs or {})
+        for system, _ in captures:
+            if system not in self.rfs:
+                self.rfs[system] = RFDecode(system=system, decode_analog_audio=44100, decode_digital_audio=True,
+                                            device=device)
+        dev = torch.device("cuda", device)
+        self.items = []
+        self.outs = []
+        self.nblocks = []
+        for system, cap in captures:
+            rf = self.rfs[system]
+            U = rf.blocklen - rf.blockcut - rf.blockcut_end
+            nb = blocks_in_capture(rf, int(cap.numel()))
+            nout = nb * U
+            keys = [k for k in U_KEYS if k != "demod_pilot" or system == "PAL"]
+            o = {k: torch.empty(nout, dtype=torch.int16 if k == "efm" else torch.float32, device=dev) for k in keys}
+            o["audio_left"] = torch.empty(nb * 991, dtype=torch.float32, device=dev)
+            o["audio_right"] = torch.empty(nb * 991, dtype=torch.float32, device=dev)
+            self.outs.append(o)
+            self.nblocks.append(nb)
+            self.items.append((rf, cap.data_ptr(), nb, U, {k: v.data_ptr() for k, v in o.items()}, mtf_level))
+        self.queue = queue if queue is not None else DemodQueue(device)
+        self.queue.submit(self.items)
+        self.fields = None
+        self.pictures = None
+        self.picture_offsets = None
+
+    @property
+    def samples(self):
+        """Input samples demodulated (block outputs kept) per pass."""
+        tot = 0
+        for (rf, _, nb, U, _, _) in self.items:
+            tot += nb * U
+        return tot
+
+    def demod(self, stream=None, graph=True):
+        self.queue.run(stream or self.stream, graph)
+
+    def locate(self, stream=None):
+        """Line locations of every capture's fields (LocatedFields per
+        capture, in capture order)."""
+        from .lines import LineLocator
+        stream = stream or self.stream
+        self.locators = []
+        self.fields = []
+        for (system, _), o, nb in zip(self.captures, self.outs, self.nblocks):
+            loc = LineLocator(self.rfs[system])
+            arrays = {k: o[k] for k in FIELD_KEYS if k in o}
+            self.fields.append(loc.locate(arrays, nb, stream))
+            self.locators.append(loc)
+        return self.fields
+
+    def field_geometry(self, system):
+        rf = self.rfs[system]
+        w = rf.SysParams["outlinelen"]
+        h = rf.SysParams["frame_lines"] // 2 + 1
+        return w, h
+
+    def tbc(self, stream=None):
+        """One TBC launch over every located field of every capture; uint16
+        pictures, capture after capture, field after field, in
+        `self.pictures` (offsets per capture in `self.picture_offsets`)."""
+        import numpy as np
+        from .field import tbc_fields
+        from .lines import field_levels, tbc_batch
+        torch = self.torch
+        stream = stream or self.stream
+        sizes = []
+        for (system, _), fl in zip(self.captures, self.fields):
+            w, h = self.field_geometry(system)
+            sizes.append(len(fl) * w * h)
+        offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        total = int(offs[-1])
+        if self.pictures is None or self.pictures.numel() < total:
+            with torch.cuda.stream(stream):
+                self.pictures = torch.empty(max(total, 1), dtype=torch.uint16,
+                                            device=torch.device("cuda", self.device))
+        self.picture_offsets = offs
+        base = self.pictures.data_ptr()
+        descs = []
+        for (system, _), fl, o, off in zip(self.captures, self.fields, self.outs, offs[:-1]):
+            rf = self.rfs[system]
+            if len(fl):
+                descs.append(tbc_batch(rf, fl, o["demod"].data_ptr(), base + 2 * int(off), field_levels(rf)))
+        n = sum(len(d) for d in descs)
+        if n == 0:
+            return self.pictures[:0]
+        allf = (L.TbcField * n)()
+        k = 0
+        for d in descs:
+            ctypes.memmove(ctypes.addressof(allf) + k * ctypes.sizeof(L.TbcField), ctypes.addressof(d),
+                           ctypes.sizeof(d))
+            k += len(d)
+        # the sinc table is the same for both systems: any context runs the batch
+        rf0 = self.rfs[self.captures[0][0]]
+        tbc_fields(rf0, allf, stream=_raw_stream(stream), asynchronous=True)
+        return self.pictures[:total]
+
+    def picture(self, capture, field):
+        """uint16 (lines, width) view of one field's picture."""
+        system = self.captures[capture][0]
+        w, h = self.field_geometry(system)
+        o = int(self.picture_offsets[capture]) + field * w * h
+        return self.pictures[o:o + w * h].view(h, w)
+
+    def run(self, stream=None, graph=True):
+        """Demodulate, locate and resample everything; returns the number of
+        fields."""
+        stream = stream or self.stream
+        self.demod(stream, graph)
+        self.locate(stream)
+        self.tbc(stream)
+        return sum(len(f) for f in self.fields)
+
+    def close(self):
+        self.queue.close()

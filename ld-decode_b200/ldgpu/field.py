@@ -43,11 +43,13 @@ def tbc_descriptor(rf, buf, linelocs, lineoffset, outwidth, linesout, outlinecou
 def tbc_fields(rf, descs, stream=None, asynchronous=False):
     """Run ldg_tbc_fields on a list (or prebuilt ctypes array) of descriptors;
     asynchronous=True: ldg_tbc_fields_async (device buffers only; errors come
-    from tbc_status)."""
+    from tbc_status).  `stream`: a raw handle; None runs on torch's default
+    stream (cudaStreamLegacy), so that device inputs written there (line
+    locations, demodulator outputs) are complete first."""
     rf._load_lut()
     arr = descs if isinstance(descs, ctypes.Array) else (L.TbcField * len(descs))(*descs)
     fn = rf._ctx._lib.ldg_tbc_fields_async if asynchronous else rf._ctx._lib.ldg_tbc_fields
-    L.check(fn(rf._ctx.handle, arr, len(arr), stream))
+    L.check(fn(rf._ctx.handle, arr, len(arr), stream if stream else 1))
 
 
 def tbc_status(rf):

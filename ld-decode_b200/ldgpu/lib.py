@@ -41,6 +41,10 @@ class DemodArgs(ctypes.Structure):
     ]
 
 
+class WorkItem(ctypes.Structure):
+    _fields_ = [("ctx", c_p), ("args", DemodArgs)]
+
+
 class TbcField(ctypes.Structure):
     _fields_ = [
         ("buf", c_p), ("buf_len", ctypes.c_int64), ("linelocs", c_p), ("nlines", ctypes.c_int32),
@@ -113,6 +117,12 @@ SIGNATURES = {
                                      ctypes.c_double, ctypes.c_double]),
     "ldg_set_sinc_lut": (ctypes.c_int, [c_p, c_p, ctypes.c_int32, ctypes.c_int32]),
     "ldg_demod_blocks": (ctypes.c_int, [c_p, ctypes.POINTER(DemodArgs)]),
+    "ldg_queue_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int32]),
+    "ldg_queue_destroy": (None, [c_p]),
+    "ldg_queue_submit": (ctypes.c_int, [c_p, ctypes.POINTER(WorkItem), ctypes.c_int32]),
+    "ldg_queue_set_schedule": (ctypes.c_int, [c_p, ctypes.c_int32, ctypes.c_int32]),
+    "ldg_queue_info": (ctypes.c_int, [c_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)]),
+    "ldg_queue_run": (ctypes.c_int, [c_p, c_p, ctypes.c_int32]),
     "ldg_tbc_fields": (ctypes.c_int, [c_p, ctypes.POINTER(TbcField), ctypes.c_int32, c_p]),
     "ldg_synchronize": (ctypes.c_int, [c_p]),
     "ldg_demod_scratch_bytes": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),

@@ -385,6 +385,13 @@ def tbc_batch(rf, fields, demod_ptr, out_u16_ptr, levels, coord_f32=False, first
     return (L.TbcField * n).from_buffer_copy(d.tobytes()) if n else (L.TbcField * 0)()
 
 
+def _lib_stream(stream):
+    """Stream handle for the C ABI: torch's default stream (handle 0 or
+    None) becomes cudaStreamLegacy (1), since a NULL handle would select the
+    context's own stream, which is not ordered with torch's work."""
+    return stream if stream else 1
+
+
 class LineLocator:
     """Batched Field.process() for a demodulated capture on the device."""
 
@@ -441,7 +448,7 @@ class LineLocator:
         minlen = math.floor(10 * rf.samplesperline * rf.linelen)
         rc = lib.ldg_sync_runs(rf._ctx.handle, ctypes.c_void_p(d05_ptr), int(n), sync_threshold(rf), minlen,
                                math.floor(rf.freq), math.ceil(rf.freq), starts.ctypes.data, lens.ctypes.data,
-                               means.ctypes.data, cap, ctypes.byref(nr), stream)
+                               means.ctypes.data, cap, ctypes.byref(nr), _lib_stream(stream))
         if rc == LDG_ERR_RANGE:
             return self.sync_runs(d05_ptr, n, stream, cap=int(nr.value) + 16)
         L.check(rc)
@@ -504,7 +511,7 @@ class LineLocator:
         a.phase_adjust = pam.data_ptr()
         a.field_phase = fph.data_ptr()
         a.scratch = scratch.data_ptr()
-        a.stream = stream
+        a.stream = _lib_stream(stream)
         ts = torch.cuda.ExternalStream(stream) if stream else torch.cuda.current_stream()
         ready = []
         if self.pal:
@@ -580,10 +587,12 @@ class LineLocator:
         (demodulated and complete in stream order on `stream`): scans the
         new samples, walks the chain, refines on the GPU.  `stream` is a
         torch.cuda.Stream (device work and allocations are ordered on it) or
-        None.  The sync-run scan runs on `scan_stream` when given (so it need
+        None for torch's current stream.  The sync-run scan runs on `scan_stream` when given (so it need
         not queue behind earlier refinement work on `stream`).  Returns the
         range of new indices into `self.fields`."""
         raw_scan = scan_stream.cuda_stream if isinstance(scan_stream, self.torch.cuda.Stream) else scan_stream
+        if stream is None:
+            stream = self.torch.cuda.current_stream()
         if isinstance(stream, self.torch.cuda.Stream):
             with self.torch.cuda.stream(stream):
                 return self._advance(nblocks, stream.cuda_stream, force_host,

@@ -280,13 +280,10 @@ class RFDecode(RFParams):
         rv["setupcount"] = self.setupcount
         return rv
 
-    def demod_blocks_device(self, in_ptr, nblocks, in_stride, outs, mtf_level=0, cut=True,
-                            in_kind=L.LDG_IN_INT16, stream=None):
-        """Batched form: demodulate `nblocks` blocks whose inputs and outputs
-        already live in device memory.  `outs` maps output names (demod,
-        demod_raw, demod_05, demod_burst, demod_pilot, rfhpf, efm,
-        audio_left, audio_right) to device pointers laid out block after
-        block; `mtf_level` is unscaled, as for demodblock.  Only enqueues."""
+    def demod_args(self, in_ptr, nblocks, in_stride, outs, mtf_level=0, cut=True, in_kind=L.LDG_IN_INT16,
+                   stream=None):
+        """ldg_demod_args for a device batch (see demod_blocks_device); loads
+        the filters of `mtf_level` into the context."""
         self._load_mtf(self.scaled_mtf(mtf_level))
         sl = self.output_slices(cut)
         a = L.DemodArgs()
@@ -311,6 +308,16 @@ class RFDecode(RFParams):
         has_audio = outs.get("audio_left") or outs.get("audio_right")
         a.audio = L.Slice(sl["audio"][0], sl["audio"][1] if has_audio else 0, 0)
         a.stream = stream
+        return a, sl
+
+    def demod_blocks_device(self, in_ptr, nblocks, in_stride, outs, mtf_level=0, cut=True,
+                            in_kind=L.LDG_IN_INT16, stream=None):
+        """Batched form: demodulate `nblocks` blocks whose inputs and outputs
+        already live in device memory.  `outs` maps output names (demod,
+        demod_raw, demod_05, demod_burst, demod_pilot, rfhpf, efm,
+        audio_left, audio_right) to device pointers laid out block after
+        block; `mtf_level` is unscaled, as for demodblock.  Only enqueues."""
+        a, sl = self.demod_args(in_ptr, nblocks, in_stride, outs, mtf_level, cut, in_kind, stream)
         L.check(self._ctx._lib.ldg_demod_blocks(self._ctx.handle, ctypes.byref(a)))
         return sl
 

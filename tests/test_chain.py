@@ -102,7 +102,7 @@ def test_abi_struct_sizes():
     for name, t in [("ldg_chain_params", L.ChainParams), ("ldg_chain_state", L.ChainState),
                     ("ldg_field_plan", L.FieldPlan), ("ldg_lines_consts", L.LinesConsts),
                     ("ldg_lines_args", L.LinesArgs), ("ldg_tbc_field", L.TbcField),
-                    ("ldg_demod_args", L.DemodArgs), ("ldg_slice", L.Slice)]:
+                    ("ldg_demod_args", L.DemodArgs), ("ldg_slice", L.Slice), ("ldg_work_item", L.WorkItem)]:
         assert h.ldg_abi_sizeof(name.encode()) == ctypes.sizeof(t), name
 
 
