@@ -205,13 +205,15 @@ class MixedBatch:
         capture, in capture order)."""
         from .lines import LineLocator
         stream = stream or self.stream
-        self.locators = []
+        if getattr(self, "locators", None) is None:
+            # one per capture, kept across passes (pinned staging buffers);
+            # a pass releases the previous pass's line-location buffers in
+            # stream order
+            self.locators = [LineLocator(self.rfs[system]) for system, _ in self.captures]
         self.fields = []
-        for (system, _), o, nb in zip(self.captures, self.outs, self.nblocks):
-            loc = LineLocator(self.rfs[system])
+        for loc, o, nb in zip(self.locators, self.outs, self.nblocks):
             arrays = {k: o[k] for k in FIELD_KEYS if k in o}
             self.fields.append(loc.locate(arrays, nb, stream))
-            self.locators.append(loc)
         return self.fields
 
     def field_geometry(self, system):
