@@ -144,6 +144,7 @@ def run_gpu(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     from ldgpu import RFDecode
+    from ldgpu import lib as L
     from ldgpu.field import tbc_fields, tbc_status
     from ldgpu.fieldread import blocks_in_capture
     from ldgpu.lines import LineLocator, field_levels, tbc_batch
@@ -365,6 +366,24 @@ def run_gpu(args):
     tbc_med = timed(lambda: tbc_fields(rf, all_descs, stream=sh))
     tbc_ms = [tbc_med]
 
+    # dropout detection of every field (Field.dropout_detect; not part of the
+    # step, which is demod + TBC): one ldg_dropouts launch
+    from ldgpu.dropouts import detect_located
+    drop_lists = detect_located(rf, flist, outs, stream=sh)
+    drop_total = sum(len(d[0]) for d in drop_lists)
+    from ldgpu import dropouts as LD
+    a = flist.arrays()
+    ddescs = [LD._field(*(outs[k].data_ptr() + 4 * int(a["startloc"][i]) for k in
+                          ("demod", "demod_05", "demod_raw", "rfhpf")),
+                        a["length"][i], int(a["linelocs_ptr"][i]), a["nlines"][i], a["lineoffset"][i],
+                        a["linecount"][i], a["isfirst"][i], a["hsync_len"][i]) for i in range(nf)]
+    darr = (L.DropoutField * nf)(*ddescs)
+    dprm = LD.dropout_params(rf)
+    d_drops = torch.empty(nf * LD.OUT_CAP * 3, dtype=torch.int32, device="cuda")
+    d_counts = torch.empty(2 * nf, dtype=torch.int32, device="cuda")
+    drop_med = timed(lambda: L.check(rf._ctx._lib.ldg_dropouts(rf._ctx.handle, ctypes.byref(dprm), darr, nf,
+                                                               d_drops.data_ptr(), d_counts.data_ptr(), None, sh)))
+
     peak, peak_kind = peaks()
     demod_bytes = nout * BYTES_PER_SAMPLE_DEMOD + nblocks * AUDIO_BYTES_PER_BLOCK
     achieved = demod_bytes / (dmed * 1e-3) / 1e9
@@ -414,6 +433,8 @@ def run_gpu(args):
                      "kernel": "ldg::demod_kernel",
                      "algorithmic_bytes_per_launch": demod_bytes},
         "tbc_roofline": {"achieved": tbc_bytes / (statistics.median(tbc_ms) * 1e-3) / 1e9, "unit": "GB/s"},
+        "dropouts": {"ms_all_fields": drop_med, "us_per_field": 1e3 * drop_med / nf, "dropouts_found": drop_total,
+                     "note": "ldg_dropouts over every field (Field.dropout_detect); outside the step"},
         "e2e": e2e,
         "plain": plain,
         "cpu_baseline": cpu,

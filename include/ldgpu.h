@@ -236,6 +236,51 @@ int ldg_queue_info(ldg_queue* q, int64_t* total_blocks, int32_t* grid);
  * head and scratch): order them on one stream. */
 int ldg_queue_run(ldg_queue* q, void* stream, int32_t use_graph);
 
+/* ---- Dropout detection (Field.dropout_detect, core.py:2829-2983) ---- */
+
+/* One field: its read (field-local sample 0 of each array), device memory. */
+typedef struct {
+    const float* demod;      /* video["demod"]     */
+    const float* demod_05;   /* video["demod_05"]  */
+    const float* demod_raw;  /* video["demod_raw"] */
+    const float* rfhpf;      /* rfhpf              */
+    int64_t len;             /* samples in the read */
+    const double* linelocs;  /* FP64 line locations, field-local */
+    int32_t nlines;
+    int32_t lineoffset, linecount, isfirst;
+    int32_t hsync_len;       /* int(Field.LT["hsync"][1]) */
+    int32_t pad;
+} ldg_dropout_field;
+
+typedef struct {
+    int32_t system;          /* LDG_NTSC / LDG_PAL */
+    int32_t video_rot;       /* rf.delays["video_rot"] (> 0) */
+    int32_t outlinelen;      /* SysParams outlinelen */
+    int32_t err_cap;         /* error samples kept per field */
+    int32_t out_cap;         /* dropouts kept per field */
+    int32_t pad;
+    double freq_mhz;         /* rf.freq */
+    double freq_hz_half;     /* rf.freq_hz_half */
+    double ire0, hz_ire;     /* DecoderParams */
+    double vsync_ire;        /* SysParams */
+} ldg_dropout_params;
+
+/* Field.dropout_detect for nfields fields in one launch: the per-sample
+ * error mask (dropout_detect_demod, core.py:2829-2887; the rfhpf standard
+ * deviation in FP64 over the field read), the merge of the error samples
+ * into spans (build_errlist, 2889-2908) and the spans as TBC line ranges
+ * (dropout_errlist_to_tbc, 2910-2960).  `fields` is a host array; every
+ * buffer is device memory.  Device outputs: drops[(f * out_cap + j) * 3 +
+ * {0, 1, 2}] = dropOuts fieldLine / startx / endx of dropout j of field f
+ * (core.py:2978-2983, 4536-4542); counts[2 f] = its dropouts, or -1 more than
+ * out_cap, -2 line locations out of order, -3 a vertical-sync line past the
+ * line locations (the reference raises IndexError); counts[2 f + 1] = error
+ * samples, or -1 more than err_cap (no dropouts listed then); rfstd (may be
+ * NULL) = the rfhpf standard deviation per field.  Enqueued on `stream`
+ * without waiting. */
+int ldg_dropouts(ldg_ctx* ctx, const ldg_dropout_params* p, const ldg_dropout_field* fields, int32_t nfields,
+                 int32_t* drops, int32_t* counts, double* rfstd, void* stream);
+
 /* ---- AC3-RF (2.88 MHz QPSK) demodulation, lddecode/ac3rf.py ---- */
 
 typedef struct ldg_ac3 ldg_ac3;
@@ -329,6 +374,8 @@ typedef struct ldg_field_plan {
     double start;
     int64_t readloc, first_block, nblocks, startloc, length;  /* the field's read window (fieldread) */
     int32_t valid, isfirst, linecount, proclines, has_prev, sync_confidence;
+    int32_t hsync_len;                        /* int(Field.LT["hsync"][1]) (dropout detection) */
+    int32_t pad0;
     double nextfieldoffset;
     double linelocs1[LDG_CHAIN_MAX_LINES];   /* pulse-level line locations (field-local samples) */
     uint8_t linebad[LDG_CHAIN_MAX_LINES];

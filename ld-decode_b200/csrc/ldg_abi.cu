@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "ldg_demod.cuh"
+#include "ldg_dropouts.cuh"
 #include "ldg_fft.cuh"
 #include "ldg_noalloc.h"
 #include "ldg_tbc.cuh"
@@ -101,6 +102,14 @@ struct ldg_ctx {
     } tws[4];
     int tws_next = 0;
     size_t lines_cap = 0;
+    // ldg_dropouts: device field descriptors and error lists; reused once the
+    // launch that last used them has completed
+    ldg::DropField* d_drop_fields = nullptr;
+    size_t drop_fields_cap = 0;
+    int* d_drop_errs = nullptr;
+    size_t drop_errs_cap = 0;
+    cudaEvent_t drop_done = nullptr;
+    bool drop_used = false;
     std::mutex mu;
 };
 
@@ -207,6 +216,10 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     cudaFree(c->d_status);
     cudaFree(c->d_lines);
     cudaFree(c->d_slots);
+    if (c->drop_used) cudaEventSynchronize(c->drop_done);
+    cudaFree(c->d_drop_fields);
+    cudaFree(c->d_drop_errs);
+    if (c->drop_done) cudaEventDestroy(c->drop_done);
     for (auto& w : c->tws) {
         if (w.used) cudaEventSynchronize(w.done);
         cudaFree(w.d_fields);
@@ -610,6 +623,72 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
     LDG_CK(cudaEventRecord(w.done, st));
     w.used = true;
+    return LDG_OK;
+}
+
+int ldg_dropouts(ldg_ctx* c, const ldg_dropout_params* p, const ldg_dropout_field* fields, int32_t nfields,
+                 int32_t* drops, int32_t* counts, double* rfstd, void* stream) {
+    if (!c || !p || (!fields && nfields) || (nfields && (!drops || !counts)))
+        return fail(LDG_ERR_ARG, "ldg_dropouts: NULL argument");
+    if (nfields < 0) return fail(LDG_ERR_ARG, "ldg_dropouts: negative field count");
+    if (p->system != LDG_NTSC && p->system != LDG_PAL) return fail(LDG_ERR_ARG, "ldg_dropouts: bad system");
+    if (p->video_rot <= 0) return fail(LDG_ERR_ARG, "ldg_dropouts: video_rot must be positive");
+    if (p->err_cap <= 0 || p->out_cap <= 0 || p->outlinelen <= 0)
+        return fail(LDG_ERR_ARG, "ldg_dropouts: caps and outlinelen must be positive");
+    if (!(p->hz_ire != 0) || !(p->freq_mhz > 0)) return fail(LDG_ERR_ARG, "ldg_dropouts: bad levels or rate");
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_dropout_field& f = fields[i];
+        if (!f.demod || !f.demod_05 || !f.demod_raw || !f.rfhpf || !f.linelocs)
+            return fail(LDG_ERR_ARG, "ldg_dropouts: NULL buffer");
+        if (f.len <= 0 || f.len > (1LL << 31) - 1) return fail(LDG_ERR_ARG, "ldg_dropouts: bad field length");
+        if (f.nlines < 2 || f.nlines > ldg::kMaxDropRegions + 1)
+            return fail(LDG_ERR_ARG, "ldg_dropouts: nlines must be in [2, 513]");
+        if (f.lineoffset < 0 || f.linecount <= 0 || f.lineoffset + f.linecount + 1 >= f.nlines)
+            return fail(LDG_ERR_ARG, "ldg_dropouts: lines lineoffset .. lineoffset + linecount + 1 must exist");
+        if (f.hsync_len < 0) return fail(LDG_ERR_ARG, "ldg_dropouts: negative hsync length");
+    }
+    if (nfields == 0) return LDG_OK;
+    const ldg_dropout_field& f0 = fields[0];
+    if (!is_device_ptr(f0.demod) || !is_device_ptr(f0.linelocs) || !is_device_ptr(drops) || !is_device_ptr(counts))
+        return fail(LDG_ERR_ARG, "ldg_dropouts: buffers must be device memory");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    if (!c->drop_done) LDG_CK(cudaEventCreateWithFlags(&c->drop_done, cudaEventDisableTiming));
+    if (c->drop_used) LDG_CK(cudaEventSynchronize(c->drop_done));
+    int rc = grow((void**)&c->d_drop_fields, &c->drop_fields_cap, (size_t)nfields * sizeof(ldg::DropField));
+    if (rc) return rc;
+    rc = grow((void**)&c->d_drop_errs, &c->drop_errs_cap, (size_t)nfields * p->err_cap * sizeof(int));
+    if (rc) return rc;
+    std::vector<ldg::DropField> h(nfields);
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_dropout_field& f = fields[i];
+        h[i] = {f.demod, f.demod_05, f.demod_raw, f.rfhpf, f.len, f.linelocs, f.nlines, f.lineoffset, f.linecount,
+                f.isfirst, f.hsync_len};
+    }
+    // pageable source: the copy has taken the data when the call returns
+    LDG_CK(cudaMemcpyAsync(c->d_drop_fields, h.data(), h.size() * sizeof(ldg::DropField), cudaMemcpyHostToDevice, st));
+    const bool pal = p->system == LDG_PAL;
+    auto hz = [&](double ire) { return (float)(p->ire0 + p->hz_ire * ire); };
+    ldg::DropConsts k;
+    k.system = p->system;
+    k.video_rot = p->video_rot;
+    k.outlinelen = p->outlinelen;
+    k.err_cap = p->err_cap;
+    k.out_cap = p->out_cap;
+    k.freq_mhz = p->freq_mhz;
+    k.fhalf = p->freq_hz_half;
+    // core.py:2846-2867: iretohz with DecoderParams, stored in float32 arrays
+    k.vmin = hz(pal ? -70 : -50);
+    k.vmax = hz(pal ? 150 : 160);
+    k.vmin05 = hz(-30);
+    k.vmax05 = hz(115);
+    k.smin = hz(pal ? p->vsync_ire - 60 : p->vsync_ire - 35);
+    k.smin05 = hz(p->vsync_ire - 10);
+    cudaError_t e = ldg::launch_dropouts(c->d_drop_fields, nfields, k, c->d_drop_errs, drops, counts, rfstd, st);
+    if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("dropout launch: ") + cudaGetErrorString(e));
+    LDG_CK(cudaEventRecord(c->drop_done, st));
+    c->drop_used = true;
     return LDG_OK;
 }
 

@@ -635,6 +635,7 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
         int dep = 0;
         if (!invalid) {
             const Timings LT = fp.get_timings();
+            pl.hsync_len = (int)LT.hsync_hi;
             const std::vector<VPulse> vp = fp.refinepulses(LT);
             const double meanlinelen = fp.compute_line_len(vp);
             // getLine0 (core.py:2156-2239)
@@ -773,6 +774,8 @@ extern "C" int64_t ldg_abi_sizeof(const char* name) {
     if (n == "ldg_demod_args") return sizeof(ldg_demod_args);
     if (n == "ldg_slice") return sizeof(ldg_slice);
     if (n == "ldg_work_item") return sizeof(ldg_work_item);
+    if (n == "ldg_dropout_field") return sizeof(ldg_dropout_field);
+    if (n == "ldg_dropout_params") return sizeof(ldg_dropout_params);
     return -1;
 }
 

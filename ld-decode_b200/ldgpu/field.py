@@ -138,6 +138,13 @@ class Field(FieldLogic):
             return pic, self.dsaudio, self.efmout
         return dsout, self.dsaudio, self.efmout
 
+    def dropout_detect(self):
+        """core.py:2962-2983 on the GPU: (lines, starts, ends) of the field's
+        dropouts, as LDdecode writes them into dropOuts."""
+        from .dropouts import detect_host_field
+        return detect_host_field(self.rf, self.data, self.linelocs, self.lineoffset, self.linecount,
+                                 self.isFirstField, int(self.LT["hsync"][1]))
+
     def audio_offset(self, audio, lastfieldwritten):
         """A/V alignment offset of the first audio sample (core.py:2644-2670)."""
         if lastfieldwritten and audio >= 16000:

@@ -18,6 +18,7 @@ LDG_IN_INT16, LDG_IN_FLOAT32 = 0, 1
 (LDG_F_RFHPF, LDG_F_VIDEO_G, LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT,
  LDG_F_EFM, LDG_F_VIDEO_G_ODD) = range(8)
 LDG_NFILTERS = 8
+LDG_ERR_ARG, LDG_ERR_CUDA, LDG_ERR_STATE, LDG_ERR_UNSUPPORTED, LDG_ERR_RANGE = -1, -2, -3, -4, -5
 
 ERRORS = {-1: "argument", -2: "cuda", -3: "state", -4: "unsupported", -5: "range"}
 
@@ -83,9 +84,22 @@ class FieldPlan(ctypes.Structure):
     _fields_ = [
         ("start", c_f64), ("readloc", c_i64), ("first_block", c_i64), ("nblocks", c_i64), ("startloc", c_i64),
         ("length", c_i64), ("valid", c_i32), ("isfirst", c_i32), ("linecount", c_i32), ("proclines", c_i32),
-        ("has_prev", c_i32), ("sync_confidence", c_i32), ("nextfieldoffset", c_f64),
+        ("has_prev", c_i32), ("sync_confidence", c_i32), ("hsync_len", c_i32), ("pad0", c_i32),
+        ("nextfieldoffset", c_f64),
         ("linelocs1", c_f64 * LDG_CHAIN_MAX_LINES), ("linebad", ctypes.c_uint8 * LDG_CHAIN_MAX_LINES),
     ]
+
+
+class DropoutField(ctypes.Structure):
+    _fields_ = [("demod", c_p), ("demod_05", c_p), ("demod_raw", c_p), ("rfhpf", c_p), ("len", c_i64),
+                ("linelocs", c_p), ("nlines", c_i32), ("lineoffset", c_i32), ("linecount", c_i32),
+                ("isfirst", c_i32), ("hsync_len", c_i32), ("pad", c_i32)]
+
+
+class DropoutParams(ctypes.Structure):
+    _fields_ = [("system", c_i32), ("video_rot", c_i32), ("outlinelen", c_i32), ("err_cap", c_i32),
+                ("out_cap", c_i32), ("pad", c_i32), ("freq_mhz", c_f64), ("freq_hz_half", c_f64),
+                ("ire0", c_f64), ("hz_ire", c_f64), ("vsync_ire", c_f64)]
 
 
 class LinesConsts(ctypes.Structure):
@@ -117,6 +131,8 @@ SIGNATURES = {
                                      ctypes.c_double, ctypes.c_double]),
     "ldg_set_sinc_lut": (ctypes.c_int, [c_p, c_p, ctypes.c_int32, ctypes.c_int32]),
     "ldg_demod_blocks": (ctypes.c_int, [c_p, ctypes.POINTER(DemodArgs)]),
+    "ldg_dropouts": (ctypes.c_int, [c_p, ctypes.POINTER(DropoutParams), ctypes.POINTER(DropoutField),
+                                    ctypes.c_int32, c_p, c_p, c_p, c_p]),
     "ldg_queue_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int32]),
     "ldg_queue_destroy": (None, [c_p]),
     "ldg_queue_submit": (ctypes.c_int, [c_p, ctypes.POINTER(WorkItem), ctypes.c_int32]),

@@ -47,7 +47,8 @@ _ML = L.LDG_CHAIN_MAX_LINES
 PLAN_DTYPE = _dtype_of(L.FieldPlan, {
     "start": "f8", "readloc": "i8", "first_block": "i8", "nblocks": "i8", "startloc": "i8", "length": "i8",
     "valid": "i4", "isfirst": "i4", "linecount": "i4", "proclines": "i4", "has_prev": "i4",
-    "sync_confidence": "i4", "nextfieldoffset": "f8", "linelocs1": ("f8", (_ML,)), "linebad": ("u1", (_ML,))})
+    "sync_confidence": "i4", "hsync_len": "i4", "pad0": "i4", "nextfieldoffset": "f8", "linelocs1": ("f8", (_ML,)),
+    "linebad": ("u1", (_ML,))})
 TBC_DTYPE = _dtype_of(L.TbcField, {
     "buf": "u8", "buf_len": "i8", "linelocs": "u8", "nlines": "i4", "lineoffset": "i4", "outwidth": "i4",
     "linesout": "i4", "outlinecount": "i4", "coord_f32": "i4", "inlinelen": "f8", "outlinelen": "f8",
@@ -225,8 +226,9 @@ class FieldLines:
     """Line locations of one field of a capture (device or host)."""
 
     def __init__(self, window, isfirst, linecount, lineoffset, linelocs_ptr=None, linelocs=None, nlines=0,
-                 field_phase=None, phase_adjust=None, sync_confidence=100, rows=None):
+                 field_phase=None, phase_adjust=None, sync_confidence=100, rows=None, hsync_len=0):
         self.window = window
+        self.hsync_len = int(hsync_len)    # int(Field.LT["hsync"][1])
         self.sync_confidence = int(sync_confidence)
         self.isFirstField = bool(isfirst)
         self.linecount = int(linecount)
@@ -280,7 +282,8 @@ class LocatedFields:
         if self._cache is not None:
             return self._cache
         pal = self.rf.system == "PAL"
-        keys = ("startloc", "length", "readloc", "isfirst", "linecount", "lineoffset", "nlines", "linelocs_ptr")
+        keys = ("startloc", "length", "readloc", "isfirst", "linecount", "lineoffset", "nlines", "linelocs_ptr",
+                "hsync_len")
         cols = {k: [] for k in keys}
         for part in self._parts:
             if part[0] == "batch":
@@ -298,6 +301,7 @@ class LocatedFields:
                     cols["linecount"].append(pl.linecount.astype(np.int64))
                     cols["lineoffset"].append(np.zeros(n, np.int64))
                 cols["nlines"].append(np.full(n, proclines_for(self.rf)))
+                cols["hsync_len"].append(pl.hsync_len.astype(np.int64))
                 rowb = ll.stride(0) * ll.element_size()
                 cols["linelocs_ptr"].append(np.uint64(ll.data_ptr()) + np.uint64(rowb) * np.arange(n, dtype=np.uint64))
             else:
@@ -310,6 +314,7 @@ class LocatedFields:
                 cols["linecount"].append([fl.linecount])
                 cols["lineoffset"].append([fl.lineoffset])
                 cols["nlines"].append([fl.nlines])
+                cols["hsync_len"].append([fl.hsync_len])
                 cols["linelocs_ptr"].append(np.array([dev.data_ptr()], np.uint64))
         self._cache = {k: (np.concatenate([np.asarray(x) for x in v]) if v else np.zeros(0, np.int64))
                        for k, v in cols.items()}
@@ -335,7 +340,7 @@ class LocatedFields:
                                   (2 if p.isfirst else 3) if pal else 0, linelocs_ptr=ll.data_ptr() + k * rowb,
                                   nlines=proclines_for(self.rf), field_phase=None if pal else (fph, k),
                                   phase_adjust=None if pal else (pam, k), sync_confidence=p.sync_confidence,
-                                  rows=(ll, k))
+                                  rows=(ll, k), hsync_len=int(p.hsync_len))
             k -= len(pl)
         raise IndexError("field index out of range")
 
@@ -677,7 +682,7 @@ class LineLocator:
             fl = FieldLines(w, f.isFirstField, f.linecount, f.lineoffset, linelocs=ll_host, nlines=len(ll_host),
                             field_phase=getattr(f, "fieldPhaseID", None),
                             phase_adjust=getattr(f, "phase_adjust_median", None),
-                            sync_confidence=f.sync_confidence)
+                            sync_confidence=f.sync_confidence, hsync_len=int(f.LT["hsync"][1]))
             dev_ll = torch.from_numpy(ll_host).to(torch.device("cuda", torch.cuda.current_device()))
             fl.linelocs_ptr = dev_ll.data_ptr()
             out._parts.append(("host", fl, dev_ll))

@@ -242,3 +242,25 @@ def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
     if return_symbols:
         return out, (torch.cat(qpsk_syms).numpy() if qpsk_syms else None)
     return out
+
+
+def inject_dropouts(cap, seed, count, min_len=40, max_len=1200, level=30):
+    """Replace `count` seeded spans of a capture (numpy int16 array or torch
+    int16 tensor, in place) with low-level noise: the RF carrier lost for
+    min_len..max_len samples, as a disc dropout looks.  Integer arithmetic
+    only, so the result is the same on every CPU and device.  Returns the
+    spans as (start, length) pairs, sorted."""
+    n = int(cap.shape[0])
+    rng = np.random.default_rng(seed)
+    starts = np.sort(rng.integers(0, max(n - max_len, 1), count))
+    lens = rng.integers(min_len, max_len + 1, count)
+    spans = []
+    for s0, ln in zip(starts.tolist(), lens.tolist()):
+        ln = min(ln, n - s0)
+        noise = rng.integers(-level, level + 1, ln).astype(np.int16)
+        if isinstance(cap, torch.Tensor):
+            cap[s0:s0 + ln] = torch.from_numpy(noise).to(cap.device)
+        else:
+            cap[s0:s0 + ln] = noise
+        spans.append((s0, ln))
+    return spans

@@ -18,7 +18,12 @@ by ldgpu.synth, and saves small .npz fixtures:
                         int16 output, next-field offset, mute flag;
   ac3_loopback.npz   -- AC3-RF demodulator (lddecode/ac3rf.py) on a seeded
                         DQPSK signal: baseband I/Q windows and the symbols of
-                        a clean (streamed in uneven blocks) and a noisy run.
+                        a clean (streamed in uneven blocks) and a noisy run;
+  dropouts_<sys>.npz -- dropout detection (Field.dropout_detect,
+                        core.py:2829-2996) on a capture with seeded dropouts:
+                        per field the line locations, flags, hsync length,
+                        rfhpf standard deviation, error sample indices, the
+                        merged error list and the final dropout lines/ranges.
 
 Nothing at test time reads /root/reference; only this script does.
 Usage: python tests/golden/make_golden.py
@@ -40,7 +45,7 @@ sys.path.insert(0, REF)
 import numpy as np  # noqa: E402
 
 from lddecode import core as refcore  # noqa: E402
-from ldgpu.synth import synth_capture  # noqa: E402
+from ldgpu.synth import inject_dropouts, synth_capture  # noqa: E402
 
 sys.path.insert(0, HERE)
 from audio_cases import AUDIO_CASES, audio_case_inputs  # noqa: E402
@@ -223,6 +228,62 @@ def field_fixture(system, seed, nfields=2):
     np.savez_compressed(os.path.join(HERE, f"field_{system.lower()}.npz"), **out)
 
 
+def dropout_fixture(system, seed, nfields=3, ndrop=60):
+    kw = dict(system=system, decode_analog_audio=0, decode_digital_audio=False)
+    rf = refcore.RFDecode(**kw)
+    src = BlockSource(rf, None, 1)
+    fieldcls = refcore.FieldPAL if system == "PAL" else refcore.FieldNTSC
+    if system == "PAL":
+        src.readlen = rf.linelen * 400
+    else:
+        src.readlen = ((rf.linelen * 350) // 16384) * 16384
+    fieldlen = int(rf.freq_hz / (rf.SysParams["FPS"] * 2))
+    ncap = (nfields + 3) * fieldlen + src.readlen + 8 * rf.blocklen
+    cap = synth_capture(system, ncap, seed=seed, start=CAPTURE_START, snr_db=38.0).numpy()
+    spans = inject_dropouts(cap, seed + 1000, ndrop)
+    src.cap = cap
+    out = {"capture_sha256": np.array(sha(cap)), "capture_len": np.array(ncap),
+           "capture_seed": np.array(seed), "capture_start": np.array(CAPTURE_START), "snr_db": np.array(38.0),
+           "drop_seed": np.array(seed + 1000), "drop_count": np.array(ndrop),
+           "drop_spans": np.array(spans, dtype=np.int64), "mtf_level": np.array(1.0)}
+    prev = None
+    start = 0
+    i = 0
+    tries = 0
+    while i < nfields:
+        rd = src.read_field(start)
+        assert rd is not None
+        decode, readloc = rd
+        f = fieldcls(rf, decode, prevfield=prev, initphase=(i == 0), fields_written=i,
+                     readloc=decode["startloc"])
+        f.process()
+        tries += 1
+        assert tries < nfields + 4
+        if not f.valid:
+            start = start + f.nextfieldoffset
+            prev = None
+            continue
+        iserr = f.dropout_detect_demod()
+        errmap = np.nonzero(iserr)[0]
+        errlist = f.build_errlist(errmap) if len(errmap) and errmap[-1] > f.linelocs[f.lineoffset] else []
+        lines, starts, ends = f.dropout_detect()
+        p = f"f{i}_"
+        out[p + "startloc"] = np.array(decode["startloc"])
+        out[p + "length"] = np.array(len(decode["video"]))
+        out[p + "linelocs"] = np.array(f.linelocs, dtype=np.float64)
+        out[p + "flags"] = np.array([int(f.isFirstField), f.linecount, f.lineoffset], dtype=np.int64)
+        out[p + "hsync_len"] = np.array(int(f.LT["hsync"][1]))
+        out[p + "rfstd"] = np.array(float(refcore.nb_std(f.data["rfhpf"])))
+        out[p + "errmap"] = errmap.astype(np.int64)
+        out[p + "errlist"] = np.array(errlist, dtype=np.float64).reshape(-1, 2)
+        out[p + "dropouts"] = np.array([lines, starts, ends], dtype=np.int64).reshape(3, -1)
+        start = start + f.nextfieldoffset - (readloc - decode["startloc"])
+        prev = f
+        i += 1
+    out["nfields"] = np.array(nfields)
+    np.savez_compressed(os.path.join(HERE, f"dropouts_{system.lower()}.npz"), **out)
+
+
 def lut_fixture():
     lut = np.load(os.path.join(REF, "lddecode", "sinc_lut.npz"))["downscale_sinc_lut"]
     rows = np.concatenate([np.arange(0, 65537, 997), [32767, 32768, 65535, 65536]])
@@ -292,6 +353,10 @@ def ac3_fixture():
 
 
 def main():
+    if sys.argv[1:] == ["dropouts"]:
+        dropout_fixture("NTSC", seed=41)
+        dropout_fixture("PAL", seed=42)
+        return
     audio_fixture()
     ac3_fixture()
     lut_fixture()
@@ -301,6 +366,8 @@ def main():
             demod_fixture(name, rf, kw, seed=11 + i)
     field_fixture("NTSC", seed=21)
     field_fixture("PAL", seed=22)
+    dropout_fixture("NTSC", seed=41)
+    dropout_fixture("PAL", seed=42)
     print("golden fixtures written to", HERE)
 
 

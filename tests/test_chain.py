@@ -67,6 +67,7 @@ def test_chain_matches_host_process(capture, monkeypatch):
         assert p.linecount == (263 if f.isFirstField else 262)
         assert p.nextfieldoffset == nxt
         assert p.sync_confidence == f.sync_confidence
+        assert p.hsync_len == int(f.LT["hsync"][1])
     assert nvalid >= 5
     print(rf.system, "reads", len(plans), "valid", nvalid)
 
@@ -102,7 +103,8 @@ def test_abi_struct_sizes():
     for name, t in [("ldg_chain_params", L.ChainParams), ("ldg_chain_state", L.ChainState),
                     ("ldg_field_plan", L.FieldPlan), ("ldg_lines_consts", L.LinesConsts),
                     ("ldg_lines_args", L.LinesArgs), ("ldg_tbc_field", L.TbcField),
-                    ("ldg_demod_args", L.DemodArgs), ("ldg_slice", L.Slice), ("ldg_work_item", L.WorkItem)]:
+                    ("ldg_demod_args", L.DemodArgs), ("ldg_slice", L.Slice), ("ldg_work_item", L.WorkItem),
+                    ("ldg_dropout_field", L.DropoutField), ("ldg_dropout_params", L.DropoutParams)]:
         assert h.ldg_abi_sizeof(name.encode()) == ctypes.sizeof(t), name
 
 
