@@ -236,6 +236,40 @@ int ldg_queue_info(ldg_queue* q, int64_t* total_blocks, int32_t* grid);
  * head and scratch): order them on one stream. */
 int ldg_queue_run(ldg_queue* q, void* stream, int32_t use_graph);
 
+/* ---- Ingest ---- */
+
+/* .lds captures (DomesdayDuplicator: four 10-bit samples in 5 bytes, most
+ * significant bits first) to the signed 16-bit samples of the reference's
+ * loader, load_packed_data_4_40 / unpack_data_4_40 (utils.py:371-410):
+ * out[i] = (v - 512) << 6, v the 10-bit value of sample first + i of
+ * `packed` (its sample 0 starts at byte 0).  `packed` (4-byte aligned, at
+ * least ((first + n - 1) / 4 + 1) * 5 bytes) and `out` (8-byte aligned) are
+ * device memory on the current device; enqueued on `stream`. */
+int ldg_unpack_lds(const uint8_t* packed, int64_t nbytes, int64_t first, int64_t n, int16_t* out, void* stream);
+
+/* ---- RF TBC (Field.rf_tbc, core.py:2724-2752) ---- */
+
+typedef struct {
+    const int16_t* input;    /* the field read's raw samples, Field.data["input"] (field-local sample 0) */
+    int64_t len;
+    const double* linelocs;  /* FP64 line locations, field-local */
+    int32_t nlines;
+    int32_t startline;       /* Field.lineoffset (NTSC), 1 (PAL) */
+    int32_t linecount;       /* output lines */
+    int32_t linelen;         /* int(round(inlinelen)) output samples per line */
+    double delay;            /* rf.delays["video_white"] */
+    int16_t* out;            /* linecount * linelen int16 */
+} ldg_rftbc_field;
+
+/* Field.rf_tbc for nfields fields: line l of the output is the cubic
+ * scaler (utils.py:37-70) over input[linelocs[l] - delay, linelocs[l+1] -
+ * delay] to linelen samples, rounded half to even, int16; FP64 without
+ * fused multiply-adds, bit-identical to the reference.  `fields` is a host
+ * array; all buffers device memory.  Enqueued on `stream` without waiting; a
+ * tap outside a field's read is reported by ldg_tbc_status (LDG_ERR_RANGE)
+ * and gives 0. */
+int ldg_rf_tbc(ldg_ctx* ctx, const ldg_rftbc_field* fields, int32_t nfields, void* stream);
+
 /* ---- Dropout detection (Field.dropout_detect, core.py:2829-2983) ---- */
 
 /* One field: its read (field-local sample 0 of each array), device memory. */

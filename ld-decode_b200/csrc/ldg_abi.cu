@@ -110,6 +110,10 @@ struct ldg_ctx {
     size_t drop_errs_cap = 0;
     cudaEvent_t drop_done = nullptr;
     bool drop_used = false;
+    ldg::RfTbcField* d_rftbc = nullptr;  // ldg_rf_tbc descriptors, same reuse rule
+    size_t rftbc_cap = 0;
+    cudaEvent_t rftbc_done = nullptr;
+    bool rftbc_used = false;
     std::mutex mu;
 };
 
@@ -217,6 +221,9 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     cudaFree(c->d_lines);
     cudaFree(c->d_slots);
     if (c->drop_used) cudaEventSynchronize(c->drop_done);
+    if (c->rftbc_used) cudaEventSynchronize(c->rftbc_done);
+    cudaFree(c->d_rftbc);
+    if (c->rftbc_done) cudaEventDestroy(c->rftbc_done);
     cudaFree(c->d_drop_fields);
     cudaFree(c->d_drop_errs);
     if (c->drop_done) cudaEventDestroy(c->drop_done);
@@ -623,6 +630,43 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
     LDG_CK(cudaEventRecord(w.done, st));
     w.used = true;
+    return LDG_OK;
+}
+
+int ldg_rf_tbc(ldg_ctx* c, const ldg_rftbc_field* fields, int32_t nfields, void* stream) {
+    if (!c || (!fields && nfields)) return fail(LDG_ERR_ARG, "ldg_rf_tbc: NULL argument");
+    if (nfields < 0) return fail(LDG_ERR_ARG, "ldg_rf_tbc: negative field count");
+    int max_lines = 0;
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_rftbc_field& f = fields[i];
+        if (!f.input || !f.linelocs || !f.out) return fail(LDG_ERR_ARG, "ldg_rf_tbc: NULL buffer");
+        if (f.len <= 0 || f.linelen <= 0 || f.linecount <= 0 || f.startline < 0)
+            return fail(LDG_ERR_ARG, "ldg_rf_tbc: bad field geometry");
+        if (f.startline + f.linecount >= f.nlines)
+            return fail(LDG_ERR_ARG, "ldg_rf_tbc: lines startline .. startline + linecount must exist");
+        if (f.linecount > max_lines) max_lines = f.linecount;
+    }
+    if (nfields == 0) return LDG_OK;
+    if (!is_device_ptr(fields[0].input) || !is_device_ptr(fields[0].linelocs) || !is_device_ptr(fields[0].out))
+        return fail(LDG_ERR_ARG, "ldg_rf_tbc: buffers must be device memory");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    if (!c->rftbc_done) LDG_CK(cudaEventCreateWithFlags(&c->rftbc_done, cudaEventDisableTiming));
+    if (c->rftbc_used) LDG_CK(cudaEventSynchronize(c->rftbc_done));
+    int rc = grow((void**)&c->d_rftbc, &c->rftbc_cap, (size_t)nfields * sizeof(ldg::RfTbcField));
+    if (rc) return rc;
+    std::vector<ldg::RfTbcField> h(nfields);
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_rftbc_field& f = fields[i];
+        h[i] = {f.input, f.len, f.linelocs, f.nlines, f.startline, f.linecount, f.linelen, f.delay, f.out,
+                c->d_status};
+    }
+    LDG_CK(cudaMemcpyAsync(c->d_rftbc, h.data(), h.size() * sizeof(ldg::RfTbcField), cudaMemcpyHostToDevice, st));
+    cudaError_t e = ldg::launch_rf_tbc(c->d_rftbc, nfields, max_lines, st);
+    if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("rf_tbc launch: ") + cudaGetErrorString(e));
+    LDG_CK(cudaEventRecord(c->rftbc_done, st));
+    c->rftbc_used = true;
     return LDG_OK;
 }
 

@@ -776,6 +776,7 @@ extern "C" int64_t ldg_abi_sizeof(const char* name) {
     if (n == "ldg_work_item") return sizeof(ldg_work_item);
     if (n == "ldg_dropout_field") return sizeof(ldg_dropout_field);
     if (n == "ldg_dropout_params") return sizeof(ldg_dropout_params);
+    if (n == "ldg_rftbc_field") return sizeof(ldg_rftbc_field);
     return -1;
 }
 

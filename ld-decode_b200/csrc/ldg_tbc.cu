@@ -243,4 +243,54 @@ cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout,
     return cudaSuccess;
 }
 
+// RF TBC (Field.rf_tbc, lddecode/core.py:2724-2752): each output line l is
+// the cubic scaler (utils.py:37-70) over the raw input between linelocs[l]
+// and linelocs[l + 1], both moved back by the video delay, rounded half to
+// even and stored as int16.  The arithmetic is the reference's FP64
+// expression term by term with every product and sum rounded on its own
+// (no fused multiply-adds), so the output is bit-identical.  One CTA per
+// (line, field).
+__global__ void __launch_bounds__(256) rf_tbc_kernel(const RfTbcField* fields) {
+    const RfTbcField& f = fields[blockIdx.y];
+    const int line = blockIdx.x;
+    if (line >= f.nout) return;
+    const int l = f.startline + line;
+    const double begin = __dsub_rn(f.ll[l], f.delay);
+    const double end = __dsub_rn(f.ll[l + 1], f.delay);
+    const double sf = __ddiv_rn(__dsub_rn(end, begin), (double)f.linelen);
+    int16_t* out = f.out + (long long)line * f.linelen;
+    for (int i = threadIdx.x; i < f.linelen; i += blockDim.x) {
+        const double coord = __dadd_rn(__dmul_rn((double)i, sf), begin);
+        // taps int(coord) - 1 .. int(coord) + 2 inside the read: 1 <= coord < len - 2
+        if (!(coord >= 1.0 && coord < (double)(f.len - 2))) {
+            atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
+            out[i] = 0;
+            continue;
+        }
+        const long long ic = (long long)coord;
+        const long long s = ic - 1;
+        const double p0 = f.in[s], p1 = f.in[s + 1], p2 = f.in[s + 2], p3 = f.in[s + 3];
+        const double x = __dsub_rn(coord, (double)ic);
+        // p1 + 0.5 x (p2 - p0 + x (2 p0 - 5 p1 + 4 p2 - p3 + x (3 (p1 - p2) + p3 - p0)))
+        const double c = __dsub_rn(__dadd_rn(__dmul_rn(3.0, __dsub_rn(p1, p2)), p3), p0);
+        const double b = __dadd_rn(
+            __dsub_rn(__dadd_rn(__dsub_rn(__dmul_rn(2.0, p0), __dmul_rn(5.0, p1)), __dmul_rn(4.0, p2)), p3),
+            __dmul_rn(x, c));
+        const double a = __dadd_rn(__dsub_rn(p2, p0), __dmul_rn(x, b));
+        const double v = __dadd_rn(p1, __dmul_rn(__dmul_rn(0.5, x), a));
+        out[i] = (int16_t)(int)rint(v);
+    }
+}
+
+cudaError_t launch_rf_tbc(const RfTbcField* dfields, int nfields, int max_lines, cudaStream_t stream) {
+    if (nfields <= 0 || max_lines <= 0) return cudaSuccess;
+    for (int off = 0; off < nfields; off += 65535) {
+        const int n = nfields - off < 65535 ? nfields - off : 65535;
+        rf_tbc_kernel<<<dim3((unsigned)max_lines, (unsigned)n), 256, 0, stream>>>(dfields + off);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 }  // namespace ldg

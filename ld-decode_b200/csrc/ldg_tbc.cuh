@@ -31,4 +31,19 @@ struct TbcField {
 cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout, const float* lut,
                        double threshold_mult, cudaStream_t stream);
 
+struct RfTbcField {
+    const int16_t* in;   // raw samples of the field read (field-local sample 0)
+    long long len;
+    const double* ll;
+    int nlines;
+    int startline;       // lineoffset (NTSC) or 1 (PAL)
+    int nout;            // output lines (linecount)
+    int linelen;         // output samples per line
+    double delay;        // video_white delay (samples)
+    int16_t* out;
+    int* status;         // LDG_TBC_OUT_OF_RANGE when a tap leaves the read
+};
+
+cudaError_t launch_rf_tbc(const RfTbcField* dfields, int nfields, int max_lines, cudaStream_t stream);
+
 }  // namespace ldg

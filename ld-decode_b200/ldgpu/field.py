@@ -138,6 +138,13 @@ class Field(FieldLogic):
             return pic, self.dsaudio, self.efmout
         return dsout, self.dsaudio, self.efmout
 
+    def rf_tbc(self, linelocs=None):
+        """core.py:2724-2752 on the GPU: the TBC'd raw RF as int16."""
+        from .rftbc import rf_tbc_host_field
+        if linelocs is None:
+            linelocs = self.linelocs
+        return rf_tbc_host_field(self.rf, self.data["input"], linelocs, self.lineoffset, self.linecount)
+
     def dropout_detect(self):
         """core.py:2962-2983 on the GPU: (lines, starts, ends) of the field's
         dropouts, as LDdecode writes them into dropOuts."""

@@ -90,6 +90,11 @@ class FieldPlan(ctypes.Structure):
     ]
 
 
+class RfTbcField(ctypes.Structure):
+    _fields_ = [("input", c_p), ("len", c_i64), ("linelocs", c_p), ("nlines", c_i32), ("startline", c_i32),
+                ("linecount", c_i32), ("linelen", c_i32), ("delay", c_f64), ("out", c_p)]
+
+
 class DropoutField(ctypes.Structure):
     _fields_ = [("demod", c_p), ("demod_05", c_p), ("demod_raw", c_p), ("rfhpf", c_p), ("len", c_i64),
                 ("linelocs", c_p), ("nlines", c_i32), ("lineoffset", c_i32), ("linecount", c_i32),
@@ -131,6 +136,8 @@ SIGNATURES = {
                                      ctypes.c_double, ctypes.c_double]),
     "ldg_set_sinc_lut": (ctypes.c_int, [c_p, c_p, ctypes.c_int32, ctypes.c_int32]),
     "ldg_demod_blocks": (ctypes.c_int, [c_p, ctypes.POINTER(DemodArgs)]),
+    "ldg_unpack_lds": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, c_p, c_p]),
+    "ldg_rf_tbc": (ctypes.c_int, [c_p, ctypes.POINTER(RfTbcField), ctypes.c_int32, c_p]),
     "ldg_dropouts": (ctypes.c_int, [c_p, ctypes.POINTER(DropoutParams), ctypes.POINTER(DropoutField),
                                     ctypes.c_int32, c_p, c_p, c_p, c_p]),
     "ldg_queue_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int32]),

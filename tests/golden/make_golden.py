@@ -19,6 +19,12 @@ by ldgpu.synth, and saves small .npz fixtures:
   ac3_loopback.npz   -- AC3-RF demodulator (lddecode/ac3rf.py) on a seeded
                         DQPSK signal: baseband I/Q windows and the symbols of
                         a clean (streamed in uneven blocks) and a noisy run;
+  lds_unpack.npz     -- the reference's .lds unpacker (unpack_data_4_40,
+                        utils.py:371-391) on seeded random packed bytes at
+                        several offsets and lengths;
+  rftbc_<sys>.npz    -- RF TBC (Field.rf_tbc, core.py:2724-2752, cubic scale
+                        utils.py:37-70) of two fields: SHA-256 of each int16
+                        output, a subsample and two whole lines;
   dropouts_<sys>.npz -- dropout detection (Field.dropout_detect,
                         core.py:2829-2996) on a capture with seeded dropouts:
                         per field the line locations, flags, hsync length,
@@ -284,6 +290,69 @@ def dropout_fixture(system, seed, nfields=3, ndrop=60):
     np.savez_compressed(os.path.join(HERE, f"dropouts_{system.lower()}.npz"), **out)
 
 
+def rftbc_fixture(system, seed, nfields=2):
+    kw = dict(system=system, decode_analog_audio=0, decode_digital_audio=False)
+    rf = refcore.RFDecode(**kw)
+    src = BlockSource(rf, None, 1)
+    fieldcls = refcore.FieldPAL if system == "PAL" else refcore.FieldNTSC
+    if system == "PAL":
+        src.readlen = rf.linelen * 400
+    else:
+        src.readlen = ((rf.linelen * 350) // 16384) * 16384
+    fieldlen = int(rf.freq_hz / (rf.SysParams["FPS"] * 2))
+    ncap = (nfields + 2) * fieldlen + src.readlen + 8 * rf.blocklen
+    cap = synth_capture(system, ncap, seed=seed, start=CAPTURE_START).numpy()
+    src.cap = cap
+    out = {"capture_sha256": np.array(sha(cap)), "capture_len": np.array(ncap), "capture_seed": np.array(seed),
+           "capture_start": np.array(CAPTURE_START), "mtf_level": np.array(1.0),
+           "video_white": np.array(float(rf.delays["video_white"])), "inlinelen": np.array(float(rf.linelen))}
+    prev = None
+    start = 0
+    i = 0
+    while i < nfields:
+        decode, readloc = src.read_field(start)
+        f = fieldcls(rf, decode, prevfield=prev, initphase=(i == 0), fields_written=i,
+                     readloc=decode["startloc"])
+        f.process()
+        if not f.valid:
+            start = start + f.nextfieldoffset
+            prev = None
+            continue
+        rt = np.asarray(f.rf_tbc())
+        linelen = int(round(f.inlinelen))
+        p = f"f{i}_"
+        out[p + "startloc"] = np.array(decode["startloc"])
+        out[p + "length"] = np.array(len(decode["input"]))
+        out[p + "linelocs"] = np.array(f.linelocs, dtype=np.float64)
+        out[p + "flags"] = np.array([int(f.isFirstField), f.linecount, f.lineoffset], dtype=np.int64)
+        out[p + "sha256"] = np.array(sha(rt.astype(np.int16)))
+        out[p + "n"] = np.array(len(rt))
+        out[p + "sub"] = rt[::13].astype(np.int16)
+        out[p + "lines"] = np.stack([rt[20 * linelen:21 * linelen], rt[150 * linelen:151 * linelen]]).astype(np.int16)
+        start = start + f.nextfieldoffset - (readloc - decode["startloc"])
+        prev = f
+        i += 1
+    out["nfields"] = np.array(nfields)
+    np.savez_compressed(os.path.join(HERE, f"rftbc_{system.lower()}.npz"), **out)
+
+
+def lds_fixture():
+    import io
+    from lddecode import utils as refutils
+    rng = np.random.default_rng(71)
+    data = rng.integers(0, 256, 5 * 1200, dtype=np.uint8)
+    out = {"packed": data}
+    # (first sample, samples): the reference's file loader on an in-memory .lds (it needs
+    # multiples of 4 samples, as the decoder reads them)
+    cases = [(0, 4000), (401, 4000), (0, 4096), (2, 4096), (5, 1000), (8, 1), (3, 2048), (3001, 1024)]
+    f = io.BytesIO(data.tobytes())
+    for k, (sample, readlen) in enumerate(cases):
+        out[f"case{k}"] = np.array([sample, readlen])
+        out[f"out{k}"] = np.asarray(refutils.load_packed_data_4_40(f, sample, readlen))
+    out["ncases"] = np.array(len(cases))
+    np.savez_compressed(os.path.join(HERE, "lds_unpack.npz"), **out)
+
+
 def lut_fixture():
     lut = np.load(os.path.join(REF, "lddecode", "sinc_lut.npz"))["downscale_sinc_lut"]
     rows = np.concatenate([np.arange(0, 65537, 997), [32767, 32768, 65535, 65536]])
@@ -357,6 +426,13 @@ def main():
         dropout_fixture("NTSC", seed=41)
         dropout_fixture("PAL", seed=42)
         return
+    if sys.argv[1:] == ["lds"]:
+        lds_fixture()
+        return
+    if sys.argv[1:] == ["rftbc"]:
+        rftbc_fixture("NTSC", seed=21)
+        rftbc_fixture("PAL", seed=22)
+        return
     audio_fixture()
     ac3_fixture()
     lut_fixture()
@@ -368,6 +444,9 @@ def main():
     field_fixture("PAL", seed=22)
     dropout_fixture("NTSC", seed=41)
     dropout_fixture("PAL", seed=42)
+    rftbc_fixture("NTSC", seed=21)
+    rftbc_fixture("PAL", seed=22)
+    lds_fixture()
     print("golden fixtures written to", HERE)
 
 

@@ -104,7 +104,8 @@ def test_abi_struct_sizes():
                     ("ldg_field_plan", L.FieldPlan), ("ldg_lines_consts", L.LinesConsts),
                     ("ldg_lines_args", L.LinesArgs), ("ldg_tbc_field", L.TbcField),
                     ("ldg_demod_args", L.DemodArgs), ("ldg_slice", L.Slice), ("ldg_work_item", L.WorkItem),
-                    ("ldg_dropout_field", L.DropoutField), ("ldg_dropout_params", L.DropoutParams)]:
+                    ("ldg_dropout_field", L.DropoutField), ("ldg_dropout_params", L.DropoutParams),
+                    ("ldg_rftbc_field", L.RfTbcField)]:
         assert h.ldg_abi_sizeof(name.encode()) == ctypes.sizeof(t), name
 
 
