@@ -177,8 +177,9 @@ def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
 
     `start` offsets the absolute sample index (so different seeds/offsets give
     different field phases).  With qpsk=True the 2.88 MHz carrier is
-    differential QPSK at 288 kbaud (RRC, alpha 0.5); return_symbols=True also
-    returns the transmitted symbols (per chunk, concatenated).  The same (system, nsamples, seed, start, device
+    differential QPSK at 288 kbaud (RRC, alpha 0.5), one continuous symbol
+    stream over the whole capture; return_symbols=True also returns the
+    transmitted symbols.  The same (system, nsamples, seed, start, device
     type) always gives the same capture.
     """
     dev = torch.device(device)
@@ -189,11 +190,22 @@ def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
         sym_rate = 288e3
         sps_ = 40  # generate symbols at 11.52 MS/s then interpolate
         rrc = torch.tensor(_rrc(0.5, sps_, 6), dtype=torch.float64, device=dev)
+        # the whole symbol stream up front, so the symbol clock and the
+        # differential phase run on across chunks: symbol k of the stream is
+        # centred on sample (k + 6) * FS / sym_rate (the RRC's 6-symbol delay)
+        nsym_all = int(nsamples * sym_rate / FS_HZ) + 2
+        sgen = torch.Generator(device=dev)
+        sgen.manual_seed(int(seed) * 1000003 + 999331)
+        qsyms = torch.randint(0, 4, (nsym_all,), generator=sgen, device=dev)
+        # differential QPSK: symbol s advances the transmitted carrier phase by
+        # 0, -90, +90 or 180 degrees; a receiver mixing with exp(+j w t) sees
+        # the negated step, which its differential detector reports as s
+        quarter = torch.remainder(torch.cumsum(torch.tensor([0, -1, 1, 2], device=dev)[qsyms], 0), 4)
+        ph = math.pi / 4 + (math.pi / 2) * quarter.to(torch.float64)
+        qiq = torch.complex(torch.cos(ph), torch.sin(ph))
     sigma = math.sqrt(0.5 / (10 ** (snr_db / 10)))
     out = torch.empty(nsamples, dtype=torch.int16, device=dev)
     phase = 0
-    qpsk_phase = 0.0
-    qpsk_syms = []
     for c0 in range(0, nsamples, CHUNK):
         clen = min(CHUNK, nsamples - c0)
         gen = torch.Generator(device=dev)
@@ -219,19 +231,17 @@ def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
             e = _efm_wave(gen, c0, clen + 256, dev)
             sig = sig + 0.12 * _fftconv(e, efm_taps)[128:128 + clen]
         if qpsk:
-            nsym = int(clen * sym_rate / FS_HZ) + 16
-            # differential QPSK: symbol s advances the transmitted carrier phase by
-            # 0, -90, +90 or 180 degrees; a receiver mixing with exp(+j w t) sees
-            # the negated step, which its differential detector reports as s
-            syms = torch.randint(0, 4, (nsym,), generator=gen, device=dev)
-            step = torch.tensor([0.0, -0.5, 0.5, 1.0], dtype=torch.float64, device=dev)[syms]
-            iq = torch.exp(1j * (math.pi / 4 + math.pi * (qpsk_phase + torch.cumsum(step, 0))))
-            qpsk_phase = float(torch.remainder(qpsk_phase + step.sum(), 2.0).item())
-            qpsk_syms.append(syms.to(torch.uint8).cpu())
-            up = torch.zeros(nsym * sps_, dtype=torch.complex128, device=dev)
-            up[::sps_] = iq
+            # upsampled symbols k0 .. k1 (the RRC reaches 12 symbols back), filtered,
+            # evaluated at this chunk's absolute sample times
+            rs = sym_rate * sps_ / FS_HZ
+            k0 = int(c0 * sym_rate / FS_HZ) - 13
+            k1 = int((c0 + clen) * sym_rate / FS_HZ) + 2
+            up = torch.zeros((k1 - k0) * sps_, dtype=torch.complex128, device=dev)
+            ka, kb = max(k0, 0), min(k1, nsym_all)
+            if kb > ka:
+                up[(ka - k0) * sps_:(kb - k0) * sps_:sps_] = qiq[ka:kb]
             bb = torch.complex(_fftconv(up.real, rrc), _fftconv(up.imag, rrc))
-            ti = torch.arange(clen, device=dev, dtype=torch.float64) * (sym_rate * sps_ / FS_HZ)
+            ti = (torch.arange(c0, c0 + clen, device=dev, dtype=torch.float64) * rs) - k0 * sps_
             i0 = torch.clamp(ti.floor().to(torch.int64), 0, bb.shape[0] - 2)
             fr = ti - i0
             bbi = bb[i0] * (1 - fr) + bb[i0 + 1] * fr
@@ -240,7 +250,7 @@ def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
         sig = sig + sigma * torch.randn(clen, generator=gen, device=dev, dtype=torch.float64)
         out[c0:c0 + clen] = torch.clamp(torch.round(sig * scale), -32768, 32767).to(torch.int16)
     if return_symbols:
-        return out, (torch.cat(qpsk_syms).numpy() if qpsk_syms else None)
+        return out, (qsyms.to(torch.uint8).cpu().numpy() if qpsk else None)
     return out
 
 
