@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--chunks", type=int, default=4,
                     help="pipeline chunks of blocks per step (1: demod, then line locations, then TBC)")
+    ap.add_argument("--chunk-taper", type=float, default=0.7,
+                    help="chunk c gets a share of the blocks proportional to taper**c")
     ap.add_argument("--mixed", type=int, default=0,
                     help="mixed-batch workload instead: this many captures, lengths uniform in 0.5-8 s, "
                          "half NTSC / half PAL, own seed and SNR (30-45 dB) each")
@@ -181,7 +183,11 @@ def run_gpu(args):
     loc = LineLocator(rf)
     levels = field_levels(rf)
     nchunks = max(1, min(args.chunks, nblocks // 64))
-    bounds = [round(c * nblocks / nchunks) for c in range(nchunks + 1)]
+    # chunk c holds a share proportional to taper**c of the blocks: a smaller
+    # last chunk shortens the tail (its line locations and TBC) after the demod
+    w = [args.chunk_taper ** c for c in range(nchunks)]
+    cum = np.concatenate([[0.0], np.cumsum(w)]) / sum(w)
+    bounds = [int(round(x * nblocks)) for x in cum]
     streamB = torch.cuda.Stream(priority=-1)   # line locations
     streamC = torch.cuda.Stream(priority=-1)   # TBC of ranges whose line locations are final
     streamS = torch.cuda.Stream(priority=-1)   # sync-run scans
