@@ -138,51 +138,90 @@ struct AudioTaps {
     const float2* filt1[2];
 };
 
-// S holds Z = FFT_M(x[2m] + i x[2m+1]).  Computes X[k] for k = 0..M, parks
-// it, taps the audio sub-bands and, if F is given, leaves the C2R input of
-// X * F in S.
-__device__ void post_r2c(float2* S, const Tables& t, float2* park, const float2* F, const AudioTaps* au) {
-    for (int k = threadIdx.x; k <= kM / 2; k += kThreads) {
-        if (k == 0) {
-            const float2 z = S[0];
-            const float x0 = z.x + z.y, xm = z.x - z.y;
-            park[0] = make_float2(x0, xm);
-            if (F) c2r_dc(S, x0, xm, F);
-            continue;
-        }
-        const float2 zk = S[pad(k)], zm = S[pad(kM - k)];
-        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-        const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
-        const float2 wk = __ldg(t.t32 + k);
-        const float2 tt = cmul(wk, o);
-        const float2 xk = cadd(e, tt);
-        const float2 xm = cconj(csub(e, tt));
-        park[k] = xk;
-        if (k != kM / 2) park[kM - k] = xm;
-        if (au) {
+// Post-processing of one bin pair (k, M-k), 0 < k <= M/2, from Z[k], Z[M-k]
+// (S), the real-FFT twiddle wk and, if F is given, the filter bins.
+__device__ __forceinline__ void post_pair(float2* S, float2* park, const AudioTaps* au, int k, float2 zk, float2 zm,
+                                          float2 wk, const float2* F, float2 fk, float2 fm) {
+    const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    const float2 tt = cmul(wk, o);
+    const float2 xk = cadd(e, tt);
+    const float2 xm = cconj(csub(e, tt));
+    park[k] = xk;
+    if (k != kM / 2) park[kM - k] = xm;
+    if (au) {
 #pragma unroll
-            for (int ch = 0; ch < 2; ++ch) {
-                const int rel = k - au->lowbin[ch];
-                if (rel >= 0 && rel <= 512) {
-                    const float2 xb = rel < 512 ? xk : cconj(xk);
-                    au->A[ch * padded(1024) + pad(rel)] = cmul(xb, __ldg(au->filt1[ch] + rel));
-                }
+        for (int ch = 0; ch < 2; ++ch) {
+            const int rel = k - au->lowbin[ch];
+            if (rel >= 0 && rel <= 512) {
+                const float2 xb = rel < 512 ? xk : cconj(xk);
+                au->A[ch * padded(1024) + pad(rel)] = cmul(xb, __ldg(au->filt1[ch] + rel));
             }
         }
-        if (F) c2r_pair(S, k, cmul(xk, __ldg(F + k)), cmul(xm, __ldg(F + kM - k)), wk);
+    }
+    if (F) c2r_pair(S, k, cmul(xk, fk), cmul(xm, fm), wk);
+}
+
+// S holds Z = FFT_M(x[2m] + i x[2m+1]).  Computes X[k] for k = 0..M, parks
+// it, taps the audio sub-bands and, if F is given, leaves the C2R input of
+// X * F in S.  Thread t handles k = t + 1024 i; two bins per step with all
+// their loads issued before the arithmetic (latency of the global twiddle
+// and filter loads overlapped).
+__device__ void post_r2c(float2* S, const Tables& t, float2* park, const float2* F, const AudioTaps* au) {
+    const int t0 = threadIdx.x;
+    const float2 zero = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int i = 0; i < 8; i += 2) {
+        const int ka = t0 + i * kThreads, kb = ka + kThreads;  // kb > 0; ka == 0 only for thread 0
+        const float2 zka = S[pad(ka)];
+        const float2 zma = ka ? S[pad(kM - ka)] : zero;
+        const float2 zkb = S[pad(kb)], zmb = S[pad(kM - kb)];
+        const float2 wa = __ldg(t.t32 + ka), wb = __ldg(t.t32 + kb);
+        float2 fka = zero, fma = zero, fkb = zero, fmb = zero;
+        if (F) {
+            fka = __ldg(F + ka);
+            fma = __ldg(F + kM - ka);
+            fkb = __ldg(F + kb);
+            fmb = __ldg(F + kM - kb);
+        }
+        if (ka == 0) {
+            const float x0 = zka.x + zka.y, xm = zka.x - zka.y;
+            park[0] = make_float2(x0, xm);
+            if (F) c2r_dc(S, x0, xm, F);
+        } else {
+            post_pair(S, park, au, ka, zka, zma, wa, F, fka, fma);
+        }
+        post_pair(S, park, au, kb, zkb, zmb, wb, F, fkb, fmb);
+    }
+    if (t0 == 0) {  // k = M/2
+        const int k = kM / 2;
+        const float2 z = S[pad(k)];
+        post_pair(S, park, au, k, z, z, __ldg(t.t32 + k), F, F ? __ldg(F + k) : zero, F ? __ldg(F + k) : zero);
     }
 }
 
-// C2R input of X * F in S, X from the parked spectrum.
+// C2R input of X * F in S, X from the parked spectrum; two bins per step,
+// loads first.
 __device__ void pre_c2r(float2* S, const Tables& t, const float2* park, const float2* F) {
-    for (int k = threadIdx.x; k <= kM / 2; k += kThreads) {
-        if (k == 0) {
-            const float2 z = park[0];
-            c2r_dc(S, z.x, z.y, F);
-            continue;
+    const int t0 = threadIdx.x;
+#pragma unroll 1
+    for (int i = 0; i < 8; i += 2) {
+        const int ka = t0 + i * kThreads, kb = ka + kThreads;
+        const float2 xka = park[ka], xkb = park[kb], xmb = park[kM - kb];
+        const float2 xma = ka ? park[kM - ka] : xka;
+        const float2 fka = __ldg(F + ka), fma = __ldg(F + kM - ka), fkb = __ldg(F + kb), fmb = __ldg(F + kM - kb);
+        const float2 wa = __ldg(t.t32 + ka), wb = __ldg(t.t32 + kb);
+        if (ka == 0) {
+            c2r_dc(S, xka.x, xka.y, F);
+        } else {
+            c2r_pair(S, ka, cmul(xka, fka), cmul(xma, fma), wa);
         }
-        const float2 xk = park[k], xm = park[kM - k];
-        c2r_pair(S, k, cmul(xk, __ldg(F + k)), cmul(xm, __ldg(F + kM - k)), __ldg(t.t32 + k));
+        c2r_pair(S, kb, cmul(xkb, fkb), cmul(xmb, fmb), wb);
+    }
+    if (t0 == 0) {
+        const int k = kM / 2;
+        const float2 x = park[k];
+        c2r_pair(S, k, cmul(x, __ldg(F + k)), cmul(x, __ldg(F + k)), __ldg(t.t32 + k));
     }
 }
 
@@ -248,11 +287,7 @@ __device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float
         const float clip_hi = p.fs_hz * 0.75f;
         float* oraw = p.o_raw ? p.o_raw + (long long)blk * p.s_video.len : nullptr;
         const int vs = p.s_video.start, vl = p.s_video.len;
-        for (int m = threadIdx.x; m < kM; m += kThreads) {
-            const float2 ze = parkZ[m];
-            const float2 zo = S[pad(m)];
-            const float de = (m == 0) ? 0.0f : fm_disc(ze, S[pad(m - 1)], kfs);
-            const float dodd = fm_disc(zo, ze, kfs);
+        auto disc_store = [&](int m, float de, float dodd) {
             if (oraw) {
                 const int i0 = 2 * m - vs;
                 if (i0 >= 0 && i0 + 1 < vl && ((reinterpret_cast<uintptr_t>(oraw + i0) & 7) == 0)) {
@@ -263,6 +298,20 @@ __device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float
                 }
             }
             parkX[m] = make_float2(fminf(fmaxf(de, 1500000.0f), clip_hi), fminf(fmaxf(dodd, 1500000.0f), clip_hi));
+        };
+        // two samples per step, the parked (L2) loads first
+#pragma unroll 1
+        for (int m = threadIdx.x; m < kM; m += 2 * kThreads) {
+            const int mb = m + kThreads;
+            const float2 zea = parkZ[m], zeb = parkZ[mb];
+            const float2 zoa = S[pad(m)], zob = S[pad(mb)];
+            const float2 zpa = m ? S[pad(m - 1)] : zoa, zpb = S[pad(mb - 1)];
+            const float dea = (m == 0) ? 0.0f : fm_disc(zea, zpa, kfs);
+            const float doa = fm_disc(zoa, zea, kfs);
+            const float deb = fm_disc(zeb, zpb, kfs);
+            const float dob = fm_disc(zob, zeb, kfs);
+            disc_store(m, dea, doa);
+            disc_store(mb, deb, dob);
         }
     }
     __syncthreads();
