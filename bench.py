@@ -47,7 +47,7 @@ AUDIO_BYTES_PER_BLOCK = 2 * 991 * 4
 # DRAM bytes (read + write) per block of the demod kernel, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the NTSC 1 s case divided by
 # its 1261 blocks; traffic scales with blocks.  None until measured.
-DRAM_BYTES_PER_BLOCK = 1_087_000
+DRAM_BYTES_PER_BLOCK = 980_500
 
 
 def parse():

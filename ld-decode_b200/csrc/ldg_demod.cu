@@ -240,6 +240,16 @@ __device__ void audio_stage(const DemodParams& p, float2* A, const Tables& t, in
     }
 }
 
+// Invalidate this CTA's scratch (parkX and parkZ, kScratchPerCta bytes,
+// 128-byte aligned) in L2 without write-back: discard.global.L2 per 128-byte
+// line.  Every thread of the CTA is past its last scratch access.
+__device__ __forceinline__ void discard_scratch(float2* base) {
+    char* b = reinterpret_cast<char*>(base);
+    constexpr int kLines = (int)(kScratchPerCta / 128);
+    for (int l = threadIdx.x; l < kLines; l += kThreads)
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(b + (size_t)l * 128) : "memory");
+}
+
 // One block: every requested output of block `blk` of p.  parkX/parkZ: this
 // CTA's scratch (kScratchPerCta).  Ends with the CTA's threads in step.
 __device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float2* S, float2* A, const Tables& t,
@@ -336,6 +346,9 @@ __device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float
                                 p.roll[o]});
     }
     __syncthreads();
+    // the parked spectra are dead: drop their L2 lines without writing them
+    // back (the next block on this scratch writes before it reads)
+    discard_scratch(parkX);
 }
 
 struct CtaSmem {
