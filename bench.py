@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--mixed", type=int, default=0,
                     help="mixed-batch workload instead: this many captures, lengths uniform in 0.5-8 s, "
                          "half NTSC / half PAL, own seed and SNR (30-45 dB) each")
+    ap.add_argument("--locate-threads", type=int, default=4,
+                    help="mixed batch: host threads locating the captures' lines")
     ap.add_argument("--mixed-budget-gb", type=float, default=100.0,
                     help="device memory per wave of the mixed batch (inputs + demodulator outputs)")
     return ap.parse_args()
@@ -610,6 +612,7 @@ def run_mixed(args):
     rfs = {s: RFDecode(system=s, decode_analog_audio=44100, decode_digital_audio=True, device=local)
            for s in ("NTSC", "PAL")}
     queue = DemodQueue(local)
+    loc_rfs = []  # per locate thread {system: RFDecode}, kept across waves
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     tune = None
     wave_ms, demod_ms, samples, fields, launches = [], [], 0, 0, 0
@@ -621,7 +624,8 @@ def run_mixed(args):
                                            start=plan[i][2] % 1000003, device="cuda")) for i in g]
         torch.cuda.synchronize()
         gen_s += time.perf_counter() - t0
-        mb = MixedBatch(caps, device=local, rfs=rfs, queue=queue)
+        mb = MixedBatch(caps, device=local, rfs=rfs, queue=queue, locate_threads=args.locate_threads,
+                        locate_rfs=loc_rfs)
         st = mb.stream
         if tune is None:
             tune = autotune(queue, st, grabs=(1, 2, 4, 8), ctas=(0, 2 * sms), reps=2)
@@ -687,7 +691,8 @@ def run_mixed(args):
                         "own seed each",
             "waves": len(groups),
             "per_wave": "one ldg_queue launch over every block of the wave's captures (CUDA graph), "
-                        "line locations per capture, one TBC launch over all their fields",
+                        f"line locations per capture on {args.locate_threads} host threads, one TBC launch "
+                        "over all their fields",
             "l2": "inputs and outputs exceed L2 each pass; no flush",
             "parallelism": f"replicas x{world}",
             "mtf_level": 1,

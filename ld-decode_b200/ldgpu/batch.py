@@ -151,7 +151,7 @@ class MixedBatch:
     stream is given; wait for it (or torch.cuda.synchronize()) before
     reading the outputs."""
 
-    def __init__(self, captures, device=0, mtf_level=1, rfs=None, queue=None):
+    def __init__(self, captures, device=0, mtf_level=1, rfs=None, queue=None, locate_threads=1, locate_rfs=None):
         import torch
         from .fieldread import blocks_in_capture
         from .rfdecode import RFDecode
@@ -183,6 +183,20 @@ class MixedBatch:
             self.outs.append(o)
             self.nblocks.append(nb)
             self.items.append((rf, cap.data_ptr(), nb, U, {k: v.data_ptr() for k, v in o.items()}, mtf_level))
+        # line locations of the captures on `locate_threads` host threads, each
+        # with its own contexts (a context's sync-run scratch serves one call
+        # at a time) and its own stream; locate_rfs: one {system: RFDecode}
+        # per thread, reused across batches
+        self.locate_threads = max(1, int(locate_threads))
+        self.locate_rfs = locate_rfs if locate_rfs is not None else []
+        if self.locate_threads > 1:
+            while len(self.locate_rfs) < self.locate_threads:
+                self.locate_rfs.append({})
+            for d in self.locate_rfs[:self.locate_threads]:
+                for system, _ in captures:
+                    if system not in d:
+                        d[system] = RFDecode(system=system, decode_analog_audio=44100, decode_digital_audio=True,
+                                             device=device)
         self.queue = queue if queue is not None else DemodQueue(device)
         self.queue.submit(self.items)
         self.fields = None
@@ -203,17 +217,45 @@ class MixedBatch:
     def locate(self, stream=None):
         """Line locations of every capture's fields (LocatedFields per
         capture, in capture order)."""
+        import os
         from .lines import LineLocator
+        torch = self.torch
         stream = stream or self.stream
+        T = self.locate_threads
+        n = len(self.captures)
         if getattr(self, "locators", None) is None:
-            # one per capture, kept across passes (pinned staging buffers);
-            # a pass releases the previous pass's line-location buffers in
-            # stream order
-            self.locators = [LineLocator(self.rfs[system]) for system, _ in self.captures]
-        self.fields = []
-        for loc, o, nb in zip(self.locators, self.outs, self.nblocks):
-            arrays = {k: o[k] for k in FIELD_KEYS if k in o}
-            self.fields.append(loc.locate(arrays, nb, stream))
+            # one per capture, kept across passes (pinned staging buffers); a
+            # pass releases the previous pass's line-location buffers in
+            # stream order.  Capture i is located by thread i % T.
+            cores = max(1, (os.cpu_count() or 1) // T)
+            self.locators = []
+            for i, (system, _) in enumerate(self.captures):
+                rf = self.rfs[system] if T == 1 else self.locate_rfs[i % T][system]
+                loc = LineLocator(rf)
+                loc.threads = max(1, min(loc.threads, cores))
+                self.locators.append(loc)
+            self._loc_streams = [stream] if T == 1 else [torch.cuda.Stream(device=self.device) for _ in range(T)]
+        self.fields = [None] * n
+
+        def work(ti):
+            st = self._loc_streams[ti]
+            with torch.cuda.stream(st):
+                for i in range(ti, n, T):
+                    arrays = {k: self.outs[i][k] for k in FIELD_KEYS if k in self.outs[i]}
+                    self.fields[i] = self.locators[i].locate(arrays, self.nblocks[i], st)
+
+        if T == 1:
+            work(0)
+            return self.fields
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        for st in self._loc_streams:
+            st.wait_event(ev)
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(T) as ex:
+            list(ex.map(work, range(T)))
+        for st in self._loc_streams:
+            stream.wait_stream(st)
         return self.fields
 
     def field_geometry(self, system):

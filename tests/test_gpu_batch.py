@@ -28,7 +28,7 @@ def batch(cuda_ok):
     for system, secs, seed, snr in CAPTURES:
         n = max(int(secs * 40e6), 32768 + 2000) if secs < 0.001 else int(secs * 40e6)
         caps.append((system, synth_capture(system, n, seed=seed, snr_db=snr, start=seed * 1000, device="cuda")))
-    mb = MixedBatch(caps)
+    mb = MixedBatch(caps, locate_threads=3)
     yield mb
     mb.close()
 
