@@ -772,7 +772,7 @@ int ldg_demod_status(ldg_ctx* c, int32_t* flags) {
 
 namespace ldg {
 
-int noalloc_fail(int code, const std::string& msg) { return fail(code, msg); }
+int api_fail(int code, const std::string& msg) { return fail(code, msg); }
 
 int lines_fail(int code, const std::string& msg) { return fail(code, msg); }
 

@@ -74,20 +74,20 @@ __global__ void __launch_bounds__(kThreads) lds_unpack_kernel(const uint8_t* __r
 
 extern "C" int ldg_unpack_lds(const uint8_t* packed, int64_t nbytes, int64_t first, int64_t n, int16_t* out,
                               void* stream) {
-    using ldg::noalloc_fail;
-    if (!packed || !out) return noalloc_fail(LDG_ERR_ARG, "ldg_unpack_lds: NULL buffer");
-    if (first < 0 || n < 0 || nbytes < 0) return noalloc_fail(LDG_ERR_ARG, "ldg_unpack_lds: negative size");
+    using ldg::api_fail;
+    if (!packed || !out) return api_fail(LDG_ERR_ARG, "ldg_unpack_lds: NULL buffer");
+    if (first < 0 || n < 0 || nbytes < 0) return api_fail(LDG_ERR_ARG, "ldg_unpack_lds: negative size");
     if (n == 0) return LDG_OK;
     const long long last_group = (first + n - 1) / 4;
     if ((last_group + 1) * 5 > nbytes)
-        return noalloc_fail(LDG_ERR_RANGE, "ldg_unpack_lds: the packed buffer ends before the last sample");
+        return api_fail(LDG_ERR_RANGE, "ldg_unpack_lds: the packed buffer ends before the last sample");
     if ((reinterpret_cast<uintptr_t>(packed) & 3) != 0 || (reinterpret_cast<uintptr_t>(out) & 7) != 0)
-        return noalloc_fail(LDG_ERR_ARG, "ldg_unpack_lds: packed must be 4-byte and out 8-byte aligned");
+        return api_fail(LDG_ERR_ARG, "ldg_unpack_lds: packed must be 4-byte and out 8-byte aligned");
     const long long groups = last_group - first / 4 + 1;
     const long long grid = (groups + kGroups - 1) / kGroups;
-    if (grid > 0x7fffffffLL) return noalloc_fail(LDG_ERR_ARG, "ldg_unpack_lds: too many samples");
+    if (grid > 0x7fffffffLL) return api_fail(LDG_ERR_ARG, "ldg_unpack_lds: too many samples");
     lds_unpack_kernel<<<(unsigned)grid, kThreads, 0, (cudaStream_t)stream>>>(packed, nbytes, first, n, out);
     const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return noalloc_fail(LDG_ERR_CUDA, std::string("ldg_unpack_lds: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return api_fail(LDG_ERR_CUDA, std::string("ldg_unpack_lds: ") + cudaGetErrorString(e));
     return LDG_OK;
 }

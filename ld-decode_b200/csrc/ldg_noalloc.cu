@@ -67,7 +67,7 @@ extern "C" int ldg_demod_blocks_noalloc(ldg_ctx* ctx, const ldg_demod_args* a, i
     int prev = -1;
     if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
     if (prev != device && cudaSetDevice(device) != cudaSuccess)
-        return ldg::noalloc_fail(LDG_ERR_CUDA, "ldg_demod_blocks_noalloc: cannot make the context's device current");
+        return ldg::api_fail(LDG_ERR_CUDA, "ldg_demod_blocks_noalloc: cannot make the context's device current");
     struct Restore {
         int prev, dev;
         ~Restore() {
@@ -77,10 +77,10 @@ extern "C" int ldg_demod_blocks_noalloc(ldg_ctx* ctx, const ldg_demod_args* a, i
     float2* scratch = nullptr;
     rc = scratch_address(device, &scratch);
     if (rc != LDG_OK)
-        return ldg::noalloc_fail(rc, "ldg_demod_blocks_noalloc: cudaGetSymbolAddress of the static scratch failed");
+        return ldg::api_fail(rc, "ldg_demod_blocks_noalloc: cudaGetSymbolAddress of the static scratch failed");
     p.scratch = scratch;
     const cudaError_t e = ldg::launch_demod(p, grid, static_cast<cudaStream_t>(ldg::noalloc_stream(ctx, a)));
     if (e != cudaSuccess)
-        return ldg::noalloc_fail(LDG_ERR_CUDA, std::string("demod launch: ") + cudaGetErrorString(e));
+        return ldg::api_fail(LDG_ERR_CUDA, std::string("demod launch: ") + cudaGetErrorString(e));
     return LDG_OK;
 }

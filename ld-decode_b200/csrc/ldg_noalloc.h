@@ -1,5 +1,6 @@
-// Internal helpers shared by the allocation-free demod entry point
-// (ldg_noalloc.cu) and the context implementation (ldg_abi.cu).
+// Internal helpers shared by the context implementation (ldg_abi.cu), the
+// allocation-free demod entry point (ldg_noalloc.cu), the mixed-batch queue
+// (ldg_queue.cu) and the ingest kernels (ldg_ingest.cu).
 #pragma once
 #include <string>
 
@@ -13,7 +14,8 @@ namespace ldg {
 // ctas == 0; ctas > max_slots is rejected.  Allocates nothing.
 int noalloc_prepare(ldg_ctx* ctx, const ldg_demod_args* a, int ctas, int max_slots, DemodParams* p, int* grid,
                     int* device);
-int noalloc_fail(int code, const std::string& msg);
+// Record msg as this thread's ldg_last_error() and return code.
+int api_fail(int code, const std::string& msg);
 
 // Validate a batch whose buffers are all device memory and fill `p` from it
 // and ctx's filters (scheduling fields zero); `who` names the caller in

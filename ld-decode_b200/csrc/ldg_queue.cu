@@ -40,7 +40,7 @@ struct ldg_queue {
 
 namespace {
 
-int qfail(int code, const std::string& msg) { return ldg::noalloc_fail(code, msg); }  // ldg_last_error()
+int qfail(int code, const std::string& msg) { return ldg::api_fail(code, msg); }  // ldg_last_error()
 
 #define QCK(call)                                                                                  \
     do {                                                                                           \
