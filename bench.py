@@ -173,6 +173,7 @@ def run_gpu(args):
     outs["audio_left"] = torch.empty(nblocks * 991, dtype=torch.float32, device="cuda")
     outs["audio_right"] = torch.empty(nblocks * 991, dtype=torch.float32, device="cuda")
     ptrs = {k: v.data_ptr() for k, v in outs.items()}
+    import types
 
     def demod():
         rf.demod_blocks_device(cap.data_ptr(), nblocks, U, ptrs, mtf_level=1, stream=sh)
@@ -183,6 +184,15 @@ def run_gpu(args):
     fkeys = ["demod", "demod_05", "demod_burst"] + (["demod_pilot"] if system == "PAL" else [])
     farr = {k: outs[k] for k in fkeys}
     loc = LineLocator(rf)
+    # one set of device buffers per step in flight: the end-to-end steps
+    # alternate two sets, so a step's device->host copies overlap the next
+    # step's input copy and demod (a set is reused once its copies are done)
+    main = types.SimpleNamespace(cap=cap, outs=outs, ptrs=ptrs, farr=farr, loc=loc, pics=None, done=None)
+
+    def make_set():
+        o = {k: torch.empty_like(v) for k, v in outs.items()}
+        return types.SimpleNamespace(cap=torch.empty_like(cap), outs=o, ptrs={k: v.data_ptr() for k, v in o.items()},
+                                     farr={k: o[k] for k in fkeys}, loc=LineLocator(rf), pics=None, done=None)
     levels = field_levels(rf)
     nchunks = max(1, min(args.chunks, nblocks // 64))
     # chunk c holds a share proportional to taper**c of the blocks: a smaller
@@ -196,25 +206,31 @@ def run_gpu(args):
     elem = {k: v.element_size() for k, v in outs.items()}
     per_block = {k: (991 if k.startswith("audio") else U) for k in outs}
 
-    def demod_range(b0, b1):
-        o = {k: v + elem[k] * per_block[k] * b0 for k, v in ptrs.items()}
-        rf.demod_blocks_device(cap.data_ptr() + 2 * b0 * U, b1 - b0, U, o, mtf_level=1, stream=sh)
+    def demod_range(b0, b1, bs):
+        o = {k: v + elem[k] * per_block[k] * b0 for k, v in bs.ptrs.items()}
+        rf.demod_blocks_device(bs.cap.data_ptr() + 2 * b0 * U, b1 - b0, U, o, mtf_level=1, stream=sh)
 
     outlinelen = rf.SysParams["outlinelen"]
     outlines = rf.SysParams["frame_lines"] // 2 + 1
     fsz = outlinelen * outlines
-    pics = None
     marks = {}
 
     streamH = torch.cuda.Stream()              # host -> device input copies (end to end)
     streamD = torch.cuda.Stream()              # device -> host output copies (end to end)
 
-    def step(io=None):
-        """One pass over the capture.  io: pinned host buffers; then each
-        chunk's input is copied in just before its demod (streamH) and each
-        chunk's EFM/audio and each field range's pictures are copied out as
-        soon as they are final (streamD)."""
-        loc.begin(farr)
+    def step(io=None, bs=None):
+        """One pass over the capture with buffer set `bs` (default: the
+        main set).  io: pinned host buffers; then each chunk's input is
+        copied in just before its demod (streamH) and each chunk's EFM/audio
+        and each field range's pictures are copied out as soon as they are
+        final (streamD)."""
+        bs = bs or main
+        loc = bs.loc
+        if io is not None and bs.done is not None:
+            # the set's previous outputs must be on the host before it is refilled
+            stream.wait_event(bs.done)
+            streamH.wait_event(bs.done)
+        loc.begin(bs.farr)
         evs = []
         for c in range(nchunks):
             if io is not None:
@@ -222,11 +238,11 @@ def run_gpu(args):
                 a0 = bounds[c] * U + (N - U if c else 0)
                 a1 = min(bounds[c + 1] * U + (N - U), nsamples)
                 with torch.cuda.stream(streamH):
-                    cap[a0:a1].copy_(io["cap"][a0:a1], non_blocking=True)
+                    bs.cap[a0:a1].copy_(io["cap"][a0:a1], non_blocking=True)
                     hev = torch.cuda.Event()
                     hev.record(streamH)
                 stream.wait_event(hev)
-            demod_range(bounds[c], bounds[c + 1])
+            demod_range(bounds[c], bounds[c + 1], bs)
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(stream)
             evs.append(ev)
@@ -235,32 +251,33 @@ def run_gpu(args):
                 o0, o1 = bounds[c] * U, bounds[c + 1] * U
                 q0, q1 = bounds[c] * 991, bounds[c + 1] * 991
                 with torch.cuda.stream(streamD):
-                    io["efm"][o0:o1].copy_(outs["efm"][o0:o1], non_blocking=True)
-                    io["audio_left"][q0:q1].copy_(outs["audio_left"][q0:q1], non_blocking=True)
-                    io["audio_right"][q0:q1].copy_(outs["audio_right"][q0:q1], non_blocking=True)
+                    io["efm"][o0:o1].copy_(bs.outs["efm"][o0:o1], non_blocking=True)
+                    io["audio_left"][q0:q1].copy_(bs.outs["audio_left"][q0:q1], non_blocking=True)
+                    io["audio_right"][q0:q1].copy_(bs.outs["audio_right"][q0:q1], non_blocking=True)
         for c in range(nchunks):
             streamB.wait_event(evs[c])
             streamS.wait_event(evs[c])
             loc.advance(bounds[c + 1], stream=streamB, scan_stream=streamS)
             # TBC of each range of fields as its line locations become final
             # (stream C: overlaps the NTSC burst chain's next range and the demod)
-            while loc.ready and pics is not None:
+            while loc.ready and bs.pics is not None:
                 lo, hi, ev = loc.ready.pop(0)
                 streamC.wait_event(ev)
-                tbc_fields(rf, tbc_batch(rf, loc.fields, outs["demod"].data_ptr(), pics.data_ptr(), levels,
+                tbc_fields(rf, tbc_batch(rf, loc.fields, bs.outs["demod"].data_ptr(), bs.pics.data_ptr(), levels,
                                          first=lo, count=hi - lo), stream=streamC.cuda_stream, asynchronous=True)
                 if io is not None:
                     tev = torch.cuda.Event()
                     tev.record(streamC)
                     streamD.wait_event(tev)
                     with torch.cuda.stream(streamD):
-                        io["pics"][lo * fsz:hi * fsz].copy_(pics[lo * fsz:hi * fsz], non_blocking=True)
+                        io["pics"][lo * fsz:hi * fsz].copy_(bs.pics[lo * fsz:hi * fsz], non_blocking=True)
         marks["demod_end"] = evs[-1]
         stream.wait_stream(streamB)
         stream.wait_stream(streamC)
         stream.wait_stream(streamS)
         if io is not None:
-            stream.wait_stream(streamD)
+            bs.done = torch.cuda.Event()
+            bs.done.record(streamD)
         end = torch.cuda.Event(enable_timing=True)
         end.record(stream)
         marks["end"] = end
@@ -269,7 +286,8 @@ def run_gpu(args):
     flist = step()
     torch.cuda.synchronize()
     nf = len(flist)
-    pics = torch.empty(nf * fsz, dtype=torch.uint16, device="cuda")
+    main.pics = torch.empty(nf * fsz, dtype=torch.uint16, device="cuda")
+    pics = main.pics
 
     def barrier():
         replica_barrier(world)
@@ -318,18 +336,26 @@ def run_gpu(args):
     # ---- end to end: pinned host capture in, fields/efm/audio out
     e2e = None
     if not args.no_e2e:
-        io = {"cap": cap.cpu().pin_memory(),
-              "pics": torch.empty(nf * fsz, dtype=torch.uint16).pin_memory(),
-              "efm": torch.empty(nout, dtype=torch.int16).pin_memory(),
-              "audio_left": torch.empty(nblocks * 991, dtype=torch.float32).pin_memory(),
-              "audio_right": torch.empty(nblocks * 991, dtype=torch.float32).pin_memory()}
-        step(io)  # warm the copy path
+        host_cap = cap.cpu().pin_memory()
+
+        def make_io():
+            return {"cap": host_cap,
+                    "pics": torch.empty(nf * fsz, dtype=torch.uint16).pin_memory(),
+                    "efm": torch.empty(nout, dtype=torch.int16).pin_memory(),
+                    "audio_left": torch.empty(nblocks * 991, dtype=torch.float32).pin_memory(),
+                    "audio_right": torch.empty(nblocks * 991, dtype=torch.float32).pin_memory()}
+        alt = make_set()
+        alt.pics = torch.empty(nf * fsz, dtype=torch.uint16, device="cuda")
+        sets, ios = [main, alt], [make_io(), make_io()]
+        for k in range(2):  # warm the copy path on both sets
+            assert len(step(ios[k], sets[k])) == nf
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         e0.record(stream)
-        for _ in range(args.steps):
-            step(io)
+        for k in range(args.steps):
+            step(ios[k % 2], sets[k % 2])
+        stream.wait_stream(streamD)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -340,7 +366,12 @@ def run_gpu(args):
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                "path": "pinned host capture -> ldg_demod_blocks -> ldg_sync_runs + ldg_field_chain + "
                        "ldg_lines_refine -> ldg_tbc_fields -> host fields, EFM, audio; per chunk, the input "
-                       "copy and the output copies overlap the other chunks' work"}
+                       "copy and the output copies overlap the other chunks' work; two buffer sets, so a "
+                       "step's output copies also overlap the next step"}
+        # the end-to-end outputs of the last step equal the device-resident run's
+        last = ios[(args.steps - 1) % 2]
+        e2e["outputs_match"] = bool(torch.equal(last["pics"].view(torch.int16), pics.cpu().view(torch.int16)) and
+                                    torch.equal(last["efm"], outs["efm"].cpu()))
 
     # ---- plain form: one demodblock() call per block through the Python API
     plain = None

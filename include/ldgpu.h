@@ -236,6 +236,16 @@ int ldg_queue_info(ldg_queue* q, int64_t* total_blocks, int32_t* grid);
  * head and scratch): order them on one stream. */
 int ldg_queue_run(ldg_queue* q, void* stream, int32_t use_graph);
 
+/* ---- Copies by the SMs (no counterpart in the reference) ---- */
+
+/* dst[0, nbytes) = src[0, nbytes) by a kernel on `stream` (the current
+ * device), each buffer device memory or pinned host memory (read or written
+ * through its mapping over PCIe).  For small transfers that the host waits
+ * on while bulk copies occupy the copy engines: a cudaMemcpyAsync would
+ * queue behind them, the kernel does not.  Pageable host memory is rejected
+ * (LDG_ERR_ARG). */
+int ldg_copy_async(void* dst, const void* src, int64_t nbytes, void* stream);
+
 /* ---- Ingest ---- */
 
 /* .lds captures (DomesdayDuplicator: four 10-bit samples in 5 bytes, most

@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "ldg_copy.cuh"
 #include "ldg_demod.cuh"
 #include "ldg_dropouts.cuh"
 #include "ldg_fft.cuh"
@@ -110,6 +111,7 @@ struct ldg_ctx {
     size_t drop_errs_cap = 0;
     cudaEvent_t drop_done = nullptr;
     bool drop_used = false;
+    long long* h_word = nullptr;         // pinned, mapped: results the host reads right after a kernel
     ldg::RfTbcField* d_rftbc = nullptr;  // ldg_rf_tbc descriptors, same reuse rule
     size_t rftbc_cap = 0;
     cudaEvent_t rftbc_done = nullptr;
@@ -222,6 +224,7 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     cudaFree(c->d_slots);
     if (c->drop_used) cudaEventSynchronize(c->drop_done);
     if (c->rftbc_used) cudaEventSynchronize(c->rftbc_done);
+    if (c->h_word) cudaFreeHost(c->h_word);
     cudaFree(c->d_rftbc);
     if (c->rftbc_done) cudaEventDestroy(c->rftbc_done);
     cudaFree(c->d_drop_fields);
@@ -625,7 +628,14 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
         d.out_u16 = f.out_u16;
         sego += f.nlines - 1;
     }
-    LDG_CK(cudaMemcpyAsync(w.d_fields, w.h_fields, nfields * sizeof(ldg::TbcField), cudaMemcpyHostToDevice, st));
+    // descriptors read by SMs from the pinned workspace: a copy-engine transfer
+    // would queue behind bulk output copies on the same engines
+    void* hf = ldg::device_view(w.h_fields);
+    if (hf) {
+        LDG_CK(ldg::sm_copy(w.d_fields, hf, nfields * sizeof(ldg::TbcField), st));
+    } else {
+        LDG_CK(cudaMemcpyAsync(w.d_fields, w.h_fields, nfields * sizeof(ldg::TbcField), cudaMemcpyHostToDevice, st));
+    }
     cudaError_t e = ldg::launch_tbc(w.d_fields, nfields, max_nout, c->d_lut, 15.0, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
     LDG_CK(cudaEventRecord(w.done, st));
@@ -781,6 +791,19 @@ int ctx_device(const ldg_ctx* c) { return c->device; }
 std::mutex& ctx_mutex(ldg_ctx* c) { return c->mu; }
 
 cudaStream_t ctx_stream(const ldg_ctx* c) { return c->stream; }
+
+int ctx_host_word(ldg_ctx* c, long long** host, long long** dev) {
+    if (!c->h_word) {
+        void* p = nullptr;
+        LDG_CK(cudaHostAlloc(&p, 256, cudaHostAllocMapped));
+        c->h_word = static_cast<long long*>(p);
+    }
+    void* d = nullptr;
+    LDG_CK(cudaHostGetDevicePointer(&d, c->h_word, 0));
+    *host = c->h_word;
+    *dev = static_cast<long long*>(d);
+    return LDG_OK;
+}
 
 int ctx_lines_scratch(ldg_ctx* c, size_t need, void** out) {
     int rc = grow(&c->d_lines, &c->lines_cap, need);

@@ -31,6 +31,7 @@
 #include <mutex>
 #include <string>
 
+#include "ldg_copy.cuh"
 #include "ldgpu.h"
 
 struct ldg_ctx;
@@ -40,6 +41,7 @@ int lines_fail(int code, const std::string& msg);
 int ctx_device(const ldg_ctx* c);
 std::mutex& ctx_mutex(ldg_ctx* c);
 int ctx_lines_scratch(ldg_ctx* c, size_t need, void** out);
+int ctx_host_word(ldg_ctx* c, long long** host, long long** dev);
 }  // namespace ldg
 
 namespace {
@@ -211,6 +213,22 @@ __global__ void run_pair_kernel(const long long* __restrict__ edges, const long 
             rm[r] = mean;
         }
     }
+}
+
+// Runs and the edge count straight into host-mapped pinned memory (coalesced
+// over PCIe), so the host reads them after a stream synchronisation without
+// a copy-engine transfer.
+__global__ void export_runs_kernel(const long long* __restrict__ total, long long cap, const long long* __restrict__ rs,
+                                   const long long* __restrict__ rl, const double* __restrict__ rm,
+                                   long long* ors, long long* orl, double* orm, long long* count) {
+    const long long nruns = min(*total / 2, cap);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nruns; i += stride) {
+        ors[i] = rs[i];
+        orl[i] = rl[i];
+        orm[i] = rm[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *count = *total;
 }
 
 // --------------------------------------------------------- per-line helpers
@@ -915,6 +933,27 @@ int ldg_sync_runs(ldg_ctx* c, const float* d05, int64_t n, double threshold, int
     edge_scan_kernel<<<1, 1024, 0, st>>>(counts, ntiles, offsets, total);
     edge_write_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, offsets, edges, ecap);
     run_pair_kernel<<<4 * 148, 256, 0, st>>>(edges, total, cap, d05, min_long, trim_lo, trim_hi, rs, rl, rm);
+    // pinned (mapped) outputs: the runs and the count are written by a kernel
+    // and the host waits for the stream only (no copy-engine transfer, which
+    // would queue behind bulk copies of an end-to-end pipeline)
+    long long *hw = nullptr, *dw = nullptr;
+    void* drs = ldg::device_view(run_start);
+    void* drl = ldg::device_view(run_len);
+    void* drm = ldg::device_view(run_mean);
+    if (drs && drl && drm && ldg::ctx_host_word(c, &hw, &dw) == LDG_OK) {
+        *hw = -1;
+        export_runs_kernel<<<2 * 148, 256, 0, st>>>(total, cap, rs, rl, rm, static_cast<long long*>(drs),
+                                                    static_cast<long long*>(drl), static_cast<double*>(drm), dw);
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+            return cuda_fail("run export");
+        const long long nedges = *reinterpret_cast<volatile long long*>(hw);
+        const long long nr = nedges / 2;
+        *nruns = nr;
+        if (nedges < 0) return done(ldg::lines_fail(LDG_ERR_CUDA, "ldg_sync_runs: run count not written"));
+        if (nr > cap || nedges > ecap)
+            return done(ldg::lines_fail(LDG_ERR_RANGE, "ldg_sync_runs: more runs than cap"));
+        return done(LDG_OK);
+    }
     long long nedges = 0;
     if (cudaMemcpyAsync(&nedges, total, sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)

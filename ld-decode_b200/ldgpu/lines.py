@@ -485,7 +485,9 @@ class LineLocator:
         hb[nb_i:nb_i + nf * ml * 8].view(np.float64).reshape(nf, ml)[:] = plans.linelocs1
         hb[nb_i + nf * ml * 8:].reshape(nf, ml)[:] = plans.linebad
         dbuf = torch.empty(total, dtype=torch.uint8, device=dev)
-        dbuf.copy_(hbuf, non_blocking=True)
+        # copied by SMs from the pinned block: a copy-engine transfer would
+        # wait behind any bulk copies queued on the engines
+        L.check(lib.ldg_copy_async(dbuf.data_ptr(), hbuf.data_ptr(), total, _lib_stream(stream)))
         self._pin_ring[self._pin_next - 1][1].record()
         base = dbuf.data_ptr()
         out_ll = torch.empty((nf, ml), dtype=torch.float64, device=dev)
