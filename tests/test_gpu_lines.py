@@ -70,6 +70,53 @@ def test_sync_runs_match_host(capture):
     np.testing.assert_allclose(m[ok], hm[ok], rtol=1e-12)
 
 
+def test_sync_runs_pageable_outputs(capture):
+    """Pageable host outputs take the copy-engine path; pinned ones are
+    written by the export kernel.  Both give the same runs."""
+    import ctypes
+    import math
+    from ldgpu import lib as L
+    from ldgpu.lines import sync_threshold
+    rf, arrays, host, nb, ref = capture
+    n = arrays["demod_05"].numel()
+    cap = max(1024, n // 256)
+    outs = [np.empty(cap, np.int64), np.empty(cap, np.int64), np.empty(cap, np.float64)]
+    nr = ctypes.c_int64(0)
+    L.check(L.load().ldg_sync_runs(rf._ctx.handle, ctypes.c_void_p(arrays["demod_05"].data_ptr()), n,
+                                   sync_threshold(rf), math.floor(10 * rf.samplesperline * rf.linelen),
+                                   math.floor(rf.freq), math.ceil(rf.freq), outs[0].ctypes.data, outs[1].ctypes.data,
+                                   outs[2].ctypes.data, cap, ctypes.byref(nr), None))
+    k = nr.value
+    s, ln, m = LineLocator(rf).sync_runs(arrays["demod_05"].data_ptr(), n)
+    np.testing.assert_array_equal(outs[0][:k], s)
+    np.testing.assert_array_equal(outs[1][:k], ln)
+    np.testing.assert_array_equal(outs[2][:k].view(np.int64), m.view(np.int64))
+
+
+def test_sm_copy(cuda_ok):
+    """ldg_copy_async: pinned host <-> device copies by a kernel, aligned and
+    unaligned, and pageable host memory rejected."""
+    import torch
+    from ldgpu import lib as L
+    lib = L.load()
+    rng = np.random.default_rng(4)
+    src = torch.from_numpy(rng.integers(0, 256, 1 << 20, dtype=np.uint8)).pin_memory()
+    dev = torch.zeros(1 << 20, dtype=torch.uint8, device="cuda")
+    back = torch.zeros(1 << 20, dtype=torch.uint8).pin_memory()
+    for off, n in [(0, 1 << 20), (3, 1000), (16, 65536 + 5), (1, 1)]:
+        dev.zero_()
+        back.zero_()
+        torch.cuda.synchronize()
+        L.check(lib.ldg_copy_async(dev.data_ptr() + off, src.data_ptr() + off, n, None))
+        L.check(lib.ldg_copy_async(back.data_ptr() + off, dev.data_ptr() + off, n, None))
+        torch.cuda.synchronize()
+        assert torch.equal(back[off:off + n], src[off:off + n])
+        assert int(back[:off].sum()) == 0 and int(back[off + n:].sum()) == 0
+    pageable = np.zeros(64, np.uint8)
+    with pytest.raises(L.LdgError, match="pinned"):
+        L.check(lib.ldg_copy_async(dev.data_ptr(), pageable.ctypes.data, 64, None))
+
+
 def test_batched_linelocs_match_host(capture):
     rf, arrays, host, nb, ref = capture
     loc = LineLocator(rf)
