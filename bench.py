@@ -70,6 +70,11 @@ def parse():
                          "half NTSC / half PAL, own seed and SNR (30-45 dB) each")
     ap.add_argument("--locate-threads", type=int, default=4,
                     help="mixed batch: host threads locating the captures' lines")
+    ap.add_argument("--mixed-pipeline", type=int, default=4,
+                    help="mixed batch: groups of captures per wave whose line locations and TBC overlap the next "
+                         "group's demodulation")
+    ap.add_argument("--reserve-sms", type=int, default=40,
+                    help="mixed batch, pipelined: SMs the group queues leave to the line-location and TBC kernels")
     ap.add_argument("--mixed-budget-gb", type=float, default=100.0,
                     help="device memory per wave of the mixed batch (inputs + demodulator outputs)")
     return ap.parse_args()
@@ -656,7 +661,7 @@ def run_mixed(args):
         torch.cuda.synchronize()
         gen_s += time.perf_counter() - t0
         mb = MixedBatch(caps, device=local, rfs=rfs, queue=queue, locate_threads=args.locate_threads,
-                        locate_rfs=loc_rfs)
+                        locate_rfs=loc_rfs, pipeline=args.mixed_pipeline, reserve_sms=args.reserve_sms)
         st = mb.stream
         if tune is None:
             tune = autotune(queue, st, grabs=(1, 2, 4, 8), ctas=(0, 2 * sms), reps=2)
@@ -721,9 +726,9 @@ def run_mixed(args):
                         f"uniform in 0.5-8 s ({sum(p[1] for p in plan) / 40e6:.1f} s in all), SNR 30-45 dB, "
                         "own seed each",
             "waves": len(groups),
-            "per_wave": "one ldg_queue launch over every block of the wave's captures (CUDA graph), "
-                        f"line locations per capture on {args.locate_threads} host threads, one TBC launch "
-                        "over all their fields",
+            "per_wave": f"{args.mixed_pipeline} groups of captures, one ldg_queue launch (CUDA graph) per group "
+                        f"on {148 - args.reserve_sms} of the SMs; each group's line locations (on "
+                        f"{args.locate_threads} host threads) and one TBC launch overlap the next group's demod",
             "l2": "inputs and outputs exceed L2 each pass; no flush",
             "parallelism": f"replicas x{world}",
             "mtf_level": 1,

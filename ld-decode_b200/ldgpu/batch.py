@@ -19,6 +19,8 @@ one after another (LDdecode.readfield, core.py:4060-4200).  Here:
 
 import ctypes
 
+import numpy as np
+
 from . import lib as L
 
 U_KEYS = ("demod", "demod_raw", "demod_05", "demod_burst", "demod_pilot", "rfhpf", "efm")
@@ -146,12 +148,15 @@ class MixedBatch:
 
     captures: list of (system, int16 device tensor).  One RFDecode per
     system (analog audio and EFM outputs on), one DemodQueue over all
-    captures' blocks, one LineLocator per capture, one TBC launch.  Work is
+    captures' blocks, one LineLocator per capture, one TBC launch; with
+    pipeline = K > 1, K queues over consecutive groups of captures whose
+    line locations and TBC overlap the next group's demodulation.  Work is
     enqueued on `self.stream` (a torch.cuda.Stream of its own) unless a
     stream is given; wait for it (or torch.cuda.synchronize()) before
     reading the outputs."""
 
-    def __init__(self, captures, device=0, mtf_level=1, rfs=None, queue=None, locate_threads=1, locate_rfs=None):
+    def __init__(self, captures, device=0, mtf_level=1, rfs=None, queue=None, locate_threads=1, locate_rfs=None,
+                 pipeline=1, reserve_sms=24):
         import torch
         from .fieldread import blocks_in_capture
         from .rfdecode import RFDecode
@@ -202,6 +207,31 @@ class MixedBatch:
         self.fields = None
         self.pictures = None
         self.picture_offsets = None
+        self._pics = {}       # slot -> (uint16 device tensor, {capture: offset})
+        self._pic_index = {}  # capture -> (tensor, offset)
+        # pipelined form: the captures in `pipeline` consecutive groups of
+        # about equal blocks, one queue each, launched back to back with
+        # `reserve_sms` SMs left free, so that a group's line locations and
+        # TBC run beside the next group's demodulation
+        self.pipeline = max(1, min(int(pipeline), len(captures)))
+        self.reserve_sms = int(reserve_sms)
+        self._groups = [list(range(len(captures)))]
+        self._group_queues = []
+        if self.pipeline > 1:
+            cum = np.cumsum(self.nblocks)
+            total = cum[-1]
+            cuts = [0]
+            for g in range(1, self.pipeline):
+                cuts.append(int(np.searchsorted(cum, g * total / self.pipeline)) + 1)
+            cuts.append(len(captures))
+            cuts = sorted(set(min(max(c, 0), len(captures)) for c in cuts))
+            self._groups = [list(range(a, b)) for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
+            sms = torch.cuda.get_device_properties(device).multi_processor_count
+            for idx in self._groups:
+                q = DemodQueue(device)
+                q.submit([self.items[i] for i in idx])
+                q.set_schedule(self.queue.schedule[0] or 1, max(1, sms - self.reserve_sms))
+                self._group_queues.append(q)
 
     @property
     def samples(self):
@@ -217,16 +247,27 @@ class MixedBatch:
     def locate(self, stream=None):
         """Line locations of every capture's fields (LocatedFields per
         capture, in capture order)."""
+        stream = stream or self.stream
+        ev = self.torch.cuda.Event()
+        ev.record(stream)
+        self.fields = [None] * len(self.captures)
+        self._locate(list(range(len(self.captures))), ev)
+        for st in self._loc_streams:
+            stream.wait_stream(st)
+        return self.fields
+
+    def _locate(self, indices, ready):
+        """Locate captures `indices` once event `ready` has completed, on the
+        locate threads (capture i by thread i % T) and their streams."""
         import os
         from .lines import LineLocator
         torch = self.torch
-        stream = stream or self.stream
         T = self.locate_threads
         n = len(self.captures)
         if getattr(self, "locators", None) is None:
             # one per capture, kept across passes (pinned staging buffers); a
             # pass releases the previous pass's line-location buffers in
-            # stream order.  Capture i is located by thread i % T.
+            # stream order
             cores = max(1, (os.cpu_count() or 1) // T)
             self.locators = []
             for i, (system, _) in enumerate(self.captures):
@@ -234,29 +275,27 @@ class MixedBatch:
                 loc = LineLocator(rf)
                 loc.threads = max(1, min(loc.threads, cores))
                 self.locators.append(loc)
-            self._loc_streams = [stream] if T == 1 else [torch.cuda.Stream(device=self.device) for _ in range(T)]
-        self.fields = [None] * n
+            self._loc_streams = [torch.cuda.Stream(device=self.device) for _ in range(T)]
+        if self.fields is None or len(self.fields) != n:
+            self.fields = [None] * n
+        for st in self._loc_streams:
+            st.wait_event(ready)
 
         def work(ti):
             st = self._loc_streams[ti]
             with torch.cuda.stream(st):
-                for i in range(ti, n, T):
+                for i in indices:
+                    if i % T != ti:
+                        continue
                     arrays = {k: self.outs[i][k] for k in FIELD_KEYS if k in self.outs[i]}
                     self.fields[i] = self.locators[i].locate(arrays, self.nblocks[i], st)
 
         if T == 1:
             work(0)
-            return self.fields
-        ev = torch.cuda.Event()
-        ev.record(stream)
-        for st in self._loc_streams:
-            st.wait_event(ev)
+            return
         from concurrent.futures import ThreadPoolExecutor
         with ThreadPoolExecutor(T) as ex:
             list(ex.map(work, range(T)))
-        for st in self._loc_streams:
-            stream.wait_stream(st)
-        return self.fields
 
     def field_geometry(self, system):
         rf = self.rfs[system]
@@ -268,57 +307,97 @@ class MixedBatch:
         """One TBC launch over every located field of every capture; uint16
         pictures, capture after capture, field after field, in
         `self.pictures` (offsets per capture in `self.picture_offsets`)."""
-        import numpy as np
+        stream = stream or self.stream
+        pics, offs = self._tbc(list(range(len(self.captures))), stream, 0)
+        self.pictures = pics
+        self.picture_offsets = np.array([offs[i] for i in range(len(self.captures))] +
+                                        [offs[len(self.captures) - 1] + self._pic_size(len(self.captures) - 1)])
+        return pics
+
+    def _pic_size(self, i):
+        w, h = self.field_geometry(self.captures[i][0])
+        return len(self.fields[i]) * w * h
+
+    def _tbc(self, indices, stream, slot):
+        """One TBC launch over the located fields of captures `indices`, into
+        picture buffer `slot`; returns (buffer, {capture: offset})."""
         from .field import tbc_fields
         from .lines import field_levels, tbc_batch
         torch = self.torch
-        stream = stream or self.stream
-        sizes = []
-        for (system, _), fl in zip(self.captures, self.fields):
-            w, h = self.field_geometry(system)
-            sizes.append(len(fl) * w * h)
-        offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
-        total = int(offs[-1])
-        if self.pictures is None or self.pictures.numel() < total:
+        offs, total = {}, 0
+        for i in indices:
+            offs[i] = total
+            total += self._pic_size(i)
+        buf = self._pics.get(slot, (None, None))[0]
+        if buf is None or buf.numel() < total:
             with torch.cuda.stream(stream):
-                self.pictures = torch.empty(max(total, 1), dtype=torch.uint16,
-                                            device=torch.device("cuda", self.device))
-        self.picture_offsets = offs
-        base = self.pictures.data_ptr()
+                buf = torch.empty(max(total, 1), dtype=torch.uint16, device=torch.device("cuda", self.device))
+        self._pics[slot] = (buf, offs)
+        for i in indices:
+            self._pic_index[i] = (buf, offs[i])
+        base = buf.data_ptr()
         descs = []
-        for (system, _), fl, o, off in zip(self.captures, self.fields, self.outs, offs[:-1]):
+        for i in indices:
+            system = self.captures[i][0]
             rf = self.rfs[system]
-            if len(fl):
-                descs.append(tbc_batch(rf, fl, o["demod"].data_ptr(), base + 2 * int(off), field_levels(rf)))
+            if len(self.fields[i]):
+                descs.append(tbc_batch(rf, self.fields[i], self.outs[i]["demod"].data_ptr(), base + 2 * offs[i],
+                                       field_levels(rf)))
         n = sum(len(d) for d in descs)
-        if n == 0:
-            return self.pictures[:0]
-        allf = (L.TbcField * n)()
-        k = 0
-        for d in descs:
-            ctypes.memmove(ctypes.addressof(allf) + k * ctypes.sizeof(L.TbcField), ctypes.addressof(d),
-                           ctypes.sizeof(d))
-            k += len(d)
-        # the sinc table is the same for both systems: any context runs the batch
-        rf0 = self.rfs[self.captures[0][0]]
-        tbc_fields(rf0, allf, stream=_raw_stream(stream), asynchronous=True)
-        return self.pictures[:total]
+        if n:
+            allf = (L.TbcField * n)()
+            k = 0
+            for d in descs:
+                ctypes.memmove(ctypes.addressof(allf) + k * ctypes.sizeof(L.TbcField), ctypes.addressof(d),
+                               ctypes.sizeof(d))
+                k += len(d)
+            # the sinc table is the same for both systems: any context runs the batch
+            rf0 = self.rfs[self.captures[indices[0]][0]]
+            tbc_fields(rf0, allf, stream=_raw_stream(stream), asynchronous=True)
+        return buf[:max(total, 0)], offs
 
     def picture(self, capture, field):
         """uint16 (lines, width) view of one field's picture."""
         system = self.captures[capture][0]
         w, h = self.field_geometry(system)
-        o = int(self.picture_offsets[capture]) + field * w * h
-        return self.pictures[o:o + w * h].view(h, w)
+        buf, off = self._pic_index[capture]
+        o = off + field * w * h
+        return buf[o:o + w * h].view(h, w)
 
     def run(self, stream=None, graph=True):
         """Demodulate, locate and resample everything; returns the number of
-        fields."""
+        fields.  Pipelined when built with pipeline > 1: the group queues
+        are launched back to back, and each group's line locations and TBC
+        are enqueued as soon as its demodulation is done."""
         stream = stream or self.stream
-        self.demod(stream, graph)
-        self.locate(stream)
-        self.tbc(stream)
+        if self.pipeline == 1:
+            self.demod(stream, graph)
+            self.locate(stream)
+            self.tbc(stream)
+            return sum(len(f) for f in self.fields)
+        torch = self.torch
+        if not hasattr(self, "_tbc_stream"):
+            self._tbc_stream = torch.cuda.Stream(device=self.device, priority=-1)
+        grab = self.queue.schedule[0]  # the autotuned blocks per pop, if any
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        evs = []
+        for q in self._group_queues:
+            if q.schedule != (grab, max(1, sms - self.reserve_sms)):
+                q.set_schedule(grab, max(1, sms - self.reserve_sms))
+            q.run(stream, graph)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            evs.append(ev)
+        self.fields = [None] * len(self.captures)
+        for g, (idx, ev) in enumerate(zip(self._groups, evs)):
+            self._locate(idx, ev)
+            for st in self._loc_streams:
+                self._tbc_stream.wait_stream(st)
+            self._tbc(idx, self._tbc_stream, g)
+        stream.wait_stream(self._tbc_stream)
         return sum(len(f) for f in self.fields)
 
     def close(self):
         self.queue.close()
+        for q in self._group_queues:
+            q.close()

@@ -136,3 +136,27 @@ def test_mixed_path_equals_captures_alone(batch):
         got = mb.pictures[off:off + len(fl) * w * h]
         assert torch.equal(got.view(torch.int16), pics.view(torch.int16)), i
         assert mb.picture(i, 0).shape == (h, w)
+
+
+def test_pipelined_groups_equal_one_pass(batch):
+    """The same captures in 3 groups (3 queues, each group's line
+    locations and TBC overlapping the next group's demodulation) give the
+    same fields and pictures as the one-queue pass."""
+    import torch
+    from ldgpu.batch import MixedBatch
+    mb = batch
+    torch.cuda.synchronize()
+    mb.run()
+    torch.cuda.synchronize()
+    want = {i: [mb.picture(i, f).clone() for f in range(len(mb.fields[i]))] for i in range(len(mb.captures))}
+    mp = MixedBatch(mb.captures, pipeline=3, reserve_sms=40, locate_threads=2, rfs=mb.rfs)
+    assert len(mp._groups) == 3 and sum(len(g) for g in mp._groups) == len(mb.captures)
+    for _ in range(2):
+        n = mp.run()
+        torch.cuda.synchronize()
+        assert n == sum(len(f) for f in mb.fields)
+        for i in range(len(mb.captures)):
+            assert len(mp.fields[i]) == len(mb.fields[i])
+            for f in range(len(mb.fields[i])):
+                assert torch.equal(mp.picture(i, f).view(torch.int16), want[i][f].view(torch.int16)), (i, f)
+    mp.close()
