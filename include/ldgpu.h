@@ -172,6 +172,13 @@ int ldg_synchronize(ldg_ctx* ctx);
  * counterpart in the reference. */
 int ldg_demod_status(ldg_ctx* ctx, int32_t* flags);
 
+/* PAL_V4300D_NotchFilter (core.py:329, 774-798): search bins [lo, hi) of
+ * each block's spectrum (the reference uses int(N * 8.42 / MHz) ..
+ * int(1 + N * 8.6 / MHz)); bins above the band's mean + 3 std are zeroed
+ * with their neighbours before the video, EFM and audio filters (rfhpf uses
+ * the spectrum before).  0, 0 turns it off (the default). */
+int ldg_set_notch(ldg_ctx* ctx, int32_t lo, int32_t hi);
+
 /* Device scratch the demodulator uses for a batch of `nblocks` blocks
  * (bytes; parked spectra, one slot per resident CTA). */
 int ldg_demod_scratch_bytes(ldg_ctx* ctx, int64_t nblocks, int64_t* bytes);

@@ -111,6 +111,7 @@ struct ldg_ctx {
     size_t drop_errs_cap = 0;
     cudaEvent_t drop_done = nullptr;
     bool drop_used = false;
+    int notch_lo = 0, notch_hi = 0;      // PAL_V4300D_NotchFilter search band (bins), 0 0: off
     long long* h_word = nullptr;         // pinned, mapped: results the host reads right after a kernel
     ldg::RfTbcField* d_rftbc = nullptr;  // ldg_rf_tbc descriptors, same reuse rule
     size_t rftbc_cap = 0;
@@ -287,6 +288,16 @@ int ldg_set_sinc_lut(ldg_ctx* c, const float* lut, int32_t rows, int32_t taps) {
     return LDG_OK;
 }
 
+int ldg_set_notch(ldg_ctx* c, int32_t lo, int32_t hi) {
+    if (!c) return fail(LDG_ERR_ARG, "ldg_set_notch: NULL context");
+    if (!(lo == 0 && hi == 0) && !(lo >= 2 && hi > lo && hi <= ldg::kM - 2 && hi - lo <= 1024))
+        return fail(LDG_ERR_ARG, "ldg_set_notch: the band must satisfy 2 <= lo < hi <= blocklen/2 - 2, at most 1024 bins");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->notch_lo = lo;
+    c->notch_hi = hi;
+    return LDG_OK;
+}
+
 int ldg_demod_scratch_bytes(ldg_ctx* c, int64_t nblocks, int64_t* bytes) {
     if (!c || !bytes) return fail(LDG_ERR_ARG, "ldg_demod_scratch_bytes: NULL argument");
     const long long grid = nblocks < c->sms ? nblocks : c->sms;
@@ -426,6 +437,8 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     p.nslots = c->nslots;
     p.error = c->d_slots + c->nslots;
     p.blocks_per_cta = per_cta;
+    p.notch_lo = c->notch_lo;
+    p.notch_hi = c->notch_hi;
 
     cudaError_t e = ldg::launch_demod(p, grid, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("demod launch: ") + cudaGetErrorString(e));
@@ -883,6 +896,8 @@ int device_params(ldg_ctx* c, const ldg_demod_args* a, const std::string& who, D
     p->s_audio = {a->audio.start, a->audio.len, 0};
     p->tw16 = c->d_tw16;
     p->tw32 = c->d_tw32;
+    p->notch_lo = c->notch_lo;
+    p->notch_hi = c->notch_hi;
     return LDG_OK;
 }
 

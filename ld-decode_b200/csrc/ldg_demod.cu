@@ -240,6 +240,47 @@ __device__ void audio_stage(const DemodParams& p, float2* A, const Tables& t, in
     }
 }
 
+// PAL_V4300D_NotchFilter (lddecode/core.py:774-798) on the parked input
+// spectrum: in bins [lo, hi), every bin whose magnitude exceeds the band's
+// mean + 3 std (FP64, population std) is zeroed with its two neighbours; the
+// mirrored negative-frequency bins are implicit in the half spectrum.  One
+// warp; the decisions use the magnitudes before any bin is zeroed.  At most
+// 1024 bins (checked on the host).
+__device__ void notch_park(float2* park, int lo, int hi) {
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    const int n = hi - lo;
+    auto mag = [&](int i) {
+        const float2 x = park[lo + i];
+        return sqrt((double)x.x * (double)x.x + (double)x.y * (double)x.y);
+    };
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s += mag(i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double mean = s / (double)n;
+    double q = 0.0;
+    for (int i = lane; i < n; i += 32) {
+        const double d = mag(i) - mean;
+        q += d * d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+    const double m = mean + sqrt(q / (double)n) * 3.0;
+    unsigned flags = 0;
+    for (int i = lane, j = 0; i < n; i += 32, ++j)
+        if (mag(i) > m) flags |= 1u << j;
+    __syncwarp();
+    for (int i = lane, j = 0; i < n; i += 32, ++j) {
+        if ((flags >> j) & 1u) {
+            const float2 z = make_float2(0.f, 0.f);
+            park[lo + i - 1] = z;
+            park[lo + i] = z;
+            park[lo + i + 1] = z;
+        }
+    }
+}
+
 // Invalidate this CTA's scratch (parkX and parkZ, kScratchPerCta bytes,
 // 128-byte aligned) in L2 without write-back: discard.global.L2 per 128-byte
 // line.  Every thread of the CTA is past its last scratch access.
@@ -271,6 +312,12 @@ __device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float
         post_r2c(S, t, parkX, p.o_rfhpf ? p.f_rfhpf : nullptr, p.audio ? &au : nullptr);
     }
     __syncthreads();
+    // rfhpf (already in S) and the audio taps use the spectrum before the
+    // notch, as the reference does (its notch band lies far from the audio bands)
+    if (p.notch_hi > p.notch_lo) {
+        notch_park(parkX, p.notch_lo, p.notch_hi);
+        __syncthreads();
+    }
     if (p.audio) audio_stage(p, A, t, blk);
 
     // ---- rfhpf

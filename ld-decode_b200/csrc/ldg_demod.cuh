@@ -64,6 +64,9 @@ struct DemodParams {
     int nslots;
     int* error;
     int blocks_per_cta;   // per-slot mode: consecutive blocks a CTA works through
+
+    // PAL_V4300D_NotchFilter: bins [notch_lo, notch_hi) searched (0, 0: off)
+    int notch_lo, notch_hi;
 };
 
 constexpr int kDemodErrSlotWait = 1;

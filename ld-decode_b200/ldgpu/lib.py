@@ -136,6 +136,7 @@ SIGNATURES = {
                                      ctypes.c_double, ctypes.c_double]),
     "ldg_set_sinc_lut": (ctypes.c_int, [c_p, c_p, ctypes.c_int32, ctypes.c_int32]),
     "ldg_demod_blocks": (ctypes.c_int, [c_p, ctypes.POINTER(DemodArgs)]),
+    "ldg_set_notch": (ctypes.c_int, [c_p, ctypes.c_int32, ctypes.c_int32]),
     "ldg_copy_async": (ctypes.c_int, [c_p, c_p, ctypes.c_int64, c_p]),
     "ldg_unpack_lds": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, c_p, c_p]),
     "ldg_rf_tbc": (ctypes.c_int, [c_p, ctypes.POINTER(RfTbcField), ctypes.c_int32, c_p]),

@@ -150,6 +150,11 @@ class RFDecode(RFParams):
                          has_analog_audio, extra_options, decoder_params_override, _design=False)
         self.device = device
         self._ctx = L.Context(system, blocklen, self.freq_hz, device)
+        if self.system == "PAL" and self.PAL_V4300D_NotchFilter:
+            # the reference's search band (core.py:783-786)
+            lo = int(self.blocklen * (8.42 / self.freq))
+            hi = int(1 + (self.blocklen * (8.6 / self.freq)))
+            L.check(self._ctx._lib.ldg_set_notch(self._ctx.handle, lo, hi))
         self._mtf_loaded = None
         self._lut_loaded = False
         self.computefilters()
@@ -225,8 +230,6 @@ class RFDecode(RFParams):
             raise Exception("demodblock called without raw or FFT data")
         if len(x) != self.blocklen:
             raise ValueError(f"demodblock needs {self.blocklen} samples, got {len(x)}")
-        if self.PAL_V4300D_NotchFilter and self.system == "PAL":
-            raise NotImplementedError("PAL_V4300D_NotchFilter is not available on the GPU path")
         if x.dtype == np.int16:
             kind = L.LDG_IN_INT16
             x = np.ascontiguousarray(x)

@@ -36,9 +36,24 @@ def audio_slice(spec, lowbin, nbins, blocklen):
                            spec[blocklen - lowbin - h:blocklen - lowbin]])
 
 
+def notch_v4300d(X, blocklen, freq_mhz):
+    """PAL_V4300D_NotchFilter (core.py:774-798): in 8.42-8.6 MHz, bins whose
+    magnitude exceeds mean + 3 std of the band are zeroed with their two
+    neighbours and the mirrored negative-frequency bins.  Returns a copy."""
+    X = np.array(X, copy=True)
+    sl = slice(int(blocklen * (8.42 / freq_mhz)), int(1 + (blocklen * (8.6 / freq_mhz))))
+    sq = np.sqrt(X[sl].real ** 2 + X[sl].imag ** 2)
+    m = np.mean(sq) + (np.std(sq) * 3)
+    for i in np.where(sq > m)[0]:
+        for d in (-1, 0, 1):
+            X[i + d + sl.start] = 0
+            X[blocklen - (i + d + sl.start)] = 0
+    return X
+
+
 def demodblock(data, filters, system="NTSC", freq_hz=40e6, blocklen=32768,
                blockcut=1024, blockcut_end=32, video_rot=3, mtf_level=0.0,
-               cut=True, efm=False, audio=None, fftdata=None):
+               cut=True, efm=False, audio=None, fftdata=None, pal_notch=False):
     """Restatement of RFDecode.demodblock_cpu (core.py:755-879).
 
     `mtf_level` is the already-scaled exponent (core.py:747-752 applies the
@@ -60,6 +75,9 @@ def demodblock(data, filters, system="NTSC", freq_hz=40e6, blocklen=32768,
     hp = np.fft.ifft(X * F["Frfhpf"]).real
     end = -blockcut_end - video_rot
     rv["rfhpf"] = hp[blockcut - video_rot:end if end != 0 else None].astype(np.float32)
+
+    if pal_notch and system == "PAL":
+        X = notch_v4300d(X, blocklen, freq_hz / 1e6)
 
     Y = X * F["RFVideo"]
     if mtf_level != 0:

@@ -9,6 +9,9 @@ by ldgpu.synth, and saves small .npz fixtures:
                         audio slice geometry, computedelays results;
   demod_<cfg>.npz    -- one input block and the reference demodblock outputs
                         (subsampled video/rfhpf/efm, full audio) at two MTF levels;
+  demod_pal_notch.npz -- a PAL block with spurious 8.5 MHz tones through the
+                        reference demodblock with PAL_V4300D_NotchFilter on
+                        (core.py:774-798): outputs and the zeroed bins;
   field_<sys>.npz    -- a capture, and for two consecutive fields the
                         reference's sync pulses, line locations, field flags,
                         TBC coordinates summary and the final uint16 picture;
@@ -353,6 +356,42 @@ def lds_fixture():
     np.savez_compressed(os.path.join(HERE, "lds_unpack.npz"), **out)
 
 
+def notch_fixture(seed=33):
+    kw = dict(system="PAL", decode_analog_audio=44100, decode_digital_audio=True,
+              extra_options={"PAL_V4300D_NotchFilter": True})
+    rf = refcore.RFDecode(**kw)
+    cap = synth_capture("PAL", rf.blocklen + 4096, seed=seed).numpy()
+    t = np.arange(len(cap), dtype=np.float64)
+    # spurious carriers inside the notch search band (8.42-8.6 MHz), as the
+    # LD-V4300D players add them
+    tone = 300.0 * np.cos(2 * np.pi * 8.52e6 / 40e6 * t) + 120.0 * np.cos(2 * np.pi * 8.471e6 / 40e6 * t + 1.0)
+    cap = np.clip(np.round(cap + tone), -32768, 32767).astype(np.int16)
+    block = cap[1000:1000 + rf.blocklen].copy()
+    out = {"block": block}
+    rv = rf.demodblock(data=block, mtf_level=1, cut=True)
+    for k in rv["video"].dtype.names:
+        v = np.asarray(rv["video"][k])
+        out[f"m1_{k}"] = v[::STRIDE]
+        out[f"m1_{k}_sum"] = np.array([np.sum(v.astype(np.float64)), np.sum(v.astype(np.float64) ** 2)])
+    out["m1_rfhpf"] = rv["rfhpf"][::STRIDE]
+    out["m1_efm"] = rv["efm"][::STRIDE]
+    out["m1_audio_left"] = np.asarray(rv["audio"]["audio_left"])
+    # the bins the reference zeroes (its own rule, on the block's spectrum)
+    X = np.fft.fft(block.astype(np.float64))
+    sl = slice(int(rf.blocklen * (8.42 / rf.freq)), int(1 + (rf.blocklen * (8.6 / rf.freq))))
+    sq = np.sqrt(X[sl].real ** 2 + X[sl].imag ** 2)
+    m = np.mean(sq) + np.std(sq) * 3
+    zero = sorted({sl.start + i + d for i in np.where(sq > m)[0] for d in (-1, 0, 1)})
+    out["notch_bins"] = np.array(zero, dtype=np.int64)
+    out["notch_slice"] = np.array([sl.start, sl.stop])
+    out["mtf_scaled"] = np.array([((1 * rf.mtf_mult) + rf.mtf_offset) * rf.DecoderParams["MTF_basemult"]])
+    # the same block without the notch, to show that it acts
+    rf2 = refcore.RFDecode(system="PAL", decode_analog_audio=44100, decode_digital_audio=True)
+    rv2 = rf2.demodblock(data=block, mtf_level=1, cut=True)
+    out["plain_demod"] = np.asarray(rv2["video"]["demod"])[::STRIDE]
+    np.savez_compressed(os.path.join(HERE, "demod_pal_notch.npz"), **out)
+
+
 def lut_fixture():
     lut = np.load(os.path.join(REF, "lddecode", "sinc_lut.npz"))["downscale_sinc_lut"]
     rows = np.concatenate([np.arange(0, 65537, 997), [32767, 32768, 65535, 65536]])
@@ -426,6 +465,9 @@ def main():
         dropout_fixture("NTSC", seed=41)
         dropout_fixture("PAL", seed=42)
         return
+    if sys.argv[1:] == ["notch"]:
+        notch_fixture()
+        return
     if sys.argv[1:] == ["lds"]:
         lds_fixture()
         return
@@ -447,6 +489,7 @@ def main():
     rftbc_fixture("NTSC", seed=21)
     rftbc_fixture("PAL", seed=22)
     lds_fixture()
+    notch_fixture()
     print("golden fixtures written to", HERE)
 
 

@@ -128,3 +128,43 @@ def test_delays_match_reference(rf):
     assert rf.delays["video_rot"] == int(rot)
     assert abs(rf.delays["video_sync"] - sync) < 0.01
     assert abs(rf.delays["video_white"] - white) < 0.01
+
+
+def test_pal_v4300d_notch(cuda_ok):
+    """PAL_V4300D_NotchFilter on a block with spurious 8.5 MHz carriers: the
+    GPU demodulator against the oracle with the notch and the reference's
+    own outputs; the batched device path gives the plain call's bits."""
+    import torch
+    from ldgpu import RFDecode
+    from oracle import demod as odemod
+    g = golden("demod_pal_notch")
+    rf = RFDecode(system="PAL", decode_analog_audio=44100, decode_digital_audio=True,
+                  extra_options={"PAL_V4300D_NotchFilter": True})
+    block = g["block"]
+    gpu = rf.demodblock(data=block, mtf_level=1, cut=True)
+    ref = odemod.demodblock(block, rf.Filters, system="PAL", freq_hz=rf.freq_hz, blocklen=rf.blocklen,
+                            blockcut=rf.blockcut, blockcut_end=rf.blockcut_end, video_rot=rf.delays["video_rot"],
+                            mtf_level=rf.scaled_mtf(1), cut=True, efm=True, audio=rf.audio, pal_notch=True)
+    for k in video_keys("PAL"):
+        rms, mx = err_stats(gpu["video"][k], ref["video"][k])
+        assert rms <= RMS_HZ and mx <= MAX_HZ, (k, rms, mx)
+        rms, mx = err_stats(gpu["video"][k][::9], g["m1_" + k])
+        assert rms <= RMS_HZ and mx <= MAX_HZ, (k, rms, mx)
+    d = np.abs(gpu["efm"].astype(int) - ref["efm"].astype(int))
+    assert d.max() <= 1 and np.mean(d == 0) > 0.999
+    rms, mx = err_stats(gpu["rfhpf"], ref["rfhpf"])
+    assert rms <= 0.05 and mx <= 1.0
+    # without the notch the outputs are far from the notched reference
+    plain = RFDecode(system="PAL", decode_analog_audio=44100, decode_digital_audio=True)
+    p = plain.demodblock(data=block, mtf_level=1, cut=True)
+    assert np.abs(p["video"]["demod"][::9].astype(np.float64) - g["m1_demod"]).max() > 1000.0
+    # device batch form: same bits as the per-block call
+    U = rf.blocklen - rf.blockcut - rf.blockcut_end
+    d_in = torch.from_numpy(np.ascontiguousarray(block)).cuda()
+    out = torch.empty(U, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    rf.demod_blocks_device(d_in.data_ptr(), 1, U, {"demod": out.data_ptr()}, mtf_level=1)
+    rf.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy(), gpu["video"]["demod"])
+    rf.close()
+    plain.close()

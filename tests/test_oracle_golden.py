@@ -55,6 +55,30 @@ def test_oracle_demod_matches_reference(system):
     assert len(rv["audio"]["audio_left"]) == 1024
 
 
+def test_oracle_pal_notch_matches_reference():
+    """PAL_V4300D_NotchFilter (core.py:774-798) on a block with spurious
+    8.5 MHz carriers: the oracle zeroes the reference's bins and its outputs
+    match the reference's; without the notch they do not."""
+    g = golden("demod_pal_notch")
+    rf = _rf("PAL")
+    X = np.fft.fft(g["block"].astype(np.float64))
+    Xn = odemod.notch_v4300d(X, rf.blocklen, rf.freq)
+    zeroed = np.nonzero((Xn == 0) & (X != 0))[0]
+    want = g["notch_bins"]
+    np.testing.assert_array_equal(zeroed[zeroed < rf.blocklen // 2], want)
+    np.testing.assert_array_equal(zeroed[zeroed >= rf.blocklen // 2], np.sort(rf.blocklen - want))
+    rv = odemod.demodblock(g["block"], rf.Filters, system="PAL", freq_hz=rf.freq_hz, blocklen=rf.blocklen,
+                           blockcut=rf.blockcut, blockcut_end=rf.blockcut_end, video_rot=3,
+                           mtf_level=float(g["mtf_scaled"][0]), cut=True, efm=True, audio=rf.audio, pal_notch=True)
+    for k in ("demod", "demod_raw", "demod_05", "demod_burst", "demod_pilot"):
+        mine = rv["video"][k][::STRIDE].astype(np.float64)
+        assert np.abs(mine - g[f"m1_{k}"]).max() <= 2.0, k
+    np.testing.assert_allclose(rv["rfhpf"][::STRIDE], g["m1_rfhpf"], rtol=0, atol=1e-3)
+    assert np.abs(rv["efm"][::STRIDE].astype(int) - g["m1_efm"]).max() <= 1
+    assert np.abs(rv["audio"]["audio_left"].astype(np.float64) - g["m1_audio_left"]).max() <= 1.0
+    assert np.abs(g["m1_demod"].astype(np.float64) - g["plain_demod"]).max() > 1000.0
+
+
 def field_demod_oracle(rf, cap, window, mtf_scaled, keys=("demod",)):
     """Capture-wide concatenated oracle outputs for one field window."""
     U = rf.blocklen - rf.blockcut - rf.blockcut_end
