@@ -114,6 +114,8 @@ typedef struct {
     double ire0, hz_ire, vsync_ire, out_scale, output_zero; /* hz_to_output */
     float* out_f32;          /* linesout*outwidth float32 (may be NULL) */
     uint16_t* out_u16;       /* linesout*outwidth uint16 (may be NULL) */
+    double wow_smoothing;    /* Field.wow_level_adjust_smoothing: 0 off, else the level-adjust
+                                IIR of utils.py:141-149 with alpha = 1 / (smoothing * outwidth) */
 } ldg_tbc_field;
 
 int ldg_abi_version(void);

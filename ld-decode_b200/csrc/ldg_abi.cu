@@ -469,6 +469,8 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
             return fail(LDG_ERR_ARG, "ldg_tbc_fields: bad line length or level");
         if (f.outlinelen != (double)(int)f.outlinelen)
             return fail(LDG_ERR_ARG, "ldg_tbc_fields: outlinelen must be an integer");
+        if (!(f.wow_smoothing >= 0) || !(f.wow_smoothing * f.outwidth >= 1 || f.wow_smoothing == 0))
+            return fail(LDG_ERR_ARG, "ldg_tbc_fields: wow_smoothing must be 0 or at least 1 / outwidth");
         ll_total += f.nlines;
         seg_total += f.nlines - 1;
         if ((long long)f.linesout * f.outwidth > max_nout) max_nout = (long long)f.linesout * f.outwidth;
@@ -477,7 +479,7 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     int rc = grow((void**)&c->d_ll, &c->ll_cap, ll_total * sizeof(double));
     if (rc) return rc;
-    rc = grow((void**)&c->d_seg, &c->seg_cap, seg_total * sizeof(double));
+    rc = grow((void**)&c->d_seg, &c->seg_cap, 3 * seg_total * sizeof(double));
     if (rc) return rc;
     if (nfields > c->fields_cap) {
         cudaFree(c->d_fields);
@@ -532,6 +534,9 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         d.u16_scale = f.out_scale / f.hz_ire;
         d.u16_offset = f.output_zero - f.vsync_ire * f.out_scale - f.ire0 * d.u16_scale;
         d.seg_level = c->d_seg + sego;
+        d.seg_start = c->d_seg + seg_total + sego;
+        d.seg_lo = reinterpret_cast<long long*>(c->d_seg + 2 * seg_total + sego);
+        d.smooth_b = f.wow_smoothing > 0 ? 1.0 - 1.0 / (f.wow_smoothing * (double)f.outwidth) : 0.0;
         d.status = c->d_status;
         d.out_f32 = x.f32 ? (float*)(c->d_stage + x.f32_off) : f.out_f32;
         d.out_u16 = x.u16 ? (uint16_t*)(c->d_stage + x.u16_off) : f.out_u16;
@@ -589,6 +594,8 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
             return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: bad line length or level");
         if (f.outlinelen != (double)(int)f.outlinelen)
             return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: outlinelen must be an integer");
+        if (!(f.wow_smoothing >= 0) || !(f.wow_smoothing * f.outwidth >= 1 || f.wow_smoothing == 0))
+            return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: wow_smoothing must be 0 or at least 1 / outwidth");
         if (!f.out_f32 && !f.out_u16) return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: no output");
         seg_total += f.nlines - 1;
         if ((long long)f.linesout * f.outwidth > max_nout) max_nout = (long long)f.linesout * f.outwidth;
@@ -615,7 +622,7 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
         LDG_CK(cudaMallocHost(&w.h_fields, nfields * sizeof(ldg::TbcField)));
         w.cap = nfields;
     }
-    int rc = grow((void**)&w.d_seg, &w.seg_cap, seg_total * sizeof(double));
+    int rc = grow((void**)&w.d_seg, &w.seg_cap, 3 * seg_total * sizeof(double));
     if (rc) return rc;
     size_t sego = 0;
     for (int i = 0; i < nfields; ++i) {
@@ -636,6 +643,9 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
         d.u16_scale = f.out_scale / f.hz_ire;
         d.u16_offset = f.output_zero - f.vsync_ire * f.out_scale - f.ire0 * d.u16_scale;
         d.seg_level = w.d_seg + sego;
+        d.seg_start = w.d_seg + seg_total + sego;
+        d.seg_lo = reinterpret_cast<long long*>(w.d_seg + 2 * seg_total + sego);
+        d.smooth_b = f.wow_smoothing > 0 ? 1.0 - 1.0 / (f.wow_smoothing * (double)f.outwidth) : 0.0;
         d.status = c->d_status;
         d.out_f32 = f.out_f32;
         d.out_u16 = f.out_u16;

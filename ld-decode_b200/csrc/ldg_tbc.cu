@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(kWowThreads) wow_levels_kernel(const TbcField*
         const long long a = min(lo, f.nwow), b = min(hi, f.nwow);
         cnt = b > a ? b - a : 0;
         slope_s[t] = slope;
+        f.seg_lo[t] = a;
     }
     key[t] = (t < nseg) ? slope : 1.0e300;
     wt[t] = cnt;
@@ -142,6 +143,23 @@ __global__ void __launch_bounds__(kWowThreads) wow_levels_kernel(const TbcField*
     if (t < nseg) {
         const double s = slope_s[t];
         f.seg_level[t] = (fabs(s - med) > thr) ? med : s;
+    }
+    if (f.smooth_b > 0) {
+        // level-adjust IIR (utils.py:141-149), y[0] = la[0], y[i] = a la[i] +
+        // b y[i-1]: over segment j (constant level c_j) it is c_j + (y_before
+        // - c_j) b^(i - lo_j + 1); the value entering each segment is carried
+        // from segment to segment by one thread
+        __syncthreads();
+        if (t == 0) {
+            double y = f.seg_level[0];
+            for (int j = 0; j < nseg; ++j) {
+                const double c = f.seg_level[j];
+                f.seg_start[j] = y;
+                const long long hi = (j + 1 < nseg) ? f.seg_lo[j + 1] : f.nwow;
+                const long long len = hi - f.seg_lo[j];
+                if (len > 0) y = c + (y - c) * pow(f.smooth_b, (double)len);
+            }
+        }
     }
 }
 
@@ -217,7 +235,12 @@ __global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcFie
         if (k == p) mine = part;
     }
     if (i >= nout) return;
-    const float out = (float)(f.seg_level[jj] * mine);
+    double level = f.seg_level[jj];
+    if (f.smooth_b > 0) {
+        const long long ig = igbase + i;  // index into the wow array
+        level = level + (f.seg_start[jj] - level) * pow(f.smooth_b, (double)(ig - f.seg_lo[jj] + 1));
+    }
+    const float out = (float)(level * mine);
     if (f.out_f32) f.out_f32[i] = out;
     if (f.out_u16) {
         double v = (double)out * f.u16_scale + f.u16_offset + 0.5;

@@ -23,6 +23,9 @@ struct TbcField {
     double u16_scale;    // out_scale / hz_ire
     double u16_offset;   // output_zero - vsync_ire*out_scale - ire0*u16_scale
     double* seg_level;   // nlines-1 level-adjust factors (device scratch)
+    double smooth_b;     // 1 - alpha of the level-adjust IIR, 0: off
+    double* seg_start;   // with the IIR: the smoothed level just before segment j
+    long long* seg_lo;   // first wow pixel of segment j
     int* status;         // LDG_TBC_* bits
     float* out_f32;
     uint16_t* out_u16;

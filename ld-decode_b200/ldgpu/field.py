@@ -17,7 +17,7 @@ from .linelocs import FieldLogic, FieldLogicNTSC, FieldLogicPAL
 
 
 def tbc_descriptor(rf, buf, linelocs, lineoffset, outwidth, linesout, outlinecount, levels,
-                   out_u16=None, out_f32=None, coord_f32=False, buf_len=None, nlines=None):
+                   out_u16=None, out_f32=None, coord_f32=False, buf_len=None, nlines=None, wow_smoothing=0.0):
     """Fill an ldg_tbc_field from numpy arrays or raw device pointers (ints;
     then buf_len / nlines must be given).
 
@@ -37,6 +37,7 @@ def tbc_descriptor(rf, buf, linelocs, lineoffset, outwidth, linesout, outlinecou
     d.ire0, d.hz_ire, d.vsync_ire, d.out_scale, d.output_zero = [float(v) for v in levels]
     d.out_f32 = None if out_f32 is None else (out_f32 if isinstance(out_f32, int) else out_f32.ctypes.data)
     d.out_u16 = None if out_u16 is None else (out_u16 if isinstance(out_u16, int) else out_u16.ctypes.data)
+    d.wow_smoothing = float(wow_smoothing or 0.0)
     return d
 
 
@@ -108,8 +109,6 @@ class Field(FieldLogic):
             outwidth = self.outlinelen
         if linesout is None:
             linesout = self.outlinecount
-        if self.wow_level_adjust_smoothing:
-            raise NotImplementedError("wow_level_adjust_smoothing is not available on the GPU path")
         if self.wow_interpolation_method != "linear":
             raise NotImplementedError("only linear wow interpolation is available on the GPU path")
         buf = np.ascontiguousarray(self.data["video"][channel], dtype=np.float32)
@@ -118,7 +117,8 @@ class Field(FieldLogic):
         dsout = np.empty(nout, dtype=np.float32)
         pic = np.empty(nout, dtype=np.uint16) if final else None
         desc = tbc_descriptor(self.rf, buf, ll, self.lineoffset, outwidth, linesout, self.outlinecount,
-                              self.levels(), out_u16=pic, out_f32=dsout, coord_f32=self.coord_f32)
+                              self.levels(), out_u16=pic, out_f32=dsout, coord_f32=self.coord_f32,
+                              wow_smoothing=self.wow_level_adjust_smoothing)
         tbc_fields(self.rf, [desc])
 
         dsaudio = None

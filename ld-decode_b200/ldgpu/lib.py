@@ -54,7 +54,7 @@ class TbcField(ctypes.Structure):
         ("inlinelen", ctypes.c_double), ("outlinelen", ctypes.c_double),
         ("ire0", ctypes.c_double), ("hz_ire", ctypes.c_double), ("vsync_ire", ctypes.c_double),
         ("out_scale", ctypes.c_double), ("output_zero", ctypes.c_double),
-        ("out_f32", c_p), ("out_u16", c_p),
+        ("out_f32", c_p), ("out_u16", c_p), ("wow_smoothing", ctypes.c_double),
     ]
 
 

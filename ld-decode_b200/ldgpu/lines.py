@@ -53,7 +53,7 @@ TBC_DTYPE = _dtype_of(L.TbcField, {
     "buf": "u8", "buf_len": "i8", "linelocs": "u8", "nlines": "i4", "lineoffset": "i4", "outwidth": "i4",
     "linesout": "i4", "outlinecount": "i4", "coord_f32": "i4", "inlinelen": "f8", "outlinelen": "f8",
     "ire0": "f8", "hz_ire": "f8", "vsync_ire": "f8", "out_scale": "f8", "output_zero": "f8",
-    "out_f32": "u8", "out_u16": "u8"})
+    "out_f32": "u8", "out_u16": "u8", "wow_smoothing": "f8"})
 
 
 def proclines_for(rf):

@@ -9,6 +9,9 @@ by ldgpu.synth, and saves small .npz fixtures:
                         audio slice geometry, computedelays results;
   demod_<cfg>.npz    -- one input block and the reference demodblock outputs
                         (subsampled video/rfhpf/efm, full audio) at two MTF levels;
+  tbc_smoothing_<sys>.npz -- the first golden field through the reference's
+                        TBC with wow_level_adjust_smoothing = 2 (utils.py:
+                        141-149): line locations and the uint16 picture;
   demod_pal_notch.npz -- a PAL block with spurious 8.5 MHz tones through the
                         reference demodblock with PAL_V4300D_NotchFilter on
                         (core.py:774-798): outputs and the zeroed bins;
@@ -392,6 +395,37 @@ def notch_fixture(seed=33):
     np.savez_compressed(os.path.join(HERE, "demod_pal_notch.npz"), **out)
 
 
+def smoothing_fixture(system, seed, smoothing=2.0):
+    kw = dict(system=system, decode_analog_audio=0, decode_digital_audio=False)
+    rf = refcore.RFDecode(**kw)
+    src = BlockSource(rf, None, 1)
+    fieldcls = refcore.FieldPAL if system == "PAL" else refcore.FieldNTSC
+    src.readlen = rf.linelen * 400 if system == "PAL" else ((rf.linelen * 350) // 16384) * 16384
+    fieldlen = int(rf.freq_hz / (rf.SysParams["FPS"] * 2))
+    ncap = 2 * fieldlen + src.readlen + 8 * rf.blocklen
+    cap = synth_capture(system, ncap, seed=seed, start=CAPTURE_START).numpy()
+    src.cap = cap
+    start = 0
+    while True:
+        decode, readloc = src.read_field(start)
+        f = fieldcls(rf, decode, prevfield=None, initphase=True, fields_written=0, readloc=decode["startloc"],
+                     wow_level_adjust_smoothing=smoothing)
+        f.process()
+        if f.valid:
+            break
+        start += f.nextfieldoffset
+    f.downscale(linesout=f.outlinecount, final=True)
+    np.savez_compressed(os.path.join(HERE, f"tbc_smoothing_{system.lower()}.npz"),
+                        capture_sha256=np.array(sha(cap)), capture_len=np.array(ncap), capture_seed=np.array(seed),
+                        capture_start=np.array(CAPTURE_START), mtf_level=np.array(1.0), smoothing=np.array(smoothing),
+                        start=np.array(start), startloc=np.array(decode["startloc"]),
+                        linelocs=np.array(f.linelocs, dtype=np.float64),
+                        flags=np.array([int(f.isFirstField), f.linecount, f.lineoffset], dtype=np.int64),
+                        levels=np.array([rf.DecoderParams["ire0"], rf.DecoderParams["hz_ire"],
+                                         rf.DecoderParams["vsync_ire"], f.out_scale, rf.SysParams["outputZero"]]),
+                        dspicture=np.asarray(f.dspicture))
+
+
 def lut_fixture():
     lut = np.load(os.path.join(REF, "lddecode", "sinc_lut.npz"))["downscale_sinc_lut"]
     rows = np.concatenate([np.arange(0, 65537, 997), [32767, 32768, 65535, 65536]])
@@ -465,6 +499,10 @@ def main():
         dropout_fixture("NTSC", seed=41)
         dropout_fixture("PAL", seed=42)
         return
+    if sys.argv[1:] == ["smoothing"]:
+        smoothing_fixture("NTSC", seed=21)
+        smoothing_fixture("PAL", seed=22)
+        return
     if sys.argv[1:] == ["notch"]:
         notch_fixture()
         return
@@ -490,6 +528,8 @@ def main():
     rftbc_fixture("PAL", seed=22)
     lds_fixture()
     notch_fixture()
+    smoothing_fixture("NTSC", seed=21)
+    smoothing_fixture("PAL", seed=22)
     print("golden fixtures written to", HERE)
 
 

@@ -123,3 +123,46 @@ def test_tbc_batched_fields(case):
     tbc_fields(rf, descs)
     np.testing.assert_array_equal(outs[0][1], single)
     assert not np.array_equal(outs[1][1], single)
+
+
+@pytest.mark.parametrize("system", ["NTSC", "PAL"])
+def test_tbc_level_smoothing(cuda_ok, system):
+    """wow_level_adjust_smoothing = 2: the GPU picture against the
+    reference's (compat mode) and against the FP64 oracle with the same IIR
+    (FP64 coordinates)."""
+    from ldgpu import RFDecode
+    from ldgpu.field import FieldNTSC, FieldPAL
+    from ldgpu.fieldread import field_window
+    from ldgpu.synth import synth_capture
+    g = golden("tbc_smoothing_" + system.lower())
+    rf = RFDecode(system=system)
+    cap = synth_capture(system, int(g["capture_len"]), seed=int(g["capture_seed"]),
+                        start=int(g["capture_start"])).numpy()
+    w = field_window(rf, float(g["start"]))
+    buf = oracle_capture(rf, cap, w.first_block, w.nblocks, rf.scaled_mtf(float(g["mtf_level"])))["demod"]
+    isfirst, linecount, lineoffset = (int(v) for v in g["flags"])
+    ire0, hz_ire, vsync_ire, out_scale, ozero = g["levels"]
+    smoothing = float(g["smoothing"])
+    cls = FieldPAL if system == "PAL" else FieldNTSC
+    outw = rf.SysParams["outlinelen"]
+    outlines = rf.SysParams["frame_lines"] // 2 + 1
+    coords, wow = otbc.pixel_coords(g["linelocs"], rf.linelen, outw, outlines, lineoffset)
+    for coord_f32 in (True, False):
+        f = cls(rf, {"video": {"demod": buf}, "startloc": int(g["startloc"])}, wow_level_adjust_smoothing=smoothing)
+        f.linelocs = g["linelocs"]
+        f.lineoffset, f.linecount, f.isFirstField = lineoffset, linecount, bool(isfirst)
+        f.coord_f32 = coord_f32
+        f.out_scale = out_scale
+        pic, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+        if coord_f32:
+            d = np.abs(pic.astype(int) - g["dspicture"].astype(int))
+            print(system, "smoothing, compat vs reference: max", d.max(), "exact", np.mean(d == 0))
+            assert d.max() <= 1 and np.mean(d == 0) >= 0.99
+        else:
+            ds = otbc.scale_field(buf, coords, wow, rf.downscale_sinc_lut, lineoffset, outw, outlines * outw,
+                                  smoothing=smoothing)
+            opic = otbc.hz_to_output(ds, ire0, hz_ire, ozero, vsync_ire, out_scale)
+            d = np.abs(pic.astype(int) - opic.astype(int))
+            print(system, "smoothing, fp64 vs oracle: max", d.max(), "within 1", np.mean(d <= 1))
+            assert np.mean(d <= 1) >= 0.9999 and d.max() <= 2
+    rf.close()

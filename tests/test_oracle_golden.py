@@ -125,3 +125,31 @@ def test_oracle_tbc_matches_reference(system):
         d = np.abs(pic.astype(int) - ref.astype(int))
         assert d.max() <= 1, (i, d.max())
         assert np.mean(d == 0) > 0.99, (i, np.mean(d == 0))
+
+
+@pytest.mark.parametrize("system", ["NTSC", "PAL"])
+def test_oracle_tbc_smoothing_matches_reference(system):
+    """wow_level_adjust_smoothing = 2 (the level-adjust IIR, utils.py:141-149):
+    the oracle's picture (compat mode) against the reference's."""
+    g = golden("tbc_smoothing_" + system.lower())
+    rf = RFParams(system=system)
+    cap = synth_capture(system, int(g["capture_len"]), seed=int(g["capture_seed"]),
+                        start=int(g["capture_start"])).numpy()
+    outw = rf.SysParams["outlinelen"]
+    outlines = rf.SysParams["frame_lines"] // 2 + 1
+    w = field_window(rf, float(g["start"]))
+    assert w.startloc == int(g["startloc"])
+    buf = field_demod_oracle(rf, cap, w, rf.scaled_mtf(float(g["mtf_level"])))["demod"]
+    lineoffset = int(g["flags"][2])
+    coords, wow = otbc.pixel_coords(g["linelocs"], rf.linelen, outw, outlines, lineoffset)
+    ire0, hz_ire, vsync_ire, out_scale, ozero = g["levels"]
+    ds = otbc.scale_field(buf, coords, wow, rf.downscale_sinc_lut, lineoffset, outw, outlines * outw,
+                          coord_f32=True, smoothing=float(g["smoothing"]))
+    pic = otbc.hz_to_output(ds, ire0, hz_ire, ozero, vsync_ire, out_scale)
+    d = np.abs(pic.astype(int) - g["dspicture"].astype(int))
+    assert d.max() <= 1 and np.mean(d == 0) > 0.99, (d.max(), np.mean(d == 0))
+    # the smoothing acts: without it the picture differs by more
+    ds0 = otbc.scale_field(buf, coords, wow, rf.downscale_sinc_lut, lineoffset, outw, outlines * outw,
+                           coord_f32=True)
+    pic0 = otbc.hz_to_output(ds0, ire0, hz_ire, ozero, vsync_ire, out_scale)
+    assert np.abs(pic0.astype(int) - g["dspicture"].astype(int)).max() > 1
