@@ -55,7 +55,9 @@ enum {
     LDG_F_EFM = 6,     /* Fefm                      (core.py:422-465, 848) */
     LDG_F_VIDEO_G_ODD = 7, /* RFVideo * MTF^mtf * exp(+2 pi i k/N): the
                               odd-sample half of the analytic inverse FFT */
-    LDG_NFILTERS = 8
+    LDG_F_AUDIO2_LEFT = 8,  /* audio2_filter, left  (core.py:722-737, 908) */
+    LDG_F_AUDIO2_RIGHT = 9, /* audio2_filter, right */
+    LDG_NFILTERS = 10
 };
 
 /* input sample type of ldg_demod_args.in */
@@ -202,6 +204,29 @@ int ldg_demod_scratch_bytes(ldg_ctx* ctx, int64_t nblocks, int64_t* bytes);
  * come from `ctx`, which is created (and allocates) beforehand.  Enqueues
  * on args->stream (or the context's stream) and returns without waiting. */
 int ldg_demod_blocks_noalloc(ldg_ctx* ctx, const ldg_demod_args* args, int32_t ctas);
+
+/* ---- Analog audio stage 2 (RFDecode.audio_phase2, core.py:884-950) ---- */
+
+/* One transform of stage-1 audio: `len` (2 .. blocklen) samples per channel
+ * from `left` / `right` (device), results to out_left / out_right (device). */
+typedef struct {
+    const float* left;
+    const float* right;
+    int64_t len;
+    float* out_left;
+    float* out_right;
+} ldg_audio2_segment;
+
+/* RFDecode.runfilter_audio_phase2 (core.py:884-915) for `n` segments in one
+ * launch: carrier removed (center_left / center_right, SysParams
+ * audio_lfreq / audio_rfreq), samples within 8 of each left-channel spike
+ * above 500 kHz zeroed in both channels (findpeaks, utils.py:1207-1216),
+ * the stage-2 filter (LDG_F_AUDIO2_*) applied by a blocklen-point transform
+ * with zero padding, carrier added back; float32 results.  The caller
+ * stitches longer inputs as audio_phase2 does (core.py:917-950).
+ * `segs` is a host array; enqueued on `stream` without waiting. */
+int ldg_audio_phase2(ldg_ctx* ctx, const ldg_audio2_segment* segs, int32_t n, double center_left,
+                     double center_right, void* stream);
 
 /* ---- Mixed batches: many captures in one launch (no reference counterpart;
  * the reference demodulates one capture's blocks at a time in

@@ -112,6 +112,10 @@ struct ldg_ctx {
     cudaEvent_t drop_done = nullptr;
     bool drop_used = false;
     int notch_lo = 0, notch_hi = 0;      // PAL_V4300D_NotchFilter search band (bins), 0 0: off
+    ldg::Audio2Seg* d_a2 = nullptr;      // ldg_audio_phase2 segments; reused once the last launch is done
+    size_t a2_cap = 0;
+    cudaEvent_t a2_done = nullptr;
+    bool a2_used = false;
     long long* h_word = nullptr;         // pinned, mapped: results the host reads right after a kernel
     ldg::RfTbcField* d_rftbc = nullptr;  // ldg_rf_tbc descriptors, same reuse rule
     size_t rftbc_cap = 0;
@@ -226,6 +230,9 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     if (c->drop_used) cudaEventSynchronize(c->drop_done);
     if (c->rftbc_used) cudaEventSynchronize(c->rftbc_done);
     if (c->h_word) cudaFreeHost(c->h_word);
+    if (c->a2_used) cudaEventSynchronize(c->a2_done);
+    cudaFree(c->d_a2);
+    if (c->a2_done) cudaEventDestroy(c->a2_done);
     cudaFree(c->d_rftbc);
     if (c->rftbc_done) cudaEventDestroy(c->rftbc_done);
     cudaFree(c->d_drop_fields);
@@ -663,6 +670,50 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
     LDG_CK(cudaEventRecord(w.done, st));
     w.used = true;
+    return LDG_OK;
+}
+
+int ldg_audio_phase2(ldg_ctx* c, const ldg_audio2_segment* segs, int32_t n, double center_left,
+                     double center_right, void* stream) {
+    if (!c || (!segs && n)) return fail(LDG_ERR_ARG, "ldg_audio_phase2: NULL argument");
+    if (n < 0) return fail(LDG_ERR_ARG, "ldg_audio_phase2: negative segment count");
+    for (int i = 0; i < n; ++i) {
+        const ldg_audio2_segment& g = segs[i];
+        if (!g.left || !g.right || !g.out_left || !g.out_right) return fail(LDG_ERR_ARG, "ldg_audio_phase2: NULL buffer");
+        if (g.len < 2 || g.len > ldg::kN)
+            return fail(LDG_ERR_ARG, "ldg_audio_phase2: a segment holds 2 .. blocklen samples");
+    }
+    if (n == 0) return LDG_OK;
+    if (!is_device_ptr(segs[0].left) || !is_device_ptr(segs[0].out_left))
+        return fail(LDG_ERR_ARG, "ldg_audio_phase2: buffers must be device memory");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->d_filter[LDG_F_AUDIO2_LEFT] || !c->d_filter[LDG_F_AUDIO2_RIGHT])
+        return fail(LDG_ERR_STATE, "ldg_audio_phase2: stage-2 audio filters not set");
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    if (!c->a2_done) LDG_CK(cudaEventCreateWithFlags(&c->a2_done, cudaEventDisableTiming));
+    if (c->a2_used) LDG_CK(cudaEventSynchronize(c->a2_done));
+    int rc = grow((void**)&c->d_a2, &c->a2_cap, (size_t)n * sizeof(ldg::Audio2Seg));
+    if (rc) return rc;
+    std::vector<ldg::Audio2Seg> h(n);
+    for (int i = 0; i < n; ++i)
+        h[i] = {segs[i].left, segs[i].right, (int)segs[i].len, segs[i].out_left, segs[i].out_right};
+    LDG_CK(cudaMemcpyAsync(c->d_a2, h.data(), h.size() * sizeof(ldg::Audio2Seg), cudaMemcpyHostToDevice, st));
+    ldg::Audio2Params p;
+    memset(&p, 0, sizeof(p));
+    p.segs = c->d_a2;
+    p.cf32[0] = (float)center_left;
+    p.cf32[1] = (float)center_right;
+    p.cf[0] = center_left;
+    p.cf[1] = center_right;
+    p.filt[0] = c->d_filter[LDG_F_AUDIO2_LEFT];
+    p.filt[1] = c->d_filter[LDG_F_AUDIO2_RIGHT];
+    p.tw16 = c->d_tw16;
+    p.tw32 = c->d_tw32;
+    cudaError_t e = ldg::launch_audio2(p, n, st);
+    if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("audio2 launch: ") + cudaGetErrorString(e));
+    LDG_CK(cudaEventRecord(c->a2_done, st));
+    c->a2_used = true;
     return LDG_OK;
 }
 

@@ -777,6 +777,7 @@ extern "C" int64_t ldg_abi_sizeof(const char* name) {
     if (n == "ldg_dropout_field") return sizeof(ldg_dropout_field);
     if (n == "ldg_dropout_params") return sizeof(ldg_dropout_params);
     if (n == "ldg_rftbc_field") return sizeof(ldg_rftbc_field);
+    if (n == "ldg_audio2_segment") return sizeof(ldg_audio2_segment);
     return -1;
 }
 

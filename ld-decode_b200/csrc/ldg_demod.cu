@@ -506,6 +506,105 @@ __global__ void __launch_bounds__(kThreads, 1) demod_queue_kernel(const __grid_c
     }
 }
 
+// ---- analog audio stage 2 (RFDecode.runfilter_audio_phase2, core.py:884-915)
+
+namespace {
+
+// raw[j] = x[j] - carrier (float32), zero where a left-channel spike is
+// within 8 samples or beyond the segment (the transform's zero padding)
+struct Audio2Loader {
+    const float* x;
+    float cf;
+    int n;
+    const unsigned* mask;
+    __device__ float val(int j) const {
+        if (j >= n || ((mask[j >> 5] >> (j & 31)) & 1u)) return 0.0f;
+        return __ldg(x + j) - cf;
+    }
+    __device__ float2 operator()(int, int m) const { return make_float2(val(2 * m), val(2 * m + 1)); }
+};
+
+struct Audio2Storer {
+    float* out;
+    double cf;
+    int n;
+    __device__ void operator()(int, int m, float2 v) const {
+        const int j = 2 * m;
+        if (j < n) out[j] = (float)((double)(v.x * kInvM) + cf);
+        if (j + 1 < n) out[j + 1] = (float)((double)(v.y * kInvM) + cf);
+    }
+};
+
+// Input spectrum from Z (as post_r2c), times the filter, into the C2R input
+// (no parking).
+__device__ void audio2_filter(float2* S, const Tables& t, const float2* F) {
+    for (int k = threadIdx.x; k <= kM / 2; k += kThreads) {
+        if (k == 0) {
+            const float2 z = S[0];
+            c2r_dc(S, z.x + z.y, z.x - z.y, F);
+            continue;
+        }
+        const float2 zk = S[pad(k)], zm = S[pad(kM - k)];
+        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+        const float2 wk = __ldg(t.t32 + k);
+        const float2 tt = cmul(wk, o);
+        const float2 xk = cadd(e, tt);
+        const float2 xm = cconj(csub(e, tt));
+        c2r_pair(S, k, cmul(xk, __ldg(F + k)), cmul(xm, __ldg(F + kM - k)), wk);
+    }
+}
+
+}  // namespace
+
+// One CTA per (segment, channel): the left channel's spikes (findpeaks,
+// utils.py:1207-1216: samples above 500 kHz from the carrier rising above
+// the segment's last value) mark +-8 samples that are zeroed in both
+// channels; then R2C, the stage-2 filter, C2R, carrier added back.
+__global__ void __launch_bounds__(kThreads, 1) audio2_kernel(const __grid_constant__ Audio2Params p) {
+    extern __shared__ float2 smem[];
+    const CtaSmem c = cta_setup(smem, p.tw16, p.tw32);
+    const Audio2Seg sg = p.segs[blockIdx.x];
+    const int ch = blockIdx.y;
+    const int n = sg.len;
+    unsigned* mask = reinterpret_cast<unsigned*>(c.A);  // kN bits in the audio-band area
+    for (int w = threadIdx.x; w < kN / 32; w += kThreads) mask[w] = 0u;
+    __syncthreads();
+    const float cfl = p.cf32[0];
+    auto a2 = [&](int i) {
+        const float v = __ldg(sg.left + i) - cfl;
+        return v < 500000.0f ? 0.0f : v;
+    };
+    const float last = a2(n - 1);
+    for (int i = threadIdx.x; i < n - 1; i += kThreads) {
+        const float ai = a2(i);
+        if (ai > last && a2(i + 1) > ai) {
+            const int l = i - 1;
+            const int lo = max(0, l - 8), hi = min(l + 8, n);
+            for (int j = lo; j < hi; ++j) atomicOr(mask + (j >> 5), 1u << (j & 31));
+        }
+    }
+    __syncthreads();
+    const float* x = ch ? sg.right : sg.left;
+    fft16k<false>(c.S, c.t, Audio2Loader{x, p.cf32[ch], n, mask});
+    audio2_filter(c.S, c.t, p.filt[ch]);
+    __syncthreads();
+    fft16k<true>(c.S, c.t, SmemIO(), Audio2Storer{ch ? sg.out_right : sg.out_left, p.cf[ch], n});
+}
+
+cudaError_t launch_audio2(const Audio2Params& p, int nsegs, cudaStream_t stream) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(audio2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kSmemBytes);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    if (nsegs <= 0) return cudaSuccess;
+    audio2_kernel<<<dim3((unsigned)nsegs, 2), kThreads, kSmemBytes, stream>>>(p);
+    return cudaGetLastError();
+}
+
 cudaError_t prepare_demod_queue() {
     static bool configured = false;
     if (!configured) {

@@ -91,7 +91,27 @@ constexpr int kSmemFloat2 = (16384 + 1024) + 2 * (1024 + 64) + 4 * 16 + 4 * 256 
 constexpr size_t kSmemBytes = size_t(kSmemFloat2) * 8;
 constexpr size_t kScratchPerCta = size_t(2) * 16384 * 8;
 
+// Analog audio stage 2 (one transform of up to kN stage-1 samples per
+// segment and channel).
+struct Audio2Seg {
+    const float* left;
+    const float* right;
+    int len;              // 2 .. kN
+    float* out_left;
+    float* out_right;
+};
+
+struct Audio2Params {
+    const Audio2Seg* segs;
+    float cf32[2];        // carriers as float32 (the reference subtracts them from float32 audio)
+    double cf[2];         // carriers added back in FP64
+    const float2* filt[2];  // half spectra of the stage-2 filters (bins 0..kN/2)
+    const float2* tw16;
+    const float2* tw32;
+};
+
 cudaError_t launch_demod(const DemodParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_audio2(const Audio2Params& p, int nsegs, cudaStream_t stream);
 // Sets the queue kernel's shared-memory size (call before a stream capture).
 cudaError_t prepare_demod_queue();
 cudaError_t launch_demod_queue(const QueueParams& q, int grid, cudaStream_t stream);

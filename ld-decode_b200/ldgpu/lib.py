@@ -16,8 +16,8 @@ LDG_OK = 0
 LDG_NTSC, LDG_PAL = 0, 1
 LDG_IN_INT16, LDG_IN_FLOAT32 = 0, 1
 (LDG_F_RFHPF, LDG_F_VIDEO_G, LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT,
- LDG_F_EFM, LDG_F_VIDEO_G_ODD) = range(8)
-LDG_NFILTERS = 8
+ LDG_F_EFM, LDG_F_VIDEO_G_ODD, LDG_F_AUDIO2_LEFT, LDG_F_AUDIO2_RIGHT) = range(10)
+LDG_NFILTERS = 10
 LDG_ERR_ARG, LDG_ERR_CUDA, LDG_ERR_STATE, LDG_ERR_UNSUPPORTED, LDG_ERR_RANGE = -1, -2, -3, -4, -5
 
 ERRORS = {-1: "argument", -2: "cuda", -3: "state", -4: "unsupported", -5: "range"}
@@ -90,6 +90,10 @@ class FieldPlan(ctypes.Structure):
     ]
 
 
+class Audio2Segment(ctypes.Structure):
+    _fields_ = [("left", c_p), ("right", c_p), ("len", c_i64), ("out_left", c_p), ("out_right", c_p)]
+
+
 class RfTbcField(ctypes.Structure):
     _fields_ = [("input", c_p), ("len", c_i64), ("linelocs", c_p), ("nlines", c_i32), ("startline", c_i32),
                 ("linecount", c_i32), ("linelen", c_i32), ("delay", c_f64), ("out", c_p)]
@@ -139,6 +143,8 @@ SIGNATURES = {
     "ldg_set_notch": (ctypes.c_int, [c_p, ctypes.c_int32, ctypes.c_int32]),
     "ldg_copy_async": (ctypes.c_int, [c_p, c_p, ctypes.c_int64, c_p]),
     "ldg_unpack_lds": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, c_p, c_p]),
+    "ldg_audio_phase2": (ctypes.c_int, [c_p, ctypes.POINTER(Audio2Segment), ctypes.c_int32, ctypes.c_double,
+                                        ctypes.c_double, c_p]),
     "ldg_rf_tbc": (ctypes.c_int, [c_p, ctypes.POINTER(RfTbcField), ctypes.c_int32, c_p]),
     "ldg_dropouts": (ctypes.c_int, [c_p, ctypes.POINTER(DropoutParams), ctypes.POINTER(DropoutField),
                                     ctypes.c_int32, c_p, c_p, c_p, c_p]),

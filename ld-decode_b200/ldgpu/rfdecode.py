@@ -185,6 +185,8 @@ class RFDecode(RFParams):
         if "Fefm" in F:
             self._set_filter(L.LDG_F_EFM, flt.half_spectrum(F["Fefm"]))
         if self.decode_analog_audio != 0:
+            self._set_filter(L.LDG_F_AUDIO2_LEFT, flt.half_spectrum(self.audio["left"].audio2_filter))
+            self._set_filter(L.LDG_F_AUDIO2_RIGHT, flt.half_spectrum(self.audio["right"].audio2_filter))
             for ch, name in enumerate(("left", "right")):
                 a = self.audio[name]
                 f1 = np.ascontiguousarray(np.stack([a.filt1.real, a.filt1.imag], axis=1).reshape(-1))
@@ -326,47 +328,75 @@ class RFDecode(RFParams):
 
     # ---- second-stage audio (per field, host FP64 as in the reference)
 
+    def _phase2_segments(self, left, right, starts):
+        """ldg_audio_phase2 over transforms of `blocklen` samples starting at
+        `starts` (each clipped to the input); float32 results per start."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        n = len(left)
+        tl = torch.from_numpy(np.ascontiguousarray(left, np.float32)).to(dev)
+        tr = torch.from_numpy(np.ascontiguousarray(right, np.float32)).to(dev)
+        lens = [min(self.blocklen, n - s0) for s0 in starts]
+        outs = torch.empty((2, max(1, sum(lens))), dtype=torch.float32, device=dev)
+        segs = (L.Audio2Segment * len(starts))()
+        off = 0
+        for i, (s0, ln) in enumerate(zip(starts, lens)):
+            segs[i].left = tl.data_ptr() + 4 * s0
+            segs[i].right = tr.data_ptr() + 4 * s0
+            segs[i].len = ln
+            segs[i].out_left = outs[0].data_ptr() + 4 * off
+            segs[i].out_right = outs[1].data_ptr() + 4 * off
+            off += ln
+        torch.cuda.synchronize(dev)
+        L.check(self._ctx._lib.ldg_audio_phase2(self._ctx.handle, segs, len(starts),
+                                                float(self.SysParams["audio_lfreq"]),
+                                                float(self.SysParams["audio_rfreq"]), 1))
+        h = outs.cpu().numpy()
+        res, off = [], 0
+        for ln in lens:
+            res.append((h[0, off:off + ln], h[1, off:off + ln]))
+            off += ln
+        return res
+
     def runfilter_audio_phase2(self, frame_audio, start):
-        """core.py:884-915."""
-        outputs = []
-        clips = None
-        for acname, cf, ch in (("audio_left", self.SysParams["audio_lfreq"], "left"),
-                               ("audio_right", self.SysParams["audio_rfreq"], "right")):
-            raw = frame_audio[acname][start:start + self.blocklen].copy()
-            raw -= cf
-            if acname == "audio_left":
-                clips = _findpeaks(raw, 500000)
-            for loc in clips:
-                raw[max(0, loc - 8):min(loc + 8, len(raw))] = 0
-            filt = self.audio[ch].audio2_filter
-            if len(raw) < len(filt):
-                a2_in = np.zeros_like(filt)
-                a2_in[:len(raw)] = raw
-            else:
-                a2_in = raw
-            out = np.fft.ifft(np.fft.fft(a2_in) * filt).real[:len(raw)] + cf
-            outputs.append(out)
-        return np.rec.array(outputs, names=["audio_left", "audio_right"])
+        """core.py:884-915 on the GPU (ldg_audio_phase2): one transform of
+        `blocklen` stage-1 samples from `start`."""
+        left = np.asarray(frame_audio["audio_left"])
+        right = np.asarray(frame_audio["audio_right"])
+        (l, r), = self._phase2_segments(left, right, [start])
+        return np.rec.array([l, r], names=["audio_left", "audio_right"])
 
     def audio_phase2(self, field_audio):
-        """core.py:917-950."""
-        out = np.zeros(len(field_audio["audio_left"]), dtype=field_audio.dtype)
-        tmp = self.runfilter_audio_phase2(field_audio, 0)
-        if len(tmp) >= len(out):
-            return tmp[:len(out)]
-        out[:tmp.shape[0]] = tmp
-        end = field_audio.shape[0]
+        """core.py:917-950: every transform of the stitching in one GPU
+        launch, stitched as the reference does (512 samples dropped at each
+        join)."""
+        left = np.asarray(field_audio["audio_left"])
+        right = np.asarray(field_audio["audio_right"])
+        n = len(left)
         askip = 512
         sjump = self.blocklen - askip
-        ostart = tmp.shape[0]
-        for sample in range(sjump, field_audio.shape[0] - sjump, sjump):
-            tmp = self.runfilter_audio_phase2(field_audio, sample)
-            oend = ostart + tmp.shape[0] - askip
-            out[ostart:oend] = tmp[askip:]
-            ostart += tmp.shape[0] - askip
-        tmp = self.runfilter_audio_phase2(field_audio, end - self.blocklen - 1)
-        out[out.shape[0] - (tmp.shape[0] - askip):] = tmp[askip:]
-        return out
+        if n <= self.blocklen:
+            starts = [0]
+        else:
+            starts = [0] + list(range(sjump, n - sjump, sjump)) + [n - self.blocklen - 1]
+        segs = self._phase2_segments(left, right, starts)
+        if len(segs[0][0]) >= n:
+            # one transform: the reference returns its FP64 result as is
+            return np.rec.array([segs[0][0][:n].astype(np.float64), segs[0][1][:n].astype(np.float64)],
+                                names=["audio_left", "audio_right"])
+        out = np.zeros(n, dtype=field_audio.dtype)
+        out["audio_left"][:len(segs[0][0])] = segs[0][0]
+        out["audio_right"][:len(segs[0][1])] = segs[0][1]
+        ostart = len(segs[0][0])
+        for l, r in segs[1:-1]:
+            oend = ostart + len(l) - askip
+            out["audio_left"][ostart:oend] = l[askip:]
+            out["audio_right"][ostart:oend] = r[askip:]
+            ostart += len(l) - askip
+        l, r = segs[-1]
+        out["audio_left"][n - (len(l) - askip):] = l[askip:]
+        out["audio_right"][n - (len(r) - askip):] = r[askip:]
+        return out.view(np.recarray)
 
     # ---- init-time delay calibration (core.py:952-1046), on the GPU
 
@@ -425,11 +455,3 @@ class RFDecode(RFParams):
 
     def close(self):
         self._ctx.close()
-
-
-def _findpeaks(array, low=0):
-    """Indices (minus one) of rising samples above array[-1], after zeroing
-    values below `low` (utils.py:1206-1216)."""
-    a2 = array.copy()
-    a2[a2 < low] = 0
-    return [int(i) - 1 for i in np.where(np.logical_and(a2[:-1] > a2[-1], a2[1:] > a2[:-1]))[0]]

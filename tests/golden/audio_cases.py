@@ -26,3 +26,21 @@ def audio_case_inputs(system, linecount, dtype, alen, glitch, seed, line_period,
     left = lf + rng.integers(-150000, 150000, alen).astype(np.float64)
     right = rf_ + rng.integers(-150000, 150000, alen).astype(np.float64)
     return lineinfo, left.astype(dtype), right.astype(dtype), linelen
+
+
+AUDIO2_CASES = [("short", 28739), ("long", 80000)]
+AUDIO2_STRIDE = 7
+
+
+def audio2_inputs(audio_freqs, seed, n):
+    """Seeded stage-1 audio (tones plus noise around the two carriers, with
+    dropout spikes 2.5 MHz above the left carrier) for audio stage 2."""
+    rng = np.random.default_rng(seed * 1000 + n)
+    t = np.arange(n) / 1.25e6
+    chans = []
+    for cf, f0 in zip(audio_freqs, (1000.0, 440.0)):
+        x = cf + 60e3 * np.sin(2 * np.pi * f0 * t) + rng.normal(0, 2e3, n)
+        chans.append(x.astype(np.float32))
+    for pos in rng.integers(50, n - 50, 6):
+        chans[0][pos:pos + 3] = np.float32(audio_freqs[0] + 2.5e6)
+    return chans

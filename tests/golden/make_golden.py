@@ -12,6 +12,10 @@ by ldgpu.synth, and saves small .npz fixtures:
   tbc_smoothing_<sys>.npz -- the first golden field through the reference's
                         TBC with wow_level_adjust_smoothing = 2 (utils.py:
                         141-149): line locations and the uint16 picture;
+  audio2_<sys>.npz   -- analog audio stage 2 (RFDecode.audio_phase2,
+                        core.py:884-950) on seeded field-length stage-1
+                        audio with spikes (blanked by its peak finder), one
+                        field-length and one longer (several transforms);
   demod_pal_notch.npz -- a PAL block with spurious 8.5 MHz tones through the
                         reference demodblock with PAL_V4300D_NotchFilter on
                         (core.py:774-798): outputs and the zeroed bins;
@@ -426,6 +430,22 @@ def smoothing_fixture(system, seed, smoothing=2.0):
                         dspicture=np.asarray(f.dspicture))
 
 
+def audio2_fixture(system, seed):
+    from audio_cases import AUDIO2_CASES, AUDIO2_STRIDE, audio2_inputs
+    rf = refcore.RFDecode(system=system, decode_analog_audio=44100, decode_digital_audio=False)
+    out = {"seed": np.array(seed)}
+    for tag, n in AUDIO2_CASES:
+        left, right = audio2_inputs((rf.SysParams["audio_lfreq"], rf.SysParams["audio_rfreq"]), seed, n)
+        out[f"{tag}_in_sha256"] = np.array(sha(np.concatenate([left, right])))
+        res = rf.audio_phase2(np.rec.fromarrays([left, right], names=["audio_left", "audio_right"]))
+        for ch in ("left", "right"):
+            v = np.asarray(res["audio_" + ch], dtype=np.float64)
+            out[f"{tag}_{ch}_out"] = v[::AUDIO2_STRIDE]
+            out[f"{tag}_{ch}_sum"] = np.array([np.sum(v), np.sum((v - v.mean()) ** 2)])
+            out[f"{tag}_{ch}_len"] = np.array(len(v))
+    np.savez_compressed(os.path.join(HERE, f"audio2_{system.lower()}.npz"), **out)
+
+
 def lut_fixture():
     lut = np.load(os.path.join(REF, "lddecode", "sinc_lut.npz"))["downscale_sinc_lut"]
     rows = np.concatenate([np.arange(0, 65537, 997), [32767, 32768, 65535, 65536]])
@@ -499,6 +519,10 @@ def main():
         dropout_fixture("NTSC", seed=41)
         dropout_fixture("PAL", seed=42)
         return
+    if sys.argv[1:] == ["audio2"]:
+        audio2_fixture("NTSC", seed=81)
+        audio2_fixture("PAL", seed=82)
+        return
     if sys.argv[1:] == ["smoothing"]:
         smoothing_fixture("NTSC", seed=21)
         smoothing_fixture("PAL", seed=22)
@@ -530,6 +554,8 @@ def main():
     notch_fixture()
     smoothing_fixture("NTSC", seed=21)
     smoothing_fixture("PAL", seed=22)
+    audio2_fixture("NTSC", seed=81)
+    audio2_fixture("PAL", seed=82)
     print("golden fixtures written to", HERE)
 
 

@@ -105,7 +105,7 @@ def test_abi_struct_sizes():
                     ("ldg_lines_args", L.LinesArgs), ("ldg_tbc_field", L.TbcField),
                     ("ldg_demod_args", L.DemodArgs), ("ldg_slice", L.Slice), ("ldg_work_item", L.WorkItem),
                     ("ldg_dropout_field", L.DropoutField), ("ldg_dropout_params", L.DropoutParams),
-                    ("ldg_rftbc_field", L.RfTbcField)]:
+                    ("ldg_rftbc_field", L.RfTbcField), ("ldg_audio2_segment", L.Audio2Segment)]:
         assert h.ldg_abi_sizeof(name.encode()) == ctypes.sizeof(t), name
 
 
