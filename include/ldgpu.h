@@ -118,7 +118,14 @@ typedef struct {
     uint16_t* out_u16;       /* linesout*outwidth uint16 (may be NULL) */
     double wow_smoothing;    /* Field.wow_level_adjust_smoothing: 0 off, else the level-adjust
                                 IIR of utils.py:141-149 with alpha = 1 / (smoothing * outwidth) */
+    int32_t wow_interp;      /* Field.wow_interpolation_method (core.py:2602-2613): 0 or
+                                LDG_WOW_LINEAR, LDG_WOW_QUADRATIC (k = 2, scipy's default
+                                knots), LDG_WOW_CUBIC (k = 3, natural ends); the spline
+                                forms need nlines >= 4 */
+    int32_t pad1;
 } ldg_tbc_field;
+
+enum { LDG_WOW_LINEAR = 1, LDG_WOW_QUADRATIC = 2, LDG_WOW_CUBIC = 3 };
 
 int ldg_abi_version(void);
 const char* ldg_last_error(void);

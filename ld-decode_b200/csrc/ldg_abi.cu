@@ -142,6 +142,74 @@ bool slice_ok(const ldg_slice& s, int n) {
            s.roll >= 0 && s.roll < n;
 }
 
+long long tbc_nwow(const ldg_tbc_field& f) {
+    return (long long)(f.outlinecount + f.lineoffset + 1) * (long long)f.outlinelen;
+}
+
+// Argument checks shared by ldg_tbc_fields and ldg_tbc_fields_async.
+int check_tbc_field(const ldg_tbc_field& f, const std::string& who) {
+    if (!f.buf || !f.linelocs) return fail(LDG_ERR_ARG, who + ": NULL buffer");
+    if (f.nlines < 2 || f.nlines > 513) return fail(LDG_ERR_ARG, who + ": nlines must be in [2, 513]");
+    if (f.outwidth <= 0 || f.linesout <= 0 || f.outlinecount <= 0 || f.lineoffset < 0 || f.buf_len <= 0)
+        return fail(LDG_ERR_ARG, who + ": bad field geometry");
+    if (!(f.inlinelen > 0) || !(f.outlinelen > 0) || !(f.hz_ire != 0))
+        return fail(LDG_ERR_ARG, who + ": bad line length or level");
+    if (f.outlinelen != (double)(int)f.outlinelen) return fail(LDG_ERR_ARG, who + ": outlinelen must be an integer");
+    if (!(f.wow_smoothing >= 0) || !(f.wow_smoothing * f.outwidth >= 1 || f.wow_smoothing == 0))
+        return fail(LDG_ERR_ARG, who + ": wow_smoothing must be 0 or at least 1 / outwidth");
+    if (f.wow_interp < 0 || f.wow_interp > LDG_WOW_CUBIC)
+        return fail(LDG_ERR_ARG, who + ": wow_interp must be 0 or one of LDG_WOW_*");
+    if (f.wow_interp >= LDG_WOW_QUADRATIC) {
+        if (f.nlines < 4) return fail(LDG_ERR_ARG, who + ": quadratic / cubic wow interpolation needs nlines >= 4");
+        const long long last = (long long)f.outwidth * (f.lineoffset + 1) + (long long)f.linesout * f.outwidth;
+        if (last > tbc_nwow(f) || tbc_nwow(f) >= (1ll << 31))
+            return fail(LDG_ERR_ARG, who + ": output pixels beyond the wow array");
+    }
+    return LDG_OK;
+}
+
+// Doubles of spline scratch a field needs: its pieces, median and
+// threshold, and with smoothing the IIR state every 32 output pixels.
+size_t tbc_spline_doubles(const ldg_tbc_field& f) {
+    if (f.wow_interp < LDG_WOW_QUADRATIC) return 0;
+    const size_t nout = (size_t)f.linesout * f.outwidth;
+    return (size_t)ldg::kSplStride * f.nlines + 2 + (f.wow_smoothing > 0 ? (nout + 31) / 32 : 0);
+}
+
+// Device descriptor of one field: geometry, levels and scratch pointers
+// (segment scratch at seg + sego in three arrays of seg_total, spline
+// scratch at spl).
+void fill_tbc_field(const ldg_tbc_field& f, ldg::TbcField& d, double* seg, size_t seg_total, size_t sego,
+                    double* spl, int* status) {
+    d.buf_len = f.buf_len;
+    d.nlines = f.nlines;
+    d.lineoffset = f.lineoffset;
+    d.outwidth = f.outwidth;
+    d.linesout = f.linesout;
+    d.nwow = tbc_nwow(f);
+    d.coord_f32 = f.coord_f32;
+    d.inlinelen = f.inlinelen;
+    d.outscale = f.inlinelen / f.outlinelen;
+    d.inv_inl = 1.0 / f.inlinelen;
+    d.u16_scale = f.out_scale / f.hz_ire;
+    d.u16_offset = f.output_zero - f.vsync_ire * f.out_scale - f.ire0 * d.u16_scale;
+    d.seg_level = seg + sego;
+    d.seg_start = seg + seg_total + sego;
+    d.seg_lo = reinterpret_cast<long long*>(seg + 2 * seg_total + sego);
+    d.smooth_b = f.wow_smoothing > 0 ? 1.0 - 1.0 / (f.wow_smoothing * (double)f.outwidth) : 0.0;
+    d.smooth_a = f.wow_smoothing > 0 ? 1.0 / (f.wow_smoothing * (double)f.outwidth) : 0.0;
+    d.status = status;
+    d.spline_k = f.wow_interp >= LDG_WOW_QUADRATIC ? f.wow_interp : 1;
+    d.npieces = d.spline_k == 3 ? f.nlines - 1 : (d.spline_k == 2 ? f.nlines - 2 : 0);
+    if (d.spline_k >= 2) {
+        d.spl = spl;
+        d.stat = spl + (size_t)ldg::kSplStride * f.nlines;
+        d.ybefore = f.wow_smoothing > 0 ? d.stat + 2 : nullptr;
+    } else {
+        d.spl = d.stat = d.ybefore = nullptr;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -464,29 +532,22 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
     if (nfields == 0) return LDG_OK;
     std::lock_guard<std::mutex> lk(c->mu);
     if (!c->d_lut) return fail(LDG_ERR_STATE, "ldg_tbc_fields: sinc table not set");
-    size_t ll_total = 0, seg_total = 0;
+    size_t ll_total = 0, seg_total = 0, spl_total = 0;
     long long max_nout = 0;
     for (int i = 0; i < nfields; ++i) {
         const ldg_tbc_field& f = fields[i];
-        if (!f.buf || !f.linelocs) return fail(LDG_ERR_ARG, "ldg_tbc_fields: NULL buffer");
-        if (f.nlines < 2 || f.nlines > 513) return fail(LDG_ERR_ARG, "ldg_tbc_fields: nlines must be in [2, 513]");
-        if (f.outwidth <= 0 || f.linesout <= 0 || f.outlinecount <= 0 || f.lineoffset < 0 || f.buf_len <= 0)
-            return fail(LDG_ERR_ARG, "ldg_tbc_fields: bad field geometry");
-        if (!(f.inlinelen > 0) || !(f.outlinelen > 0) || !(f.hz_ire != 0))
-            return fail(LDG_ERR_ARG, "ldg_tbc_fields: bad line length or level");
-        if (f.outlinelen != (double)(int)f.outlinelen)
-            return fail(LDG_ERR_ARG, "ldg_tbc_fields: outlinelen must be an integer");
-        if (!(f.wow_smoothing >= 0) || !(f.wow_smoothing * f.outwidth >= 1 || f.wow_smoothing == 0))
-            return fail(LDG_ERR_ARG, "ldg_tbc_fields: wow_smoothing must be 0 or at least 1 / outwidth");
+        const int rc = check_tbc_field(f, "ldg_tbc_fields");
+        if (rc) return rc;
         ll_total += f.nlines;
         seg_total += f.nlines - 1;
+        spl_total += tbc_spline_doubles(f);
         if ((long long)f.linesout * f.outwidth > max_nout) max_nout = (long long)f.linesout * f.outwidth;
     }
     DeviceGuard g(c->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     int rc = grow((void**)&c->d_ll, &c->ll_cap, ll_total * sizeof(double));
     if (rc) return rc;
-    rc = grow((void**)&c->d_seg, &c->seg_cap, 3 * seg_total * sizeof(double));
+    rc = grow((void**)&c->d_seg, &c->seg_cap, (3 * seg_total + spl_total) * sizeof(double));
     if (rc) return rc;
     if (nfields > c->fields_cap) {
         cudaFree(c->d_fields);
@@ -518,7 +579,8 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         rc = grow((void**)&c->d_stage, &c->stage_bytes, stage);
         if (rc) return rc;
     }
-    size_t llo = 0, sego = 0;
+    size_t llo = 0, sego = 0, splo = 0;
+    bool any_spline = false;
     for (int i = 0; i < nfields; ++i) {
         const ldg_tbc_field& f = fields[i];
         ldg::TbcField& d = h[i];
@@ -527,28 +589,14 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         if (!ll_dev) memcpy(lls.data() + llo, f.linelocs, f.nlines * sizeof(double));
         d.buf = x.buf ? (const float*)(c->d_stage + x.buf_off) : f.buf;
         if (x.buf) LDG_CK(cudaMemcpyAsync((void*)d.buf, f.buf, (size_t)f.buf_len * 4, cudaMemcpyHostToDevice, st));
-        d.buf_len = f.buf_len;
         d.linelocs = ll_dev ? f.linelocs : c->d_ll + llo;
-        d.nlines = f.nlines;
-        d.lineoffset = f.lineoffset;
-        d.outwidth = f.outwidth;
-        d.linesout = f.linesout;
-        d.nwow = (long long)(f.outlinecount + f.lineoffset + 1) * (long long)f.outlinelen;
-        d.coord_f32 = f.coord_f32;
-        d.inlinelen = f.inlinelen;
-        d.outscale = f.inlinelen / f.outlinelen;
-        d.inv_inl = 1.0 / f.inlinelen;
-        d.u16_scale = f.out_scale / f.hz_ire;
-        d.u16_offset = f.output_zero - f.vsync_ire * f.out_scale - f.ire0 * d.u16_scale;
-        d.seg_level = c->d_seg + sego;
-        d.seg_start = c->d_seg + seg_total + sego;
-        d.seg_lo = reinterpret_cast<long long*>(c->d_seg + 2 * seg_total + sego);
-        d.smooth_b = f.wow_smoothing > 0 ? 1.0 - 1.0 / (f.wow_smoothing * (double)f.outwidth) : 0.0;
-        d.status = c->d_status;
+        fill_tbc_field(f, d, c->d_seg, seg_total, sego, c->d_seg + 3 * seg_total + splo, c->d_status);
+        any_spline |= d.spline_k >= 2;
         d.out_f32 = x.f32 ? (float*)(c->d_stage + x.f32_off) : f.out_f32;
         d.out_u16 = x.u16 ? (uint16_t*)(c->d_stage + x.u16_off) : f.out_u16;
         llo += f.nlines;
         sego += f.nlines - 1;
+        splo += tbc_spline_doubles(f);
     }
     // linelocs given in host memory: one copy for all of them (device ones were copied above)
     {
@@ -561,7 +609,7 @@ int ldg_tbc_fields(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfields, voi
         }
     }
     LDG_CK(cudaMemcpyAsync(c->d_fields, h.data(), nfields * sizeof(ldg::TbcField), cudaMemcpyHostToDevice, st));
-    cudaError_t e = ldg::launch_tbc(c->d_fields, nfields, max_nout, c->d_lut, 15.0, st);
+    cudaError_t e = ldg::launch_tbc(c->d_fields, nfields, max_nout, c->d_lut, 15.0, any_spline, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
     if (any_host) {
         for (int i = 0; i < nfields; ++i) {
@@ -589,22 +637,15 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
     if (nfields == 0) return LDG_OK;
     std::lock_guard<std::mutex> lk(c->mu);
     if (!c->d_lut) return fail(LDG_ERR_STATE, "ldg_tbc_fields_async: sinc table not set");
-    size_t seg_total = 0;
+    size_t seg_total = 0, spl_total = 0;
     long long max_nout = 0;
     for (int i = 0; i < nfields; ++i) {
         const ldg_tbc_field& f = fields[i];
-        if (!f.buf || !f.linelocs) return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: NULL buffer");
-        if (f.nlines < 2 || f.nlines > 513) return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: nlines must be in [2, 513]");
-        if (f.outwidth <= 0 || f.linesout <= 0 || f.outlinecount <= 0 || f.lineoffset < 0 || f.buf_len <= 0)
-            return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: bad field geometry");
-        if (!(f.inlinelen > 0) || !(f.outlinelen > 0) || !(f.hz_ire != 0))
-            return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: bad line length or level");
-        if (f.outlinelen != (double)(int)f.outlinelen)
-            return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: outlinelen must be an integer");
-        if (!(f.wow_smoothing >= 0) || !(f.wow_smoothing * f.outwidth >= 1 || f.wow_smoothing == 0))
-            return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: wow_smoothing must be 0 or at least 1 / outwidth");
+        const int rc = check_tbc_field(f, "ldg_tbc_fields_async");
+        if (rc) return rc;
         if (!f.out_f32 && !f.out_u16) return fail(LDG_ERR_ARG, "ldg_tbc_fields_async: no output");
         seg_total += f.nlines - 1;
+        spl_total += tbc_spline_doubles(f);
         if ((long long)f.linesout * f.outwidth > max_nout) max_nout = (long long)f.linesout * f.outwidth;
     }
     DeviceGuard g(c->device);
@@ -629,34 +670,21 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
         LDG_CK(cudaMallocHost(&w.h_fields, nfields * sizeof(ldg::TbcField)));
         w.cap = nfields;
     }
-    int rc = grow((void**)&w.d_seg, &w.seg_cap, 3 * seg_total * sizeof(double));
+    int rc = grow((void**)&w.d_seg, &w.seg_cap, (3 * seg_total + spl_total) * sizeof(double));
     if (rc) return rc;
-    size_t sego = 0;
+    size_t sego = 0, splo = 0;
+    bool any_spline = false;
     for (int i = 0; i < nfields; ++i) {
         const ldg_tbc_field& f = fields[i];
         ldg::TbcField& d = w.h_fields[i];
         d.buf = f.buf;
-        d.buf_len = f.buf_len;
         d.linelocs = f.linelocs;
-        d.nlines = f.nlines;
-        d.lineoffset = f.lineoffset;
-        d.outwidth = f.outwidth;
-        d.linesout = f.linesout;
-        d.nwow = (long long)(f.outlinecount + f.lineoffset + 1) * (long long)f.outlinelen;
-        d.coord_f32 = f.coord_f32;
-        d.inlinelen = f.inlinelen;
-        d.outscale = f.inlinelen / f.outlinelen;
-        d.inv_inl = 1.0 / f.inlinelen;
-        d.u16_scale = f.out_scale / f.hz_ire;
-        d.u16_offset = f.output_zero - f.vsync_ire * f.out_scale - f.ire0 * d.u16_scale;
-        d.seg_level = w.d_seg + sego;
-        d.seg_start = w.d_seg + seg_total + sego;
-        d.seg_lo = reinterpret_cast<long long*>(w.d_seg + 2 * seg_total + sego);
-        d.smooth_b = f.wow_smoothing > 0 ? 1.0 - 1.0 / (f.wow_smoothing * (double)f.outwidth) : 0.0;
-        d.status = c->d_status;
+        fill_tbc_field(f, d, w.d_seg, seg_total, sego, w.d_seg + 3 * seg_total + splo, c->d_status);
+        any_spline |= d.spline_k >= 2;
         d.out_f32 = f.out_f32;
         d.out_u16 = f.out_u16;
         sego += f.nlines - 1;
+        splo += tbc_spline_doubles(f);
     }
     // descriptors read by SMs from the pinned workspace: a copy-engine transfer
     // would queue behind bulk output copies on the same engines
@@ -666,7 +694,7 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
     } else {
         LDG_CK(cudaMemcpyAsync(w.d_fields, w.h_fields, nfields * sizeof(ldg::TbcField), cudaMemcpyHostToDevice, st));
     }
-    cudaError_t e = ldg::launch_tbc(w.d_fields, nfields, max_nout, c->d_lut, 15.0, st);
+    cudaError_t e = ldg::launch_tbc(w.d_fields, nfields, max_nout, c->d_lut, 15.0, any_spline, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("tbc launch: ") + cudaGetErrorString(e));
     LDG_CK(cudaEventRecord(w.done, st));
     w.used = true;

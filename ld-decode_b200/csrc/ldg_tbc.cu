@@ -8,6 +8,10 @@
 //                      (slopes of the expected->actual line-location spline),
 //                      their pixel-weighted median and 15*MAD outlier rule ->
 //                      one level-adjust factor per segment.
+//   wow_spline_kernel  (quadratic / cubic wow interpolation only) one CTA per
+//                      field: the spline's pieces, the exact median and MAD
+//                      of the per-pixel wow factors by radix selection, and
+//                      with level smoothing the IIR's state every 32 pixels.
 //   tbc_gather_kernel  one thread per output pixels: FP64 spline coordinate,
 //                      optional float32 rounding (the reference's own cast),
 //                      16-tap windowed-sinc gather with linear interpolation
@@ -98,6 +102,7 @@ __device__ double weighted_median(const double* key, const long long* wt, long l
 __global__ void __launch_bounds__(kWowThreads) wow_levels_kernel(const TbcField* fields,
                                                                  double threshold_mult) {
     const TbcField& f = fields[blockIdx.x];
+    if (f.spline_k >= 2) return;  // wow_spline_kernel's field
     __shared__ double key[kWowThreads];
     __shared__ long long wt[kWowThreads];
     __shared__ long long csum[kWowThreads];
@@ -163,6 +168,358 @@ __global__ void __launch_bounds__(kWowThreads) wow_levels_kernel(const TbcField*
     }
 }
 
+
+// ---- quadratic / cubic wow interpolation (core.py:2602-2621) --------------
+//
+// The reference builds scipy's make_interp_spline through the points
+// (i * inlinelen, linelocs[i]): k = 2 with scipy's default knots for even
+// degree (the data points' midpoints, the first and last omitted), k = 3
+// with natural end conditions (knots at the data points, s'' = 0 at both
+// ends).  Here each spline is built directly as piecewise polynomials:
+//   cubic      the classic second-derivative form, one tridiagonal system
+//              for M_1 .. M_{n-2} (M_0 = M_{n-1} = 0);
+//   quadratic  the derivative s' is piecewise linear and continuous over the
+//              breakpoints x_0, (x_j + x_{j+1})/2 for j = 1 .. n-3, x_{n-1};
+//              its values D_0 .. D_{n-2} at the breakpoints solve one
+//              tridiagonal system whose row i states that the integral of s'
+//              over [x_i, x_{i+1}] is y_{i+1} - y_i (the trapezoid rule is
+//              exact for the linear pieces of s').
+// Both systems are diagonally dominant and solved by the Thomas algorithm in
+// FP64.  Outside the data range the first and last pieces extend, as scipy's
+// BSpline extrapolates.
+
+constexpr int kSplThreads = 1024;
+constexpr int kSplMaxLines = 513;
+constexpr int kHistBins = 2048;
+
+// Coordinate and wow factor at x from a field's piece table pc (kSplStride
+// doubles per piece: left edge, anchor, c0..c3; value c0 + c1 t + c2 t^2 +
+// c3 t^3 at t = x - anchor).  The piece is guessed from x / inlinelen (shift
+// 0: cubic pieces start at data points; 0.5: quadratic ones at midpoints)
+// and fixed by exact comparisons with the left edges.  Every operation is
+// an explicitly rounded intrinsic so that the statistics kernel and the
+// gather get the same values.
+__device__ __forceinline__ void spline_eval(const double* pc, int np, double x, double inv_inl, double shift,
+                                            double& coord, double& wow) {
+    int p = (int)floor(__dadd_rn(__dmul_rn(x, inv_inl), -shift));
+    p = min(max(p, 0), np - 1);
+    while (p > 0 && x < pc[p * kSplStride]) --p;
+    while (p + 1 < np && x >= pc[(p + 1) * kSplStride]) ++p;
+    const double* c = pc + p * kSplStride;
+    const double t = __dadd_rn(x, -c[1]);
+    coord = __fma_rn(t, __fma_rn(t, __fma_rn(t, c[5], c[4]), c[3]), c[2]);
+    wow = __fma_rn(t, __fma_rn(t, __dmul_rn(3.0, c[5]), __dmul_rn(2.0, c[4])), c[3]);
+}
+
+// Order-preserving map of a double onto an unsigned 64-bit key.
+__device__ __forceinline__ unsigned long long order_key(double v) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+__device__ __forceinline__ double key_value(unsigned long long k) {
+    const unsigned long long u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)u);
+}
+
+struct SelectShared {
+    unsigned warp_sum[32];
+    unsigned long long prefix;  // key bits fixed so far
+    long long krem;             // wanted rank among the keys that share them
+    long long below;            // keys below that set
+    unsigned eq;                // keys equal to the result (after the last pass)
+    unsigned long long wmin[32];
+};
+
+// k-th smallest (0-based) of key(i), i in [0, n): most-significant-digit
+// radix selection in six passes (digits of 11, 11, 11, 11, 11 and 9 bits)
+// over a shared histogram; the keys are recomputed on every pass.  Lanes
+// with the same digit add once per warp (__match_any_sync), since
+// neighbouring pixels mostly fall into one bin.  On return sh.prefix is the
+// key, sh.below the number of keys below it, sh.eq the number equal to it.
+template <class KeyF>
+__device__ void radix_select(KeyF key, long long n, long long k, unsigned* hist, SelectShared& sh) {
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t == 0) {
+        sh.prefix = 0;
+        sh.krem = k;
+        sh.below = 0;
+        sh.eq = 0;
+    }
+    unsigned long long mask = 0;
+    const long long nround = (n + kSplThreads - 1) / kSplThreads * kSplThreads;
+    for (int pass = 0; pass < 6; ++pass) {
+        const int shift = pass < 5 ? 53 - 11 * pass : 0;
+        const unsigned dmask = pass < 5 ? 0x7ffu : 0x1ffu;
+        for (int b = t; b < kHistBins; b += kSplThreads) hist[b] = 0;
+        __syncthreads();
+        const unsigned long long prefix = sh.prefix;
+        for (long long i = t; i < nround; i += kSplThreads) {
+            unsigned d = 0xffffffffu;
+            if (i < n) {
+                const unsigned long long kk = key(i);
+                if ((kk & mask) == prefix) d = (unsigned)(kk >> shift) & dmask;
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            if (d != 0xffffffffu && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (unsigned)__popc(peers));
+        }
+        __syncthreads();
+        // the bin holding rank krem: block scan over bin pairs
+        const unsigned h0 = hist[2 * t], h1 = hist[2 * t + 1];
+        const unsigned s = h0 + h1;
+        unsigned incl = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) sh.warp_sum[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            unsigned y = sh.warp_sum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned z = __shfl_up_sync(0xffffffffu, y, o);
+                if (lane >= o) y += z;
+            }
+            sh.warp_sum[lane] = y;
+        }
+        __syncthreads();
+        const long long excl = (long long)(incl - s) + (w ? (long long)sh.warp_sum[w - 1] : 0);
+        const long long kr = sh.krem;
+        __syncthreads();
+        if (s > 0 && kr >= excl && kr < excl + s) {
+            const bool first = kr < excl + h0;
+            const long long bel = excl + (first ? 0 : h0);
+            sh.prefix = prefix | ((unsigned long long)(2 * t + (first ? 0 : 1)) << shift);
+            sh.krem = kr - bel;
+            sh.below += bel;
+            sh.eq = first ? h0 : h1;
+        }
+        mask |= (unsigned long long)dmask << shift;
+        __syncthreads();
+    }
+}
+
+// Smallest key(i) above `above` (all ones when there is none).
+template <class KeyF>
+__device__ unsigned long long min_key_above(KeyF key, long long n, unsigned long long above, SelectShared& sh) {
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    unsigned long long m = ~0ull;
+    for (long long i = t; i < n; i += kSplThreads) {
+        const unsigned long long kk = key(i);
+        if (kk > above && kk < m) m = kk;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, m, o);
+        m = y < m ? y : m;
+    }
+    if (lane == 0) sh.wmin[w] = m;
+    __syncthreads();
+    m = sh.wmin[lane];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, m, o);
+        m = y < m ? y : m;
+    }
+    __syncthreads();
+    return m;
+}
+
+// numpy median of key(i), i in [0, n): the middle value, or the mean of the
+// two middle values for even n.
+template <class KeyF>
+__device__ double select_median(KeyF key, long long n, unsigned* hist, SelectShared& sh) {
+    const long long r1 = (n & 1) ? n / 2 : n / 2 - 1;
+    radix_select(key, n, r1, hist, sh);
+    const unsigned long long k1 = sh.prefix;
+    const long long upto = sh.below + sh.eq;  // keys <= k1
+    __syncthreads();
+    const double v1 = key_value(k1);
+    if (n & 1) return v1;
+    const double v2 = upto >= r1 + 2 ? v1 : key_value(min_key_above(key, n, k1, sh));
+    return __dadd_rn(v1, v2) / 2;
+}
+
+// One CTA per spline field.  Thread 0 solves the tridiagonal system, the
+// pieces are built in parallel (shared table and the field's scratch copy),
+// then the median and MAD of the wow factors over the whole wow array [0,
+// nwow) are selected exactly, and with level smoothing the IIR runs as a
+// scan of affine maps over 1024 contiguous chunks (each chunk's map from one
+// pass, the chunks' start values by a block scan, then a second pass that
+// records the level just before every 32nd output pixel for the gather).
+__global__ void __launch_bounds__(kSplThreads) wow_spline_kernel(const TbcField* fields, double threshold_mult) {
+    const TbcField& f = fields[blockIdx.x];
+    if (f.spline_k < 2) return;
+    __shared__ double pc[kSplStride * kSplMaxLines];
+    __shared__ double cp[kSplMaxLines], dp[kSplMaxLines];
+    __shared__ unsigned hist[kHistBins];
+    __shared__ SelectShared sh;
+    __shared__ double wmapA[32], wmapB[32], wy[32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int n = f.nlines;
+    const bool cubic = f.spline_k == 3;
+    if (n < 4 || n > kSplMaxLines) {
+        if (t == 0) f.status[0] = LDG_TBC_BAD_LINES;
+        return;
+    }
+    const double inl = f.inlinelen;
+    const double* y = f.linelocs;
+    auto X = [&](int i) { return (double)i * inl; };
+    // quadratic breakpoints
+    auto BK = [&](int j) {
+        return j == 0 ? X(0) : (j == n - 2 ? X(n - 1) : __dmul_rn(__dadd_rn(X(j), X(j + 1)), 0.5));
+    };
+    if (t == 0) {
+        const int m = n - 2 + (cubic ? 0 : 1);  // unknowns
+        for (int r = 0; r < m; ++r) {
+            double a = 0, b = 0, c = 0, d = 0;
+            if (cubic) {
+                const int i = r + 1;
+                const double h0 = X(i) - X(i - 1), h1 = X(i + 1) - X(i);
+                a = h0;
+                b = 2.0 * (h0 + h1);
+                c = h1;
+                d = 6.0 * ((y[i + 1] - y[i]) / h1 - (y[i] - y[i - 1]) / h0);
+            } else {
+                // integral of s' over [x_r, x_{r+1}], split at breakpoint r when it lies inside
+                auto add = [&](double p, double q, int j, double& cj, double& cj1) {
+                    const double b0 = BK(j), wj = BK(j + 1) - b0;
+                    const double rp = (p - b0) / wj, rq = (q - b0) / wj;
+                    const double hw = (q - p) / 2;
+                    cj += hw * ((1.0 - rp) + (1.0 - rq));
+                    cj1 += hw * (rp + rq);
+                };
+                if (r == 0) {
+                    add(X(0), X(1), 0, b, c);
+                } else if (r == n - 2) {
+                    add(X(n - 2), X(n - 1), n - 3, a, b);
+                } else {
+                    add(X(r), BK(r), r - 1, a, b);
+                    add(BK(r), X(r + 1), r, b, c);
+                }
+                d = y[r + 1] - y[r];
+            }
+            if (r == 0) {
+                cp[0] = c / b;
+                dp[0] = d / b;
+            } else {
+                const double den = b - a * cp[r - 1];
+                cp[r] = c / den;
+                dp[r] = (d - a * dp[r - 1]) / den;
+            }
+        }
+        for (int r = m - 2; r >= 0; --r) dp[r] = dp[r] - cp[r] * dp[r + 1];
+    }
+    __syncthreads();
+    const int np = f.npieces;
+    for (int p = t; p < np; p += kSplThreads) {
+        double e[kSplStride];
+        if (cubic) {
+            auto M = [&](int i) { return (i == 0 || i == n - 1) ? 0.0 : dp[i - 1]; };
+            const double h = X(p + 1) - X(p);
+            const double m0 = M(p), m1 = M(p + 1);
+            e[0] = X(p);
+            e[1] = X(p);
+            e[2] = y[p];
+            e[3] = (y[p + 1] - y[p]) / h - h * (2.0 * m0 + m1) / 6.0;
+            e[4] = m0 / 2.0;
+            e[5] = (m1 - m0) / (6.0 * h);
+        } else {
+            const double left = BK(p), wp = BK(p + 1) - left;
+            const int a = p == 0 ? 0 : (p == n - 3 ? n - 1 : p + 1);
+            const double dd = dp[p + 1] - dp[p];
+            e[0] = left;
+            e[1] = X(a);
+            e[2] = y[a];
+            e[3] = dp[p] + dd * (X(a) - left) / wp;
+            e[4] = dd / (2.0 * wp);
+            e[5] = 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < kSplStride; ++q) {
+            pc[p * kSplStride + q] = e[q];
+            f.spl[p * kSplStride + q] = e[q];
+        }
+    }
+    __syncthreads();
+    const long long L = f.nwow;
+    const double shift = cubic ? 0.0 : 0.5;
+    const double outscale = f.outscale, inv_inl = f.inv_inl;
+    auto wow_at = [&](long long i) {
+        double c, wv;
+        spline_eval(pc, np, __dmul_rn((double)i, outscale), inv_inl, shift, c, wv);
+        return wv;
+    };
+    const double med = select_median([&](long long i) { return order_key(wow_at(i)); }, L, hist, sh);
+    const double mad = select_median([&](long long i) { return order_key(fabs(__dadd_rn(wow_at(i), -med))); },
+                                     L, hist, sh);
+    const double thr = mad > 0 ? threshold_mult * mad : 0.001;
+    if (t == 0) {
+        f.stat[0] = med;
+        f.stat[1] = thr;
+    }
+    if (!(f.smooth_b > 0)) return;
+    auto level_at = [&](long long i) {
+        const double wv = wow_at(i);
+        return fabs(__dadd_rn(wv, -med)) > thr ? med : wv;
+    };
+    // level-adjust IIR (utils.py:141-149): y[0] = la[0], y[i] = a la[i] + b y[i-1]
+    const double a = f.smooth_a, b = f.smooth_b;
+    const long long C = (L + kSplThreads - 1) / kSplThreads;
+    const long long i0 = (long long)t * C, i1 = min(L, i0 + C);
+    double A = 1.0, B = 0.0;  // this chunk as y_out = A y_in + B
+    for (long long i = i0; i < i1; ++i) {
+        const double la = level_at(i);
+        if (i == 0) {
+            A = 0.0;
+            B = la;
+        } else {
+            A = __dmul_rn(b, A);
+            B = __dadd_rn(__dmul_rn(a, la), __dmul_rn(b, B));
+        }
+    }
+    // inclusive scan of the maps over the warp, then over the warps
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double Ap = __shfl_up_sync(0xffffffffu, A, o), Bp = __shfl_up_sync(0xffffffffu, B, o);
+        if (lane >= o) {
+            B = __fma_rn(A, Bp, B);
+            A = __dmul_rn(A, Ap);
+        }
+    }
+    if (lane == 31) {
+        wmapA[w] = A;
+        wmapB[w] = B;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double yy = 0.0;
+        for (int q = 0; q < 32; ++q) {
+            wy[q] = yy;
+            yy = __fma_rn(wmapA[q], yy, wmapB[q]);
+        }
+    }
+    __syncthreads();
+    const double Ae = __shfl_up_sync(0xffffffffu, A, 1), Be = __shfl_up_sync(0xffffffffu, B, 1);
+    double yv = lane == 0 ? wy[w] : __fma_rn(Ae, wy[w], Be);
+    // second pass: record y just before output pixel 32*m (wow index igbase + 32*m)
+    const long long igbase = (long long)f.outwidth * (f.lineoffset + 1);
+    const long long nout = (long long)f.linesout * f.outwidth;
+    const long long nyb = (nout + 31) / 32;
+    long long mq = (i0 + 1 - igbase + 31) / 32;
+    if (i0 + 1 - igbase <= 0) mq = 0;
+    for (long long i = i0; i < i1; ++i) {
+        const double la = level_at(i);
+        yv = i == 0 ? la : __dadd_rn(__dmul_rn(a, la), __dmul_rn(b, yv));
+        if (mq < nyb && i + 1 == igbase + 32 * mq) {
+            f.ybefore[mq] = yv;
+            ++mq;
+        }
+    }
+}
+
 constexpr int kGatherThreads = 256;
 
 // Input coordinate (FP64) of output pixel ig, optionally rounded to float32
@@ -203,8 +560,15 @@ __global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcFie
     const long long i = wbase + lane;
     const int nseg = f.nlines - 1;
     const long long igbase = (long long)f.outwidth * (f.lineoffset + 1);
-    int jj;
-    const double cc = pixel_coord(f, igbase + (i < nout ? i : 0), nseg, jj);
+    int jj = 0;
+    double cc, wv = 0.0;
+    if (f.spline_k >= 2) {
+        const double x = __dmul_rn((double)(igbase + (i < nout ? i : 0)), f.outscale);
+        spline_eval(f.spl, f.npieces, x, f.inv_inl, f.spline_k == 2 ? 0.5 : 0.0, cc, wv);
+        if (f.coord_f32) cc = (double)__double2float_rn(cc);
+    } else {
+        cc = pixel_coord(f, igbase + (i < nout ? i : 0), nseg, jj);
+    }
     const long long ci = (long long)cc;
     const double ph = __dmul_rn(cc - (double)ci, 65536.0);
     const int ps = (int)ph;
@@ -234,11 +598,34 @@ __global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcFie
         part += __shfl_xor_sync(0xffffffffu, part, 4);
         if (k == p) mine = part;
     }
+    double level;
+    if (f.spline_k >= 2) {
+        const double med = f.stat[0];
+        level = fabs(__dadd_rn(wv, -med)) > f.stat[1] ? med : wv;
+        if (f.smooth_b > 0) {
+            // the IIR over this warp's 32 pixels as a scan of affine maps,
+            // started from the level just before the warp's first pixel
+            double A = f.smooth_b, B = __dmul_rn(f.smooth_a, level);
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double Ap = __shfl_up_sync(0xffffffffu, A, o), Bp = __shfl_up_sync(0xffffffffu, B, o);
+                if (lane >= o) {
+                    B = __fma_rn(A, Bp, B);
+                    A = __dmul_rn(A, Ap);
+                }
+            }
+            level = __fma_rn(A, f.ybefore[wbase >> 5], B);
+        }
+    } else {
+        level = 0.0;
+    }
     if (i >= nout) return;
-    double level = f.seg_level[jj];
-    if (f.smooth_b > 0) {
-        const long long ig = igbase + i;  // index into the wow array
-        level = level + (f.seg_start[jj] - level) * pow(f.smooth_b, (double)(ig - f.seg_lo[jj] + 1));
+    if (f.spline_k < 2) {
+        level = f.seg_level[jj];
+        if (f.smooth_b > 0) {
+            const long long ig = igbase + i;  // index into the wow array
+            level = level + (f.seg_start[jj] - level) * pow(f.smooth_b, (double)(ig - f.seg_lo[jj] + 1));
+        }
     }
     const float out = (float)(level * mine);
     if (f.out_f32) f.out_f32[i] = out;
@@ -250,11 +637,16 @@ __global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcFie
 }
 
 cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout, const float* lut,
-                       double threshold_mult, cudaStream_t stream) {
+                       double threshold_mult, bool any_spline, cudaStream_t stream) {
     if (nfields <= 0) return cudaSuccess;
     wow_levels_kernel<<<nfields, kWowThreads, 0, stream>>>(dfields, threshold_mult);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (any_spline) {
+        wow_spline_kernel<<<nfields, kSplThreads, 0, stream>>>(dfields, threshold_mult);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     const long long per_cta = kGatherThreads;
     const unsigned gx = (unsigned)((max_nout + per_cta - 1) / per_cta);
     for (int off = 0; off < nfields; off += 65535) {  // grid.y limit

@@ -29,10 +29,20 @@ struct TbcField {
     int* status;         // LDG_TBC_* bits
     float* out_f32;
     uint16_t* out_u16;
+    // quadratic / cubic wow interpolation (spline_k 2 / 3; 1: the linear
+    // segments above)
+    int spline_k;
+    int npieces;         // polynomial pieces: nlines - 1 (cubic), nlines - 2 (quadratic)
+    double* spl;         // kSplStride doubles per piece: left edge, anchor, c0..c3 (scratch)
+    double* stat;        // median, outlier threshold of the wow factors (scratch)
+    double* ybefore;     // with the IIR: smoothed level just before output pixel 32*m (scratch)
+    double smooth_a;     // alpha of the level-adjust IIR
 };
 
+constexpr int kSplStride = 6;
+
 cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout, const float* lut,
-                       double threshold_mult, cudaStream_t stream);
+                       double threshold_mult, bool any_spline, cudaStream_t stream);
 
 struct RfTbcField {
     const int16_t* in;   // raw samples of the field read (field-local sample 0)

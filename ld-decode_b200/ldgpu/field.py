@@ -17,11 +17,15 @@ from .linelocs import FieldLogic, FieldLogicNTSC, FieldLogicPAL
 
 
 def tbc_descriptor(rf, buf, linelocs, lineoffset, outwidth, linesout, outlinecount, levels,
-                   out_u16=None, out_f32=None, coord_f32=False, buf_len=None, nlines=None, wow_smoothing=0.0):
+                   out_u16=None, out_f32=None, coord_f32=False, buf_len=None, nlines=None, wow_smoothing=0.0,
+                   wow_interpolation_method="linear"):
     """Fill an ldg_tbc_field from numpy arrays or raw device pointers (ints;
     then buf_len / nlines must be given).
 
-    `levels` = (ire0, hz_ire, vsync_ire, out_scale, output_zero)."""
+    `levels` = (ire0, hz_ire, vsync_ire, out_scale, output_zero);
+    `wow_interpolation_method` "linear", "quadratic" or "cubic"."""
+    if wow_interpolation_method not in L.WOW_METHODS:
+        raise ValueError(f"unknown wow_interpolation_method {wow_interpolation_method!r}")
     d = L.TbcField()
     d.buf = buf if isinstance(buf, int) else buf.ctypes.data
     d.buf_len = int(buf_len if buf_len is not None else len(buf))
@@ -38,6 +42,7 @@ def tbc_descriptor(rf, buf, linelocs, lineoffset, outwidth, linesout, outlinecou
     d.out_f32 = None if out_f32 is None else (out_f32 if isinstance(out_f32, int) else out_f32.ctypes.data)
     d.out_u16 = None if out_u16 is None else (out_u16 if isinstance(out_u16, int) else out_u16.ctypes.data)
     d.wow_smoothing = float(wow_smoothing or 0.0)
+    d.wow_interp = L.WOW_METHODS[wow_interpolation_method]
     return d
 
 
@@ -85,12 +90,21 @@ class Field(FieldLogic):
 
     def computewow_scaled(self):
         """Host FP64 restatement of core.py:2591-2623 (the GPU recomputes the
-        same values internally; this is for callers that want the arrays)."""
+        same values internally; this is for callers that want the arrays).
+        The quadratic / cubic forms call scipy's make_interp_spline with the
+        reference's arguments."""
         act = np.asarray(self.linelocs, dtype=np.float64)
         n = len(act)
         exp = np.array([i * self.inlinelen for i in range(n)], dtype=np.float64)
         nout = self.outlinecount * self.outlinelen + (self.lineoffset + 1) * self.outlinelen
         x = np.arange(nout) * (self.inlinelen / self.outlinelen)
+        if self.wow_interpolation_method != "linear":
+            from scipy import interpolate
+            k, bc = {"quadratic": (2, None), "cubic": (3, "natural")}[self.wow_interpolation_method]
+            spl = interpolate.make_interp_spline(exp, act, k=k, bc_type=bc, check_finite=False)
+            self.interpolated_pixel_locs = spl(x)
+            self.wowfactors = spl(x, 1)
+            return self.interpolated_pixel_locs, self.wowfactors
         seg = np.clip(np.searchsorted(exp, x, side="right") - 1, 0, n - 2)
         x0, x1 = exp[seg], exp[seg + 1]
         y0, y1 = act[seg], act[seg + 1]
@@ -109,8 +123,6 @@ class Field(FieldLogic):
             outwidth = self.outlinelen
         if linesout is None:
             linesout = self.outlinecount
-        if self.wow_interpolation_method != "linear":
-            raise NotImplementedError("only linear wow interpolation is available on the GPU path")
         buf = np.ascontiguousarray(self.data["video"][channel], dtype=np.float32)
         ll = np.ascontiguousarray(lineinfo, dtype=np.float64)
         nout = linesout * outwidth
@@ -118,7 +130,8 @@ class Field(FieldLogic):
         pic = np.empty(nout, dtype=np.uint16) if final else None
         desc = tbc_descriptor(self.rf, buf, ll, self.lineoffset, outwidth, linesout, self.outlinecount,
                               self.levels(), out_u16=pic, out_f32=dsout, coord_f32=self.coord_f32,
-                              wow_smoothing=self.wow_level_adjust_smoothing)
+                              wow_smoothing=self.wow_level_adjust_smoothing,
+                              wow_interpolation_method=self.wow_interpolation_method)
         tbc_fields(self.rf, [desc])
 
         dsaudio = None

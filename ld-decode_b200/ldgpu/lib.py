@@ -55,7 +55,12 @@ class TbcField(ctypes.Structure):
         ("ire0", ctypes.c_double), ("hz_ire", ctypes.c_double), ("vsync_ire", ctypes.c_double),
         ("out_scale", ctypes.c_double), ("output_zero", ctypes.c_double),
         ("out_f32", c_p), ("out_u16", c_p), ("wow_smoothing", ctypes.c_double),
+        ("wow_interp", ctypes.c_int32), ("pad1", ctypes.c_int32),
     ]
+
+
+LDG_WOW_LINEAR, LDG_WOW_QUADRATIC, LDG_WOW_CUBIC = 1, 2, 3
+WOW_METHODS = {"linear": LDG_WOW_LINEAR, "quadratic": LDG_WOW_QUADRATIC, "cubic": LDG_WOW_CUBIC}
 
 
 LDG_CHAIN_MAX_LINES = 336

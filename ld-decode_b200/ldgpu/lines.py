@@ -53,7 +53,7 @@ TBC_DTYPE = _dtype_of(L.TbcField, {
     "buf": "u8", "buf_len": "i8", "linelocs": "u8", "nlines": "i4", "lineoffset": "i4", "outwidth": "i4",
     "linesout": "i4", "outlinecount": "i4", "coord_f32": "i4", "inlinelen": "f8", "outlinelen": "f8",
     "ire0": "f8", "hz_ire": "f8", "vsync_ire": "f8", "out_scale": "f8", "output_zero": "f8",
-    "out_f32": "u8", "out_u16": "u8", "wow_smoothing": "f8"})
+    "out_f32": "u8", "out_u16": "u8", "wow_smoothing": "f8", "wow_interp": "i4", "pad1": "i4"})
 
 
 def proclines_for(rf):
@@ -349,11 +349,13 @@ class LocatedFields:
             yield self[k]
 
 
-def tbc_batch(rf, fields, demod_ptr, out_u16_ptr, levels, coord_f32=False, first=0, count=None):
+def tbc_batch(rf, fields, demod_ptr, out_u16_ptr, levels, coord_f32=False, first=0, count=None,
+              wow_interpolation_method="linear", wow_smoothing=0.0):
     """ldg_tbc_field descriptors for LocatedFields (or a list of FieldLines),
     fields [first, first + count): field i is written as uint16
     outlinelen x outlinecount at out_u16_ptr + i * field bytes; built as one
-    numpy record array."""
+    numpy record array.  wow_interpolation_method / wow_smoothing are the
+    Field options of the same names (core.py:1598, 2602-2613)."""
     outw = rf.SysParams["outlinelen"]
     outl = rf.SysParams["frame_lines"] // 2 + 1
     if isinstance(fields, LocatedFields):
@@ -387,6 +389,8 @@ def tbc_batch(rf, fields, demod_ptr, out_u16_ptr, levels, coord_f32=False, first
     d["ire0"], d["hz_ire"], d["vsync_ire"], d["out_scale"], d["output_zero"] = [float(v) for v in levels]
     d["out_u16"] = np.uint64(out_u16_ptr) + np.uint64(2 * outw * outl) * np.arange(first, first + n,
                                                                                    dtype=np.uint64)
+    d["wow_interp"] = L.WOW_METHODS[wow_interpolation_method]
+    d["wow_smoothing"] = float(wow_smoothing or 0.0)
     return (L.TbcField * n).from_buffer_copy(d.tobytes()) if n else (L.TbcField * 0)()
 
 

@@ -3,7 +3,9 @@
 FP64 numpy restatement of the reference's field resampler:
   * Field.computewow_scaled (lddecode/core.py:2591-2623): a linear spline
     through (i * inlinelen, linelocs[i]) evaluated at every output pixel,
-    giving the input coordinate and its derivative (the wow factor);
+    giving the input coordinate and its derivative (the wow factor); the
+    quadratic and cubic (natural) forms call scipy's make_interp_spline
+    with the reference's arguments, as the reference does;
   * scale_field (lddecode/utils.py:127-183): wow level adjustment with the
     median / 15*MAD outlier rule, then a 16-tap windowed-sinc gather with
     linear interpolation between the 65536 LUT phases;
@@ -22,17 +24,24 @@ TAPS = 16
 PHASES = 1 << 16
 
 
-def pixel_coords(linelocs, inlinelen, outlinelen, outlinecount, lineoffset):
+def pixel_coords(linelocs, inlinelen, outlinelen, outlinecount, lineoffset, method="linear"):
     """Input coordinate and wow (d coord / d x) of every output pixel,
     x = i * inlinelen/outlinelen for i in [0, (outlinecount+lineoffset+1) *
-    outlinelen) (core.py:2595-2621).  Pixel x uses the spline segment j with
-    j*inlinelen <= x < (j+1)*inlinelen, clamped to the first/last segment,
-    which is how a degree-1 B-spline picks its interval."""
+    outlinelen) (core.py:2595-2621).  Linear: pixel x uses the spline
+    segment j with j*inlinelen <= x < (j+1)*inlinelen, clamped to the
+    first/last segment, which is how a degree-1 B-spline picks its interval.
+    Quadratic / cubic: core.py:2605-2613 (k = 2 with scipy's default knots,
+    k = 3 with natural end conditions)."""
     act = np.asarray(linelocs, dtype=np.float64)
     n = len(act)
     exp = np.array([i * inlinelen for i in range(n)], dtype=np.float64)
     nout = outlinecount * outlinelen + (lineoffset + 1) * outlinelen
     x = np.arange(nout) * (inlinelen / outlinelen)
+    if method != "linear":
+        from scipy import interpolate
+        k, bc = {"quadratic": (2, None), "cubic": (3, "natural")}[method]
+        spl = interpolate.make_interp_spline(exp, act, k=k, bc_type=bc, check_finite=False)
+        return spl(x), spl(x, 1)
     seg = np.searchsorted(exp, x, side="right") - 1
     seg = np.clip(seg, 0, n - 2)
     x0, x1 = exp[seg], exp[seg + 1]

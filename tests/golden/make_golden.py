@@ -12,6 +12,13 @@ by ldgpu.synth, and saves small .npz fixtures:
   tbc_smoothing_<sys>.npz -- the first golden field through the reference's
                         TBC with wow_level_adjust_smoothing = 2 (utils.py:
                         141-149): line locations and the uint16 picture;
+  wow_interp_<sys>.npz -- the first golden field through the reference's
+                        TBC with wow_interpolation_method quadratic / cubic
+                        (core.py:2591-2623), on its own line locations and on
+                        line locations with added sinusoidal wow and two
+                        displaced lines (with and without level smoothing):
+                        coordinates, wow factors, their median / MAD and
+                        every PIC_STRIDE-th sample of the uint16 picture;
   audio2_<sys>.npz   -- analog audio stage 2 (RFDecode.audio_phase2,
                         core.py:884-950) on seeded field-length stage-1
                         audio with spikes (blanked by its peak finder), one
@@ -430,6 +437,66 @@ def smoothing_fixture(system, seed, smoothing=2.0):
                         dspicture=np.asarray(f.dspicture))
 
 
+PIC_STRIDE = 11
+# (method, perturbed line locations, level smoothing)
+WOW_CASES = (("cubic", False, 0.0), ("quadratic", True, 0.0), ("cubic", True, 0.0), ("cubic", True, 2.0))
+
+
+def perturb_linelocs(ll, lineoffset):
+    """Sinusoidal wow of 0.8 samples (period 37 lines) plus two lines moved
+    by +4 / -5 samples (H-sync errors that the 15*MAD rule catches)."""
+    ll = np.asarray(ll, dtype=np.float64)
+    out = ll + 0.8 * np.sin(2 * np.pi * np.arange(len(ll)) / 37.0)
+    out[lineoffset + 60] += 4.0
+    out[lineoffset + 140] -= 5.0
+    return out
+
+
+def wow_interp_fixture(system, seed):
+    kw = dict(system=system, decode_analog_audio=0, decode_digital_audio=False)
+    rf = refcore.RFDecode(**kw)
+    src = BlockSource(rf, None, 1)
+    fieldcls = refcore.FieldPAL if system == "PAL" else refcore.FieldNTSC
+    src.readlen = rf.linelen * 400 if system == "PAL" else ((rf.linelen * 350) // 16384) * 16384
+    fieldlen = int(rf.freq_hz / (rf.SysParams["FPS"] * 2))
+    ncap = 2 * fieldlen + src.readlen + 8 * rf.blocklen
+    cap = synth_capture(system, ncap, seed=seed, start=CAPTURE_START).numpy()
+    src.cap = cap
+    start = 0
+    while True:
+        decode, readloc = src.read_field(start)
+        f = fieldcls(rf, decode, prevfield=None, initphase=True, fields_written=0, readloc=decode["startloc"])
+        f.process()
+        if f.valid:
+            break
+        start += f.nextfieldoffset
+    base = np.array(f.linelocs, dtype=np.float64)
+    out = dict(capture_sha256=np.array(sha(cap)), capture_len=np.array(ncap), capture_seed=np.array(seed),
+               capture_start=np.array(CAPTURE_START), mtf_level=np.array(1.0), start=np.array(start),
+               startloc=np.array(decode["startloc"]), pic_stride=np.array(PIC_STRIDE),
+               flags=np.array([int(f.isFirstField), f.linecount, f.lineoffset], dtype=np.int64),
+               levels=np.array([rf.DecoderParams["ire0"], rf.DecoderParams["hz_ire"],
+                                rf.DecoderParams["vsync_ire"], f.out_scale, rf.SysParams["outputZero"]]))
+    for i, (method, perturbed, smoothing) in enumerate(WOW_CASES):
+        ll = perturb_linelocs(base, f.lineoffset) if perturbed else base.copy()
+        f.linelocs = ll
+        f.wow_interpolation_method = method
+        f.wow_level_adjust_smoothing = smoothing
+        f.downscale(linesout=f.outlinecount, final=True)
+        wow = f.wowfactors
+        med = np.median(wow)
+        p = f"c{i}_"
+        out[p + "case"] = np.array([method, str(perturbed), str(smoothing)])
+        out[p + "smoothing"] = np.array(smoothing)
+        out[p + "linelocs"] = ll
+        out[p + "coords"] = f.interpolated_pixel_locs[::COORD_STRIDE]
+        out[p + "wow"] = wow[::COORD_STRIDE]
+        out[p + "wow_stats"] = np.array([len(wow), med, np.median(np.abs(wow - med))])
+        out[p + "picture"] = np.asarray(f.dspicture)[::PIC_STRIDE]
+        out[p + "picture_sha256"] = np.array(sha(np.asarray(f.dspicture)))
+    np.savez_compressed(os.path.join(HERE, f"wow_interp_{system.lower()}.npz"), **out)
+
+
 def audio2_fixture(system, seed):
     from audio_cases import AUDIO2_CASES, AUDIO2_STRIDE, audio2_inputs
     rf = refcore.RFDecode(system=system, decode_analog_audio=44100, decode_digital_audio=False)
@@ -527,6 +594,10 @@ def main():
         smoothing_fixture("NTSC", seed=21)
         smoothing_fixture("PAL", seed=22)
         return
+    if sys.argv[1:] == ["wow"]:
+        wow_interp_fixture("NTSC", seed=21)
+        wow_interp_fixture("PAL", seed=22)
+        return
     if sys.argv[1:] == ["notch"]:
         notch_fixture()
         return
@@ -556,6 +627,8 @@ def main():
     smoothing_fixture("PAL", seed=22)
     audio2_fixture("NTSC", seed=81)
     audio2_fixture("PAL", seed=82)
+    wow_interp_fixture("NTSC", seed=21)
+    wow_interp_fixture("PAL", seed=22)
     print("golden fixtures written to", HERE)
 
 

@@ -166,3 +166,84 @@ def test_tbc_level_smoothing(cuda_ok, system):
             print(system, "smoothing, fp64 vs oracle: max", d.max(), "within 1", np.mean(d <= 1))
             assert np.mean(d <= 1) >= 0.9999 and d.max() <= 2
     rf.close()
+
+
+@pytest.mark.parametrize("system", ["NTSC", "PAL"])
+def test_tbc_wow_interpolation(cuda_ok, system):
+    """wow_interpolation_method quadratic / cubic (core.py:2602-2613), with
+    and without level smoothing, on the reference's line locations and on
+    line locations with added wow and two displaced lines: the GPU picture
+    against the reference's (compat mode, every pic_stride-th sample) and
+    against the FP64 oracle with the same spline (FP64 coordinates); a batch
+    mixing spline and linear fields through the asynchronous entry point
+    gives each field's single-call picture."""
+    import torch
+    from ldgpu import RFDecode
+    from ldgpu.field import FieldNTSC, FieldPAL, tbc_descriptor, tbc_fields, tbc_status
+    from ldgpu.fieldread import field_window
+    from ldgpu.synth import synth_capture
+    g = golden("wow_interp_" + system.lower())
+    rf = RFDecode(system=system)
+    cap = synth_capture(system, int(g["capture_len"]), seed=int(g["capture_seed"]),
+                        start=int(g["capture_start"])).numpy()
+    w = field_window(rf, float(g["start"]))
+    buf = oracle_capture(rf, cap, w.first_block, w.nblocks, rf.scaled_mtf(float(g["mtf_level"])))["demod"]
+    isfirst, linecount, lineoffset = (int(v) for v in g["flags"])
+    levels = g["levels"]
+    ire0, hz_ire, vsync_ire, out_scale, ozero = levels
+    stride = int(g["pic_stride"])
+    cls = FieldPAL if system == "PAL" else FieldNTSC
+    outw = rf.SysParams["outlinelen"]
+    outlines = rf.SysParams["frame_lines"] // 2 + 1
+    singles = {}
+    for i in range(4):
+        p = f"c{i}_"
+        method, smoothing = str(g[p + "case"][0]), float(g[p + "smoothing"])
+        ll = g[p + "linelocs"]
+        coords, wow = otbc.pixel_coords(ll, rf.linelen, outw, outlines, lineoffset, method=method)
+        for coord_f32 in (True, False):
+            f = cls(rf, {"video": {"demod": buf}, "startloc": int(g["startloc"])},
+                    wow_level_adjust_smoothing=smoothing, wow_interpolation_method=method)
+            f.linelocs = ll
+            f.lineoffset, f.linecount, f.isFirstField = lineoffset, linecount, bool(isfirst)
+            f.coord_f32 = coord_f32
+            f.out_scale = out_scale
+            pic, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+            if coord_f32:
+                d = np.abs(pic[::stride].astype(int) - g[p + "picture"].astype(int))
+                print(system, method, smoothing, "compat vs reference: max", d.max(), "exact", np.mean(d == 0))
+                assert d.max() <= 1 and np.mean(d == 0) >= 0.99
+            else:
+                singles[i] = pic
+                ds = otbc.scale_field(buf, coords, wow, rf.downscale_sinc_lut, lineoffset, outw, outlines * outw,
+                                      smoothing=smoothing)
+                opic = otbc.hz_to_output(ds, ire0, hz_ire, ozero, vsync_ire, out_scale)
+                d = np.abs(pic.astype(int) - opic.astype(int))
+                print(system, method, smoothing, "fp64 vs oracle: max", d.max(), "within 1", np.mean(d <= 1))
+                assert np.mean(d <= 1) >= 0.9999 and d.max() <= 2
+    # one asynchronous batch: the four spline cases and a linear field
+    nout = outlines * outw
+    dbuf = torch.from_numpy(np.ascontiguousarray(buf, np.float32)).cuda()
+    dll = [torch.from_numpy(np.ascontiguousarray(g[f"c{i}_linelocs"])).cuda() for i in range(4)]
+    dll.append(dll[2])
+    meths = [str(g[f"c{i}_case"][0]) for i in range(4)] + ["linear"]
+    smooth = [float(g[f"c{i}_smoothing"]) for i in range(4)] + [2.0]
+    out = torch.zeros(5 * nout, dtype=torch.int16, device="cuda")
+    descs = [tbc_descriptor(rf, dbuf.data_ptr(), dll[k].data_ptr(), lineoffset, outw, outlines, outlines,
+                            levels, out_u16=out.data_ptr() + 2 * k * nout, buf_len=len(buf), nlines=len(dll[k]),
+                            wow_smoothing=smooth[k], wow_interpolation_method=meths[k]) for k in range(5)]
+    torch.cuda.synchronize()
+    tbc_fields(rf, descs, asynchronous=True)
+    torch.cuda.synchronize()
+    tbc_status(rf)
+    got = out.cpu().numpy().view(np.uint16).reshape(5, nout)
+    for k in range(4):
+        assert np.array_equal(got[k], singles[k]), k
+    f = cls(rf, {"video": {"demod": buf}, "startloc": int(g["startloc"])}, wow_level_adjust_smoothing=2.0)
+    f.linelocs = g["c2_linelocs"]
+    f.lineoffset, f.linecount, f.isFirstField = lineoffset, linecount, bool(isfirst)
+    f.out_scale = out_scale
+    lin, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+    assert np.array_equal(got[4], lin)
+    assert not np.array_equal(lin, singles[3])
+    rf.close()

@@ -153,3 +153,46 @@ def test_oracle_tbc_smoothing_matches_reference(system):
                            coord_f32=True)
     pic0 = otbc.hz_to_output(ds0, ire0, hz_ire, ozero, vsync_ire, out_scale)
     assert np.abs(pic0.astype(int) - g["dspicture"].astype(int)).max() > 1
+
+
+@pytest.mark.parametrize("system", ["NTSC", "PAL"])
+def test_oracle_wow_interpolation_matches_reference(system):
+    """wow_interpolation_method quadratic / cubic (core.py:2602-2613) on the
+    reference's line locations and on line locations with added wow and two
+    displaced lines, with and without level smoothing: the oracle's
+    coordinates, wow factors, their median / MAD and the picture (compat
+    mode, every pic_stride-th sample) against the reference's."""
+    g = golden("wow_interp_" + system.lower())
+    rf = RFParams(system=system)
+    cap = synth_capture(system, int(g["capture_len"]), seed=int(g["capture_seed"]),
+                        start=int(g["capture_start"])).numpy()
+    outw = rf.SysParams["outlinelen"]
+    outlines = rf.SysParams["frame_lines"] // 2 + 1
+    w = field_window(rf, float(g["start"]))
+    assert w.startloc == int(g["startloc"])
+    buf = field_demod_oracle(rf, cap, w, rf.scaled_mtf(float(g["mtf_level"])))["demod"]
+    lineoffset = int(g["flags"][2])
+    ire0, hz_ire, vsync_ire, out_scale, ozero = g["levels"]
+    stride = int(g["pic_stride"])
+    ncase = len([k for k in g.files if k.endswith("_case")])
+    assert ncase == 4
+    for i in range(ncase):
+        p = f"c{i}_"
+        method = str(g[p + "case"][0])
+        coords, wow = otbc.pixel_coords(g[p + "linelocs"], rf.linelen, outw, outlines, lineoffset, method=method)
+        np.testing.assert_allclose(coords[::101], g[p + "coords"], rtol=0, atol=1e-9)
+        np.testing.assert_allclose(wow[::101], g[p + "wow"], rtol=1e-13)
+        n, med, mad = g[p + "wow_stats"]
+        assert len(wow) == int(n) and np.median(wow) == med
+        assert np.median(np.abs(wow - med)) == mad
+        ds = otbc.scale_field(buf, coords, wow, rf.downscale_sinc_lut, lineoffset, outw, outlines * outw,
+                              coord_f32=True, smoothing=float(g[p + "smoothing"]))
+        pic = otbc.hz_to_output(ds, ire0, hz_ire, ozero, vsync_ire, out_scale)[::stride]
+        d = np.abs(pic.astype(int) - g[p + "picture"].astype(int))
+        assert d.max() <= 1 and np.mean(d == 0) > 0.99, (i, d.max(), np.mean(d == 0))
+    # the spline forms differ from the linear one (and the displaced lines trip the 15*MAD rule)
+    c_lin, w_lin = otbc.pixel_coords(g["c2_linelocs"], rf.linelen, outw, outlines, lineoffset)
+    c_cub, w_cub = otbc.pixel_coords(g["c2_linelocs"], rf.linelen, outw, outlines, lineoffset, method="cubic")
+    assert np.abs(c_lin - c_cub).max() > 0.05
+    med = np.median(w_cub)
+    assert np.any(np.abs(w_cub - med) > 15 * np.median(np.abs(w_cub - med)))
