@@ -103,7 +103,7 @@ typedef struct {
 /* One field for the time-base corrector. */
 typedef struct {
     const float* buf;        /* field demod samples (field-local index 0) */
-    int64_t buf_len;
+    int64_t buf_len;         /* < 2^31 */
     const double* linelocs;  /* FP64 line locations, field-local samples */
     int32_t nlines;          /* len(linelocs), <= 513 */
     int32_t lineoffset;      /* Field.lineoffset */

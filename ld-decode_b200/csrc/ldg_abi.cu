@@ -150,7 +150,8 @@ long long tbc_nwow(const ldg_tbc_field& f) {
 int check_tbc_field(const ldg_tbc_field& f, const std::string& who) {
     if (!f.buf || !f.linelocs) return fail(LDG_ERR_ARG, who + ": NULL buffer");
     if (f.nlines < 2 || f.nlines > 513) return fail(LDG_ERR_ARG, who + ": nlines must be in [2, 513]");
-    if (f.outwidth <= 0 || f.linesout <= 0 || f.outlinecount <= 0 || f.lineoffset < 0 || f.buf_len <= 0)
+    if (f.outwidth <= 0 || f.linesout <= 0 || f.outlinecount <= 0 || f.lineoffset < 0 || f.buf_len <= 0 ||
+        f.buf_len >= (1ll << 31))
         return fail(LDG_ERR_ARG, who + ": bad field geometry");
     if (!(f.inlinelen > 0) || !(f.outlinelen > 0) || !(f.hz_ire != 0))
         return fail(LDG_ERR_ARG, who + ": bad line length or level");
@@ -356,10 +357,26 @@ int ldg_set_sinc_lut(ldg_ctx* c, const float* lut, int32_t rows, int32_t taps) {
     if (rows != 65537 || taps != 16) return fail(LDG_ERR_UNSUPPORTED, "ldg_set_sinc_lut: table must be 65537 x 16");
     std::lock_guard<std::mutex> lk(c->mu);
     DeviceGuard g(c->device);
-    const size_t bytes = (size_t)rows * taps * sizeof(float);
+    // device layout for the gather: per phase p < 65536 and tap pair k < 8
+    // one float4 (w[p][2k], w[p][2k+1], w[p+1][2k] - w[p][2k],
+    // w[p+1][2k+1] - w[p][2k+1]), the differences rounded to float32 as the
+    // kernel's own subtraction would be; one 16-byte load per lane and pixel
+    std::vector<float> h((size_t)ldg::kLutPhases * 32);
+    for (int ph = 0; ph < ldg::kLutPhases; ++ph) {
+        const float* a = lut + (size_t)ph * 16;
+        const float* b = a + 16;
+        float* o = h.data() + (size_t)ph * 32;
+        for (int k = 0; k < 8; ++k) {
+            o[4 * k + 0] = a[2 * k];
+            o[4 * k + 1] = a[2 * k + 1];
+            o[4 * k + 2] = b[2 * k] - a[2 * k];
+            o[4 * k + 3] = b[2 * k + 1] - a[2 * k + 1];
+        }
+    }
+    const size_t bytes = h.size() * sizeof(float);
     if (!c->d_lut) LDG_CK(cudaMalloc(&c->d_lut, bytes));
     LDG_CK(cudaStreamSynchronize(c->stream));
-    LDG_CK(cudaMemcpy(c->d_lut, lut, bytes, cudaMemcpyHostToDevice));
+    LDG_CK(cudaMemcpy(c->d_lut, h.data(), bytes, cudaMemcpyHostToDevice));
     return LDG_OK;
 }
 

@@ -545,9 +545,10 @@ __device__ __forceinline__ double pixel_coord(const TbcField& f, long long ig, i
 // One warp per 32 consecutive output pixels of one field; blockIdx.y is the
 // field.  Each lane computes its own pixel's FP64 coordinate; then groups of
 // 8 lanes gather one pixel at a time: lane k of a group reads taps 2k, 2k+1
-// of the input and of the two LUT rows, so a pixel's 64-byte input span and
-// its two 64-byte LUT rows are each one contiguous access (instead of 16
-// scattered ones per lane); the 8 partial sums meet by shuffles.
+// of the input and one float4 of the interleaved LUT (the two taps of phase
+// ps and their differences to phase ps + 1), so a pixel's 64-byte input
+// span and its 128 bytes of LUT are each one contiguous access; the 8
+// partial sums meet in a transposing reduction (lane k ends with pixel k).
 __global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcField* fields, const float* lut,
                                                                     int nfields) {
     const int fi = blockIdx.y;
@@ -576,28 +577,42 @@ __global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcFie
     const long long st = ci - 7;
     const bool ok = i < nout && st >= 0 && st + 16 <= f.buf_len && ps >= 0 && ps < 65536;
     if (i < nout && !ok && f.status) atomicOr(f.status, LDG_TBC_OUT_OF_RANGE);
-    double mine = 0.0;
-#pragma unroll 2
+    // first tap as a 32-bit offset (buf_len < 2^31); phase -1 marks a pixel left at 0
+    const int sti = ok ? (int)st : 0;
+    const int psi = ok ? ps : -1;
+    double acc[8];  // this lane's two-tap share of each of the group's 8 pixels
+#pragma unroll
     for (int p = 0; p < 8; ++p) {
         const int src = grp * 8 + p;  // the group's p-th pixel
-        const long long pst = __shfl_sync(0xffffffffu, st, src);
-        const int pps = __shfl_sync(0xffffffffu, ps, src);
+        const int pst = __shfl_sync(0xffffffffu, sti, src);
+        const int pps = __shfl_sync(0xffffffffu, psi, src);
         const float pal = __shfl_sync(0xffffffffu, alpha, src);
-        const bool pok = __shfl_sync(0xffffffffu, ok, src);
         double part = 0.0;
-        if (pok) {
-            const float2 a = __ldg(reinterpret_cast<const float2*>(lut + (size_t)pps * 16) + k);
-            const float2 b = __ldg(reinterpret_cast<const float2*>(lut + (size_t)(pps + 1) * 16) + k);
+        if (pps >= 0) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(lut + (size_t)pps * 32) + k);
             const float* in = f.buf + pst + 2 * k;
             const float x0 = __ldg(in), x1 = __ldg(in + 1);
-            const float w0 = fmaf(pal, b.x - a.x, a.x), w1 = fmaf(pal, b.y - a.y, a.y);
+            const float w0 = fmaf(pal, q.z, q.x), w1 = fmaf(pal, q.w, q.y);
             part = (double)(x0 * w0) + (double)(x1 * w1);
         }
-        part += __shfl_xor_sync(0xffffffffu, part, 1);
-        part += __shfl_xor_sync(0xffffffffu, part, 2);
-        part += __shfl_xor_sync(0xffffffffu, part, 4);
-        if (k == p) mine = part;
+        acc[p] = part;
     }
+    // transposing reduction over the group's 8 lanes: at each step a lane
+    // keeps half of its pixels and adds the partner's shares of them, so lane
+    // k ends with the whole sum for pixel k (its own)
+    double b4[4], b2[2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const bool hi = (k & 4) != 0;
+        b4[j] = (hi ? acc[j + 4] : acc[j]) + __shfl_xor_sync(0xffffffffu, hi ? acc[j] : acc[j + 4], 4);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const bool hi = (k & 2) != 0;
+        b2[j] = (hi ? b4[j + 2] : b4[j]) + __shfl_xor_sync(0xffffffffu, hi ? b4[j] : b4[j + 2], 2);
+    }
+    const bool hi1 = (k & 1) != 0;
+    const double mine = (hi1 ? b2[1] : b2[0]) + __shfl_xor_sync(0xffffffffu, hi1 ? b2[0] : b2[1], 1);
     double level;
     if (f.spline_k >= 2) {
         const double med = f.stat[0];

@@ -40,7 +40,10 @@ struct TbcField {
 };
 
 constexpr int kSplStride = 6;
+constexpr int kLutPhases = 65536;  // sinc table phases (rows 0..65536, the last a copy)
 
+// lut: the sinc table interleaved for the gather (kLutPhases x 8 float4:
+// two taps of phase p and their differences to phase p + 1).
 cudaError_t launch_tbc(const TbcField* dfields, int nfields, long long max_nout, const float* lut,
                        double threshold_mult, bool any_spline, cudaStream_t stream);
 
