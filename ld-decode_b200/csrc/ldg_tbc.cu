@@ -233,10 +233,12 @@ struct SelectShared {
 
 // k-th smallest (0-based) of key(i), i in [0, n): most-significant-digit
 // radix selection in six passes (digits of 11, 11, 11, 11, 11 and 9 bits)
-// over a shared histogram; the keys are recomputed on every pass.  Lanes
-// with the same digit add once per warp (__match_any_sync), since
-// neighbouring pixels mostly fall into one bin.  On return sh.prefix is the
-// key, sh.below the number of keys below it, sh.eq the number equal to it.
+// over a shared histogram; the keys are recomputed on every pass.  Each
+// thread walks its own contiguous chunk of pixels and adds runs of equal
+// digits at once; the 32 lanes of a warp look at pixels ~n/1024 apart,
+// whose digits mostly differ where the runs are short.  On
+// return sh.prefix is the key, sh.below the number of keys below it, sh.eq
+// the number equal to it.
 template <class KeyF>
 __device__ void radix_select(KeyF key, long long n, long long k, unsigned* hist, SelectShared& sh) {
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -247,22 +249,29 @@ __device__ void radix_select(KeyF key, long long n, long long k, unsigned* hist,
         sh.eq = 0;
     }
     unsigned long long mask = 0;
-    const long long nround = (n + kSplThreads - 1) / kSplThreads * kSplThreads;
+    const long long chunk = (n + kSplThreads - 1) / kSplThreads;
+    const long long i0 = (long long)t * chunk, i1 = min(n, i0 + chunk);
     for (int pass = 0; pass < 6; ++pass) {
         const int shift = pass < 5 ? 53 - 11 * pass : 0;
         const unsigned dmask = pass < 5 ? 0x7ffu : 0x1ffu;
         for (int b = t; b < kHistBins; b += kSplThreads) hist[b] = 0;
         __syncthreads();
         const unsigned long long prefix = sh.prefix;
-        for (long long i = t; i < nround; i += kSplThreads) {
-            unsigned d = 0xffffffffu;
-            if (i < n) {
-                const unsigned long long kk = key(i);
-                if ((kk & mask) == prefix) d = (unsigned)(kk >> shift) & dmask;
+        // runs of one digit (the rule in the high passes, where a whole
+        // chunk shares its sign and exponent) are counted in a register
+        unsigned run_d = 0xffffffffu, run_n = 0;
+        for (long long i = i0; i < i1; ++i) {
+            const unsigned long long kk = key(i);
+            if ((kk & mask) != prefix) continue;
+            const unsigned d = (unsigned)(kk >> shift) & dmask;
+            if (d != run_d) {
+                if (run_n) atomicAdd(&hist[run_d], run_n);
+                run_d = d;
+                run_n = 0;
             }
-            const unsigned peers = __match_any_sync(0xffffffffu, d);
-            if (d != 0xffffffffu && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (unsigned)__popc(peers));
+            ++run_n;
         }
+        if (run_n) atomicAdd(&hist[run_d], run_n);
         __syncthreads();
         // the bin holding rank krem: block scan over bin pairs
         const unsigned h0 = hist[2 * t], h1 = hist[2 * t + 1];
