@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define LDG_ABI_VERSION 1
+#define LDG_ABI_VERSION 2
 
 #define LDG_OK 0
 #define LDG_ERR_ARG (-1)         /* invalid argument or size */

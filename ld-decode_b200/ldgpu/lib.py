@@ -190,6 +190,16 @@ SIGNATURES = {
     "ldg_ac3_dpll_reclock": (ctypes.c_int, [c_p, c_p, c_p, ctypes.c_int64, c_p, ctypes.POINTER(ctypes.c_int64)]),
 }
 
+# ABI of the library this binding is written for (LDG_ABI_VERSION in
+# include/ldgpu.h) and the structures whose layout it mirrors
+ABI_VERSION = 2
+ABI_STRUCTS = [("ldg_chain_params", ChainParams), ("ldg_chain_state", ChainState),
+               ("ldg_field_plan", FieldPlan), ("ldg_lines_consts", LinesConsts),
+               ("ldg_lines_args", LinesArgs), ("ldg_tbc_field", TbcField),
+               ("ldg_demod_args", DemodArgs), ("ldg_slice", Slice), ("ldg_work_item", WorkItem),
+               ("ldg_dropout_field", DropoutField), ("ldg_dropout_params", DropoutParams),
+               ("ldg_rftbc_field", RfTbcField), ("ldg_audio2_segment", Audio2Segment)]
+
 _lib = None
 _lock = threading.Lock()
 
@@ -217,6 +227,15 @@ def load(path=None):
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
+        # a library built from other sources than this binding would misread
+        # every descriptor: refuse it
+        if lib.ldg_abi_version() != ABI_VERSION:
+            raise ImportError(f"{p}: ABI version {lib.ldg_abi_version()}, this binding needs {ABI_VERSION} "
+                              "(rebuild with python ld-decode_b200/build.py)")
+        for sname, t in ABI_STRUCTS:
+            if lib.ldg_abi_sizeof(sname.encode()) != ctypes.sizeof(t):
+                raise ImportError(f"{p}: {sname} is {lib.ldg_abi_sizeof(sname.encode())} bytes, "
+                                  f"the binding's {ctypes.sizeof(t)} (rebuild the library)")
         _lib = lib
         return lib
 

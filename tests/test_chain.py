@@ -100,12 +100,8 @@ def test_chain_stops_on_level_recalibration():
 
 def test_abi_struct_sizes():
     h = L.load()
-    for name, t in [("ldg_chain_params", L.ChainParams), ("ldg_chain_state", L.ChainState),
-                    ("ldg_field_plan", L.FieldPlan), ("ldg_lines_consts", L.LinesConsts),
-                    ("ldg_lines_args", L.LinesArgs), ("ldg_tbc_field", L.TbcField),
-                    ("ldg_demod_args", L.DemodArgs), ("ldg_slice", L.Slice), ("ldg_work_item", L.WorkItem),
-                    ("ldg_dropout_field", L.DropoutField), ("ldg_dropout_params", L.DropoutParams),
-                    ("ldg_rftbc_field", L.RfTbcField), ("ldg_audio2_segment", L.Audio2Segment)]:
+    assert len(L.ABI_STRUCTS) == 13
+    for name, t in L.ABI_STRUCTS:
         assert h.ldg_abi_sizeof(name.encode()) == ctypes.sizeof(t), name
 
 
