@@ -69,6 +69,10 @@ def parse():
                     help="pipeline chunks of blocks per step (1: demod, then line locations, then TBC)")
     ap.add_argument("--chunk-taper", type=float, default=0.7,
                     help="chunk c gets a share of the blocks proportional to taper**c")
+    ap.add_argument("--wow-interp", default="linear", choices=["linear", "quadratic", "cubic"],
+                    help="Field.wow_interpolation_method of the TBC (the reference's default is linear)")
+    ap.add_argument("--wow-smoothing", type=float, default=0.0,
+                    help="Field.wow_level_adjust_smoothing of the TBC (0: off, the reference's default)")
     ap.add_argument("--mixed", type=int, default=0,
                     help="mixed-batch workload instead: this many captures, lengths uniform in 0.5-8 s, "
                          "half NTSC / half PAL, own seed and SNR (30-45 dB) each")
@@ -161,6 +165,7 @@ def run_gpu(args):
     from ldgpu.field import tbc_fields, tbc_status
     from ldgpu.fieldread import blocks_in_capture
     from ldgpu.lines import LineLocator, field_levels, tbc_batch
+    wow_opts = dict(wow_interpolation_method=args.wow_interp, wow_smoothing=args.wow_smoothing)
     from ldgpu.synth import synth_capture
 
     system = args.system
@@ -279,7 +284,8 @@ def run_gpu(args):
                 lo, hi, ev = loc.ready.pop(0)
                 streamC.wait_event(ev)
                 tbc_fields(rf, tbc_batch(rf, loc.fields, bs.outs["demod"].data_ptr(), bs.pics.data_ptr(), levels,
-                                         first=lo, count=hi - lo), stream=streamC.cuda_stream, asynchronous=True)
+                                         first=lo, count=hi - lo, **wow_opts),
+                           stream=streamC.cuda_stream, asynchronous=True)
                 if io is not None:
                     tev = torch.cuda.Event()
                     tev.record(streamC)
@@ -443,7 +449,7 @@ def run_gpu(args):
             out.append(a.elapsed_time(b))
         return statistics.median(out)
 
-    all_descs = tbc_batch(rf, flist, outs["demod"].data_ptr(), pics.data_ptr(), levels)
+    all_descs = tbc_batch(rf, flist, outs["demod"].data_ptr(), pics.data_ptr(), levels, **wow_opts)
     dmed = timed(demod)
     tbc_med = timed(lambda: tbc_fields(rf, all_descs, stream=sh))
     tbc_ms = [tbc_med]
@@ -475,7 +481,8 @@ def run_gpu(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(rf, cap, fields, U, nblocks, max_blocks=256)
+        cpu = cpu_baseline(rf, cap, fields, U, nblocks, max_blocks=256, method=args.wow_interp,
+                           smoothing=args.wow_smoothing)
 
     res = {
         "metric": METRIC,
@@ -500,6 +507,8 @@ def run_gpu(args):
             "l2": "inputs (800 MB) and outputs (> 8 GB) exceed L2 each step; no flush",
             "parallelism": f"replicas x{world} (one capture per GPU)",
             "mtf_level": 1,
+            "wow_interpolation_method": args.wow_interp,
+            "wow_level_adjust_smoothing": args.wow_smoothing,
         },
         "fields_per_s": world * nf / (ms_per_step * 1e-3),
         "isolated_step_ms": isolated_ms,
@@ -549,7 +558,7 @@ def cpu_demod_sample(rfp, cap, blocks, U, threads):
         return list(ex.map(one, blocks))
 
 
-def cpu_tbc_sample(rfp, outs_by_block, fields, U, first_block):
+def cpu_tbc_sample(rfp, outs_by_block, fields, U, first_block, method="linear", smoothing=0.0):
     from oracle import tbc as otbc
     outw = rfp.SysParams["outlinelen"]
     outlines = rfp.SysParams["frame_lines"] // 2 + 1
@@ -560,14 +569,15 @@ def cpu_tbc_sample(rfp, outs_by_block, fields, U, first_block):
         if lo < 0 or lo + w.length > len(demod):
             continue
         buf = demod[lo:lo + w.length]
-        coords, wow = otbc.pixel_coords(ll, rfp.linelen, outw, outlines, lineoffset)
-        ds = otbc.scale_field(buf, coords, wow, rfp.downscale_sinc_lut, lineoffset, outw, outlines * outw)
+        coords, wow = otbc.pixel_coords(ll, rfp.linelen, outw, outlines, lineoffset, method=method)
+        ds = otbc.scale_field(buf, coords, wow, rfp.downscale_sinc_lut, lineoffset, outw, outlines * outw,
+                              smoothing=smoothing)
         otbc.hz_to_output(ds, levels[0], levels[1], levels[4], levels[2], levels[3])
         n += 1
     return n
 
 
-def cpu_baseline(rf, cap, fields, U, nblocks, max_blocks):
+def cpu_baseline(rf, cap, fields, U, nblocks, max_blocks, method="linear", smoothing=0.0):
     """The CPU oracle on a bounded sample of the workload, all host threads."""
     threads = os.cpu_count() or 1
     hc = cap[: (max_blocks + 1) * U + rf.blocklen].cpu().numpy()
@@ -575,7 +585,7 @@ def cpu_baseline(rf, cap, fields, U, nblocks, max_blocks):
     t0 = time.perf_counter()
     outs = cpu_demod_sample(rf, hc, list(range(nb)), U, threads)
     t1 = time.perf_counter()
-    nft = cpu_tbc_sample(rf, outs, fields, U, 0)
+    nft = cpu_tbc_sample(rf, outs, fields, U, 0, method, smoothing)
     t2 = time.perf_counter()
     return {"value": nb * U / (t2 - t0) / 1e6, "unit": "MSPS", "cores": threads, "kind": "port",
             "sample": f"first {nb} blocks ({nb * U} samples) demod + TBC of the {nft} fields inside them; "
@@ -609,11 +619,11 @@ def run_reference(args):
     fields = _fields_cpu(rf, host, nblk, FieldLogicPAL if args.system == "PAL" else FieldLogicNTSC)
     for _ in range(args.warmup):
         o = cpu_demod_sample(rf, cap, list(range(nblk)), U, threads)
-        cpu_tbc_sample(rf, o, fields, U, 0)
+        cpu_tbc_sample(rf, o, fields, U, 0, args.wow_interp, args.wow_smoothing)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         o = cpu_demod_sample(rf, cap, list(range(nblk)), U, threads)
-        nft = cpu_tbc_sample(rf, o, fields, U, 0)
+        nft = cpu_tbc_sample(rf, o, fields, U, 0, args.wow_interp, args.wow_smoothing)
     dt = (time.perf_counter() - t0) / args.steps
     v = nblk * U / dt / 1e6
     res = {"metric": METRIC, "value": v, "unit": "MSPS", "n_gpus": args.gpus, "steps": args.steps,
@@ -622,7 +632,8 @@ def run_reference(args):
            "impl": "reference",
            "config": {"workload": f"{args.system} capture sample: {nblk} blocks x 32768 (stride {U}), "
                                   f"{nft} fields per step (bounded sample of the {args.seconds:g} s workload)",
-                      "parallelism": f"{threads} host threads"},
+                      "parallelism": f"{threads} host threads", "wow_interpolation_method": args.wow_interp,
+                      "wow_level_adjust_smoothing": args.wow_smoothing},
            "cpu_baseline": {"value": v, "unit": "MSPS", "cores": threads, "kind": "port",
                             "sample": f"{nblk} blocks demod + TBC of {nft} fields per step (their line "
                                       "locations computed once, outside the timed steps)"},
