@@ -164,14 +164,14 @@ __device__ __forceinline__ void post_pair(float2* S, float2* park, const AudioTa
 
 // S holds Z = FFT_M(x[2m] + i x[2m+1]).  Computes X[k] for k = 0..M, parks
 // it, taps the audio sub-bands and, if F is given, leaves the C2R input of
-// X * F in S.  Thread t handles k = t + 1024 i; two bins per step with all
+// X * F in S.  Thread t handles k = t + kThreads i; two bins per step with all
 // their loads issued before the arithmetic (latency of the global twiddle
 // and filter loads overlapped).
 __device__ void post_r2c(float2* S, const Tables& t, float2* park, const float2* F, const AudioTaps* au) {
     const int t0 = threadIdx.x;
     const float2 zero = make_float2(0.f, 0.f);
 #pragma unroll 1
-    for (int i = 0; i < 8; i += 2) {
+    for (int i = 0; i < kM / 2 / kThreads; i += 2) {
         const int ka = t0 + i * kThreads, kb = ka + kThreads;  // kb > 0; ka == 0 only for thread 0
         const float2 zka = S[pad(ka)];
         const float2 zma = ka ? S[pad(kM - ka)] : zero;
@@ -205,7 +205,7 @@ __device__ void post_r2c(float2* S, const Tables& t, float2* park, const float2*
 __device__ void pre_c2r(float2* S, const Tables& t, const float2* park, const float2* F) {
     const int t0 = threadIdx.x;
 #pragma unroll 1
-    for (int i = 0; i < 8; i += 2) {
+    for (int i = 0; i < kM / 2 / kThreads; i += 2) {
         const int ka = t0 + i * kThreads, kb = ka + kThreads;
         const float2 xka = park[ka], xkb = park[kb], xmb = park[kM - kb];
         const float2 xma = ka ? park[kM - ka] : xka;
