@@ -168,3 +168,34 @@ def test_pal_v4300d_notch(cuda_ok):
     np.testing.assert_array_equal(out.cpu().numpy(), gpu["video"]["demod"])
     rf.close()
     plain.close()
+
+
+LOWBAND = {
+    "ntsc_lowband": dict(system="NTSC", decode_analog_audio=44100, decode_digital_audio=True,
+                         extra_options={"lowband": True, "deemp_str": 1.5, "NTSC_ColorNotchFilter": True,
+                                        "MTF_level": 0.7, "MTF_offset": 0.1}),
+    "pal_lowband": dict(system="PAL", decode_analog_audio=44100, decode_digital_audio=True,
+                        extra_options={"lowband": True, "deemp_coeff": (2.0, 7.0)}),
+}
+
+
+@pytest.mark.parametrize("name", list(LOWBAND))
+def test_lowband_filter_banks(cuda_ok, name):
+    """The reference's lowband configurations (core.py:209, 251 filter
+    parameters; NTSC colour notch, MTF level/offset and de-emphasis strength;
+    PAL de-emphasis coefficients) through the GPU demodulator: every output
+    within the demod tolerances of the FP64 oracle with the same filters, on
+    the golden block and on a seeded capture block, at both MTF levels."""
+    from ldgpu import RFDecode
+    from ldgpu.synth import synth_capture
+    kw = LOWBAND[name]
+    r = RFDecode(**kw)
+    try:
+        g = golden("demod_" + kw["system"].lower())
+        cap = synth_capture(kw["system"], 3 * r.blocklen, seed=77).numpy()
+        for block in (g["block"], cap[r.blocklen:2 * r.blocklen]):
+            for mtf in (0, 1):
+                stats = _check_block(r, block, mtf)
+                print(name, "mtf", mtf, {k: (round(a, 2), round(b, 1)) for k, (a, b) in stats.items()})
+    finally:
+        r.close()
