@@ -265,18 +265,27 @@ struct WowWalk {
     }
 };
 
+constexpr int kCollect = kHistBins / 2;  // keys ranked in shared memory (the histogram's space)
+
 struct SelectShared {
     unsigned warp_sum[32];
     unsigned long long prefix;  // key bits fixed so far
     long long krem;             // wanted rank among the keys that share them
     long long below;            // keys below that set
-    unsigned eq;                // keys equal to the result (after the last pass)
+    unsigned eq;                // keys sharing the prefix (after the last pass: equal to the result)
     unsigned long long wmin[32];
+    int ncoll, has_next;        // collected keys; the next key in rank order was among them
+    long long cless;            // collected keys below the result
+    unsigned long long next;    // that next key
 };
 
 // k-th smallest (0-based) of key(i), i in [0, n): most-significant-digit
-// radix selection in six passes (digits of 11, 11, 11, 11, 11 and 9 bits)
-// over a shared histogram; the keys are recomputed on every pass.  Each
+// radix selection in up to six passes (digits of 11, 11, 11, 11, 11 and 9
+// bits) over a shared histogram; the keys are recomputed on every pass.
+// Once at most kCollect keys share the digits found so far, one more pass
+// collects them into shared memory and the result is found among them by
+// exact ranking (each thread counts the keys below and equal to its own),
+// which also gives the next key in rank order when it is among them.  Each
 // thread walks its own contiguous chunk of pixels and adds runs of equal
 // digits at once; the 32 lanes of a warp look at pixels ~n/1024 apart,
 // whose digits mostly differ where the runs are short.  On
@@ -290,6 +299,7 @@ __device__ void radix_select(Visit visit, long long n, long long k, unsigned* hi
         sh.krem = k;
         sh.below = 0;
         sh.eq = 0;
+        sh.has_next = 0;
     }
     unsigned long long mask = 0;
     const long long chunk = (n + kSplThreads - 1) / kSplThreads;
@@ -349,6 +359,45 @@ __device__ void radix_select(Visit visit, long long n, long long k, unsigned* hi
         }
         mask |= (unsigned long long)dmask << shift;
         __syncthreads();
+        if (pass < 5 && sh.eq <= (unsigned)kCollect) {  // uniform: a shared value after a barrier
+            unsigned long long* coll = reinterpret_cast<unsigned long long*>(hist);
+            const unsigned long long pre = sh.prefix;
+            if (t == 0) sh.ncoll = 0;
+            __syncthreads();
+            visit(i0, i1, [&](long long, unsigned long long kk) {
+                if ((kk & mask) == pre) {
+                    const int pos = atomicAdd(&sh.ncoll, 1);
+                    if (pos < kCollect) coll[pos] = kk;
+                }
+            });
+            __syncthreads();
+            const int nc = min(sh.ncoll, kCollect);
+            const long long kr = sh.krem;
+            __syncthreads();
+            if (t < nc) {
+                const unsigned long long mine = coll[t];
+                int less = 0, same = 0;
+                for (int q = 0; q < nc; ++q) {
+                    const unsigned long long o = coll[q];
+                    less += o < mine;
+                    same += o == mine;
+                }
+                // threads holding equal keys store equal values
+                if (less <= kr && kr < less + same) {
+                    sh.prefix = mine;
+                    sh.cless = less;
+                    sh.eq = (unsigned)same;
+                }
+                if (kr + 1 < nc && less <= kr + 1 && kr + 1 < less + same) {
+                    sh.next = mine;
+                    sh.has_next = 1;
+                }
+            }
+            __syncthreads();
+            if (t == 0) sh.below += sh.cless;
+            __syncthreads();
+            return;
+        }
     }
 }
 
@@ -386,10 +435,12 @@ __device__ double select_median(Visit visit, long long n, unsigned* hist, Select
     radix_select(visit, n, r1, hist, sh);
     const unsigned long long k1 = sh.prefix;
     const long long upto = sh.below + sh.eq;  // keys <= k1
+    const bool has_next = sh.has_next != 0;
+    const unsigned long long kn = sh.next;
     __syncthreads();
     const double v1 = key_value(k1);
     if (n & 1) return v1;
-    const double v2 = upto >= r1 + 2 ? v1 : key_value(min_key_above(visit, n, k1, sh));
+    const double v2 = has_next ? key_value(kn) : (upto >= r1 + 2 ? v1 : key_value(min_key_above(visit, n, k1, sh)));
     return __dadd_rn(v1, v2) / 2;
 }
 
@@ -405,7 +456,8 @@ __global__ void __launch_bounds__(kSplThreads) wow_spline_kernel(const TbcField*
     if (f.spline_k < 2) return;
     __shared__ double pc[kSplStride * kSplMaxLines];
     __shared__ double cp[kSplMaxLines], dp[kSplMaxLines];
-    __shared__ unsigned hist[kHistBins];
+    __shared__ unsigned long long hist_mem[kHistBins / 2];  // 8-byte aligned: also the collected keys
+    unsigned* hist = reinterpret_cast<unsigned*>(hist_mem);
     __shared__ SelectShared sh;
     __shared__ double wmapA[32], wmapB[32], wy[32];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
