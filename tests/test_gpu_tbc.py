@@ -247,3 +247,41 @@ def test_tbc_wow_interpolation(cuda_ok, system):
     assert np.array_equal(got[4], lin)
     assert not np.array_equal(lin, singles[3])
     rf.close()
+
+
+def test_tbc_argument_checks(cuda_ok):
+    """ldg_tbc_fields rejects, before any launch: an unknown wow_interp, a
+    quadratic / cubic field with fewer than 4 line locations, and a field
+    buffer of 2^31 samples or more."""
+    from ldgpu import RFDecode
+    from ldgpu import lib as L
+    from ldgpu.field import tbc_descriptor, tbc_fields
+    rf = RFDecode(system="NTSC")
+    try:
+        outw = rf.SysParams["outlinelen"]
+        buf = np.zeros(200000, np.float32)
+        ll = np.arange(60, dtype=np.float64) * rf.linelen + 100.0
+        pic = np.zeros(20 * outw, np.uint16)
+        levels = (8.1e6, 12142.86, -40.0, 1.0, 1024.0)
+
+        def desc(lls, **kw):
+            return tbc_descriptor(rf, buf, lls, 0, outw, 20, 20, levels, out_u16=pic, **kw)
+
+        tbc_fields(rf, [desc(ll, wow_interpolation_method="cubic")])  # valid
+        d = desc(ll)
+        d.wow_interp = 7
+        with pytest.raises(L.LdgError) as e:
+            tbc_fields(rf, [d])
+        assert e.value.code == L.LDG_ERR_ARG
+        with pytest.raises(L.LdgError) as e:
+            tbc_fields(rf, [desc(ll[:3], wow_interpolation_method="quadratic")])
+        assert e.value.code == L.LDG_ERR_ARG
+        d = desc(ll)
+        d.buf_len = 1 << 31
+        with pytest.raises(L.LdgError) as e:
+            tbc_fields(rf, [d])
+        assert e.value.code == L.LDG_ERR_ARG
+        with pytest.raises(ValueError):
+            desc(ll, wow_interpolation_method="spline")
+    finally:
+        rf.close()
