@@ -435,6 +435,24 @@ def run_gpu(args):
         dt = time.perf_counter() - t0
         plain = {"value": nplain * U / dt / 1e6, "unit": "MSPS",
                  "form": "RFDecode.demodblock per block, host numpy in/out (DemodCache worker style)"}
+        # DemodCache's pool (core.py:1165-1200): worker threads, one RFDecode
+        # (context, stream) each, blocks handed out in turn
+        from concurrent.futures import ThreadPoolExecutor
+        nthr = 8
+        workers = [RFDecode(system=system, decode_analog_audio=44100, decode_digital_audio=True, device=local)
+                   for _ in range(nthr)]
+        def run_worker(w):
+            for b in range(w, nplain, nthr):
+                workers[w].demodblock(data=hc[b * U:b * U + N], mtf_level=1, cut=True)
+        with ThreadPoolExecutor(nthr) as ex:
+            list(ex.map(run_worker, range(nthr)))  # warm-up
+            t0 = time.perf_counter()
+            list(ex.map(run_worker, range(nthr)))
+            dt = time.perf_counter() - t0
+        for w in workers:
+            w.close()
+        plain["threads"] = {"value": nplain * U / dt / 1e6, "unit": "MSPS", "threads": nthr,
+                            "form": "the same calls from a pool of worker threads, one RFDecode each (DemodCache)"}
 
     # ---- roofline of the dominant kernel (demod)
     # ---- the kernels on their own (whole-capture launches, events on the launching stream)
