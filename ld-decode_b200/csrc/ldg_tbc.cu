@@ -652,7 +652,7 @@ __device__ __forceinline__ double pixel_coord(const TbcField& f, long long ig, i
 // ps and their differences to phase ps + 1), so a pixel's 64-byte input
 // span and its 128 bytes of LUT are each one contiguous access; the 8
 // partial sums meet in a transposing reduction (lane k ends with pixel k).
-__global__ void __launch_bounds__(kGatherThreads) tbc_gather_kernel(const TbcField* fields, const float* lut,
+__global__ void __launch_bounds__(kGatherThreads, 8) tbc_gather_kernel(const TbcField* fields, const float* lut,
                                                                     int nfields) {
     const int fi = blockIdx.y;
     if (fi >= nfields) return;
