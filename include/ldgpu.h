@@ -100,6 +100,29 @@ typedef struct {
     void* stream;      /* cudaStream_t, or NULL for the context's stream */
 } ldg_demod_args;
 
+/* One field for the analog audio downscale (the audio of Field.downscale,
+ * downscale_audio core.py:1423-1580).  The host computes the field's output
+ * clock as the reference does: ticks at timeoffset + i * soundgap, i <
+ * nticks, with freq < 0 meaning line-locked (core.py:1445-1452). */
+typedef struct {
+    const float* audio_left;   /* field-local stage-1 audio (device), demod sample s <-> audio s / scale */
+    const float* audio_right;
+    int64_t audio_len;
+    const double* linelocs;    /* FP64 line locations, field-local demod samples (device) */
+    int32_t nlines;            /* >= 2 */
+    int32_t nticks;            /* output samples + 1, in [1, 2048] */
+    double timeoffset;         /* time of the first tick (s) */
+    double soundgap;           /* 1 / output rate (s) */
+    int16_t* out;              /* 2 * (nticks - 1) interleaved L/R (device) */
+} ldg_audio_field;
+
+typedef struct {
+    double line_period;        /* SysParams line_period (us) */
+    double linelen;            /* RFDecode.linelen */
+    double scale;              /* Filters audio_fdiv: demod samples per audio sample */
+    double lfreq, rfreq;       /* SysParams audio_lfreq / audio_rfreq (Hz) */
+} ldg_audio_params;
+
 /* One field for the time-base corrector. */
 typedef struct {
     const float* buf;        /* field demod samples (field-local index 0) */
@@ -161,6 +184,18 @@ int ldg_demod_blocks(ldg_ctx* ctx, const ldg_demod_args* args);
 /* Resample a batch of fields (Field.downscale's video part,
  * core.py:2691-2713). */
 int ldg_tbc_fields(ldg_ctx* ctx, const ldg_tbc_field* fields, int32_t nfields, void* stream);
+
+/* Analog audio of a batch of fields to 16-bit output (downscale_audio,
+ * core.py:1423-1580; rescale utils.py:1328-1332): per output sample the
+ * mean of the stage-1 audio run between two ticks' line-interpolated
+ * positions, times the line-length wow factor (jumps over 1.5 % keep the
+ * previous factor), minus the carrier, scaled, rounded, clipped, negated.
+ * A sample whose run falls outside the field's audio is 0 and sets
+ * muted[i] (the reference logs "Analog audio processing error, muting
+ * samples").  Device buffers; enqueued on `stream` without waiting.  No
+ * counterpart for a batch in the reference. */
+int ldg_audio_downscale(ldg_ctx* ctx, const ldg_audio_field* fields, int32_t nfields, const ldg_audio_params* params,
+                        int32_t* muted, void* stream);
 
 /* ldg_tbc_fields for device-resident buffers without waiting: enqueues on
  * `stream` and returns (the descriptors go through one of four pinned

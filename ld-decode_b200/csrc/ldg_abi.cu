@@ -18,6 +18,7 @@
 #include "ldg_dropouts.cuh"
 #include "ldg_fft.cuh"
 #include "ldg_noalloc.h"
+#include "ldg_audio.cuh"
 #include "ldg_tbc.cuh"
 #include "ldgpu.h"
 
@@ -117,6 +118,10 @@ struct ldg_ctx {
     cudaEvent_t a2_done = nullptr;
     bool a2_used = false;
     long long* h_word = nullptr;         // pinned, mapped: results the host reads right after a kernel
+    ldg::AudioField* d_aud = nullptr;    // ldg_audio_downscale descriptors, same reuse rule
+    size_t aud_cap = 0;
+    cudaEvent_t aud_done = nullptr;
+    bool aud_used = false;
     ldg::RfTbcField* d_rftbc = nullptr;  // ldg_rf_tbc descriptors, same reuse rule
     size_t rftbc_cap = 0;
     cudaEvent_t rftbc_done = nullptr;
@@ -298,6 +303,9 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     cudaFree(c->d_slots);
     if (c->drop_used) cudaEventSynchronize(c->drop_done);
     if (c->rftbc_used) cudaEventSynchronize(c->rftbc_done);
+    if (c->aud_used) cudaEventSynchronize(c->aud_done);
+    cudaFree(c->d_aud);
+    if (c->aud_done) cudaEventDestroy(c->aud_done);
     if (c->h_word) cudaFreeHost(c->h_word);
     if (c->a2_used) cudaEventSynchronize(c->a2_done);
     cudaFree(c->d_a2);
@@ -759,6 +767,47 @@ int ldg_audio_phase2(ldg_ctx* c, const ldg_audio2_segment* segs, int32_t n, doub
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("audio2 launch: ") + cudaGetErrorString(e));
     LDG_CK(cudaEventRecord(c->a2_done, st));
     c->a2_used = true;
+    return LDG_OK;
+}
+
+int ldg_audio_downscale(ldg_ctx* c, const ldg_audio_field* fields, int32_t nfields, const ldg_audio_params* p,
+                        int32_t* muted, void* stream) {
+    if (!c || !p || (!fields && nfields)) return fail(LDG_ERR_ARG, "ldg_audio_downscale: NULL argument");
+    if (nfields < 0) return fail(LDG_ERR_ARG, "ldg_audio_downscale: negative field count");
+    if (!(p->line_period > 0) || !(p->linelen > 0) || !(p->scale > 0))
+        return fail(LDG_ERR_ARG, "ldg_audio_downscale: line period, line length and scale must be positive");
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_audio_field& f = fields[i];
+        if (!f.audio_left || !f.audio_right || !f.linelocs || (f.nticks > 1 && !f.out))
+            return fail(LDG_ERR_ARG, "ldg_audio_downscale: NULL buffer");
+        if (f.audio_len <= 0 || f.nlines < 2) return fail(LDG_ERR_ARG, "ldg_audio_downscale: bad field geometry");
+        if (f.nticks < 1 || f.nticks > ldg::kAudioMaxTicks)
+            return fail(LDG_ERR_UNSUPPORTED, "ldg_audio_downscale: 1 .. 2048 ticks per field are supported");
+        if (!(f.soundgap > 0)) return fail(LDG_ERR_ARG, "ldg_audio_downscale: soundgap must be positive");
+    }
+    if (nfields == 0) return LDG_OK;
+    if (!is_device_ptr(fields[0].audio_left) || !is_device_ptr(fields[0].linelocs) ||
+        (fields[0].out && !is_device_ptr(fields[0].out)) || (muted && !is_device_ptr(muted)))
+        return fail(LDG_ERR_ARG, "ldg_audio_downscale: buffers must be device memory");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    if (!c->aud_done) LDG_CK(cudaEventCreateWithFlags(&c->aud_done, cudaEventDisableTiming));
+    if (c->aud_used) LDG_CK(cudaEventSynchronize(c->aud_done));
+    int rc = grow((void**)&c->d_aud, &c->aud_cap, (size_t)nfields * sizeof(ldg::AudioField));
+    if (rc) return rc;
+    std::vector<ldg::AudioField> h(nfields);
+    for (int i = 0; i < nfields; ++i) {
+        const ldg_audio_field& f = fields[i];
+        h[i] = {f.audio_left, f.audio_right, f.audio_len, f.linelocs, f.nlines, f.nticks, f.timeoffset, f.soundgap,
+                f.out};
+    }
+    LDG_CK(cudaMemcpyAsync(c->d_aud, h.data(), h.size() * sizeof(ldg::AudioField), cudaMemcpyHostToDevice, st));
+    const ldg::AudioConsts k{p->line_period, p->linelen, p->scale, p->lfreq, p->rfreq};
+    cudaError_t e = ldg::launch_audio_downscale(c->d_aud, nfields, k, muted, st);
+    if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("audio launch: ") + cudaGetErrorString(e));
+    LDG_CK(cudaEventRecord(c->aud_done, st));
+    c->aud_used = true;
     return LDG_OK;
 }
 

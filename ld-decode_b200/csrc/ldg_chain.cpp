@@ -778,6 +778,8 @@ extern "C" int64_t ldg_abi_sizeof(const char* name) {
     if (n == "ldg_dropout_params") return sizeof(ldg_dropout_params);
     if (n == "ldg_rftbc_field") return sizeof(ldg_rftbc_field);
     if (n == "ldg_audio2_segment") return sizeof(ldg_audio2_segment);
+    if (n == "ldg_audio_field") return sizeof(ldg_audio_field);
+    if (n == "ldg_audio_params") return sizeof(ldg_audio_params);
     return -1;
 }
 

@@ -11,8 +11,15 @@ jump exists).
 Same call signature and results as the reference: int16 interleaved L/R,
 negated (`-dsa_rescale_and_clip`), samples whose run falls outside the audio
 muted to 0 with a warning, and the time offset for the next field.
+
+`downscale_audio_located` does the same for every field of a batched
+decode in one GPU launch (ldg_audio_downscale): each field's output clock
+and A/V offset are scalars the host computes as the reference does (the
+offset comes from the previous written field's position, not from the
+previous field's audio, so the fields are independent).
 """
 
+import ctypes
 import logging
 
 import numpy as np
@@ -124,3 +131,90 @@ def downscale_audio(audio, lineinfo, rf, linecount, timeoffset=0, freq=44100, rv
         rv["dsaudio"] = output16
         rv["audio_next_offset"] = arange[-1] - frametime
     return output16, arange[-1] - frametime
+
+
+def av_offset(rf, readloc, is_first, audio, lastfieldwritten):
+    """Field.downscale's A/V alignment offset of a field's first audio
+    sample (core.py:2644-2670): from the last written field's number and
+    read position; 0 without one or below 16 kHz."""
+    if lastfieldwritten and audio >= 16000:
+        sp = rf.SysParams
+        rf_samples_per_field = rf.freq_hz / sp["FPS"] / 2
+        read_gap = (readloc - lastfieldwritten[1]) / rf_samples_per_field
+        field_number = int(np.round(lastfieldwritten[0] + read_gap))
+        linecount = sum(sp["field_lines"]) * (field_number // 2)
+        if not is_first:
+            linecount += sp["field_lines"][0]
+        samples_per_line = (sp["line_period"] / 1000000) / (1 / audio)
+        cnt = linecount * samples_per_line
+        frac = cnt - np.floor(cnt)
+        return (1 - frac) * (1 / audio) if frac > .5 else -frac * (1 / audio)
+    return 0
+
+
+def field_clock(line_period, linecount, timeoffset, freq):
+    """(timeoffset, soundgap, nticks, next field's offset) of a field's
+    output clock, as compute_locs_and_swow sets it up (core.py:1445-1455)."""
+    if freq < 0:
+        timeoffset = 0
+        freq = (1000000 / line_period) * -freq
+    frametime = linecount / (1000000 / line_period)
+    soundgap = 1 / freq
+    stop = frametime + (soundgap / 2)
+    nticks = max(int(np.ceil((stop - timeoffset) / soundgap)), 0)
+    last = timeoffset + np.float64(nticks - 1) * soundgap
+    return timeoffset, soundgap, nticks, last - frametime
+
+
+def downscale_audio_located(rf, fields, audio_left, audio_right, freq=44100, stream=None):
+    """The analog audio of every located field on the GPU.
+
+    `fields`: ldgpu.lines.LocatedFields (in decode order, all written);
+    `audio_left` / `audio_right`: the capture-wide stage-1 audio (device
+    float32 tensors, audio_fdiv-th of the demod rate per block, as
+    demod_blocks_device writes it).  Field i is given lastfieldwritten =
+    (i, startloc of field i - 1), as LDdecode.readfield passes it.
+
+    Returns (out, offsets, muted, next_offsets): `out` one device int16
+    tensor, field i's interleaved L/R samples at out[offsets[i]:offsets[i+1]]
+    (the reference's dsaudio), `muted` a device int32 flag per field (some
+    sample fell outside the audio and was muted), `next_offsets` the
+    audio_next_offset of every field (host)."""
+    import torch
+
+    from . import lib as L
+    a = fields.arrays()
+    n = len(a["startloc"])
+    sp = rf.SysParams
+    U = rf.blocklen - rf.blockcut - rf.blockcut_end
+    scale = float(rf.Filters["audio_fdiv"])
+    per_block = int(round(U / scale))
+    clocks = []
+    for i in range(n):
+        lfw = None if i == 0 else (i, int(a["startloc"][i - 1]))
+        off = av_offset(rf, int(a["startloc"][i]), bool(a["isfirst"][i]), freq, lfw)
+        clocks.append(field_clock(sp["line_period"], int(a["linecount"][i]), off, freq))
+    nout = [max(c[2] - 1, 0) for c in clocks]
+    offsets = np.concatenate([[0], np.cumsum(2 * np.asarray(nout, dtype=np.int64))])
+    out = torch.empty(max(int(offsets[-1]), 1), dtype=torch.int16, device=audio_left.device)
+    muted = torch.zeros(max(n, 1), dtype=torch.int32, device=audio_left.device)
+    descs = (L.AudioField * n)()
+    for i in range(n):
+        first_block = int(a["startloc"][i]) // U
+        nblk = int(a["length"][i]) // U
+        d = descs[i]
+        d.audio_left = audio_left.data_ptr() + 4 * first_block * per_block
+        d.audio_right = audio_right.data_ptr() + 4 * first_block * per_block
+        d.audio_len = nblk * per_block
+        d.linelocs = int(a["linelocs_ptr"][i])
+        d.nlines = int(a["nlines"][i])
+        d.nticks = int(clocks[i][2])
+        d.timeoffset = float(clocks[i][0])
+        d.soundgap = float(clocks[i][1])
+        d.out = out.data_ptr() + 2 * int(offsets[i])
+    p = L.AudioParams(float(sp["line_period"]), float(rf.linelen), scale, float(sp["audio_lfreq"]),
+                      float(sp["audio_rfreq"]))
+    if n:
+        L.check(rf._ctx._lib.ldg_audio_downscale(rf._ctx.handle, descs, n, ctypes.byref(p), muted.data_ptr(),
+                                                 stream if stream else 1))
+    return out, offsets, muted, np.array([c[3] for c in clocks])

@@ -167,19 +167,8 @@ class Field(FieldLogic):
 
     def audio_offset(self, audio, lastfieldwritten):
         """A/V alignment offset of the first audio sample (core.py:2644-2670)."""
-        if lastfieldwritten and audio >= 16000:
-            sp = self.rf.SysParams
-            rf_samples_per_field = self.rf.freq_hz / sp["FPS"] / 2
-            read_gap = (self.readloc - lastfieldwritten[1]) / rf_samples_per_field
-            field_number = int(np.round(lastfieldwritten[0] + read_gap))
-            linecount = sum(sp["field_lines"]) * (field_number // 2)
-            if not self.isFirstField:
-                linecount += sp["field_lines"][0]
-            samples_per_line = (sp["line_period"] / 1000000) / (1 / audio)
-            cnt = linecount * samples_per_line
-            frac = cnt - np.floor(cnt)
-            return (1 - frac) * (1 / audio) if frac > .5 else -frac * (1 / audio)
-        return 0
+        from .audio import av_offset
+        return av_offset(self.rf, self.readloc, self.isFirstField, audio, lastfieldwritten)
 
 
 class FieldNTSC(FieldLogicNTSC, Field):

@@ -99,6 +99,17 @@ class Audio2Segment(ctypes.Structure):
     _fields_ = [("left", c_p), ("right", c_p), ("len", c_i64), ("out_left", c_p), ("out_right", c_p)]
 
 
+class AudioField(ctypes.Structure):
+    _fields_ = [("audio_left", c_p), ("audio_right", c_p), ("audio_len", c_i64), ("linelocs", c_p),
+                ("nlines", ctypes.c_int32), ("nticks", ctypes.c_int32), ("timeoffset", ctypes.c_double),
+                ("soundgap", ctypes.c_double), ("out", c_p)]
+
+
+class AudioParams(ctypes.Structure):
+    _fields_ = [("line_period", ctypes.c_double), ("linelen", ctypes.c_double), ("scale", ctypes.c_double),
+                ("lfreq", ctypes.c_double), ("rfreq", ctypes.c_double)]
+
+
 class RfTbcField(ctypes.Structure):
     _fields_ = [("input", c_p), ("len", c_i64), ("linelocs", c_p), ("nlines", c_i32), ("startline", c_i32),
                 ("linecount", c_i32), ("linelen", c_i32), ("delay", c_f64), ("out", c_p)]
@@ -151,6 +162,8 @@ SIGNATURES = {
     "ldg_audio_phase2": (ctypes.c_int, [c_p, ctypes.POINTER(Audio2Segment), ctypes.c_int32, ctypes.c_double,
                                         ctypes.c_double, c_p]),
     "ldg_rf_tbc": (ctypes.c_int, [c_p, ctypes.POINTER(RfTbcField), ctypes.c_int32, c_p]),
+    "ldg_audio_downscale": (ctypes.c_int, [c_p, ctypes.POINTER(AudioField), ctypes.c_int32,
+                                           ctypes.POINTER(AudioParams), c_p, c_p]),
     "ldg_dropouts": (ctypes.c_int, [c_p, ctypes.POINTER(DropoutParams), ctypes.POINTER(DropoutField),
                                     ctypes.c_int32, c_p, c_p, c_p, c_p]),
     "ldg_queue_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int32]),
@@ -198,7 +211,8 @@ ABI_STRUCTS = [("ldg_chain_params", ChainParams), ("ldg_chain_state", ChainState
                ("ldg_lines_args", LinesArgs), ("ldg_tbc_field", TbcField),
                ("ldg_demod_args", DemodArgs), ("ldg_slice", Slice), ("ldg_work_item", WorkItem),
                ("ldg_dropout_field", DropoutField), ("ldg_dropout_params", DropoutParams),
-               ("ldg_rftbc_field", RfTbcField), ("ldg_audio2_segment", Audio2Segment)]
+               ("ldg_rftbc_field", RfTbcField), ("ldg_audio2_segment", Audio2Segment),
+               ("ldg_audio_field", AudioField), ("ldg_audio_params", AudioParams)]
 
 _lib = None
 _lock = threading.Lock()
