@@ -73,6 +73,8 @@ def parse():
                     help="Field.wow_interpolation_method of the TBC (the reference's default is linear)")
     ap.add_argument("--wow-smoothing", type=float, default=0.0,
                     help="Field.wow_level_adjust_smoothing of the TBC (0: off, the reference's default)")
+    ap.add_argument("--no-analog-audio", action="store_true",
+                    help="leave the 44.1 kHz analog audio of the fields out of the step")
     ap.add_argument("--mixed", type=int, default=0,
                     help="mixed-batch workload instead: this many captures, lengths uniform in 0.5-8 s, "
                          "half NTSC / half PAL, own seed and SNR (30-45 dB) each")
@@ -164,6 +166,7 @@ def run_gpu(args):
     from ldgpu import lib as L
     from ldgpu.field import tbc_fields, tbc_status
     from ldgpu.fieldread import blocks_in_capture
+    from ldgpu.audio import downscale_audio_located
     from ldgpu.lines import LineLocator, field_levels, tbc_batch
     wow_opts = dict(wow_interpolation_method=args.wow_interp, wow_smoothing=args.wow_smoothing)
     from ldgpu.synth import synth_capture
@@ -201,12 +204,13 @@ def run_gpu(args):
     # one set of device buffers per step in flight: the end-to-end steps
     # alternate two sets, so a step's device->host copies overlap the next
     # step's input copy and demod (a set is reused once its copies are done)
-    main = types.SimpleNamespace(cap=cap, outs=outs, ptrs=ptrs, farr=farr, loc=loc, pics=None, done=None)
+    main = types.SimpleNamespace(cap=cap, outs=outs, ptrs=ptrs, farr=farr, loc=loc, pics=None, aud=None, done=None)
 
     def make_set():
         o = {k: torch.empty_like(v) for k, v in outs.items()}
         return types.SimpleNamespace(cap=torch.empty_like(cap), outs=o, ptrs={k: v.data_ptr() for k, v in o.items()},
-                                     farr={k: o[k] for k in fkeys}, loc=LineLocator(rf), pics=None, done=None)
+                                     farr={k: o[k] for k in fkeys}, loc=LineLocator(rf), pics=None, aud=None,
+                                     done=None)
     levels = field_levels(rf)
     nchunks = max(1, min(args.chunks, nblocks // 64))
     # chunk c holds a share proportional to taper**c of the blocks: a smaller
@@ -217,6 +221,8 @@ def run_gpu(args):
     streamB = torch.cuda.Stream(priority=-1)   # line locations
     streamC = torch.cuda.Stream(priority=-1)   # TBC of ranges whose line locations are final
     streamS = torch.cuda.Stream(priority=-1)   # sync-run scans
+    streamA = torch.cuda.Stream()              # analog audio of finished ranges (after their TBC, no hurry)
+    do_audio = not args.no_analog_audio
     elem = {k: v.element_size() for k, v in outs.items()}
     per_block = {k: (991 if k.startswith("audio") else U) for k in outs}
 
@@ -227,7 +233,10 @@ def run_gpu(args):
     outlinelen = rf.SysParams["outlinelen"]
     outlines = rf.SysParams["frame_lines"] // 2 + 1
     fsz = outlinelen * outlines
-    marks = {}
+    # analog audio of each field at 44.1 kHz (Field.downscale's dsaudio): one
+    # fixed slot of AS int16 per field
+    AS = 2 * 1024
+    marks = {"audio_ranges": 0}
 
     streamH = torch.cuda.Stream()              # host -> device input copies (end to end)
     streamD = torch.cuda.Stream()              # device -> host output copies (end to end)
@@ -272,8 +281,6 @@ def run_gpu(args):
                 q0, q1 = bounds[c] * 991, bounds[c + 1] * 991
                 with torch.cuda.stream(streamD):
                     io["efm"][o0:o1].copy_(bs.outs["efm"][o0:o1], non_blocking=True)
-                    io["audio_left"][q0:q1].copy_(bs.outs["audio_left"][q0:q1], non_blocking=True)
-                    io["audio_right"][q0:q1].copy_(bs.outs["audio_right"][q0:q1], non_blocking=True)
         for c in range(nchunks):
             streamB.wait_event(evs[c])
             streamS.wait_event(evs[c])
@@ -286,19 +293,32 @@ def run_gpu(args):
                 tbc_fields(rf, tbc_batch(rf, loc.fields, bs.outs["demod"].data_ptr(), bs.pics.data_ptr(), levels,
                                          first=lo, count=hi - lo, **wow_opts),
                            stream=streamC.cuda_stream, asynchronous=True)
+                if do_audio:
+                    # the same fields' analog audio, 16-bit 44.1 kHz (one launch, default priority)
+                    streamA.wait_event(ev)
+                    downscale_audio_located(rf, loc.fields, bs.outs["audio_left"], bs.outs["audio_right"], 44100,
+                                            stream=streamA.cuda_stream, first=lo, count=hi - lo, out=bs.aud,
+                                            stride=AS)
+                    marks["audio_ranges"] += 1
                 if io is not None:
                     tev = torch.cuda.Event()
                     tev.record(streamC)
                     streamD.wait_event(tev)
+                    if do_audio:
+                        aev = torch.cuda.Event()
+                        aev.record(streamA)
+                        streamD.wait_event(aev)
                     with torch.cuda.stream(streamD):
                         io["pics"][lo * fsz:hi * fsz].copy_(bs.pics[lo * fsz:hi * fsz], non_blocking=True)
+                        if do_audio:
+                            io["aud"][lo * AS:hi * AS].copy_(bs.aud[lo * AS:hi * AS], non_blocking=True)
         marks["demod_end"] = evs[-1]
         end = torch.cuda.Event(enable_timing=True)
         if overlap:
             # the next step (on the other buffer set) starts its demod while
             # this step's line locations, TBC and copies finish
             bs.done = []
-            for st_ in ([streamB, streamC, streamS] + ([streamD] if io is not None else [])):
+            for st_ in ([streamB, streamC, streamS, streamA] + ([streamD] if io is not None else [])):
                 e = torch.cuda.Event()
                 e.record(st_)
                 bs.done.append(e)
@@ -308,6 +328,7 @@ def run_gpu(args):
             stream.wait_stream(streamB)
             stream.wait_stream(streamC)
             stream.wait_stream(streamS)
+            stream.wait_stream(streamA)
             end.record(stream)
         marks["end"] = end
         return loc.fields
@@ -316,12 +337,14 @@ def run_gpu(args):
     torch.cuda.synchronize()
     nf = len(flist)
     main.pics = torch.empty(nf * fsz, dtype=torch.uint16, device="cuda")
+    main.aud = torch.zeros(nf * AS, dtype=torch.int16, device="cuda")
     pics = main.pics
     # the second buffer set (overlapped and end-to-end steps); its capture is
     # the same, copied once on the device
     alt = make_set()
     alt.cap.copy_(cap)
     alt.pics = torch.empty(nf * fsz, dtype=torch.uint16, device="cuda")
+    alt.aud = torch.zeros(nf * AS, dtype=torch.int16, device="cuda")
 
     def barrier():
         replica_barrier(world)
@@ -357,9 +380,11 @@ def run_gpu(args):
     barrier()
     o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     o0.record(stream)
+    ar0 = marks["audio_ranges"]
     for k in range(args.steps):
         step(None, (main, alt)[k % 2], overlap=True)
-    for st_ in (streamB, streamC, streamS):
+    audio_ranges = (marks["audio_ranges"] - ar0) / args.steps
+    for st_ in (streamB, streamC, streamS, streamA):
         stream.wait_stream(st_)
     o1.record(stream)
     torch.cuda.synchronize()
@@ -393,8 +418,7 @@ def run_gpu(args):
             return {"cap": host_cap,
                     "pics": torch.empty(nf * fsz, dtype=torch.uint16).pin_memory(),
                     "efm": torch.empty(nout, dtype=torch.int16).pin_memory(),
-                    "audio_left": torch.empty(nblocks * 991, dtype=torch.float32).pin_memory(),
-                    "audio_right": torch.empty(nblocks * 991, dtype=torch.float32).pin_memory()}
+                    "aud": torch.zeros(nf * AS, dtype=torch.int16).pin_memory()}
         sets, ios = [main, alt], [make_io(), make_io()]
         for k in range(2):  # warm the copy path on both sets
             assert len(step(ios[k], sets[k])) == nf
@@ -410,17 +434,19 @@ def run_gpu(args):
         barrier()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, "cuda")
         h2d = nsamples * 2
-        d2h = nf * fsz * 2 + nout * 2 + 2 * nblocks * 991 * 4
+        d2h = nf * fsz * 2 + nout * 2 + (nf * AS * 2 if do_audio else 0)
         e2e = {"value": world * nout / (e2e_ms * 1e-3) / 1e6, "unit": "MSPS", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                "path": "pinned host capture -> ldg_demod_blocks -> ldg_sync_runs + ldg_field_chain + "
-                       "ldg_lines_refine -> ldg_tbc_fields -> host fields, EFM, audio; per chunk, the input "
+                       "ldg_lines_refine -> ldg_tbc_fields + ldg_audio_downscale -> host fields, EFM, 44.1 kHz "
+                       "audio; per chunk, the input "
                        "copy and the output copies overlap the other chunks' work; two buffer sets, so a "
                        "step's output copies also overlap the next step"}
         # the end-to-end outputs of the last step equal the device-resident run's
         last = ios[(args.steps - 1) % 2]
         e2e["outputs_match"] = bool(torch.equal(last["pics"].view(torch.int16), pics.cpu().view(torch.int16)) and
-                                    torch.equal(last["efm"], outs["efm"].cpu()))
+                                    torch.equal(last["efm"], outs["efm"].cpu()) and
+                                    torch.equal(last["aud"], main.aud.cpu()))
 
     # ---- plain form: one demodblock() call per block through the Python API
     plain = None
@@ -519,7 +545,8 @@ def run_gpu(args):
             "workload": f"{system} {args.seconds:g} s capture, {nsamples} int16 samples at 40 MSPS, "
                         f"{nblocks} blocks x 32768 (stride {U}), {nf} fields per GPU",
             "outputs": "demod, demod_raw, demod_05, demod_burst" + (", demod_pilot" if system == "PAL" else "")
-                       + ", rfhpf, efm, audio L/R stage 1, uint16 TBC fields",
+                       + ", rfhpf, efm, audio L/R stage 1, uint16 TBC fields, 16-bit 44.1 kHz analog audio "
+                         "per field",
             "linelocs": "in the step: GPU sync-run scan, native field chain, GPU H-sync/burst/pilot refinement "
                         f"(FP64); host time per step {statistics.median(host_ms):.1f} ms, overlapped with the GPU",
             "l2": "inputs (800 MB) and outputs (> 8 GB) exceed L2 each step; no flush",
@@ -551,7 +578,8 @@ def run_gpu(args):
         "plain": plain,
         "cpu_baseline": cpu,
         # per step: demod 1, sync runs 4, refine 3 (NTSC) / 1 (PAL) per segment, TBC 2
-        "gpu_launches": int(args.steps * (nchunks * (1 + 4 + 2) + segs * (3 if system == "NTSC" else 1))),
+        "gpu_launches": int(args.steps * (nchunks * (1 + 4 + 2) + segs * (3 if system == "NTSC" else 1)
+                                          + audio_ranges)),
         "clocks": clocks,
     }
     if rank == 0:

@@ -118,10 +118,6 @@ struct ldg_ctx {
     cudaEvent_t a2_done = nullptr;
     bool a2_used = false;
     long long* h_word = nullptr;         // pinned, mapped: results the host reads right after a kernel
-    ldg::AudioField* d_aud = nullptr;    // ldg_audio_downscale descriptors, same reuse rule
-    size_t aud_cap = 0;
-    cudaEvent_t aud_done = nullptr;
-    bool aud_used = false;
     ldg::RfTbcField* d_rftbc = nullptr;  // ldg_rf_tbc descriptors, same reuse rule
     size_t rftbc_cap = 0;
     cudaEvent_t rftbc_done = nullptr;
@@ -303,9 +299,6 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     cudaFree(c->d_slots);
     if (c->drop_used) cudaEventSynchronize(c->drop_done);
     if (c->rftbc_used) cudaEventSynchronize(c->rftbc_done);
-    if (c->aud_used) cudaEventSynchronize(c->aud_done);
-    cudaFree(c->d_aud);
-    if (c->aud_done) cudaEventDestroy(c->aud_done);
     if (c->h_word) cudaFreeHost(c->h_word);
     if (c->a2_used) cudaEventSynchronize(c->a2_done);
     cudaFree(c->d_a2);
@@ -789,25 +782,18 @@ int ldg_audio_downscale(ldg_ctx* c, const ldg_audio_field* fields, int32_t nfiel
     if (!is_device_ptr(fields[0].audio_left) || !is_device_ptr(fields[0].linelocs) ||
         (fields[0].out && !is_device_ptr(fields[0].out)) || (muted && !is_device_ptr(muted)))
         return fail(LDG_ERR_ARG, "ldg_audio_downscale: buffers must be device memory");
-    std::lock_guard<std::mutex> lk(c->mu);
     DeviceGuard g(c->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-    if (!c->aud_done) LDG_CK(cudaEventCreateWithFlags(&c->aud_done, cudaEventDisableTiming));
-    if (c->aud_used) LDG_CK(cudaEventSynchronize(c->aud_done));
-    int rc = grow((void**)&c->d_aud, &c->aud_cap, (size_t)nfields * sizeof(ldg::AudioField));
-    if (rc) return rc;
+    // the descriptors go in the launches' parameters: no device buffer, no wait
     std::vector<ldg::AudioField> h(nfields);
     for (int i = 0; i < nfields; ++i) {
         const ldg_audio_field& f = fields[i];
         h[i] = {f.audio_left, f.audio_right, f.audio_len, f.linelocs, f.nlines, f.nticks, f.timeoffset, f.soundgap,
                 f.out};
     }
-    LDG_CK(cudaMemcpyAsync(c->d_aud, h.data(), h.size() * sizeof(ldg::AudioField), cudaMemcpyHostToDevice, st));
     const ldg::AudioConsts k{p->line_period, p->linelen, p->scale, p->lfreq, p->rfreq};
-    cudaError_t e = ldg::launch_audio_downscale(c->d_aud, nfields, k, muted, st);
+    cudaError_t e = ldg::launch_audio_downscale(h.data(), nfields, k, muted, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("audio launch: ") + cudaGetErrorString(e));
-    LDG_CK(cudaEventRecord(c->aud_done, st));
-    c->aud_used = true;
     return LDG_OK;
 }
 

@@ -22,9 +22,9 @@ __device__ __forceinline__ int16_t rescale_clip_neg(double x) {
     return (int16_t)(-(int)v);
 }
 
-__global__ void __launch_bounds__(kAudioThreads) audio_downscale_kernel(const AudioField* fields, AudioConsts c,
-                                                                       int* muted) {
-    const AudioField& f = fields[blockIdx.x];
+__global__ void __launch_bounds__(kAudioThreads) audio_downscale_kernel(const __grid_constant__ AudioBatch b,
+                                                                       AudioConsts c, int* muted) {
+    const AudioField& f = b.f[blockIdx.x];
     __shared__ double locs[kAudioMaxTicks], swow[kAudioMaxTicks];
     __shared__ int any_jump, any_mute;
     const int t = threadIdx.x;
@@ -79,8 +79,26 @@ __global__ void __launch_bounds__(kAudioThreads) audio_downscale_kernel(const Au
         const long long s = (long long)locs[i], e = (long long)locs[i + 1];
         int16_t ol = 0, orr = 0;
         if (e > s && e < f.len && s >= -f.len) {
+            // summed in index order; eight samples per channel loaded ahead
+            // of their adds (one memory latency per eight, not per sample)
             float suml = 0.0f, sumr = 0.0f;
-            for (long long k = s; k < e; ++k) {
+            long long k = s;
+            if (s >= 0) {
+                for (; k + 8 <= e; k += 8) {
+                    float xl[8], xr[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        xl[u] = __ldg(f.al + k + u);
+                        xr[u] = __ldg(f.ar + k + u);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        suml = __fadd_rn(suml, xl[u]);
+                        sumr = __fadd_rn(sumr, xr[u]);
+                    }
+                }
+            }
+            for (; k < e; ++k) {
                 const long long q = k < 0 ? k + f.len : k;  // numpy's negative index
                 suml = __fadd_rn(suml, __ldg(f.al + q));
                 sumr = __fadd_rn(sumr, __ldg(f.ar + q));
@@ -101,11 +119,17 @@ __global__ void __launch_bounds__(kAudioThreads) audio_downscale_kernel(const Au
 
 }  // namespace
 
-cudaError_t launch_audio_downscale(const AudioField* dfields, int nfields, AudioConsts c, int* muted,
+cudaError_t launch_audio_downscale(const AudioField* fields, int nfields, AudioConsts c, int* muted,
                                    cudaStream_t stream) {
-    if (nfields <= 0) return cudaSuccess;
-    audio_downscale_kernel<<<nfields, kAudioThreads, 0, stream>>>(dfields, c, muted);
-    return cudaGetLastError();
+    for (int off = 0; off < nfields; off += kAudioBatch) {
+        const int n = nfields - off < kAudioBatch ? nfields - off : kAudioBatch;
+        AudioBatch b;
+        for (int i = 0; i < n; ++i) b.f[i] = fields[off + i];
+        audio_downscale_kernel<<<n, kAudioThreads, 0, stream>>>(b, c, muted ? muted + off : nullptr);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace ldg

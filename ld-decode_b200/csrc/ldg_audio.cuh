@@ -22,7 +22,16 @@ struct AudioConsts {
     double line_period, linelen, scale, lfreq, rfreq;
 };
 
-cudaError_t launch_audio_downscale(const AudioField* dfields, int nfields, AudioConsts c, int* muted,
+// Up to kAudioBatch field descriptors travel in the kernel's parameters
+// (8 KB), so a launch needs no device descriptor buffer and the host never
+// waits for an earlier launch.
+constexpr int kAudioBatch = 128;
+struct AudioBatch {
+    AudioField f[kAudioBatch];
+};
+
+// fields: host array of n descriptors (any n; launched kAudioBatch at a time)
+cudaError_t launch_audio_downscale(const AudioField* fields, int nfields, AudioConsts c, int* muted,
                                    cudaStream_t stream);
 
 }  // namespace ldg

@@ -166,55 +166,109 @@ def field_clock(line_period, linecount, timeoffset, freq):
     return timeoffset, soundgap, nticks, last - frametime
 
 
-def downscale_audio_located(rf, fields, audio_left, audio_right, freq=44100, stream=None):
-    """The analog audio of every located field on the GPU.
+def field_clocks(rf, startloc, isfirst, linecount, first, count, freq):
+    """av_offset and field_clock for fields [first, first + count) of a
+    decode whose field i follows lastfieldwritten = (i, startloc[i - 1]),
+    as numpy arrays (the same double operations, element by element):
+    (timeoffset, soundgap, nticks, next_offset)."""
+    sp = rf.SysParams
+    i = np.arange(first, first + count, dtype=np.int64)
+    startloc = np.asarray(startloc, dtype=np.int64)
+    isfirst = np.asarray(isfirst, dtype=bool)[first:first + count]
+    linecount = np.asarray(linecount, dtype=np.int64)[first:first + count]
+    off = np.zeros(count, dtype=np.float64)
+    if freq >= 16000 and count:
+        rf_samples_per_field = rf.freq_hz / sp["FPS"] / 2
+        prev = startloc[np.maximum(i - 1, 0)]
+        read_gap = (startloc[i] - prev) / rf_samples_per_field
+        field_number = np.round(i + read_gap).astype(np.int64)
+        lc = sum(sp["field_lines"]) * (field_number // 2) + np.where(isfirst, 0, sp["field_lines"][0])
+        samples_per_line = (sp["line_period"] / 1000000) / (1 / freq)
+        cnt = lc * samples_per_line
+        frac = cnt - np.floor(cnt)
+        off = np.where(frac > .5, (1 - frac) * (1 / freq), -frac * (1 / freq))
+        off[i == 0] = 0
+    if freq < 0:
+        off = np.zeros(count, dtype=np.float64)
+        freq = (1000000 / sp["line_period"]) * -freq
+    frametime = linecount / (1000000 / sp["line_period"])
+    soundgap = 1 / freq
+    stop = frametime + (soundgap / 2)
+    nticks = np.maximum(np.ceil((stop - off) / soundgap).astype(np.int64), 0)
+    last = off + (nticks - 1).astype(np.float64) * soundgap
+    return off, soundgap, nticks, last - frametime
+
+
+def downscale_audio_located(rf, fields, audio_left, audio_right, freq=44100, stream=None, first=0, count=None,
+                            out=None, stride=None, muted=None):
+    """The analog audio of located fields on the GPU, one launch.
 
     `fields`: ldgpu.lines.LocatedFields (in decode order, all written);
     `audio_left` / `audio_right`: the capture-wide stage-1 audio (device
     float32 tensors, audio_fdiv-th of the demod rate per block, as
     demod_blocks_device writes it).  Field i is given lastfieldwritten =
-    (i, startloc of field i - 1), as LDdecode.readfield passes it.
+    (i, startloc of field i - 1), as LDdecode.readfield passes it.  Fields
+    [first, first + count) are done (default: all).
 
-    Returns (out, offsets, muted, next_offsets): `out` one device int16
-    tensor, field i's interleaved L/R samples at out[offsets[i]:offsets[i+1]]
-    (the reference's dsaudio), `muted` a device int32 flag per field (some
-    sample fell outside the audio and was muted), `next_offsets` the
-    audio_next_offset of every field (host)."""
+    Without `out`: returns (out, offsets, muted, next_offsets), `out` one
+    device int16 tensor with field first + j's interleaved L/R samples (the
+    reference's dsaudio) at out[offsets[j]:offsets[j+1]], `muted` a device
+    int32 flag per field (a sample fell outside the audio and was muted),
+    `next_offsets` the fields' audio_next_offset (host).  With `out` (device
+    int16) and `stride`: field i's samples start at out[i * stride]; the
+    offsets returned are those starts and ends; `muted` may be given (one
+    int32 per field, indexed from `first`) or None."""
     import torch
 
     from . import lib as L
     a = fields.arrays()
-    n = len(a["startloc"])
+    n_all = len(a["startloc"])
+    count = n_all - first if count is None else count
     sp = rf.SysParams
     U = rf.blocklen - rf.blockcut - rf.blockcut_end
     scale = float(rf.Filters["audio_fdiv"])
     per_block = int(round(U / scale))
-    clocks = []
-    for i in range(n):
-        lfw = None if i == 0 else (i, int(a["startloc"][i - 1]))
-        off = av_offset(rf, int(a["startloc"][i]), bool(a["isfirst"][i]), freq, lfw)
-        clocks.append(field_clock(sp["line_period"], int(a["linecount"][i]), off, freq))
-    nout = [max(c[2] - 1, 0) for c in clocks]
-    offsets = np.concatenate([[0], np.cumsum(2 * np.asarray(nout, dtype=np.int64))])
-    out = torch.empty(max(int(offsets[-1]), 1), dtype=torch.int16, device=audio_left.device)
-    muted = torch.zeros(max(n, 1), dtype=torch.int32, device=audio_left.device)
-    descs = (L.AudioField * n)()
-    for i in range(n):
-        first_block = int(a["startloc"][i]) // U
-        nblk = int(a["length"][i]) // U
-        d = descs[i]
-        d.audio_left = audio_left.data_ptr() + 4 * first_block * per_block
-        d.audio_right = audio_right.data_ptr() + 4 * first_block * per_block
-        d.audio_len = nblk * per_block
-        d.linelocs = int(a["linelocs_ptr"][i])
-        d.nlines = int(a["nlines"][i])
-        d.nticks = int(clocks[i][2])
-        d.timeoffset = float(clocks[i][0])
-        d.soundgap = float(clocks[i][1])
-        d.out = out.data_ptr() + 2 * int(offsets[i])
+    off, soundgap, nticks, nxt = field_clocks(rf, a["startloc"], a["isfirst"], a["linecount"], first, count, freq)
+    nsamp = 2 * np.maximum(nticks - 1, 0)
+    if out is None:
+        starts = np.concatenate([[0], np.cumsum(nsamp)[:-1]]).astype(np.int64) if count else np.zeros(0, np.int64)
+        out = torch.empty(max(int(nsamp.sum()), 1), dtype=torch.int16, device=audio_left.device)
+        ret_muted = muted = torch.zeros(max(count, 1), dtype=torch.int32, device=audio_left.device)
+    else:
+        if stride is None or (count and int(nsamp.max()) > stride):
+            raise ValueError("stride must hold 2 * (nticks - 1) samples of every field")
+        starts = np.arange(first, first + count, dtype=np.int64) * stride
+        ret_muted = muted
+    sel = slice(first, first + count)
+    d = np.zeros(count, _AUDIO_DTYPE)
+    fb = (np.asarray(a["startloc"][sel], dtype=np.int64) // U).astype(np.uint64)
+    d["audio_left"] = np.uint64(audio_left.data_ptr()) + np.uint64(4 * per_block) * fb
+    d["audio_right"] = np.uint64(audio_right.data_ptr()) + np.uint64(4 * per_block) * fb
+    d["audio_len"] = (np.asarray(a["length"][sel], dtype=np.int64) // U) * per_block
+    d["linelocs"] = np.asarray(a["linelocs_ptr"][sel], dtype=np.uint64)
+    d["nlines"] = a["nlines"][sel]
+    d["nticks"] = nticks
+    d["timeoffset"] = off
+    d["soundgap"] = soundgap
+    d["out"] = np.uint64(out.data_ptr()) + np.uint64(2) * starts.astype(np.uint64)
     p = L.AudioParams(float(sp["line_period"]), float(rf.linelen), scale, float(sp["audio_lfreq"]),
                       float(sp["audio_rfreq"]))
-    if n:
-        L.check(rf._ctx._lib.ldg_audio_downscale(rf._ctx.handle, descs, n, ctypes.byref(p), muted.data_ptr(),
+    if count:
+        descs = (L.AudioField * count).from_buffer_copy(d.tobytes())
+        L.check(rf._ctx._lib.ldg_audio_downscale(rf._ctx.handle, descs, count, ctypes.byref(p),
+                                                 muted.data_ptr() if muted is not None else None,
                                                  stream if stream else 1))
-    return out, offsets, muted, np.array([c[3] for c in clocks])
+    return out, np.concatenate([starts, [starts[-1] + nsamp[-1]] if count else [0]]), ret_muted, nxt
+
+
+def _audio_dtype():
+    from . import lib as L
+    fmt = {"audio_left": "u8", "audio_right": "u8", "audio_len": "i8", "linelocs": "u8", "nlines": "i4",
+           "nticks": "i4", "timeoffset": "f8", "soundgap": "f8", "out": "u8"}
+    names = [n for n, _ in L.AudioField._fields_]
+    return np.dtype({"names": names, "formats": [fmt[k] for k in names],
+                     "offsets": [getattr(L.AudioField, k).offset for k in names],
+                     "itemsize": ctypes.sizeof(L.AudioField)})
+
+
+_AUDIO_DTYPE = _audio_dtype()

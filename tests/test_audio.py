@@ -70,3 +70,28 @@ def test_ntsc_locked_rate_sample_counts():
     np.testing.assert_allclose(swow, 1.0, atol=1e-9)
     assert 1_000_000 / sysparams("NTSC")["line_period"] * 2.8 == 44055.944055944055
     assert _count(44100)[0] == 1471
+
+
+@pytest.mark.parametrize("system", ["NTSC", "PAL"])
+@pytest.mark.parametrize("freq", [44100, 48000, 8000, -4])
+def test_field_clocks_vectorised_equals_scalar(system, freq):
+    """The batched path's per-field output clocks (ldgpu.audio.field_clocks)
+    equal Field.downscale's scalar av_offset + compute_locs_and_swow set-up
+    field by field, including the first field (no lastfieldwritten)."""
+    from ldgpu.audio import av_offset, field_clock, field_clocks
+    from ldgpu.rfdecode import RFParams
+    rf = RFParams(system=system)
+    rng = np.random.default_rng(4)
+    n = 40
+    per_field = rf.freq_hz / rf.SysParams["FPS"] / 2
+    startloc = (np.arange(n) * per_field + rng.integers(-3000, 3000, n)).astype(np.int64) // 31712 * 31712
+    isfirst = (np.arange(n) % 2 == 0)
+    linecount = np.where(isfirst, 262 if system == "NTSC" else 312, 263 if system == "NTSC" else 313)
+    for first, count in ((0, n), (7, 13)):
+        off, gap, nt, nxt = field_clocks(rf, startloc, isfirst, linecount, first, count, freq)
+        for j in range(count):
+            i = first + j
+            lfw = None if i == 0 else (i, int(startloc[i - 1]))
+            o = av_offset(rf, int(startloc[i]), bool(isfirst[i]), freq, lfw)
+            t0, sg, ntk, nx = field_clock(rf.SysParams["line_period"], int(linecount[i]), o, freq)
+            assert (off[j], gap, nt[j], nxt[j]) == (t0, sg, ntk, nx), (i, off[j], t0)

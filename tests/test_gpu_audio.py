@@ -55,5 +55,17 @@ def test_audio_downscale_located_equals_host(cuda_ok, system):
                 assert np.array_equal(got, want), (freq, i, np.abs(got.astype(int) - want.astype(int)).max())
                 assert nxt[i] == wnext
             print(system, freq, nf, "fields,", offs[-1] // 2, "stereo samples equal")
+            # the same fields in two ranges into fixed slots (the batched pipeline's form)
+            if freq > 0:
+                stride = 2048
+                slots = torch.zeros(nf * stride, dtype=torch.int16, device="cuda")
+                for lo, hi in ((0, 9), (9, nf)):
+                    downscale_audio_located(rf, fields, outs["audio_left"], outs["audio_right"], freq=freq,
+                                            first=lo, count=hi - lo, out=slots, stride=stride)
+                torch.cuda.synchronize()
+                slots = slots.cpu().numpy()
+                for i in range(nf):
+                    m = offs[i + 1] - offs[i]
+                    assert np.array_equal(slots[i * stride:i * stride + m], out[offs[i]:offs[i + 1]])
     finally:
         rf.close()
