@@ -7,7 +7,9 @@ blocks and 600 fields.  One step = every block of the capture through the
 fused demodulator (all outputs: demod, demod_raw, demod_05, demod_burst,
 rfhpf, EFM, analog audio stage 1), the line locations of every field (GPU
 sync-run scan, native field chain, GPU H-sync / burst / pilot refinement)
-and every field through the TBC (uint16 4fsc fields).  The step runs in
+and every field through the TBC (uint16 4fsc fields) and the analog audio
+downscale (16-bit 44.1 kHz per field; --no-analog-audio leaves it out).
+The step runs in
 chunks of blocks (--chunks): while the GPU demodulates chunk c+1 (one CTA
 per block, so other streams' kernels get SMs between blocks), the host walks
 chunk c's fields and higher-priority streams scan, refine and resample them.
