@@ -238,9 +238,11 @@ int ldg_demod_scratch_bytes(ldg_ctx* ctx, int64_t nblocks, int64_t* bytes);
  * would allocate).  The demodulator's scratch is a static device array of
  * 32 CTA slots x 256 KB (8 MB) that every GPU loading the library keeps
  * until exit; `ctas` is the number of CTA slots to use (0: min(nblocks,
- * 32)), and ctas > 32 is rejected with LDG_ERR_ARG.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress), so
- * make that first call before any stream capture.  Calls share the array:
+ * 32)), and ctas > 32 is rejected with LDG_ERR_ARG.  Every call looks up
+ * the array's device address on the context's device (cudaGetSymbolAddress,
+ * which allocates nothing; the first lookup on a device sets the array up
+ * there, so make the first call before any stream capture), so no address
+ * outlives a device reset.  Calls share the array:
  * calls that overlap on the GPU race and must be serialised by the caller;
  * nothing in it needs clearing between calls.  The filters and tables still
  * come from `ctx`, which is created (and allocates) beforehand.  Enqueues

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "ldg_ac3.h"
+#include "ldg_attr.cuh"
 
 namespace ldg {
 
@@ -148,17 +149,9 @@ cudaError_t launch_ac3_frontend(const void* in, int in_kind, long long in_first,
     p.out_q = out_q;
     p.taps = taps;
     const size_t smem = tile_smem(taps);
-    static std::mutex mu;
-    static size_t configured = 0;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (smem > configured) {
-            cudaError_t e = cudaFuncSetAttribute(ac3_frontend_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return e;
-            configured = smem;
-        }
-    }
+    static SmemAttr attr;
+    cudaError_t e = attr.ensure(ac3_frontend_kernel, smem);
+    if (e != cudaSuccess) return e;
     const unsigned grid = (unsigned)((out_count + kTile - 1) / kTile);
     ac3_frontend_kernel<<<grid, kAc3Threads, smem, stream>>>(p);
     return cudaGetLastError();

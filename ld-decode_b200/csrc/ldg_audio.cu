@@ -77,33 +77,35 @@ __global__ void __launch_bounds__(kAudioThreads) audio_downscale_kernel(const __
     const int n = nt - 1;
     for (int i = t; i < n; i += kAudioThreads) {
         const long long s = (long long)locs[i], e = (long long)locs[i + 1];
+        // the slice audio[s:e] with numpy's bounds: a negative bound counts
+        // from the end of the buffer, then clamps at 0; an empty slice (which
+        // makes the reference's mean divide by zero and raise) is muted
+        const long long s0 = s < 0 ? max(s + (long long)f.len, 0LL) : s;
+        const long long e0 = e < 0 ? max(e + (long long)f.len, 0LL) : e;
         int16_t ol = 0, orr = 0;
-        if (e > s && e < f.len && s >= -f.len) {
+        if (e > s && e < f.len && e0 > s0) {
             // summed in index order; eight samples per channel loaded ahead
             // of their adds (one memory latency per eight, not per sample)
             float suml = 0.0f, sumr = 0.0f;
-            long long k = s;
-            if (s >= 0) {
-                for (; k + 8 <= e; k += 8) {
-                    float xl[8], xr[8];
+            long long k = s0;
+            for (; k + 8 <= e0; k += 8) {
+                float xl[8], xr[8];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        xl[u] = __ldg(f.al + k + u);
-                        xr[u] = __ldg(f.ar + k + u);
-                    }
+                for (int u = 0; u < 8; ++u) {
+                    xl[u] = __ldg(f.al + k + u);
+                    xr[u] = __ldg(f.ar + k + u);
+                }
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        suml = __fadd_rn(suml, xl[u]);
-                        sumr = __fadd_rn(sumr, xr[u]);
-                    }
+                for (int u = 0; u < 8; ++u) {
+                    suml = __fadd_rn(suml, xl[u]);
+                    sumr = __fadd_rn(sumr, xr[u]);
                 }
             }
-            for (; k < e; ++k) {
-                const long long q = k < 0 ? k + f.len : k;  // numpy's negative index
-                suml = __fadd_rn(suml, __ldg(f.al + q));
-                sumr = __fadd_rn(sumr, __ldg(f.ar + q));
+            for (; k < e0; ++k) {
+                suml = __fadd_rn(suml, __ldg(f.al + k));
+                sumr = __fadd_rn(sumr, __ldg(f.ar + k));
             }
-            const double len = (double)(e - s);
+            const double len = (double)(e0 - s0);
             const double w = swow[i];
             ol = rescale_clip_neg(__dadd_rn(__dmul_rn(__ddiv_rn((double)suml, len), w), -c.lfreq));
             orr = rescale_clip_neg(__dadd_rn(__dmul_rn(__ddiv_rn((double)sumr, len), w), -c.rfreq));

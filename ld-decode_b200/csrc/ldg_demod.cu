@@ -18,6 +18,7 @@
 // per-CTA global scratch (256 KB per CTA, L2 resident).  This restates
 // RFDecode.demodblock_cpu (lddecode/core.py:755-879) and unwrap_hilbert
 // (lddecode/utils.py:898-926).
+#include "ldg_attr.cuh"
 #include "ldg_demod.cuh"
 #include "ldg_fft.cuh"
 
@@ -593,27 +594,17 @@ __global__ void __launch_bounds__(kThreads, 1) audio2_kernel(const __grid_consta
 }
 
 cudaError_t launch_audio2(const Audio2Params& p, int nsegs, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(audio2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kSmemBytes);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    static SmemAttr attr;
+    cudaError_t e = attr.ensure(audio2_kernel, kSmemBytes);
+    if (e != cudaSuccess) return e;
     if (nsegs <= 0) return cudaSuccess;
     audio2_kernel<<<dim3((unsigned)nsegs, 2), kThreads, kSmemBytes, stream>>>(p);
     return cudaGetLastError();
 }
 
 cudaError_t prepare_demod_queue() {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(demod_queue_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kSmemBytes);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    return cudaSuccess;
+    static SmemAttr attr;
+    return attr.ensure(demod_queue_kernel, kSmemBytes);
 }
 
 cudaError_t launch_demod_queue(const QueueParams& q, int grid, cudaStream_t stream) {
@@ -625,13 +616,9 @@ cudaError_t launch_demod_queue(const QueueParams& q, int grid, cudaStream_t stre
 }
 
 cudaError_t launch_demod(const DemodParams& p, int grid, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(demod_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kSmemBytes);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    static SmemAttr attr;
+    cudaError_t e = attr.ensure(demod_kernel, kSmemBytes);
+    if (e != cudaSuccess) return e;
     if (p.nblocks <= 0) return cudaSuccess;
     demod_kernel<<<grid, kThreads, kSmemBytes, stream>>>(p);
     return cudaGetLastError();

@@ -18,7 +18,6 @@
 // two calls that overlap on the GPU (different streams, or different
 // contexts on the same device) race on it and must be serialised by the
 // caller.
-#include <mutex>
 #include <string>
 
 #include "ldg_demod.cuh"
@@ -33,25 +32,19 @@ constexpr size_t kSlotFloat2 = ldg::kScratchPerCta / sizeof(float2);
 
 static __device__ __align__(256) float2 g_noalloc_scratch[kNoAllocSlots * kSlotFloat2];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-float2* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on `device` (which must be current).
-// Looked up once per device; the host-side symbol itself is not a device
-// address and must never be handed to a kernel.
-int scratch_address(int device, float2** out) {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (device < 0 || device >= kMaxDevices) return LDG_ERR_ARG;
-    if (!g_scratch_addr[device]) {
-        void* ptr = nullptr;
-        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || ptr == nullptr) {
-            cudaGetLastError();
-            return LDG_ERR_CUDA;
-        }
-        g_scratch_addr[device] = static_cast<float2*>(ptr);
+// Device address of the scratch array on the current device.  Looked up on
+// every call (cudaGetSymbolAddress allocates nothing and is cheap), so an
+// address never outlives the device context it came from: after a
+// cudaDeviceReset the next call gets the array of the new context.  The
+// host-side symbol itself is not a device address and must never be handed
+// to a kernel.
+int scratch_address(float2** out) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || ptr == nullptr) {
+        cudaGetLastError();
+        return LDG_ERR_CUDA;
     }
-    *out = g_scratch_addr[device];
+    *out = static_cast<float2*>(ptr);
     return LDG_OK;
 }
 
@@ -75,7 +68,7 @@ extern "C" int ldg_demod_blocks_noalloc(ldg_ctx* ctx, const ldg_demod_args* a, i
         }
     } restore{prev, device};
     float2* scratch = nullptr;
-    rc = scratch_address(device, &scratch);
+    rc = scratch_address(&scratch);
     if (rc != LDG_OK)
         return ldg::api_fail(rc, "ldg_demod_blocks_noalloc: cudaGetSymbolAddress of the static scratch failed");
     p.scratch = scratch;

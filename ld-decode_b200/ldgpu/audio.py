@@ -90,11 +90,20 @@ def to_output(arange, locs, swow, audio_left, audio_right, audio_lfreq, audio_rf
     ar = np.asarray(audio_right)
     start = locs[:-1].astype(np.int64)
     end = locs[1:].astype(np.int64)
-    ok = (end > start) & (end < len(al))
+    na = len(al)
+    ok = (end > start) & (end < na)
+    # the bounds of the slice audio[start:end] as numpy and numba take it: a
+    # negative bound counts from the end, then clamps at 0
+    s0 = np.where(start < 0, np.maximum(start + na, 0), start)
+    e0 = np.where(end < 0, np.maximum(end + na, 0), end)
+    # an empty slice (a run from before the buffer's start to after it) makes
+    # the reference's compiled np.mean divide by zero, which raises; such a
+    # sample is muted here like the other failed runs
+    ok &= e0 > s0
     failed = not bool(ok.all())
     idx = np.nonzero(ok)[0]
     if len(idx):
-        s, e = start[idx], end[idx]
+        s, e = s0[idx], e0[idx]
         acc = al.dtype if al.dtype.kind == "f" else np.dtype(np.float64)
         ml = _run_means(al, s, e, acc)
         mr = _run_means(ar, s, e, acc)

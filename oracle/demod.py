@@ -53,7 +53,7 @@ def notch_v4300d(X, blocklen, freq_mhz):
 
 def demodblock(data, filters, system="NTSC", freq_hz=40e6, blocklen=32768,
                blockcut=1024, blockcut_end=32, video_rot=3, mtf_level=0.0,
-               cut=True, efm=False, audio=None, fftdata=None, pal_notch=False):
+               cut=True, efm=False, audio=None, fftdata=None, pal_notch=False, out_dtype=np.float32):
     """Restatement of RFDecode.demodblock_cpu (core.py:755-879).
 
     `mtf_level` is the already-scaled exponent (core.py:747-752 applies the
@@ -61,7 +61,9 @@ def demodblock(data, filters, system="NTSC", freq_hz=40e6, blocklen=32768,
     `audio` is None or a dict {'left': ns, 'right': ns} with lowbin, nbins,
     a1_freq, low_freq and filt1 per channel.  Returns a dict with the same
     keys the reference returns; 'video' is a dict of float32 arrays instead
-    of a record array.
+    of a record array.  `out_dtype=np.float64` keeps the video and rfhpf
+    outputs in FP64 (the reference casts them to float32) for error
+    statistics.
     """
     F = filters
     if fftdata is not None:
@@ -74,7 +76,7 @@ def demodblock(data, filters, system="NTSC", freq_hz=40e6, blocklen=32768,
     rv = {}
     hp = np.fft.ifft(X * F["Frfhpf"]).real
     end = -blockcut_end - video_rot
-    rv["rfhpf"] = hp[blockcut - video_rot:end if end != 0 else None].astype(np.float32)
+    rv["rfhpf"] = hp[blockcut - video_rot:end if end != 0 else None].astype(out_dtype)
 
     if pal_notch and system == "PAL":
         X = notch_v4300d(X, blocklen, freq_hz / 1e6)
@@ -89,13 +91,13 @@ def demodblock(data, filters, system="NTSC", freq_hz=40e6, blocklen=32768,
     v05 = np.roll(np.fft.ifft(D * F["FVideo05"]).real, -F["F05_offset"])
     vburst = np.roll(np.fft.ifft(D * F["FVideoBurst"]).real, -F["FVideoBurst_offset"])
     out = {
-        "demod": video.astype(np.float32),
-        "demod_raw": demod.astype(np.float32),
-        "demod_05": v05.astype(np.float32),
-        "demod_burst": vburst.astype(np.float32),
+        "demod": video.astype(out_dtype),
+        "demod_raw": demod.astype(out_dtype),
+        "demod_05": v05.astype(out_dtype),
+        "demod_burst": vburst.astype(out_dtype),
     }
     if system == "PAL":
-        out["demod_pilot"] = np.fft.ifft(D * F["FVideoPilot"]).real.astype(np.float32)
+        out["demod_pilot"] = np.fft.ifft(D * F["FVideoPilot"]).real.astype(out_dtype)
     if cut:
         out = {k: v[blockcut:-blockcut_end] for k, v in out.items()}
     rv["video"] = out
@@ -111,7 +113,7 @@ def demodblock(data, filters, system="NTSC", freq_hz=40e6, blocklen=32768,
         for ch in ("left", "right"):
             a = audio[ch]
             a1 = np.fft.ifft(audio_slice(X, a.lowbin, a.nbins, blocklen) * a.filt1)
-            chans.append((fm_discriminate(a1, a.a1_freq) + a.low_freq).astype(np.float32))
+            chans.append((fm_discriminate(a1, a.a1_freq) + a.low_freq).astype(out_dtype))
         fdiv = blocklen // len(chans[0])
         if cut:
             chans = [c[blockcut // fdiv:-blockcut_end // fdiv] for c in chans]

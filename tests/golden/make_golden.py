@@ -48,8 +48,14 @@ by ldgpu.synth, and saves small .npz fixtures:
                         rfhpf standard deviation, error sample indices, the
                         merged error list and the final dropout lines/ranges.
 
-Nothing at test time reads /root/reference; only this script does.
-Usage: python tests/golden/make_golden.py
+  audio_slices.npz   -- the reference's _downscale_audio_to_output (core.py:
+                        1493-1533) on hand-made run boundaries that start
+                        before the audio buffer (both bounds negative, and a
+                        start below -len that numpy clamps to 0).
+
+Nothing at test time reads the reference; only this script does.
+Usage: python tests/golden/make_golden.py --ref <ld-decode checkout> [fixture]
+(or set LDDECODE_REF to the checkout instead of --ref).
 """
 
 import hashlib
@@ -58,7 +64,21 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+
+
+def _take_ref(argv):
+    """The reference checkout: --ref PATH (removed from argv) or $LDDECODE_REF."""
+    if "--ref" in argv:
+        i = argv.index("--ref")
+        path = argv[i + 1]
+        del argv[i:i + 2]
+        return path
+    return os.environ.get("LDDECODE_REF")
+
+
+REF = _take_ref(sys.argv)
+if not REF or not os.path.isdir(os.path.join(REF, "lddecode")):
+    sys.exit("usage: make_golden.py --ref <ld-decode checkout> [fixture]  (or LDDECODE_REF=<checkout>)")
 
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
 sys.dont_write_bytecode = True
@@ -539,6 +559,35 @@ def audio_fixture():
     np.savez_compressed(os.path.join(HERE, "audio_downscale.npz"), **out)
 
 
+# (name, audio length, locs): run boundaries before the buffer's start
+AUDIO_SLICE_CASES = [
+    ("both_negative", 28800, [-90.4, -61.7, -33.2, -4.9]),
+    ("below_minus_len", 28800, [-40000.2, 7.9, 35.3, 63.6]),
+    ("below_minus_len_neg_end", 28800, [-40000.6, -100.2, -71.9]),
+]
+
+
+def audio_slices_fixture():
+    out = {}
+    sp = refcore.SysParams_NTSC
+    rng = np.random.default_rng(77)
+    for name, alen, locs in AUDIO_SLICE_CASES:
+        left = (sp["audio_lfreq"] + rng.integers(-150000, 150000, alen)).astype(np.float32)
+        right = (sp["audio_rfreq"] + rng.integers(-150000, 150000, alen)).astype(np.float32)
+        locs = np.array(locs, dtype=np.float64)
+        swow = 1.0 + 0.001 * np.arange(len(locs), dtype=np.float64)
+        arange = np.arange(len(locs), dtype=np.float64)
+        o16, failed = refcore._downscale_audio_to_output(arange, locs, swow, left, right,
+                                                         sp["audio_lfreq"], sp["audio_rfreq"])
+        out[name + "_left"] = left
+        out[name + "_right"] = right
+        out[name + "_locs"] = locs
+        out[name + "_swow"] = swow
+        out[name + "_out"] = o16
+        out[name + "_failed"] = np.array(failed)
+    np.savez_compressed(os.path.join(HERE, "audio_slices.npz"), **out)
+
+
 def ac3_fixture():
     from lddecode import ac3rf
     sys.path.insert(0, REPO)
@@ -601,6 +650,9 @@ def main():
     if sys.argv[1:] == ["notch"]:
         notch_fixture()
         return
+    if sys.argv[1:] == ["audio_slices"]:
+        audio_slices_fixture()
+        return
     if sys.argv[1:] == ["lds"]:
         lds_fixture()
         return
@@ -609,6 +661,7 @@ def main():
         rftbc_fixture("PAL", seed=22)
         return
     audio_fixture()
+    audio_slices_fixture()
     ac3_fixture()
     lut_fixture()
     for i, (name, kw) in enumerate(CONFIGS.items()):

@@ -95,3 +95,30 @@ def test_field_clocks_vectorised_equals_scalar(system, freq):
             o = av_offset(rf, int(startloc[i]), bool(isfirst[i]), freq, lfw)
             t0, sg, ntk, nx = field_clock(rf.SysParams["line_period"], int(linecount[i]), o, freq)
             assert (off[j], gap, nt[j], nxt[j]) == (t0, sg, ntk, nx), (i, off[j], t0)
+
+
+@pytest.mark.parametrize("name", ["both_negative", "below_minus_len", "below_minus_len_neg_end"])
+def test_runs_before_buffer_follow_reference_slices(name):
+    """Runs that start before the audio buffer (tests/golden/audio_slices.npz,
+    the reference's _downscale_audio_to_output on hand-made boundaries): both
+    bounds negative wrap to the buffer's end, a start below -len clamps to 0,
+    and each mean divides by the slice's own length."""
+    g = golden("audio_slices")
+    sp = sysparams("NTSC")
+    locs = g[name + "_locs"]
+    arange = np.arange(len(locs), dtype=np.float64)
+    out, failed = A.to_output(arange, locs, g[name + "_swow"], g[name + "_left"], g[name + "_right"],
+                              sp["audio_lfreq"], sp["audio_rfreq"])
+    np.testing.assert_array_equal(out, g[name + "_out"])
+    assert failed == bool(g[name + "_failed"])
+
+
+def test_run_across_buffer_start_is_muted():
+    """A run from before the buffer's start to after it is an empty numpy
+    slice, whose mean makes the reference raise ZeroDivisionError; the
+    restatement mutes that sample and reports it."""
+    sp = sysparams("NTSC")
+    a = np.full(1000, sp["audio_lfreq"], dtype=np.float32)
+    locs = np.array([-14.3, 13.7, 41.2])
+    out, failed = A.to_output(np.arange(3.0), locs, np.ones(3), a, a, sp["audio_lfreq"], sp["audio_rfreq"])
+    assert failed and out[0] == 0 and out[1] == 0

@@ -69,3 +69,49 @@ def test_audio_downscale_located_equals_host(cuda_ok, system):
                     assert np.array_equal(slots[i * stride:i * stride + m], out[offs[i]:offs[i + 1]])
     finally:
         rf.close()
+
+
+@pytest.mark.parametrize("dtype", ["float32"])
+def test_audio_runs_before_buffer_start(cuda_ok, dtype):
+    """A field whose first output samples fall before its audio buffer (a
+    negative time offset and a first line near the buffer's start): runs
+    with both bounds negative wrap to the buffer's end as the reference's
+    slices do, the run across the start is muted (the reference's mean of
+    that empty slice raises), and the GPU equals the host restatement."""
+    import ctypes
+
+    import torch
+    from ldgpu import RFDecode
+    from ldgpu import lib as L
+    from ldgpu.audio import _AUDIO_DTYPE, downscale_audio, field_clock
+    rf = RFDecode(system="NTSC", decode_analog_audio=44100, decode_digital_audio=False)
+    try:
+        sp = rf.SysParams
+        rng = np.random.default_rng(5)
+        linecount, alen, freq, toff = 263, 28800, 44100, -1.2e-4
+        n = linecount + 12
+        wow = 1 + 0.002 * np.sin(np.arange(n) / 37.0)
+        lineinfo = 100.5 + np.concatenate([[0], np.cumsum(wow[:-1] * rf.linelen)])
+        left = (sp["audio_lfreq"] + rng.integers(-150000, 150000, alen)).astype(dtype)
+        right = (sp["audio_rfreq"] + rng.integers(-150000, 150000, alen)).astype(dtype)
+        want, _ = downscale_audio({"audio_left": left, "audio_right": right}, lineinfo, rf, linecount, toff, freq)
+        off, soundgap, nticks, _ = field_clock(sp["line_period"], linecount, toff, freq)
+        dl, dr = torch.from_numpy(left).cuda(), torch.from_numpy(right).cuda()
+        dli = torch.from_numpy(lineinfo).cuda()
+        out = torch.full((2 * (nticks - 1),), 12345, dtype=torch.int16, device="cuda")
+        muted = torch.zeros(1, dtype=torch.int32, device="cuda")
+        d = np.zeros(1, _AUDIO_DTYPE)
+        d["audio_left"], d["audio_right"], d["audio_len"] = dl.data_ptr(), dr.data_ptr(), alen
+        d["linelocs"], d["nlines"], d["nticks"] = dli.data_ptr(), n, nticks
+        d["timeoffset"], d["soundgap"], d["out"] = off, soundgap, out.data_ptr()
+        p = L.AudioParams(float(sp["line_period"]), float(rf.linelen), float(rf.Filters["audio_fdiv"]),
+                          float(sp["audio_lfreq"]), float(sp["audio_rfreq"]))
+        descs = (L.AudioField * 1).from_buffer_copy(d.tobytes())
+        L.check(rf._ctx._lib.ldg_audio_downscale(rf._ctx.handle, descs, 1, ctypes.byref(p), muted.data_ptr(), 1))
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert muted.item() == 1
+        assert np.array_equal(got, want)
+        assert want[0] != 0  # the first runs (both bounds negative) are not muted
+    finally:
+        rf.close()
