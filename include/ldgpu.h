@@ -597,6 +597,30 @@ int64_t ldg_abi_sizeof(const char* name);
  * field's phase_adjust output when first_field > 0. */
 int ldg_lines_refine(ldg_ctx* ctx, const ldg_lines_args* args);
 
+/* ---- EFM phase-locked loop (efm_pll.EFM_PLL, efm_pll.py:80-244) ----
+ * Host code (the loop is serial and edge-driven): T-values from the int16
+ * EFM output of the demodulator, bit-identical to the reference's.  One PLL
+ * per decoded stream; its state carries from call to call (field to field,
+ * as LDdecode.writeout feeds it, core.py:3918-3925).  A PLL is not safe for
+ * concurrent use; different PLLs may run on different threads. */
+typedef struct ldg_efm_pll ldg_efm_pll;
+
+/* EFM_PLL() (efm_pll.py:100-122). */
+int ldg_efm_pll_create(ldg_efm_pll** out);
+int ldg_efm_pll_destroy(ldg_efm_pll* pll);
+
+/* EFM_PLL.process(inputBuffer) (efm_pll.py:124-167, pushEdge 169-240):
+ * `in` n int16 samples (host memory); the T-values of this call go to
+ * out[0 .. *out_count).  out_cap >= n is required, as the reference sizes
+ * its result buffer to the input (the count is far smaller: at most one
+ * T-value per three loop periods of ~9.3 samples). */
+int ldg_efm_pll_process(ldg_efm_pll* pll, const int16_t* in, int64_t n, int8_t* out, int64_t out_cap,
+                        int64_t* out_count);
+
+/* The loop state, for tests: dstate = {delta, currentPeriod, phaseAdjust,
+ * refClockTime}, istate = {zcPreviousInput, frequencyHysteresis, tCounter}. */
+int ldg_efm_pll_state(const ldg_efm_pll* pll, double* dstate, int32_t* istate);
+
 #ifdef __cplusplus
 }
 #endif

@@ -201,6 +201,10 @@ SIGNATURES = {
     "ldg_ac3_dpll_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_double]),
     "ldg_ac3_dpll_destroy": (None, [c_p]),
     "ldg_ac3_dpll_reclock": (ctypes.c_int, [c_p, c_p, c_p, ctypes.c_int64, c_p, ctypes.POINTER(ctypes.c_int64)]),
+    "ldg_efm_pll_create": (ctypes.c_int, [ctypes.POINTER(c_p)]),
+    "ldg_efm_pll_destroy": (ctypes.c_int, [c_p]),
+    "ldg_efm_pll_process": (ctypes.c_int, [c_p, c_p, c_i64, c_p, c_i64, ctypes.POINTER(c_i64)]),
+    "ldg_efm_pll_state": (ctypes.c_int, [c_p, c_p, c_p]),
 }
 
 # ABI of the library this binding is written for (LDG_ABI_VERSION in

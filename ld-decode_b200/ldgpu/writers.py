@@ -13,9 +13,12 @@ appends one field at a time in writeout (core.py:3918-4015):
                 ffmpeg for a .tbc.ldf (core.py:3587-3589, 4005-4012), here
                 they go to <name>.rftbc as the raw samples ffmpeg would get.
 
-The .efm file holds the EFM PLL's output (efm_pll.EFM_PLL, serial on the
-host) and the .tbc.db metadata is SQLite; both stay with the reference's
-own code.  The batched path hands whole batches of fields over at once;
+  <name>.efm    the EFM PLL's T-values of every field's EFM samples
+                (efm_pll.EFM_PLL over the fields in order, core.py:3583,
+                3924-3925), from the native PLL (ldgpu.efm.EFM_PLL).
+
+The .tbc.db metadata is SQLite and stays with the reference's own code.
+The batched path hands whole batches of fields over at once;
 `FieldWriter(..., background=True)` writes them on a host thread so that
 the files are written while the GPU works on the next batch.
 """
@@ -28,15 +31,21 @@ import numpy as np
 
 class FieldWriter:
     """Appends fields to the reference's output files (see the module
-    docstring).  `audio`, `prefm`, `rftbc` select the optional files, as
-    the reference's analog_audio, write_pre_efm and write_rf_tbc do."""
+    docstring).  `audio`, `efm`, `prefm`, `rftbc` select the optional
+    files, as the reference's analog_audio, digital_audio, write_pre_efm
+    and write_rf_tbc do."""
 
-    def __init__(self, fname_out, audio=False, prefm=False, rftbc=False, background=False):
+    def __init__(self, fname_out, audio=False, prefm=False, rftbc=False, background=False, efm=False):
         self.fname_out = fname_out
         self.video = open(fname_out + ".tbc", "wb")
         self.audio = open(fname_out + ".pcm", "wb") if audio else None
         self.prefm = open(fname_out + ".prefm", "wb") if prefm else None
         self.rftbc = open(fname_out + ".rftbc", "wb") if rftbc else None
+        self.efm = open(fname_out + ".efm", "wb") if efm else None
+        self.efm_pll = None
+        if efm:
+            from .efm import EFM_PLL
+            self.efm_pll = EFM_PLL()
         self.fields_written = 0
         self._q = None
         self._thread = None
@@ -61,6 +70,8 @@ class FieldWriter:
             self.audio.write(self._check(audio, np.int16, "audio").tobytes())
         if efm is not None and self.prefm is not None:
             self.prefm.write(self._check(efm, np.int16, "efm").tobytes())
+        if efm is not None and self.efm is not None:
+            self.efm.write(self.efm_pll.process(self._check(efm, np.int16, "efm")).tobytes())
         if rftbc is not None and self.rftbc is not None:
             self.rftbc.write(self._check(rftbc, np.int16, "rftbc").tobytes())
         self.fields_written += 1
@@ -112,7 +123,7 @@ class FieldWriter:
         if self._q is not None:
             self._q.join()
         self._raise()
-        for f in (self.video, self.audio, self.prefm, self.rftbc):
+        for f in (self.video, self.audio, self.prefm, self.rftbc, self.efm):
             if f is not None:
                 f.flush()
 
@@ -124,9 +135,11 @@ class FieldWriter:
                 self._q.put(None)
                 self._thread.join()
                 self._thread = None
-            for f in (self.video, self.audio, self.prefm, self.rftbc):
+            for f in (self.video, self.audio, self.prefm, self.rftbc, self.efm):
                 if f is not None:
                     f.close()
+            if self.efm_pll is not None:
+                self.efm_pll.close()
 
     def __enter__(self):
         return self

@@ -48,6 +48,10 @@ by ldgpu.synth, and saves small .npz fixtures:
                         rfhpf standard deviation, error sample indices, the
                         merged error list and the final dropout lines/ranges.
 
+  efm_pll.npz        -- the reference's EFM_PLL (efm_pll.py:80-244) over seeded
+                        EFM-like signals (tests/golden/efm_cases.py) fed in
+                        buffers of uneven length: every call's T-values and
+                        the loop state at the end;
   audio_slices.npz   -- the reference's _downscale_audio_to_output (core.py:
                         1493-1533) on hand-made run boundaries that start
                         before the audio buffer (both bounds negative, and a
@@ -588,6 +592,24 @@ def audio_slices_fixture():
     np.savez_compressed(os.path.join(HERE, "audio_slices.npz"), **out)
 
 
+def efm_pll_fixture():
+    from lddecode import efm_pll
+    from efm_cases import EFM_CASES, efm_case, split
+    out = {}
+    for c in EFM_CASES:
+        name = c[0]
+        x, bufs = efm_case(name)
+        pll = efm_pll.EFM_PLL()
+        res = [np.array(pll.process(b), dtype=np.int8) for b in split(x, bufs)]
+        out[name + "_in_sha256"] = np.array(sha(x))
+        out[name + "_t"] = np.concatenate(res)
+        out[name + "_counts"] = np.array([len(r) for r in res], dtype=np.int64)
+        out[name + "_state_f"] = np.array([pll.delta, pll.currentPeriod, pll.phaseAdjust, pll.refClockTime])
+        out[name + "_state_i"] = np.array([pll.zcPreviousInput, pll.frequencyHysteresis, pll.tCounter],
+                                          dtype=np.int64)
+    np.savez_compressed(os.path.join(HERE, "efm_pll.npz"), **out)
+
+
 def ac3_fixture():
     from lddecode import ac3rf
     sys.path.insert(0, REPO)
@@ -650,6 +672,9 @@ def main():
     if sys.argv[1:] == ["notch"]:
         notch_fixture()
         return
+    if sys.argv[1:] == ["efm_pll"]:
+        efm_pll_fixture()
+        return
     if sys.argv[1:] == ["audio_slices"]:
         audio_slices_fixture()
         return
@@ -662,6 +687,7 @@ def main():
         return
     audio_fixture()
     audio_slices_fixture()
+    efm_pll_fixture()
     ac3_fixture()
     lut_fixture()
     for i, (name, kw) in enumerate(CONFIGS.items()):

@@ -57,3 +57,25 @@ def test_background_errors_reach_the_caller(tmp_path):
     with pytest.raises(TypeError):
         w.flush()
     w.close()
+
+
+def test_efm_file_holds_the_reference_pll_output(tmp_path):
+    """<name>.efm: the reference's EFM_PLL output of the fields' EFM samples
+    in order (tests/golden/efm_pll.npz, one seeded signal cut into
+    field-like pieces), written from a background thread."""
+    import sys
+    from conftest import GOLDEN, golden
+    sys.path.insert(0, GOLDEN)
+    from efm_cases import efm_case, split
+    g = golden("efm_pll")
+    x, bufs = efm_case("drift_up")
+    parts = split(x, bufs)
+    name = str(tmp_path / "d")
+    pics = np.zeros((len(parts), 16), dtype=np.uint16)
+    with FieldWriter(name, efm=True, prefm=True, background=True) as w:
+        w.write_batch(pics[:5], None, parts[:5])
+        w.write_batch(pics[5:], None, parts[5:])
+    with open(name + ".efm", "rb") as f:
+        assert f.read() == g["drift_up_t"].tobytes()
+    with open(name + ".prefm", "rb") as f:
+        assert f.read() == x.tobytes()
