@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the CPU-baseline leg (and with it the accuracy check against the oracle)")
+    ap.add_argument("--fft-variant", default="auto", choices=["auto", "stockham", "in_place"],
+                    help="FFT decomposition of the demodulator; auto: autotune_demod picks it (and blocks per "
+                         "CTA) on the capture's first blocks before the warm-up")
     ap.add_argument("--other-system-seconds", type=float, default=2.0,
                     help="also time a capture of this length of the other system (PAL for NTSC) in a "
                          "subprocess and report it under other_system (0: off)")
@@ -205,6 +208,15 @@ def run_gpu(args):
     outs["audio_right"] = torch.empty(nblocks * 991, dtype=torch.float32, device="cuda")
     ptrs = {k: v.data_ptr() for k, v in outs.items()}
     import types
+
+    # FFT decomposition and blocks per CTA: fixed, or timed on the capture's first blocks
+    tune = None
+    if args.fft_variant == "auto":
+        from ldgpu.batch import autotune_demod
+        nt = min(nblocks, 16 * torch.cuda.get_device_properties(local).multi_processor_count)
+        tune = autotune_demod(rf, cap.data_ptr(), nt, U, ptrs, mtf_level=1, stream=stream)
+    else:
+        rf.fft_variant = {"stockham": 0, "in_place": 1}[args.fft_variant]
 
     def demod():
         rf.demod_blocks_device(cap.data_ptr(), nblocks, U, ptrs, mtf_level=1, stream=sh)
@@ -601,12 +613,18 @@ def run_gpu(args):
                               "chunk c+1; after_last_demod is the exposed tail of a step run alone "
                               "(isolated_step_ms); ms_per_step runs the steps back to back on two buffer sets, "
                               "so a step's tail overlaps the next step's demod"},
+        "autotune": None if tune is None else {
+            "best": {"fft": ("stockham", "in_place")[tune["best"][0]], "blocks_per_cta": tune["best"][1]},
+            "ms": {f"{('stockham', 'in_place')[k[0]]}_bpc{k[1]}": v for k, v in tune["ms"].items()},
+            "blocks": tune["blocks"],
+            "swept": "FFT decomposition (Stockham / in-place Cooley-Tukey 16384-point transforms) x blocks per CTA, "
+                     "ldg_demod_blocks on the capture's first blocks; one CTA per block (cluster size 1)"},
         "linelocs_host_ms": {k: v / args.steps for k, v in loc.timing.items()},
         "linelocs_chain": {"threads": loc.threads, "equals_sequential_walk": chain_check,
                            "segments": segs, "host_decoded": loc.stats["host"] / args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "ldg::demod_kernel",
+                     "kernel": "ldg::demod_ip_kernel" if rf.fft_variant == 1 else "ldg::demod_kernel",
                      "algorithmic_bytes_per_launch": demod_bytes},
         "tbc_roofline": {"achieved": tbc_bytes / (statistics.median(tbc_ms) * 1e-3) / 1e9, "unit": "GB/s"},
         "dropouts": {"ms_all_fields": drop_med, "us_per_field": 1e3 * drop_med / nf, "dropouts_found": drop_total,
@@ -973,7 +991,7 @@ def run_mixed(args):
                         locate_rfs=loc_rfs, pipeline=args.mixed_pipeline, reserve_sms=args.reserve_sms)
         st = mb.stream
         if tune is None:
-            tune = autotune(queue, st, grabs=(1, 2, 4, 8), ctas=(0, 2 * sms), reps=2)
+            tune = autotune(queue, st, grabs=(1, 2, 4, 8), ctas=(0, 2 * sms), reps=2, variants=(0, 1))
         for _ in range(args.warmup):
             mb.run()
         torch.cuda.synchronize()
@@ -1049,10 +1067,12 @@ def run_mixed(args):
         "roofline": {"bound": "hbm", "achieved": alg / (dsum * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (dsum * 1e-3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
                      "kernel": "ldg::demod_queue_kernel"},
-        "autotune": {"best": {"grab": tune["best"][0], "ctas": tune["best"][1] or sms},
-                     "ms": {f"grab{k[0]}_ctas{k[1] or sms}": v for k, v in tune["ms"].items()},
-                     "swept": "blocks per queue pop and persistent CTAs; the FFT decomposition (16384-point "
-                              "complex, radix 16-16-16-4 in one CTA) and cluster size (1) are fixed"},
+        "autotune": {"best": {"grab": tune["best"][0], "ctas": tune["best"][1] or sms,
+                              "fft": ("stockham", "in_place")[tune["best"][2]]},
+                     "ms": {f"{('stockham', 'in_place')[k[2]]}_grab{k[0]}_ctas{k[1] or sms}": v
+                            for k, v in tune["ms"].items()},
+                     "swept": "FFT decomposition (Stockham / in-place Cooley-Tukey 16384-point transforms), blocks "
+                              "per queue pop and persistent CTAs; one CTA per block (cluster size 1)"},
         "synth_s": gen_s,
         "gpu_launches": int(launches),
         "clocks": clocks,

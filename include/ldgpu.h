@@ -225,6 +225,26 @@ int ldg_demod_status(ldg_ctx* ctx, int32_t* flags);
  * the spectrum before).  0, 0 turns it off (the default). */
 int ldg_set_notch(ldg_ctx* ctx, int32_t lo, int32_t hi);
 
+/* FFT decomposition of the demodulator -- no counterpart in the reference
+ * (its transforms are scipy's).  Both compute every output from the same
+ * float32 spectra and filters, to the same accuracy; they differ in the
+ * order of the float32 roundings and in speed:
+ *   LDG_VARIANT_STOCKHAM  16384-point Stockham passes of radix 16, 16, 16, 4
+ *                         (two barriers per pass), spectra in bin order;
+ *   LDG_VARIANT_IN_PLACE  in-place Cooley-Tukey stages of the same radices
+ *                         (one barrier per stage), spectra in digit-reversed
+ *                         position order between the transforms.
+ * The default is LDG_VARIANT_STOCKHAM; ldgpu.batch.autotune times both. */
+enum { LDG_VARIANT_STOCKHAM = 0, LDG_VARIANT_IN_PLACE = 1 };
+int ldg_set_demod_variant(ldg_ctx* ctx, int32_t variant);
+int ldg_get_demod_variant(ldg_ctx* ctx, int32_t* variant);
+
+/* ldg_demod_blocks' schedule (no counterpart in the reference): each CTA
+ * demodulates `blocks_per_cta` consecutive blocks (1..64) in one scratch
+ * slot; 0 (the default) takes 2 for batches of at least 16 blocks per SM
+ * and 1 below.  Outputs do not depend on it. */
+int ldg_set_demod_schedule(ldg_ctx* ctx, int32_t blocks_per_cta);
+
 /* Device scratch the demodulator uses for a batch of `nblocks` blocks
  * (bytes; parked spectra, one slot per resident CTA). */
 int ldg_demod_scratch_bytes(ldg_ctx* ctx, int64_t nblocks, int64_t* bytes);
@@ -302,6 +322,10 @@ int ldg_queue_submit(ldg_queue* q, const ldg_work_item* items, int32_t n);
 /* Scheduling: `grab` consecutive blocks per pop (1..64), `ctas` persistent
  * CTAs (0: one per SM; at most 4 x SMs).  Default 1, 0. */
 int ldg_queue_set_schedule(ldg_queue* q, int32_t grab, int32_t ctas);
+
+/* FFT decomposition of the queue's launch (as ldg_set_demod_variant):
+ * -1 (the default) takes the first submitted item's context's. */
+int ldg_queue_set_variant(ldg_queue* q, int32_t variant);
 
 /* Blocks submitted and the CTAs a run launches. */
 int ldg_queue_info(ldg_queue* q, int64_t* total_blocks, int32_t* grid);

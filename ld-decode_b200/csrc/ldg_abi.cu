@@ -15,6 +15,7 @@
 
 #include "ldg_copy.cuh"
 #include "ldg_demod.cuh"
+#include "ldg_fft_ip.cuh"
 #include "ldg_dropouts.cuh"
 #include "ldg_fft.cuh"
 #include "ldg_noalloc.h"
@@ -76,6 +77,13 @@ struct ldg_ctx {
     double a_low[2] = {0, 0};
     float2* d_tw16 = nullptr;  // W_16384^i
     float2* d_tw32 = nullptr;  // W_32768^k, k <= 8192
+    // in-place variant: per filter the bin-pair table (ip::kPairs float4) and,
+    // for the RFVideo filters, the position-order table (kM float2); W_N^k per pair
+    float4* d_fpair[LDG_NFILTERS] = {};
+    float2* d_fpos[LDG_NFILTERS] = {};
+    float2* d_twpair = nullptr;
+    int variant = ldg::kVariantStockham;
+    int blocks_per_cta = 0;  // ldg_demod_blocks: consecutive blocks per CTA (0: 2 for large batches, else 1)
     float* d_lut = nullptr;
     float2* d_scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -126,6 +134,18 @@ struct ldg_ctx {
 };
 
 namespace {
+
+// The FFT decomposition and the in-place variant's filter layouts (ctx->mu held).
+void variant_tables(const ldg_ctx* c, ldg::DemodParams* p) {
+    p->variant = c->variant;
+    p->fp_rfhpf = c->d_fpair[LDG_F_RFHPF];
+    const int fslot[4] = {LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT};
+    for (int o = 0; o < 4; ++o) p->fp_video[o] = c->d_fpair[fslot[o]];
+    p->fp_efm = c->d_fpair[LDG_F_EFM];
+    p->g_pos = c->d_fpos[LDG_F_VIDEO_G];
+    p->godd_pos = c->d_fpos[LDG_F_VIDEO_G_ODD];
+    p->tw_pair = c->d_twpair;
+}
 
 int grow(void** p, size_t* cap, size_t need) {
     if (need <= *cap) return LDG_OK;
@@ -267,10 +287,18 @@ int ldg_ctx_create(ldg_ctx** out, int32_t device, int32_t system, int32_t blockl
         const double ang = -two_pi * (double)k / ldg::kN;
         t32[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
     }
+    std::vector<float2> twp(ldg::ip::kPairs);
+    for (int u = 0; u < ldg::ip::kPairs; ++u) {
+        const int k = ldg::ip::bin_of(ldg::ip::pair_pos(u));
+        const double ang = -two_pi * (double)k / ldg::kN;
+        twp[u] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
     if (cudaMalloc(&c->d_tw16, t16.size() * sizeof(float2)) != cudaSuccess ||
         cudaMemcpy(c->d_tw16, t16.data(), t16.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMalloc(&c->d_tw32, t32.size() * sizeof(float2)) != cudaSuccess ||
         cudaMemcpy(c->d_tw32, t32.data(), t32.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc(&c->d_twpair, twp.size() * sizeof(float2)) != cudaSuccess ||
+        cudaMemcpy(c->d_twpair, twp.data(), twp.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess || cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
         const std::string msg = cudaGetErrorString(cudaGetLastError());
         ldg_ctx_destroy(c);
@@ -285,6 +313,9 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     DeviceGuard g(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& f : c->d_filter) cudaFree(f);
+    for (auto& f : c->d_fpair) cudaFree(f);
+    for (auto& f : c->d_fpos) cudaFree(f);
+    cudaFree(c->d_twpair);
     for (auto& a : c->d_audio) cudaFree(a);
     cudaFree(c->d_tw16);
     cudaFree(c->d_tw32);
@@ -327,9 +358,50 @@ int ldg_set_filter(ldg_ctx* c, int32_t which, const double* reim, int64_t nbins)
     DeviceGuard g(c->device);
     std::vector<float2> h(nbins);
     for (int64_t k = 0; k < nbins; ++k) h[k] = make_float2((float)reim[2 * k], (float)reim[2 * k + 1]);
+    // the in-place variant's layouts of the same float32 values: per bin pair
+    // u the bins k = bin_of(pair_pos(u)) and M - k (M itself for k = 0), and
+    // for the RFVideo filters every bin at its position
+    std::vector<float4> fp(ldg::ip::kPairs);
+    for (int u = 0; u < ldg::ip::kPairs; ++u) {
+        const int k = ldg::ip::bin_of(ldg::ip::pair_pos(u));
+        const int m = k == 0 ? ldg::kM : ldg::kM - k;
+        fp[u] = make_float4(h[k].x, h[k].y, h[m].x, h[m].y);
+    }
+    const bool pos = which == LDG_F_VIDEO_G || which == LDG_F_VIDEO_G_ODD;
+    std::vector<float2> fq(pos ? ldg::kM : 0);
+    for (int p = 0; p < (int)fq.size(); ++p) fq[p] = h[ldg::ip::bin_of(p)];
     if (!c->d_filter[which]) LDG_CK(cudaMalloc(&c->d_filter[which], nbins * sizeof(float2)));
+    if (!c->d_fpair[which]) LDG_CK(cudaMalloc(&c->d_fpair[which], fp.size() * sizeof(float4)));
+    if (pos && !c->d_fpos[which]) LDG_CK(cudaMalloc(&c->d_fpos[which], fq.size() * sizeof(float2)));
     LDG_CK(cudaStreamSynchronize(c->stream));
     LDG_CK(cudaMemcpy(c->d_filter[which], h.data(), nbins * sizeof(float2), cudaMemcpyHostToDevice));
+    LDG_CK(cudaMemcpy(c->d_fpair[which], fp.data(), fp.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    if (pos) LDG_CK(cudaMemcpy(c->d_fpos[which], fq.data(), fq.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    return LDG_OK;
+}
+
+int ldg_set_demod_variant(ldg_ctx* c, int32_t variant) {
+    if (!c) return fail(LDG_ERR_ARG, "ldg_set_demod_variant: NULL context");
+    if (variant < 0 || variant >= ldg::kNumVariants)
+        return fail(LDG_ERR_ARG, "ldg_set_demod_variant: variant must be LDG_VARIANT_STOCKHAM or LDG_VARIANT_IN_PLACE");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->variant = variant;
+    return LDG_OK;
+}
+
+int ldg_set_demod_schedule(ldg_ctx* c, int32_t blocks_per_cta) {
+    if (!c) return fail(LDG_ERR_ARG, "ldg_set_demod_schedule: NULL context");
+    if (blocks_per_cta < 0 || blocks_per_cta > 64)
+        return fail(LDG_ERR_ARG, "ldg_set_demod_schedule: blocks_per_cta must be in [0, 64]");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->blocks_per_cta = blocks_per_cta;
+    return LDG_OK;
+}
+
+int ldg_get_demod_variant(ldg_ctx* c, int32_t* variant) {
+    if (!c || !variant) return fail(LDG_ERR_ARG, "ldg_get_demod_variant: NULL argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    *variant = c->variant;
     return LDG_OK;
 }
 
@@ -429,7 +501,8 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     const long long nb = a->nblocks;
     // one CTA per block; scratch slots for twice the SMs' worth of resident CTAs
     const int nslots = 2 * c->sms;
-    const int per_cta = nb >= 16 * c->sms ? 2 : 1;  // two blocks per CTA amortise its set-up
+    // two blocks per CTA amortise its set-up on large batches, unless set
+    const int per_cta = c->blocks_per_cta ? c->blocks_per_cta : (nb >= 16 * c->sms ? 2 : 1);
     const int grid = (int)((nb + per_cta - 1) / per_cta);
     int rc = grow((void**)&c->d_scratch, &c->scratch_bytes, (size_t)nslots * ldg::kScratchPerCta);
     if (rc) return rc;
@@ -532,6 +605,7 @@ int ldg_demod_blocks(ldg_ctx* c, const ldg_demod_args* a) {
     p.blocks_per_cta = per_cta;
     p.notch_lo = c->notch_lo;
     p.notch_hi = c->notch_hi;
+    variant_tables(c, &p);
 
     cudaError_t e = ldg::launch_demod(p, grid, st);
     if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("demod launch: ") + cudaGetErrorString(e));
@@ -1039,6 +1113,7 @@ int device_params(ldg_ctx* c, const ldg_demod_args* a, const std::string& who, D
     p->tw32 = c->d_tw32;
     p->notch_lo = c->notch_lo;
     p->notch_hi = c->notch_hi;
+    variant_tables(c, p);
     return LDG_OK;
 }
 

@@ -21,6 +21,7 @@
 #include "ldg_attr.cuh"
 #include "ldg_demod.cuh"
 #include "ldg_fft.cuh"
+#include "ldg_fft_ip.cuh"
 
 namespace ldg {
 
@@ -292,6 +293,45 @@ __device__ __forceinline__ void discard_scratch(float2* base) {
         asm volatile("discard.global.L2 [%0], 128;" ::"l"(b + (size_t)l * 128) : "memory");
 }
 
+// FM discriminator: demod[2m] from (z_e[m], z_o[m-1]), demod[2m+1] from
+// (z_o[m], z_e[m]) -- the even samples parked (parkZ), the odd ones in S,
+// both in natural order; the clipped pairs replace X in the parking slot.
+__device__ __forceinline__ void discriminate(const DemodParams& p, int blk, const float2* S, float2* parkX,
+                                             const float2* parkZ) {
+    {
+        const float kfs = p.fs_hz / kTwoPi;
+        const float clip_hi = p.fs_hz * 0.75f;
+        float* oraw = p.o_raw ? p.o_raw + (long long)blk * p.s_video.len : nullptr;
+        const int vs = p.s_video.start, vl = p.s_video.len;
+        auto disc_store = [&](int m, float de, float dodd) {
+            if (oraw) {
+                const int i0 = 2 * m - vs;
+                if (i0 >= 0 && i0 + 1 < vl && ((reinterpret_cast<uintptr_t>(oraw + i0) & 7) == 0)) {
+                    __stcs(reinterpret_cast<float2*>(oraw + i0), make_float2(de, dodd));
+                } else {
+                    if (i0 >= 0 && i0 < vl) __stcs(oraw + i0, de);
+                    if (i0 + 1 >= 0 && i0 + 1 < vl) __stcs(oraw + i0 + 1, dodd);
+                }
+            }
+            parkX[m] = make_float2(fminf(fmaxf(de, 1500000.0f), clip_hi), fminf(fmaxf(dodd, 1500000.0f), clip_hi));
+        };
+        // two samples per step, the parked (L2) loads first
+#pragma unroll 1
+        for (int m = threadIdx.x; m < kM; m += 2 * kThreads) {
+            const int mb = m + kThreads;
+            const float2 zea = parkZ[m], zeb = parkZ[mb];
+            const float2 zoa = S[pad(m)], zob = S[pad(mb)];
+            const float2 zpa = m ? S[pad(m - 1)] : zoa, zpb = S[pad(mb - 1)];
+            const float dea = (m == 0) ? 0.0f : fm_disc(zea, zpa, kfs);
+            const float doa = fm_disc(zoa, zea, kfs);
+            const float deb = fm_disc(zeb, zpb, kfs);
+            const float dob = fm_disc(zob, zeb, kfs);
+            disc_store(m, dea, doa);
+            disc_store(mb, deb, dob);
+        }
+    }
+}
+
 // One block: every requested output of block `blk` of p.  parkX/parkZ: this
 // CTA's scratch (kScratchPerCta).  Ends with the CTA's threads in step.
 __device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float2* S, float2* A, const Tables& t,
@@ -338,40 +378,7 @@ __device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float
     fft16k<true>(S, t, AnalyticLoader{parkX, p.f_g, p.f_godd, false}, ParkStorer{parkZ});
     fft16k<true>(S, t, AnalyticLoader{parkX, p.f_g, p.f_godd, true});
 
-    // ---- FM discriminator: demod[2m] from (z_e[m], z_o[m-1]), demod[2m+1]
-    // from (z_o[m], z_e[m]); the clipped pairs replace X in the parking slot
-    {
-        const float kfs = p.fs_hz / kTwoPi;
-        const float clip_hi = p.fs_hz * 0.75f;
-        float* oraw = p.o_raw ? p.o_raw + (long long)blk * p.s_video.len : nullptr;
-        const int vs = p.s_video.start, vl = p.s_video.len;
-        auto disc_store = [&](int m, float de, float dodd) {
-            if (oraw) {
-                const int i0 = 2 * m - vs;
-                if (i0 >= 0 && i0 + 1 < vl && ((reinterpret_cast<uintptr_t>(oraw + i0) & 7) == 0)) {
-                    __stcs(reinterpret_cast<float2*>(oraw + i0), make_float2(de, dodd));
-                } else {
-                    if (i0 >= 0 && i0 < vl) __stcs(oraw + i0, de);
-                    if (i0 + 1 >= 0 && i0 + 1 < vl) __stcs(oraw + i0 + 1, dodd);
-                }
-            }
-            parkX[m] = make_float2(fminf(fmaxf(de, 1500000.0f), clip_hi), fminf(fmaxf(dodd, 1500000.0f), clip_hi));
-        };
-        // two samples per step, the parked (L2) loads first
-#pragma unroll 1
-        for (int m = threadIdx.x; m < kM; m += 2 * kThreads) {
-            const int mb = m + kThreads;
-            const float2 zea = parkZ[m], zeb = parkZ[mb];
-            const float2 zoa = S[pad(m)], zob = S[pad(mb)];
-            const float2 zpa = m ? S[pad(m - 1)] : zoa, zpb = S[pad(mb - 1)];
-            const float dea = (m == 0) ? 0.0f : fm_disc(zea, zpa, kfs);
-            const float doa = fm_disc(zoa, zea, kfs);
-            const float deb = fm_disc(zeb, zpb, kfs);
-            const float dob = fm_disc(zob, zeb, kfs);
-            disc_store(m, dea, doa);
-            disc_store(mb, deb, dob);
-        }
-    }
+    discriminate(p, blk, S, parkX, parkZ);
     __syncthreads();
 
     // ---- spectrum D of the clipped demod, then the video outputs
@@ -402,32 +409,295 @@ __device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float
 struct CtaSmem {
     float2* S;
     float2* A;
-    Tables t;
+    Tables t;       // Stockham pass tables (t.s3 / t.s4 only for the Stockham variant) and the 1024-point ones
+    ip::Twiddles tw;  // in-place stage tables (in-place variant)
 };
 
-// Carves the dynamic shared memory and loads the pass twiddle tables.
+// Carves the dynamic shared memory -- working set, audio bands, 1024-point
+// tables, then the 16384-point tables of the variant -- and loads the tables.
+template <int V>
 __device__ __forceinline__ CtaSmem cta_setup(float2* smem, const float2* tw16, const float2* tw32) {
     CtaSmem c;
     c.S = smem;
     c.A = smem + padded(kM);
     float2* s2 = c.A + 2 * padded(1024);
-    float2* s3 = s2 + kS2;
-    float2* s4 = s3 + kS3;
-    load_pass_tables(s2, s3, s4, tw16);
+    float2* s4a = s2 + kS2;
+    float2* rest = s4a + kS4a;
+    load_1k_tables(s2, s4a, tw16);
     c.t.t16 = tw16;
     c.t.t32 = tw32;
     c.t.s2 = s2;
-    c.t.s3 = s3;
-    c.t.s4 = s4;
+    c.t.s4a = s4a;
+    if (V == kVariantStockham) {
+        float2* s3 = rest;
+        float2* s4 = s3 + kS3;
+        load_pass_tables(s3, s4, tw16);
+        c.t.s3 = s3;
+        c.t.s4 = s4;
+        c.tw = {nullptr, nullptr, nullptr};
+    } else {
+        float2* t1 = rest;
+        float2* t2 = t1 + ip::kT1;
+        float2* t3 = t2 + ip::kT2;
+        ip::load_stage_tables(t1, t2, t3, tw16);
+        c.tw = {t1, t2, t3};
+        c.t.s3 = nullptr;
+        c.t.s4 = nullptr;
+    }
     __syncthreads();
     return c;
 }
 
+// ---- the in-place variant: spectra in position order (ldg_fft_ip.cuh)
+
+// X[k] * G[k] at positions p .. p+3 (k = bin_of(p)) from the parked spectrum
+// (position order, X[0] and X[M] packed at position 0) and G at positions;
+// `odd` as AnalyticLoader.
+struct AnalyticLoaderIp {
+    const float2* X;
+    const float2* Gpos;
+    const float2* G;  // natural order: G[0], G[M]
+    bool odd;
+    __device__ void quad(int p, float2 (&v)[4]) const {
+        const float4 x01 = *reinterpret_cast<const float4*>(X + p);
+        const float4 x23 = *reinterpret_cast<const float4*>(X + p + 2);
+        const float4 g01 = __ldg(reinterpret_cast<const float4*>(Gpos + p));
+        const float4 g23 = __ldg(reinterpret_cast<const float4*>(Gpos + p + 2));
+        v[0] = cmul(make_float2(x01.x, x01.y), make_float2(g01.x, g01.y));
+        v[1] = cmul(make_float2(x01.z, x01.w), make_float2(g01.z, g01.w));
+        v[2] = cmul(make_float2(x23.x, x23.y), make_float2(g23.x, g23.y));
+        v[3] = cmul(make_float2(x23.z, x23.w), make_float2(g23.z, g23.w));
+        if (p == 0) {
+            const float2 a = cscale(__ldg(G), x01.x);
+            const float2 b = cscale(__ldg(G + kM), x01.y);
+            v[0] = odd ? csub(a, b) : cadd(a, b);
+        }
+    }
+};
+
+// C2R pre-processing of one bin pair at positions p (bin k) and q (bin M-k)
+// (c2r_pair in position order; p == q for k = M/2).
+__device__ __forceinline__ void c2r_pair_ip(float2* S, int p, int q, float2 hk, float2 hm, float2 wk) {
+    const float2 e = make_float2(0.5f * (hk.x + hm.x), 0.5f * (hk.y - hm.y));
+    const float2 d = make_float2(0.5f * (hk.x - hm.x), 0.5f * (hk.y + hm.y));
+    const float2 o = cmul(d, cconj(wk));
+    S[pad(p)] = make_float2(e.x - o.y, e.y + o.x);
+    if (q != p) S[pad(q)] = make_float2(e.x + o.y, o.x - e.y);
+}
+
+// post_pair in position order: X[k], X[M-k] of the pair at (p, q) from
+// Z[k] = S[p], Z[M-k] = S[q]; parked at p and q; the audio taps use the
+// pair's bin at or below M/2; with F, the C2R input of X * F left at p, q.
+__device__ __forceinline__ void post_pair_ip(float2* S, float2* park, const AudioTaps* au, int p, int q, float2 zk,
+                                             float2 zm, float2 wk, bool hasF, float4 f) {
+    const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    const float2 tt = cmul(wk, o);
+    const float2 xk = cadd(e, tt);
+    const float2 xm = cconj(csub(e, tt));
+    park[p] = xk;
+    if (q != p) park[q] = xm;
+    if (au) {
+        const int k = ip::bin_of(p);
+        const bool low = k <= kM / 2;
+        const int kk = low ? k : kM - k;
+        const float2 xkk = low ? xk : xm;
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch) {
+            const int rel = kk - au->lowbin[ch];
+            if (rel >= 0 && rel <= 512) {
+                const float2 xb = rel < 512 ? xkk : cconj(xkk);
+                au->A[ch * padded(1024) + pad(rel)] = cmul(xb, __ldg(au->filt1[ch] + rel));
+            }
+        }
+    }
+    if (hasF) c2r_pair_ip(S, p, q, cmul(xk, make_float2(f.x, f.y)), cmul(xm, make_float2(f.z, f.w)), wk);
+}
+
+// post_r2c in position order: S holds Z at positions; parks X (position
+// order), taps the audio bands and, with FP, leaves the C2R input of X * F
+// in S.  Thread t takes pairs u = t + kThreads i, two per step, loads first.
+__device__ void post_r2c_ip(float2* S, const float2* twp, float2* park, const float4* FP, const AudioTaps* au) {
+    const int t0 = threadIdx.x;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 1
+    for (int i = 0; i < 8; i += 2) {
+        const int ua = t0 + i * kThreads, ub = ua + kThreads;
+        const int pa = ip::pair_pos(ua), pb = ip::pair_pos(ub);
+        const int qa = ip::partner_pos(pa), qb = ip::partner_pos(pb);
+        const float2 zka = S[pad(pa)], zma = S[pad(qa)];
+        const float2 zkb = S[pad(pb)], zmb = S[pad(qb)];
+        const float2 wa = __ldg(twp + ua), wb = __ldg(twp + ub);
+        float4 fa = zero4, fb = zero4;
+        if (FP) {
+            fa = __ldg(FP + ua);
+            fb = __ldg(FP + ub);
+        }
+        if (pa != 0) post_pair_ip(S, park, au, pa, qa, zka, zma, wa, FP != nullptr, fa);
+        if (pb != 0) {
+            post_pair_ip(S, park, au, pb, qb, zkb, zmb, wb, FP != nullptr, fb);
+        } else {  // bins 0 and M
+            const float x0 = zkb.x + zkb.y, xm = zkb.x - zkb.y;
+            park[0] = make_float2(x0, xm);
+            if (FP) {
+                const float h0 = x0 * fb.x, hm = xm * fb.z;
+                S[0] = make_float2(0.5f * (h0 + hm), 0.5f * (h0 - hm));
+            }
+        }
+    }
+    if (t0 == 0) {  // u = M/2: position 2, bin M/2, its own partner
+        const int u = kM / 2;
+        const float2 z = S[pad(2)];
+        post_pair_ip(S, park, au, 2, 2, z, z, __ldg(twp + u), FP != nullptr, FP ? __ldg(FP + u) : zero4);
+    }
+}
+
+// pre_c2r in position order: the C2R input of X * F in S, X from the parked
+// spectrum (position order).
+__device__ void pre_c2r_ip(float2* S, const float2* twp, const float2* park, const float4* FP) {
+    const int t0 = threadIdx.x;
+#pragma unroll 1
+    for (int i = 0; i < 8; i += 2) {
+        const int ua = t0 + i * kThreads, ub = ua + kThreads;
+        const int pa = ip::pair_pos(ua), pb = ip::pair_pos(ub);
+        const int qa = ip::partner_pos(pa), qb = ip::partner_pos(pb);
+        const float2 xka = park[pa], xma = park[qa], xkb = park[pb], xmb = park[qb];
+        const float4 fa = __ldg(FP + ua), fb = __ldg(FP + ub);
+        const float2 wa = __ldg(twp + ua), wb = __ldg(twp + ub);
+        c2r_pair_ip(S, pa, qa, cmul(xka, make_float2(fa.x, fa.y)), cmul(xma, make_float2(fa.z, fa.w)), wa);
+        if (pb != 0) {
+            c2r_pair_ip(S, pb, qb, cmul(xkb, make_float2(fb.x, fb.y)), cmul(xmb, make_float2(fb.z, fb.w)), wb);
+        } else {
+            const float h0 = xkb.x * fb.x, hm = xkb.y * fb.z;
+            S[0] = make_float2(0.5f * (h0 + hm), 0.5f * (h0 - hm));
+        }
+    }
+    if (t0 == 0) {
+        const int u = kM / 2;
+        const float2 x = park[2];
+        const float4 f = __ldg(FP + u);
+        c2r_pair_ip(S, 2, 2, cmul(x, make_float2(f.x, f.y)), cmul(x, make_float2(f.z, f.w)), __ldg(twp + u));
+    }
+}
+
+// notch_park on the position-order parked spectrum.
+__device__ void notch_park_ip(float2* park, int lo, int hi) {
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    const int n = hi - lo;
+    auto mag = [&](int i) {
+        const float2 x = park[ip::pos_of(lo + i)];
+        return sqrt((double)x.x * (double)x.x + (double)x.y * (double)x.y);
+    };
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s += mag(i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double mean = s / (double)n;
+    double q = 0.0;
+    for (int i = lane; i < n; i += 32) {
+        const double d = mag(i) - mean;
+        q += d * d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+    const double m = mean + sqrt(q / (double)n) * 3.0;
+    unsigned flags = 0;
+    for (int i = lane, j = 0; i < n; i += 32, ++j)
+        if (mag(i) > m) flags |= 1u << j;
+    __syncwarp();
+    for (int i = lane, j = 0; i < n; i += 32, ++j) {
+        if ((flags >> j) & 1u) {
+            const float2 z = make_float2(0.f, 0.f);
+            park[ip::pos_of(lo + i - 1)] = z;
+            park[ip::pos_of(lo + i)] = z;
+            park[ip::pos_of(lo + i + 1)] = z;
+        }
+    }
+}
+
+// demod_block with the in-place transforms: the same outputs from the same
+// steps, spectra in position order.
+__device__ __forceinline__ void demod_block_ip(const DemodParams& p, int blk, float2* S, float2* A, const Tables& t,
+                                               const ip::Twiddles& tw, float2* parkX, float2* parkZ) {
+    if (p.in_kind == 0) {
+        ip::fft16k_fwd(S, tw, InLoader16{static_cast<const int16_t*>(p.in) + (long long)blk * p.in_stride});
+    } else {
+        ip::fft16k_fwd(S, tw, InLoader32{static_cast<const float*>(p.in) + (long long)blk * p.in_stride});
+    }
+    if (p.audio) {
+        for (int idx = threadIdx.x; idx < 2 * 511; idx += kThreads) {
+            const int ch = idx / 511, k = 513 + idx % 511;
+            A[ch * padded(1024) + pad(k)] = make_float2(0.f, 0.f);
+        }
+    }
+    {
+        AudioTaps au{A, {p.a_lowbin[0], p.a_lowbin[1]}, {p.a_filt1[0], p.a_filt1[1]}};
+        post_r2c_ip(S, p.tw_pair, parkX, p.o_rfhpf ? p.fp_rfhpf : nullptr, p.audio ? &au : nullptr);
+    }
+    __syncthreads();
+    if (p.notch_hi > p.notch_lo) {
+        notch_park_ip(parkX, p.notch_lo, p.notch_hi);
+        __syncthreads();
+    }
+    if (p.audio) audio_stage(p, A, t, blk);
+
+    if (p.o_rfhpf) {
+        ip::fft16k_inv(S, tw, SmemIO(),
+                       RealStorer{p.o_rfhpf + (long long)blk * p.s_rfhpf.len, p.s_rfhpf.start, p.s_rfhpf.len, 0});
+    }
+    if (p.o_efm) {
+        pre_c2r_ip(S, p.tw_pair, parkX, p.fp_efm);
+        __syncthreads();
+        ip::fft16k_inv(S, tw, SmemIO(),
+                       EfmStorer{p.o_efm + (long long)blk * p.s_efm.len, p.s_efm.start, p.s_efm.len});
+    }
+
+    ip::fft16k_inv(S, tw, AnalyticLoaderIp{parkX, p.g_pos, p.f_g, false}, ParkStorer{parkZ});
+    ip::fft16k_inv(S, tw, AnalyticLoaderIp{parkX, p.godd_pos, p.f_g, true});
+
+    discriminate(p, blk, S, parkX, parkZ);
+    __syncthreads();
+
+    ip::fft16k_fwd(S, tw, ParkLoader{parkX});
+    int first = -1;
+#pragma unroll
+    for (int o = 0; o < OUT_NVIDEO; ++o)
+        if (first < 0 && p.o_video[o]) first = o;
+    post_r2c_ip(S, p.tw_pair, parkX, first >= 0 ? p.fp_video[first] : nullptr, nullptr);
+    __syncthreads();
+#pragma unroll
+    for (int o = 0; o < OUT_NVIDEO; ++o) {
+        if (p.o_video[o] == nullptr) continue;
+        if (o != first) {
+            pre_c2r_ip(S, p.tw_pair, parkX, p.fp_video[o]);
+            __syncthreads();
+        }
+        ip::fft16k_inv(S, tw, SmemIO(),
+                       RealStorer{p.o_video[o] + (long long)blk * p.s_video.len, p.s_video.start, p.s_video.len,
+                                  p.roll[o]});
+    }
+    __syncthreads();
+    discard_scratch(parkX);
+}
+
+template <int V>
+__device__ __forceinline__ void run_block(const DemodParams& p, int blk, const CtaSmem& c, float2* parkX,
+                                          float2* parkZ) {
+    if (V == kVariantStockham) {
+        demod_block(p, blk, c.S, c.A, c.t, parkX, parkZ);
+    } else {
+        demod_block_ip(p, blk, c.S, c.A, c.t, c.tw, parkX, parkZ);
+    }
+}
+
 }  // namespace
 
-__global__ void __launch_bounds__(kThreads, 1) demod_kernel(const __grid_constant__ DemodParams p) {
-    extern __shared__ float2 smem[];
-    const CtaSmem c = cta_setup(smem, p.tw16, p.tw32);
+namespace {
+
+template <int V>
+__device__ __forceinline__ void demod_body(const DemodParams& p, float2* smem) {
+    const CtaSmem c = cta_setup<V>(smem, p.tw16, p.tw32);
 
     __shared__ int s_got;
     const bool per_block = p.slot_lock != nullptr;
@@ -454,7 +724,7 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const __grid_constan
     const int blk_step = per_block ? 1 : (int)gridDim.x;
     float2* parkX = p.scratch + (size_t)slot * 2 * kM;
     float2* parkZ = parkX + kM;
-    for (; blk < blk_end; blk += blk_step) demod_block(p, blk, c.S, c.A, c.t, parkX, parkZ);
+    for (; blk < blk_end; blk += blk_step) run_block<V>(p, blk, c, parkX, parkZ);
     if (per_block) {
         // every thread is done with the slot's scratch before it is handed on
         __syncthreads();
@@ -469,9 +739,9 @@ __global__ void __launch_bounds__(kThreads, 1) demod_kernel(const __grid_constan
 // CTA pops `grab` consecutive global block indices at a time from *head,
 // finds the capture that holds each (binary search over first_block), keeps
 // that capture's parameters in shared memory, and demodulates the block.
-__global__ void __launch_bounds__(kThreads, 1) demod_queue_kernel(const __grid_constant__ QueueParams q) {
-    extern __shared__ float2 smem[];
-    const CtaSmem c = cta_setup(smem, q.tw16, q.tw32);
+template <int V>
+__device__ __forceinline__ void queue_body(const QueueParams& q, float2* smem) {
+    const CtaSmem c = cta_setup<V>(smem, q.tw16, q.tw32);
     __shared__ DemodParams sp;
     __shared__ long long s_pop;
     __shared__ int s_item;
@@ -502,9 +772,33 @@ __global__ void __launch_bounds__(kThreads, 1) demod_queue_kernel(const __grid_c
                 cur = it;
                 __syncthreads();
             }
-            demod_block(sp, (int)(g - q.first_block[it]), c.S, c.A, c.t, parkX, parkZ);
+            run_block<V>(sp, (int)(g - q.first_block[it]), c, parkX, parkZ);
         }
     }
+}
+
+}  // namespace
+
+// The demodulator with the Stockham transforms (natural-order spectra).
+__global__ void __launch_bounds__(kThreads, 1) demod_kernel(const __grid_constant__ DemodParams p) {
+    extern __shared__ float2 smem[];
+    demod_body<kVariantStockham>(p, smem);
+}
+
+// The demodulator with the in-place transforms (position-order spectra).
+__global__ void __launch_bounds__(kThreads, 1) demod_ip_kernel(const __grid_constant__ DemodParams p) {
+    extern __shared__ float2 smem[];
+    demod_body<kVariantInPlace>(p, smem);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) demod_queue_kernel(const __grid_constant__ QueueParams q) {
+    extern __shared__ float2 smem[];
+    queue_body<kVariantStockham>(q, smem);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) demod_queue_ip_kernel(const __grid_constant__ QueueParams q) {
+    extern __shared__ float2 smem[];
+    queue_body<kVariantInPlace>(q, smem);
 }
 
 // ---- analog audio stage 2 (RFDecode.runfilter_audio_phase2, core.py:884-915)
@@ -564,7 +858,7 @@ __device__ void audio2_filter(float2* S, const Tables& t, const float2* F) {
 // channels; then R2C, the stage-2 filter, C2R, carrier added back.
 __global__ void __launch_bounds__(kThreads, 1) audio2_kernel(const __grid_constant__ Audio2Params p) {
     extern __shared__ float2 smem[];
-    const CtaSmem c = cta_setup(smem, p.tw16, p.tw32);
+    const CtaSmem c = cta_setup<kVariantStockham>(smem, p.tw16, p.tw32);
     const Audio2Seg sg = p.segs[blockIdx.x];
     const int ch = blockIdx.y;
     const int n = sg.len;
@@ -603,24 +897,37 @@ cudaError_t launch_audio2(const Audio2Params& p, int nsegs, cudaStream_t stream)
 }
 
 cudaError_t prepare_demod_queue() {
-    static SmemAttr attr;
-    return attr.ensure(demod_queue_kernel, kSmemBytes);
+    static SmemAttr attr, attr_ip;
+    cudaError_t e = attr.ensure(demod_queue_kernel, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    return attr_ip.ensure(demod_queue_ip_kernel, kSmemBytesIp);
 }
 
 cudaError_t launch_demod_queue(const QueueParams& q, int grid, cudaStream_t stream) {
     cudaError_t e = prepare_demod_queue();
     if (e != cudaSuccess) return e;
     if (q.total <= 0 || grid <= 0) return cudaSuccess;
-    demod_queue_kernel<<<grid, kThreads, kSmemBytes, stream>>>(q);
+    if (q.variant == kVariantInPlace) {
+        demod_queue_ip_kernel<<<grid, kThreads, kSmemBytesIp, stream>>>(q);
+    } else {
+        demod_queue_kernel<<<grid, kThreads, kSmemBytes, stream>>>(q);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_demod(const DemodParams& p, int grid, cudaStream_t stream) {
-    static SmemAttr attr;
+    static SmemAttr attr, attr_ip;
     cudaError_t e = attr.ensure(demod_kernel, kSmemBytes);
     if (e != cudaSuccess) return e;
+    e = attr_ip.ensure(demod_ip_kernel, kSmemBytesIp);
+    if (e != cudaSuccess) return e;
     if (p.nblocks <= 0) return cudaSuccess;
-    demod_kernel<<<grid, kThreads, kSmemBytes, stream>>>(p);
+    if (p.variant == kVariantInPlace) {
+        if (!p.tw_pair || !p.g_pos || !p.godd_pos) return cudaErrorInvalidValue;
+        demod_ip_kernel<<<grid, kThreads, kSmemBytesIp, stream>>>(p);
+    } else {
+        demod_kernel<<<grid, kThreads, kSmemBytes, stream>>>(p);
+    }
     return cudaGetLastError();
 }
 

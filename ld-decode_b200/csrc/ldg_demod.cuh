@@ -67,7 +67,20 @@ struct DemodParams {
 
     // PAL_V4300D_NotchFilter: bins [notch_lo, notch_hi) searched (0, 0: off)
     int notch_lo, notch_hi;
+
+    // FFT decomposition: kVariantStockham (natural-order spectra, ldg_fft.cuh)
+    // or kVariantInPlace (position-order spectra, ldg_fft_ip.cuh), which
+    // reads the filters through the tables below
+    int variant;
+    const float4* fp_rfhpf;          // bin-pair tables: pair u -> (F[k], F[M-k]), k = bin_of(pair_pos(u))
+    const float4* fp_video[OUT_NVIDEO];
+    const float4* fp_efm;
+    const float2* g_pos;             // G at positions: g_pos[p] = G[bin_of(p)], p < M
+    const float2* godd_pos;
+    const float2* tw_pair;           // W_N^k of pair u
 };
+
+enum { kVariantStockham = 0, kVariantInPlace = 1, kNumVariants = 2 };
 
 constexpr int kDemodErrSlotWait = 1;
 
@@ -84,11 +97,18 @@ struct QueueParams {
     float2* scratch;               // kScratchPerCta per CTA of the launch
     const float2* tw16;
     const float2* tw32;
+    int variant;                   // FFT decomposition for every item (as DemodParams.variant)
 };
 
-// Dynamic shared memory the kernel needs.
-constexpr int kSmemFloat2 = (16384 + 1024) + 2 * (1024 + 64) + 4 * 16 + 4 * 256 + 4096;
+// Dynamic shared memory the kernels need: the padded working set, the two
+// padded audio bands, the 1024-point tables (4 x 16 and 256 entries), then
+// the 16384-point tables of the decomposition (Stockham: 4 x 256 and 4096;
+// in place: 4 x 1024, 4 x 64 and 4 x 4).
+constexpr int kSmemFloat2Common = (16384 + 1024) + 2 * (1024 + 64) + 4 * 16 + 256;
+constexpr int kSmemFloat2 = kSmemFloat2Common + 4 * 256 + 4096;
+constexpr int kSmemFloat2Ip = kSmemFloat2Common + 4 * 1024 + 4 * 64 + 4 * 4;
 constexpr size_t kSmemBytes = size_t(kSmemFloat2) * 8;
+constexpr size_t kSmemBytesIp = size_t(kSmemFloat2Ip) * 8;
 constexpr size_t kScratchPerCta = size_t(2) * 16384 * 8;
 
 // Analog audio stage 2 (one transform of up to kN stage-1 samples per

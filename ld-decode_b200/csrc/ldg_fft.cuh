@@ -52,20 +52,26 @@ struct Tables {
     const float2* s2;   // [4][16]:   W_256^(k 2^r)  (pass Ns = 16, radix 16)
     const float2* s3;   // [4][256]:  W_4096^(k 2^r) (pass Ns = 256, radix 16)
     const float2* s4;   // [4096]:    W_16384^k      (pass Ns = 4096, radix 4)
+    const float2* s4a;  // [256]:     W_1024^k       (1024-point pass Ns = 256, radix 4)
 };
 
-constexpr int kS2 = 4 * 16, kS3 = 4 * 256, kS4 = 4096;  // float2 entries of the shared tables
+constexpr int kS2 = 4 * 16, kS3 = 4 * 256, kS4 = 4096, kS4a = 256;  // float2 entries of the shared tables
 
-// Fill the shared pass tables from the global W_16384 table (all threads).
-__device__ __forceinline__ void load_pass_tables(float2* s2, float2* s3, float2* s4, const float2* t16) {
+// Fill the 1024-point tables (s2, s4a) from the global W_16384 table (all threads).
+__device__ __forceinline__ void load_1k_tables(float2* s2, float2* s4a, const float2* t16) {
+    for (int i = threadIdx.x; i < kS2; i += blockDim.x) {
+        const int r = i >> 4, k = i & 15;
+        s2[i] = __ldg(t16 + ((k << r) * 64 & 16383));
+    }
+    for (int i = threadIdx.x; i < kS4a; i += blockDim.x) s4a[i] = __ldg(t16 + 16 * i);
+}
+
+// Fill the 16384-point Stockham pass tables from the global W_16384 table (all threads).
+__device__ __forceinline__ void load_pass_tables(float2* s3, float2* s4, const float2* t16) {
     for (int i = threadIdx.x; i < kS4; i += blockDim.x) s4[i] = __ldg(t16 + i);
     for (int i = threadIdx.x; i < kS3; i += blockDim.x) {
         const int r = i >> 8, k = i & 255;
         s3[i] = __ldg(t16 + ((k << r) * 4 & 16383));
-    }
-    for (int i = threadIdx.x; i < kS2; i += blockDim.x) {
-        const int r = i >> 4, k = i & 15;
-        s2[i] = __ldg(t16 + ((k << r) * 64 & 16383));
     }
 }
 
@@ -137,7 +143,7 @@ template <int R, int M, int Ns, bool INV>
 __device__ __forceinline__ void apply_twiddles(float2 (&v)[R], const Tables& t, int k) {
     if constexpr (R == 4) {
         static_assert((M == 16384 && Ns == 4096) || (M == 1024 && Ns == 256), "radix-4 pass");
-        const float2 w1 = sw<INV>(t.s4, M == 16384 ? k : 16 * k);
+        const float2 w1 = M == 16384 ? sw<INV>(t.s4, k) : sw<INV>(t.s4a, k);
         const float2 w2 = cmul(w1, w1);
         const float2 w3 = cmul(w2, w1);
         v[1] = cmul(v[1], w1);

@@ -1,0 +1,210 @@
+// In-place 16384-point complex FFT of a padded shared-memory working set,
+// the second decomposition of the demodulator's transforms (the first is
+// the Stockham form of ldg_fft.cuh).
+//
+// Cooley-Tukey in place, radices 16, 16, 16, 4: each thread loads its 16
+// points of a butterfly group, transforms them in registers and stores them
+// back to the same 16 addresses, so a stage needs no barrier between its
+// loads and its stores -- one barrier per stage, and the warps of a stage
+// run their loads, arithmetic and stores out of step with each other.  The
+// price is the order of the spectrum: the forward transform (decimation in
+// frequency: butterfly, then twiddle) takes its input in natural order and
+// leaves bin k at position pos_of(k), the four radix digits of k reversed;
+// the inverse (decimation in time: twiddle, then butterfly, the stages in
+// the opposite order) takes its input at those positions and leaves its
+// output in natural order.  Spectra therefore stay in position order
+// between a forward and an inverse transform (the parked spectra, the
+// filters' bin-pair tables), and only time-domain data is in natural order.
+//
+// Stage s works on groups of R points at stride L inside blocks of R*L
+// points: L = 1024, 64, 4 (radix 16) and L = 1 (radix 4, four groups per
+// thread).  The padding pad(i) = i + i/16 of ldg_fft.cuh makes every stage's
+// loads and stores, and the position-order passes over bin pairs, free of
+// bank conflicts.  Twiddles W_(RL)^(j q) come from per-stage shared tables
+// holding W^j, W^2j, W^4j, W^8j (FP64-made, stored FP32); the other eleven
+// are at most three complex products away, as in ldg_fft.cuh.
+#pragma once
+#include "ldg_fft.cuh"
+
+namespace ldg {
+namespace ip {
+
+// bin of position p, and position of bin k (M = 16384 = 16*16*16*4)
+__host__ __device__ __forceinline__ constexpr int bin_of(int p) {
+    return (p >> 10) | (((p >> 6) & 15) << 4) | (((p >> 2) & 15) << 8) | ((p & 3) << 12);
+}
+__host__ __device__ __forceinline__ constexpr int pos_of(int k) {
+    return ((k & 15) << 10) | (((k >> 4) & 15) << 6) | (((k >> 8) & 15) << 2) | (k >> 12);
+}
+
+// The bin pairs (k, M - k) of a real transform's half-length spectrum, one
+// position of each pair in a fixed order u = 0 .. M/2: positions whose
+// partner pos_of(M - bin_of(p)) comes later.  u < 7680: [1024, 8704);
+// then [64, 544), [4, 34) and 0 (bins 0 / M), 1 (4096, partner 3), 2 (M/2).
+constexpr int kPairs = kM / 2 + 1;
+__host__ __device__ __forceinline__ constexpr int pair_pos(int u) {
+    return u < 7680 ? 1024 + u : u < 8160 ? 64 + (u - 7680) : u < 8190 ? 4 + (u - 8160) : u - 8190;
+}
+__host__ __device__ __forceinline__ constexpr int partner_pos(int p) { return pos_of((kM - bin_of(p)) & (kM - 1)); }
+
+// shared twiddle tables: [4][1024] W_16384^(j 2^r); [4][64] W_1024^(j 2^r); [4][4] W_64^(j 2^r)
+constexpr int kT1 = 4 * 1024, kT2 = 4 * 64, kT3 = 4 * 4;
+
+struct Twiddles {
+    const float2* t1;
+    const float2* t2;
+    const float2* t3;
+};
+
+// Fill the stage tables from the global W_16384^i table (all threads).
+__device__ __forceinline__ void load_stage_tables(float2* t1, float2* t2, float2* t3, const float2* t16) {
+    for (int i = threadIdx.x; i < kT1; i += blockDim.x) {
+        const int r = i >> 10, j = i & 1023;
+        t1[i] = __ldg(t16 + ((j << r) & 16383));
+    }
+    for (int i = threadIdx.x; i < kT2; i += blockDim.x) {
+        const int r = i >> 6, j = i & 63;
+        t2[i] = __ldg(t16 + (((j << r) * 16) & 16383));
+    }
+    for (int i = threadIdx.x; i < kT3; i += blockDim.x) {
+        const int r = i >> 2, j = i & 3;
+        t3[i] = __ldg(t16 + (((j << r) * 256) & 16383));
+    }
+}
+
+// w[q] = W^(j q), q = 0..15, from W^j, W^2j, W^4j, W^8j (conjugated for the inverse)
+template <bool INV>
+__device__ __forceinline__ void group_twiddles(float2 (&w)[16], const float2* tab, int stride, int j) {
+    w[0] = make_float2(1.f, 0.f);
+    w[1] = tab[j];
+    w[2] = tab[stride + j];
+    w[4] = tab[2 * stride + j];
+    w[8] = tab[3 * stride + j];
+    if (INV) {
+        w[1] = cconj(w[1]);
+        w[2] = cconj(w[2]);
+        w[4] = cconj(w[4]);
+        w[8] = cconj(w[8]);
+    }
+    w[3] = cmul(w[2], w[1]);
+    w[5] = cmul(w[4], w[1]);
+    w[6] = cmul(w[4], w[2]);
+    w[7] = cmul(w[4], w[3]);
+    w[9] = cmul(w[8], w[1]);
+    w[10] = cmul(w[8], w[2]);
+    w[11] = cmul(w[8], w[3]);
+    w[12] = cmul(w[8], w[4]);
+    w[13] = cmul(w[8], w[5]);
+    w[14] = cmul(w[8], w[6]);
+    w[15] = cmul(w[8], w[7]);
+}
+
+// One radix-16 stage at stride L (1024, 64 or 4).  Forward: load, butterfly,
+// twiddle the outputs, store; inverse: load, twiddle the inputs, butterfly,
+// store.  LD (first forward stage, L = 1024) supplies the natural-order
+// input ld(0, n); ST (last inverse stage, L = 1024) takes the natural-order
+// output st(0, n, v) instead of shared memory.  Ends with a barrier.
+template <int L, bool INV, class LD, class ST>
+__device__ __noinline__ void stage16(float2* S, const Twiddles& tw, const LD& ld, const ST& st) {
+    static_assert(L == 1024 || L == 64 || L == 4, "stride");
+    constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
+    constexpr bool to_smem = std::is_same<ST, SmemIO>::value;
+    const int t = threadIdx.x;
+    int base, j;
+    if (L == 1024) {
+        base = 0;
+        j = t;
+    } else if (L == 64) {
+        base = (t >> 6) << 10;
+        j = t & 63;
+    } else {
+        base = (t >> 2) << 6;
+        j = t & 3;
+    }
+    float2* Sb = S + pad(base + j);
+    // pad(base + j + L r) = pad(base + j) + off(r)
+    auto off = [](int r) { return L >= 16 ? r * padded(L) : 4 * r + (r >> 2); };
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        if constexpr (from_smem) {
+            v[r] = Sb[off(r)];
+        } else {
+            v[r] = ld(0, j + L * r);
+        }
+    }
+    float2 w[16];
+    const float2* tab = L == 1024 ? tw.t1 : L == 64 ? tw.t2 : tw.t3;
+    group_twiddles<INV>(w, tab, L == 1024 ? 1024 : L == 64 ? 64 : 4, j);
+    if (INV) {
+#pragma unroll
+        for (int r = 1; r < 16; ++r) v[r] = cmul(v[r], w[r]);
+    }
+    dft_dif<16, INV>(v);  // v[i] = Y[bitrev(i)]
+    if (!INV) {
+#pragma unroll
+        for (int i = 1; i < 16; ++i) v[i] = cmul(v[i], w[bitrev(i, 4)]);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int q = bitrev(i, 4);
+        if constexpr (to_smem) {
+            Sb[off(q)] = v[i];
+        } else {
+            st(0, j + L * q, v[i]);
+        }
+    }
+    __syncthreads();
+}
+
+// The radix-4 stage (L = 1): groups 4g .. 4g+3, g = t + 1024 i, no twiddles.
+// LD (first inverse stage) supplies the position-order input ld.quad(p, v4)
+// for the four points at positions p .. p+3.  Ends with a barrier.
+template <bool INV, class LD>
+__device__ __noinline__ void stage4(float2* S, const LD& ld) {
+    constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int g = threadIdx.x + kThreads * i;
+        float2* Sb = S + pad(4 * g);  // pad(4g + r) = pad(4g) + r
+        float2 v[4];
+        if constexpr (from_smem) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) v[r] = Sb[r];
+        } else {
+            ld.quad(4 * g, v);
+        }
+        dft_dif<4, INV>(v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) Sb[bitrev(q, 2)] = v[q];
+    }
+    __syncthreads();
+}
+
+// Forward (exp(-2 pi i nk/M)): natural-order input (through `ld` unless
+// SmemIO), bin k left at S[pad(pos_of(k))].  Callers sync before when S was
+// just written.
+template <class LD = SmemIO>
+__device__ __forceinline__ void fft16k_fwd(float2* S, const Twiddles& tw, const LD& ld = LD()) {
+    const SmemIO s;
+    stage16<1024, false>(S, tw, ld, s);
+    stage16<64, false>(S, tw, s, s);
+    stage16<4, false>(S, tw, s, s);
+    stage4<false>(S, s);
+}
+
+// Inverse (exp(+2 pi i nk/M), unnormalised): bin k taken from position
+// pos_of(k) (S, or `ld.quad` when LD is not SmemIO), natural-order output
+// (S, or `st` when ST is not SmemIO).  Callers sync before when S was just
+// written.
+template <class LD = SmemIO, class ST = SmemIO>
+__device__ __forceinline__ void fft16k_inv(float2* S, const Twiddles& tw, const LD& ld = LD(), const ST& st = ST()) {
+    const SmemIO s;
+    stage4<true>(S, ld);
+    stage16<4, true>(S, tw, s, s);
+    stage16<64, true>(S, tw, s, s);
+    stage16<1024, true>(S, tw, s, st);
+}
+
+}  // namespace ip
+}  // namespace ldg

@@ -30,6 +30,8 @@ struct ldg_queue {
     long long total = 0;
     int grab = 1;
     int ctas = 0;                    // 0: one per SM
+    int variant = -1;                // FFT decomposition; -1: the first item's context's
+    int item_variant = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int graph_grid = 0;
@@ -154,6 +156,7 @@ int ldg_queue_submit(ldg_queue* q, const ldg_work_item* items, int32_t n) {
         QCK(cudaMemcpy(q->d_first, first.data(), (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice));
         q->tw16 = h[0].tw16;
         q->tw32 = h[0].tw32;
+        q->item_variant = h[0].variant;
     }
     q->nitems = n;
     q->total = first[n];
@@ -174,6 +177,21 @@ int ldg_queue_set_schedule(ldg_queue* q, int32_t grab, int32_t ctas) {
     }
     q->grab = grab;
     q->ctas = ctas;
+    return LDG_OK;
+}
+
+int ldg_queue_set_variant(ldg_queue* q, int32_t variant) {
+    if (!q) return qfail(LDG_ERR_ARG, "ldg_queue_set_variant: NULL queue");
+    if (variant < -1 || variant >= ldg::kNumVariants)
+        return qfail(LDG_ERR_ARG, "ldg_queue_set_variant: variant must be -1, LDG_VARIANT_STOCKHAM or LDG_VARIANT_IN_PLACE");
+    std::lock_guard<std::mutex> lk(q->mu);
+    if (variant != q->variant) {
+        Dev g(q->device);
+        int rc = wait_idle(q);
+        if (rc) return rc;
+        drop_graph(q);
+    }
+    q->variant = variant;
     return LDG_OK;
 }
 
@@ -213,6 +231,7 @@ int ldg_queue_run(ldg_queue* q, void* stream, int32_t use_graph) {
     p.scratch = q->d_scratch;
     p.tw16 = q->tw16;
     p.tw32 = q->tw32;
+    p.variant = q->variant >= 0 ? q->variant : q->item_variant;
     QCK(ldg::prepare_demod_queue());
     if (use_graph) {
         if (!q->exec || q->graph_grid != grid) {

@@ -77,6 +77,10 @@ class DemodQueue:
         L.check(self._lib.ldg_queue_info(self.handle, ctypes.byref(total), ctypes.byref(grid)))
         return total.value, grid.value
 
+    def set_variant(self, variant):
+        """FFT decomposition of the launch (-1: the first item's context's)."""
+        L.check(self._lib.ldg_queue_set_variant(self.handle, int(variant)))
+
     def run(self, stream=None, graph=True):
         """Enqueue one pass over every submitted block on `stream` (a
         torch.cuda.Stream or raw handle; None: torch's current stream)."""
@@ -94,31 +98,87 @@ class DemodQueue:
             pass
 
 
-def autotune(queue, stream=None, grabs=(1, 2, 4, 8), ctas=(0,), reps=3, graph=True):
-    """Time every (grab, ctas) schedule on the queue's submitted batch with
-    CUDA events on `stream` (one untimed run each, then the best of `reps`)
-    and keep the fastest.  Returns {"best": (grab, ctas), "ms": {...}}."""
+def autotune(queue, stream=None, grabs=(1, 2, 4, 8), ctas=(0,), reps=3, graph=True, variants=(None,)):
+    """Time every (grab, ctas, variant) schedule on the queue's submitted
+    batch with CUDA events on `stream` (one untimed run each, then the best
+    of `reps`) and keep the fastest.  `variants`: FFT decompositions to try
+    (None: the first item's context's).  Returns {"best": (grab, ctas,
+    variant), "ms": {...}}."""
     import torch
     st = stream if stream is not None else torch.cuda.current_stream()
     times = {}
-    for g in grabs:
-        for c in ctas:
-            queue.set_schedule(g, c)
-            queue.run(st, graph)
+    for v in variants:
+        queue.set_variant(-1 if v is None else v)
+        for g in grabs:
+            for c in ctas:
+                queue.set_schedule(g, c)
+                queue.run(st, graph)
+                best = None
+                for _ in range(reps):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    queue.run(st, graph)
+                    e1.record(st)
+                    e1.synchronize()
+                    ms = e0.elapsed_time(e1)
+                    best = ms if best is None else min(best, ms)
+                times[(g, c, v)] = best
+    choice = min(times, key=times.get)
+    queue.set_variant(-1 if choice[2] is None else choice[2])
+    queue.set_schedule(choice[0], choice[1])
+    return {"best": choice, "ms": times}
+
+
+_DEMOD_TUNED = {}  # (device, system) -> (variant, blocks_per_cta), the winner kept per device
+
+
+def autotune_demod(rf, in_ptr, nblocks, in_stride, outs, mtf_level=1, stream=None, variants=(0, 1),
+                   blocks_per_cta=(1, 2, 4), reps=3, keep=True):
+    """Time ldg_demod_blocks on a device batch (the caller's input and
+    outputs, e.g. the first blocks of a capture) under every FFT
+    decomposition (`variants`: L.LDG_VARIANT_STOCKHAM / LDG_VARIANT_IN_PLACE)
+    and blocks per CTA, with CUDA events on `stream` (one untimed launch
+    each, then the best of `reps`), and leave `rf` set to the fastest.
+    With `keep`, the winner is remembered for the device and system and
+    `tuned_demod` hands it to later contexts.  Returns {"best": (variant,
+    blocks_per_cta), "ms": {(variant, bpc): ms}, "blocks": nblocks}."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    sh = st.cuda_stream if hasattr(st, "cuda_stream") else st
+    times = {}
+    for v in variants:
+        rf.fft_variant = v
+        for b in blocks_per_cta:
+            L.check(rf._ctx._lib.ldg_set_demod_schedule(rf._ctx.handle, int(b)))
+            rf.demod_blocks_device(in_ptr, nblocks, in_stride, outs, mtf_level=mtf_level, stream=sh)
             best = None
             for _ in range(reps):
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(st)
-                queue.run(st, graph)
+                rf.demod_blocks_device(in_ptr, nblocks, in_stride, outs, mtf_level=mtf_level, stream=sh)
                 e1.record(st)
                 e1.synchronize()
                 ms = e0.elapsed_time(e1)
                 best = ms if best is None else min(best, ms)
-            times[(g, c)] = best
+            times[(v, b)] = best
     choice = min(times, key=times.get)
-    queue.set_schedule(*choice)
-    return {"best": choice, "ms": times}
+    rf.fft_variant = choice[0]
+    L.check(rf._ctx._lib.ldg_set_demod_schedule(rf._ctx.handle, int(choice[1])))
+    if keep:
+        _DEMOD_TUNED[(rf.device, rf.system)] = choice
+    return {"best": choice, "ms": times, "blocks": nblocks}
+
+
+def tuned_demod(rf):
+    """Apply the schedule autotune_demod kept for rf's device and system, if
+    any; returns it or None."""
+    choice = _DEMOD_TUNED.get((rf.device, rf.system))
+    if choice is not None:
+        rf.fft_variant = choice[0]
+        L.check(rf._ctx._lib.ldg_set_demod_schedule(rf._ctx.handle, int(choice[1])))
+    return choice
 
 
 def output_bytes_per_sample(system, audio=True, efm=True):
@@ -363,6 +423,10 @@ class MixedBatch:
         buf, off = self._pic_index[capture]
         o = off + field * w * h
         return buf[o:o + w * h].view(h, w)
+
+    def set_variant(self, variant):
+        """FFT decomposition of the launch (-1: the first item's context's)."""
+        L.check(self._lib.ldg_queue_set_variant(self.handle, int(variant)))
 
     def run(self, stream=None, graph=True):
         """Demodulate, locate and resample everything; returns the number of

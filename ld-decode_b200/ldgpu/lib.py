@@ -15,6 +15,7 @@ LIBPATH = os.path.join(HERE, "libldgpu.so")
 LDG_OK = 0
 LDG_NTSC, LDG_PAL = 0, 1
 LDG_IN_INT16, LDG_IN_FLOAT32 = 0, 1
+LDG_VARIANT_STOCKHAM, LDG_VARIANT_IN_PLACE = 0, 1
 (LDG_F_RFHPF, LDG_F_VIDEO_G, LDG_F_DEMOD, LDG_F_05, LDG_F_BURST, LDG_F_PILOT,
  LDG_F_EFM, LDG_F_VIDEO_G_ODD, LDG_F_AUDIO2_LEFT, LDG_F_AUDIO2_RIGHT) = range(10)
 LDG_NFILTERS = 10
@@ -201,6 +202,10 @@ SIGNATURES = {
     "ldg_ac3_dpll_create": (ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_double]),
     "ldg_ac3_dpll_destroy": (None, [c_p]),
     "ldg_ac3_dpll_reclock": (ctypes.c_int, [c_p, c_p, c_p, ctypes.c_int64, c_p, ctypes.POINTER(ctypes.c_int64)]),
+    "ldg_set_demod_variant": (ctypes.c_int, [c_p, c_i32]),
+    "ldg_get_demod_variant": (ctypes.c_int, [c_p, ctypes.POINTER(c_i32)]),
+    "ldg_set_demod_schedule": (ctypes.c_int, [c_p, c_i32]),
+    "ldg_queue_set_variant": (ctypes.c_int, [c_p, c_i32]),
     "ldg_efm_pll_create": (ctypes.c_int, [ctypes.POINTER(c_p)]),
     "ldg_efm_pll_destroy": (ctypes.c_int, [c_p]),
     "ldg_efm_pll_process": (ctypes.c_int, [c_p, c_p, c_i64, c_p, c_i64, ctypes.POINTER(c_i64)]),

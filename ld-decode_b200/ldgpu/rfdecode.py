@@ -145,11 +145,13 @@ class RFDecode(RFParams):
 
     def __init__(self, inputfreq=40, system="NTSC", blocklen=BLOCKSIZE,
                  decode_digital_audio=False, decode_analog_audio=0, has_analog_audio=True,
-                 extra_options={}, decoder_params_override={}, device=0):
+                 extra_options={}, decoder_params_override={}, device=0, fft_variant=None):
         super().__init__(inputfreq, system, blocklen, decode_digital_audio, decode_analog_audio,
                          has_analog_audio, extra_options, decoder_params_override, _design=False)
         self.device = device
         self._ctx = L.Context(system, blocklen, self.freq_hz, device)
+        if fft_variant is not None:
+            self.fft_variant = fft_variant
         if self.system == "PAL" and self.PAL_V4300D_NotchFilter:
             # the reference's search band (core.py:783-786)
             lo = int(self.blocklen * (8.42 / self.freq))
@@ -159,6 +161,19 @@ class RFDecode(RFParams):
         self._lut_loaded = False
         self.computefilters()
         self.blockcut_end = self.Filters["F05_offset"]
+
+    # ---- FFT decomposition of the demodulator (no counterpart in the reference)
+
+    @property
+    def fft_variant(self):
+        """L.LDG_VARIANT_STOCKHAM or L.LDG_VARIANT_IN_PLACE (ldg_set_demod_variant)."""
+        v = ctypes.c_int32()
+        L.check(self._ctx._lib.ldg_get_demod_variant(self._ctx.handle, ctypes.byref(v)))
+        return v.value
+
+    @fft_variant.setter
+    def fft_variant(self, v):
+        L.check(self._ctx._lib.ldg_set_demod_variant(self._ctx.handle, int(v)))
 
     # ---- filter upload (float32 half spectra)
 

@@ -19,10 +19,13 @@ RMS_HZ = 1000.0   # demod error target (RMS)
 MAX_HZ = 20000.0  # single-sample bound (near-zero analytic magnitude spots)
 
 
-@pytest.fixture(scope="module", params=["NTSC", "PAL"])
+# every test runs under both FFT decompositions of the demodulator
+@pytest.fixture(scope="module", params=[("NTSC", 0), ("NTSC", 1), ("PAL", 0), ("PAL", 1)],
+                ids=["NTSC-stockham", "NTSC-inplace", "PAL-stockham", "PAL-inplace"])
 def rf(request, cuda_ok):
     from ldgpu import RFDecode
-    r = RFDecode(system=request.param, decode_analog_audio=44100, decode_digital_audio=True)
+    system, variant = request.param
+    r = RFDecode(system=system, decode_analog_audio=44100, decode_digital_audio=True, fft_variant=variant)
     yield r
     r.close()
 
@@ -130,7 +133,8 @@ def test_delays_match_reference(rf):
     assert abs(rf.delays["video_white"] - white) < 0.01
 
 
-def test_pal_v4300d_notch(cuda_ok):
+@pytest.mark.parametrize("variant", [0, 1], ids=["stockham", "inplace"])
+def test_pal_v4300d_notch(cuda_ok, variant):
     """PAL_V4300D_NotchFilter on a block with spurious 8.5 MHz carriers: the
     GPU demodulator against the oracle with the notch and the reference's
     own outputs; the batched device path gives the plain call's bits."""
@@ -139,7 +143,7 @@ def test_pal_v4300d_notch(cuda_ok):
     from oracle import demod as odemod
     g = golden("demod_pal_notch")
     rf = RFDecode(system="PAL", decode_analog_audio=44100, decode_digital_audio=True,
-                  extra_options={"PAL_V4300D_NotchFilter": True})
+                  extra_options={"PAL_V4300D_NotchFilter": True}, fft_variant=variant)
     block = g["block"]
     gpu = rf.demodblock(data=block, mtf_level=1, cut=True)
     ref = odemod.demodblock(block, rf.Filters, system="PAL", freq_hz=rf.freq_hz, blocklen=rf.blocklen,
@@ -155,7 +159,7 @@ def test_pal_v4300d_notch(cuda_ok):
     rms, mx = err_stats(gpu["rfhpf"], ref["rfhpf"])
     assert rms <= 0.05 and mx <= 1.0
     # without the notch the outputs are far from the notched reference
-    plain = RFDecode(system="PAL", decode_analog_audio=44100, decode_digital_audio=True)
+    plain = RFDecode(system="PAL", decode_analog_audio=44100, decode_digital_audio=True, fft_variant=variant)
     p = plain.demodblock(data=block, mtf_level=1, cut=True)
     assert np.abs(p["video"]["demod"][::9].astype(np.float64) - g["m1_demod"]).max() > 1000.0
     # device batch form: same bits as the per-block call
@@ -179,8 +183,9 @@ LOWBAND = {
 }
 
 
+@pytest.mark.parametrize("variant", [0, 1], ids=["stockham", "inplace"])
 @pytest.mark.parametrize("name", list(LOWBAND))
-def test_lowband_filter_banks(cuda_ok, name):
+def test_lowband_filter_banks(cuda_ok, name, variant):
     """The reference's lowband configurations (core.py:209, 251 filter
     parameters; NTSC colour notch, MTF level/offset and de-emphasis strength;
     PAL de-emphasis coefficients) through the GPU demodulator: every output
@@ -189,7 +194,7 @@ def test_lowband_filter_banks(cuda_ok, name):
     from ldgpu import RFDecode
     from ldgpu.synth import synth_capture
     kw = LOWBAND[name]
-    r = RFDecode(**kw)
+    r = RFDecode(**kw, fft_variant=variant)
     try:
         g = golden("demod_" + kw["system"].lower())
         cap = synth_capture(kw["system"], 3 * r.blocklen, seed=77).numpy()
@@ -199,3 +204,29 @@ def test_lowband_filter_banks(cuda_ok, name):
                 print(name, "mtf", mtf, {k: (round(a, 2), round(b, 1)) for k, (a, b) in stats.items()})
     finally:
         r.close()
+
+
+@pytest.mark.parametrize("system", ["NTSC", "PAL"])
+def test_variants_agree(cuda_ok, system):
+    """The two FFT decompositions on the same seeded blocks: every output
+    within float32 rounding of each other (far inside the oracle tolerances),
+    and the in-place one within the same oracle tolerances (checked above)."""
+    from ldgpu import RFDecode
+    from ldgpu.synth import synth_capture
+    a = RFDecode(system=system, decode_analog_audio=44100, decode_digital_audio=True, fft_variant=0)
+    b = RFDecode(system=system, decode_analog_audio=44100, decode_digital_audio=True, fft_variant=1)
+    try:
+        assert (a.fft_variant, b.fft_variant) == (0, 1)
+        cap = synth_capture(system, 3 * 32768, seed=4242).numpy()
+        for off in (0, 50000):
+            x = cap[off:off + 32768]
+            ga = a.demodblock(data=x, mtf_level=1, cut=True)
+            gb = b.demodblock(data=x, mtf_level=1, cut=True)
+            for k in video_keys(system):
+                rms, mx = err_stats(ga["video"][k], gb["video"][k])
+                assert rms <= 10.0 and mx <= MAX_HZ, (k, rms, mx)
+            d = np.abs(ga["efm"].astype(int) - gb["efm"].astype(int))
+            assert d.max() <= 1
+    finally:
+        a.close()
+        b.close()
