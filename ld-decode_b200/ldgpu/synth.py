@@ -74,10 +74,24 @@ class _System:
         self.emp_ba = emphasis_ba(t_lo, t_hi, FS_HZ)
 
 
-def composite_ire(sysd, n):
-    """Composite video level in IRE at absolute sample indices n (int64)."""
+def composite_ire(sysd, n, shift=None, pal8=False, bruch_line=(8, 7)):
+    """Composite video level in IRE at absolute sample indices n (int64),
+    the video time base moved by `shift` samples (float64 per sample) when
+    given.  PAL with `pal8`: the V-switch alternates line after line across
+    frames (a 625-line frame flips it) and the burst is blanked at the start
+    of each field in a 4-field Bruch sequence, so that the decoder's line 6
+    carries burst in the second and third fields of the sequence and none in
+    the first and fourth; with the subcarrier's 4-frame phase cycle this
+    gives the 8-field sequence.  The raster's field starting at frame
+    half-line 0 is the one the decoder calls the second field; the blanking
+    ends at line bruch_line[0] (or one line later) of that field and at line
+    bruch_line[1] (or one later) of the other, counted from each field's
+    first full line."""
     d = sysd
-    t = n.to(torch.float64) / (FS_HZ / 1e6)  # microseconds
+    tn = n.to(torch.float64)
+    if shift is not None:
+        tn = tn + shift
+    t = tn / (FS_HZ / 1e6)  # microseconds
     hl_len = d.lp / 2
     frame_len = d.frame_lines * d.lp
     tf = torch.remainder(t, frame_len)
@@ -101,8 +115,20 @@ def composite_ire(sysd, n):
     w = 2 * math.pi * d.fsc * (t * 1e-6)
     sinw, cosw = torch.sin(w), torch.cos(w)
     vsw = torch.where(torch.remainder(line, 2) == 0, 1.0, -1.0) if d.pal else 1.0
-
+    if d.pal and pal8:
+        # absolute line count for the V-switch, absolute field count for the Bruch sequence
+        frame = torch.floor(t / frame_len).to(torch.int64)
+        vsw = torch.where(torch.remainder(frame * d.frame_lines + line, 2) == 0, 1.0, -1.0)
+        second = hl >= d.frame_lines
+        field_abs = 2 * frame + second.to(torch.int64)
+        lf = torch.where(second, (hl - d.frame_lines) // 2, hl // 2)  # line within the field
+        f4 = torch.remainder(field_abs, 4)
+        keep = (f4 == 0) | (f4 == 1)
+        b0 = torch.where(second, bruch_line[1], bruch_line[0])
+        blanked = lf < torch.where(keep, b0, b0 + 1)
     in_burst = reg & (tau >= d.burst[0]) & (tau < d.burst[1])
+    if d.pal and pal8:
+        in_burst = in_burst & ~blanked
     if d.pal:
         burst = d.burst_amp * (-sinw * 0.70710678 + vsw * cosw * 0.70710678)
     else:
@@ -172,8 +198,14 @@ def _rrc(beta, sps_, span):
 
 
 def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
-                  efm=True, qpsk=False, device="cpu", start=0, scale=2000.0, return_symbols=False):
+                  efm=True, qpsk=False, device="cpu", start=0, scale=2000.0, return_symbols=False, wow=None,
+                  pal8=False, bruch_line=(8, 7)):
     """int16 torch tensor of `nsamples` RF samples at 40 MSPS.
+
+    `wow` = (amplitude, period) in samples moves the video time base
+    sinusoidally, as a disc's speed error does: the video at sample n is the
+    raster's at n + amplitude * sin(2 pi n / period).  PAL with `pal8`: the
+    8-field sequence (see composite_ire).
 
     `start` offsets the absolute sample index (so different seeds/offsets give
     different field phases).  With qpsk=True the 2.88 MHz carrier is
@@ -211,7 +243,10 @@ def synth_capture(system, nsamples, seed=0, snr_db=40.0, tones=(1000.0, 440.0),
         gen = torch.Generator(device=dev)
         gen.manual_seed(int(seed) * 1000003 + c0 // CHUNK)
         n = torch.arange(start + c0 - LEAD, start + c0 + clen, device=dev, dtype=torch.int64)
-        ire = composite_ire(sysd, n)
+        shift = None
+        if wow is not None:
+            shift = wow[0] * torch.sin(n.to(torch.float64) * (2 * math.pi / wow[1]))
+        ire = composite_ire(sysd, n, shift, pal8, bruch_line)
         base = _fftconv(ire, taps)[LEAD:]
         fhz = sysd.ire0 + base * sysd.hz_ire
         # FM phase as an exact integer accumulator (2^24 steps per cycle) so

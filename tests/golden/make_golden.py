@@ -48,6 +48,14 @@ by ldgpu.synth, and saves small .npz fixtures:
                         rfhpf standard deviation, error sample indices, the
                         merged error list and the final dropout lines/ranges.
 
+  fields_<case>.npz  -- line location over 10-12 consecutive fields of a
+                        capture per case of tests/golden/field_cases.py (clean,
+                        30 dB SNR, seeded dropouts, 0.8-sample wow, dropouts
+                        on vertical sync, PAL through its 8-field sequence):
+                        per field the reference's sync pulses, valid-pulse
+                        classes, line locations, bad lines, flags (field order,
+                        line count, line offset, phase ID, sync confidence),
+                        next-field offset and a picture digest;
   efm_pll.npz        -- the reference's EFM_PLL (efm_pll.py:80-244) over seeded
                         EFM-like signals (tests/golden/efm_cases.py) fed in
                         buffers of uneven length: every call's T-values and
@@ -273,6 +281,74 @@ def field_fixture(system, seed, nfields=2):
         i += 1
     out["skipped_starts"] = np.array(skipped, dtype=np.float64)
     np.savez_compressed(os.path.join(HERE, f"field_{system.lower()}.npz"), **out)
+
+
+FIELDS_PIC_STRIDE = 97
+
+
+def fields_fixture(case):
+    """Consecutive fields of one capture through the reference's readfield
+    walk (decodefield offsets, invalid fields skipped as readfield skips
+    them)."""
+    from field_cases import field_case_capture
+    name, system, nfields = case[0], case[1], case[2]
+    kw = dict(system=system, decode_analog_audio=0, decode_digital_audio=False)
+    rf = refcore.RFDecode(**kw)
+    src = BlockSource(rf, None, 1)
+    fieldcls = refcore.FieldPAL if system == "PAL" else refcore.FieldNTSC
+    if system == "PAL":
+        src.readlen = rf.linelen * 400
+    else:
+        src.readlen = ((rf.linelen * 350) // 16384) * 16384
+    cap, meta = field_case_capture(case, rf.blocklen, src.readlen)
+    src.cap = cap
+    out = {"capture_sha256": np.array(sha(cap)), "capture_len": np.array(len(cap)), "mtf_level": np.array(1.0)}
+    prev = None
+    start = 0
+    i = 0
+    tries = 0
+    skipped = []
+    while i < nfields:
+        rd = src.read_field(start)
+        assert rd is not None, (name, i)
+        decode, readloc = rd
+        f = fieldcls(rf, decode, prevfield=prev, initphase=(i == 0), fields_written=i,
+                     readloc=decode["startloc"])
+        f.process()
+        tries += 1
+        assert tries < nfields + 6, name
+        if not f.valid:
+            skipped.append(start)
+            start = start + f.nextfieldoffset
+            prev = None
+            continue
+        dsout, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+        p = f"f{i}_"
+        out[p + "start"] = np.array(start, dtype=np.float64)
+        out[p + "readloc"] = np.array(readloc)
+        out[p + "startloc"] = np.array(decode["startloc"])
+        out[p + "pulse_start"] = np.array([q.start for q in f.rawpulses], dtype=np.int64)
+        out[p + "pulse_len"] = np.array([q.len for q in f.rawpulses], dtype=np.int64)
+        out[p + "valid_type"] = np.array([v[0] for v in f.validpulses], dtype=np.int64)
+        out[p + "valid_start"] = np.array([v[1].start for v in f.validpulses], dtype=np.int64)
+        out[p + "valid_good"] = np.array([bool(v[2]) for v in f.validpulses])
+        out[p + "linelocs1"] = np.array(f.linelocs1, dtype=np.float64)
+        out[p + "linelocs"] = np.array(f.linelocs, dtype=np.float64)
+        out[p + "linebad"] = np.array(f.linebad, dtype=bool)
+        out[p + "flags"] = np.array([int(f.isFirstField), f.linecount, f.lineoffset,
+                                     f.fieldPhaseID, f.sync_confidence], dtype=np.int64)
+        out[p + "nextfieldoffset"] = np.array(f.nextfieldoffset, dtype=np.float64)
+        pic = np.asarray(f.dspicture)
+        out[p + "dspicture_sha256"] = np.array(sha(pic))
+        out[p + "dspicture_sub"] = pic[::FIELDS_PIC_STRIDE]
+        start = start + f.nextfieldoffset - (readloc - decode["startloc"])
+        prev = f
+        i += 1
+    out["nfields"] = np.array(nfields)
+    out["skipped_starts"] = np.array(skipped, dtype=np.float64)
+    for k, v in meta.items():
+        out["meta_" + k] = np.asarray(v)
+    np.savez_compressed(os.path.join(HERE, f"fields_{name}.npz"), **out)
 
 
 def dropout_fixture(system, seed, nfields=3, ndrop=60):
@@ -672,6 +748,12 @@ def main():
     if sys.argv[1:] == ["notch"]:
         notch_fixture()
         return
+    if sys.argv[1:2] == ["fields"]:
+        from field_cases import FIELD_CASES
+        for case in FIELD_CASES:
+            if len(sys.argv) < 3 or case[0] in sys.argv[2:]:
+                fields_fixture(case)
+        return
     if sys.argv[1:] == ["efm_pll"]:
         efm_pll_fixture()
         return
@@ -688,6 +770,9 @@ def main():
     audio_fixture()
     audio_slices_fixture()
     efm_pll_fixture()
+    from field_cases import FIELD_CASES
+    for case in FIELD_CASES:
+        fields_fixture(case)
     ac3_fixture()
     lut_fixture()
     for i, (name, kw) in enumerate(CONFIGS.items()):

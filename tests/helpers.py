@@ -38,3 +38,33 @@ def oracle_capture(rf, cap, first_block, nblocks, mtf_scaled, keys=("demod",)):
 def err_stats(gpu, ref):
     d = gpu.astype(np.float64) - ref.astype(np.float64)
     return float(np.sqrt(np.mean(d * d))), float(np.abs(d).max())
+
+
+class OracleBlocks:
+    """Cut oracle outputs of a capture's blocks, computed on demand by a
+    thread pool (numpy's transforms release the GIL) and cached, joined into
+    field read windows the way DemodCache.read joins them."""
+
+    def __init__(self, rf, cap, mtf_scaled, keys, threads=8):
+        self.rf, self.cap, self.mtf, self.keys = rf, cap, mtf_scaled, keys
+        self.U = rf.blocklen - rf.blockcut - rf.blockcut_end
+        self.threads = threads
+        self.cache = {}
+
+    def _one(self, b):
+        rf = self.rf
+        rv = odemod.demodblock(self.cap[b * self.U:b * self.U + rf.blocklen], rf.Filters, system=rf.system,
+                               freq_hz=rf.freq_hz, blocklen=rf.blocklen, blockcut=rf.blockcut,
+                               blockcut_end=rf.blockcut_end, video_rot=rf.delays["video_rot"],
+                               mtf_level=self.mtf, cut=True)
+        return {k: rv["video"][k] for k in self.keys}
+
+    def window(self, first_block, nblocks):
+        from concurrent.futures import ThreadPoolExecutor
+        need = [b for b in range(first_block, first_block + nblocks) if b not in self.cache]
+        if need:
+            with ThreadPoolExecutor(self.threads) as ex:
+                for b, rv in zip(need, ex.map(self._one, need)):
+                    self.cache[b] = rv
+        bl = range(first_block, first_block + nblocks)
+        return {k: np.concatenate([self.cache[b][k] for b in bl]) for k in self.keys}
