@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define LDG_ABI_VERSION 2
+#define LDG_ABI_VERSION 3
 
 #define LDG_OK 0
 #define LDG_ERR_ARG (-1)         /* invalid argument or size */
@@ -600,8 +600,19 @@ typedef struct ldg_lines_args {
     const double* prev_phase_adjust_dev;  /* if set: device copy of prev_phase_adjust (read in stream order) */
     int32_t first_field;        /* work on fields [first_field, first_field + count) of the nfields */
     int32_t count;              /* 0: to the end */
-    int32_t stages;             /* bits: 1 H-sync (PAL: all of PAL), 2 NTSC burst chain, 4 NTSC apply; 0: all */
+    int32_t stages;             /* bits: 1 H-sync (PAL: all of PAL's line locations), 2 NTSC burst chain /
+                                   PAL 8-field sequence, 4 NTSC apply; 0: all */
     int32_t pad2;
+    /* PAL 8-field sequence (determine_field_number, core.py:3095-3203): the
+     * field before the first one -- the burst phase adjusts of its lines 7,
+     * 11, 15, 19 (NaN: none) and its field phase ID (0: no such field) --
+     * taken from the device copies when set (read in stream order).  PAL
+     * phase_adjust holds nfields x 4 such adjusts, field_phase the IDs. */
+    double prev_pal_adjust[4];
+    const double* prev_pal_adjust_dev;
+    const int32_t* prev_field_phase_dev;
+    int32_t prev_field_phase;
+    int32_t pad3;
 } ldg_lines_args;
 
 int64_t ldg_lines_scratch_bytes(int32_t nfields);

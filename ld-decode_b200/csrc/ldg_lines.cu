@@ -16,7 +16,11 @@
 //                        of compute_line_bursts (2998-3047, clb_findbursts
 //                        utils.py:1339-1368) per line; PAL:
 //                        refine_linelocs_pilot twice (3054-3093) and
-//                        fix_badlines (2566-2589) -> final line locations.
+//                        fix_badlines (2566-2589) -> final line locations;
+//                        PAL: the burst levels and line 7-19 burst crossings
+//                        of determine_field_number (3095-3203).
+//   pal_sequence_kernel  PAL, one warp walking the fields in order: the
+//                        8-field sequence (field phase IDs).
 //   burst_chain_kernel   NTSC, one CTA walking the fields in order: the
 //                        burst phase of every line starts from the previous
 //                        field's phase_adjust_median (compute_burst_offsets,
@@ -509,6 +513,39 @@ __device__ void burst_record(const LineParams& P, const double* ll, int line, in
     for (int k = 0; k < kZc; ++k) r.cyc[k] = ((double)bstart + (double)zcs[k] - s_rem) / zcburstdiv;
 }
 
+// FieldPAL.get_burstlevel (core.py:3095-3104, numpy slice semantics at
+// the window's end): the RMS of demod over 2.4 us from 5.5 us into line
+// l_adj, less its mean, times sqrt(2); NaN for the reference's None (a
+// sample above 30 IRE) or an empty slice.  lc = linecount + lineoffset of
+// the moment (get_linelen's last-line rule).
+__device__ double pal_burstlevel(const LineParams& P, const double* ll, int l_adj, int lc, const float* demod,
+                                 long long n, double hz_ire) {
+    const double begin = ll[l_adj] + 5.5 * (P.samplesperline * line_len(ll, l_adj, lc, P.linelen));
+    const double length = 2.4 * (P.samplesperline * P.linelen);
+    const long long lo = (long long)begin;
+    const long long hi = min((long long)(begin + length + 1.0), n);
+    if (lo < 0 || hi <= lo) return nan("");
+    const long long m = hi - lo;
+    double acc = 0;  // float32 samples near 7 MHz: this double sum is exact
+    for (long long k = 0; k < m; ++k) acc += (double)demod[lo + k];
+    const float mean_f = (float)(acc / (double)m);
+    float mx = -INFINITY;
+    double s1 = 0;
+    for (long long k = 0; k < m; ++k) {
+        const float v = demod[lo + k] - mean_f;
+        mx = fmaxf(mx, v);
+        s1 += (double)v;
+    }
+    if ((double)mx > 30 * hz_ire) return nan("");
+    const double mu = s1 / (double)m;
+    double ss = 0;
+    for (long long k = 0; k < m; ++k) {
+        const double d = (double)(demod[lo + k] - mean_f) - mu;
+        ss += d * d;
+    }
+    return sqrt(ss / (double)m) * 1.4142135623730951;
+}
+
 // _angle_mean_phase / phase_distance helpers (core.py:3085-3093)
 __device__ __forceinline__ double phase_distance(double x, double c) {
     double d = (x - floor(x)) - c;
@@ -666,6 +703,34 @@ __global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P)
         a.linelocs[(long long)f * kMaxL + i] = tmp[i];
         a.linebad[(long long)f * kMaxL + i] = bad[i];
     }
+    __syncthreads();
+    // inputs of the 8-field sequence (FieldPAL.process, core.py:3212-3236):
+    // calc_burstmedian runs while the field's line count and offset are still
+    // compute_linelocs' (263 / 262 and 0), determine_field_number after they
+    // become 312 / 313 and 2 / 3
+    {
+        const bool isf = a.isfirst[f] != 0;
+        const int lc_med = isf ? 263 : 262;
+        const int off = isf ? 2 : 3;
+        const int lc_seq = (isf ? 312 : 313) + off;
+        const float* demod = a.demod + base;
+        double lvl = INFINITY;
+        if (i >= 11 && i < 313) {
+            const double b = pal_burstlevel(P, tmp, i, lc_med, demod, n, P.hz_ire);
+            if (!isnan(b)) lvl = b;
+        }
+        for (int k = i; k < 512; k += blockDim.x) red[k] = k == i ? lvl : INFINITY;
+        const int cnt = __syncthreads_count(lvl != INFINITY);
+        bitonic512(red);
+        if (i == 0) {
+            double* out = P.adjs + (long long)f * kBurstLines;
+            out[0] = pal_burstlevel(P, tmp, 6 + off, lc_seq, demod, n, P.hz_ire);
+            out[1] = cnt ? sorted_median(red, cnt) / P.hz_ire : 0.0;
+        }
+        if (i < 4)
+            burst_record(P, tmp, 7 + 4 * i + off, lc_seq, a.burst + base, demod, n,
+                         P.rec[(long long)f * kBurstLines + i]);
+    }
 }
 
 // np.median of 16 doubles (mean of the two middle ones): Batcher's
@@ -817,6 +882,85 @@ __global__ void __launch_bounds__(kBurstThreads) burst_chain_kernel(LineParams P
         }
         __syncthreads();
         cur = nxt;
+    }
+}
+
+// PAL 8-field sequence (determine_field_number, core.py:3128-3203), fields in
+// order.  Lane j follows line 7 + 4j: its burst phase starts from the
+// previous field's (0 when there is none, when that line had no result or
+// when that field decided its ID before measuring phases), two passes of
+// clb_findbursts' phase update, rising or not.  The field's ID comes from
+// line 6's burst level against the field's median (present / absent / out of
+// both ranges) and the majority of rising lines, or is the previous ID + 1
+// when that evidence is missing or split.
+__global__ void __launch_bounds__(32) pal_sequence_kernel(LineParams P) {
+    const ldg_lines_args& a = P.a;
+    const int f0 = a.first_field, f1 = a.first_field + a.count;
+    const int j = threadIdx.x;
+    double seed = nan("");
+    int prev_id;
+    if (f0 > 0) {
+        if (j < 4) seed = a.phase_adjust[(long long)(f0 - 1) * 4 + j];
+        prev_id = a.field_phase[f0 - 1];
+    } else {
+        if (j < 4) seed = a.prev_pal_adjust_dev ? a.prev_pal_adjust_dev[j] : a.prev_pal_adjust[j];
+        prev_id = a.prev_field_phase_dev ? *a.prev_field_phase_dev : a.prev_field_phase;
+    }
+    for (int f = f0; f < f1; ++f) {
+        const bool has_prev = a.has_prev[f] != 0;
+        const int following = has_prev ? (prev_id + 1 == 9 ? 1 : prev_id + 1) : 1;
+        const double b6 = P.adjs[(long long)f * kBurstLines + 0];
+        const double bm = P.adjs[(long long)f * kBurstLines + 1];
+        int hasburst = -1;
+        if (!isnan(b6)) {
+            const double b = b6 / P.hz_ire;
+            if (b >= bm * 0.8 && b <= bm * 1.2) hasburst = 1;
+            else if (b < bm * 0.2) hasburst = 0;
+        }
+        double out = nan("");
+        int id = following;
+        if (hasburst >= 0) {  // warp-uniform
+            const bool isf = a.isfirst[f] != 0;
+            const int m4 = isf ? (hasburst ? 3 : 1) : (hasburst ? 2 : 4);
+            bool valid = false, rising = false;
+            if (j < 4) {
+                const BurstRec r = P.rec[(long long)f * kBurstLines + j];
+                if (r.valid) {
+                    double pa = -((has_prev && !isnan(seed)) ? seed : 0.0);
+                    int rising_count = 0;
+                    for (int pass = 0; pass < 2; ++pass) {
+                        rising_count = 0;
+                        if (r.count) {
+                            double dev[kZc];
+                            int odd = 0;
+#pragma unroll
+                            for (int k = 0; k < kZc; ++k) {
+                                const double cyc = r.cyc[k] + pa;
+                                const int rnd = (int)(cyc + .5);
+                                if (rnd % 2 != 0) odd |= 1 << k;
+                                dev[k] = (double)rnd - cyc;
+                            }
+                            pa += median16(dev);
+                            rising_count = __popc((unsigned)(r.rising ^ odd) & 0xffffu);
+                        }
+                    }
+                    rising = (double)rising_count > ((double)r.count / 2);
+                    out = -pa;
+                    valid = true;
+                }
+            }
+            const int count = __popc(__ballot_sync(0xffffffffu, valid));
+            const int rcount = __popc(__ballot_sync(0xffffffffu, valid && rising));
+            if (count != 0 && rcount * 2 != count) {
+                bool firstfour = rcount * 2 > count;
+                if (m4 == 2) firstfour = !firstfour;
+                id = m4 + (firstfour ? 0 : 4);
+            }
+        }
+        if (j < 4) a.phase_adjust[(long long)f * 4 + j] = out;
+        if (j == 0) a.field_phase[f] = id;
+        seed = out;
+        prev_id = id;
     }
 }
 
@@ -988,8 +1132,7 @@ extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
     if (a->nfields == 0) return LDG_OK;
     if (!a->d05 || !a->startloc || !a->wlen || !a->isfirst || !a->linecount || !a->has_prev || !a->linelocs1 ||
         !a->linebad1 || !a->linelocs || !a->linebad || !a->scratch ||
-        (a->k.system == 0 && (!a->demod || !a->burst || !a->phase_adjust || !a->field_phase)) ||
-        (a->k.system == 1 && !a->pilot))
+        !a->demod || !a->burst || !a->phase_adjust || !a->field_phase || (a->k.system == 1 && !a->pilot))
         return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: NULL buffer");
     if (a->k.system == 0 && a->proclines < kBurstLines)
         return ldg::lines_fail(LDG_ERR_ARG, "ldg_lines_refine: NTSC needs proclines >= 266");
@@ -1027,6 +1170,7 @@ extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
     cudaStream_t st = (cudaStream_t)a->stream;
     const int stages = a->stages ? a->stages : 7;
     if (stages & 1) lines_hsync_kernel<<<P.a.count, kLineThreads, 0, st>>>(P);
+    if (P.system == 1 && (stages & 2)) pal_sequence_kernel<<<1, 32, 0, st>>>(P);
     if (P.system == 0) {
         if (stages & 2) burst_chain_kernel<<<1, kBurstThreads, 0, st>>>(P);
         const double shift = (117.25 / 360) / P.fsc_mhz * P.freq;

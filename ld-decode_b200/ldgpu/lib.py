@@ -142,6 +142,8 @@ class LinesArgs(ctypes.Structure):
         ("prev_phase_adjust", c_f64), ("linelocs", c_p), ("linebad", c_p), ("phase_adjust", c_p),
         ("field_phase", c_p), ("scratch", c_p), ("stream", c_p), ("prev_phase_adjust_dev", c_p),
         ("first_field", c_i32), ("count", c_i32), ("stages", c_i32), ("pad2", c_i32),
+        ("prev_pal_adjust", c_f64 * 4), ("prev_pal_adjust_dev", c_p), ("prev_field_phase_dev", c_p),
+        ("prev_field_phase", c_i32), ("pad3", c_i32),
     ]
 
 
@@ -214,7 +216,7 @@ SIGNATURES = {
 
 # ABI of the library this binding is written for (LDG_ABI_VERSION in
 # include/ldgpu.h) and the structures whose layout it mirrors
-ABI_VERSION = 2
+ABI_VERSION = 3
 ABI_STRUCTS = [("ldg_chain_params", ChainParams), ("ldg_chain_state", ChainState),
                ("ldg_field_plan", FieldPlan), ("ldg_lines_consts", LinesConsts),
                ("ldg_lines_args", LinesArgs), ("ldg_tbc_field", TbcField),

@@ -226,7 +226,8 @@ class FieldLines:
     """Line locations of one field of a capture (device or host)."""
 
     def __init__(self, window, isfirst, linecount, lineoffset, linelocs_ptr=None, linelocs=None, nlines=0,
-                 field_phase=None, phase_adjust=None, sync_confidence=100, rows=None, hsync_len=0):
+                 field_phase=None, phase_adjust=None, sync_confidence=100, rows=None, hsync_len=0, linebad=None,
+                 bad_rows=None, pal_adjust=None):
         self.window = window
         self.hsync_len = int(hsync_len)    # int(Field.LT["hsync"][1])
         self.sync_confidence = int(sync_confidence)
@@ -239,6 +240,9 @@ class FieldLines:
         self._phase = field_phase          # int, or (device tensor, row)
         self._pam = phase_adjust           # float, or (device tensor, row)
         self._rows = rows                  # (device tensor, row) of a batched field
+        self._linebad = linebad            # host bool array (host-decoded fields) or None
+        self._bad_rows = bad_rows          # (device uint8 tensor, row) of a batched field
+        self._pal_adjust = pal_adjust      # PAL: dict, or (device (n, 4) tensor, row)
 
     @staticmethod
     def _value(v, cast):
@@ -255,6 +259,26 @@ class FieldLines:
     def phase_adjust_median(self):
         return self._value(self._pam, float)
 
+    @property
+    def pal_phase_adjust(self):
+        """PAL: FieldPAL.phase_adjust, the burst phase adjusts of lines 7,
+        11, 15 and 19 that the next field's determine_field_number seeds from
+        (None where the line had none)."""
+        v = self._pal_adjust
+        if isinstance(v, tuple):
+            t, i = v
+            v = t[i].cpu().numpy()
+            return {l: (None if np.isnan(x) else float(x)) for l, x in zip(range(7, 22, 4), v)}
+        return v
+
+    @property
+    def linebad(self):
+        """Field.linebad: the bad-line flags of the line locations (bool array)."""
+        if self._linebad is not None:
+            return np.asarray(self._linebad, dtype=bool)
+        t, i = self._bad_rows
+        return t[i].cpu().numpy()[:self.nlines].astype(bool)
+
     def host_linelocs(self):
         """The line locations as a host float64 array."""
         if self.linelocs is not None:
@@ -270,7 +294,7 @@ class LocatedFields:
 
     def __init__(self, rf):
         self.rf = rf
-        self._parts = []   # ("batch", plans, ll, pam, fph) | ("host", FieldLines, device tensor)
+        self._parts = []   # ("batch", plans, ll, pam, fph, bad) | ("host", FieldLines, device tensor)
         self._cache = None
 
     def __len__(self):
@@ -287,7 +311,7 @@ class LocatedFields:
         cols = {k: [] for k in keys}
         for part in self._parts:
             if part[0] == "batch":
-                _, pl, ll, _, _ = part
+                _, pl, ll, _, _, _ = part
                 n = len(pl)
                 isf = pl.isfirst.astype(bool)
                 cols["startloc"].append(pl.startloc)
@@ -329,7 +353,7 @@ class LocatedFields:
                     return part[1]
                 k -= 1
                 continue
-            _, pl, ll, pam, fph = part
+            _, pl, ll, pam, fph, bad = part
             if k < len(pl):
                 from .fieldread import FieldWindow
                 p = pl[k]
@@ -338,9 +362,10 @@ class LocatedFields:
                 rowb = ll.stride(0) * ll.element_size()
                 return FieldLines(w, p.isfirst, (312 if p.isfirst else 313) if pal else p.linecount,
                                   (2 if p.isfirst else 3) if pal else 0, linelocs_ptr=ll.data_ptr() + k * rowb,
-                                  nlines=proclines_for(self.rf), field_phase=None if pal else (fph, k),
+                                  nlines=proclines_for(self.rf), field_phase=(fph, k),
                                   phase_adjust=None if pal else (pam, k), sync_confidence=p.sync_confidence,
-                                  rows=(ll, k), hsync_len=int(p.hsync_len))
+                                  rows=(ll, k), hsync_len=int(p.hsync_len), bad_rows=(bad, k),
+                                  pal_adjust=(pam, k) if pal else None)
             k -= len(pl)
         raise IndexError("field index out of range")
 
@@ -496,7 +521,8 @@ class LineLocator:
         base = dbuf.data_ptr()
         out_ll = torch.empty((nf, ml), dtype=torch.float64, device=dev)
         out_bad = torch.empty((nf, ml), dtype=torch.uint8, device=dev)
-        pam = torch.zeros(nf, dtype=torch.float64, device=dev)
+        # NTSC: phase_adjust_median per field; PAL: the line 7/11/15/19 burst phase adjusts
+        pam = torch.zeros((nf, 4) if self.pal else nf, dtype=torch.float64, device=dev)
         fph = torch.zeros(nf, dtype=torch.int32, device=dev)
         scratch = torch.empty(max(int(lib.ldg_lines_scratch_bytes(nf)), 256), dtype=torch.uint8, device=dev)
         a = L.LinesArgs()
@@ -515,8 +541,19 @@ class LineLocator:
         a.has_prev = base + 2 * nf * 8 + 2 * nf * 4
         a.linelocs1 = base + nb_i
         a.linebad1 = base + nb_i + nf * ml * 8
-        a.prev_phase_adjust = float(prev_pam)
-        a.prev_phase_adjust_dev = prev_pam_dev
+        if self.pal:
+            # the previous field's line phases and ID: host values or device copies
+            kind, adj, fid = self._pal_seed
+            if kind == "host":
+                for j in range(4):
+                    a.prev_pal_adjust[j] = adj[j]
+                a.prev_field_phase = int(fid)
+            else:
+                a.prev_pal_adjust_dev = adj
+                a.prev_field_phase_dev = fid
+        else:
+            a.prev_phase_adjust = float(prev_pam)
+            a.prev_phase_adjust_dev = prev_pam_dev
         a.linelocs = out_ll.data_ptr()
         a.linebad = out_bad.data_ptr()
         a.phase_adjust = pam.data_ptr()
@@ -570,6 +607,7 @@ class LineLocator:
         self._scan_lo = 0
         self._state = L.ChainState()
         self._pam = ("host", 0.0)       # NTSC burst seed for the next batched field
+        self._pal_seed = ("host", [float("nan")] * 4, 0)  # PAL: the previous field's line phases and ID
         self._prev_host = None          # the previous field, if it was host-decoded
         self._last_dev = None           # index of the last batched field
         self._ire0 = float(self.rf.DecoderParams["ire0"])
@@ -649,13 +687,16 @@ class LineLocator:
                 base = len(out)
                 ll, bad, pam, fph, ready = self._refine(ptrs, self._cap_len, valid, pam_host, stream, pam_dev)
                 self.ready.extend((base + lo, base + hi, ev) for lo, hi, ev in ready)
-                out._parts.append(("batch", valid, ll, pam, fph))
+                out._parts.append(("batch", valid, ll, pam, fph, bad))
                 out._cache = None
                 self._last_dev = len(out) - 1
                 self._prev_host = None
                 if not self.pal:
                     self._pam = ("dev", pam.data_ptr() + 8 * (len(valid) - 1))
-                    self._keep.append(pam)
+                else:
+                    self._pal_seed = ("dev", pam.data_ptr() + 32 * (len(valid) - 1),
+                                      fph.data_ptr() + 4 * (len(valid) - 1))
+                self._keep.append((pam, fph))
                 t = self._tick("refine", t)
             state = st_out
             if stop in (L.LDG_CHAIN_STOP_END, L.LDG_CHAIN_STOP_FULL):
@@ -682,13 +723,16 @@ class LineLocator:
                 state.prev_valid = 0
                 self._prev_host = None
                 self._pam = ("host", 0.0)
+                self._pal_seed = ("host", [float("nan")] * 4, 0)
                 t = self._tick("host_fields", t)
                 continue
             ll_host = np.ascontiguousarray(f.linelocs, dtype=np.float64)
             fl = FieldLines(w, f.isFirstField, f.linecount, f.lineoffset, linelocs=ll_host, nlines=len(ll_host),
                             field_phase=getattr(f, "fieldPhaseID", None),
                             phase_adjust=getattr(f, "phase_adjust_median", None),
-                            sync_confidence=f.sync_confidence, hsync_len=int(f.LT["hsync"][1]))
+                            sync_confidence=f.sync_confidence, hsync_len=int(f.LT["hsync"][1]),
+                            linebad=np.asarray(f.linebad, dtype=bool),
+                            pal_adjust=dict(getattr(f, "phase_adjust", None) or {}) if self.pal else None)
             dev_ll = torch.from_numpy(ll_host).to(torch.device("cuda", torch.cuda.current_device()))
             fl.linelocs_ptr = dev_ll.data_ptr()
             out._parts.append(("host", fl, dev_ll))
@@ -703,6 +747,10 @@ class LineLocator:
             state.fields_written += 1
             self._prev_host = f
             self._pam = ("host", float(f.phase_adjust_median) if not self.pal else 0.0)
+            if self.pal:
+                pa = getattr(f, "phase_adjust", None) or {}
+                adj = [float("nan") if pa.get(l) is None else float(pa[l]) for l in range(7, 22, 4)]
+                self._pal_seed = ("host", adj, int(f.fieldPhaseID))
             if float(rf.DecoderParams["ire0"]) != self._ire0:
                 # the level re-calibration changed the sync threshold: rescan
                 self._ire0 = float(rf.DecoderParams["ire0"])
@@ -759,7 +807,6 @@ class LineLocator:
         p.sync_confidence = fl.sync_confidence
         p.phase_adjust_median = pam if not self.pal else 0
         p.fieldPhaseID = fl.fieldPhaseID if fl.fieldPhaseID is not None else 1
-        # the batch does not keep the PAL burst phases of lines 7-19 that
-        # determine_field_number seeds from (field phase ID metadata only)
-        p.phase_adjust = {l: None for l in range(7, 22, 4)}
+        if self.pal:
+            p.phase_adjust = fl.pal_phase_adjust or {}
         return p

@@ -115,7 +115,7 @@ def test_library_exports_every_header_symbol():
     for s in syms:
         assert hasattr(h, s), s
         assert s in lib.SIGNATURES, s
-    assert h.ldg_abi_version() == lib.ABI_VERSION == 2
+    assert h.ldg_abi_version() == lib.ABI_VERSION == 3
 
 
 def test_library_without_gpu_fails_cleanly():
