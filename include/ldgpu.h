@@ -269,6 +269,16 @@ int ldg_demod_scratch_bytes(ldg_ctx* ctx, int64_t nblocks, int64_t* bytes);
  * on args->stream (or the context's stream) and returns without waiting. */
 int ldg_demod_blocks_noalloc(ldg_ctx* ctx, const ldg_demod_args* args, int32_t ctas);
 
+/* demodblock's fftdata (RFDecode.demodblock_cpu, core.py:758-761: the
+ * spectrum takes precedence over the samples): out[b*N + n] =
+ * ifft(X_b).real[n] for `nblocks` full N-bin complex128 spectra X_b
+ * (interleaved re, im; the FFT of a real block, as DemodCache passes it),
+ * as float32 blocks for ldg_demod_blocks (LDG_IN_FLOAT32).  Both buffers
+ * device memory; enqueued on `stream` (NULL: the context's) without
+ * waiting.  A spectrum that is not Hermitian enters through its real
+ * inverse, i.e. through its Hermitian part. */
+int ldg_blocks_from_spectra(ldg_ctx* ctx, const double* spectra, int64_t nblocks, float* out, void* stream);
+
 /* ---- Analog audio stage 2 (RFDecode.audio_phase2, core.py:884-950) ---- */
 
 /* One transform of stage-1 audio: `len` (2 .. blocklen) samples per channel

@@ -793,6 +793,26 @@ int ldg_tbc_fields_async(ldg_ctx* c, const ldg_tbc_field* fields, int32_t nfield
     return LDG_OK;
 }
 
+int ldg_blocks_from_spectra(ldg_ctx* c, const double* spectra, int64_t nblocks, float* out, void* stream) {
+    if (!c || (nblocks && (!spectra || !out))) return fail(LDG_ERR_ARG, "ldg_blocks_from_spectra: NULL argument");
+    if (nblocks < 0 || nblocks > (1LL << 24)) return fail(LDG_ERR_ARG, "ldg_blocks_from_spectra: bad block count");
+    if (nblocks == 0) return LDG_OK;
+    if (!is_device_ptr(spectra) || !is_device_ptr(out))
+        return fail(LDG_ERR_ARG, "ldg_blocks_from_spectra: buffers must be device memory");
+    if ((reinterpret_cast<uintptr_t>(spectra) & 15) || (reinterpret_cast<uintptr_t>(out) & 7))
+        return fail(LDG_ERR_ARG, "ldg_blocks_from_spectra: spectra must be 16-byte and out 8-byte aligned");
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    ldg::SpectrumParams p;
+    p.spectra = reinterpret_cast<const double2*>(spectra);
+    p.out = out;
+    p.tw16 = c->d_tw16;
+    p.tw32 = c->d_tw32;
+    const cudaError_t e = ldg::launch_spectrum_blocks(p, (int)nblocks, st);
+    if (e != cudaSuccess) return fail(LDG_ERR_CUDA, std::string("spectrum launch: ") + cudaGetErrorString(e));
+    return LDG_OK;
+}
+
 int ldg_audio_phase2(ldg_ctx* c, const ldg_audio2_segment* segs, int32_t n, double center_left,
                      double center_right, void* stream) {
     if (!c || (!segs && n)) return fail(LDG_ERR_ARG, "ldg_audio_phase2: NULL argument");

@@ -887,6 +887,42 @@ __global__ void __launch_bounds__(kThreads, 1) audio2_kernel(const __grid_consta
     fft16k<true>(c.S, c.t, SmemIO(), Audio2Storer{ch ? sg.out_right : sg.out_left, p.cf[ch], n});
 }
 
+// ---- demodblock's fftdata (RFDecode.demodblock_cpu, core.py:758-761)
+
+// The real block ifft(X).real of a full N-bin spectrum (complex128), one CTA
+// per block: its Hermitian part (X[k] + conj(X[N-k])) / 2 on the
+// non-negative bins, the C2R pre-processing and one inverse 16384-point
+// transform.
+__global__ void __launch_bounds__(kThreads, 1) spectrum_block_kernel(const __grid_constant__ SpectrumParams p) {
+    extern __shared__ float2 smem[];
+    const CtaSmem c = cta_setup<kVariantStockham>(smem, p.tw16, p.tw32);
+    const double2* X = p.spectra + (long long)blockIdx.x * kN;
+    auto herm = [&](int k) {  // bins 0 < k < N/2
+        const double2 a = X[k], b = X[kN - k];
+        return make_float2((float)(0.5 * (a.x + b.x)), (float)(0.5 * (a.y - b.y)));
+    };
+    for (int k = threadIdx.x; k <= kM / 2; k += kThreads) {
+        if (k == 0) {
+            // bins 0 and N/2: their real parts (the imaginary parts leave ifft(X).real alone)
+            const double h0 = X[0].x, hm = X[kM].x;
+            c.S[0] = make_float2((float)(0.5 * (h0 + hm)), (float)(0.5 * (h0 - hm)));
+            continue;
+        }
+        c2r_pair(c.S, k, herm(k), herm(kM - k), __ldg(c.t.t32 + k));
+    }
+    __syncthreads();
+    fft16k<true>(c.S, c.t, SmemIO(), RealStorer{p.out + (long long)blockIdx.x * kN, 0, kN, 0});
+}
+
+cudaError_t launch_spectrum_blocks(const SpectrumParams& p, int nblocks, cudaStream_t stream) {
+    static SmemAttr attr;
+    cudaError_t e = attr.ensure(spectrum_block_kernel, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    if (nblocks <= 0) return cudaSuccess;
+    spectrum_block_kernel<<<nblocks, kThreads, kSmemBytes, stream>>>(p);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_audio2(const Audio2Params& p, int nsegs, cudaStream_t stream) {
     static SmemAttr attr;
     cudaError_t e = attr.ensure(audio2_kernel, kSmemBytes);

@@ -130,7 +130,16 @@ struct Audio2Params {
     const float2* tw32;
 };
 
+// Real blocks from full spectra (demodblock's fftdata): out[b * N + n] = ifft(X_b).real[n].
+struct SpectrumParams {
+    const double2* spectra;  // nblocks x N complex128
+    float* out;              // nblocks x N float32
+    const float2* tw16;
+    const float2* tw32;
+};
+
 cudaError_t launch_demod(const DemodParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_spectrum_blocks(const SpectrumParams& p, int nblocks, cudaStream_t stream);
 cudaError_t launch_audio2(const Audio2Params& p, int nsegs, cudaStream_t stream);
 // Sets the queue kernel's shared-memory size (call before a stream capture).
 cudaError_t prepare_demod_queue();

@@ -207,6 +207,7 @@ SIGNATURES = {
     "ldg_set_demod_variant": (ctypes.c_int, [c_p, c_i32]),
     "ldg_get_demod_variant": (ctypes.c_int, [c_p, ctypes.POINTER(c_i32)]),
     "ldg_set_demod_schedule": (ctypes.c_int, [c_p, c_i32]),
+    "ldg_blocks_from_spectra": (ctypes.c_int, [c_p, c_p, c_i64, c_p, c_p]),
     "ldg_queue_set_variant": (ctypes.c_int, [c_p, c_i32]),
     "ldg_efm_pll_create": (ctypes.c_int, [ctypes.POINTER(c_p)]),
     "ldg_efm_pll_destroy": (ctypes.c_int, [c_p]),

@@ -239,15 +239,30 @@ class RFDecode(RFParams):
     def demodblock_gpu(self, data=None, mtf_level=0, fftdata=None, cut=False, _rotdelay=None):
         """One block through the fused GPU demodulator.  `mtf_level` is the
         already-scaled MTF exponent, as in demodblock_cpu (core.py:755-879)."""
-        if data is not None:
+        dev_block = None
+        if fftdata is not None:
+            # the spectrum takes precedence, as in the reference; its real
+            # inverse is made on the GPU (ldg_blocks_from_spectra)
+            import torch
+            X = np.ascontiguousarray(np.asarray(fftdata, dtype=np.complex128))
+            if len(X) != self.blocklen:
+                raise ValueError(f"demodblock needs {self.blocklen} spectrum bins, got {len(X)}")
+            dev = torch.device("cuda", self.device)
+            dX = torch.from_numpy(X.view(np.float64)).to(dev)
+            dev_block = torch.empty(self.blocklen, dtype=torch.float32, device=dev)
+            torch.cuda.current_stream(dev).synchronize()  # the context's stream reads them next
+            L.check(self._ctx._lib.ldg_blocks_from_spectra(self._ctx.handle, dX.data_ptr(), 1,
+                                                           dev_block.data_ptr(), None))
+            x = None
+        elif data is not None:
             x = np.asarray(data)[: self.blocklen]
-        elif fftdata is not None:
-            x = np.fft.ifft(np.asarray(fftdata)).real
+            if len(x) != self.blocklen:
+                raise ValueError(f"demodblock needs {self.blocklen} samples, got {len(x)}")
         else:
             raise Exception("demodblock called without raw or FFT data")
-        if len(x) != self.blocklen:
-            raise ValueError(f"demodblock needs {self.blocklen} samples, got {len(x)}")
-        if x.dtype == np.int16:
+        if dev_block is not None:
+            kind = L.LDG_IN_FLOAT32
+        elif x.dtype == np.int16:
             kind = L.LDG_IN_INT16
             x = np.ascontiguousarray(x)
         else:
@@ -266,7 +281,7 @@ class RFDecode(RFParams):
         ar = np.empty(alen, dtype=np.float32) if self.decode_analog_audio else None
 
         a = L.DemodArgs()
-        a.in_ = x.ctypes.data
+        a.in_ = dev_block.data_ptr() if dev_block is not None else x.ctypes.data
         a.in_kind = kind
         a.in_stride = self.blocklen
         a.nblocks = 1

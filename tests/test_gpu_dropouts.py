@@ -106,9 +106,10 @@ def test_caps_and_bad_fields_raise(capture):
 @pytest.mark.parametrize("system", ["NTSC", "PAL"])
 def test_reference_golden_fields(cuda_ok, system):
     """The reference's own fields (its line locations and hsync length) on
-    the GPU demodulation of the golden capture: the dropout lists agree with
-    the reference's (the GPU's float32 demodulation may move a sample across
-    a limit, so a dropout edge may differ by a pixel)."""
+    the GPU demodulation of the golden capture: the dropout lists match the
+    reference's one to one -- same line, each edge within one pixel (the
+    GPU's float32 demodulation may move a sample across a limit) -- with no
+    dropout missing or extra."""
     import torch
     from ldgpu import RFDecode
     from ldgpu.dropouts import detect_host_field
@@ -134,10 +135,20 @@ def test_reference_golden_fields(cuda_ok, system):
         isfirst, linecount, lineoffset = (int(x) for x in g[p + "flags"])
         lines, starts, ends = detect_host_field(rf, data, g[p + "linelocs"], lineoffset, linecount, bool(isfirst),
                                                 int(g[p + "hsync_len"]))
-        want = set(map(tuple, g[p + "dropouts"].T.tolist()))
-        got = set(zip(lines, starts, ends))
-        same += len(want & got)
+        want = sorted(map(tuple, g[p + "dropouts"].T.tolist()))
+        got = sorted(zip(lines, starts, ends))
+        free = list(got)
+        unmatched = []
+        for w in want:
+            m = [x for x in free if x[0] == w[0] and abs(x[1] - w[1]) <= 1 and abs(x[2] - w[2]) <= 1]
+            if m:
+                best = min(m, key=lambda x: abs(x[1] - w[1]) + abs(x[2] - w[2]))
+                free.remove(best)
+                same += best == w
+            else:
+                unmatched.append(w)
         total += len(want)
-        assert abs(len(got) - len(want)) <= 2
-    assert same >= 0.9 * total and total > 20
+        assert not unmatched and not free, (system, i, "reference only", unmatched, "GPU only", free)
+    print(system, "dropouts", total, "identical", same)
+    assert total > 20
     rf.close()
