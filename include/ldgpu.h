@@ -623,6 +623,8 @@ typedef struct ldg_lines_args {
     const int32_t* prev_field_phase_dev;
     int32_t prev_field_phase;
     int32_t pad3;
+    double* linelocs2;          /* NTSC, optional out: the H-sync-refined line locations (Field.linelocs2),
+                                   nfields x LDG_CHAIN_MAX_LINES */
 } ldg_lines_args;
 
 int64_t ldg_lines_scratch_bytes(int32_t nfields);

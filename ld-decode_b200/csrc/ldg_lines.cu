@@ -688,6 +688,7 @@ __global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P)
     if (P.system == 0) {
         // NTSC: linelocs2 out, burst zero crossings per line
         if (i < nl) P.ll2[(long long)f * kMaxL + i] = ll[i];
+        if (i < nl && a.linelocs2) a.linelocs2[(long long)f * kMaxL + i] = ll[i];
         if (i < nl) a.linebad[(long long)f * kMaxL + i] = bad[i];
         if (i < kBurstLines && i < nl)
             burst_record(P, ll, i, a.linecount[f], a.burst + base, a.demod + base, n,

@@ -142,6 +142,43 @@ def downscale_audio(audio, lineinfo, rf, linecount, timeoffset=0, freq=44100, rv
     return output16, arange[-1] - frametime
 
 
+def downscale_audio_gpu(audio, lineinfo, rf, linecount, timeoffset=0, freq=44100, rv=None):
+    """downscale_audio (core.py:1538-1580) of one field on the GPU
+    (ldg_audio_downscale, one CTA): the same int16 samples, mute warning and
+    next-field offset as the host form."""
+    import torch
+
+    from . import lib as L
+    sp = rf.SysParams
+    off, soundgap, nticks, nxt = field_clock(sp["line_period"], linecount, timeoffset, freq)
+    n_out = 2 * max(nticks - 1, 0)
+    out16 = np.zeros(n_out, dtype=np.int16)
+    if n_out:
+        dev = torch.device("cuda", rf.device)
+        al = torch.from_numpy(np.ascontiguousarray(audio["audio_left"], dtype=np.float32)).to(dev)
+        ar = torch.from_numpy(np.ascontiguousarray(audio["audio_right"], dtype=np.float32)).to(dev)
+        ll = torch.from_numpy(np.ascontiguousarray(lineinfo, dtype=np.float64)).to(dev)
+        out = torch.empty(n_out, dtype=torch.int16, device=dev)
+        muted = torch.zeros(1, dtype=torch.int32, device=dev)
+        d = np.zeros(1, _AUDIO_DTYPE)
+        d["audio_left"], d["audio_right"], d["audio_len"] = al.data_ptr(), ar.data_ptr(), len(al)
+        d["linelocs"], d["nlines"], d["nticks"] = ll.data_ptr(), len(ll), nticks
+        d["timeoffset"], d["soundgap"], d["out"] = off, soundgap, out.data_ptr()
+        p = L.AudioParams(float(sp["line_period"]), float(rf.linelen), float(rf.Filters["audio_fdiv"]),
+                          float(sp["audio_lfreq"]), float(sp["audio_rfreq"]))
+        torch.cuda.current_stream(dev).synchronize()
+        descs = (L.AudioField * 1).from_buffer_copy(d.tobytes())
+        L.check(rf._ctx._lib.ldg_audio_downscale(rf._ctx.handle, descs, 1, ctypes.byref(p), muted.data_ptr(), 1))
+        torch.cuda.synchronize(dev)
+        out16 = out.cpu().numpy()
+        if int(muted.item()):
+            logger.warning("Analog audio processing error, muting samples")
+    if rv is not None:
+        rv["dsaudio"] = out16
+        rv["audio_next_offset"] = nxt
+    return out16, nxt
+
+
 def av_offset(rf, readloc, is_first, audio, lastfieldwritten):
     """Field.downscale's A/V alignment offset of a field's first audio
     sample (core.py:2644-2670): from the last written field's number and

@@ -4,8 +4,12 @@ Mirrors lddecode.core.Field / FieldNTSC / FieldPAL (lddecode/core.py:
 1587-3495).  `downscale()` keeps the reference signature
 (core.py:2626-2722) and returns (dsout, dsaudio, efmout); the resampling
 (computewow_scaled + scale_field + hz_to_output_array) runs on the GPU
-through ldg_tbc_fields.  The sync / line-location logic (process()) is the
-host restatement in ldgpu.linelocs.
+through ldg_tbc_fields, and the analog audio through ldg_audio_downscale.
+process() runs the GPU line path on the field's read (sync-run scan,
+native field chain, GPU refinement, field phase IDs); a read that needs the
+previous field's refined line locations or the reference's level
+re-calibration is decoded by the host restatement in ldgpu.linelocs, as in
+the batched path.
 """
 
 import ctypes
@@ -136,8 +140,8 @@ class Field(FieldLogic):
 
         dsaudio = None
         if audio != 0 and self.rf.decode_analog_audio:
-            from .audio import downscale_audio
-            dsaudio, self.audio_next_offset = downscale_audio(
+            from .audio import downscale_audio_gpu
+            dsaudio, self.audio_next_offset = downscale_audio_gpu(
                 self.data["audio"], lineinfo, self.rf, self.linecount, self.audio_offset(audio, lastfieldwritten),
                 audio)
         self.dsaudio = dsaudio
@@ -171,7 +175,26 @@ class Field(FieldLogic):
         return av_offset(self.rf, self.readloc, self.isFirstField, audio, lastfieldwritten)
 
 
+def _process(field, logic_cls):
+    """Field.process(): the GPU line path for the field's read
+    (LineLocator.process_field), else the host restatement (a read that
+    needs the previous field's refined line locations or the level
+    re-calibration, as in the batched path)."""
+    loc = getattr(field.rf, "_field_locator", None)
+    if loc is None:
+        from .lines import LineLocator
+        loc = field.rf._field_locator = LineLocator(field.rf)
+    if not loc.process_field(field):
+        logic_cls.process(field)
+    field.out_scale = np.double(0xD300 - 0x0100) / (100 - field.rf.DecoderParams["vsync_ire"]) \
+        if field.rf.system == "PAL" else np.double(0xC800 - 0x0400) / (100 - field.rf.DecoderParams["vsync_ire"])
+
+
 class FieldNTSC(FieldLogicNTSC, Field):
+    def process(self):
+        """core.py:3471-3495 on the GPU (see _process)."""
+        _process(self, FieldLogicNTSC)
+
     def downscale(self, lineoffset=0, final=False, *args, **kwargs):
         """core.py:3442-3451: audio only on the final pass."""
         if final is False and "audio" in kwargs:
@@ -180,6 +203,10 @@ class FieldNTSC(FieldLogicNTSC, Field):
 
 
 class FieldPAL(FieldLogicPAL, Field):
+    def process(self):
+        """core.py:3212-3239 on the GPU (see _process)."""
+        _process(self, FieldLogicPAL)
+
     def downscale(self, final=False, *args, **kwargs):
         """core.py:3205-3207."""
         return Field.downscale(self, final=final, *args, **kwargs)

@@ -143,7 +143,7 @@ class LinesArgs(ctypes.Structure):
         ("field_phase", c_p), ("scratch", c_p), ("stream", c_p), ("prev_phase_adjust_dev", c_p),
         ("first_field", c_i32), ("count", c_i32), ("stages", c_i32), ("pad2", c_i32),
         ("prev_pal_adjust", c_f64 * 4), ("prev_pal_adjust_dev", c_p), ("prev_field_phase_dev", c_p),
-        ("prev_field_phase", c_i32), ("pad3", c_i32),
+        ("prev_field_phase", c_i32), ("pad3", c_i32), ("linelocs2", c_p),
     ]
 
 

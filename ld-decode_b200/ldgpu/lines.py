@@ -489,7 +489,83 @@ class LineLocator:
         k = nr.value
         return starts[:k], lens[:k], means[:k]
 
-    def _refine(self, arrays, capture_len, plans, prev_pam, stream, prev_pam_dev=None):
+    def process_field(self, field):
+        """Field.process() of one field read on the GPU (the drop-in classes'
+        path, core.py:3212-3239 / 3471-3495): the field's own demodulated
+        read goes to the device, the sync-run scan, the native field chain
+        (one read, seeded from field.prevfield) and the GPU refinement give
+        its line locations, flags and field phase ID.  Returns False, with
+        `field` untouched, when the read needs what only the host
+        restatement does (the previous field's refined line locations, the
+        reference's level re-calibration, or a read shorter than a field
+        window); the caller then runs FieldLogic.process()."""
+        torch = self.torch
+        rf = self.rf
+        v = field.data["video"]
+        keys = self._keys()
+        n = len(v["demod_05"])
+        U = rf.blocklen - rf.blockcut - rf.blockcut_end
+        nblocks = n // U
+        dev = torch.device("cuda", torch.cuda.current_device())
+        arrays = {k: torch.from_numpy(np.ascontiguousarray(v[k], dtype=np.float32)).to(dev) for k in keys}
+        self.begin(arrays)
+        runs = self.sync_runs(arrays["demod_05"].data_ptr(), n)
+        prev = field.prevfield if getattr(field.prevfield, "valid", False) else None
+        st = L.ChainState()
+        st.start = float(rf.blockcut)  # the read window at the first block of the data
+        st.prev_valid = 1 if prev is not None else 0
+        st.prev_isfirst = int(bool(prev.isFirstField)) if prev is not None else 0
+        st.fields_written = int(field.fields_written)
+        plans, stop, _ = run_chain(rf, runs, nblocks, st, max_plans=1)
+        if len(plans) == 0:
+            return False
+        p = plans[0]
+        if not p.valid:
+            field.valid = False
+            field.nextfieldoffset = float(p.nextfieldoffset)
+            return True
+        valid = plans[:1].copy().view(np.recarray)
+        pam_host = 0.0
+        if self.pal:
+            pa = (getattr(prev, "phase_adjust", None) or {}) if prev is not None else {}
+            adj = [float("nan") if pa.get(l) is None else float(pa[l]) for l in range(7, 22, 4)]
+            self._pal_seed = ("host", adj, int(prev.fieldPhaseID) if prev is not None else 0)
+        elif prev is not None:
+            pam_host = float(prev.phase_adjust_median)
+        ll2 = None if self.pal else torch.empty((1, L.LDG_CHAIN_MAX_LINES), dtype=torch.float64, device=dev)
+        ll, bad, pam, fph, _ = self._refine(self._ptrs, n, valid, pam_host, None, linelocs2=ll2)
+        torch.cuda.synchronize()
+        nl = self.proclines
+        field.linelocs1 = np.array(p.linelocs1[:nl], dtype=np.float64)
+        field.linebad = bad[0].cpu().numpy()[:nl].astype(bool)
+        field.isFirstField = bool(p.isfirst)
+        field.sync_confidence = int(p.sync_confidence)
+        field.nextfieldoffset = float(p.nextfieldoffset)
+        field.LT = {"hsync": (None, int(p.hsync_len))}
+        field.fieldPhaseID = int(fph[0].item())
+        field.valid = True
+        final = ll[0].cpu().numpy()[:nl].copy()
+        if self.pal:
+            field.linelocs = final
+            field.linecount, field.lineoffset = 263 if field.isFirstField else 262, 0
+            field.burstmedian = field.calc_burstmedian()  # before the PAL line count and offset, as the reference
+            field.linecount = 312 if field.isFirstField else 313
+            field.lineoffset = 2 if field.isFirstField else 3
+            field.linecode = [field.decodephillipscode(l + field.lineoffset) for l in (16, 17, 18)]
+            adj = pam[0].cpu().numpy()
+            field.phase_adjust = {l: (None if np.isnan(x) else float(x)) for l, x in zip(range(7, 22, 4), adj)}
+        else:
+            field.linecount = int(p.linecount)
+            field.lineoffset = 0
+            field.linelocs2 = ll2[0].cpu().numpy()[:nl].copy()
+            field.linelocs = field.linelocs2  # linecode and the burst median read the H-sync line locations
+            field.linecode = [field.decodephillipscode(l + field.lineoffset) for l in (16, 17, 18)]
+            field.burstmedian = field.calc_burstmedian()
+            field.phase_adjust_median = float(pam[0].item())
+            field.linelocs = final
+        return True
+
+    def _refine(self, arrays, capture_len, plans, prev_pam, stream, prev_pam_dev=None, linelocs2=None):
         """ldg_lines_refine over valid plans (record array); device tensors.
         The NTSC burst seed of the first field is `prev_pam`, or the device
         double at `prev_pam_dev` when given (read in stream order)."""
@@ -560,6 +636,8 @@ class LineLocator:
         a.field_phase = fph.data_ptr()
         a.scratch = scratch.data_ptr()
         a.stream = _lib_stream(stream)
+        if linelocs2 is not None:
+            a.linelocs2 = linelocs2.data_ptr()
         ts = torch.cuda.ExternalStream(stream) if stream else torch.cuda.current_stream()
         ready = []
         if self.pal:
