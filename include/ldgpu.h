@@ -523,7 +523,16 @@ typedef struct ldg_chain_state {
     int32_t prev_isfirst;
     int64_t prev_startloc;
     int32_t fields_written;
-    int32_t pad;
+    /* What getLine0 (core.py:2156-2239) reads of the previous field's refined
+     * line locations, when the caller has it (prev_known = 1; the chain
+     * clears it after each field): skip_check() >= 50, its line at
+     * linecount as a sample position of the next field's read (line0loc_prev)
+     * and its sync confidence.  Without it the chain stops before a field
+     * that needs it (LDG_CHAIN_STOP_PREV). */
+    int32_t prev_known;
+    double prev_line0;
+    int32_t prev_skip;
+    int32_t prev_conf;
 } ldg_chain_state;
 
 typedef struct ldg_field_plan {

@@ -643,7 +643,11 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
             VBlank loc = loc_none;
             if (st.prev_valid) {
                 const VBlank loc_100 = fp.process_vblank(vp, 0, 100);
-                if (!(loc_100 == loc_none)) dep |= 1;  // needs the previous field's skip_check
+                if (st.prev_known) {
+                    if (st.prev_skip) loc = loc_100;  // limit 100 when prevfield.skip_check() >= 50
+                } else if (!(loc_100 == loc_none)) {
+                    dep |= 1;  // needs the previous field's skip_check
+                }
             }
             int sync_conf = 100;
             if (loc.zeroed_conf) sync_conf = 0;
@@ -671,21 +675,36 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
             bool range = false;
             double l0_lo = 0, l0_hi = 0;
             if (loc.ok && have_l0next && have_prev_l0) {
-                // median of (l0_local, l0_next, l0_prev): somewhere between the first two
                 const int votes = (int)loc.isfirst + (int)(!st.prev_isfirst) + (int)first_next;
                 isfirst = votes >= 2;
-                l0_lo = (double)std::min(loc.line0, l0_next);
-                l0_hi = (double)std::max(loc.line0, l0_next);
-                range = true;
                 have_l0 = true;
-                l0 = l0_lo;
+                if (st.prev_known) {
+                    // np.median of (l0_local, l0_next, l0_prev): the middle one
+                    double v[3] = {(double)loc.line0, (double)l0_next, st.prev_line0};
+                    std::sort(v, v + 3);
+                    l0 = v[1];
+                } else {
+                    // somewhere between the first two
+                    l0_lo = (double)std::min(loc.line0, l0_next);
+                    l0_hi = (double)std::max(loc.line0, l0_next);
+                    range = true;
+                    l0 = l0_lo;
+                }
             } else if (loc.ok && loc.conf > 50) {
                 sync_conf = std::min(sync_conf, 90);
                 l0 = (double)loc.line0;
                 isfirst = loc.isfirst;
                 have_l0 = true;
             } else if (have_prev_l0) {
-                dep |= 2;  // line 0 is the previous field's refined line location
+                if (st.prev_known) {
+                    // line 0 from the previous field's end
+                    l0 = st.prev_line0;
+                    isfirst = !st.prev_isfirst;
+                    sync_conf = std::min(sync_conf, std::max(st.prev_conf - 10, 10));
+                    have_l0 = true;
+                } else {
+                    dep |= 2;  // line 0 is the previous field's refined line location
+                }
             } else if (have_l0next) {
                 sync_conf = conf_next;
                 l0 = (double)l0_next;
@@ -734,6 +753,7 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
             pl.nextfieldoffset = nextfieldoffset;
             st.start += nextfieldoffset;
             st.prev_valid = 0;
+            st.prev_known = 0;
             np_out += 1;
             continue;
         }
@@ -751,6 +771,7 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
         st.prev_valid = 1;
         st.prev_isfirst = isfirst;
         st.prev_startloc = w.startloc;
+        st.prev_known = 0;  // this field's refined line locations are the caller's
         st.fields_written += 1;
         np_out += 1;
     }
@@ -808,6 +829,7 @@ Key key_of(const LdgChainParams& P, const LdgChainState& s) {
 // the chain state after a plan, as ldg_field_chain advances it
 LdgChainState advance(const LdgChainState& s, const LdgFieldPlan& p) {
     LdgChainState n = s;
+    n.prev_known = 0;
     if (p.valid) {
         n.start += p.nextfieldoffset - (double)(p.readloc - p.startloc);
         n.prev_valid = 1;

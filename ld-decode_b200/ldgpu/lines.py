@@ -435,7 +435,7 @@ class LineLocator:
         self.torch = torch
         self.proclines = proclines_for(rf)
         self.pal = rf.system == "PAL"
-        self.stats = {"batched": 0, "host": 0, "invalid": 0, "segments": 0}
+        self.stats = {"batched": 0, "host": 0, "invalid": 0, "segments": 0, "resolved": 0}
         self.timing = {}
         self._plans = np.empty(4096, PLAN_DTYPE)
         self._runbufs = None
@@ -517,6 +517,14 @@ class LineLocator:
         st.prev_isfirst = int(bool(prev.isFirstField)) if prev is not None else 0
         st.fields_written = int(field.fields_written)
         plans, stop, _ = run_chain(rf, runs, nblocks, st, max_plans=1)
+        if len(plans) == 0 and stop == L.LDG_CHAIN_STOP_PREV and prev is not None:
+            # getLine0's inputs from the previous field (skip_check, line0loc_prev)
+            st.prev_known = 1
+            st.prev_skip = 1 if prev.skip_check() >= 50 else 0
+            st.prev_line0 = float(np.asarray(prev.linelocs, dtype=np.float64)[prev.linecount]
+                                  - (field.data["startloc"] - prev.data["startloc"]))
+            st.prev_conf = int(prev.sync_confidence)
+            plans, stop, _ = run_chain(rf, runs, nblocks, st, max_plans=1)
         if len(plans) == 0:
             return False
         p = plans[0]
@@ -688,6 +696,7 @@ class LineLocator:
         self._pal_seed = ("host", [float("nan")] * 4, 0)  # PAL: the previous field's line phases and ID
         self._prev_host = None          # the previous field, if it was host-decoded
         self._last_dev = None           # index of the last batched field
+        self._last_ready = None         # event: its line locations are final
         self._ire0 = float(self.rf.DecoderParams["ire0"])
         self._reads = 0
         self._keep = []
@@ -750,41 +759,30 @@ class LineLocator:
                 plans = plans[:cut]
                 stop = L.LDG_CHAIN_STOP_PREV
                 st_out = self._state_after(plans, state)
-            valid = plans[plans.valid != 0].copy().view(np.recarray)
-            self.stats["invalid"] += len(plans) - len(valid)
-            self._reads += len(plans)
-            if len(valid):
-                self.stats["segments"] += 1
-                self.stats["batched"] += len(valid)
-                pam_host, pam_dev = 0.0, None
-                if not self.pal and valid.has_prev[0]:
-                    if self._pam[0] == "host":
-                        pam_host = self._pam[1]
-                    else:
-                        pam_dev = self._pam[1]
-                base = len(out)
-                ll, bad, pam, fph, ready = self._refine(ptrs, self._cap_len, valid, pam_host, stream, pam_dev)
-                self.ready.extend((base + lo, base + hi, ev) for lo, hi, ev in ready)
-                out._parts.append(("batch", valid, ll, pam, fph, bad))
-                out._cache = None
-                self._last_dev = len(out) - 1
-                self._prev_host = None
-                if not self.pal:
-                    self._pam = ("dev", pam.data_ptr() + 8 * (len(valid) - 1))
-                else:
-                    self._pal_seed = ("dev", pam.data_ptr() + 32 * (len(valid) - 1),
-                                      fph.data_ptr() + 4 * (len(valid) - 1))
-                self._keep.append((pam, fph))
-                t = self._tick("refine", t)
+            self._segment(plans, stream)
+            t = self._tick("refine", t)
             state = st_out
             if stop in (L.LDG_CHAIN_STOP_END, L.LDG_CHAIN_STOP_FULL):
                 if stop == L.LDG_CHAIN_STOP_FULL:
                     continue
                 break
-            # decode the next field on the host, with the previous field's results
             w = field_window(rf, state.start)
             if w.first_block + w.nblocks > nblocks:
                 break
+            # a field whose line 0 needs the previous field's refined line
+            # locations: hand them to the chain (skip_check, line0loc_prev) and
+            # let it go on; the host restatement only for what remains
+            if stop == L.LDG_CHAIN_STOP_PREV and cut is None and state.prev_valid and self._prev_inputs(state, w):
+                one, stop1, st1 = run_chain(rf, self._runs, nblocks, state, max_plans=1)
+                t = self._tick("chain", t)
+                if len(one):
+                    self.stats["resolved"] += 1
+                    self._segment(one, stream)
+                    t = self._tick("refine", t)
+                    state = st1
+                    continue
+                state.prev_known = 0
+            # decode the next field on the host, with the previous field's results
             prevfield = None
             if state.prev_valid:
                 if self._prev_host is not None:
@@ -838,6 +836,60 @@ class LineLocator:
             t = self._tick("host_fields", t)
         self._state = state
         return first_new, len(out)
+
+    def _segment(self, plans, stream):
+        """Refine the valid fields of a run of chain plans as one batch on
+        the GPU, seeded from the field before them."""
+        out = self.fields
+        valid = plans[plans.valid != 0].copy().view(np.recarray)
+        self.stats["invalid"] += len(plans) - len(valid)
+        self._reads += len(plans)
+        if not len(valid):
+            return
+        self.stats["segments"] += 1
+        self.stats["batched"] += len(valid)
+        pam_host, pam_dev = 0.0, None
+        if not self.pal and valid.has_prev[0]:
+            if self._pam[0] == "host":
+                pam_host = self._pam[1]
+            else:
+                pam_dev = self._pam[1]
+        base = len(out)
+        ll, bad, pam, fph, ready = self._refine(self._ptrs, self._cap_len, valid, pam_host, stream, pam_dev)
+        self.ready.extend((base + lo, base + hi, ev) for lo, hi, ev in ready)
+        self._last_ready = ready[-1][2]
+        out._parts.append(("batch", valid, ll, pam, fph, bad))
+        out._cache = None
+        self._last_dev = len(out) - 1
+        self._prev_host = None
+        if not self.pal:
+            self._pam = ("dev", pam.data_ptr() + 8 * (len(valid) - 1))
+        else:
+            self._pal_seed = ("dev", pam.data_ptr() + 32 * (len(valid) - 1), fph.data_ptr() + 4 * (len(valid) - 1))
+        self._keep.append((pam, fph))
+
+    def _prev_inputs(self, state, w):
+        """Fill state's previous-field inputs of getLine0 (skip_check() >= 50,
+        line0loc_prev, sync confidence) from the last located field, waiting
+        for its refinement; False when there is none."""
+        if self._prev_host is not None:
+            prev = self._prev_host
+            ll = np.asarray(prev.linelocs, dtype=np.float64)
+            skip = prev.skip_check()
+            lc, conf, prev_start = prev.linecount, prev.sync_confidence, prev.data["startloc"]
+        elif self._last_dev is not None:
+            self._last_ready.synchronize()
+            fl = self.fields[self._last_dev]
+            ll = fl.host_linelocs()
+            skip = self._proxy(self._arrays, fl, 0.0).skip_check()
+            lc, conf, prev_start = fl.linecount, fl.sync_confidence, fl.window.startloc
+        else:
+            return False
+        state.prev_known = 1
+        state.prev_skip = 1 if skip >= 50 else 0
+        state.prev_line0 = float(ll[lc] - (w.startloc - prev_start))
+        state.prev_conf = int(conf)
+        return True
 
     def _state_after(self, plans, state):
         """Chain state after the given plans (for a forced cut)."""

@@ -119,3 +119,65 @@ def test_parallel_chain_equals_serial(capture):
         assert stop2 == stop and st2.start == st.start
         assert len(got) == len(whole)
         assert got.tobytes() == whole.tobytes()
+
+
+def test_chain_takes_previous_field_inputs(monkeypatch):
+    """Seeded dropouts that hide a field's vertical interval make its line 0
+    depend on the previous field's refined line locations (getLine0,
+    core.py:2156-2239); the chain stops there, and given what getLine0
+    reads of the previous field (skip_check() >= 50, line0loc_prev, its
+    sync confidence; here from the host restatement's previous field) it
+    goes on and equals the host restatement for that field and after it."""
+    from ldgpu.fieldread import field_window
+    from ldgpu.linelocs import FieldLogic
+    from ldgpu.synth import inject_dropouts
+    rf = RFParams(system="NTSC")
+    rf.delays = {"video_rot": 3}
+    fieldlen = int(40e6 / (rf.SysParams["FPS"] * 2))
+    cap = synth_capture("NTSC", 12 * fieldlen, seed=5, start=1004, snr_db=36).numpy()
+    inject_dropouts(cap, 6, 240)
+    nb = blocks_in_capture(rf, len(cap))
+    from helpers import OracleBlocks
+    arrays = OracleBlocks(rf, cap, rf.scaled_mtf(1.0), ("demod", "demod_05", "demod_burst")).window(0, nb)
+    orig = FieldLogic.compute_linelocs
+
+    def recording(self):
+        rv = orig(self)
+        ll1, err, nxt = rv
+        self._pulse_level = (None if ll1 is None else np.array(ll1, np.float64),
+                             None if err is None else np.array(err), nxt)
+        return rv
+
+    monkeypatch.setattr(FieldLogic, "compute_linelocs", recording)
+    reads, _ = host_field_chain(rf, arrays, nb)
+    runs = host_sync_runs(rf, arrays["demod_05"])
+    st, plans, resolved = None, [], 0
+    while True:
+        got, stop, st = run_chain(rf, runs, nb, st)
+        plans.extend(got)
+        if stop == L.LDG_CHAIN_STOP_END:
+            break
+        assert stop == L.LDG_CHAIN_STOP_PREV and not st.prev_known
+        w_prev, prev = [r for r in reads[:len(plans)] if r[1].valid][-1]
+        w = field_window(rf, st.start)
+        st.prev_known = 1
+        st.prev_skip = 1 if prev.skip_check() >= 50 else 0
+        st.prev_line0 = float(np.asarray(prev.linelocs, np.float64)[prev.linecount] - (w.startloc - w_prev.startloc))
+        st.prev_conf = int(prev.sync_confidence)
+        resolved += 1
+    assert resolved >= 1
+    assert len(plans) == len(reads)
+    for p, (w, f) in zip(plans, reads):
+        assert (p.startloc, p.readloc) == (w.startloc, w.readloc)
+        assert bool(p.valid) == bool(f.valid)
+        if not f.valid:
+            continue
+        ll1, err, nxt = f._pulse_level
+        n = p.proclines
+        np.testing.assert_array_equal(np.frombuffer(p.linelocs1, np.float64)[:n], np.asarray(ll1, np.float64))
+        np.testing.assert_array_equal(np.frombuffer(p.linebad, np.uint8)[:n].astype(bool),
+                                      f.compute_deriv_error(ll1, err))
+        assert bool(p.isfirst) == bool(f.isFirstField)
+        assert p.nextfieldoffset == nxt
+        assert p.sync_confidence == f.sync_confidence
+    print("resolved", resolved, "of", len(plans), "reads")

@@ -90,7 +90,7 @@ def test_autotune_keeps_results(batch):
     res = autotune(mb.queue, mb.stream, grabs=(1, 2, 4), ctas=(0, 74), reps=1)
     assert res["best"] in res["ms"] and len(res["ms"]) == 6
     assert all(v > 0 for v in res["ms"].values())
-    assert mb.queue.schedule == res["best"]
+    assert mb.queue.schedule == res["best"][:2]
     mb.demod()
     _same(mb, refs)
     torch.cuda.synchronize()
