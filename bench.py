@@ -265,7 +265,8 @@ def run_gpu(args):
     marks = {"audio_ranges": 0}
 
     streamH = torch.cuda.Stream()              # host -> device input copies (end to end)
-    streamD = torch.cuda.Stream()              # device -> host output copies (end to end)
+    streamD = torch.cuda.Stream()              # device -> host EFM copies, chunk by chunk (end to end)
+    streamP = torch.cuda.Stream()              # device -> host picture / audio copies of finished field ranges
 
     streamJ = torch.cuda.Stream()              # joins a step's streams for its end event (overlapped steps)
 
@@ -280,10 +281,12 @@ def run_gpu(args):
         overlap = overlap or io is not None
         if bs.done is not None:
             # the set's previous step (its line locations, TBC and, end to
-            # end, its copies to the host) must be done before it is refilled
+            # end, its copies to the host) must be done before its outputs
+            # are refilled; its input may be refilled once that step's
+            # demodulator has read it
             for e in bs.done:
                 stream.wait_event(e)
-                streamH.wait_event(e)
+            streamH.wait_event(bs.demod_done)
             bs.done = None
         loc.begin(bs.farr)
         evs = []
@@ -327,24 +330,27 @@ def run_gpu(args):
                                             stride=AS)
                     marks["audio_ranges"] += 1
                 if io is not None:
+                    # on their own stream, so that the next chunks' EFM copies do not
+                    # queue behind copies that wait for the TBC
                     tev = torch.cuda.Event()
                     tev.record(streamC)
-                    streamD.wait_event(tev)
+                    streamP.wait_event(tev)
                     if do_audio:
                         aev = torch.cuda.Event()
                         aev.record(streamA)
-                        streamD.wait_event(aev)
-                    with torch.cuda.stream(streamD):
+                        streamP.wait_event(aev)
+                    with torch.cuda.stream(streamP):
                         io["pics"][lo * fsz:hi * fsz].copy_(bs.pics[lo * fsz:hi * fsz], non_blocking=True)
                         if do_audio:
                             io["aud"][lo * AS:hi * AS].copy_(bs.aud[lo * AS:hi * AS], non_blocking=True)
         marks["demod_end"] = evs[-1]
+        bs.demod_done = evs[-1]
         end = torch.cuda.Event(enable_timing=True)
         if overlap:
             # the next step (on the other buffer set) starts its demod while
             # this step's line locations, TBC and copies finish
             bs.done = []
-            for st_ in ([streamB, streamC, streamS, streamA] + ([streamD] if io is not None else [])):
+            for st_ in ([streamB, streamC, streamS, streamA] + ([streamD, streamP] if io is not None else [])):
                 e = torch.cuda.Event()
                 e.record(st_)
                 bs.done.append(e)
@@ -455,6 +461,7 @@ def run_gpu(args):
         for k in range(args.steps):
             step(ios[k % 2], sets[k % 2])
         stream.wait_stream(streamD)
+        stream.wait_stream(streamP)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
