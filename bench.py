@@ -629,7 +629,8 @@ def run_gpu(args):
         "linelocs_host_ms": {k: v / args.steps for k, v in loc.timing.items()},
         "linelocs_chain": {"threads": loc.threads, "equals_sequential_walk": chain_check,
                            "segments": segs, "host_decoded": loc.stats["host"] / args.steps,
-                           "prev_resolved": loc.stats["resolved"] / args.steps},
+                           "prev_resolved": loc.stats["resolved"] / args.steps,
+                           "prev_resolved_early": loc.stats["resolved_early"] / args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "ldg::demod_ip_kernel" if rf.fft_variant == 1 else "ldg::demod_kernel",

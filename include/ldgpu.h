@@ -524,13 +524,17 @@ typedef struct ldg_chain_state {
     int64_t prev_startloc;
     int32_t fields_written;
     /* What getLine0 (core.py:2156-2239) reads of the previous field's refined
-     * line locations, when the caller has it (prev_known = 1; the chain
-     * clears it after each field): skip_check() >= 50, its line at
-     * linecount as a sample position of the next field's read (line0loc_prev)
-     * and its sync confidence.  Without it the chain stops before a field
-     * that needs it (LDG_CHAIN_STOP_PREV). */
+     * line locations, when the caller has it (the chain clears it after each
+     * field): prev_known = 1 gives its line at linecount as a sample
+     * position of the next field's read (line0loc_prev) -- exactly when
+     * prev_line0 == prev_line0_hi, else only that it lies in [prev_line0,
+     * prev_line0_hi], which suffices when every line 0 that range allows
+     * assigns the pulses to the same line slots -- and its sync confidence;
+     * prev_skip is skip_check() >= 50 (1 / 0) or -1 for unknown.  Without
+     * what a field needs the chain stops before it (LDG_CHAIN_STOP_PREV). */
     int32_t prev_known;
     double prev_line0;
+    double prev_line0_hi;
     int32_t prev_skip;
     int32_t prev_conf;
 } ldg_chain_state;

@@ -643,10 +643,12 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
             VBlank loc = loc_none;
             if (st.prev_valid) {
                 const VBlank loc_100 = fp.process_vblank(vp, 0, 100);
-                if (st.prev_known) {
-                    if (st.prev_skip) loc = loc_100;  // limit 100 when prevfield.skip_check() >= 50
-                } else if (!(loc_100 == loc_none)) {
-                    dep |= 1;  // needs the previous field's skip_check
+                if (!(loc_100 == loc_none)) {
+                    if (st.prev_skip >= 0 && st.prev_known) {
+                        if (st.prev_skip) loc = loc_100;  // limit 100 when prevfield.skip_check() >= 50
+                    } else {
+                        dep |= 1;  // needs the previous field's skip_check
+                    }
                 }
             }
             int sync_conf = 100;
@@ -679,10 +681,17 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
                 isfirst = votes >= 2;
                 have_l0 = true;
                 if (st.prev_known) {
-                    // np.median of (l0_local, l0_next, l0_prev): the middle one
-                    double v[3] = {(double)loc.line0, (double)l0_next, st.prev_line0};
-                    std::sort(v, v + 3);
-                    l0 = v[1];
+                    // np.median of (l0_local, l0_next, l0_prev), monotonic in
+                    // l0_prev: the range its known bounds allow
+                    auto med3 = [](double a, double b, double c) {
+                        double v[3] = {a, b, c};
+                        std::sort(v, v + 3);
+                        return v[1];
+                    };
+                    l0_lo = med3((double)loc.line0, (double)l0_next, st.prev_line0);
+                    l0_hi = med3((double)loc.line0, (double)l0_next, st.prev_line0_hi);
+                    range = l0_hi != l0_lo;
+                    l0 = l0_lo;
                 } else {
                     // somewhere between the first two
                     l0_lo = (double)std::min(loc.line0, l0_next);
@@ -697,8 +706,10 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
                 have_l0 = true;
             } else if (have_prev_l0) {
                 if (st.prev_known) {
-                    // line 0 from the previous field's end
-                    l0 = st.prev_line0;
+                    // line 0 from the previous field's end (or the range it is known in)
+                    l0 = l0_lo = st.prev_line0;
+                    l0_hi = st.prev_line0_hi;
+                    range = l0_hi != l0_lo;
                     isfirst = !st.prev_isfirst;
                     sync_conf = std::min(sync_conf, std::max(st.prev_conf - 10, 10));
                     have_l0 = true;

@@ -83,8 +83,8 @@ class ChainParams(ctypes.Structure):
 
 class ChainState(ctypes.Structure):
     _fields_ = [("start", c_f64), ("prev_valid", c_i32), ("prev_isfirst", c_i32), ("prev_startloc", c_i64),
-                ("fields_written", c_i32), ("prev_known", c_i32), ("prev_line0", c_f64), ("prev_skip", c_i32),
-                ("prev_conf", c_i32)]
+                ("fields_written", c_i32), ("prev_known", c_i32), ("prev_line0", c_f64), ("prev_line0_hi", c_f64),
+                ("prev_skip", c_i32), ("prev_conf", c_i32)]
 
 
 class FieldPlan(ctypes.Structure):

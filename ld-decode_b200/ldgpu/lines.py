@@ -435,7 +435,7 @@ class LineLocator:
         self.torch = torch
         self.proclines = proclines_for(rf)
         self.pal = rf.system == "PAL"
-        self.stats = {"batched": 0, "host": 0, "invalid": 0, "segments": 0, "resolved": 0}
+        self.stats = {"batched": 0, "host": 0, "invalid": 0, "segments": 0, "resolved": 0, "resolved_early": 0}
         self.timing = {}
         self._plans = np.empty(4096, PLAN_DTYPE)
         self._runbufs = None
@@ -521,8 +521,8 @@ class LineLocator:
             # getLine0's inputs from the previous field (skip_check, line0loc_prev)
             st.prev_known = 1
             st.prev_skip = 1 if prev.skip_check() >= 50 else 0
-            st.prev_line0 = float(np.asarray(prev.linelocs, dtype=np.float64)[prev.linecount]
-                                  - (field.data["startloc"] - prev.data["startloc"]))
+            st.prev_line0 = st.prev_line0_hi = float(np.asarray(prev.linelocs, dtype=np.float64)[prev.linecount]
+                                                     - (field.data["startloc"] - prev.data["startloc"]))
             st.prev_conf = int(prev.sync_confidence)
             plans, stop, _ = run_chain(rf, runs, nblocks, st, max_plans=1)
         if len(plans) == 0:
@@ -772,14 +772,24 @@ class LineLocator:
             # a field whose line 0 needs the previous field's refined line
             # locations: hand them to the chain (skip_check, line0loc_prev) and
             # let it go on; the host restatement only for what remains
-            if stop == L.LDG_CHAIN_STOP_PREV and cut is None and state.prev_valid and self._prev_inputs(state, w):
-                one, stop1, st1 = run_chain(rf, self._runs, nblocks, state, max_plans=1)
-                t = self._tick("chain", t)
-                if len(one):
-                    self.stats["resolved"] += 1
-                    self._segment(one, stream)
-                    t = self._tick("refine", t)
-                    state = st1
+            if stop == L.LDG_CHAIN_STOP_PREV and cut is None and state.prev_valid:
+                # first from the previous field's pulse-level line locations
+                # (no wait: a range its refined ones lie in), then exactly
+                # (after waiting for its refinement)
+                done = False
+                for exact in (False, True):
+                    if not self._prev_inputs(state, w, exact):
+                        continue
+                    one, stop1, st1 = run_chain(rf, self._runs, nblocks, state, max_plans=1)
+                    t = self._tick("chain", t)
+                    if len(one):
+                        self.stats["resolved" if exact else "resolved_early"] += 1
+                        self._segment(one, stream)
+                        t = self._tick("refine", t)
+                        state = st1
+                        done = True
+                        break
+                if done:
                     continue
                 state.prev_known = 0
             # decode the next field on the host, with the previous field's results
@@ -858,6 +868,7 @@ class LineLocator:
         ll, bad, pam, fph, ready = self._refine(self._ptrs, self._cap_len, valid, pam_host, stream, pam_dev)
         self.ready.extend((base + lo, base + hi, ev) for lo, hi, ev in ready)
         self._last_ready = ready[-1][2]
+        self._last_plan = valid[-1]
         out._parts.append(("batch", valid, ll, pam, fph, bad))
         out._cache = None
         self._last_dev = len(out) - 1
@@ -868,16 +879,36 @@ class LineLocator:
             self._pal_seed = ("dev", pam.data_ptr() + 32 * (len(valid) - 1), fph.data_ptr() + 4 * (len(valid) - 1))
         self._keep.append((pam, fph))
 
-    def _prev_inputs(self, state, w):
-        """Fill state's previous-field inputs of getLine0 (skip_check() >= 50,
-        line0loc_prev, sync confidence) from the last located field, waiting
-        for its refinement; False when there is none."""
+    # how far a field's refined line location can lie from its pulse-level
+    # one (H-sync crossing, burst or pilot alignment, the NTSC subcarrier
+    # shift): a few samples; the range handed to the chain allows 32
+    PREV_LINE_MARGIN = 32.0
+
+    def _prev_inputs(self, state, w, exact):
+        """Fill state's previous-field inputs of getLine0 from the last
+        located field: exactly (skip_check() >= 50, line0loc_prev, sync
+        confidence; for a batched field after waiting for its refinement),
+        or, with exact=False, only the range line0loc_prev lies in from the
+        field's pulse-level line locations, without waiting.  False when
+        there is nothing to give."""
         if self._prev_host is not None:
+            if not exact:
+                return False  # the exact values are at hand: the second pass
             prev = self._prev_host
             ll = np.asarray(prev.linelocs, dtype=np.float64)
             skip = prev.skip_check()
             lc, conf, prev_start = prev.linecount, prev.sync_confidence, prev.data["startloc"]
         elif self._last_dev is not None:
+            if not exact:
+                p = self._last_plan
+                lc = (312 if p.isfirst else 313) if self.pal else int(p.linecount)
+                est = float(p.linelocs1[lc]) - (w.startloc - int(p.startloc))
+                state.prev_known = 1
+                state.prev_line0 = est - self.PREV_LINE_MARGIN
+                state.prev_line0_hi = est + self.PREV_LINE_MARGIN
+                state.prev_skip = -1
+                state.prev_conf = int(p.sync_confidence)
+                return True
             self._last_ready.synchronize()
             fl = self.fields[self._last_dev]
             ll = fl.host_linelocs()
@@ -887,7 +918,7 @@ class LineLocator:
             return False
         state.prev_known = 1
         state.prev_skip = 1 if skip >= 50 else 0
-        state.prev_line0 = float(ll[lc] - (w.startloc - prev_start))
+        state.prev_line0 = state.prev_line0_hi = float(ll[lc] - (w.startloc - prev_start))
         state.prev_conf = int(conf)
         return True
 

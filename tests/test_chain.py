@@ -151,7 +151,7 @@ def test_chain_takes_previous_field_inputs(monkeypatch):
     monkeypatch.setattr(FieldLogic, "compute_linelocs", recording)
     reads, _ = host_field_chain(rf, arrays, nb)
     runs = host_sync_runs(rf, arrays["demod_05"])
-    st, plans, resolved = None, [], 0
+    st, plans, resolved, ranged = None, [], 0, 0
     while True:
         got, stop, st = run_chain(rf, runs, nb, st)
         plans.extend(got)
@@ -160,10 +160,21 @@ def test_chain_takes_previous_field_inputs(monkeypatch):
         assert stop == L.LDG_CHAIN_STOP_PREV and not st.prev_known
         w_prev, prev = [r for r in reads[:len(plans)] if r[1].valid][-1]
         w = field_window(rf, st.start)
-        st.prev_known = 1
+        exact = float(np.asarray(prev.linelocs, np.float64)[prev.linecount] - (w.startloc - w_prev.startloc))
+        # a range of +-32 samples around it and skip_check unknown: the chain
+        # either plans this field exactly as with the exact inputs, or stops
+        st.prev_known, st.prev_skip, st.prev_conf = 1, -1, int(prev.sync_confidence)
+        st.prev_line0, st.prev_line0_hi = exact - 32.0, exact + 32.0
+        one, stop1, st1 = run_chain(rf, runs, nb, st, max_plans=1)
         st.prev_skip = 1 if prev.skip_check() >= 50 else 0
-        st.prev_line0 = float(np.asarray(prev.linelocs, np.float64)[prev.linecount] - (w.startloc - w_prev.startloc))
-        st.prev_conf = int(prev.sync_confidence)
+        st.prev_line0 = st.prev_line0_hi = exact
+        one_x, _, st_x = run_chain(rf, runs, nb, st, max_plans=1)
+        assert len(one_x) == 1
+        if len(one):
+            assert one.tobytes() == one_x.tobytes()
+            ranged += 1
+        else:
+            assert stop1 == L.LDG_CHAIN_STOP_PREV
         resolved += 1
     assert resolved >= 1
     assert len(plans) == len(reads)
@@ -180,4 +191,4 @@ def test_chain_takes_previous_field_inputs(monkeypatch):
         assert bool(p.isfirst) == bool(f.isFirstField)
         assert p.nextfieldoffset == nxt
         assert p.sync_confidence == f.sync_confidence
-    print("resolved", resolved, "of", len(plans), "reads")
+    print("resolved", resolved, "of", len(plans), "reads;", ranged, "from the range alone")
