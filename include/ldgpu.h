@@ -537,14 +537,27 @@ typedef struct ldg_chain_state {
     double prev_line0_hi;
     int32_t prev_skip;
     int32_t prev_conf;
+    /* Set by the chain after each valid field: the capture-wide sample
+     * position of that field's pulse-level line at linecount (PAL: 312 /
+     * 313) and its sync confidence.  When a field needs what prev_known
+     * gives and the caller has not given it, the chain first retries the
+     * field with line0loc_prev known only to lie within
+     * LDG_CHAIN_PREV_MARGIN samples of this estimate (the refined line
+     * locations move a line by a few samples at most) and skip_check
+     * unknown; it stops only if that does not decide the field. */
+    double prev_est;
+    int32_t prev_est_valid;
+    int32_t prev_est_conf;
 } ldg_chain_state;
+
+#define LDG_CHAIN_PREV_MARGIN 32.0
 
 typedef struct ldg_field_plan {
     double start;
     int64_t readloc, first_block, nblocks, startloc, length;  /* the field's read window (fieldread) */
     int32_t valid, isfirst, linecount, proclines, has_prev, sync_confidence;
     int32_t hsync_len;                        /* int(Field.LT["hsync"][1]) (dropout detection) */
-    int32_t pad0;
+    int32_t prev_range;                       /* 1: planned from the previous field's estimate (prev_est) */
     double nextfieldoffset;
     double linelocs1[LDG_CHAIN_MAX_LINES];   /* pulse-level line locations (field-local samples) */
     uint8_t linebad[LDG_CHAIN_MAX_LINES];

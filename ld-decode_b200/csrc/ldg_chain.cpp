@@ -17,9 +17,11 @@
 //
 // Decisions that depend on the previous field's GPU-refined line locations
 // (the line-0 vote of getLine0 when it can change the result, the
-// skip_check limit of processVBlank) are detected and reported instead of
-// guessed: the chain stops before such a field (LDG_CHAIN_STOP_PREV) and
-// the caller decodes it with full information.  The same holds for the
+// skip_check limit of processVBlank) are detected instead of guessed: the
+// field is retried with the range the previous field's pulse-level line
+// locations put its refined line at, and only if that range leaves the
+// result open does the chain stop before the field (LDG_CHAIN_STOP_PREV)
+// for the caller to decode it with full information.  The same holds for the
 // reference's level-recalibration branches of getpulses
 // (LDG_CHAIN_STOP_LEVELS).
 #include <algorithm>
@@ -549,6 +551,30 @@ Window field_window(const LdgChainParams& P, double start) {
 
 thread_local std::string g_chain_err;
 
+// The chain state after plan p (read at state s): the next read position,
+// the previous-field flags and the estimate of the field's line at
+// linecount; the caller's refined-line inputs are cleared.
+LdgChainState advance_state(const LdgChainParams& P, const LdgChainState& s, const LdgFieldPlan& p) {
+    LdgChainState n = s;
+    n.prev_known = 0;
+    if (p.valid) {
+        n.start += p.nextfieldoffset - (double)(p.readloc - p.startloc);
+        n.prev_valid = 1;
+        n.prev_isfirst = p.isfirst;
+        n.prev_startloc = p.startloc;
+        n.fields_written += 1;
+        const int lc = P.system == 1 ? (p.isfirst ? 312 : 313) : p.linecount;
+        n.prev_est_valid = lc >= 0 && lc < p.proclines;
+        n.prev_est = n.prev_est_valid ? (double)p.startloc + p.linelocs1[lc] : 0.0;
+        n.prev_est_conf = p.sync_confidence;
+    } else {
+        n.start += p.nextfieldoffset;
+        n.prev_valid = 0;
+        n.prev_est_valid = 0;
+    }
+    return n;
+}
+
 }  // namespace
 
 extern "C" {
@@ -571,6 +597,26 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
     int np_out = 0;
     *stop = LDG_CHAIN_STOP_END;
     const double minlength = 10.0 * P->linefreq0;  // usectoinpx(10)
+    // the field at st.start is being retried with the previous field's estimate
+    bool est_tried = false;
+    // a field that needs the previous field's refined line locations: retry
+    // it once with the range the previous field's pulse-level estimate gives
+    auto retry_with_estimate = [&](const Window& w) {
+        if (est_tried || st.prev_known || !st.prev_est_valid || !st.prev_valid) return false;
+        const double e = st.prev_est - (double)w.startloc;
+        st.prev_known = 1;
+        st.prev_line0 = e - LDG_CHAIN_PREV_MARGIN;
+        st.prev_line0_hi = e + LDG_CHAIN_PREV_MARGIN;
+        st.prev_skip = -1;
+        st.prev_conf = st.prev_est_conf;
+        est_tried = true;
+        return true;
+    };
+    auto give_up = [&]() {
+        if (est_tried) st.prev_known = 0;  // the caller's inputs were not given
+        est_tried = false;
+        *stop = LDG_CHAIN_STOP_PREV;
+    };
     while (np_out < max_plans) {
         const Window w = field_window(*P, st.start);
         if (w.first_block + w.nblocks > P->nblocks) {
@@ -724,7 +770,8 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
             }
             pl.sync_confidence = sync_conf;
             if (dep) {
-                *stop = LDG_CHAIN_STOP_PREV;
+                if (retry_with_estimate(w)) continue;
+                give_up();
                 break;
             }
             const int linecount = isfirst ? 263 : 262;
@@ -742,7 +789,8 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
                     // both ends of the vote's range hold inside it unless the skip rule,
                     // which compares against a line-0-independent estimate, is active
                     if (!same_slots(slots, s2) || slots.skipdetected || s2.skipdetected) {
-                        *stop = LDG_CHAIN_STOP_PREV;
+                        if (retry_with_estimate(w)) continue;
+                        give_up();
                         break;
                     }
                 }
@@ -758,13 +806,13 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
             }
             pl.linecount = linecount;
         }
+        pl.prev_range = est_tried ? 1 : 0;
+        est_tried = false;
         if (invalid) {
             if (!have_next) nextfieldoffset = P->linelen * 200;
             pl.valid = 0;
             pl.nextfieldoffset = nextfieldoffset;
-            st.start += nextfieldoffset;
-            st.prev_valid = 0;
-            st.prev_known = 0;
+            st = advance_state(*P, st, pl);
             np_out += 1;
             continue;
         }
@@ -778,14 +826,10 @@ int ldg_field_chain(const LdgChainParams* P, const int64_t* run_start, const int
             pl.linelocs1[l] = slots.filled[l];
             pl.linebad[l] = bad[l];
         }
-        st.start += slots.nextfield - (double)(w.readloc - w.startloc);
-        st.prev_valid = 1;
-        st.prev_isfirst = isfirst;
-        st.prev_startloc = w.startloc;
-        st.prev_known = 0;  // this field's refined line locations are the caller's
-        st.fields_written += 1;
+        st = advance_state(*P, st, pl);
         np_out += 1;
     }
+    if (est_tried) st.prev_known = 0;  // stopped while retrying: the estimate is not the caller's
     if (np_out >= max_plans && *stop == LDG_CHAIN_STOP_END) *stop = LDG_CHAIN_STOP_FULL;
     *nplans = np_out;
     *state_out = st;
@@ -837,22 +881,6 @@ Key key_of(const LdgChainParams& P, const LdgChainState& s) {
     return {readloc_of(P, s.start), s.prev_valid, s.prev_valid ? s.prev_isfirst : 0, s.fields_written > 0};
 }
 
-// the chain state after a plan, as ldg_field_chain advances it
-LdgChainState advance(const LdgChainState& s, const LdgFieldPlan& p) {
-    LdgChainState n = s;
-    n.prev_known = 0;
-    if (p.valid) {
-        n.start += p.nextfieldoffset - (double)(p.readloc - p.startloc);
-        n.prev_valid = 1;
-        n.prev_isfirst = p.isfirst;
-        n.prev_startloc = p.startloc;
-        n.fields_written += 1;
-    } else {
-        n.start += p.nextfieldoffset;
-        n.prev_valid = 0;
-    }
-    return n;
-}
 
 struct Piece {
     std::vector<LdgFieldPlan> plans;
@@ -922,7 +950,7 @@ extern "C" int ldg_field_chain_mt(const LdgChainParams* P, const int64_t* run_st
         LdgChainState s = pcs[0].in;
         for (const LdgFieldPlan& p : merged) {
             before.push_back(s);
-            s = advance(s, p);
+            s = advance_state(*P, s, p);
         }
     }
     int32_t stp = pcs[0].stop;
@@ -935,11 +963,13 @@ extern "C" int ldg_field_chain_mt(const LdgChainParams* P, const int64_t* run_st
             break;
         }
         std::vector<Key> tk;
+        std::vector<LdgChainState> ts;  // the piece's state before each of its plans
         {
             LdgChainState s = pc.in;
             for (const LdgFieldPlan& p : pc.plans) {
                 tk.push_back(key_of(*P, s));
-                s = advance(s, p);
+                ts.push_back(s);
+                s = advance_state(*P, s, p);
             }
         }
         const long long lo = pc.plans[0].readloc;
@@ -962,7 +992,7 @@ extern "C" int ldg_field_chain_mt(const LdgChainParams* P, const int64_t* run_st
         // sample in `start` differs, the read windows must not
         merged.resize(ji);
         before.resize(ji);
-        LdgChainState s = ji ? advance(before.back(), merged.back()) : pcs[0].in;
+        LdgChainState s = ji ? advance_state(*P, before.back(), merged.back()) : pcs[0].in;
         bool moved = false;
         for (size_t j = jj; j < pc.plans.size(); ++j) {
             LdgFieldPlan p = pc.plans[j];
@@ -970,10 +1000,16 @@ extern "C" int ldg_field_chain_mt(const LdgChainParams* P, const int64_t* run_st
                 moved = true;
                 break;
             }
+            // a plan decided from the previous field's estimate holds for the
+            // true chain when its estimate is the same to within a sample
+            if (p.prev_range && (!s.prev_est_valid || std::fabs(s.prev_est - ts[j].prev_est) > 1.0)) {
+                moved = true;
+                break;
+            }
             p.start = s.start;
             merged.push_back(p);
             before.push_back(s);
-            s = advance(s, p);
+            s = advance_state(*P, s, p);
         }
         st_end = s;
         stp = pc.stop;
@@ -996,7 +1032,7 @@ extern "C" int ldg_field_chain_mt(const LdgChainParams* P, const int64_t* run_st
     if ((int64_t)merged.size() > max_plans) {
         // the caller's buffer is full: stop where it ends
         LdgChainState s = pcs[0].in;
-        for (int32_t k = 0; k < max_plans; ++k) s = advance(s, merged[k]);
+        for (int32_t k = 0; k < max_plans; ++k) s = advance_state(*P, s, merged[k]);
         merged.resize(max_plans);
         st_end = s;
         stp = LDG_CHAIN_STOP_FULL;

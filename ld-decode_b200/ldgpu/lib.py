@@ -84,14 +84,15 @@ class ChainParams(ctypes.Structure):
 class ChainState(ctypes.Structure):
     _fields_ = [("start", c_f64), ("prev_valid", c_i32), ("prev_isfirst", c_i32), ("prev_startloc", c_i64),
                 ("fields_written", c_i32), ("prev_known", c_i32), ("prev_line0", c_f64), ("prev_line0_hi", c_f64),
-                ("prev_skip", c_i32), ("prev_conf", c_i32)]
+                ("prev_skip", c_i32), ("prev_conf", c_i32), ("prev_est", c_f64), ("prev_est_valid", c_i32),
+                ("prev_est_conf", c_i32)]
 
 
 class FieldPlan(ctypes.Structure):
     _fields_ = [
         ("start", c_f64), ("readloc", c_i64), ("first_block", c_i64), ("nblocks", c_i64), ("startloc", c_i64),
         ("length", c_i64), ("valid", c_i32), ("isfirst", c_i32), ("linecount", c_i32), ("proclines", c_i32),
-        ("has_prev", c_i32), ("sync_confidence", c_i32), ("hsync_len", c_i32), ("pad0", c_i32),
+        ("has_prev", c_i32), ("sync_confidence", c_i32), ("hsync_len", c_i32), ("prev_range", c_i32),
         ("nextfieldoffset", c_f64),
         ("linelocs1", c_f64 * LDG_CHAIN_MAX_LINES), ("linebad", ctypes.c_uint8 * LDG_CHAIN_MAX_LINES),
     ]

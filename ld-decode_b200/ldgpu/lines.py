@@ -47,7 +47,7 @@ _ML = L.LDG_CHAIN_MAX_LINES
 PLAN_DTYPE = _dtype_of(L.FieldPlan, {
     "start": "f8", "readloc": "i8", "first_block": "i8", "nblocks": "i8", "startloc": "i8", "length": "i8",
     "valid": "i4", "isfirst": "i4", "linecount": "i4", "proclines": "i4", "has_prev": "i4",
-    "sync_confidence": "i4", "hsync_len": "i4", "pad0": "i4", "nextfieldoffset": "f8", "linelocs1": ("f8", (_ML,)),
+    "sync_confidence": "i4", "hsync_len": "i4", "prev_range": "i4", "nextfieldoffset": "f8", "linelocs1": ("f8", (_ML,)),
     "linebad": ("u1", (_ML,))})
 TBC_DTYPE = _dtype_of(L.TbcField, {
     "buf": "u8", "buf_len": "i8", "linelocs": "u8", "nlines": "i4", "lineoffset": "i4", "outwidth": "i4",
@@ -770,26 +770,18 @@ class LineLocator:
             if w.first_block + w.nblocks > nblocks:
                 break
             # a field whose line 0 needs the previous field's refined line
-            # locations: hand them to the chain (skip_check, line0loc_prev) and
-            # let it go on; the host restatement only for what remains
-            if stop == L.LDG_CHAIN_STOP_PREV and cut is None and state.prev_valid:
-                # first from the previous field's pulse-level line locations
-                # (no wait: a range its refined ones lie in), then exactly
-                # (after waiting for its refinement)
-                done = False
-                for exact in (False, True):
-                    if not self._prev_inputs(state, w, exact):
-                        continue
-                    one, stop1, st1 = run_chain(rf, self._runs, nblocks, state, max_plans=1)
-                    t = self._tick("chain", t)
-                    if len(one):
-                        self.stats["resolved" if exact else "resolved_early"] += 1
-                        self._segment(one, stream)
-                        t = self._tick("refine", t)
-                        state = st1
-                        done = True
-                        break
-                if done:
+            # locations and that the chain could not decide from the range of
+            # their pulse-level estimate: wait for them, hand them to the
+            # chain (skip_check, line0loc_prev) and let it go on; the host
+            # restatement only for what remains
+            if stop == L.LDG_CHAIN_STOP_PREV and cut is None and state.prev_valid and self._prev_inputs(state, w):
+                one, stop1, st1 = run_chain(rf, self._runs, nblocks, state, max_plans=1)
+                t = self._tick("chain", t)
+                if len(one):
+                    self.stats["resolved"] += 1
+                    self._segment(one, stream)
+                    t = self._tick("refine", t)
+                    state = st1
                     continue
                 state.prev_known = 0
             # decode the next field on the host, with the previous field's results
@@ -807,6 +799,7 @@ class LineLocator:
                 self.stats["invalid"] += 1
                 state.start += f.nextfieldoffset
                 state.prev_valid = 0
+                state.prev_est_valid = 0
                 self._prev_host = None
                 self._pam = ("host", 0.0)
                 self._pal_seed = ("host", [float("nan")] * 4, 0)
@@ -831,6 +824,9 @@ class LineLocator:
             state.prev_isfirst = int(bool(f.isFirstField))
             state.prev_startloc = w.startloc
             state.fields_written += 1
+            state.prev_est = float(w.startloc + ll_host[f.linecount])
+            state.prev_est_valid = 1
+            state.prev_est_conf = int(f.sync_confidence)
             self._prev_host = f
             self._pam = ("host", float(f.phase_adjust_median) if not self.pal else 0.0)
             if self.pal:
@@ -858,6 +854,7 @@ class LineLocator:
             return
         self.stats["segments"] += 1
         self.stats["batched"] += len(valid)
+        self.stats["resolved_early"] += int(np.count_nonzero(valid.prev_range))
         pam_host, pam_dev = 0.0, None
         if not self.pal and valid.has_prev[0]:
             if self._pam[0] == "host":
@@ -868,7 +865,6 @@ class LineLocator:
         ll, bad, pam, fph, ready = self._refine(self._ptrs, self._cap_len, valid, pam_host, stream, pam_dev)
         self.ready.extend((base + lo, base + hi, ev) for lo, hi, ev in ready)
         self._last_ready = ready[-1][2]
-        self._last_plan = valid[-1]
         out._parts.append(("batch", valid, ll, pam, fph, bad))
         out._cache = None
         self._last_dev = len(out) - 1
@@ -879,36 +875,17 @@ class LineLocator:
             self._pal_seed = ("dev", pam.data_ptr() + 32 * (len(valid) - 1), fph.data_ptr() + 4 * (len(valid) - 1))
         self._keep.append((pam, fph))
 
-    # how far a field's refined line location can lie from its pulse-level
-    # one (H-sync crossing, burst or pilot alignment, the NTSC subcarrier
-    # shift): a few samples; the range handed to the chain allows 32
-    PREV_LINE_MARGIN = 32.0
-
-    def _prev_inputs(self, state, w, exact):
-        """Fill state's previous-field inputs of getLine0 from the last
-        located field: exactly (skip_check() >= 50, line0loc_prev, sync
-        confidence; for a batched field after waiting for its refinement),
-        or, with exact=False, only the range line0loc_prev lies in from the
-        field's pulse-level line locations, without waiting.  False when
-        there is nothing to give."""
+    def _prev_inputs(self, state, w):
+        """Fill state's previous-field inputs of getLine0 exactly from the
+        last located field (skip_check() >= 50, line0loc_prev, sync
+        confidence; for a batched field after waiting for its refinement).
+        False when there is none."""
         if self._prev_host is not None:
-            if not exact:
-                return False  # the exact values are at hand: the second pass
             prev = self._prev_host
             ll = np.asarray(prev.linelocs, dtype=np.float64)
             skip = prev.skip_check()
             lc, conf, prev_start = prev.linecount, prev.sync_confidence, prev.data["startloc"]
         elif self._last_dev is not None:
-            if not exact:
-                p = self._last_plan
-                lc = (312 if p.isfirst else 313) if self.pal else int(p.linecount)
-                est = float(p.linelocs1[lc]) - (w.startloc - int(p.startloc))
-                state.prev_known = 1
-                state.prev_line0 = est - self.PREV_LINE_MARGIN
-                state.prev_line0_hi = est + self.PREV_LINE_MARGIN
-                state.prev_skip = -1
-                state.prev_conf = int(p.sync_confidence)
-                return True
             self._last_ready.synchronize()
             fl = self.fields[self._last_dev]
             ll = fl.host_linelocs()
@@ -927,15 +904,21 @@ class LineLocator:
         st = L.ChainState()
         ctypes.memmove(ctypes.byref(st), ctypes.byref(state), ctypes.sizeof(st))
         for p in plans:
+            st.prev_known = 0
             if not p.valid:
                 st.start += p.nextfieldoffset
                 st.prev_valid = 0
+                st.prev_est_valid = 0
                 continue
             st.start += p.nextfieldoffset - (p.readloc - p.startloc)
             st.prev_valid = 1
             st.prev_isfirst = p.isfirst
             st.prev_startloc = p.startloc
             st.fields_written += 1
+            lc = (312 if p.isfirst else 313) if self.pal else int(p.linecount)
+            st.prev_est = float(p.startloc + p.linelocs1[lc])
+            st.prev_est_valid = 1
+            st.prev_est_conf = int(p.sync_confidence)
         return st
 
     def _window_host(self, arrays, w, keys):

@@ -124,10 +124,13 @@ def test_parallel_chain_equals_serial(capture):
 def test_chain_takes_previous_field_inputs(monkeypatch):
     """Seeded dropouts that hide a field's vertical interval make its line 0
     depend on the previous field's refined line locations (getLine0,
-    core.py:2156-2239); the chain stops there, and given what getLine0
-    reads of the previous field (skip_check() >= 50, line0loc_prev, its
-    sync confidence; here from the host restatement's previous field) it
-    goes on and equals the host restatement for that field and after it."""
+    core.py:2156-2239).  The chain first retries such a field with the range
+    of +-32 samples around the previous field's pulse-level estimate and
+    skip_check unknown: a plan made so (prev_range) is byte for byte the plan
+    the exact inputs give.  Where the range leaves the field open it stops;
+    given what getLine0 reads of the previous field (skip_check() >= 50,
+    line0loc_prev, its sync confidence; here from the host restatement's
+    previous field) it goes on.  Every plan equals the host restatement."""
     from ldgpu.fieldread import field_window
     from ldgpu.linelocs import FieldLogic
     from ldgpu.synth import inject_dropouts
@@ -151,32 +154,38 @@ def test_chain_takes_previous_field_inputs(monkeypatch):
     monkeypatch.setattr(FieldLogic, "compute_linelocs", recording)
     reads, _ = host_field_chain(rf, arrays, nb)
     runs = host_sync_runs(rf, arrays["demod_05"])
-    st, plans, resolved, ranged = None, [], 0, 0
-    while True:
-        got, stop, st = run_chain(rf, runs, nb, st)
-        plans.extend(got)
-        if stop == L.LDG_CHAIN_STOP_END:
-            break
-        assert stop == L.LDG_CHAIN_STOP_PREV and not st.prev_known
+
+    def with_exact_inputs(st):
         w_prev, prev = [r for r in reads[:len(plans)] if r[1].valid][-1]
         w = field_window(rf, st.start)
-        exact = float(np.asarray(prev.linelocs, np.float64)[prev.linecount] - (w.startloc - w_prev.startloc))
-        # a range of +-32 samples around it and skip_check unknown: the chain
-        # either plans this field exactly as with the exact inputs, or stops
-        st.prev_known, st.prev_skip, st.prev_conf = 1, -1, int(prev.sync_confidence)
-        st.prev_line0, st.prev_line0_hi = exact - 32.0, exact + 32.0
-        one, stop1, st1 = run_chain(rf, runs, nb, st, max_plans=1)
-        st.prev_skip = 1 if prev.skip_check() >= 50 else 0
-        st.prev_line0 = st.prev_line0_hi = exact
-        one_x, _, st_x = run_chain(rf, runs, nb, st, max_plans=1)
+        x = L.ChainState.from_buffer_copy(st)
+        x.prev_known, x.prev_conf = 1, int(prev.sync_confidence)
+        x.prev_skip = 1 if prev.skip_check() >= 50 else 0
+        x.prev_line0 = x.prev_line0_hi = float(np.asarray(prev.linelocs, np.float64)[prev.linecount]
+                                               - (w.startloc - w_prev.startloc))
+        return x
+
+    st, plans, resolved, ranged = None, [], 0, 0
+    while True:
+        got, stop, st_next = run_chain(rf, runs, nb, st, max_plans=1)
+        if len(got):
+            if got[0].prev_range:
+                ranged += 1
+                one_x, _, _ = run_chain(rf, runs, nb, with_exact_inputs(st), max_plans=1)
+                a = got.copy()
+                a.prev_range = 0
+                assert len(one_x) == 1 and a.tobytes() == one_x.tobytes()
+            plans.extend(got)
+            st = st_next
+            continue
+        if stop == L.LDG_CHAIN_STOP_END:
+            break
+        assert stop == L.LDG_CHAIN_STOP_PREV and not st_next.prev_known
+        one_x, _, st = run_chain(rf, runs, nb, with_exact_inputs(st_next), max_plans=1)
         assert len(one_x) == 1
-        if len(one):
-            assert one.tobytes() == one_x.tobytes()
-            ranged += 1
-        else:
-            assert stop1 == L.LDG_CHAIN_STOP_PREV
+        plans.extend(one_x)
         resolved += 1
-    assert resolved >= 1
+    assert resolved + ranged >= 1
     assert len(plans) == len(reads)
     for p, (w, f) in zip(plans, reads):
         assert (p.startloc, p.readloc) == (w.startloc, w.readloc)
@@ -191,4 +200,4 @@ def test_chain_takes_previous_field_inputs(monkeypatch):
         assert bool(p.isfirst) == bool(f.isFirstField)
         assert p.nextfieldoffset == nxt
         assert p.sync_confidence == f.sync_confidence
-    print("resolved", resolved, "of", len(plans), "reads;", ranged, "from the range alone")
+    print(len(plans), "reads;", ranged, "decided from the previous field's estimate,", resolved, "with exact inputs")
