@@ -384,6 +384,31 @@ def run_gpu(args):
     for _ in range(args.warmup):
         assert len(step()) == nf
     torch.cuda.synchronize()
+    # blocks per CTA for the step: the demodulator alone runs a little faster
+    # with more blocks per CTA, but the pipelined step needs SMs released
+    # between CTAs for the line-location and TBC kernels, so the step itself
+    # (back to back on the two buffer sets) is timed under each
+    step_tune = None
+    if tune is not None:
+        step_tune = {}
+        for b in (1, 2, 4):
+            rf.blocks_per_cta = b
+            for k in range(2):
+                step(None, (main, alt)[k], overlap=True)
+            torch.cuda.synchronize()
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record(stream)
+            for k in range(4):
+                step(None, (main, alt)[k % 2], overlap=True)
+            for st_ in (streamB, streamC, streamS, streamA):
+                stream.wait_stream(st_)
+            q1.record(stream)
+            torch.cuda.synchronize()
+            step_tune[b] = q0.elapsed_time(q1) / 4
+        rf.blocks_per_cta = min(step_tune, key=step_tune.get)
+        for k in range(2):
+            step(None, (main, alt)[k], overlap=True)
+        torch.cuda.synchronize()
     loc.stats = {k: 0 for k in loc.stats}
     loc.timing = {}
 
@@ -622,6 +647,8 @@ def run_gpu(args):
                               "so a step's tail overlaps the next step's demod"},
         "autotune": None if tune is None else {
             "best": {"fft": ("stockham", "in_place")[tune["best"][0]], "blocks_per_cta": tune["best"][1]},
+            "step_ms_by_blocks_per_cta": step_tune,
+            "step_blocks_per_cta": rf.blocks_per_cta,
             "ms": {f"{('stockham', 'in_place')[k[0]]}_bpc{k[1]}": v for k, v in tune["ms"].items()},
             "blocks": tune["blocks"],
             "swept": "FFT decomposition (Stockham / in-place Cooley-Tukey 16384-point transforms) x blocks per CTA, "

@@ -18,7 +18,13 @@
 //
 // Stage s works on groups of R points at stride L inside blocks of R*L
 // points: L = 1024, 64, 4 (radix 16) and L = 1 (radix 4, four groups per
-// thread).  The padding pad(i) = i + i/16 of ldg_fft.cuh makes every stage's
+// thread).  Only the L = 1024 stage mixes the whole set.  The threads of an
+// L = 64 stage work on the 1024-point block t / 64 (two warps), those of an
+// L = 4 stage on the 64-point block t / 4 and the radix-4 stage gives each
+// thread four groups of that same 64-point block, so between the stages
+// nearer the radix-4 end a barrier over the four warps of the 1024-point
+// block's pair (L = 64 <-> L = 4) or over the warp (L = 4 <-> radix 4)
+// orders every access; only L = 1024 needs the whole CTA.  The padding pad(i) = i + i/16 of ldg_fft.cuh makes every stage's
 // loads and stores, and the position-order passes over bin pairs, free of
 // bank conflicts.  Twiddles W_(RL)^(j q) come from per-stage shared tables
 // holding W^j, W^2j, W^4j, W^8j (FP64-made, stored FP32); the other eleven
@@ -99,12 +105,27 @@ __device__ __forceinline__ void group_twiddles(float2 (&w)[16], const float2* ta
     w[15] = cmul(w[8], w[7]);
 }
 
+// How far the barrier at the end of a stage reaches.
+enum Sync { kSyncCta = 0, kSyncQuad = 1, kSyncWarp = 2 };
+
+template <int SY>
+__device__ __forceinline__ void stage_sync() {
+    if constexpr (SY == kSyncCta) {
+        __syncthreads();
+    } else if constexpr (SY == kSyncQuad) {
+        // named barriers 1..8: the four warps of threads [128 q, 128 q + 128)
+        asm volatile("bar.sync %0, 128;" ::"r"(1 + (threadIdx.x >> 7)) : "memory");
+    } else {
+        __syncwarp();
+    }
+}
+
 // One radix-16 stage at stride L (1024, 64 or 4).  Forward: load, butterfly,
 // twiddle the outputs, store; inverse: load, twiddle the inputs, butterfly,
 // store.  LD (first forward stage, L = 1024) supplies the natural-order
 // input ld(0, n); ST (last inverse stage, L = 1024) takes the natural-order
-// output st(0, n, v) instead of shared memory.  Ends with a barrier.
-template <int L, bool INV, class LD, class ST>
+// output st(0, n, v) instead of shared memory.  Ends with a barrier of reach SY.
+template <int L, bool INV, int SY, class LD, class ST>
 __device__ __noinline__ void stage16(float2* S, const Twiddles& tw, const LD& ld, const ST& st) {
     static_assert(L == 1024 || L == 64 || L == 4, "stride");
     constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
@@ -154,18 +175,25 @@ __device__ __noinline__ void stage16(float2* S, const Twiddles& tw, const LD& ld
             st(0, j + L * q, v[i]);
         }
     }
-    __syncthreads();
+    stage_sync<SY>();
 }
 
-// The radix-4 stage (L = 1): groups 4g .. 4g+3, g = t + 1024 i, no twiddles.
-// LD (first inverse stage) supplies the position-order input ld.quad(p, v4)
-// for the four points at positions p .. p+3.  Ends with a barrier.
-template <bool INV, class LD>
+// The radix-4 stage (L = 1): groups 4g .. 4g+3, no twiddles.  From shared
+// memory thread t takes g = 16 (t / 4) + 4 (t % 4) + i, i < 4: the four
+// groups of its L = 4 stage's 64-point block that sit at 4 (t % 4) + i (a
+// half warp's accesses then cover all 32 banks once), so a barrier over
+// the warp orders it against that stage.  With a loader (LD, first inverse
+// stage: the position-order input ld.quad(p, v4) for the four points at
+// positions p .. p+3, from global memory) thread t takes g = t + 1024 i, so
+// that a warp reads one contiguous kilobyte per step; that order needs the
+// whole CTA's barrier (SY is then kSyncCta).  Ends with a barrier of reach SY.
+template <bool INV, int SY, class LD>
 __device__ __noinline__ void stage4(float2* S, const LD& ld) {
     constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
+    static_assert(from_smem || SY == kSyncCta, "the loader order spans the CTA");
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const int g = threadIdx.x + kThreads * i;
+        const int g = from_smem ? 16 * (threadIdx.x >> 2) + 4 * (threadIdx.x & 3) + i : threadIdx.x + kThreads * i;
         float2* Sb = S + pad(4 * g);  // pad(4g + r) = pad(4g) + r
         float2 v[4];
         if constexpr (from_smem) {
@@ -178,7 +206,7 @@ __device__ __noinline__ void stage4(float2* S, const LD& ld) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) Sb[bitrev(q, 2)] = v[q];
     }
-    __syncthreads();
+    stage_sync<SY>();
 }
 
 // Forward (exp(-2 pi i nk/M)): natural-order input (through `ld` unless
@@ -187,10 +215,10 @@ __device__ __noinline__ void stage4(float2* S, const LD& ld) {
 template <class LD = SmemIO>
 __device__ __forceinline__ void fft16k_fwd(float2* S, const Twiddles& tw, const LD& ld = LD()) {
     const SmemIO s;
-    stage16<1024, false>(S, tw, ld, s);
-    stage16<64, false>(S, tw, s, s);
-    stage16<4, false>(S, tw, s, s);
-    stage4<false>(S, s);
+    stage16<1024, false, kSyncCta>(S, tw, ld, s);
+    stage16<64, false, kSyncQuad>(S, tw, s, s);
+    stage16<4, false, kSyncWarp>(S, tw, s, s);
+    stage4<false, kSyncCta>(S, s);
 }
 
 // Inverse (exp(+2 pi i nk/M), unnormalised): bin k taken from position
@@ -200,10 +228,10 @@ __device__ __forceinline__ void fft16k_fwd(float2* S, const Twiddles& tw, const 
 template <class LD = SmemIO, class ST = SmemIO>
 __device__ __forceinline__ void fft16k_inv(float2* S, const Twiddles& tw, const LD& ld = LD(), const ST& st = ST()) {
     const SmemIO s;
-    stage4<true>(S, ld);
-    stage16<4, true>(S, tw, s, s);
-    stage16<64, true>(S, tw, s, s);
-    stage16<1024, true>(S, tw, s, st);
+    stage4<true, std::is_same<LD, SmemIO>::value ? kSyncWarp : kSyncCta>(S, ld);
+    stage16<4, true, kSyncQuad>(S, tw, s, s);
+    stage16<64, true, kSyncCta>(S, tw, s, s);
+    stage16<1024, true, kSyncCta>(S, tw, s, st);
 }
 
 }  // namespace ip

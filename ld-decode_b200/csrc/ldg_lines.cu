@@ -21,11 +21,13 @@
 //                        of determine_field_number (3095-3203).
 //   pal_sequence_kernel  PAL, one warp walking the fields in order: the
 //                        8-field sequence (field phase IDs).
-//   burst_chain_kernel   NTSC, one CTA walking the fields in order: the
-//                        burst phase of every line starts from the previous
+//   burst_round_kernel   NTSC, one CTA per field, twice, and
+//   burst_verify_kernel  one CTA walking the fields in order: the burst
+//                        phase of every line starts from the previous
 //                        field's phase_adjust_median (compute_burst_offsets,
 //                        core.py:3360-3388), two passes of the phase
-//                        update, the field's median and its field-1/4 flag.
+//                        update, the field's median and its field-1/4 flag;
+//                        speculated in parallel, verified in order.
 //   burst_apply_kernel   NTSC, one CTA per field: refine_linelocs_burst
 //                        (3390-3440), fix_badlines with linelocs2 as backup,
 //                        the 117.25-degree subcarrier shift (3493-3495).
@@ -803,86 +805,238 @@ __device__ __forceinline__ int run_rank(const double* rk, const int* ri, double 
     return lo + (pair_less(rk[lo], ri[lo], key, idx) ? 1 : 0);
 }
 
-// NTSC burst phase chain: fields in order (each seeds its lines' phase from
-// the previous field's median), lines in parallel.  Per field: two passes of
-// clb_findbursts' phase update per line; the field's median from per-warp
-// sorted runs (a value's rank is the sum of its positions in the runs); its
-// rising count.  The next field's records load while the current one is
-// worked on.
-__global__ void __launch_bounds__(kBurstThreads) burst_chain_kernel(LineParams P) {
-    constexpr int kWarps = kBurstThreads / 32;
-    const ldg_lines_args& a = P.a;
-    __shared__ double rkey[kWarps][32];
-    __shared__ int ridx[kWarps][32];
-    __shared__ double med2[2];
-    const int f0 = a.first_field, f1 = a.first_field + a.count;
-    // a later range continues from the previous field's output
-    double prev_pam = f0 > 0 ? a.phase_adjust[f0 - 1]
-                             : (a.prev_phase_adjust_dev ? *a.prev_phase_adjust_dev : a.prev_phase_adjust);
+// ---- NTSC burst phase of every field (compute_burst_offsets, core.py:3360-3388)
+//
+// Each field's lines start clb_findbursts' phase update from the previous
+// field's phase_adjust_median, so the fields form a chain.  The seed enters
+// only through the first pass's rounding int(cyc + .5) of every slot: for
+// all seeds that leave those roundings as they are, the first pass ends at
+// the same phase (the median of the rounded deviations, which moves with
+// the seed), so the second pass, the line's adjustment, its rising count
+// and the field's median are the same up to the last bits of the FP64
+// arithmetic.  So the chain runs as
+//   round 1  every field of the range at once, seeded with 0 (the range's
+//            first field with its true seed): its median;
+//   round 2  every field at once seeded with round 1's median of the field
+//            before it: adjustments, field-1/4 flag, median, and the
+//            interval of seeds that gives the same roundings (with a
+//            margin of 1e-9 cycles, also around the second pass's
+//            roundings); a field with a valid line without zero crossings
+//            (its adjustment is the seed itself) has none;
+//   verify   one CTA walking the range in order with the true seeds: a
+//            field whose true seed is round 2's seed or lies in its
+//            interval keeps round 2's results, any other is computed again
+//            from its true seed.
+// The integer results (rising counts, field-1/4 flags) are those of the
+// fields in order; the adjustments and medians agree with them to the
+// last bits (kept within 1e-9 of the host restatement by the tests).
+
+constexpr int kBurstWarps = kBurstThreads / 32;
+constexpr double kBurstMargin = 1e-9;
+
+struct BurstSmem {
+    double rkey[kBurstWarps][32];
+    int ridx[kBurstWarps][32];
+    double med2[2];
+    double lo[kBurstWarps], hi[kBurstWarps];
+    double pam, flo, fhi, seed;
+    int xonly, next;
+};
+
+// The cell of x that int(x + .5) (truncation toward zero) maps to rnd:
+// [r - .5, r + .5) for r >= 1, (-1.5, .5) for r = 0, (r - 1.5, r - .5] for r <= -1.
+__device__ __forceinline__ void round_cell(int rnd, double& lo, double& hi) {
+    lo = rnd >= 1 ? rnd - .5 : rnd - 1.5;
+    hi = rnd >= 1 ? rnd + .5 : (rnd == 0 ? .5 : rnd - .5);
+}
+
+// One field's burst phase update from seed `prev` (the previous field's
+// phase_adjust_median; 0 without one), lines in parallel: two passes of
+// clb_findbursts' phase update per line, the field's median from per-warp
+// sorted runs (a value's rank is the sum of its positions in the runs), its
+// rising count.  All kBurstThreads threads call it; `cur` is the calling
+// thread's line record.  Writes the lines' adjustments to adjs_f (NaN: none)
+// and the field-1/4 flag to *field14_f when given; leaves the median times 2
+// in sm.pam and, with `interval`, the seeds giving the same roundings in
+// (sm.flo, sm.fhi) and sm.xonly set when the result depends on the seed
+// otherwise.  Ends with the CTA in step.
+__device__ void burst_field(const BurstRec& cur, double prev, double* adjs_f, int* field14_f, bool interval,
+                            BurstSmem& sm) {
     const int l = threadIdx.x, lane = l & 31, warp = l >> 5;
     const bool line = l < kBurstLines;
+    double adj = INFINITY;
+    bool ok = false, rising = false, xo = false;
+    double plo = -INFINITY, phi = INFINITY;
+    if (line && cur.valid) {
+        double pa = -prev;
+        int rising_count = 0;
+        for (int pass = 0; pass < 2; ++pass) {
+            rising_count = 0;
+            if (cur.count) {
+                double dev[kZc];
+                int odd = 0;
+#pragma unroll
+                for (int k = 0; k < kZc; ++k) {
+                    const double cyc = cur.cyc[k] + pa;
+                    const int rnd = (int)(cyc + .5);
+                    if (rnd % 2 != 0) odd |= 1 << k;
+                    dev[k] = (double)rnd - cyc;
+                    if (interval) {
+                        double clo, chi;
+                        round_cell(rnd, clo, chi);
+                        if (pass == 0) {
+                            // seeds s with cur.cyc[k] - s in the cell
+                            plo = fmax(plo, cur.cyc[k] - chi);
+                            phi = fmin(phi, cur.cyc[k] - clo);
+                        } else if (!(fmin(cyc - clo, chi - cyc) > kBurstMargin)) {
+                            xo = true;
+                        }
+                    }
+                }
+                pa += median16(dev);
+                rising_count = __popc((unsigned)(cur.rising ^ odd) & 0xffffu);
+            } else {
+                xo = true;  // no crossings: the line's adjustment is the seed itself
+            }
+        }
+        rising = (double)rising_count > ((double)cur.count / 2);
+        adj = (-pa) / 2;
+        ok = true;
+    }
+    if (line && adjs_f) adjs_f[l] = ok ? adj : nan("");
+    double sk = adj;
+    int si = l;
+    warp_sort_pairs(sk, si);
+    sm.rkey[warp][lane] = sk;
+    sm.ridx[warp][lane] = si;
+    if (interval) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            plo = fmax(plo, __shfl_xor_sync(0xffffffffu, plo, o));
+            phi = fmin(phi, __shfl_xor_sync(0xffffffffu, phi, o));
+        }
+        if (lane == 0) {
+            sm.lo[warp] = plo;
+            sm.hi[warp] = phi;
+        }
+    }
+    const int cnt = __syncthreads_count(ok);
+    const int rsum = __syncthreads_count(ok && !(l % 2) && rising);
+    const int xany = __syncthreads_or(xo);
+    if (ok) {
+        int r = 0;
+#pragma unroll
+        for (int w = 0; w < kBurstWarps; ++w) r += run_rank(sm.rkey[w], sm.ridx[w], adj, l);
+        if (cnt & 1) {
+            if (r == cnt / 2) sm.med2[0] = sm.med2[1] = adj;
+        } else {
+            if (r == cnt / 2 - 1) sm.med2[0] = adj;
+            if (r == cnt / 2) sm.med2[1] = adj;
+        }
+    }
+    __syncthreads();
+    if (l == 0) {
+        // np.median of an empty list is NaN, which the reference then carries forward
+        const double med = cnt ? (sm.med2[0] + sm.med2[1]) / 2.0 : nan("");
+        sm.pam = med * 2;
+        if (field14_f) *field14_f = rsum > (cnt / 4);
+        if (interval) {
+            double a = -INFINITY, b = INFINITY;
+            for (int w = 0; w < kBurstWarps; ++w) {
+                a = fmax(a, sm.lo[w]);
+                b = fmin(b, sm.hi[w]);
+            }
+            sm.flo = a;
+            sm.fhi = b;
+            sm.xonly = xany || isnan(prev);
+        }
+    }
+    __syncthreads();
+}
+
+// The true seed of the range's first field: the field before it (a later
+// range continues from the previous range's output) or the caller's.
+__device__ __forceinline__ double range_seed(const LineParams& P) {
+    const ldg_lines_args& a = P.a;
+    return a.first_field > 0 ? a.phase_adjust[a.first_field - 1]
+                             : (a.prev_phase_adjust_dev ? *a.prev_phase_adjust_dev : a.prev_phase_adjust);
+}
+
+struct BurstSpec {
+    double* out1;   // round 1's median x 2 per field
+    double* seed2;  // round 2's seed per field
+    double* lo;     // round 2's interval of seeds with the same roundings
+    double* hi;
+    int* xonly;     // round 2's result depends on the seed otherwise
+};
+
+// Rounds 1 and 2: one CTA per field of the range.
+__global__ void __launch_bounds__(kBurstThreads) burst_round_kernel(LineParams P, int round, BurstSpec B) {
+    __shared__ BurstSmem sm;
+    const ldg_lines_args& a = P.a;
+    const int f = a.first_field + blockIdx.x;
+    double seed = 0.0;
+    if (a.has_prev[f]) {
+        if (f == a.first_field) seed = range_seed(P);
+        else if (round == 2) seed = B.out1[f - 1];
+    }
     BurstRec cur;
     cur.valid = 0;
-    if (line && f1 > f0) cur = P.rec[(long long)f0 * kBurstLines + l];
-    for (int f = f0; f < f1; ++f) {
-        BurstRec nxt;
-        nxt.valid = 0;
-        if (line && f + 1 < f1) nxt = P.rec[(long long)(f + 1) * kBurstLines + l];
-        const double prev = a.has_prev[f] ? prev_pam : 0.0;
-        double adj = INFINITY;
-        bool ok = false, rising = false;
-        if (line && cur.valid) {
-            double pa = -prev;
-            int rising_count = 0;
-            for (int pass = 0; pass < 2; ++pass) {
-                rising_count = 0;
-                if (cur.count) {
-                    double dev[kZc];
-                    int odd = 0;
-#pragma unroll
-                    for (int k = 0; k < kZc; ++k) {
-                        const double cyc = cur.cyc[k] + pa;
-                        const int rnd = (int)(cyc + .5);
-                        if (rnd % 2 != 0) odd |= 1 << k;
-                        dev[k] = (double)rnd - cyc;
-                    }
-                    pa += median16(dev);
-                    rising_count = __popc((unsigned)(cur.rising ^ odd) & 0xffffu);
+    if (threadIdx.x < kBurstLines) cur = P.rec[(long long)f * kBurstLines + threadIdx.x];
+    if (round == 1) {
+        burst_field(cur, seed, nullptr, nullptr, false, sm);
+        if (threadIdx.x == 0) B.out1[f] = sm.pam;
+    } else {
+        burst_field(cur, seed, P.adjs + (long long)f * kBurstLines, P.field14 + f, true, sm);
+        if (threadIdx.x == 0) {
+            a.phase_adjust[f] = sm.pam;
+            B.seed2[f] = seed;
+            B.lo[f] = sm.flo;
+            B.hi[f] = sm.fhi;
+            B.xonly[f] = sm.xonly;
+        }
+    }
+}
+
+// The fields of the range in order with their true seeds: thread 0 walks
+// over the fields round 2 already got right; a field it did not is computed
+// again by the whole CTA.
+__global__ void __launch_bounds__(kBurstThreads) burst_verify_kernel(LineParams P, BurstSpec B) {
+    __shared__ BurstSmem sm;
+    const ldg_lines_args& a = P.a;
+    const int f1 = a.first_field + a.count;
+    if (threadIdx.x == 0) sm.seed = range_seed(P);  // the result of the field before
+    int f = a.first_field;
+    while (true) {
+        if (threadIdx.x == 0) {
+            double prev = sm.seed;
+            int g = f;
+            for (; g < f1; ++g) {
+                const double p = a.has_prev[g] ? prev : 0.0;
+                const bool same = __double_as_longlong(p) == __double_as_longlong(B.seed2[g]);
+                const bool inside = !B.xonly[g] && p > B.lo[g] + kBurstMargin && p < B.hi[g] - kBurstMargin;
+                if (!same && !inside) {
+                    prev = p;
+                    break;
                 }
+                prev = a.phase_adjust[g];
             }
-            rising = (double)rising_count > ((double)cur.count / 2);
-            adj = (-pa) / 2;
-            ok = true;
-        }
-        if (line) P.adjs[(long long)f * kBurstLines + l] = ok ? adj : nan("");
-        double sk = adj;
-        int si = l;
-        warp_sort_pairs(sk, si);
-        rkey[warp][lane] = sk;
-        ridx[warp][lane] = si;
-        const int cnt = __syncthreads_count(ok);
-        const int rsum = __syncthreads_count(ok && !(l % 2) && rising);
-        if (ok) {
-            int r = 0;
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) r += run_rank(rkey[w], ridx[w], adj, l);
-            if (cnt & 1) {
-                if (r == cnt / 2) med2[0] = med2[1] = adj;
-            } else {
-                if (r == cnt / 2 - 1) med2[0] = adj;
-                if (r == cnt / 2) med2[1] = adj;
-            }
+            sm.next = g;
+            sm.seed = prev;  // the seed of field g
         }
         __syncthreads();
-        // np.median of an empty list is NaN, which the reference then carries forward
-        const double med = cnt ? (med2[0] + med2[1]) / 2.0 : nan("");
-        prev_pam = med * 2;
-        if (l == 0) {
-            P.field14[f] = rsum > (cnt / 4);
-            a.phase_adjust[f] = prev_pam;
+        const int g = sm.next;
+        if (g >= f1) break;
+        BurstRec cur;
+        cur.valid = 0;
+        if (threadIdx.x < kBurstLines) cur = P.rec[(long long)g * kBurstLines + threadIdx.x];
+        burst_field(cur, sm.seed, P.adjs + (long long)g * kBurstLines, P.field14 + g, false, sm);
+        if (threadIdx.x == 0) {
+            a.phase_adjust[g] = sm.pam;
+            sm.seed = sm.pam;
         }
+        f = g + 1;
         __syncthreads();
-        cur = nxt;
     }
 }
 
@@ -1121,6 +1275,7 @@ int64_t ldg_lines_scratch_bytes(int32_t nfields) {
     return (int64_t)(align256((size_t)nfields * kBurstLines * sizeof(BurstRec)) +
                      align256((size_t)nfields * kMaxL * sizeof(double)) +
                      align256((size_t)nfields * kBurstLines * sizeof(double)) +
+                     align256((size_t)nfields * sizeof(int)) + 4 * align256((size_t)nfields * sizeof(double)) +
                      align256((size_t)nfields * sizeof(int)));
 }
 
@@ -1165,6 +1320,17 @@ extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
     P.adjs = reinterpret_cast<double*>(s);
     s += align256(nf * kBurstLines * sizeof(double));
     P.field14 = reinterpret_cast<int*>(s);
+    s += align256(nf * sizeof(int));
+    BurstSpec B;
+    B.out1 = reinterpret_cast<double*>(s);
+    s += align256(nf * sizeof(double));
+    B.seed2 = reinterpret_cast<double*>(s);
+    s += align256(nf * sizeof(double));
+    B.lo = reinterpret_cast<double*>(s);
+    s += align256(nf * sizeof(double));
+    B.hi = reinterpret_cast<double*>(s);
+    s += align256(nf * sizeof(double));
+    B.xonly = reinterpret_cast<int*>(s);
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(ldg::ctx_device(c));
@@ -1173,7 +1339,11 @@ extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
     if (stages & 1) lines_hsync_kernel<<<P.a.count, kLineThreads, 0, st>>>(P);
     if (P.system == 1 && (stages & 2)) pal_sequence_kernel<<<1, 32, 0, st>>>(P);
     if (P.system == 0) {
-        if (stages & 2) burst_chain_kernel<<<1, kBurstThreads, 0, st>>>(P);
+        if (stages & 2) {
+            burst_round_kernel<<<P.a.count, kBurstThreads, 0, st>>>(P, 1, B);
+            burst_round_kernel<<<P.a.count, kBurstThreads, 0, st>>>(P, 2, B);
+            burst_verify_kernel<<<1, kBurstThreads, 0, st>>>(P, B);
+        }
         const double shift = (117.25 / 360) / P.fsc_mhz * P.freq;
         if (stages & 4) burst_apply_kernel<<<P.a.count, 512, 0, st>>>(P, shift);
     }

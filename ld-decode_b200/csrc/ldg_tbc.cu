@@ -647,11 +647,13 @@ __device__ __forceinline__ double pixel_coord(const TbcField& f, long long ig, i
 
 // One warp per 32 consecutive output pixels of one field; blockIdx.y is the
 // field.  Each lane computes its own pixel's FP64 coordinate; then groups of
-// 8 lanes gather one pixel at a time: lane k of a group reads taps 2k, 2k+1
+// 8 lanes gather one pixel at a time (at step p group g takes pixel 4p + g,
+// so a step's four pixels are adjacent): lane k of a group reads taps 2k, 2k+1
 // of the input and one float4 of the interleaved LUT (the two taps of phase
 // ps and their differences to phase ps + 1), so a pixel's 64-byte input
 // span and its 128 bytes of LUT are each one contiguous access; the 8
-// partial sums meet in a transposing reduction (lane k ends with pixel k).
+// partial sums meet in a transposing reduction (lane k of group g ends with
+// pixel 4k + g) and one shuffle takes each pixel's sum to its own lane.
 __global__ void __launch_bounds__(kGatherThreads, 8) tbc_gather_kernel(const TbcField* fields, const float* lut,
                                                                     int nfields) {
     const int fi = blockIdx.y;
@@ -686,7 +688,10 @@ __global__ void __launch_bounds__(kGatherThreads, 8) tbc_gather_kernel(const Tbc
     double acc[8];  // this lane's two-tap share of each of the group's 8 pixels
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
-        const int src = grp * 8 + p;  // the group's p-th pixel
+        // the group's p-th pixel: at each step the four groups take four
+        // adjacent pixels, whose 16-tap windows overlap (fewer cache lines
+        // per tap load)
+        const int src = 4 * p + grp;
         const int pst = __shfl_sync(0xffffffffu, sti, src);
         const int pps = __shfl_sync(0xffffffffu, psi, src);
         const float pal = __shfl_sync(0xffffffffu, alpha, src);
@@ -702,7 +707,7 @@ __global__ void __launch_bounds__(kGatherThreads, 8) tbc_gather_kernel(const Tbc
     }
     // transposing reduction over the group's 8 lanes: at each step a lane
     // keeps half of its pixels and adds the partner's shares of them, so lane
-    // k ends with the whole sum for pixel k (its own)
+    // k ends with the whole sum of the group's k-th pixel
     double b4[4], b2[2];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -715,7 +720,10 @@ __global__ void __launch_bounds__(kGatherThreads, 8) tbc_gather_kernel(const Tbc
         b2[j] = (hi ? b4[j + 2] : b4[j]) + __shfl_xor_sync(0xffffffffu, hi ? b4[j] : b4[j + 2], 2);
     }
     const bool hi1 = (k & 1) != 0;
-    const double mine = (hi1 ? b2[1] : b2[0]) + __shfl_xor_sync(0xffffffffu, hi1 ? b2[0] : b2[1], 1);
+    // lane k of group g now holds the sum of pixel 4 k + g; pixel `lane` is
+    // at lane 8 (lane % 4) + lane / 4
+    const double held = (hi1 ? b2[1] : b2[0]) + __shfl_xor_sync(0xffffffffu, hi1 ? b2[0] : b2[1], 1);
+    const double mine = __shfl_sync(0xffffffffu, held, 8 * (lane & 3) + (lane >> 2));
     double level;
     if (f.spline_k >= 2) {
         const double med = f.stat[0];

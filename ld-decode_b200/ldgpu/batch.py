@@ -150,7 +150,7 @@ def autotune_demod(rf, in_ptr, nblocks, in_stride, outs, mtf_level=1, stream=Non
     for v in variants:
         rf.fft_variant = v
         for b in blocks_per_cta:
-            L.check(rf._ctx._lib.ldg_set_demod_schedule(rf._ctx.handle, int(b)))
+            rf.blocks_per_cta = b
             rf.demod_blocks_device(in_ptr, nblocks, in_stride, outs, mtf_level=mtf_level, stream=sh)
             best = None
             for _ in range(reps):
@@ -165,7 +165,7 @@ def autotune_demod(rf, in_ptr, nblocks, in_stride, outs, mtf_level=1, stream=Non
             times[(v, b)] = best
     choice = min(times, key=times.get)
     rf.fft_variant = choice[0]
-    L.check(rf._ctx._lib.ldg_set_demod_schedule(rf._ctx.handle, int(choice[1])))
+    rf.blocks_per_cta = choice[1]
     if keep:
         _DEMOD_TUNED[(rf.device, rf.system)] = choice
     return {"best": choice, "ms": times, "blocks": nblocks}
@@ -177,7 +177,7 @@ def tuned_demod(rf):
     choice = _DEMOD_TUNED.get((rf.device, rf.system))
     if choice is not None:
         rf.fft_variant = choice[0]
-        L.check(rf._ctx._lib.ldg_set_demod_schedule(rf._ctx.handle, int(choice[1])))
+        rf.blocks_per_cta = choice[1]
     return choice
 
 

@@ -175,6 +175,17 @@ class RFDecode(RFParams):
     def fft_variant(self, v):
         L.check(self._ctx._lib.ldg_set_demod_variant(self._ctx.handle, int(v)))
 
+    @property
+    def blocks_per_cta(self):
+        """Consecutive blocks a demodulator CTA takes (ldg_set_demod_schedule;
+        0: the library's choice, 2 for large batches, else 1)."""
+        return getattr(self, "_blocks_per_cta", 0)
+
+    @blocks_per_cta.setter
+    def blocks_per_cta(self, n):
+        L.check(self._ctx._lib.ldg_set_demod_schedule(self._ctx.handle, int(n)))
+        self._blocks_per_cta = int(n)
+
     # ---- filter upload (float32 half spectra)
 
     def computefilters(self):
