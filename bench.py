@@ -270,12 +270,32 @@ def run_gpu(args):
 
     streamJ = torch.cuda.Stream()              # joins a step's streams for its end event (overlapped steps)
 
-    def step(io=None, bs=None, overlap=False):
+    def copy_in(io, bs):
+        """Every chunk's host -> device input copy of a step on buffer set
+        bs (stream H, once the set's previous demod has read its input);
+        returns the per-chunk events."""
+        if getattr(bs, "demod_done", None) is not None:
+            streamH.wait_event(bs.demod_done)
+        hevs = []
+        for c in range(nchunks):
+            # chunk c's blocks read [b0*U, b1*U + N - U); the previous chunk already copied up to b0*U + N - U
+            a0 = bounds[c] * U + (N - U if c else 0)
+            a1 = min(bounds[c + 1] * U + (N - U), nsamples)
+            with torch.cuda.stream(streamH):
+                bs.cap[a0:a1].copy_(io["cap"][a0:a1], non_blocking=True)
+                hev = torch.cuda.Event()
+                hev.record(streamH)
+            hevs.append(hev)
+        return hevs
+
+    def step(io=None, bs=None, overlap=False, next_in=None):
         """One pass over the capture with buffer set `bs` (default: the
         main set).  io: pinned host buffers; then each chunk's input is
-        copied in just before its demod (streamH) and each chunk's EFM/audio
+        copied in before its demod (stream H) and each chunk's EFM/audio
         and each field range's pictures are copied out as soon as they are
-        final (streamD)."""
+        final (streams D, P).  next_in = (io, set) of the next step: its
+        input copies are issued as soon as this step's demods are, so the
+        next step's first chunk does not wait for the host to reach it."""
         bs = bs or main
         loc = bs.loc
         overlap = overlap or io is not None
@@ -286,20 +306,16 @@ def run_gpu(args):
             # demodulator has read it
             for e in bs.done:
                 stream.wait_event(e)
-            streamH.wait_event(bs.demod_done)
             bs.done = None
+        hevs = None
+        if io is not None:
+            hevs = bs.prefetched if getattr(bs, "prefetched", None) else copy_in(io, bs)
+            bs.prefetched = None
         loc.begin(bs.farr)
         evs = []
         for c in range(nchunks):
-            if io is not None:
-                # chunk c's blocks read [b0*U, b1*U + N - U); the previous chunk already copied up to b0*U + N - U
-                a0 = bounds[c] * U + (N - U if c else 0)
-                a1 = min(bounds[c + 1] * U + (N - U), nsamples)
-                with torch.cuda.stream(streamH):
-                    bs.cap[a0:a1].copy_(io["cap"][a0:a1], non_blocking=True)
-                    hev = torch.cuda.Event()
-                    hev.record(streamH)
-                stream.wait_event(hev)
+            if hevs is not None:
+                stream.wait_event(hevs[c])
             demod_range(bounds[c], bounds[c + 1], bs)
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(stream)
@@ -310,6 +326,10 @@ def run_gpu(args):
                 q0, q1 = bounds[c] * 991, bounds[c + 1] * 991
                 with torch.cuda.stream(streamD):
                     io["efm"][o0:o1].copy_(bs.outs["efm"][o0:o1], non_blocking=True)
+        marks["demod_end"] = evs[-1]
+        bs.demod_done = evs[-1]
+        if next_in is not None:
+            next_in[1].prefetched = copy_in(*next_in)
         for c in range(nchunks):
             streamB.wait_event(evs[c])
             streamS.wait_event(evs[c])
@@ -343,8 +363,6 @@ def run_gpu(args):
                         io["pics"][lo * fsz:hi * fsz].copy_(bs.pics[lo * fsz:hi * fsz], non_blocking=True)
                         if do_audio:
                             io["aud"][lo * AS:hi * AS].copy_(bs.aud[lo * AS:hi * AS], non_blocking=True)
-        marks["demod_end"] = evs[-1]
-        bs.demod_done = evs[-1]
         end = torch.cuda.Event(enable_timing=True)
         if overlap:
             # the next step (on the other buffer set) starts its demod while
@@ -484,7 +502,10 @@ def run_gpu(args):
         barrier()
         e0.record(stream)
         for k in range(args.steps):
-            step(ios[k % 2], sets[k % 2])
+            # each step's input copy is issued during the step before it
+            # (the first step's inside the timed region too)
+            nxt = (ios[(k + 1) % 2], sets[(k + 1) % 2]) if k + 1 < args.steps else None
+            step(ios[k % 2], sets[k % 2], next_in=nxt)
         stream.wait_stream(streamD)
         stream.wait_stream(streamP)
         e1.record(stream)

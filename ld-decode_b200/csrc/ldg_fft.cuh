@@ -197,10 +197,20 @@ __device__ __noinline__ void stockham_pass(float2* S, const Tables& t, const LD&
     constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
     constexpr bool to_smem = std::is_same<ST, SmemIO>::value;
     float2 v[PER][R];
+    if constexpr (BT < kThreads) {
+        // a pass with fewer butterflies than threads (the 1024-point audio
+        // sets): the idle threads only keep the barrier count; this also
+        // keeps the working threads' code within the register budget
+        if (threadIdx.x >= BT) {
+            if constexpr (from_smem && to_smem) __syncthreads();
+            __syncthreads();
+            return;
+        }
+    }
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
         const int jt = threadIdx.x + q * kThreads;
-        if (jt < BT) {
+        if (BT >= kThreads || jt < BT) {
             const int b = jt / B, j = jt - b * B;
             // pad(j + r B) = pad(j) + r padded(B) because B is a multiple of 16:
             // one base register, compile-time offsets

@@ -998,44 +998,61 @@ __global__ void __launch_bounds__(kBurstThreads) burst_round_kernel(LineParams P
     }
 }
 
-// The fields of the range in order with their true seeds: thread 0 walks
-// over the fields round 2 already got right; a field it did not is computed
-// again by the whole CTA.
+// The fields of the range in order with their true seeds: the CTA stages
+// round 2's seeds, intervals, flags and medians of up to kBurstScan fields
+// in shared memory, thread 0 walks over the fields round 2 already got
+// right; a field it did not is computed again by the whole CTA.
+constexpr int kBurstScan = 512;
+
 __global__ void __launch_bounds__(kBurstThreads) burst_verify_kernel(LineParams P, BurstSpec B) {
     __shared__ BurstSmem sm;
+    __shared__ double s_seed2[kBurstScan], s_lo[kBurstScan], s_hi[kBurstScan], s_pam[kBurstScan];
+    __shared__ unsigned char s_flags[kBurstScan];  // bit 0: has a previous field; bit 1: no interval
     const ldg_lines_args& a = P.a;
     const int f1 = a.first_field + a.count;
-    if (threadIdx.x == 0) sm.seed = range_seed(P);  // the result of the field before
+    if (threadIdx.x == 0) sm.seed = range_seed(P);  // the result of the field before the range
     int f = a.first_field;
-    while (true) {
+    while (f < f1) {
+        const int n = min(kBurstScan, f1 - f);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            s_seed2[i] = B.seed2[f + i];
+            s_lo[i] = B.lo[f + i];
+            s_hi[i] = B.hi[f + i];
+            s_pam[i] = a.phase_adjust[f + i];
+            s_flags[i] = (unsigned char)((a.has_prev[f + i] ? 1 : 0) | (B.xonly[f + i] ? 2 : 0));
+        }
+        __syncthreads();
         if (threadIdx.x == 0) {
-            double prev = sm.seed;
-            int g = f;
-            for (; g < f1; ++g) {
-                const double p = a.has_prev[g] ? prev : 0.0;
-                const bool same = __double_as_longlong(p) == __double_as_longlong(B.seed2[g]);
-                const bool inside = !B.xonly[g] && p > B.lo[g] + kBurstMargin && p < B.hi[g] - kBurstMargin;
+            double prev = sm.seed;  // the result of field f - 1
+            int g = 0;
+            for (; g < n; ++g) {
+                const double p = (s_flags[g] & 1) ? prev : 0.0;
+                const bool same = __double_as_longlong(p) == __double_as_longlong(s_seed2[g]);
+                const bool inside = !(s_flags[g] & 2) && p > s_lo[g] + kBurstMargin && p < s_hi[g] - kBurstMargin;
                 if (!same && !inside) {
-                    prev = p;
+                    prev = p;  // field g's seed
                     break;
                 }
-                prev = a.phase_adjust[g];
+                prev = s_pam[g];
             }
-            sm.next = g;
-            sm.seed = prev;  // the seed of field g
+            sm.next = f + g;
+            sm.seed = prev;
         }
         __syncthreads();
         const int g = sm.next;
-        if (g >= f1) break;
-        BurstRec cur;
-        cur.valid = 0;
-        if (threadIdx.x < kBurstLines) cur = P.rec[(long long)g * kBurstLines + threadIdx.x];
-        burst_field(cur, sm.seed, P.adjs + (long long)g * kBurstLines, P.field14 + g, false, sm);
-        if (threadIdx.x == 0) {
-            a.phase_adjust[g] = sm.pam;
-            sm.seed = sm.pam;
+        if (g < f + n) {
+            BurstRec cur;
+            cur.valid = 0;
+            if (threadIdx.x < kBurstLines) cur = P.rec[(long long)g * kBurstLines + threadIdx.x];
+            burst_field(cur, sm.seed, P.adjs + (long long)g * kBurstLines, P.field14 + g, false, sm);
+            if (threadIdx.x == 0) {
+                a.phase_adjust[g] = sm.pam;
+                sm.seed = sm.pam;
+            }
+            f = g + 1;
+        } else {
+            f = g;
         }
-        f = g + 1;
         __syncthreads();
     }
 }
