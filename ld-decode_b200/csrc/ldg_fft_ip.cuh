@@ -154,15 +154,20 @@ __device__ __noinline__ void stage16(float2* S, const Twiddles& tw, const LD& ld
             v[r] = ld(0, j + L * r);
         }
     }
-    float2 w[16];
+    // the twiddles are formed next to their use (forward: after the
+    // butterfly), so they are not live across it
     const float2* tab = L == 1024 ? tw.t1 : L == 64 ? tw.t2 : tw.t3;
-    group_twiddles<INV>(w, tab, L == 1024 ? 1024 : L == 64 ? 64 : 4, j);
+    constexpr int stride = L == 1024 ? 1024 : L == 64 ? 64 : 4;
     if (INV) {
+        float2 w[16];
+        group_twiddles<INV>(w, tab, stride, j);
 #pragma unroll
         for (int r = 1; r < 16; ++r) v[r] = cmul(v[r], w[r]);
     }
     dft_dif<16, INV>(v);  // v[i] = Y[bitrev(i)]
     if (!INV) {
+        float2 w[16];
+        group_twiddles<INV>(w, tab, stride, j);
 #pragma unroll
         for (int i = 1; i < 16; ++i) v[i] = cmul(v[i], w[bitrev(i, 4)]);
     }

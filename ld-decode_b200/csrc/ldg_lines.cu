@@ -817,16 +817,19 @@ __device__ __forceinline__ int run_rank(const double* rk, const int* ri, double 
 // arithmetic.  So the chain runs as
 //   round 1  every field of the range at once, seeded with 0 (the range's
 //            first field with its true seed): its median;
-//   round 2  every field at once seeded with round 1's median of the field
-//            before it: adjustments, field-1/4 flag, median, and the
+//   rounds 2 .. kBurstRounds  every field at once seeded with the round
+//            before's median of the field before it (each round carries the
+//            true seeds at least one field further, and a seed a few
+//            thousandths of a cycle off already decides most fields); the
+//            last round keeps adjustments, field-1/4 flag, median, and the
 //            interval of seeds that gives the same roundings (with a
 //            margin of 1e-9 cycles, also around the second pass's
 //            roundings); a field with a valid line without zero crossings
 //            (its adjustment is the seed itself) has none;
 //   verify   one CTA walking the range in order with the true seeds: a
-//            field whose true seed is round 2's seed or lies in its
-//            interval keeps round 2's results, any other is computed again
-//            from its true seed.
+//            field whose true seed is the last round's seed or lies in its
+//            interval keeps that round's results, any other is computed
+//            again from its true seed.
 // The integer results (rising counts, field-1/4 flags) are those of the
 // fields in order; the adjustments and medians agree with them to the
 // last bits (kept within 1e-9 of the host restatement by the tests).
@@ -962,15 +965,19 @@ __device__ __forceinline__ double range_seed(const LineParams& P) {
                              : (a.prev_phase_adjust_dev ? *a.prev_phase_adjust_dev : a.prev_phase_adjust);
 }
 
+constexpr int kBurstRounds = 4;  // rounds before the verification walk
+
 struct BurstSpec {
-    double* out1;   // round 1's median x 2 per field
-    double* seed2;  // round 2's seed per field
-    double* lo;     // round 2's interval of seeds with the same roundings
+    double* out1;   // the medians x 2 per field of the odd rounds
+    double* out2;   // ... of the even rounds
+    double* seed2;  // the last round's seed per field
+    double* lo;     // the last round's interval of seeds with the same roundings
     double* hi;
-    int* xonly;     // round 2's result depends on the seed otherwise
+    int* xonly;     // the last round's result depends on the seed otherwise
 };
 
-// Rounds 1 and 2: one CTA per field of the range.
+// Round `round` (1 .. kBurstRounds): one CTA per field of the range, seeded
+// with 0 (round 1) or with the previous round's median of the field before.
 __global__ void __launch_bounds__(kBurstThreads) burst_round_kernel(LineParams P, int round, BurstSpec B) {
     __shared__ BurstSmem sm;
     const ldg_lines_args& a = P.a;
@@ -978,14 +985,14 @@ __global__ void __launch_bounds__(kBurstThreads) burst_round_kernel(LineParams P
     double seed = 0.0;
     if (a.has_prev[f]) {
         if (f == a.first_field) seed = range_seed(P);
-        else if (round == 2) seed = B.out1[f - 1];
+        else if (round > 1) seed = (round & 1 ? B.out2 : B.out1)[f - 1];
     }
     BurstRec cur;
     cur.valid = 0;
     if (threadIdx.x < kBurstLines) cur = P.rec[(long long)f * kBurstLines + threadIdx.x];
-    if (round == 1) {
+    if (round < kBurstRounds) {
         burst_field(cur, seed, nullptr, nullptr, false, sm);
-        if (threadIdx.x == 0) B.out1[f] = sm.pam;
+        if (threadIdx.x == 0) (round & 1 ? B.out1 : B.out2)[f] = sm.pam;
     } else {
         burst_field(cur, seed, P.adjs + (long long)f * kBurstLines, P.field14 + f, true, sm);
         if (threadIdx.x == 0) {
@@ -999,8 +1006,8 @@ __global__ void __launch_bounds__(kBurstThreads) burst_round_kernel(LineParams P
 }
 
 // The fields of the range in order with their true seeds: the CTA stages
-// round 2's seeds, intervals, flags and medians of up to kBurstScan fields
-// in shared memory, thread 0 walks over the fields round 2 already got
+// the last round's seeds, intervals, flags and medians of up to kBurstScan
+// fields in shared memory, thread 0 walks over the fields that round got
 // right; a field it did not is computed again by the whole CTA.
 constexpr int kBurstScan = 512;
 
@@ -1292,7 +1299,7 @@ int64_t ldg_lines_scratch_bytes(int32_t nfields) {
     return (int64_t)(align256((size_t)nfields * kBurstLines * sizeof(BurstRec)) +
                      align256((size_t)nfields * kMaxL * sizeof(double)) +
                      align256((size_t)nfields * kBurstLines * sizeof(double)) +
-                     align256((size_t)nfields * sizeof(int)) + 4 * align256((size_t)nfields * sizeof(double)) +
+                     align256((size_t)nfields * sizeof(int)) + 5 * align256((size_t)nfields * sizeof(double)) +
                      align256((size_t)nfields * sizeof(int)));
 }
 
@@ -1341,6 +1348,8 @@ extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
     BurstSpec B;
     B.out1 = reinterpret_cast<double*>(s);
     s += align256(nf * sizeof(double));
+    B.out2 = reinterpret_cast<double*>(s);
+    s += align256(nf * sizeof(double));
     B.seed2 = reinterpret_cast<double*>(s);
     s += align256(nf * sizeof(double));
     B.lo = reinterpret_cast<double*>(s);
@@ -1357,8 +1366,8 @@ extern "C" int ldg_lines_refine(ldg_ctx* c, const ldg_lines_args* a) {
     if (P.system == 1 && (stages & 2)) pal_sequence_kernel<<<1, 32, 0, st>>>(P);
     if (P.system == 0) {
         if (stages & 2) {
-            burst_round_kernel<<<P.a.count, kBurstThreads, 0, st>>>(P, 1, B);
-            burst_round_kernel<<<P.a.count, kBurstThreads, 0, st>>>(P, 2, B);
+            for (int r = 1; r <= kBurstRounds; ++r)
+                burst_round_kernel<<<P.a.count, kBurstThreads, 0, st>>>(P, r, B);
             burst_verify_kernel<<<1, kBurstThreads, 0, st>>>(P, B);
         }
         const double shift = (117.25 / 360) / P.fsc_mhz * P.freq;

@@ -609,6 +609,7 @@ class LineLocator:
         pam = torch.zeros((nf, 4) if self.pal else nf, dtype=torch.float64, device=dev)
         fph = torch.zeros(nf, dtype=torch.int32, device=dev)
         scratch = torch.empty(max(int(lib.ldg_lines_scratch_bytes(nf)), 256), dtype=torch.uint8, device=dev)
+        self._last_scratch = (scratch, nf)  # the last batch's work arrays (inspection)
         a = L.LinesArgs()
         a.k = lines_consts(self.rf)
         a.d05 = arrays["demod_05"]

@@ -3,8 +3,8 @@ uses them) on the GPU: Field.process() runs the GPU line path on each
 field's read and Field.downscale() the GPU TBC and analog audio.  Over the
 seeded captures of tests/golden/fields_<case>.npz, field after field with
 the reference's read offsets, the results equal the batched LineLocator's
-(the same kernels over the capture-wide arrays) and the reference's
-integers."""
+(the same kernels over the capture-wide arrays; line locations to 1e-9
+samples) and the reference's integers."""
 
 import sys
 
@@ -69,7 +69,10 @@ def test_dropin_fields_equal_batched_and_reference(cuda_ok, name):
             flags = [int(f.isFirstField), f.linecount, f.lineoffset, f.fieldPhaseID]
             np.testing.assert_array_equal(flags, g[p + "flags"][:4], err_msg=f"{name} field {i}")
             assert flags == [int(fl.isFirstField), fl.linecount, fl.lineoffset, fl.fieldPhaseID]
-            np.testing.assert_array_equal(np.asarray(f.linelocs), fl.host_linelocs())
+            # the batched path takes NTSC burst phases from parallel rounds
+            # seeded with values equal to the field-by-field ones to the
+            # last bits, so its line locations agree to ~1e-11 samples
+            np.testing.assert_allclose(np.asarray(f.linelocs), fl.host_linelocs(), rtol=0, atol=1e-9)
             np.testing.assert_array_equal(np.asarray(f.linebad, dtype=bool), fl.linebad)
             assert f.sync_confidence == fl.sync_confidence
             lfw = None if i == 0 else (i, prev_startloc)
