@@ -4,9 +4,10 @@
 // whole capture-wide output array -- the pulses findpulses
 // (lddecode/utils.py:1101-1157) finds, for every field read window at once --
 // and the mean level inside the long ones (getpulses' VSYNC level check,
-// core.py:2242-2322).  Three passes over the array: edges counted per tile,
-// an exclusive scan of the tile counts, edges written in order; then one
-// warp per run pairs its edges and averages its interior.
+// core.py:2242-2322).  Edges counted per tile (which also leaves a bitmap of
+// the below-threshold flags), an exclusive scan of the tile counts, edges
+// written in order from the bitmap; then one warp per run pairs its edges
+// and averages its interior.
 //
 // ldg_lines_refine: the per-line refinement of Field.process() for all
 // fields of a capture (pulse-level line locations from the host chain):
@@ -99,15 +100,30 @@ __device__ __forceinline__ unsigned edge_bits(unsigned b, long long base, long l
 
 constexpr int kEdgeSteps = kEdgeTile / (4 * kEdgeThreads);
 
+// Edges per tile, and the below-threshold flags of every sample as a bitmap
+// (bit i % 32 of word i / 32), so the write pass reads 1 bit per sample
+// instead of the float array again.
 __global__ void __launch_bounds__(kEdgeThreads) edge_count_kernel(const float* __restrict__ x, long long n,
-                                                                   double thr, int* __restrict__ counts) {
+                                                                   double thr, int* __restrict__ counts,
+                                                                   unsigned* __restrict__ bm) {
     const long long t0 = (long long)blockIdx.x * kEdgeTile;
     const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+    const int lane = threadIdx.x & 31;
     int c = 0;
 #pragma unroll 2
     for (int j = 0; j < kEdgeSteps; ++j) {
         const long long base = t0 + (long long)j * 4 * kEdgeThreads + 4 * threadIdx.x;
-        if (base < n) c += __popc(edge_bits(four_flags(x, n, base, thr, aligned), base, n));
+        unsigned b = 0;
+        if (base < n) {
+            b = four_flags(x, n, base, thr, aligned);
+            c += __popc(edge_bits(b, base, n));
+        }
+        // eight lanes' four flags make one word (base % 32 == 4 * (lane % 8))
+        unsigned v = ((b >> 1) & 0xfu) << (4 * (lane & 7));
+        v |= __shfl_xor_sync(0xffffffffu, v, 1);
+        v |= __shfl_xor_sync(0xffffffffu, v, 2);
+        v |= __shfl_xor_sync(0xffffffffu, v, 4);
+        if ((lane & 7) == 0) bm[base >> 5] = v;
     }
     __shared__ int warp_sum[kEdgeThreads / 32];
     int v = c;
@@ -149,19 +165,22 @@ __global__ void __launch_bounds__(1024) edge_scan_kernel(const int* __restrict__
 }
 
 // edges as 2*i + (run start ? 1 : 0), in increasing i
-__global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const float* __restrict__ x, long long n,
-                                                                   double thr, const long long* __restrict__ offsets,
+__global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const unsigned* __restrict__ bm, long long n,
+                                                                   const long long* __restrict__ offsets,
                                                                    long long* __restrict__ edges, long long cap) {
     __shared__ int warp_cnt[kEdgeThreads / 32];
     const long long t0 = (long long)blockIdx.x * kEdgeTile;
-    const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
     long long out = offsets[blockIdx.x];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int j = 0; j < kEdgeSteps; ++j) {
         const long long base = t0 + (long long)j * 4 * kEdgeThreads + 4 * threadIdx.x;
         unsigned b = 0, e = 0;
         if (base < n) {
-            b = four_flags(x, n, base, thr, aligned);
+            // the flags of samples base-1 .. base+3 from the count pass's bitmap
+            const unsigned w = bm[base >> 5];
+            const int sh = (int)(base & 31);
+            const unsigned prevb = sh ? (w >> (sh - 1)) & 1u : (base > 0 ? bm[(base >> 5) - 1] >> 31 : 0u);
+            b = prevb | (((w >> sh) & 0xfu) << 1);
             e = edge_bits(b, base, n);
         }
         const int cnt = __popc(e);
@@ -1232,7 +1251,8 @@ int ldg_sync_runs(ldg_ctx* c, const float* d05, int64_t n, double threshold, int
     const size_t b_counts = align256(ntiles * sizeof(int)), b_off = align256(ntiles * sizeof(long long));
     const size_t b_tot = 256, b_edges = align256(ecap * sizeof(long long));
     const size_t b_runs = align256(cap * sizeof(long long));
-    const size_t need = b_counts + b_off + b_tot + b_edges + 2 * b_runs + align256(cap * sizeof(double));
+    const size_t b_bm = align256((size_t)ntiles * (kEdgeTile / 32) * sizeof(unsigned));
+    const size_t need = b_counts + b_off + b_tot + b_edges + 2 * b_runs + align256(cap * sizeof(double)) + b_bm;
     void* scratch = nullptr;
     auto done = [&](int rc) {
         if (prev >= 0) cudaSetDevice(prev);
@@ -1247,14 +1267,16 @@ int ldg_sync_runs(ldg_ctx* c, const float* d05, int64_t n, double threshold, int
     long long* rs = reinterpret_cast<long long*>(p + b_counts + b_off + b_tot + b_edges);
     long long* rl = rs + b_runs / sizeof(long long);
     double* rm = reinterpret_cast<double*>(rl + b_runs / sizeof(long long));
+    unsigned* bm = reinterpret_cast<unsigned*>(p + b_counts + b_off + b_tot + b_edges + 2 * b_runs +
+                                               align256(cap * sizeof(double)));
     auto cuda_fail = [&](const char* what) {
         return done(ldg::lines_fail(LDG_ERR_CUDA, std::string("ldg_sync_runs: ") + what + ": " +
                                                       cudaGetErrorString(cudaGetLastError())));
     };
     // count, scan, write and pair back to back; the host learns the count once
-    edge_count_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, counts);
+    edge_count_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, counts, bm);
     edge_scan_kernel<<<1, 1024, 0, st>>>(counts, ntiles, offsets, total);
-    edge_write_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, offsets, edges, ecap);
+    edge_write_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(bm, n, offsets, edges, ecap);
     run_pair_kernel<<<4 * 148, 256, 0, st>>>(edges, total, cap, d05, min_long, trim_lo, trim_hi, rs, rl, rm);
     // pinned (mapped) outputs: the runs and the count are written by a kernel
     // and the host waits for the stream only (no copy-engine transfer, which
