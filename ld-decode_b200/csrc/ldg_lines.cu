@@ -355,8 +355,10 @@ __device__ void warp_minmax(const float* x, long long lo, long long hi, long lon
     }
 }
 
-// np.median of a float32 slice of up to 64 samples by rank (ties by
-// position); longer slices fall back to one lane
+// np.median of a float32 slice of up to 64 samples: the warp sorts them
+// (bitonic network over elements e = lane and e = lane + 32, unused ones
+// +inf) and reads the middle one or two; longer slices fall back to one
+// lane.  The middle values do not depend on how ties are ordered.
 __device__ double warp_median_f32(const float* x, long long lo, long long hi, long long n) {
     const int lane = threadIdx.x & 31;
     lo = max(lo, 0LL);
@@ -368,23 +370,33 @@ __device__ double warp_median_f32(const float* x, long long lo, long long hi, lo
         if (lane == 0) r = median_f32(x, lo, hi, n);
         return __shfl_sync(0xffffffffu, r, 0);
     }
-    const float v0 = lane < m ? x[lo + lane] : 0.0f;
-    const float v1 = lane + 32 < m ? x[lo + 32 + lane] : 0.0f;
-    int r0 = 0, r1 = 0;
-    for (int j = 0; j < m; ++j) {
-        const float vj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-        r0 += (vj < v0) || (vj == v0 && j < lane);
-        r1 += (vj < v1) || (vj == v1 && j < lane + 32);
+    float v0 = lane < m ? x[lo + lane] : INFINITY;
+    float v1 = lane + 32 < m ? x[lo + 32 + lane] : INFINITY;
+#pragma unroll
+    for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j == 32) {
+                // partners lane and lane + 32 in the same lane; ascending (k = 64)
+                const float a = fminf(v0, v1), b = fmaxf(v0, v1);
+                v0 = a;
+                v1 = b;
+            } else {
+                const float p0 = __shfl_xor_sync(0xffffffffu, v0, j);
+                const float p1 = __shfl_xor_sync(0xffffffffu, v1, j);
+                const bool lower = (lane & j) == 0;  // this element is the pair's first
+                const bool up0 = (lane & k) == 0, up1 = ((lane + 32) & k) == 0;
+                v0 = (lower == up0) ? fminf(v0, p0) : fmaxf(v0, p0);
+                v1 = (lower == up1) ? fminf(v1, p1) : fmaxf(v1, p1);
+            }
+        }
     }
-    const int ka = (m - 1) / 2, kb = m / 2;
-    auto pick = [&](int k) {
-        const unsigned m0 = __ballot_sync(0xffffffffu, lane < m && r0 == k);
-        const unsigned m1 = __ballot_sync(0xffffffffu, lane + 32 < m && r1 == k);
-        const float a = __shfl_sync(0xffffffffu, v0, m0 ? __ffs(m0) - 1 : 0);
-        const float b = __shfl_sync(0xffffffffu, v1, m1 ? __ffs(m1) - 1 : 0);
-        return m0 ? a : b;
+    auto at = [&](int e) {
+        const float a = __shfl_sync(0xffffffffu, v0, e & 31);
+        const float b = __shfl_sync(0xffffffffu, v1, e & 31);
+        return e < 32 ? a : b;
     };
-    const float va = pick(ka), vb = pick(kb);
+    const float va = at((m - 1) / 2), vb = at(m / 2);
     if (m & 1) return (double)va;
     return (double)((va + vb) * 0.5f);
 }
