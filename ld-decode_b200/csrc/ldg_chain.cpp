@@ -861,6 +861,9 @@ extern "C" int64_t ldg_abi_sizeof(const char* name) {
 
 // ---- the chain in pieces on host threads
 
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <thread>
 
 namespace {
@@ -887,6 +890,68 @@ struct Piece {
     LdgChainState in{}, out{};
     int32_t stop = 0;
     int rc = 0;
+};
+
+// Host threads kept for the chain's pieces: a call hands its pieces to the
+// pool instead of starting and joining threads of its own (tens of
+// microseconds each, several calls per capture chunk).  Any number of
+// callers may share it; each waits for its own pieces only.  The pool is
+// never torn down (its idle threads block on a condition variable).
+class PiecePool {
+  public:
+    static PiecePool& get() {
+        static PiecePool* pool = new PiecePool();
+        return *pool;
+    }
+    // run fn(1) .. fn(n-1) on pool threads and fn(0) on the caller; returns
+    // when all n have finished
+    void run(int n, const std::function<void(int)>& fn) {
+        struct Latch {
+            std::mutex m;
+            std::condition_variable cv;
+            int left;
+        } latch;
+        latch.left = n - 1;
+        ensure(n - 1);
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            for (int t = 1; t < n; ++t)
+                q_.push_back([&fn, &latch, t] {
+                    fn(t);
+                    std::lock_guard<std::mutex> l2(latch.m);
+                    if (--latch.left == 0) latch.cv.notify_all();
+                });
+        }
+        cv_.notify_all();
+        fn(0);
+        std::unique_lock<std::mutex> lk(latch.m);
+        latch.cv.wait(lk, [&] { return latch.left == 0; });
+    }
+
+  private:
+    void ensure(int k) {
+        std::lock_guard<std::mutex> lk(m_);
+        while ((int)nthreads_ < k) {
+            std::thread([this] { loop(); }).detach();
+            ++nthreads_;
+        }
+    }
+    void loop() {
+        for (;;) {
+            std::function<void()> task;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return !q_.empty(); });
+                task = std::move(q_.front());
+                q_.erase(q_.begin());
+            }
+            task();
+        }
+    }
+    std::mutex m_;
+    std::condition_variable cv_;
+    std::vector<std::function<void()>> q_;
+    size_t nthreads_ = 0;
 };
 
 void run_piece(const LdgChainParams& P, int64_t limit, const int64_t* rs, const int64_t* rl, const double* rm,
@@ -928,18 +993,15 @@ extern "C" int ldg_field_chain_mt(const LdgChainParams* P, const int64_t* run_st
         limit[t] = t == nthreads - 1 ? P->nblocks : std::min<long long>(P->nblocks, b0 + (t + 1) * seg + margin_blocks);
     }
     {
-        std::vector<std::thread> th;
         // a field read advances at least ~10 blocks; a piece that fills its
         // buffer stops (LDG_CHAIN_STOP_FULL) and the caller resumes
         auto cap = [&](int t) {
             const long long first = t == 0 ? b0 : b0 + t * seg;
             return (int32_t)std::min<long long>(max_plans, (limit[t] - first) / 8 + 16);
         };
-        for (int t = 1; t < nthreads; ++t)
-            th.emplace_back(run_piece, std::cref(*P), limit[t], run_start, run_len, run_mean, nruns, cap(t),
-                            std::ref(pcs[t]));
-        run_piece(*P, limit[0], run_start, run_len, run_mean, nruns, cap(0), pcs[0]);
-        for (auto& x : th) x.join();
+        PiecePool::get().run(nthreads, [&](int t) {
+            run_piece(*P, limit[t], run_start, run_len, run_mean, nruns, cap(t), pcs[t]);
+        });
     }
     for (const Piece& pc : pcs)
         if (pc.rc != 0) return pc.rc;

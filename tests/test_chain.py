@@ -121,6 +121,24 @@ def test_parallel_chain_equals_serial(capture):
         assert got.tobytes() == whole.tobytes()
 
 
+def test_parallel_chain_concurrent_callers(capture):
+    """Several host threads walking captures at once share the chain's
+    thread pool; each gets the plans of its own sequential walk."""
+    from concurrent.futures import ThreadPoolExecutor
+    from ldgpu.lines import parallel_chain
+    rf, arrays, nb = capture
+    runs = host_sync_runs(rf, arrays["demod_05"])
+    whole, _, _ = run_chain(rf, runs, nb)
+
+    def one(k):
+        got, _, _ = parallel_chain(rf, runs, nb, None, 2 + k % 3, margin_blocks=100, min_seg_blocks=30)
+        return got.tobytes()
+
+    with ThreadPoolExecutor(6) as ex:
+        outs = list(ex.map(one, range(24)))
+    assert all(o == whole.tobytes() for o in outs)
+
+
 def test_chain_takes_previous_field_inputs(monkeypatch):
     """Seeded dropouts that hide a field's vertical interval make its line 0
     depend on the previous field's refined line locations (getLine0,
