@@ -7,6 +7,7 @@
 // enqueues work; host buffers make the call copy in, run and copy out
 // synchronously (the plain, one-block-at-a-time form the reference's
 // DemodCache workers use).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -80,6 +81,7 @@ struct ldg_ctx {
     // in-place variant: per filter the bin-pair table (ip::kPairs float4) and,
     // for the RFVideo filters, the position-order table (kM float2); W_N^k per pair
     float4* d_fpair[LDG_NFILTERS] = {};
+    int fband[LDG_NFILTERS][2] = {};  // first and last bin whose float32 value is not zero
     float2* d_fpos[LDG_NFILTERS] = {};
     float2* d_twpair = nullptr;
     int variant = ldg::kVariantStockham;
@@ -145,6 +147,8 @@ void variant_tables(const ldg_ctx* c, ldg::DemodParams* p) {
     p->g_pos = c->d_fpos[LDG_F_VIDEO_G];
     p->godd_pos = c->d_fpos[LDG_F_VIDEO_G_ODD];
     p->tw_pair = c->d_twpair;
+    p->efm_klo = c->fband[LDG_F_EFM][0];
+    p->efm_khi = c->fband[LDG_F_EFM][1];
 }
 
 int grow(void** p, size_t* cap, size_t need) {
@@ -358,6 +362,12 @@ int ldg_set_filter(ldg_ctx* c, int32_t which, const double* reim, int64_t nbins)
     DeviceGuard g(c->device);
     std::vector<float2> h(nbins);
     for (int64_t k = 0; k < nbins; ++k) h[k] = make_float2((float)reim[2 * k], (float)reim[2 * k + 1]);
+    int klo = (int)nbins, khi = -1;
+    for (int k = 0; k < (int)nbins; ++k)
+        if (h[k].x != 0.f || h[k].y != 0.f) {
+            klo = std::min(klo, k);
+            khi = k;
+        }
     // the in-place variant's layouts of the same float32 values: per bin pair
     // u the bins k = bin_of(pair_pos(u)) and M - k (M itself for k = 0), and
     // for the RFVideo filters every bin at its position
@@ -377,6 +387,8 @@ int ldg_set_filter(ldg_ctx* c, int32_t which, const double* reim, int64_t nbins)
     LDG_CK(cudaMemcpy(c->d_filter[which], h.data(), nbins * sizeof(float2), cudaMemcpyHostToDevice));
     LDG_CK(cudaMemcpy(c->d_fpair[which], fp.data(), fp.size() * sizeof(float4), cudaMemcpyHostToDevice));
     if (pos) LDG_CK(cudaMemcpy(c->d_fpos[which], fq.data(), fq.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    c->fband[which][0] = klo;
+    c->fband[which][1] = khi;
     return LDG_OK;
 }
 

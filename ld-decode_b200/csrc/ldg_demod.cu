@@ -107,8 +107,14 @@ struct EfmStorer {
     __device__ void operator()(int, int m, float2 v) const {
         const int i0 = (2 * m - start) & (kN - 1);
         const int i1 = (i0 + 1) & (kN - 1);
-        if (i0 < len) __stcs(reinterpret_cast<short*>(out) + i0, (short)to_efm(v.x));
-        if (i1 < len) __stcs(reinterpret_cast<short*>(out) + i1, (short)to_efm(v.y));
+        const short a = (short)to_efm(v.x), b = (short)to_efm(v.y);
+        if (((i0 & 1) == 0) && i0 + 1 < len && ((reinterpret_cast<uintptr_t>(out + i0) & 3) == 0)) {
+            // both samples in one aligned 32-bit store (little-endian: a first)
+            __stcs(reinterpret_cast<int*>(out + i0), (int)(((unsigned)(unsigned short)b << 16) | (unsigned short)a));
+        } else {
+            if (i0 < len) __stcs(reinterpret_cast<short*>(out) + i0, a);
+            if (i1 < len) __stcs(reinterpret_cast<short*>(out) + i1, b);
+        }
     }
 };
 
@@ -202,13 +208,31 @@ __device__ void post_r2c(float2* S, const Tables& t, float2* park, const float2*
     }
 }
 
+// Is the bin pair (k, M - k) inside the band [klo, khi] where the filter's
+// float32 bins are not zero?  (Outside it X * F is zero and so is the C2R
+// input; for a band-limited filter such as the EFM one most pairs are.)
+__device__ __forceinline__ bool pair_live(int k, int klo, int khi) {
+    const int m = k == 0 ? kM : kM - k;
+    return (k >= klo && k <= khi) || (m >= klo && m <= khi);
+}
+
 // C2R input of X * F in S, X from the parked spectrum; two bins per step,
-// loads first.
-__device__ void pre_c2r(float2* S, const Tables& t, const float2* park, const float2* F) {
+// loads first.  Pairs outside F's band [klo, khi] are written as zeros
+// without their loads.
+__device__ void pre_c2r(float2* S, const Tables& t, const float2* park, const float2* F, int klo = 0,
+                        int khi = kM) {
     const int t0 = threadIdx.x;
+    const float2 zero = make_float2(0.f, 0.f);
 #pragma unroll 1
     for (int i = 0; i < kM / 2 / kThreads; i += 2) {
         const int ka = t0 + i * kThreads, kb = ka + kThreads;
+        if (!pair_live(ka, klo, khi) && !pair_live(kb, klo, khi)) {
+            S[pad(ka)] = zero;
+            if (ka) S[pad(kM - ka)] = zero;
+            S[pad(kb)] = zero;
+            S[pad(kM - kb)] = zero;
+            continue;
+        }
         const float2 xka = park[ka], xkb = park[kb], xmb = park[kM - kb];
         const float2 xma = ka ? park[kM - ka] : xka;
         const float2 fka = __ldg(F + ka), fma = __ldg(F + kM - ka), fkb = __ldg(F + kb), fmb = __ldg(F + kM - kb);
@@ -222,8 +246,12 @@ __device__ void pre_c2r(float2* S, const Tables& t, const float2* park, const fl
     }
     if (t0 == 0) {
         const int k = kM / 2;
-        const float2 x = park[k];
-        c2r_pair(S, k, cmul(x, __ldg(F + k)), cmul(x, __ldg(F + k)), __ldg(t.t32 + k));
+        if (pair_live(k, klo, khi)) {
+            const float2 x = park[k];
+            c2r_pair(S, k, cmul(x, __ldg(F + k)), cmul(x, __ldg(F + k)), __ldg(t.t32 + k));
+        } else {
+            S[pad(k)] = zero;
+        }
     }
 }
 
@@ -369,7 +397,7 @@ __device__ __forceinline__ void demod_block(const DemodParams& p, int blk, float
 
     // ---- EFM
     if (p.o_efm) {
-        pre_c2r(S, t, parkX, p.f_efm);
+        pre_c2r(S, t, parkX, p.f_efm, p.efm_klo, p.efm_khi);
         __syncthreads();
         fft16k<true>(S, t, SmemIO(), EfmStorer{p.o_efm + (long long)blk * p.s_efm.len, p.s_efm.start, p.s_efm.len});
     }
@@ -554,13 +582,23 @@ __device__ void post_r2c_ip(float2* S, const float2* twp, float2* park, const fl
 
 // pre_c2r in position order: the C2R input of X * F in S, X from the parked
 // spectrum (position order).
-__device__ void pre_c2r_ip(float2* S, const float2* twp, const float2* park, const float4* FP) {
+__device__ void pre_c2r_ip(float2* S, const float2* twp, const float2* park, const float4* FP, int klo = 0,
+                           int khi = kM) {
     const int t0 = threadIdx.x;
+    const float2 zero = make_float2(0.f, 0.f);
 #pragma unroll 1
     for (int i = 0; i < 8; i += 2) {
         const int ua = t0 + i * kThreads, ub = ua + kThreads;
         const int pa = ip::pair_pos(ua), pb = ip::pair_pos(ub);
         const int qa = ip::partner_pos(pa), qb = ip::partner_pos(pb);
+        if (!pair_live(ip::bin_of(pa), klo, khi) && !pair_live(ip::bin_of(pb), klo, khi)) {
+            // pa is never position 0 (ua < 7680); pb is for the pair of bins 0 and M
+            S[pad(pa)] = zero;
+            if (qa != pa) S[pad(qa)] = zero;
+            S[pad(pb)] = zero;
+            if (pb != 0 && qb != pb) S[pad(qb)] = zero;
+            continue;
+        }
         const float2 xka = park[pa], xma = park[qa], xkb = park[pb], xmb = park[qb];
         const float4 fa = __ldg(FP + ua), fb = __ldg(FP + ub);
         const float2 wa = __ldg(twp + ua), wb = __ldg(twp + ub);
@@ -574,9 +612,13 @@ __device__ void pre_c2r_ip(float2* S, const float2* twp, const float2* park, con
     }
     if (t0 == 0) {
         const int u = kM / 2;
-        const float2 x = park[2];
-        const float4 f = __ldg(FP + u);
-        c2r_pair_ip(S, 2, 2, cmul(x, make_float2(f.x, f.y)), cmul(x, make_float2(f.z, f.w)), __ldg(twp + u));
+        if (pair_live(kM / 2, klo, khi)) {
+            const float2 x = park[2];
+            const float4 f = __ldg(FP + u);
+            c2r_pair_ip(S, 2, 2, cmul(x, make_float2(f.x, f.y)), cmul(x, make_float2(f.z, f.w)), __ldg(twp + u));
+        } else {
+            S[pad(2)] = zero;
+        }
     }
 }
 
@@ -647,7 +689,7 @@ __device__ __forceinline__ void demod_block_ip(const DemodParams& p, int blk, fl
                        RealStorer{p.o_rfhpf + (long long)blk * p.s_rfhpf.len, p.s_rfhpf.start, p.s_rfhpf.len, 0});
     }
     if (p.o_efm) {
-        pre_c2r_ip(S, p.tw_pair, parkX, p.fp_efm);
+        pre_c2r_ip(S, p.tw_pair, parkX, p.fp_efm, p.efm_klo, p.efm_khi);
         __syncthreads();
         ip::fft16k_inv(S, tw, SmemIO(),
                        EfmStorer{p.o_efm + (long long)blk * p.s_efm.len, p.s_efm.start, p.s_efm.len});

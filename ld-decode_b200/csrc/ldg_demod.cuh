@@ -78,6 +78,9 @@ struct DemodParams {
     const float2* g_pos;             // G at positions: g_pos[p] = G[bin_of(p)], p < M
     const float2* godd_pos;
     const float2* tw_pair;           // W_N^k of pair u
+    // bins [efm_klo, efm_khi] outside which the EFM filter's float32 bins are
+    // zero (its C2R input is zero there)
+    int efm_klo, efm_khi;
 };
 
 enum { kVariantStockham = 0, kVariantInPlace = 1, kNumVariants = 2 };
