@@ -88,6 +88,9 @@ def parse():
                     help="Field.wow_level_adjust_smoothing of the TBC (0: off, the reference's default)")
     ap.add_argument("--no-analog-audio", action="store_true",
                     help="leave the 44.1 kHz analog audio of the fields out of the step")
+    ap.add_argument("--e2e-efm", default="edges", choices=["edges", "samples"],
+                    help="end to end, the EFM output crosses to the host as its zero crossings (what the EFM PLL "
+                         "consumes, with each field's slice bounds) or as the int16 samples")
     ap.add_argument("--mixed", type=int, default=0,
                     help="mixed-batch workload instead: this many captures, lengths uniform in 0.5-8 s, "
                          "half NTSC / half PAL, own seed and SNR (30-45 dB) each")
@@ -181,6 +184,7 @@ def run_gpu(args):
     from ldgpu.fieldread import blocks_in_capture
     from ldgpu.audio import downscale_audio_located
     from ldgpu.lines import LineLocator, field_levels, tbc_batch
+    from ldgpu.efm import EFM_PLL, efm_edges, field_efm_slices
     wow_opts = dict(wow_interpolation_method=args.wow_interp, wow_smoothing=args.wow_smoothing)
     from ldgpu.synth import inject_dropouts, synth_capture
 
@@ -239,11 +243,17 @@ def run_gpu(args):
                                      done=None)
     levels = field_levels(rf)
     nchunks = max(1, min(args.chunks, nblocks // 64))
+    lib = L.load()
     # chunk c holds a share proportional to taper**c of the blocks: a smaller
     # last chunk shortens the tail (its line locations and TBC) after the demod
     w = [args.chunk_taper ** c for c in range(nchunks)]
     cum = np.concatenate([[0.0], np.cumsum(w)]) / sum(w)
     bounds = [int(round(x * nblocks)) for x in cum]
+    # end to end, the EFM output as its zero crossings: room per chunk for
+    # one crossing per 4 samples (band-limited EFM crosses every ~25)
+    edges_mode = not args.no_e2e and args.e2e_efm == "edges"
+    ecap = np.array([(bounds[c + 1] - bounds[c]) * U // 4 for c in range(nchunks)], np.int64)
+    eoff = np.concatenate([[0], np.cumsum(ecap)[:-1]]).astype(np.int64)
     streamB = torch.cuda.Stream(priority=-1)   # line locations
     streamC = torch.cuda.Stream(priority=-1)   # TBC of ranges whose line locations are final
     streamS = torch.cuda.Stream(priority=-1)   # sync-run scans
@@ -320,10 +330,9 @@ def run_gpu(args):
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(stream)
             evs.append(ev)
-            if io is not None:
+            if io is not None and not edges_mode:
                 streamD.wait_event(ev)
                 o0, o1 = bounds[c] * U, bounds[c + 1] * U
-                q0, q1 = bounds[c] * 991, bounds[c + 1] * 991
                 with torch.cuda.stream(streamD):
                     io["efm"][o0:o1].copy_(bs.outs["efm"][o0:o1], non_blocking=True)
         marks["demod_end"] = evs[-1]
@@ -333,7 +342,28 @@ def run_gpu(args):
         for c in range(nchunks):
             streamB.wait_event(evs[c])
             streamS.wait_event(evs[c])
+            eev = None
+            if io is not None and edges_mode:
+                # the chunk's EFM zero crossings (stream S, before its sync-run scan,
+                # whose stream synchronisation then makes the count readable)
+                base = bounds[c] * U
+                L.check(lib.ldg_efm_edges(bs.outs["efm"].data_ptr() + 2 * base, (bounds[c + 1] - bounds[c]) * U,
+                                          1 if c else 0, base, bs.edges.data_ptr() + 8 * int(eoff[c]),
+                                          int(ecap[c]), io["ecount"].data_ptr() + 8 * c, bs.escratch.data_ptr(),
+                                          streamS.cuda_stream))
+                eev = torch.cuda.Event()
+                eev.record(streamS)
             loc.advance(bounds[c + 1], stream=streamB, scan_stream=streamS)
+            if eev is not None:
+                eev.synchronize()
+                k = int(io["ecount"][c])
+                if k > ecap[c]:
+                    raise RuntimeError(f"chunk {c}: {k} EFM crossings, room for {int(ecap[c])}")
+                io["ecounts"][c] = k
+                streamD.wait_event(eev)
+                e0_, e1_ = 8 * int(eoff[c]), 8 * (int(eoff[c]) + k)
+                with torch.cuda.stream(streamD):
+                    io["edges"][e0_:e1_].copy_(bs.edges[e0_:e1_], non_blocking=True)
             # TBC of each range of fields as its line locations become final
             # (stream C: overlaps the NTSC burst chain's next range and the demod)
             while loc.ready and bs.pics is not None:
@@ -363,6 +393,11 @@ def run_gpu(args):
                         io["pics"][lo * fsz:hi * fsz].copy_(bs.pics[lo * fsz:hi * fsz], non_blocking=True)
                         if do_audio:
                             io["aud"][lo * AS:hi * AS].copy_(bs.aud[lo * AS:hi * AS], non_blocking=True)
+                        if edges_mode:
+                            # each field's EFM slice for the PLL (its bounds and end samples)
+                            eb, es = field_efm_slices(loc.fields, bs.outs["efm"], lo, hi - lo)
+                            io["ebounds"][lo:hi].copy_(eb, non_blocking=True)
+                            io["esamples"][lo:hi].copy_(es, non_blocking=True)
         end = torch.cuda.Event(enable_timing=True)
         if overlap:
             # the next step (on the other buffer set) starts its demod while
@@ -395,6 +430,10 @@ def run_gpu(args):
     alt.cap.copy_(cap)
     alt.pics = torch.empty(nf * fsz, dtype=torch.uint16, device="cuda")
     alt.aud = torch.zeros(nf * AS, dtype=torch.int16, device="cuda")
+    for bs_ in (main, alt):
+        bs_.edges = torch.empty(8 * int(ecap.sum()) if edges_mode else 8, dtype=torch.uint8, device="cuda")
+        bs_.escratch = torch.empty(max(int(L.load().ldg_efm_edges_scratch_bytes((bounds[c + 1] - bounds[c]) * U))
+                                       for c in range(nchunks)), dtype=torch.uint8, device="cuda")
 
     def barrier():
         replica_barrier(world)
@@ -490,10 +529,18 @@ def run_gpu(args):
         host_cap = cap.cpu().pin_memory()
 
         def make_io():
-            return {"cap": host_cap,
-                    "pics": torch.empty(nf * fsz, dtype=torch.uint16).pin_memory(),
-                    "efm": torch.empty(nout, dtype=torch.int16).pin_memory(),
-                    "aud": torch.zeros(nf * AS, dtype=torch.int16).pin_memory()}
+            io = {"cap": host_cap,
+                  "pics": torch.empty(nf * fsz, dtype=torch.uint16).pin_memory(),
+                  "aud": torch.zeros(nf * AS, dtype=torch.int16).pin_memory()}
+            if edges_mode:
+                io.update({"edges": torch.empty(8 * int(ecap.sum()), dtype=torch.uint8).pin_memory(),
+                           "ecount": torch.zeros(nchunks, dtype=torch.int64).pin_memory(),
+                           "ecounts": [0] * nchunks,
+                           "ebounds": torch.zeros((nf, 2), dtype=torch.int64).pin_memory(),
+                           "esamples": torch.zeros((nf, 2), dtype=torch.int16).pin_memory()})
+            else:
+                io["efm"] = torch.empty(nout, dtype=torch.int16).pin_memory()
+            return io
         sets, ios = [main, alt], [make_io(), make_io()]
         for k in range(2):  # warm the copy path on both sets
             assert len(step(ios[k], sets[k])) == nf
@@ -513,19 +560,50 @@ def run_gpu(args):
         barrier()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, "cuda")
         h2d = nsamples * 2
-        d2h = nf * fsz * 2 + nout * 2 + (nf * AS * 2 if do_audio else 0)
+        last = ios[(args.steps - 1) % 2]
+        efm_d2h = 8 * sum(last["ecounts"]) + nf * (16 + 4) if edges_mode else nout * 2
+        d2h = nf * fsz * 2 + efm_d2h + (nf * AS * 2 if do_audio else 0)
         e2e = {"value": world * nout / (e2e_ms * 1e-3) / 1e6, "unit": "MSPS", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                "path": "pinned host capture -> ldg_demod_blocks -> ldg_sync_runs + ldg_field_chain + "
-                       "ldg_lines_refine -> ldg_tbc_fields + ldg_audio_downscale -> host fields, EFM, 44.1 kHz "
-                       "audio; per chunk, the input "
+                       "ldg_lines_refine -> ldg_tbc_fields + ldg_audio_downscale (+ ldg_efm_edges) -> host "
+                       "fields, EFM, 44.1 kHz audio; per chunk, the input "
                        "copy and the output copies overlap the other chunks' work; two buffer sets, so a "
                        "step's output copies also overlap the next step"}
         # the end-to-end outputs of the last step equal the device-resident run's
-        last = ios[(args.steps - 1) % 2]
-        e2e["outputs_match"] = bool(torch.equal(last["pics"].view(torch.int16), pics.cpu().view(torch.int16)) and
-                                    torch.equal(last["efm"], outs["efm"].cpu()) and
-                                    torch.equal(last["aud"], main.aud.cpu()))
+        same = (torch.equal(last["pics"].view(torch.int16), pics.cpu().view(torch.int16)) and
+                torch.equal(last["aud"], main.aud.cpu()))
+        if edges_mode:
+            # the crossings (chunk by chunk) equal those of the whole EFM array,
+            # the slices those of the located fields, and the PLL run from them
+            # the PLL run from the samples (first 32 fields)
+            from ldgpu import lib as Lb
+            got = np.concatenate([last["edges"][8 * int(eoff[c]):8 * (int(eoff[c]) + last["ecounts"][c])].numpy()
+                                  for c in range(nchunks)]).view(Lb.EFM_EDGE_DTYPE)
+            whole = efm_edges(outs["efm"])
+            eb, es = field_efm_slices(main.loc.fields, outs["efm"])
+            same = same and got.tobytes() == whole.tobytes() and torch.equal(last["ebounds"], eb.cpu()) and \
+                torch.equal(last["esamples"], es.cpu())
+            xs = outs["efm"].cpu().numpy()
+            pa, pb = EFM_PLL(), EFM_PLL()
+            pll_same, tvals = True, 0
+            for i in range(min(32, nf)):
+                lo_, hi_ = (int(v) for v in last["ebounds"][i])
+                ta = pa.process(xs[lo_:hi_])
+                tb = pb.process_edges(got, lo_, hi_, int(last["esamples"][i, 0]), int(last["esamples"][i, 1]))
+                pll_same = pll_same and np.array_equal(ta, tb)
+                tvals += len(ta)
+            pll_same = pll_same and pa.state() == pb.state()
+            e2e["efm"] = {"form": "zero crossings (ldg_efm_edges, 8 bytes each) + per-field slice bounds and end "
+                                  "samples; the EFM PLL (ldg_efm_pll_process_edges) turns them into the reference's "
+                                  "T-values without the samples",
+                          "crossings_per_step": int(sum(last["ecounts"])),
+                          "bytes_per_step": int(efm_d2h), "int16_samples_bytes": int(nout * 2),
+                          "pll_from_crossings_equals_pll_from_samples": bool(pll_same),
+                          "pll_fields_checked": min(32, nf), "t_values_checked": int(tvals)}
+        else:
+            same = same and torch.equal(last["efm"], outs["efm"].cpu())
+        e2e["outputs_match"] = bool(same)
 
     # ---- plain form: one demodblock() call per block through the Python API
     plain = None

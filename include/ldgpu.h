@@ -694,6 +694,43 @@ int ldg_efm_pll_process(ldg_efm_pll* pll, const int16_t* in, int64_t n, int8_t* 
  * refClockTime}, istate = {zcPreviousInput, frequencyHysteresis, tCounter}. */
 int ldg_efm_pll_state(const ldg_efm_pll* pll, double* dstate, int32_t* istate);
 
+/* One zero crossing of an EFM sample array, as EFM_PLL.process detects it
+ * (efm_pll.py:148-151): sample `pos` has a sign (negative / not negative)
+ * other than the sample before it; `prev` and `cur` are the two values, from
+ * which the PLL's interpolated fraction -prev / (cur - prev) follows. */
+typedef struct ldg_efm_edge {
+    int32_t pos;
+    int16_t prev;
+    int16_t cur;
+} ldg_efm_edge;
+
+/* GPU: the zero crossings of efm[0, n) (device int16, e.g. the demodulator's
+ * efm output over a range of blocks): every i with sign(efm[i-1]) !=
+ * sign(efm[i]); for i = 0 the sample before is efm[-1] when has_before,
+ * else 0 (no crossing at 0 for a non-negative efm[0]).  Written in
+ * increasing position to `edges` (device, at most `cap`), each pos =
+ * pos_offset + i (pos_offset + n must fit int32); their number to *count
+ * (device or host-mapped pinned memory, may be NULL), by the GPU in stream
+ * order, so the host can read it after a synchronisation without a copy.
+ * More than cap crossings: *count holds the number found, cap are written.
+ * `scratch`: ldg_efm_edges_scratch_bytes(n) bytes of device memory, not
+ * shared with a call in flight on another stream.  Runs on the current
+ * device.  No counterpart in the reference as one call. */
+int64_t ldg_efm_edges_scratch_bytes(int64_t n);
+int ldg_efm_edges(const int16_t* efm, int64_t n, int32_t has_before, int64_t pos_offset, ldg_efm_edge* edges,
+                  int64_t cap, int64_t* count, void* scratch, void* stream);
+
+/* EFM_PLL.process over the samples [lo, hi) of an array whose zero
+ * crossings are `edges` (sorted by position, host memory; those inside
+ * (lo, hi) are used, the sample at lo is tested against the PLL's previous
+ * sample as the reference's loop does), with first = sample lo and last =
+ * sample hi - 1: the same T-values and loop state as ldg_efm_pll_process
+ * on those samples (out_cap >= hi - lo, as there).  LDdecode feeds the PLL
+ * one field's slice after another (core.py:3918-3925); the slices of
+ * consecutive fields may overlap or leave gaps, and each call takes one. */
+int ldg_efm_pll_process_edges(ldg_efm_pll* pll, const ldg_efm_edge* edges, int64_t nedges, int64_t lo, int64_t hi,
+                              int16_t first, int16_t last, int8_t* out, int64_t out_cap, int64_t* out_count);
+
 #ifdef __cplusplus
 }
 #endif

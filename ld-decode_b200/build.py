@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
          "-Xptxas", "-v"]
 
-SOURCES = ["ldg_demod.cu", "ldg_tbc.cu", "ldg_abi.cu", "ldg_noalloc.cu", "ldg_ac3.cu", "ldg_chain.cpp", "ldg_lines.cu", "ldg_queue.cu", "ldg_dropouts.cu", "ldg_ingest.cu", "ldg_copy.cu", "ldg_audio.cu", "ldg_efm.cpp"]
+SOURCES = ["ldg_demod.cu", "ldg_tbc.cu", "ldg_abi.cu", "ldg_noalloc.cu", "ldg_ac3.cu", "ldg_chain.cpp", "ldg_lines.cu", "ldg_queue.cu", "ldg_dropouts.cu", "ldg_ingest.cu", "ldg_copy.cu", "ldg_audio.cu", "ldg_efm.cpp", "ldg_efm_edges.cu"]
 
 
 def nvcc():

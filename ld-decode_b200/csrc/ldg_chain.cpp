@@ -856,6 +856,7 @@ extern "C" int64_t ldg_abi_sizeof(const char* name) {
     if (n == "ldg_audio2_segment") return sizeof(ldg_audio2_segment);
     if (n == "ldg_audio_field") return sizeof(ldg_audio_field);
     if (n == "ldg_audio_params") return sizeof(ldg_audio_params);
+    if (n == "ldg_efm_edge") return sizeof(ldg_efm_edge);
     return -1;
 }
 

@@ -176,6 +176,50 @@ int ldg_efm_pll_process(ldg_efm_pll* pll, const int16_t* in, int64_t n, int8_t* 
     return LDG_OK;
 }
 
+int ldg_efm_pll_process_edges(ldg_efm_pll* pll, const ldg_efm_edge* edges, int64_t nedges, int64_t lo, int64_t hi,
+                              int16_t first, int16_t last, int8_t* out, int64_t out_cap, int64_t* out_count) {
+    if (!pll || !out_count || (nedges > 0 && !edges) || (hi > lo && !out))
+        return ldg::api_fail(LDG_ERR_ARG, "ldg_efm_pll_process_edges: NULL argument");
+    if (nedges < 0 || hi < lo || lo < 0 || out_cap < hi - lo)
+        return ldg::api_fail(LDG_ERR_ARG, "ldg_efm_pll_process_edges: bad range or out smaller than the slice");
+    ldg_efm_pll& s = *pll;
+    int64_t count = 0;
+    *out_count = 0;
+    if (hi == lo) return LDG_OK;
+    double delta = s.delta;
+    int64_t run_start = lo;
+    auto edge = [&](int64_t i, int16_t prev, int16_t cur) {
+        delta = add_ones(delta, i - run_start);
+        const double fraction = (double)(-(int64_t)prev) / (double)((int64_t)cur - (int64_t)prev);
+        if (!push_edge(s, delta + fraction, out, out_cap, count)) return false;
+        delta = 1.0 - fraction;
+        run_start = i + 1;
+        return true;
+    };
+    // the sample at lo against the PLL's previous sample
+    if ((((int)s.zc_prev) ^ (int)first) < 0 && !edge(lo, s.zc_prev, first)) {
+        *out_count = count;
+        return ldg::api_fail(LDG_ERR_RANGE, "ldg_efm_pll_process_edges: more T-values than input samples");
+    }
+    // crossings strictly inside the slice: their previous sample is in it too
+    int64_t a = 0, b = nedges;
+    while (a < b) {  // first edge with pos > lo
+        const int64_t m = (a + b) / 2;
+        if ((int64_t)edges[m].pos <= lo) a = m + 1;
+        else b = m;
+    }
+    for (int64_t k = a; k < nedges && (int64_t)edges[k].pos < hi; ++k) {
+        if (!edge(edges[k].pos, edges[k].prev, edges[k].cur)) {
+            *out_count = count;
+            return ldg::api_fail(LDG_ERR_RANGE, "ldg_efm_pll_process_edges: more T-values than input samples");
+        }
+    }
+    s.delta = add_ones(delta, hi - run_start);
+    s.zc_prev = last;
+    *out_count = count;
+    return LDG_OK;
+}
+
 int ldg_efm_pll_state(const ldg_efm_pll* pll, double* dstate, int32_t* istate) {
     if (!pll || !dstate || !istate) return ldg::api_fail(LDG_ERR_ARG, "ldg_efm_pll_state: NULL argument");
     dstate[0] = pll->delta;

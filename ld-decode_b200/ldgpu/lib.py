@@ -9,6 +9,8 @@ import ctypes
 import os
 import threading
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libldgpu.so")
 
@@ -118,6 +120,13 @@ class RfTbcField(ctypes.Structure):
                 ("linecount", c_i32), ("linelen", c_i32), ("delay", c_f64), ("out", c_p)]
 
 
+class EfmEdge(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_int32), ("prev", ctypes.c_int16), ("cur", ctypes.c_int16)]
+
+
+EFM_EDGE_DTYPE = np.dtype([("pos", "<i4"), ("prev", "<i2"), ("cur", "<i2")])
+
+
 class DropoutField(ctypes.Structure):
     _fields_ = [("demod", c_p), ("demod_05", c_p), ("demod_raw", c_p), ("rfhpf", c_p), ("len", c_i64),
                 ("linelocs", c_p), ("nlines", c_i32), ("lineoffset", c_i32), ("linecount", c_i32),
@@ -215,6 +224,10 @@ SIGNATURES = {
     "ldg_efm_pll_destroy": (ctypes.c_int, [c_p]),
     "ldg_efm_pll_process": (ctypes.c_int, [c_p, c_p, c_i64, c_p, c_i64, ctypes.POINTER(c_i64)]),
     "ldg_efm_pll_state": (ctypes.c_int, [c_p, c_p, c_p]),
+    "ldg_efm_pll_process_edges": (ctypes.c_int, [c_p, c_p, c_i64, c_i64, c_i64, ctypes.c_int16, ctypes.c_int16, c_p,
+                                                 c_i64, ctypes.POINTER(c_i64)]),
+    "ldg_efm_edges_scratch_bytes": (c_i64, [c_i64]),
+    "ldg_efm_edges": (ctypes.c_int, [c_p, c_i64, c_i32, c_i64, c_p, c_i64, c_p, c_p, c_p]),
 }
 
 # ABI of the library this binding is written for (LDG_ABI_VERSION in
@@ -226,7 +239,7 @@ ABI_STRUCTS = [("ldg_chain_params", ChainParams), ("ldg_chain_state", ChainState
                ("ldg_demod_args", DemodArgs), ("ldg_slice", Slice), ("ldg_work_item", WorkItem),
                ("ldg_dropout_field", DropoutField), ("ldg_dropout_params", DropoutParams),
                ("ldg_rftbc_field", RfTbcField), ("ldg_audio2_segment", Audio2Segment),
-               ("ldg_audio_field", AudioField), ("ldg_audio_params", AudioParams)]
+               ("ldg_audio_field", AudioField), ("ldg_audio_params", AudioParams), ("ldg_efm_edge", EfmEdge)]
 
 _lib = None
 _lock = threading.Lock()

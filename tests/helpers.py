@@ -68,3 +68,16 @@ class OracleBlocks:
                     self.cache[b] = rv
         bl = range(first_block, first_block + nblocks)
         return {k: np.concatenate([self.cache[b][k] for b in bl]) for k in self.keys}
+
+
+def efm_crossings(x, before=None):
+    """Zero crossings of int16 array x as EFM_PLL.process tests them
+    (efm_pll.py:148-151): i with sign(x[i-1]) != sign(x[i]), x[-1] = before
+    (no crossing at 0 without it); an EFM_EDGE_DTYPE array."""
+    from ldgpu import lib as L
+    x = np.asarray(x, np.int16)
+    prev = np.concatenate([[before if before is not None else 0], x[:-1]]).astype(np.int16)
+    i = np.nonzero((prev.astype(np.int32) ^ x.astype(np.int32)) < 0)[0]
+    e = np.empty(len(i), L.EFM_EDGE_DTYPE)
+    e["pos"], e["prev"], e["cur"] = i, prev[i], x[i]
+    return e

@@ -100,7 +100,7 @@ def test_chain_stops_on_level_recalibration():
 
 def test_abi_struct_sizes():
     h = L.load()
-    assert len(L.ABI_STRUCTS) == 15
+    assert len(L.ABI_STRUCTS) == 16
     for name, t in L.ABI_STRUCTS:
         assert h.ldg_abi_sizeof(name.encode()) == ctypes.sizeof(t), name
 

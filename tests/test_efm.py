@@ -80,3 +80,28 @@ def test_efm_pll_rejects_small_output_and_wrong_dtype():
     n = ctypes.c_int64()
     rc = L.load().ldg_efm_pll_process(pll._h, x.ctypes.data, 100, out.ctypes.data, 10, ctypes.byref(n))
     assert rc == L.LDG_ERR_ARG
+
+
+@pytest.mark.parametrize("name", [c[0] for c in EFM_CASES])
+def test_efm_pll_from_edges_equals_samples(name):
+    """The PLL run from the signal's zero crossings over field-like slices
+    that overlap or leave gaps (as consecutive fields' EFM slices do) gives
+    the T-values and state of the PLL fed those slices' samples."""
+    from ldgpu.efm import EFM_PLL
+    from helpers import efm_crossings
+    x, _ = efm_case(name)
+    edges = efm_crossings(x)
+    rng = np.random.default_rng(7)
+    slices, lo = [], 0
+    while lo < len(x) - 10:
+        hi = min(len(x), lo + int(rng.integers(1, 40000)))
+        slices.append((lo, hi))
+        lo = max(0, hi + int(rng.integers(-3, 4)))  # overlap, touch or gap
+    a, b = EFM_PLL(), EFM_PLL()
+    for lo, hi in slices:
+        want = a.process(x[lo:hi])
+        got = b.process_edges(edges, lo, hi, x[lo], x[hi - 1])
+        np.testing.assert_array_equal(got, want)
+    assert a.state() == b.state()
+    a.close()
+    b.close()
