@@ -307,8 +307,26 @@ def run_gpu(args):
         input copies are issued as soon as this step's demods are, so the
         next step's first chunk does not wait for the host to reach it."""
         bs = bs or main
-        loc = bs.loc
-        overlap = overlap or io is not None
+        evs = step_start(io, bs)
+        if next_in is not None:
+            next_in[1].prefetched = copy_in(*next_in)
+        return step_finish(io, bs, evs, overlap or io is not None)
+
+    def steps_pipelined(n, ios=None):
+        """n steps back to back on the two buffer sets, each step's input copy
+        and demods issued before the host works through the step before it
+        (its line locations, TBC and copies), so the GPU always has the
+        next capture's demod queued."""
+        sets_ = (main, alt)
+        pend = step_start(ios[0] if ios else None, sets_[0])
+        for k in range(n):
+            nxt = step_start(ios[(k + 1) % 2] if ios else None, sets_[(k + 1) % 2]) if k + 1 < n else None
+            step_finish(ios[k % 2] if ios else None, sets_[k % 2], pend, True)
+            pend = nxt
+
+    def step_start(io, bs):
+        """A step's input copy (end to end) and demods; returns the chunks'
+        demod events."""
         if bs.done is not None:
             # the set's previous step (its line locations, TBC and, end to
             # end, its copies to the host) must be done before its outputs
@@ -321,7 +339,6 @@ def run_gpu(args):
         if io is not None:
             hevs = bs.prefetched if getattr(bs, "prefetched", None) else copy_in(io, bs)
             bs.prefetched = None
-        loc.begin(bs.farr)
         evs = []
         for c in range(nchunks):
             if hevs is not None:
@@ -337,8 +354,13 @@ def run_gpu(args):
                     io["efm"][o0:o1].copy_(bs.outs["efm"][o0:o1], non_blocking=True)
         marks["demod_end"] = evs[-1]
         bs.demod_done = evs[-1]
-        if next_in is not None:
-            next_in[1].prefetched = copy_in(*next_in)
+        return evs
+
+    def step_finish(io, bs, evs, overlap):
+        """The rest of a step started by step_start: line locations chunk by
+        chunk, TBC and audio of each finished range, the copies out."""
+        loc = bs.loc
+        loc.begin(bs.farr)
         for c in range(nchunks):
             streamB.wait_event(evs[c])
             streamS.wait_event(evs[c])
@@ -450,21 +472,18 @@ def run_gpu(args):
         step_tune = {}
         for b in (1, 2, 4):
             rf.blocks_per_cta = b
-            for k in range(2):
-                step(None, (main, alt)[k], overlap=True)
+            steps_pipelined(2)
             torch.cuda.synchronize()
             q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             q0.record(stream)
-            for k in range(4):
-                step(None, (main, alt)[k % 2], overlap=True)
+            steps_pipelined(4)
             for st_ in (streamB, streamC, streamS, streamA):
                 stream.wait_stream(st_)
             q1.record(stream)
             torch.cuda.synchronize()
             step_tune[b] = q0.elapsed_time(q1) / 4
         rf.blocks_per_cta = min(step_tune, key=step_tune.get)
-        for k in range(2):
-            step(None, (main, alt)[k], overlap=True)
+        steps_pipelined(2)
         torch.cuda.synchronize()
     loc.stats = {k: 0 for k in loc.stats}
     loc.timing = {}
@@ -488,15 +507,16 @@ def run_gpu(args):
     # the same steps back to back on the two buffer sets, each step's demod
     # starting while the previous step's line locations and TBC finish: the
     # throughput of a stream of captures (the reported value)
-    for k in range(2):
-        assert len(step(None, (main, alt)[k], overlap=True)) == nf
+    steps_pipelined(2)
     torch.cuda.synchronize()
+    assert len(main.loc.fields) == nf and len(alt.loc.fields) == nf
     barrier()
     o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     o0.record(stream)
     ar0 = marks["audio_ranges"]
-    for k in range(args.steps):
-        step(None, (main, alt)[k % 2], overlap=True)
+    hw0 = time.perf_counter()
+    steps_pipelined(args.steps)
+    pipelined_host_ms = (time.perf_counter() - hw0) * 1e3 / args.steps
     audio_ranges = (marks["audio_ranges"] - ar0) / args.steps
     for st_ in (streamB, streamC, streamS, streamA):
         stream.wait_stream(st_)
@@ -548,11 +568,11 @@ def run_gpu(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         e0.record(stream)
-        for k in range(args.steps):
-            # each step's input copy is issued during the step before it
-            # (the first step's inside the timed region too)
-            nxt = (ios[(k + 1) % 2], sets[(k + 1) % 2]) if k + 1 < args.steps else None
-            step(ios[k % 2], sets[k % 2], next_in=nxt)
+        # each step's input copy and demods are issued before the host works
+        # through the step before it (the first step's inside the timed region too)
+        hw0 = time.perf_counter()
+        steps_pipelined(args.steps, ios)
+        e2e_host_ms = (time.perf_counter() - hw0) * 1e3 / args.steps
         stream.wait_stream(streamD)
         stream.wait_stream(streamP)
         e1.record(stream)
@@ -604,6 +624,33 @@ def run_gpu(args):
         else:
             same = same and torch.equal(last["efm"], outs["efm"].cpu())
         e2e["outputs_match"] = bool(same)
+        # the PCIe floor: the step's copies alone, each direction and both at once
+        def copies(h2d_on, d2h_on):
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            q0.record(stream)
+            if h2d_on:
+                with torch.cuda.stream(streamH):
+                    main.cap.copy_(host_cap, non_blocking=True)
+            if d2h_on:
+                with torch.cuda.stream(streamD):
+                    last["pics"].view(torch.int16).copy_(main.pics.view(torch.int16), non_blocking=True)
+                    if edges_mode:
+                        nb_ = 8 * sum(last["ecounts"])
+                        last["edges"][:nb_].copy_(main.edges[:nb_], non_blocking=True)
+                    else:
+                        last["efm"].copy_(outs["efm"], non_blocking=True)
+            stream.wait_stream(streamH)
+            stream.wait_stream(streamD)
+            q1.record(stream)
+            torch.cuda.synchronize()
+            return q0.elapsed_time(q1)
+        copies(True, True)
+        pcie = {"h2d_ms": copies(True, False), "d2h_ms": copies(False, True), "both_ms": copies(True, True)}
+        pcie["h2d_gbs"] = h2d / pcie["h2d_ms"] / 1e6
+        pcie["d2h_gbs"] = (nf * fsz * 2 + efm_d2h) / pcie["d2h_ms"] / 1e6
+        e2e["pcie_alone"] = pcie
+        e2e["host_ms_per_step"] = e2e_host_ms  # the host's own loop (it returns before the GPU finishes)
 
     # ---- plain form: one demodblock() call per block through the Python API
     plain = None
@@ -737,13 +784,15 @@ def run_gpu(args):
         },
         "fields_per_s": world * nf / (ms_per_step * 1e-3),
         "isolated_step_ms": isolated_ms,
+        "host_ms_per_pipelined_step": pipelined_host_ms,
         "kernel_ms": {"demod_alone": dmed, "tbc_alone": tbc_med,
                       "step_demod_chunks_median": statistics.median(demod_ms),
                       "after_last_demod_median": statistics.median(tail_ms),
                       "note": f"{nchunks} chunks: line locations and TBC of chunk c overlap the demod of "
                               "chunk c+1; after_last_demod is the exposed tail of a step run alone "
                               "(isolated_step_ms); ms_per_step runs the steps back to back on two buffer sets, "
-                              "so a step's tail overlaps the next step's demod"},
+                              "each step's demods issued before the host works through the step before it, so a "
+                              "step's tail overlaps the next step's demod"},
         "autotune": None if tune is None else {
             "best": {"fft": ("stockham", "in_place")[tune["best"][0]], "blocks_per_cta": tune["best"][1]},
             "step_ms_by_blocks_per_cta": step_tune,
