@@ -416,10 +416,10 @@ def run_gpu(args):
                         if do_audio:
                             io["aud"][lo * AS:hi * AS].copy_(bs.aud[lo * AS:hi * AS], non_blocking=True)
                         if edges_mode:
-                            # each field's EFM slice for the PLL (its bounds and end samples)
-                            eb, es = field_efm_slices(loc.fields, bs.outs["efm"], lo, hi - lo)
-                            io["ebounds"][lo:hi].copy_(eb, non_blocking=True)
-                            io["esamples"][lo:hi].copy_(es, non_blocking=True)
+                            # each field's EFM slice for the PLL (its bounds and end
+                            # samples), written by the kernel straight into pinned memory
+                            field_efm_slices(loc.fields, bs.outs["efm"], lo, hi - lo, bounds=io["ebounds"][lo:hi],
+                                             samples=io["esamples"][lo:hi])
         end = torch.cuda.Event(enable_timing=True)
         if overlap:
             # the next step (on the other buffer set) starts its demod while

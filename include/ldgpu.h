@@ -720,6 +720,17 @@ int64_t ldg_efm_edges_scratch_bytes(int64_t n);
 int ldg_efm_edges(const int16_t* efm, int64_t n, int32_t has_before, int64_t pos_offset, ldg_efm_edge* edges,
                   int64_t cap, int64_t* count, void* scratch, void* stream);
 
+/* GPU: the EFM slice Field.downscale hands to the PLL for each of n fields,
+ * efm[int(linelocs[1]) : int(linelocs[end_line])] (core.py:2704-2707, with
+ * end_line = linecount + 1 and positions made capture-wide by the field's
+ * startloc): bounds[2i], bounds[2i+1] = that range of efm, samples[2i],
+ * samples[2i+1] = its first and last sample.  linelocs[i] is the device
+ * address of field i's FP64 line locations.  The input and output arrays
+ * may be device memory or pinned host memory (read and written by the
+ * kernel in stream order).  No counterpart in the reference as one call. */
+int ldg_efm_field_slices(const int64_t* startloc, const uint64_t* linelocs, const int32_t* end_line, int32_t n,
+                         const int16_t* efm, int64_t efm_len, int64_t* bounds, int16_t* samples, void* stream);
+
 /* EFM_PLL.process over the samples [lo, hi) of an array whose zero
  * crossings are `edges` (sorted by position, host memory; those inside
  * (lo, hi) are used, the sample at lo is tested against the PLL's previous

@@ -184,3 +184,45 @@ int ldg_efm_edges(const int16_t* efm, int64_t n, int32_t has_before, int64_t pos
 }
 
 }  // extern "C"
+
+namespace {
+
+// one thread per field: its EFM slice [startloc + int(ll[1]), startloc +
+// int(ll[end_line])) and the samples at both ends
+__global__ void efm_slices_kernel(const long long* __restrict__ startloc, const unsigned long long* __restrict__ llp,
+                                  const int* __restrict__ end_line, int n, const int16_t* __restrict__ efm,
+                                  long long efm_len, long long* bounds, int16_t* samples) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* ll = reinterpret_cast<const double*>(llp[i]);
+    const long long lo = startloc[i] + (long long)ll[1];  // truncation, as int() of the location
+    const long long hi = startloc[i] + (long long)ll[end_line[i]];
+    bounds[2 * i] = lo;
+    bounds[2 * i + 1] = hi;
+    samples[2 * i] = lo >= 0 && lo < efm_len ? efm[lo] : (int16_t)0;
+    samples[2 * i + 1] = hi - 1 >= 0 && hi - 1 < efm_len ? efm[hi - 1] : (int16_t)0;
+}
+
+}  // namespace
+
+extern "C" int ldg_efm_field_slices(const int64_t* startloc, const uint64_t* linelocs, const int32_t* end_line,
+                                    int32_t n, const int16_t* efm, int64_t efm_len, int64_t* bounds,
+                                    int16_t* samples, void* stream) {
+    if (n < 0 || (n > 0 && (!startloc || !linelocs || !end_line || !efm || !bounds || !samples)))
+        return ldg::api_fail(LDG_ERR_ARG, "ldg_efm_field_slices: NULL buffer or negative count");
+    if (n == 0) return LDG_OK;
+    const void* p[5] = {startloc, linelocs, end_line, bounds, samples};
+    void* d[5];
+    for (int k = 0; k < 5; ++k) {
+        d[k] = ldg::device_view(p[k]);
+        if (!d[k])
+            return ldg::api_fail(LDG_ERR_ARG, "ldg_efm_field_slices: arrays must be device memory or pinned host memory");
+    }
+    efm_slices_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+        static_cast<const long long*>(d[0]), static_cast<const unsigned long long*>(d[1]),
+        static_cast<const int*>(d[2]), n, efm, efm_len, static_cast<long long*>(d[3]), static_cast<int16_t*>(d[4]));
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return ldg::api_fail(LDG_ERR_CUDA, std::string("ldg_efm_field_slices: ") + cudaGetErrorString(e));
+    return LDG_OK;
+}

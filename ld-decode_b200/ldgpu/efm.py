@@ -108,68 +108,45 @@ def efm_edges(efm, has_before=False, pos_offset=0, stream=None):
     return out[:k * L.EFM_EDGE_DTYPE.itemsize].cpu().numpy().view(L.EFM_EDGE_DTYPE)
 
 
-def field_efm_slices(fields, efm, first=0, count=None):
+def field_efm_slices(fields, efm, first=0, count=None, bounds=None, samples=None, stream=None):
     """The EFM slice Field.downscale hands to the PLL for each of
     fields[first:first + count] (a LocatedFields): data['efm'][int(linelocs[1])
     : int(linelocs[linecount + 1])] (core.py:2704-2707) as capture-wide sample
     ranges [lo, hi), with the samples at lo and hi - 1 -- what
-    EFM_PLL.process_edges needs besides the crossings.  Device tensors
-    (int64 (count, 2), int16 (count, 2)) made by gathers on the current
-    stream from the fields' device line locations; the few per-field
-    integers from the host go over by an SM copy from pinned memory, not by
-    a copy-engine transfer that would queue behind bulk copies."""
+    EFM_PLL.process_edges needs besides the crossings.  One kernel
+    (ldg_efm_field_slices) on `stream` (default: torch's current stream),
+    reading the fields' device line locations; it writes into `bounds`
+    (int64 (count, 2)) and `samples` (int16 (count, 2)) when given -- device
+    or pinned host tensors, so the results can land on the host without a
+    copy -- else into new device tensors.  Returns (bounds, samples)."""
     import torch
-    n = len(fields) if count is None else count
-    dev = efm.device
     lib = L.load()
-    stream = torch.cuda.current_stream(dev)
-
-    def to_dev(a):
-        a = np.ascontiguousarray(a, np.int64)
-        h = torch.from_numpy(a).pin_memory()
-        d = torch.empty(a.shape, dtype=torch.int64, device=dev)
-        if a.size:
-            L.check(lib.ldg_copy_async(d.data_ptr(), h.data_ptr(), a.nbytes, stream.cuda_stream))
-        return d, h
-
-    bounds, samples, keep = [], [], []
-    k = 0  # field index of the part's first field
-    for part in fields._parts:
-        m = len(part[1]) if part[0] == "batch" else 1
-        lo, hi = max(first, k), min(first + n, k + m)
-        if lo < hi:
-            if part[0] == "batch":
-                _, pl, ll, _, _, _ = part
-                rows = torch.arange(lo - k, hi - k, device=dev)
-                if fields.rf.system == "PAL":
-                    lc = np.where(pl.isfirst[lo - k:hi - k] != 0, 312, 313)
-                else:
-                    lc = pl.linecount[lo - k:hi - k].astype(np.int64)
-                lc_t, h1 = to_dev(np.asarray(lc, np.int64) + 1)
-                st, h2 = to_dev(pl.startloc[lo - k:hi - k])
-                keep.extend((h1, h2))
-                a = st + ll[rows, 1].to(torch.int64)   # int() of a positive location truncates
-                b = st + ll[rows, lc_t].to(torch.int64)
-            else:
-                fl = part[1]
-                ll = np.asarray(fl.host_linelocs(), np.float64)
-                st = fl.window.startloc
-                ab, h1 = to_dev(np.array([[st + int(ll[1]), st + int(ll[fl.linecount + 1])]], np.int64))
-                keep.append(h1)
-                a, b = ab[:, 0], ab[:, 1]
-            bounds.append(torch.stack([a, b], 1))
-            samples.append(torch.stack([efm[a], efm[b - 1]], 1))
-        k += m
-    if not bounds:
-        return (torch.zeros((0, 2), dtype=torch.int64, device=dev), torch.zeros((0, 2), dtype=torch.int16, device=dev))
-    out = torch.cat(bounds), torch.cat(samples)
-    # the pinned sources stay alive until the copies that read them have run
+    a = fields.arrays()
+    n = len(a["startloc"]) - first if count is None else count
+    dev = efm.device
+    if bounds is None:
+        bounds = torch.empty((n, 2), dtype=torch.int64, device=dev)
+    if samples is None:
+        samples = torch.empty((n, 2), dtype=torch.int16, device=dev)
+    if n == 0:
+        return bounds, samples
+    sel = slice(first, first + n)
+    # the per-field inputs, read by the kernel from pinned host memory
+    h = torch.empty(n * 20, dtype=torch.uint8).pin_memory()
+    hb = h.numpy()
+    hb[:8 * n].view(np.int64)[:] = a["startloc"][sel]
+    hb[8 * n:16 * n].view(np.uint64)[:] = a["linelocs_ptr"][sel]
+    hb[16 * n:].view(np.int32)[:] = np.asarray(a["linecount"][sel], np.int32) + 1
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    L.check(lib.ldg_efm_field_slices(h.data_ptr(), h.data_ptr() + 8 * n, h.data_ptr() + 16 * n, n, efm.data_ptr(),
+                                     int(efm.numel()), bounds.data_ptr(), samples.data_ptr(), st))
+    # the pinned inputs stay alive until the kernel that reads them has run
     ev = torch.cuda.Event()
-    ev.record(stream)
-    _PINNED_IN_FLIGHT.append((ev, keep))
+    ev.record(torch.cuda.ExternalStream(st) if stream is not None else torch.cuda.current_stream(dev))
+    _PINNED_IN_FLIGHT.append((ev, h))
     while _PINNED_IN_FLIGHT and _PINNED_IN_FLIGHT[0][0].query():
         _PINNED_IN_FLIGHT.pop(0)
-    return out
+    return bounds, samples
 
 
 _PINNED_IN_FLIGHT = []

@@ -227,6 +227,7 @@ SIGNATURES = {
     "ldg_efm_pll_process_edges": (ctypes.c_int, [c_p, c_p, c_i64, c_i64, c_i64, ctypes.c_int16, ctypes.c_int16, c_p,
                                                  c_i64, ctypes.POINTER(c_i64)]),
     "ldg_efm_edges_scratch_bytes": (c_i64, [c_i64]),
+    "ldg_efm_field_slices": (ctypes.c_int, [c_p, c_p, c_p, c_i32, c_p, c_i64, c_p, c_p, c_p]),
     "ldg_efm_edges": (ctypes.c_int, [c_p, c_i64, c_i32, c_i64, c_p, c_i64, c_p, c_p, c_p]),
 }
 

@@ -437,6 +437,7 @@ class LineLocator:
         self.pal = rf.system == "PAL"
         self.stats = {"batched": 0, "host": 0, "invalid": 0, "segments": 0, "resolved": 0, "resolved_early": 0}
         self.timing = {}
+        self._rbuf, self._nruns = None, 0  # the capture's sync runs (grown in place)
         self._plans = np.empty(4096, PLAN_DTYPE)
         self._runbufs = None
         self._keep = []
@@ -717,7 +718,34 @@ class LineLocator:
             # the next scan restarts after the last complete run: what follows
             # is above the threshold or the start of a run still open at hi
             self._scan_lo = int(st[-1] + ln[-1])
-            self._runs = tuple(np.concatenate([a, b]) for a, b in zip(self._runs, (st, ln.copy(), mn.copy())))
+            self._append_runs(st, ln, mn)
+
+    def _append_runs(self, st, ln, mn):
+        """Append to the capture's run list in place (capacity doubling, so a
+        scan per chunk does not copy every earlier run again)."""
+        n0, k = self._nruns, len(st)
+        if self._rbuf is None or n0 + k > len(self._rbuf[0]):
+            cap = max(2 * (n0 + k), 4096)
+            nb = (np.empty(cap, np.int64), np.empty(cap, np.int64), np.empty(cap, np.float64))
+            if self._rbuf is not None:
+                for dst, src in zip(nb, self._rbuf):
+                    dst[:n0] = src[:n0]
+            self._rbuf = nb
+        for dst, src in zip(self._rbuf, (st, ln, mn)):
+            dst[n0:n0 + k] = src
+        self._nruns = n0 + k
+
+    @property
+    def _runs(self):
+        if self._rbuf is None:
+            return (np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0, np.float64))
+        return tuple(a[:self._nruns] for a in self._rbuf)
+
+    @_runs.setter
+    def _runs(self, runs):
+        self._rbuf, self._nruns = None, 0
+        if len(runs[0]):
+            self._append_runs(*runs)
 
     def advance(self, nblocks, stream=None, force_host=(), scan_stream=None):
         """Fields whose read windows lie within the first `nblocks` blocks

@@ -91,6 +91,12 @@ def test_pll_from_gpu_edges_of_demodulated_efm(cuda_ok):
     assert edges.tobytes() == efm_crossings(x).tobytes()
     bounds, samples = field_efm_slices(fields, efm)
     bounds, samples = bounds.cpu().numpy(), samples.cpu().numpy()
+    # into pinned host memory directly, for a range of the fields
+    hb = torch.zeros((3, 2), dtype=torch.int64).pin_memory()
+    hs = torch.zeros((3, 2), dtype=torch.int16).pin_memory()
+    field_efm_slices(fields, efm, 1, 3, bounds=hb, samples=hs)
+    torch.cuda.synchronize()
+    assert (hb.numpy() == bounds[1:4]).all() and (hs.numpy() == samples[1:4]).all()
     a, b = EFM_PLL(), EFM_PLL()
     total = 0
     for i, fl in enumerate(fields):
