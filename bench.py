@@ -91,6 +91,9 @@ def parse():
     ap.add_argument("--e2e-efm", default="edges", choices=["edges", "samples"],
                     help="end to end, the EFM output crosses to the host as its zero crossings (what the EFM PLL "
                          "consumes, with each field's slice bounds) or as the int16 samples")
+    ap.add_argument("--mixed-sub", type=int, default=8,
+                    help="after the default step, a mixed batch of this many captures in a subprocess, reported "
+                         "under mixed_batch (0: off)")
     ap.add_argument("--mixed", type=int, default=0,
                     help="mixed-batch workload instead: this many captures, lengths uniform in 0.5-8 s, "
                          "half NTSC / half PAL, own seed and SNR (30-45 dB) each")
@@ -740,7 +743,7 @@ def run_gpu(args):
         osys = "PAL" if system == "NTSC" else "NTSC"
         cmd = [sys.executable, os.path.abspath(__file__), "--system", osys, "--seconds",
                str(args.other_system_seconds), "--steps", str(args.steps), "--warmup", str(args.warmup),
-               "--no-cpu", "--no-e2e", "--other-system-seconds", "0", "--seed", str(args.seed)]
+               "--no-cpu", "--no-e2e", "--other-system-seconds", "0", "--mixed-sub", "0", "--seed", str(args.seed)]
         try:
             r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
             line = [x for x in r.stdout.splitlines() if x.startswith("{")]
@@ -754,6 +757,23 @@ def run_gpu(args):
                 other = {"system": osys, "error": (r.stderr or r.stdout)[-400:]}
         except Exception as e:  # noqa: BLE001
             other = {"system": osys, "error": str(e)[:400]}
+
+    # the mixed-batch form (many captures of both systems through the device
+    # work queue), a few captures in its own process, recorded beside the headline
+    mixed = None
+    if rank == 0 and world == 1 and args.mixed_sub > 0:
+        cmd = [sys.executable, os.path.abspath(__file__), "--mixed", str(args.mixed_sub), "--steps", "2",
+               "--warmup", "1", "--seed", str(args.seed)]
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+            line = [x for x in r.stdout.splitlines() if x.startswith("{")]
+            o = json.loads(line[-1]) if r.returncode == 0 and line else None
+            mixed = {"error": (r.stderr or r.stdout)[-400:]} if o is None else {
+                "value": o["value"], "unit": o["unit"], "ms_per_step": o["ms_per_step"],
+                "fields_per_s": o.get("fields_per_s"), "workload": o["config"].get("workload"),
+                "command": " ".join(cmd[1:])}
+        except Exception as e:  # noqa: BLE001
+            mixed = {"error": str(e)[:400]}
 
     res = {
         "metric": METRIC,
@@ -818,6 +838,7 @@ def run_gpu(args):
         "cpu_baseline": cpu,
         "accuracy": accuracy,
         "other_system": other,
+        "mixed_batch": mixed,
         # per step: demod 1, sync runs 4, refine 3 (NTSC) / 1 (PAL) per segment, TBC 2
         "gpu_launches": int(args.steps * (nchunks * (1 + 4 + 2) + segs * (3 if system == "NTSC" else 1)
                                           + audio_ranges)),

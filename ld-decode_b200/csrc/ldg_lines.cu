@@ -61,6 +61,7 @@ constexpr int kBurstLines = 266;    // compute_burst_offsets covers lines 0..265
 constexpr int kPilotLines = 323;    // refine_linelocs_pilot covers lines 0..322
 constexpr int kZc = 16;             // clb_findbursts' fixed zero-crossing slots
 constexpr int kBurstThreads = 288;  // >= kBurstLines, whole warps
+constexpr int kHsWin = 512;         // samples of a line's H-sync window in shared memory (40 MSPS needs ~480)
 
 // ---------------------------------------------------------------- sync runs
 
@@ -289,8 +290,18 @@ __device__ bool calczc(const float* x, long long n, double start_offset, double 
     return true;
 }
 
+// A line's window of a sample array staged in shared memory: x[i] from the
+// window when i lies in [base, end), else from global memory.
+struct WinView {
+    const float* g;
+    const float* s;
+    long long base, end;
+    __device__ __forceinline__ float operator[](long long i) const { return (i >= base && i < end) ? s[i - base] : g[i]; }
+};
+
 // np.median of a float32 slice (even length: float32 mean of the middle two)
-__device__ double median_f32(const float* x, long long lo, long long hi, long long n) {
+template <class X>
+__device__ double median_f32(const X& x, long long lo, long long hi, long long n) {
     lo = max(lo, 0LL);
     hi = min(hi, n);
     float v[128];
@@ -312,7 +323,8 @@ __device__ double median_f32(const float* x, long long lo, long long hi, long lo
 // Warp-cooperative forms (every lane returns the same result).
 
 // calczc with 32 samples tested per step and the first crossing by ballot
-__device__ bool warp_calczc(const float* x, long long n, double start_offset, double target, int edge, double count,
+template <class X>
+__device__ bool warp_calczc(const X& x, long long n, double start_offset, double target, int edge, double count,
                             double& out) {
     const int lane = threadIdx.x & 31;
     const long long s = (long long)start_offset;
@@ -338,7 +350,8 @@ __device__ bool warp_calczc(const float* x, long long n, double start_offset, do
     return false;
 }
 
-__device__ void warp_minmax(const float* x, long long lo, long long hi, long long n, float& mn, float& mx) {
+template <class X>
+__device__ void warp_minmax(const X& x, long long lo, long long hi, long long n, float& mn, float& mx) {
     const int lane = threadIdx.x & 31;
     lo = max(lo, 0LL);
     hi = min(hi, n);
@@ -359,7 +372,8 @@ __device__ void warp_minmax(const float* x, long long lo, long long hi, long lon
 // (bitonic network over elements e = lane and e = lane + 32, unused ones
 // +inf) and reads the middle one or two; longer slices fall back to one
 // lane.  The middle values do not depend on how ties are ordered.
-__device__ double warp_median_f32(const float* x, long long lo, long long hi, long long n) {
+template <class X>
+__device__ double warp_median_f32(const X& x, long long lo, long long hi, long long n) {
     const int lane = threadIdx.x & 31;
     lo = max(lo, 0LL);
     hi = min(hi, n);
@@ -677,9 +691,13 @@ __global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P)
         bad[i] = a.linebad1[(long long)f * kMaxL + i];
     }
     __syncthreads();
-    // refine_linelocs_hsync: one warp per line
+    // refine_linelocs_hsync: one warp per line; each line's samples (from just
+    // before its search start to past its porch) staged in shared memory by
+    // one burst of independent loads, so the searches below do not wait on
+    // one global load after another
     {
         const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+        __shared__ float win[kLineThreads / 32][kHsWin];
         for (int li = threadIdx.x >> 5; li < nl; li += nwarps) {
             bool b = bad[li];
             double v2 = ll1[li];
@@ -687,20 +705,27 @@ __global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P)
                 b = true;
             } else {
                 const double l1 = ll1[li] - P.freq;
+                const long long wb = max((long long)l1 - 64, 0LL);
+                const long long we = min(wb + kHsWin, n);
+                float* w = win[threadIdx.x >> 5];
+                __syncwarp();
+                for (long long i = wb + lane; i < we; i += 32) w[i - wb] = d05[i];
+                __syncwarp();
+                const WinView x{d05, w, wb, we};
                 double zc;
-                if (warp_calczc(d05, n, l1, P.half_sync, 0, P.freq * 2, zc) && !b) {
+                if (warp_calczc(x, n, l1, P.half_sync, 0, P.freq * 2, zc) && !b) {
                     v2 = zc;
                     float mn, mx;
-                    warp_minmax(d05, (long long)(zc - (P.freq * 0.75)), (long long)(zc + (P.freq * 8)), n, mn, mx);
+                    warp_minmax(x, (long long)(zc - (P.freq * 0.75)), (long long)(zc + (P.freq * 8)), n, mn, mx);
                     if ((double)mn < P.lo_ok || (double)mx > P.hi_ok) {
                         b = true;
                     } else {
                         const double porch =
-                            warp_median_f32(d05, (long long)(zc + (P.freq * 8)), (long long)(zc + (P.freq * 9)), n);
+                            warp_median_f32(x, (long long)(zc + (P.freq * 8)), (long long)(zc + (P.freq * 9)), n);
                         const double sync =
-                            warp_median_f32(d05, (long long)(zc + (P.freq * 1)), (long long)(zc + (P.freq * 2.5)), n);
+                            warp_median_f32(x, (long long)(zc + (P.freq * 1)), (long long)(zc + (P.freq * 2.5)), n);
                         double zc2;
-                        if (warp_calczc(d05, n, l1, (porch + sync) / 2, 0, 400, zc2) && fabs(zc2 - zc) < (P.freq / 2))
+                        if (warp_calczc(x, n, l1, (porch + sync) / 2, 0, 400, zc2) && fabs(zc2 - zc) < (P.freq / 2))
                             v2 = zc2;
                         else
                             b = true;
