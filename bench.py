@@ -260,7 +260,10 @@ def run_gpu(args):
     streamB = torch.cuda.Stream(priority=-1)   # line locations
     streamC = torch.cuda.Stream(priority=-1)   # TBC of ranges whose line locations are final
     streamS = torch.cuda.Stream(priority=-1)   # sync-run scans
-    streamA = torch.cuda.Stream()              # analog audio of finished ranges (after their TBC, no hurry)
+    # analog audio of finished ranges: high priority too, since the range's
+    # copies out wait for it and the buffer set's next demod waits for those
+    streamA = torch.cuda.Stream(priority=-1)
+    streamE = torch.cuda.Stream()              # EFM zero crossings of each demodulated chunk (end to end)
     do_audio = not args.no_analog_audio
     elem = {k: v.element_size() for k, v in outs.items()}
     per_block = {k: (991 if k.startswith("audio") else U) for k in outs}
@@ -350,6 +353,19 @@ def run_gpu(args):
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(stream)
             evs.append(ev)
+            if io is not None and edges_mode:
+                # the chunk's EFM zero crossings (stream E, beside the next
+                # chunk's demod and off the line-location streams); the count
+                # lands in pinned memory and is read when the copy is issued
+                streamE.wait_event(ev)
+                base = bounds[c] * U
+                L.check(lib.ldg_efm_edges(bs.outs["efm"].data_ptr() + 2 * base, (bounds[c + 1] - bounds[c]) * U,
+                                          1 if c else 0, base, bs.edges.data_ptr() + 8 * int(eoff[c]),
+                                          int(ecap[c]), io["ecount"].data_ptr() + 8 * c, bs.escratch.data_ptr(),
+                                          streamE.cuda_stream))
+                eev = torch.cuda.Event()
+                eev.record(streamE)
+                bs.eevs[c] = eev
             if io is not None and not edges_mode:
                 streamD.wait_event(ev)
                 o0, o1 = bounds[c] * U, bounds[c + 1] * U
@@ -364,31 +380,32 @@ def run_gpu(args):
         chunk, TBC and audio of each finished range, the copies out."""
         loc = bs.loc
         loc.begin(bs.farr)
+        pend_e = list(range(nchunks)) if io is not None and edges_mode else []
+
+        def edges_out(block):
+            # each chunk's crossings to the host once its count is known (in
+            # chunk order; without blocking until the step's end)
+            while pend_e:
+                c_ = pend_e[0]
+                eev = bs.eevs[c_]
+                if not block and not eev.query():
+                    return
+                eev.synchronize()
+                k = int(io["ecount"][c_])
+                if k > ecap[c_]:
+                    raise RuntimeError(f"chunk {c_}: {k} EFM crossings, room for {int(ecap[c_])}")
+                io["ecounts"][c_] = k
+                streamD.wait_event(eev)
+                e0_, e1_ = 8 * int(eoff[c_]), 8 * (int(eoff[c_]) + k)
+                with torch.cuda.stream(streamD):
+                    io["edges"][e0_:e1_].copy_(bs.edges[e0_:e1_], non_blocking=True)
+                pend_e.pop(0)
+
         for c in range(nchunks):
             streamB.wait_event(evs[c])
             streamS.wait_event(evs[c])
-            eev = None
-            if io is not None and edges_mode:
-                # the chunk's EFM zero crossings (stream S, before its sync-run scan,
-                # whose stream synchronisation then makes the count readable)
-                base = bounds[c] * U
-                L.check(lib.ldg_efm_edges(bs.outs["efm"].data_ptr() + 2 * base, (bounds[c + 1] - bounds[c]) * U,
-                                          1 if c else 0, base, bs.edges.data_ptr() + 8 * int(eoff[c]),
-                                          int(ecap[c]), io["ecount"].data_ptr() + 8 * c, bs.escratch.data_ptr(),
-                                          streamS.cuda_stream))
-                eev = torch.cuda.Event()
-                eev.record(streamS)
             loc.advance(bounds[c + 1], stream=streamB, scan_stream=streamS)
-            if eev is not None:
-                eev.synchronize()
-                k = int(io["ecount"][c])
-                if k > ecap[c]:
-                    raise RuntimeError(f"chunk {c}: {k} EFM crossings, room for {int(ecap[c])}")
-                io["ecounts"][c] = k
-                streamD.wait_event(eev)
-                e0_, e1_ = 8 * int(eoff[c]), 8 * (int(eoff[c]) + k)
-                with torch.cuda.stream(streamD):
-                    io["edges"][e0_:e1_].copy_(bs.edges[e0_:e1_], non_blocking=True)
+            edges_out(False)
             # TBC of each range of fields as its line locations become final
             # (stream C: overlaps the NTSC burst chain's next range and the demod)
             while loc.ready and bs.pics is not None:
@@ -398,7 +415,7 @@ def run_gpu(args):
                                          first=lo, count=hi - lo, **wow_opts),
                            stream=streamC.cuda_stream, asynchronous=True)
                 if do_audio:
-                    # the same fields' analog audio, 16-bit 44.1 kHz (one launch, default priority)
+                    # the same fields' analog audio, 16-bit 44.1 kHz (one launch)
                     streamA.wait_event(ev)
                     downscale_audio_located(rf, loc.fields, bs.outs["audio_left"], bs.outs["audio_right"], 44100,
                                             stream=streamA.cuda_stream, first=lo, count=hi - lo, out=bs.aud,
@@ -418,17 +435,20 @@ def run_gpu(args):
                         io["pics"][lo * fsz:hi * fsz].copy_(bs.pics[lo * fsz:hi * fsz], non_blocking=True)
                         if do_audio:
                             io["aud"][lo * AS:hi * AS].copy_(bs.aud[lo * AS:hi * AS], non_blocking=True)
-                        if edges_mode:
-                            # each field's EFM slice for the PLL (its bounds and end
-                            # samples), written by the kernel straight into pinned memory
-                            field_efm_slices(loc.fields, bs.outs["efm"], lo, hi - lo, bounds=io["ebounds"][lo:hi],
-                                             samples=io["esamples"][lo:hi])
+                    if edges_mode:
+                        # each field's EFM slice for the PLL (its bounds and end samples),
+                        # written by the kernel straight into pinned memory; on the TBC's
+                        # high-priority stream, not among the copies, where it would wait
+                        # for SMs behind the next chunk's demod and hold up the copies
+                        field_efm_slices(loc.fields, bs.outs["efm"], lo, hi - lo, bounds=io["ebounds"][lo:hi],
+                                         samples=io["esamples"][lo:hi], stream=streamC.cuda_stream)
+        edges_out(True)
         end = torch.cuda.Event(enable_timing=True)
         if overlap:
             # the next step (on the other buffer set) starts its demod while
             # this step's line locations, TBC and copies finish
             bs.done = []
-            for st_ in ([streamB, streamC, streamS, streamA] + ([streamD, streamP] if io is not None else [])):
+            for st_ in ([streamB, streamC, streamS, streamA] + ([streamD, streamP, streamE] if io is not None else [])):
                 e = torch.cuda.Event()
                 e.record(st_)
                 bs.done.append(e)
@@ -457,6 +477,7 @@ def run_gpu(args):
     alt.aud = torch.zeros(nf * AS, dtype=torch.int16, device="cuda")
     for bs_ in (main, alt):
         bs_.edges = torch.empty(8 * int(ecap.sum()) if edges_mode else 8, dtype=torch.uint8, device="cuda")
+        bs_.eevs = [None] * nchunks
         bs_.escratch = torch.empty(max(int(L.load().ldg_efm_edges_scratch_bytes((bounds[c + 1] - bounds[c]) * U))
                                        for c in range(nchunks)), dtype=torch.uint8, device="cuda")
 
@@ -840,7 +861,7 @@ def run_gpu(args):
         "other_system": other,
         "mixed_batch": mixed,
         # per step: demod 1, sync runs 4, refine 3 (NTSC) / 1 (PAL) per segment, TBC 2
-        "gpu_launches": int(args.steps * (nchunks * (1 + 4 + 2) + segs * (3 if system == "NTSC" else 1)
+        "gpu_launches": int(args.steps * (nchunks * (1 + 2 + 2) + segs * (3 if system == "NTSC" else 1)
                                           + audio_ranges)),
         "clocks": clocks,
     }

@@ -20,6 +20,7 @@
 #include "ldg_dropouts.cuh"
 #include "ldg_fft.cuh"
 #include "ldg_noalloc.h"
+#include "ldg_scan.cuh"
 #include "ldg_audio.cuh"
 #include "ldg_tbc.cuh"
 #include "ldgpu.h"
@@ -128,6 +129,12 @@ struct ldg_ctx {
     cudaEvent_t a2_done = nullptr;
     bool a2_used = false;
     long long* h_word = nullptr;         // pinned, mapped: results the host reads right after a kernel
+    // ldg_sync_runs' single-pass scan: [0] ticket counter, then flags, counts
+    // and prefixes of scan_cap tiles; scan_base = tickets handed out so far
+    unsigned long long* d_scan = nullptr;
+    long long scan_cap = 0;
+    unsigned long long scan_base = 0, scan_call = 0;
+    bool scan_dirty = false;
     ldg::RfTbcField* d_rftbc = nullptr;  // ldg_rf_tbc descriptors, same reuse rule
     size_t rftbc_cap = 0;
     cudaEvent_t rftbc_done = nullptr;
@@ -335,6 +342,7 @@ void ldg_ctx_destroy(ldg_ctx* c) {
     if (c->drop_used) cudaEventSynchronize(c->drop_done);
     if (c->rftbc_used) cudaEventSynchronize(c->rftbc_done);
     if (c->h_word) cudaFreeHost(c->h_word);
+    cudaFree(c->d_scan);
     if (c->a2_used) cudaEventSynchronize(c->a2_done);
     cudaFree(c->d_a2);
     if (c->a2_done) cudaEventDestroy(c->a2_done);
@@ -1064,6 +1072,34 @@ int ctx_host_word(ldg_ctx* c, long long** host, long long** dev) {
     *dev = static_cast<long long*>(d);
     return LDG_OK;
 }
+
+int ctx_scan_state(ldg_ctx* c, long long ntiles, cudaStream_t st, ScanState* out) {
+    if (!c->d_scan || ntiles > c->scan_cap || c->scan_dirty) {
+        // a fresh state: tickets from 0, flags 0 (call numbers start at 1,
+        // so no flag of a new call matches them)
+        const long long cap = std::max<long long>(ntiles + ntiles / 4, 4096);
+        if (c->d_scan) cudaFree(c->d_scan);
+        c->d_scan = nullptr;
+        c->scan_cap = 0;
+        void* p = nullptr;
+        LDG_CK(cudaMalloc(&p, (size_t)(1 + 3 * cap) * sizeof(unsigned long long)));
+        c->d_scan = static_cast<unsigned long long*>(p);
+        LDG_CK(cudaMemsetAsync(p, 0, (size_t)(1 + 3 * cap) * sizeof(unsigned long long), st));
+        c->scan_cap = cap;
+        c->scan_base = 0;
+        c->scan_dirty = false;
+    }
+    out->ticket = c->d_scan;
+    out->flags = c->d_scan + 1;
+    out->agg = reinterpret_cast<long long*>(c->d_scan + 1 + c->scan_cap);
+    out->incl = out->agg + c->scan_cap;
+    out->base = c->scan_base;
+    out->call = ++c->scan_call;
+    c->scan_base += (unsigned long long)ntiles;
+    return LDG_OK;
+}
+
+void ctx_scan_invalidate(ldg_ctx* c) { c->scan_dirty = true; }
 
 int ctx_lines_scratch(ldg_ctx* c, size_t need, void** out) {
     int rc = grow(&c->d_lines, &c->lines_cap, need);

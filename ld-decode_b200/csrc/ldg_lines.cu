@@ -4,10 +4,10 @@
 // whole capture-wide output array -- the pulses findpulses
 // (lddecode/utils.py:1101-1157) finds, for every field read window at once --
 // and the mean level inside the long ones (getpulses' VSYNC level check,
-// core.py:2242-2322).  Edges counted per tile (which also leaves a bitmap of
-// the below-threshold flags), an exclusive scan of the tile counts, edges
-// written in order from the bitmap; then one warp per run pairs its edges
-// and averages its interior.
+// core.py:2242-2322).  Two launches: the edges of every tile counted,
+// scanned (decoupled look-back) and written in order by one single-pass
+// kernel; then the runs paired and the long runs' interiors averaged, the
+// results written straight into the caller's pinned buffers.
 //
 // ldg_lines_refine: the per-line refinement of Field.process() for all
 // fields of a capture (pulse-level line locations from the host chain):
@@ -39,6 +39,7 @@
 #include <string>
 
 #include "ldg_copy.cuh"
+#include "ldg_scan.cuh"
 #include "ldgpu.h"
 
 struct ldg_ctx;
@@ -54,7 +55,7 @@ int ctx_host_word(ldg_ctx* c, long long** host, long long** dev);
 namespace {
 
 constexpr int kMaxL = LDG_CHAIN_MAX_LINES;
-constexpr int kEdgeTile = 8192;
+constexpr int kEdgeTile = 16384;  // samples per sync-run scan tile
 constexpr int kEdgeThreads = 256;
 constexpr int kLineThreads = 352;   // >= proclines (326 PAL)
 constexpr int kBurstLines = 266;    // compute_burst_offsets covers lines 0..265
@@ -67,8 +68,8 @@ constexpr int kHsWin = 512;         // samples of a line's H-sync window in shar
 
 __device__ __forceinline__ bool below(const float* x, long long i, double thr) { return (double)x[i] <= thr; }
 
-// the below-threshold flags of samples base-1 .. base+3 (4 per thread per
-// step; a float4 load when the array is 16-byte aligned)
+// the below-threshold flags of samples base .. base+3 (bit k: sample
+// base+k; none at or past n); a float4 load when the array is 16-byte aligned
 __device__ __forceinline__ unsigned four_flags(const float* __restrict__ x, long long n, long long base, double thr,
                                                bool aligned) {
     float v[4];
@@ -82,179 +83,204 @@ __device__ __forceinline__ unsigned four_flags(const float* __restrict__ x, long
 #pragma unroll
         for (int k = 0; k < 4; ++k) v[k] = base + k < n ? x[base + k] : 0.0f;
     }
-    const bool prev = base > 0 && base - 1 < n ? below(x, base - 1, thr) : false;
-    unsigned b = prev ? 1u : 0u;  // bit 0: sample base-1; bit k+1: sample base+k
+    unsigned b = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-        if (base + k < n && (double)v[k] <= thr) b |= 2u << k;
+        if (base + k < n && (double)v[k] <= thr) b |= 1u << k;
     return b;
 }
 
-// edge bits of a thread's 4 samples (bit k: sample base+k starts or ends a run)
-__device__ __forceinline__ unsigned edge_bits(unsigned b, long long base, long long n) {
-    unsigned e = (b ^ (b >> 1)) & 0xfu;
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-        if (base + k >= n) e &= ~(1u << k);
-    return e;
-}
+// look-back states of a tile (low two bits of its flag word; the high bits
+// hold the call's number, so words of earlier calls never match)
+constexpr unsigned long long kTileAgg = 1, kTileIncl = 2;
+constexpr int kLookbackSpins = 1 << 20;  // ~0.1-1 s of polling; then the call fails
+constexpr int kEdgeSteps = kEdgeTile / (4 * kEdgeThreads);  // coalesced float4 steps per thread
+constexpr int kEdgeWords = kEdgeTile / 32;                  // flag words of a tile
+constexpr int kWordsPerThread = kEdgeWords / kEdgeThreads;
+static_assert(kWordsPerThread == 2, "a thread owns two consecutive flag words");
 
-constexpr int kEdgeSteps = kEdgeTile / (4 * kEdgeThreads);
-
-// Edges per tile, and the below-threshold flags of every sample as a bitmap
-// (bit i % 32 of word i / 32), so the write pass reads 1 bit per sample
-// instead of the float array again.
-__global__ void __launch_bounds__(kEdgeThreads) edge_count_kernel(const float* __restrict__ x, long long n,
-                                                                   double thr, int* __restrict__ counts,
-                                                                   unsigned* __restrict__ bm) {
-    const long long t0 = (long long)blockIdx.x * kEdgeTile;
+// Sync-run edges in one pass (single-pass scan with decoupled look-back).
+// Each CTA takes the next tile by ticket (so every tile it waits on belongs
+// to a CTA that is already running); reads its samples with coalesced
+// float4 loads into a shared bitmap of below-threshold flags (bit b of word
+// w: sample 32 w + b); each thread then owns two consecutive words (64
+// samples), whose edges -- samples whose flag differs from the sample
+// before -- it counts; one CTA-wide scan of the counts; the tile's total
+// goes to the look-back (warp 0: publish the tile's count, add the counts
+// or the inclusive prefix of the tiles before it 32 at a time, publish its
+// own inclusive prefix); every thread writes its edges as 2*i + (run start ?
+// 1 : 0) in increasing i.  The last tile writes the total.  Each sample is
+// read once, and the scan costs one launch instead of three (count, scan of
+// the tile counts, write), which matters when it runs beside the
+// demodulator and each launch waits for SMs to come free.  A wait that
+// outlasts kLookbackSpins sets *err (host-mapped) and takes the missing
+// count as 0.
+__global__ void __launch_bounds__(kEdgeThreads) edge_pass_kernel(
+    const float* __restrict__ x, long long n, double thr, unsigned long long* ticket, unsigned long long base,
+    unsigned long long call, unsigned long long* flags, long long* agg, long long* incl, long long ntiles,
+    long long* __restrict__ edges, long long cap, long long* __restrict__ total, long long* err) {
+    __shared__ unsigned bm[kEdgeWords];
+    __shared__ long long s_tile, s_excl;
+    __shared__ int warp_tot[kEdgeThreads / 32];
+    __shared__ unsigned s_before;  // flag of the sample before the tile
+    if (threadIdx.x == 0) s_tile = (long long)(atomicAdd(ticket, 1ull) - base);
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile < 0 || tile >= ntiles) return;  // more CTAs than tiles: never launched so
+    const long long t0 = tile * kEdgeTile;
     const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
-    const int lane = threadIdx.x & 31;
-    int c = 0;
-#pragma unroll 2
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_before = t0 > 0 && t0 - 1 < n && below(x, t0 - 1, thr) ? 1u : 0u;
+#pragma unroll 4
     for (int j = 0; j < kEdgeSteps; ++j) {
-        const long long base = t0 + (long long)j * 4 * kEdgeThreads + 4 * threadIdx.x;
-        unsigned b = 0;
-        if (base < n) {
-            b = four_flags(x, n, base, thr, aligned);
-            c += __popc(edge_bits(b, base, n));
-        }
-        // eight lanes' four flags make one word (base % 32 == 4 * (lane % 8))
-        unsigned v = ((b >> 1) & 0xfu) << (4 * (lane & 7));
+        const long long b0 = t0 + (long long)j * 4 * kEdgeThreads + 4 * threadIdx.x;
+        unsigned f = 0;  // flags of samples b0 .. b0+3 (none past n)
+        if (b0 < n) f = four_flags(x, n, b0, thr, aligned);
+        // eight lanes' four flags make one word (b0 % 32 == 4 * (lane % 8))
+        unsigned v = f << (4 * (lane & 7));
         v |= __shfl_xor_sync(0xffffffffu, v, 1);
         v |= __shfl_xor_sync(0xffffffffu, v, 2);
         v |= __shfl_xor_sync(0xffffffffu, v, 4);
-        if ((lane & 7) == 0) bm[base >> 5] = v;
+        if ((lane & 7) == 0) bm[j * (kEdgeThreads / 8) + (threadIdx.x >> 3)] = v;
     }
-    __shared__ int warp_sum[kEdgeThreads / 32];
-    int v = c;
-    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = v;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int sum = 0;
-        for (int w = 0; w < kEdgeThreads / 32; ++w) sum += warp_sum[w];
-        counts[blockIdx.x] = sum;
+    // this thread's 64 samples: words 2t and 2t+1, and the flag before them
+    const int w0 = kWordsPerThread * threadIdx.x;
+    const unsigned f0 = bm[w0], f1 = bm[w0 + 1];
+    const unsigned pb = w0 ? bm[w0 - 1] >> 31 : s_before;
+    const long long s0 = t0 + 32LL * w0;  // first sample of word w0
+    unsigned e0 = f0 ^ ((f0 << 1) | pb);
+    unsigned e1 = f1 ^ ((f1 << 1) | (f0 >> 31));
+    // no edges at or past n (flags there are 0, so a run open at n has no end edge)
+    if (s0 + 64 > n) {
+        const long long k0 = n - s0, k1 = n - s0 - 32;
+        e0 &= k0 <= 0 ? 0u : k0 >= 32 ? 0xffffffffu : (1u << k0) - 1u;
+        e1 &= k1 <= 0 ? 0u : k1 >= 32 ? 0xffffffffu : (1u << k1) - 1u;
     }
-}
-
-// exclusive scan of the tile counts (one CTA; ntiles is ~n / 8192)
-__global__ void __launch_bounds__(1024) edge_scan_kernel(const int* __restrict__ counts, long long ntiles,
-                                                         long long* __restrict__ offsets,
-                                                         long long* __restrict__ total) {
-    __shared__ long long part[1024];
-    __shared__ long long carry;
-    if (threadIdx.x == 0) carry = 0;
+    const int cnt = __popc(e0) + __popc(e1);
+    // CTA-wide exclusive scan of the counts
+    int inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) warp_tot[warp] = inc;
     __syncthreads();
-    for (long long base = 0; base < ntiles; base += 1024) {
-        const long long i = base + threadIdx.x;
-        const long long v = i < ntiles ? counts[i] : 0;
-        part[threadIdx.x] = v;
-        __syncthreads();
-        for (int o = 1; o < 1024; o <<= 1) {
-            const long long add = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
-            __syncthreads();
-            part[threadIdx.x] += add;
-            __syncthreads();
-        }
-        if (i < ntiles) offsets[i] = carry + part[threadIdx.x] - v;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry += part[1023];
-        __syncthreads();
+    int before = 0, tile_count = 0;
+#pragma unroll
+    for (int w = 0; w < kEdgeThreads / 32; ++w) {
+        before += w < warp ? warp_tot[w] : 0;
+        tile_count += warp_tot[w];
     }
-    if (threadIdx.x == 0) *total = carry;
-}
-
-// edges as 2*i + (run start ? 1 : 0), in increasing i
-__global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const unsigned* __restrict__ bm, long long n,
-                                                                   const long long* __restrict__ offsets,
-                                                                   long long* __restrict__ edges, long long cap) {
-    __shared__ int warp_cnt[kEdgeThreads / 32];
-    const long long t0 = (long long)blockIdx.x * kEdgeTile;
-    long long out = offsets[blockIdx.x];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int j = 0; j < kEdgeSteps; ++j) {
-        const long long base = t0 + (long long)j * 4 * kEdgeThreads + 4 * threadIdx.x;
-        unsigned b = 0, e = 0;
-        if (base < n) {
-            // the flags of samples base-1 .. base+3 from the count pass's bitmap
-            const unsigned w = bm[base >> 5];
-            const int sh = (int)(base & 31);
-            const unsigned prevb = sh ? (w >> (sh - 1)) & 1u : (base > 0 ? bm[(base >> 5) - 1] >> 31 : 0u);
-            b = prevb | (((w >> sh) & 0xfu) << 1);
-            e = edge_bits(b, base, n);
-        }
-        const int cnt = __popc(e);
-        // inclusive warp scan of the per-thread counts
-        int inc = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        if (lane == 31) warp_cnt[warp] = inc;
-        __syncthreads();
-        int before = 0, chunk = 0;
-#pragma unroll
-        for (int w = 0; w < kEdgeThreads / 32; ++w) {
-            before += w < warp ? warp_cnt[w] : 0;
-            chunk += warp_cnt[w];
-        }
-        long long k = out + before + inc - cnt;
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (e & (1u << q)) {
-                if (k < cap) edges[k] = 2 * (base + q) + ((b >> (q + 1)) & 1u);
-                ++k;
+    if (warp == 0) {
+        volatile unsigned long long* vf = flags;
+        volatile long long* va = agg;
+        volatile long long* vi = incl;
+        const long long count = tile_count;
+        long long excl = 0;
+        if (tile > 0) {
+            if (lane == 0) {
+                va[tile] = count;
+                __threadfence();
+                vf[tile] = (call << 2) | kTileAgg;
             }
-        out += chunk;
-        __syncthreads();
-    }
-}
-
-// one warp per run: pair edges 2r (start) and 2r+1 (end), interior mean of long
-// runs; the run count is total / 2 (an odd total leaves a run open at the
-// end), read on the device, runs beyond `cap` are not written
-__global__ void run_pair_kernel(const long long* __restrict__ edges, const long long* __restrict__ total,
-                                long long cap, const float* __restrict__ x, long long min_long, long long trim_lo,
-                                long long trim_hi, long long* __restrict__ rs, long long* __restrict__ rl,
-                                double* __restrict__ rm) {
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    const long long nruns = min(*total / 2, cap);
-    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nruns; r += nwarps) {
-        const long long s = edges[2 * r] >> 1, e = edges[2 * r + 1] >> 1;
-        const long long len = e - s;
-        double mean = nan("");
-        if (len > min_long) {
-            const long long lo = s + trim_lo, hi = s + len - trim_hi;
-            double acc = 0;
-            for (long long i = lo + lane; i < hi; i += 32) acc += (double)x[i];
-            for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (hi > lo) mean = acc / (double)(hi - lo);
+            // the warp looks back 32 tiles at a time (lane l: tile p - l) and
+            // stops at the nearest one whose inclusive prefix is out; tiles
+            // before 0 count as an inclusive prefix of 0
+            bool timed_out = false;
+            for (long long p = tile - 1;; p -= 32) {
+                const long long q = p - lane;
+                unsigned long long f = (call << 2) | kTileIncl;
+                if (q >= 0) {
+                    f = vf[q];
+                    for (int spins = 0; (f >> 2) != call && spins < kLookbackSpins; ++spins) {
+                        __nanosleep(64);
+                        f = vf[q];
+                    }
+                }
+                if (__any_sync(0xffffffffu, (f >> 2) != call)) {
+                    timed_out = true;
+                    break;
+                }
+                __threadfence();
+                const unsigned inc_mask = __ballot_sync(0xffffffffu, (f & 3ull) == kTileIncl);
+                const int stop = inc_mask ? __ffs(inc_mask) - 1 : 32;
+                long long v = 0;
+                if (lane < stop && q >= 0) v = va[q];
+                if (lane == stop && q >= 0) v = vi[q];
+#pragma unroll
+                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                excl += v;
+                if (inc_mask) break;
+            }
+            if (timed_out && lane == 0) *reinterpret_cast<volatile long long*>(err) = 1;
         }
         if (lane == 0) {
+            vi[tile] = excl + count;
+            __threadfence();
+            vf[tile] = (call << 2) | kTileIncl;
+            if (tile == ntiles - 1) *total = excl + count;
+            s_excl = excl;
+        }
+    }
+    __syncthreads();
+    long long k = s_excl + before + inc - cnt;
+    for (unsigned e = e0; e; e &= e - 1) {
+        const int b = __ffs(e) - 1;
+        if (k < cap) edges[k] = 2 * (s0 + b) + ((f0 >> b) & 1u);
+        ++k;
+    }
+    for (unsigned e = e1; e; e &= e - 1) {
+        const int b = __ffs(e) - 1;
+        if (k < cap) edges[k] = 2 * (s0 + 32 + b) + ((f1 >> b) & 1u);
+        ++k;
+    }
+}
+
+// Pair edges 2r (start) and 2r+1 (end) into runs, with the interior mean of
+// long runs; the run count is total / 2 (an odd total leaves a run open at
+// the end), read on the device, and runs beyond `cap` are not written.  A
+// warp takes 32 consecutive runs, one per lane, so the outputs -- host-mapped
+// pinned memory, read by the host after a stream synchronisation without a
+// copy-engine transfer -- are written coalesced; the warp then averages its
+// long runs one at a time.  Block 0 writes the edge count to *count_out.
+__global__ void run_pair_kernel(const long long* __restrict__ edges, const long long* __restrict__ total,
+                                long long cap, const float* __restrict__ x, long long min_long, long long trim_lo,
+                                long long trim_hi, long long* rs, long long* rl, double* rm, long long* count_out) {
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long tot = *total;
+    const long long nruns = min(tot / 2, cap);
+    for (long long r0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; r0 < nruns;
+         r0 += nwarps * 32) {
+        const long long r = r0 + lane;
+        const bool valid = r < nruns;
+        long long s = 0, len = 0;
+        if (valid) {
+            s = edges[2 * r] >> 1;
+            len = (edges[2 * r + 1] >> 1) - s;
+        }
+        double mean = nan("");
+        unsigned longs = __ballot_sync(0xffffffffu, valid && len > min_long);
+        while (longs) {
+            const int l = __ffs(longs) - 1;
+            longs &= longs - 1;
+            const long long ls = __shfl_sync(0xffffffffu, s, l), ll = __shfl_sync(0xffffffffu, len, l);
+            const long long lo = ls + trim_lo, hi = ls + ll - trim_hi;
+            double acc = 0;
+            for (long long i = lo + lane; i < hi; i += 32) acc += (double)x[i];
+#pragma unroll
+            for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == l && hi > lo) mean = acc / (double)(hi - lo);
+        }
+        if (valid) {
             rs[r] = s;
             rl[r] = len;
             rm[r] = mean;
         }
     }
-}
-
-// Runs and the edge count straight into host-mapped pinned memory (coalesced
-// over PCIe), so the host reads them after a stream synchronisation without
-// a copy-engine transfer.
-__global__ void export_runs_kernel(const long long* __restrict__ total, long long cap, const long long* __restrict__ rs,
-                                   const long long* __restrict__ rl, const double* __restrict__ rm,
-                                   long long* ors, long long* orl, double* orm, long long* count) {
-    const long long nruns = min(*total / 2, cap);
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nruns; i += stride) {
-        ors[i] = rs[i];
-        orl[i] = rl[i];
-        orm[i] = rm[i];
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) *count = *total;
+    if (count_out && blockIdx.x == 0 && threadIdx.x == 0) *count_out = tot;
 }
 
 // --------------------------------------------------------- per-line helpers
@@ -1285,11 +1311,9 @@ int ldg_sync_runs(ldg_ctx* c, const float* d05, int64_t n, double threshold, int
     cudaStream_t st = (cudaStream_t)stream;
     const long long ntiles = (n + kEdgeTile - 1) / kEdgeTile;
     const long long ecap = 2 * cap + 2;
-    const size_t b_counts = align256(ntiles * sizeof(int)), b_off = align256(ntiles * sizeof(long long));
     const size_t b_tot = 256, b_edges = align256(ecap * sizeof(long long));
     const size_t b_runs = align256(cap * sizeof(long long));
-    const size_t b_bm = align256((size_t)ntiles * (kEdgeTile / 32) * sizeof(unsigned));
-    const size_t need = b_counts + b_off + b_tot + b_edges + 2 * b_runs + align256(cap * sizeof(double)) + b_bm;
+    const size_t need = b_tot + b_edges + 2 * b_runs + align256(cap * sizeof(double));
     void* scratch = nullptr;
     auto done = [&](int rc) {
         if (prev >= 0) cudaSetDevice(prev);
@@ -1297,53 +1321,54 @@ int ldg_sync_runs(ldg_ctx* c, const float* d05, int64_t n, double threshold, int
     };
     if (ldg::ctx_lines_scratch(c, need, &scratch) != LDG_OK) return done(LDG_ERR_CUDA);
     char* p = static_cast<char*>(scratch);
-    int* counts = reinterpret_cast<int*>(p);
-    long long* offsets = reinterpret_cast<long long*>(p + b_counts);
-    long long* total = reinterpret_cast<long long*>(p + b_counts + b_off);
-    long long* edges = reinterpret_cast<long long*>(p + b_counts + b_off + b_tot);
-    long long* rs = reinterpret_cast<long long*>(p + b_counts + b_off + b_tot + b_edges);
+    long long* total = reinterpret_cast<long long*>(p);
+    long long* edges = reinterpret_cast<long long*>(p + b_tot);
+    long long* rs = reinterpret_cast<long long*>(p + b_tot + b_edges);
     long long* rl = rs + b_runs / sizeof(long long);
     double* rm = reinterpret_cast<double*>(rl + b_runs / sizeof(long long));
-    unsigned* bm = reinterpret_cast<unsigned*>(p + b_counts + b_off + b_tot + b_edges + 2 * b_runs +
-                                               align256(cap * sizeof(double)));
     auto cuda_fail = [&](const char* what) {
+        ldg::ctx_scan_invalidate(c);
         return done(ldg::lines_fail(LDG_ERR_CUDA, std::string("ldg_sync_runs: ") + what + ": " +
                                                       cudaGetErrorString(cudaGetLastError())));
     };
-    // count, scan, write and pair back to back; the host learns the count once
-    edge_count_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, counts, bm);
-    edge_scan_kernel<<<1, 1024, 0, st>>>(counts, ntiles, offsets, total);
-    edge_write_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(bm, n, offsets, edges, ecap);
-    run_pair_kernel<<<4 * 148, 256, 0, st>>>(edges, total, cap, d05, min_long, trim_lo, trim_hi, rs, rl, rm);
-    // pinned (mapped) outputs: the runs and the count are written by a kernel
-    // and the host waits for the stream only (no copy-engine transfer, which
-    // would queue behind bulk copies of an end-to-end pipeline)
+    // the look-back state (tickets, per-tile flags and counts) and the
+    // host-mapped words: [0] the edge count, [1] the look-back error flag
+    ldg::ScanState ss;
     long long *hw = nullptr, *dw = nullptr;
+    if (ldg::ctx_scan_state(c, ntiles, st, &ss) != LDG_OK || ldg::ctx_host_word(c, &hw, &dw) != LDG_OK)
+        return cuda_fail("scan state");
+    volatile long long* vhw = hw;
+    vhw[0] = -1;
+    vhw[1] = 0;
+    edge_pass_kernel<<<(unsigned)ntiles, kEdgeThreads, 0, st>>>(d05, n, threshold, ss.ticket, ss.base, ss.call,
+                                                                ss.flags, ss.agg, ss.incl, ntiles, edges, ecap,
+                                                                total, dw + 1);
+    // runs straight into the caller's pinned (mapped) buffers when they are:
+    // the host then waits for the stream only (no copy-engine transfer, which
+    // would queue behind bulk copies of an end-to-end pipeline)
     void* drs = ldg::device_view(run_start);
     void* drl = ldg::device_view(run_len);
     void* drm = ldg::device_view(run_mean);
-    if (drs && drl && drm && ldg::ctx_host_word(c, &hw, &dw) == LDG_OK) {
-        *hw = -1;
-        export_runs_kernel<<<2 * 148, 256, 0, st>>>(total, cap, rs, rl, rm, static_cast<long long*>(drs),
-                                                    static_cast<long long*>(drl), static_cast<double*>(drm), dw);
-        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
-            return cuda_fail("run export");
-        const long long nedges = *reinterpret_cast<volatile long long*>(hw);
-        const long long nr = nedges / 2;
-        *nruns = nr;
-        if (nedges < 0) return done(ldg::lines_fail(LDG_ERR_CUDA, "ldg_sync_runs: run count not written"));
-        if (nr > cap || nedges > ecap)
-            return done(ldg::lines_fail(LDG_ERR_RANGE, "ldg_sync_runs: more runs than cap"));
-        return done(LDG_OK);
+    const bool mapped = drs && drl && drm;
+    if (mapped) {
+        run_pair_kernel<<<4 * 148, 256, 0, st>>>(edges, total, cap, d05, min_long, trim_lo, trim_hi,
+                                                 static_cast<long long*>(drs), static_cast<long long*>(drl),
+                                                 static_cast<double*>(drm), dw);
+    } else {
+        run_pair_kernel<<<4 * 148, 256, 0, st>>>(edges, total, cap, d05, min_long, trim_lo, trim_hi, rs, rl, rm,
+                                                 dw);
     }
-    long long nedges = 0;
-    if (cudaMemcpyAsync(&nedges, total, sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-        return cuda_fail("run count");
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) return cuda_fail("scan");
+    if (vhw[1] != 0) {
+        ldg::ctx_scan_invalidate(c);
+        return done(ldg::lines_fail(LDG_ERR_CUDA, "ldg_sync_runs: a tile's look-back wait timed out"));
+    }
+    const long long nedges = vhw[0];
+    if (nedges < 0) return cuda_fail("run count not written");
     const long long nr = nedges / 2;
     *nruns = nr;
     if (nr > cap || nedges > ecap) return done(ldg::lines_fail(LDG_ERR_RANGE, "ldg_sync_runs: more runs than cap"));
-    if (nr > 0) {
+    if (!mapped && nr > 0) {
         if (cudaMemcpyAsync(run_start, rs, nr * sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaMemcpyAsync(run_len, rl, nr * sizeof(long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaMemcpyAsync(run_mean, rm, nr * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
