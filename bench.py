@@ -373,6 +373,10 @@ def run_gpu(args):
                     io["efm"][o0:o1].copy_(bs.outs["efm"][o0:o1], non_blocking=True)
         marks["demod_end"] = evs[-1]
         bs.demod_done = evs[-1]
+        if io is not None and edges_mode:
+            # stream E holds the next step's crossings by the time this step
+            # finishes: the set's reuse waits for its own only
+            bs.edges_done = bs.eevs[-1]
         return evs
 
     def step_finish(io, bs, evs, overlap):
@@ -448,11 +452,14 @@ def run_gpu(args):
             # the next step (on the other buffer set) starts its demod while
             # this step's line locations, TBC and copies finish
             bs.done = []
-            for st_ in ([streamB, streamC, streamS, streamA] + ([streamD, streamP, streamE] if io is not None else [])):
+            for st_ in ([streamB, streamC, streamS, streamA] + ([streamD, streamP] if io is not None else [])):
                 e = torch.cuda.Event()
                 e.record(st_)
                 bs.done.append(e)
                 streamJ.wait_event(e)
+            if io is not None and edges_mode:
+                bs.done.append(bs.edges_done)
+                streamJ.wait_event(bs.edges_done)
             end.record(streamJ)
         else:
             stream.wait_stream(streamB)
