@@ -78,31 +78,44 @@ __device__ __forceinline__ void load_stage_tables(float2* t1, float2* t2, float2
     }
 }
 
-// w[q] = W^(j q), q = 0..15, from W^j, W^2j, W^4j, W^8j (conjugated for the inverse)
-template <bool INV>
-__device__ __forceinline__ void group_twiddles(float2 (&w)[16], const float2* tab, int stride, int j) {
-    w[0] = make_float2(1.f, 0.f);
-    w[1] = tab[j];
-    w[2] = tab[stride + j];
-    w[4] = tab[2 * stride + j];
-    w[8] = tab[3 * stride + j];
+// The group's twiddles W^(j q), q = 1..15, from W^j, W^2j, W^4j, W^8j
+// (conjugated for the inverse) by at most three complex products, each
+// handed to mul(q, W^(j q)) as soon as it is formed, so that only W^j,
+// W^2j, W^4j, W^8j and W^3j stay live beside the 16 points.
+template <bool INV, class M>
+__device__ __forceinline__ void apply_twiddles(const float2* tab, int stride, int j, M&& mul) {
+    float2 w1 = tab[j], w2 = tab[stride + j], w4 = tab[2 * stride + j], w8 = tab[3 * stride + j];
     if (INV) {
-        w[1] = cconj(w[1]);
-        w[2] = cconj(w[2]);
-        w[4] = cconj(w[4]);
-        w[8] = cconj(w[8]);
+        w1 = cconj(w1);
+        w2 = cconj(w2);
+        w4 = cconj(w4);
+        w8 = cconj(w8);
     }
-    w[3] = cmul(w[2], w[1]);
-    w[5] = cmul(w[4], w[1]);
-    w[6] = cmul(w[4], w[2]);
-    w[7] = cmul(w[4], w[3]);
-    w[9] = cmul(w[8], w[1]);
-    w[10] = cmul(w[8], w[2]);
-    w[11] = cmul(w[8], w[3]);
-    w[12] = cmul(w[8], w[4]);
-    w[13] = cmul(w[8], w[5]);
-    w[14] = cmul(w[8], w[6]);
-    w[15] = cmul(w[8], w[7]);
+    mul(1, w1);
+    mul(2, w2);
+    mul(4, w4);
+    mul(8, w8);
+    const float2 w3 = cmul(w2, w1);
+    mul(3, w3);
+    {
+        const float2 w5 = cmul(w4, w1);
+        mul(5, w5);
+        mul(13, cmul(w8, w5));
+    }
+    {
+        const float2 w6 = cmul(w4, w2);
+        mul(6, w6);
+        mul(14, cmul(w8, w6));
+    }
+    {
+        const float2 w7 = cmul(w4, w3);
+        mul(7, w7);
+        mul(15, cmul(w8, w7));
+    }
+    mul(9, cmul(w8, w1));
+    mul(10, cmul(w8, w2));
+    mul(11, cmul(w8, w3));
+    mul(12, cmul(w8, w4));
 }
 
 // How far the barrier at the end of a stage reaches.
@@ -158,18 +171,14 @@ __device__ __noinline__ void stage16(float2* S, const Twiddles& tw, const LD& ld
     // butterfly), so they are not live across it
     const float2* tab = L == 1024 ? tw.t1 : L == 64 ? tw.t2 : tw.t3;
     constexpr int stride = L == 1024 ? 1024 : L == 64 ? 64 : 4;
-    if (INV) {
-        float2 w[16];
-        group_twiddles<INV>(w, tab, stride, j);
-#pragma unroll
-        for (int r = 1; r < 16; ++r) v[r] = cmul(v[r], w[r]);
-    }
+    if (INV) apply_twiddles<INV>(tab, stride, j, [&](int q, float2 w) { v[q] = cmul(v[q], w); });
     dft_dif<16, INV>(v);  // v[i] = Y[bitrev(i)]
     if (!INV) {
-        float2 w[16];
-        group_twiddles<INV>(w, tab, stride, j);
-#pragma unroll
-        for (int i = 1; i < 16; ++i) v[i] = cmul(v[i], w[bitrev(i, 4)]);
+        // v[i] holds bin bitrev(i): it takes W^(j bitrev(i))
+        apply_twiddles<INV>(tab, stride, j, [&](int q, float2 w) {
+            const int i = bitrev(q, 4);
+            v[i] = cmul(v[i], w);
+        });
     }
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
