@@ -16,6 +16,8 @@
 //                      optional float32 rounding (the reference's own cast),
 //                      16-tap windowed-sinc gather with linear interpolation
 //                      between LUT phases, level adjust, uint16 conversion.
+#include <climits>
+
 #include "ldg_tbc.cuh"
 
 namespace ldg {
@@ -654,6 +656,56 @@ __device__ __forceinline__ double pixel_coord(const TbcField& f, long long ig, i
 // span and its 128 bytes of LUT are each one contiguous access; the 8
 // partial sums meet in a transposing reduction (lane k of group g ends with
 // pixel 4k + g) and one shuffle takes each pixel's sum to its own lane.
+// One lane's share of a pixel: taps 2k and 2k+1 of the 16 starting at
+// buf[st], weights from LUT phase ps (the interleaved float4 of w and the
+// next-phase difference) at fraction alpha; float32 products, FP64 sum.
+__device__ __forceinline__ double two_taps(const float* buf, const float* lut, int st, int ps, float alpha, int k) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(lut + (size_t)ps * 32) + k);
+    const float* in = buf + st + 2 * k;
+    const float x0 = __ldg(in), x1 = __ldg(in + 1);
+    const float w0 = fmaf(alpha, q.z, q.x), w1 = fmaf(alpha, q.w, q.y);
+    return (double)(x0 * w0) + (double)(x1 * w1);
+}
+
+// Sum over a group's 8 lanes of their shares of the group's 8 pixels
+// (share(p): this lane's share of pixel p), as a transposing reduction: at
+// each level a lane keeps half of its pixels and adds the partner's shares
+// of them, so lane k ends with the whole sum of pixel k.  The shares are
+// formed in the order the reduction consumes them (pixels j and j + 4, for
+// j = 0, 2, 1, 3), so at most two partial sums are live beside them.
+template <class S>
+__device__ __forceinline__ double group_sum(int k, S&& share) {
+    const bool h4 = (k & 4) != 0, h2 = (k & 2) != 0, h1 = (k & 1) != 0;
+    double b2[2];
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj) {
+        double b4[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int j = jj + 2 * h;
+            const double a = share(j), c = share(j + 4);
+            b4[h] = (h4 ? c : a) + __shfl_xor_sync(0xffffffffu, h4 ? a : c, 4);
+        }
+        b2[jj] = (h2 ? b4[1] : b4[0]) + __shfl_xor_sync(0xffffffffu, h2 ? b4[0] : b4[1], 2);
+    }
+    return (h1 ? b2[1] : b2[0]) + __shfl_xor_sync(0xffffffffu, h1 ? b2[0] : b2[1], 1);
+}
+
+// The gather's shares with each pixel's first tap and phase in separate
+// shuffles (phase -1: a pixel left at 0), for warps whose first taps do not
+// fit 16-bit offsets.
+__device__ __noinline__ void gather_unpacked(const float* buf, const float* lut, int sti, int psi, float alpha, int grp,
+                                             int k, double* acc) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int src = 4 * p + grp;
+        const int pst = __shfl_sync(0xffffffffu, sti, src);
+        const int pps = __shfl_sync(0xffffffffu, psi, src);
+        const float pal = __shfl_sync(0xffffffffu, alpha, src);
+        acc[p] = pps >= 0 ? two_taps(buf, lut, pst, pps, pal, k) : 0.0;
+    }
+}
+
 __global__ void __launch_bounds__(kGatherThreads, 8) tbc_gather_kernel(const TbcField* fields, const float* lut,
                                                                     int nfields) {
     const int fi = blockIdx.y;
@@ -685,44 +737,32 @@ __global__ void __launch_bounds__(kGatherThreads, 8) tbc_gather_kernel(const Tbc
     // first tap as a 32-bit offset (buf_len < 2^31); phase -1 marks a pixel left at 0
     const int sti = ok ? (int)st : 0;
     const int psi = ok ? ps : -1;
-    double acc[8];  // this lane's two-tap share of each of the group's 8 pixels
-#pragma unroll
-    for (int p = 0; p < 8; ++p) {
-        // the group's p-th pixel: at each step the four groups take four
-        // adjacent pixels, whose 16-tap windows overlap (fewer cache lines
-        // per tap load)
-        const int src = 4 * p + grp;
-        const int pst = __shfl_sync(0xffffffffu, sti, src);
-        const int pps = __shfl_sync(0xffffffffu, psi, src);
-        const float pal = __shfl_sync(0xffffffffu, alpha, src);
-        double part = 0.0;
-        if (pps >= 0) {
-            const float4 q = __ldg(reinterpret_cast<const float4*>(lut + (size_t)pps * 32) + k);
-            const float* in = f.buf + pst + 2 * k;
-            const float x0 = __ldg(in), x1 = __ldg(in + 1);
-            const float w0 = fmaf(pal, q.z, q.x), w1 = fmaf(pal, q.w, q.y);
-            part = (double)(x0 * w0) + (double)(x1 * w1);
-        }
-        acc[p] = part;
+    // The 32 pixels' first taps lie within a few hundred samples of each
+    // other: as offsets from the warp's lowest one they fit 16 bits, and
+    // each pixel's offset and phase travel in one shuffle instead of two
+    // (the shuffles share the load pipe's writeback with the tap loads).
+    // 0xffff as the offset marks a pixel left at 0.
+    const int low = __reduce_min_sync(0xffffffffu, ok ? sti : INT_MAX);
+    const bool packed = __all_sync(0xffffffffu, !ok || sti - low < 0xffff);
+    const unsigned pk = ok ? ((unsigned)(sti - low) << 16) | (unsigned)ps : 0xffff0000u;
+    double held;  // after the group sum: the whole sum of pixel 4 k + grp
+    if (packed) {
+        held = group_sum(k, [&](int p) {
+            // the group's p-th pixel: at each step the four groups take four
+            // adjacent pixels, whose 16-tap windows overlap (fewer cache lines
+            // per tap load)
+            const int src = 4 * p + grp;
+            const unsigned q = __shfl_sync(0xffffffffu, pk, src);
+            const float pal = __shfl_sync(0xffffffffu, alpha, src);
+            return (q >> 16) != 0xffffu ? two_taps(f.buf, lut, low + (int)(q >> 16), (int)(q & 0xffffu), pal, k)
+                                        : 0.0;
+        });
+    } else {
+        double wide[8];  // first taps too far apart for 16-bit offsets (wild line locations): rare
+        gather_unpacked(f.buf, lut, sti, psi, alpha, grp, k, wide);
+        held = group_sum(k, [&](int p) { return wide[p]; });
     }
-    // transposing reduction over the group's 8 lanes: at each step a lane
-    // keeps half of its pixels and adds the partner's shares of them, so lane
-    // k ends with the whole sum of the group's k-th pixel
-    double b4[4], b2[2];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const bool hi = (k & 4) != 0;
-        b4[j] = (hi ? acc[j + 4] : acc[j]) + __shfl_xor_sync(0xffffffffu, hi ? acc[j] : acc[j + 4], 4);
-    }
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-        const bool hi = (k & 2) != 0;
-        b2[j] = (hi ? b4[j + 2] : b4[j]) + __shfl_xor_sync(0xffffffffu, hi ? b4[j] : b4[j + 2], 2);
-    }
-    const bool hi1 = (k & 1) != 0;
-    // lane k of group g now holds the sum of pixel 4 k + g; pixel `lane` is
-    // at lane 8 (lane % 4) + lane / 4
-    const double held = (hi1 ? b2[1] : b2[0]) + __shfl_xor_sync(0xffffffffu, hi1 ? b2[0] : b2[1], 1);
+    // pixel `lane` is at lane 8 (lane % 4) + lane / 4
     const double mine = __shfl_sync(0xffffffffu, held, 8 * (lane & 3) + (lane >> 2));
     double level;
     if (f.spline_k >= 2) {
