@@ -84,6 +84,26 @@ def test_tbc_fp64_matches_oracle(case):
     assert d.max() <= 1 and np.mean(d <= 1) >= 0.9999
 
 
+def test_tbc_wide_first_taps(case):
+    """A field whose line 100 spans 2.4 M samples: 32 consecutive pixels of
+    that line start their taps more than 65535 samples apart, which the
+    gather handles by its separate path (first taps and phases shuffled one
+    by one); the picture still equals the FP64 oracle's."""
+    rf, g, cap, w, buf = case
+    stretch = 2_400_000
+    long_buf = np.concatenate([buf, np.tile(buf, stretch // len(buf) + 2)]).astype(np.float32)
+    ll = np.array(g["f0_linelocs"], dtype=np.float64)
+    ll[101:] += stretch
+    g2 = dict(g)
+    g2["f0_linelocs"] = ll
+    f = _field(rf, g2, long_buf, coord_f32=False)
+    pic, _, _ = f.downscale(linesout=f.outlinecount, final=True)
+    _, opic = _oracle_picture(rf, g2, long_buf, coord_f32=False)
+    d = np.abs(pic.astype(int) - opic.astype(int))
+    print(rf.system, "wide first taps vs oracle: max", d.max(), "within1", np.mean(d <= 1))
+    assert d.max() <= 1 and np.mean(d <= 1) >= 0.9999
+
+
 def test_demod_plus_tbc_end_to_end(case):
     """GPU demod of the field's blocks, then GPU TBC, vs the FP64 oracle."""
     import torch
