@@ -48,12 +48,11 @@ from ldgpu.replicas import barrier as replica_barrier  # noqa: E402
 from ldgpu.replicas import capture_seed, dist_env, max_over_ranks  # noqa: E402
 
 METRIC = "RF MSPS demod+TBC on 1 B200 (batched FP32 vs plain) + HBM roofline %"
-BYTES_PER_SAMPLE_DEMOD = 2 + 4 * 4 + 4 + 2  # input + 4 video f32 + rfhpf f32 + efm i16 (per output sample)
-AUDIO_BYTES_PER_BLOCK = 2 * 991 * 4
 # DRAM bytes (read + write) per block of the demod kernel, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the NTSC 1 s case divided by
-# its 1261 blocks; traffic scales with blocks.  None until measured.
-DRAM_BYTES_PER_BLOCK = 980_500
+# its 1261 blocks; traffic scales with blocks.  NTSC only (PAL writes a fifth
+# float32 output and was not captured).
+DRAM_BYTES_PER_BLOCK = {"NTSC": 980_500}
 
 
 def parse():
@@ -752,11 +751,14 @@ def run_gpu(args):
                                                                d_drops.data_ptr(), d_counts.data_ptr(), None, sh)))
 
     peak, peak_kind = peaks()
-    demod_bytes = nout * BYTES_PER_SAMPLE_DEMOD + nblocks * AUDIO_BYTES_PER_BLOCK
+    # algorithmic bytes: the int16 input once, every output array once (NTSC:
+    # 4 float32 video outputs + rfhpf + int16 EFM = 24 B per sample, PAL 28 B,
+    # plus the two audio bands' 991 float32 per block)
+    demod_bytes = nout * 2 + sum(v.numel() * v.element_size() for v in outs.values())
     achieved = demod_bytes / (dmed * 1e-3) / 1e9
     # TBC: uint16 field written + the demod span of the field read once
     tbc_bytes = nf * fsz * 2 + sum(int(ll[-1] - ll[0]) * 4 for (_, ll, _, _) in fields)
-    traffic = DRAM_BYTES_PER_BLOCK * nblocks if DRAM_BYTES_PER_BLOCK else None
+    traffic = DRAM_BYTES_PER_BLOCK[system] * nblocks if system in DRAM_BYTES_PER_BLOCK else None
 
     cpu = accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu:
