@@ -262,7 +262,10 @@ def run_gpu(args):
     # analog audio of finished ranges: high priority too, since the range's
     # copies out wait for it and the buffer set's next demod waits for those
     streamA = torch.cuda.Stream(priority=-1)
-    streamE = torch.cuda.Stream()              # EFM zero crossings of each demodulated chunk (end to end)
+    # EFM zero crossings of each demodulated chunk (end to end): high priority
+    # too -- at the demod's priority each of its three launches waited for a
+    # whole demod chunk to be dispatched, and the step's end waits for them
+    streamE = torch.cuda.Stream(priority=-1)
     do_audio = not args.no_analog_audio
     elem = {k: v.element_size() for k, v in outs.items()}
     per_block = {k: (991 if k.startswith("audio") else U) for k in outs}
@@ -354,7 +357,7 @@ def run_gpu(args):
             evs.append(ev)
             if io is not None and edges_mode:
                 # the chunk's EFM zero crossings (stream E, beside the next
-                # chunk's demod and off the line-location streams); the count
+                # chunk's demod and off the sync-run scan's stream); the count
                 # lands in pinned memory and is read when the copy is issued
                 streamE.wait_event(ev)
                 base = bounds[c] * U
