@@ -81,6 +81,11 @@ def parse():
                     help="pipeline chunks of blocks per step (1: demod, then line locations, then TBC)")
     ap.add_argument("--chunk-taper", type=float, default=0.7,
                     help="chunk c gets a share of the blocks proportional to taper**c")
+    ap.add_argument("--e2e-chunks", type=int, default=5,
+                    help="end to end: pipeline chunks per step")
+    ap.add_argument("--e2e-first", type=float, default=0.5,
+                    help="end to end: the first chunk's share relative to the taper's (< 1: the first "
+                         "demod starts sooner after the capture's copy begins)")
     ap.add_argument("--wow-interp", default="linear", choices=["linear", "quadratic", "cubic"],
                     help="Field.wow_interpolation_method of the TBC (the reference's default is linear)")
     ap.add_argument("--wow-smoothing", type=float, default=0.0,
@@ -244,18 +249,26 @@ def run_gpu(args):
                                      farr={k: o[k] for k in fkeys}, loc=LineLocator(rf), pics=None, aud=None,
                                      done=None)
     levels = field_levels(rf)
-    nchunks = max(1, min(args.chunks, nblocks // 64))
     lib = L.load()
-    # chunk c holds a share proportional to taper**c of the blocks: a smaller
-    # last chunk shortens the tail (its line locations and TBC) after the demod
-    w = [args.chunk_taper ** c for c in range(nchunks)]
-    cum = np.concatenate([[0.0], np.cumsum(w)]) / sum(w)
-    bounds = [int(round(x * nblocks)) for x in cum]
-    # end to end, the EFM output as its zero crossings: room per chunk for
-    # one crossing per 4 samples (band-limited EFM crosses every ~25)
     edges_mode = not args.no_e2e and args.e2e_efm == "edges"
-    ecap = np.array([(bounds[c + 1] - bounds[c]) * U // 4 for c in range(nchunks)], np.int64)
-    eoff = np.concatenate([[0], np.cumsum(ecap)[:-1]]).astype(np.int64)
+
+    def chunk_plan(n, taper, first=1.0):
+        """The step's chunks: chunk c holds a share proportional to taper**c
+        of the blocks (the first's scaled by `first`) -- a smaller last chunk
+        shortens the tail (its line locations and TBC) after the demod; end to
+        end, the EFM output as its zero crossings: room per chunk for one
+        crossing per 4 samples (band-limited EFM crosses every ~25)."""
+        nonlocal nchunks, bounds, ecap, eoff
+        nchunks = max(1, min(n, nblocks // 64))
+        w = [taper ** c for c in range(nchunks)]
+        w[0] *= first
+        cum = np.concatenate([[0.0], np.cumsum(w)]) / sum(w)
+        bounds = [int(round(x * nblocks)) for x in cum]
+        ecap = np.array([(bounds[c + 1] - bounds[c]) * U // 4 for c in range(nchunks)], np.int64)
+        eoff = np.concatenate([[0], np.cumsum(ecap)[:-1]]).astype(np.int64)
+
+    nchunks = bounds = ecap = eoff = None
+    chunk_plan(args.chunks, args.chunk_taper)
     streamB = torch.cuda.Stream(priority=-1)   # line locations
     streamC = torch.cuda.Stream(priority=-1)   # TBC of ranges whose line locations are final
     streamS = torch.cuda.Stream(priority=-1)   # sync-run scans
@@ -484,11 +497,15 @@ def run_gpu(args):
     alt.cap.copy_(cap)
     alt.pics = torch.empty(nf * fsz, dtype=torch.uint16, device="cuda")
     alt.aud = torch.zeros(nf * AS, dtype=torch.int16, device="cuda")
-    for bs_ in (main, alt):
-        bs_.edges = torch.empty(8 * int(ecap.sum()) if edges_mode else 8, dtype=torch.uint8, device="cuda")
-        bs_.eevs = [None] * nchunks
-        bs_.escratch = torch.empty(max(int(L.load().ldg_efm_edges_scratch_bytes((bounds[c + 1] - bounds[c]) * U))
-                                       for c in range(nchunks)), dtype=torch.uint8, device="cuda")
+    def edge_buffers():
+        # the sets' crossing buffers for the current chunk plan
+        for bs_ in (main, alt):
+            bs_.edges = torch.empty(8 * int(ecap.sum()) if edges_mode else 8, dtype=torch.uint8, device="cuda")
+            bs_.eevs = [None] * nchunks
+            bs_.escratch = torch.empty(max(int(L.load().ldg_efm_edges_scratch_bytes((bounds[c + 1] - bounds[c]) * U))
+                                           for c in range(nchunks)), dtype=torch.uint8, device="cuda")
+
+    edge_buffers()
 
     def barrier():
         replica_barrier(world)
@@ -580,6 +597,11 @@ def run_gpu(args):
     e2e = None
     if not args.no_e2e:
         host_cap = cap.cpu().pin_memory()
+        # end to end the chunks may differ: the first chunk's input copy
+        # precedes any demod, so a smaller first chunk starts the pipeline sooner
+        dr_plan = (nchunks, bounds, ecap, eoff)
+        chunk_plan(args.e2e_chunks or args.chunks, args.chunk_taper, args.e2e_first)
+        edge_buffers()
 
         def make_io():
             io = {"cap": host_cap,
@@ -684,6 +706,8 @@ def run_gpu(args):
         pcie["d2h_gbs"] = (nf * fsz * 2 + efm_d2h) / pcie["d2h_ms"] / 1e6
         e2e["pcie_alone"] = pcie
         e2e["host_ms_per_step"] = e2e_host_ms  # the host's own loop (it returns before the GPU finishes)
+        e2e["chunks"] = {"n": nchunks, "taper": args.chunk_taper, "first_share": round(bounds[1] / nblocks, 3)}
+        nchunks, bounds, ecap, eoff = dr_plan
 
     # ---- plain form: one demodblock() call per block through the Python API
     plain = None
