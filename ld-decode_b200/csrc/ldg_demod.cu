@@ -700,11 +700,19 @@ __device__ __forceinline__ void demod_block_ip(const DemodParams& p, int blk, fl
             A[ch * padded(1024) + pad(k)] = make_float2(0.f, 0.f);
         }
     }
-    {
-        AudioTaps au{A, {p.a_lowbin[0], p.a_lowbin[1]}, {p.a_filt1[0], p.a_filt1[1]}};
-        post_r2c_ip(S, p.tw_pair, parkX, p.o_rfhpf ? p.fp_rfhpf : nullptr, p.audio ? &au : nullptr);
-    }
+    post_r2c_ip(S, p.tw_pair, parkX, p.o_rfhpf ? p.fp_rfhpf : nullptr, nullptr);
     __syncthreads();
+    if (p.audio) {
+        // the audio bands' bins, gathered from the parked spectrum (before the
+        // notch, as the taps in post_r2c of the Stockham form): one L2 load per
+        // thread instead of a band test in every bin pair's post-processing
+        for (int idx = threadIdx.x; idx < 2 * 513; idx += kThreads) {
+            const int ch = idx >= 513, rel = idx - 513 * ch;
+            const float2 x = parkX[ip::pos_of(p.a_lowbin[ch] + rel)];
+            A[ch * padded(1024) + pad(rel)] = cmul(rel < 512 ? x : cconj(x), __ldg(p.a_filt1[ch] + rel));
+        }
+        __syncthreads();
+    }
     if (p.notch_hi > p.notch_lo) {
         notch_park_ip(parkX, p.notch_lo, p.notch_hi);
         __syncthreads();
