@@ -81,8 +81,8 @@ def parse():
                     help="pipeline chunks of blocks per step (1: demod, then line locations, then TBC)")
     ap.add_argument("--chunk-taper", type=float, default=0.7,
                     help="chunk c gets a share of the blocks proportional to taper**c")
-    ap.add_argument("--e2e-chunks", type=int, default=5,
-                    help="end to end: pipeline chunks per step")
+    ap.add_argument("--e2e-chunks", type=int, default=None,
+                    help="end to end: pipeline chunks per step (default: --chunks)")
     ap.add_argument("--e2e-first", type=float, default=0.5,
                     help="end to end: the first chunk's share relative to the taper's (< 1: the first "
                          "demod starts sooner after the capture's copy begins)")
