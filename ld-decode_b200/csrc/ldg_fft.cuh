@@ -186,7 +186,7 @@ struct SmemIO {};
 // of line so each pass gets the whole 64-register budget (inlined into the
 // demod kernel, live state around the passes made the allocator spill).
 template <int R, int M, int NB, int Ns, bool INV, class LD, class ST>
-__device__ __noinline__ void stockham_pass(float2* S, const Tables& t, const LD& ld, const ST& st) {
+__device__ __noinline__ void stockham_pass(float2* S, const Tables t, const LD ld, const ST st) {
     constexpr int B = M / R;                       // butterflies per set
     constexpr int BT = B * NB;                     // butterflies per pass
     constexpr int PER = (BT + kThreads - 1) / kThreads;

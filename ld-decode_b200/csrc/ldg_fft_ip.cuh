@@ -139,7 +139,7 @@ __device__ __forceinline__ void stage_sync() {
 // input ld(0, n); ST (last inverse stage, L = 1024) takes the natural-order
 // output st(0, n, v) instead of shared memory.  Ends with a barrier of reach SY.
 template <int L, bool INV, int SY, class LD, class ST>
-__device__ __noinline__ void stage16(float2* S, const Twiddles& tw, const LD& ld, const ST& st) {
+__device__ __noinline__ void stage16(float2* S, const Twiddles tw, const LD ld, const ST st) {
     static_assert(L == 1024 || L == 64 || L == 4, "stride");
     constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
     constexpr bool to_smem = std::is_same<ST, SmemIO>::value;
@@ -202,7 +202,7 @@ __device__ __noinline__ void stage16(float2* S, const Twiddles& tw, const LD& ld
 // that a warp reads one contiguous kilobyte per step; that order needs the
 // whole CTA's barrier (SY is then kSyncCta).  Ends with a barrier of reach SY.
 template <bool INV, int SY, class LD>
-__device__ __noinline__ void stage4(float2* S, const LD& ld) {
+__device__ __noinline__ void stage4(float2* S, const LD ld) {
     constexpr bool from_smem = std::is_same<LD, SmemIO>::value;
     static_assert(from_smem || SY == kSyncCta, "the loader order spans the CTA");
 #pragma unroll
