@@ -53,7 +53,7 @@ __device__ __forceinline__ float tap_sum(const float* u, long long ulo, long lon
     return acc;
 }
 
-__global__ void __launch_bounds__(kAc3Threads) ac3_frontend_kernel(const Ac3Params p) {
+__global__ void __launch_bounds__(kAc3Threads) ac3_frontend_kernel(const __grid_constant__ Ac3Params p) {
     extern __shared__ float sm[];
     const Ac3Taps& t = p.taps;
     const long long J = p.out_first + (long long)blockIdx.x * kTile;

@@ -701,7 +701,7 @@ __device__ void pilot_pass(const LineParams& P, double* ll, const float* pilot, 
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(LineParams P) {
+__global__ void __launch_bounds__(kLineThreads) lines_hsync_kernel(const __grid_constant__ LineParams P) {
     const int f = P.a.first_field + blockIdx.x;
     const ldg_lines_args& a = P.a;
     const long long base = a.startloc[f];
@@ -1060,7 +1060,7 @@ struct BurstSpec {
 
 // Round `round` (1 .. kBurstRounds): one CTA per field of the range, seeded
 // with 0 (round 1) or with the previous round's median of the field before.
-__global__ void __launch_bounds__(kBurstThreads) burst_round_kernel(LineParams P, int round, BurstSpec B) {
+__global__ void __launch_bounds__(kBurstThreads) burst_round_kernel(const __grid_constant__ LineParams P, int round, const __grid_constant__ BurstSpec B) {
     __shared__ BurstSmem sm;
     const ldg_lines_args& a = P.a;
     const int f = a.first_field + blockIdx.x;
@@ -1093,7 +1093,7 @@ __global__ void __launch_bounds__(kBurstThreads) burst_round_kernel(LineParams P
 // right; a field it did not is computed again by the whole CTA.
 constexpr int kBurstScan = 512;
 
-__global__ void __launch_bounds__(kBurstThreads) burst_verify_kernel(LineParams P, BurstSpec B) {
+__global__ void __launch_bounds__(kBurstThreads) burst_verify_kernel(const __grid_constant__ LineParams P, const __grid_constant__ BurstSpec B) {
     __shared__ BurstSmem sm;
     __shared__ double s_seed2[kBurstScan], s_lo[kBurstScan], s_hi[kBurstScan], s_pam[kBurstScan];
     __shared__ unsigned char s_flags[kBurstScan];  // bit 0: has a previous field; bit 1: no interval
@@ -1154,7 +1154,7 @@ __global__ void __launch_bounds__(kBurstThreads) burst_verify_kernel(LineParams 
 // line 6's burst level against the field's median (present / absent / out of
 // both ranges) and the majority of rising lines, or is the previous ID + 1
 // when that evidence is missing or split.
-__global__ void __launch_bounds__(32) pal_sequence_kernel(LineParams P) {
+__global__ void __launch_bounds__(32) pal_sequence_kernel(const __grid_constant__ LineParams P) {
     const ldg_lines_args& a = P.a;
     const int f0 = a.first_field, f1 = a.first_field + a.count;
     const int j = threadIdx.x;
@@ -1226,7 +1226,7 @@ __global__ void __launch_bounds__(32) pal_sequence_kernel(LineParams P) {
 }
 
 // NTSC: refine_linelocs_burst's application, fix_badlines, subcarrier shift
-__global__ void __launch_bounds__(512) burst_apply_kernel(LineParams P, double shift) {
+__global__ void __launch_bounds__(512) burst_apply_kernel(const __grid_constant__ LineParams P, double shift) {
     const int f = P.a.first_field + blockIdx.x;
     const ldg_lines_args& a = P.a;
     const int nl = a.proclines;

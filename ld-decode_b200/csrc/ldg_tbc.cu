@@ -691,19 +691,18 @@ __device__ __forceinline__ double group_sum(int k, S&& share) {
     return (h1 ? b2[1] : b2[0]) + __shfl_xor_sync(0xffffffffu, h1 ? b2[0] : b2[1], 1);
 }
 
-// The gather's shares with each pixel's first tap and phase in separate
-// shuffles (phase -1: a pixel left at 0), for warps whose first taps do not
-// fit 16-bit offsets.
-__device__ __noinline__ void gather_unpacked(const float* buf, const float* lut, int sti, int psi, float alpha, int grp,
-                                             int k, double* acc) {
-#pragma unroll
-    for (int p = 0; p < 8; ++p) {
+// The group sum with each pixel's first tap and phase in separate shuffles
+// (phase -1: a pixel left at 0), for warps whose first taps do not fit
+// 16-bit offsets.
+__device__ __noinline__ double gather_unpacked(const float* buf, const float* lut, int sti, int psi, float alpha,
+                                               int grp, int k) {
+    return group_sum(k, [&](int p) {
         const int src = 4 * p + grp;
         const int pst = __shfl_sync(0xffffffffu, sti, src);
         const int pps = __shfl_sync(0xffffffffu, psi, src);
         const float pal = __shfl_sync(0xffffffffu, alpha, src);
-        acc[p] = pps >= 0 ? two_taps(buf, lut, pst, pps, pal, k) : 0.0;
-    }
+        return pps >= 0 ? two_taps(buf, lut, pst, pps, pal, k) : 0.0;
+    });
 }
 
 __global__ void __launch_bounds__(kGatherThreads, 8) tbc_gather_kernel(const TbcField* fields, const float* lut,
@@ -758,9 +757,8 @@ __global__ void __launch_bounds__(kGatherThreads, 8) tbc_gather_kernel(const Tbc
                                         : 0.0;
         });
     } else {
-        double wide[8];  // first taps too far apart for 16-bit offsets (wild line locations): rare
-        gather_unpacked(f.buf, lut, sti, psi, alpha, grp, k, wide);
-        held = group_sum(k, [&](int p) { return wide[p]; });
+        // first taps too far apart for 16-bit offsets (wild line locations): rare
+        held = gather_unpacked(f.buf, lut, sti, psi, alpha, grp, k);
     }
     // pixel `lane` is at lane 8 (lane % 4) + lane / 4
     const double mine = __shfl_sync(0xffffffffu, held, 8 * (lane & 3) + (lane >> 2));
