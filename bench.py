@@ -52,7 +52,7 @@ METRIC = "RF MSPS demod+TBC on 1 B200 (batched FP32 vs plain) + HBM roofline %"
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the NTSC 1 s case divided by
 # its 1261 blocks; traffic scales with blocks.  NTSC only (PAL writes a fifth
 # float32 output and was not captured).
-DRAM_BYTES_PER_BLOCK = {"NTSC": 980_500}
+DRAM_BYTES_PER_BLOCK = {"NTSC": 719_500}
 
 
 def parse():
