@@ -568,8 +568,11 @@ typedef struct ldg_field_plan {
  * `cap`) and, for runs longer than min_long samples, the FP64 mean of
  * d05[start + trim_lo, start + len - trim_hi) (NaN otherwise).  A run still
  * open at the end of the array is not reported.  LDG_ERR_RANGE if more
- * than `cap` runs (*nruns then holds the count needed).  Synchronises
- * `stream`. */
+ * than `cap` runs (*nruns then holds the count needed).  Two kernels (a
+ * single-pass scan and the run pairing; pinned run arrays are written by
+ * the second directly); calls on one context are serialised and each
+ * synchronises `stream`; LDG_ERR_CUDA (the next call starts afresh) if a
+ * tile of the scan waited for its predecessors' counts past its bound. */
 int ldg_sync_runs(ldg_ctx* ctx, const float* d05, int64_t n, double threshold, int64_t min_long, int64_t trim_lo,
                   int64_t trim_hi, int64_t* run_start, int64_t* run_len, double* run_mean, int64_t cap,
                   int64_t* nruns, void* stream);
