@@ -371,7 +371,7 @@ __device__ __forceinline__ void discriminate(const DemodParams& p, int blk, cons
             parkX[m] = make_float2(fminf(fmaxf(de, 1500000.0f), clip_hi), fminf(fmaxf(dodd, 1500000.0f), clip_hi));
         };
         // two samples per step, the parked (L2) loads first
-#pragma unroll 1
+#pragma unroll 2
         for (int m = threadIdx.x; m < kM; m += 2 * kThreads) {
             const int mb = m + kThreads;
             const float2 zea = parkZ[m], zeb = parkZ[mb];
